@@ -1,0 +1,428 @@
+"""diagham_b200: DiagHam's on-the-fly H.v + Lanczos path on one B200.
+
+Python view of the C ABI in include/diagham_b200.h (libdiagham_b200.so, built in this directory by
+diagham_b200/_build.py).  Class and method names follow the reference classes they replace:
+
+    FermionOnSphere                     FQHE/src/HilbertSpace/FermionOnSphere.h
+    Spin1_2Chain                        Spin/src/HilbertSpace/Spin1_2Chain.h
+    ParticleOnSphereGenericHamiltonian  FQHE/src/Hamiltonian/ParticleOnSphereGenericHamiltonian.h
+    SpinChainJ1J2Hamiltonian            (J1-J2 pattern of SpinChainJ1J2RealHamiltonianWithTranslations on a plain chain)
+    BasicLanczosAlgorithm, FullReorthogonalizedLanczosAlgorithm, BasicLanczosAlgorithmWithGroundState
+                                        src/LanczosAlgorithm/*.h
+
+Vectors are FP64 numpy arrays (host) or torch CUDA tensors (used in place).  Every call goes to
+the GPU; there is no CPU fallback: importing without the built library raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libdiagham_b200.so")
+
+DH_OK = 0
+DH_INDEX_RANK = 0
+DH_INDEX_LOOKUP = 1
+DH_PRECISION_FP64 = 0
+DH_PRECISION_FP32 = 1
+DH_LANCZOS_BASIC = 0
+DH_LANCZOS_FULL_REORTHOGONALIZED = 1
+DH_LANCZOS_BLOCK = 2
+DH_LANCZOS_WITH_GROUND_STATE = 3
+
+# every exported entry point with its argument types (restype int unless stated)
+_c_int, _c_dbl, _c_i64, _c_u64, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_int64, ctypes.c_uint64, ctypes.c_void_p
+_ip = ctypes.POINTER(ctypes.c_int)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+SIGNATURES = {
+    "dh_last_error": ([], ctypes.c_char_p),
+    "dh_version": ([], ctypes.c_char_p),
+    "dh_device_count": ([_ip], _c_int),
+    "dh_fermion_on_sphere_create": ([_c_int, _c_int, _c_int, ctypes.c_ulong, _vp], _c_int),
+    "dh_spin12_chain_create": ([_c_int, _c_int, _c_int, _vp], _c_int),
+    "dh_space_destroy": ([_vp], _c_int),
+    "dh_space_get_dimension": ([_vp, _i64p], _c_int),
+    "dh_space_get_states": ([_vp, _vp, _vp, _c_i64, _c_i64], _c_int),
+    "dh_space_find_state_index": ([_vp, _vp, _c_i64, _vp], _c_int),
+    "dh_space_set_index_mode": ([_vp, _c_int], _c_int),
+    "dh_particle_on_sphere_generic_hamiltonian_create": ([_vp, _c_int, _c_int, _vp, _c_dbl, _vp], _c_int),
+    "dh_spin_chain_j1j2_hamiltonian_create": ([_vp, _c_dbl, _c_dbl, _vp], _c_int),
+    "dh_hamiltonian_destroy": ([_vp], _c_int),
+    "dh_hamiltonian_get_dimension": ([_vp, _i64p], _c_int),
+    "dh_hamiltonian_shift": ([_vp, _c_dbl], _c_int),
+    "dh_hamiltonian_set_precision": ([_vp, _c_int], _c_int),
+    "dh_hamiltonian_set_pseudopotentials": ([_vp, _vp], _c_int),
+    "dh_hamiltonian_set_stream": ([_vp, _vp], _c_int),
+    "dh_hamiltonian_low_level_add_multiply": ([_vp, _vp, _vp, _c_i64, _c_i64], _c_int),
+    "dh_hamiltonian_low_level_multiply": ([_vp, _vp, _vp, _c_i64, _c_i64], _c_int),
+    "dh_hamiltonian_low_level_multiple_add_multiply": ([_vp, _vp, _vp, _c_int, _c_i64, _c_i64], _c_int),
+    "dh_hamiltonian_matrix_element": ([_vp, _vp, _vp, _vp], _c_int),
+    "dh_hamiltonian_row_elements": ([_vp, _c_i64, _vp, _vp, _vp, _c_int, _ip], _c_int),
+    "dh_hamiltonian_pseudopotential_adjoint": ([_vp, _vp, _vp, _vp], _c_int),
+    "dh_hamiltonian_get_interaction_factors": ([_vp, _vp, _c_int, _ip], _c_int),
+    "dh_lanczos_create": ([_vp, _c_int, _c_int, _c_int, _c_int, _vp], _c_int),
+    "dh_lanczos_destroy": ([_vp], _c_int),
+    "dh_lanczos_set_eigenvalue_precision": ([_vp, _c_dbl], _c_int),
+    "dh_lanczos_initialize": ([_vp, _vp, _c_int], _c_int),
+    "dh_lanczos_initialize_random": ([_vp, _c_u64], _c_int),
+    "dh_lanczos_run": ([_vp, _c_int], _c_int),
+    "dh_lanczos_test_convergence": ([_vp, _ip], _c_int),
+    "dh_lanczos_get_eigenvalues": ([_vp, _vp, _c_int], _c_int),
+    "dh_lanczos_get_ground_state_energy": ([_vp, _vp], _c_int),
+    "dh_lanczos_get_ground_state": ([_vp, _vp], _c_int),
+    "dh_lanczos_get_counters": ([_vp, _i64p, _ip], _c_int),
+    "dh_lanczos_solve": ([_vp, _c_int, _c_int, _vp, _ip, _ip], _c_int),
+    "dh_lanczos_solve_refined": ([_vp, _c_int, _c_dbl, _vp], _c_int),
+    "dh_coulomb_pseudopotentials": ([_c_int, _vp], _c_int),
+    "dh_clebsch_gordan": ([_c_int, _c_int, _c_int, _c_int, _c_int, _vp], _c_int),
+}
+
+_lib = None
+
+
+class DiagHamError(RuntimeError):
+    pass
+
+
+def library_path():
+    return _LIB_PATH
+
+
+def load(path=None):
+    """Load libdiagham_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or _LIB_PATH
+    if not os.path.exists(p):
+        raise DiagHamError("libdiagham_b200.so is not built: run python -m diagham_b200._build (or __graft_entry__.build())")
+    lib = ctypes.CDLL(p)
+    for name, (args, res) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+def _check(rc):
+    if rc != DH_OK:
+        msg = _lib.dh_last_error().decode(errors="replace")
+        raise DiagHamError("error %d: %s" % (rc, msg))
+
+
+def version():
+    return load().dh_version().decode()
+
+
+def device_count():
+    n = ctypes.c_int(0)
+    _check(load().dh_device_count(ctypes.byref(n)))
+    return n.value
+
+
+class _Buf:
+    """A pointer to FP64 (or other) data: numpy (host) or torch CUDA tensor (device, in place)."""
+
+    def __init__(self, a, dtype=np.float64, writable=False, size=None):
+        self.keep = None
+        self.out = None
+        if hasattr(a, "data_ptr") and hasattr(a, "is_cuda"):
+            import torch
+            want = {np.float64: torch.float64, np.uint64: torch.int64, np.int64: torch.int64}[dtype]
+            if a.is_cuda:
+                if a.dtype != want or not a.is_contiguous():
+                    raise TypeError("CUDA tensors must be contiguous %s" % want)
+                self.ptr = a.data_ptr()
+                self.n = a.numel()
+                return
+            a = a.detach().numpy()
+        arr = np.ascontiguousarray(a, dtype=dtype)
+        if writable and arr is not a:
+            self.out = a
+        self.keep = arr
+        self.ptr = arr.ctypes.data
+        self.n = arr.size
+
+    def finish(self):
+        if self.out is not None:
+            self.out[...] = self.keep.reshape(self.out.shape)
+
+
+class _Space:
+    _handle = None
+
+    def GetHilbertSpaceDimension(self):
+        d = ctypes.c_int64(0)
+        _check(_lib.dh_space_get_dimension(self._handle, ctypes.byref(d)))
+        return d.value
+
+    @property
+    def dim(self):
+        return self.GetHilbertSpaceDimension()
+
+    def states(self, first=0, n=None):
+        """(StateDescription, StateLzMax) of states first..first+n, reference layout."""
+        d = self.dim
+        n = d - first if n is None else n
+        words = np.zeros(n, np.uint64)
+        lz = np.zeros(n, np.int32)
+        _check(_lib.dh_space_get_states(self._handle, words.ctypes.data, lz.ctypes.data, first, n))
+        return words, lz
+
+    def FindStateIndex(self, words):
+        w = _Buf(words, np.uint64)
+        out = np.zeros(w.n, np.int64)
+        _check(_lib.dh_space_find_state_index(self._handle, w.ptr, w.n, out.ctypes.data))
+        return out
+
+    def set_index_mode(self, mode):
+        m = {"rank": DH_INDEX_RANK, "lookup": DH_INDEX_LOOKUP}.get(mode, mode)
+        _check(_lib.dh_space_set_index_mode(self._handle, m))
+
+    def __del__(self):
+        if self._handle and _lib is not None:
+            _lib.dh_space_destroy(self._handle)
+            self._handle = None
+
+
+class FermionOnSphere(_Space):
+    """FermionOnSphere(nbrFermions, totalLz, lzMax, memory): FermionOnSphere.cc:75."""
+
+    def __init__(self, nbr_fermions, total_lz, lz_max, memory=9 << 20):
+        load()
+        h = ctypes.c_void_p()
+        _check(_lib.dh_fermion_on_sphere_create(nbr_fermions, total_lz, lz_max, memory, ctypes.byref(h)))
+        self._handle = h
+        self.nbr_fermions, self.total_lz, self.lz_max = nbr_fermions, total_lz, lz_max
+
+
+class Spin1_2Chain(_Space):
+    """Spin1_2Chain(chainLength, sz, memorySize): Spin1_2Chain.cc:113."""
+
+    def __init__(self, chain_length, sz, memory=1 << 20):
+        load()
+        h = ctypes.c_void_p()
+        _check(_lib.dh_spin12_chain_create(chain_length, sz, memory, ctypes.byref(h)))
+        self._handle = h
+        self.chain_length, self.sz = chain_length, sz
+
+
+class _Hamiltonian:
+    _handle = None
+
+    def GetHilbertSpaceDimension(self):
+        d = ctypes.c_int64(0)
+        _check(_lib.dh_hamiltonian_get_dimension(self._handle, ctypes.byref(d)))
+        return d.value
+
+    @property
+    def dim(self):
+        return self.GetHilbertSpaceDimension()
+
+    def ShiftHamiltonian(self, shift):
+        _check(_lib.dh_hamiltonian_shift(self._handle, float(shift)))
+
+    def set_precision(self, precision):
+        p = {"fp64": DH_PRECISION_FP64, "fp32": DH_PRECISION_FP32}.get(precision, precision)
+        _check(_lib.dh_hamiltonian_set_precision(self._handle, p))
+
+    def set_stream(self, stream):
+        _check(_lib.dh_hamiltonian_set_stream(self._handle, ctypes.c_void_p(stream)))
+
+    def LowLevelAddMultiply(self, src, dst, first=0, nbr=-1):
+        s, d = _Buf(src), _Buf(dst, writable=True)
+        _check(_lib.dh_hamiltonian_low_level_add_multiply(self._handle, s.ptr, d.ptr, first, nbr))
+        d.finish()
+        return dst
+
+    def LowLevelMultiply(self, src, dst=None, first=0, nbr=-1):
+        if dst is None:
+            dst = np.zeros(self.dim, np.float64)
+        s, d = _Buf(src), _Buf(dst, writable=True)
+        _check(_lib.dh_hamiltonian_low_level_multiply(self._handle, s.ptr, d.ptr, first, nbr))
+        d.finish()
+        return dst
+
+    def LowLevelMultipleAddMultiply(self, srcs, dsts, first=0, nbr=-1):
+        """srcs, dsts: (k, dim) arrays (k vectors one after the other)."""
+        k = srcs.shape[0]
+        s, d = _Buf(srcs), _Buf(dsts, writable=True)
+        _check(_lib.dh_hamiltonian_low_level_multiple_add_multiply(self._handle, s.ptr, d.ptr, k, first, nbr))
+        d.finish()
+        return dsts
+
+    def MatrixElement(self, v1, v2):
+        a, b = _Buf(v1), _Buf(v2)
+        out = ctypes.c_double(0.0)
+        _check(_lib.dh_hamiltonian_matrix_element(self._handle, a.ptr, b.ptr, ctypes.byref(out)))
+        return out.value
+
+    def __del__(self):
+        if self._handle and _lib is not None:
+            _lib.dh_hamiltonian_destroy(self._handle)
+            self._handle = None
+
+
+class ParticleOnSphereGenericHamiltonian(_Hamiltonian):
+    """ParticleOnSphereGenericHamiltonian(particles, nbrParticles, lzmax, pseudoPotential, l2Factor):
+    ParticleOnSphereGenericHamiltonian.cc:66 with on-the-fly multiplication."""
+
+    def __init__(self, space, nbr_particles, lz_max, pseudopotentials, l2_factor=0.0):
+        load()
+        self.space = space  # the Hamiltonian does not own the space; keep it alive
+        v = np.ascontiguousarray(pseudopotentials, np.float64)
+        if v.size != lz_max + 1:
+            raise ValueError("need lz_max + 1 pseudopotentials")
+        h = ctypes.c_void_p()
+        _check(_lib.dh_particle_on_sphere_generic_hamiltonian_create(space._handle, nbr_particles, lz_max,
+                                                                     v.ctypes.data, float(l2_factor), ctypes.byref(h)))
+        self._handle = h
+        self.lz_max = lz_max
+
+    def set_pseudopotentials(self, v):
+        v = np.ascontiguousarray(v, np.float64)
+        _check(_lib.dh_hamiltonian_set_pseudopotentials(self._handle, v.ctypes.data))
+
+    def row_elements(self, row, cap=8192):
+        t = np.zeros(cap, np.int32)
+        s = np.zeros(cap, np.int32)
+        f = np.zeros(cap, np.int32)
+        n = ctypes.c_int(0)
+        _check(_lib.dh_hamiltonian_row_elements(self._handle, row, t.ctypes.data, s.ctypes.data, f.ctypes.data, cap,
+                                                ctypes.byref(n)))
+        if n.value > cap:
+            return self.row_elements(row, n.value)
+        return t[:n.value], s[:n.value], f[:n.value]
+
+    def interaction_factors(self):
+        n = ctypes.c_int(0)
+        _check(_lib.dh_hamiltonian_get_interaction_factors(self._handle, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, np.float64)
+        _check(_lib.dh_hamiltonian_get_interaction_factors(self._handle, out.ctypes.data, n.value, ctypes.byref(n)))
+        return out
+
+    def pseudopotential_adjoint(self, u, v):
+        """out[m] = <u| dH/dV_m |v>."""
+        a, b = _Buf(u), _Buf(v)
+        out = np.zeros(self.lz_max + 1, np.float64)
+        _check(_lib.dh_hamiltonian_pseudopotential_adjoint(self._handle, a.ptr, b.ptr, out.ctypes.data))
+        return out
+
+
+class SpinChainJ1J2Hamiltonian(_Hamiltonian):
+    """Periodic J1-J2 chain on a plain Spin1_2Chain (element pattern of
+    SpinChainJ1J2RealHamiltonianWithTranslations.cc:94-192, API of SpinChainHamiltonian.cc:257)."""
+
+    def __init__(self, chain, j1, j2):
+        load()
+        self.space = chain
+        h = ctypes.c_void_p()
+        _check(_lib.dh_spin_chain_j1j2_hamiltonian_create(chain._handle, float(j1), float(j2), ctypes.byref(h)))
+        self._handle = h
+
+
+class _Lanczos:
+    ALGORITHM = DH_LANCZOS_BASIC
+
+    def __init__(self, hamiltonian, nbr_eigenvalue=1, max_iter=500, block_size=1):
+        load()
+        self.hamiltonian = hamiltonian
+        self.nbr_eigenvalue = nbr_eigenvalue
+        h = ctypes.c_void_p()
+        _check(_lib.dh_lanczos_create(hamiltonian._handle, self.ALGORITHM, nbr_eigenvalue, block_size, max_iter,
+                                      ctypes.byref(h)))
+        self._handle = h
+
+    def SetEigenvaluePrecision(self, precision):
+        _check(_lib.dh_lanczos_set_eigenvalue_precision(self._handle, float(precision)))
+
+    def InitializeLanczosAlgorithm(self, vector=None, seed=0):
+        if vector is None:
+            _check(_lib.dh_lanczos_initialize_random(self._handle, seed))
+        else:
+            b = _Buf(vector)
+            _check(_lib.dh_lanczos_initialize(self._handle, b.ptr, 1))
+
+    def RunLanczosAlgorithm(self, nbr_iter):
+        _check(_lib.dh_lanczos_run(self._handle, nbr_iter))
+
+    def TestConvergence(self):
+        c = ctypes.c_int(0)
+        _check(_lib.dh_lanczos_test_convergence(self._handle, ctypes.byref(c)))
+        return bool(c.value)
+
+    def GetEigenvalues(self, n=None):
+        n = self.nbr_eigenvalue if n is None else n
+        out = np.zeros(n, np.float64)
+        _check(_lib.dh_lanczos_get_eigenvalues(self._handle, out.ctypes.data, n))
+        return out
+
+    def GetGroundStateEnergy(self):
+        e = ctypes.c_double(0.0)
+        _check(_lib.dh_lanczos_get_ground_state_energy(self._handle, ctypes.byref(e)))
+        return e.value
+
+    def GetGroundState(self, out=None):
+        dim = self.hamiltonian.dim
+        if out is None:
+            out = np.zeros(dim, np.float64)
+        b = _Buf(out, writable=True)
+        _check(_lib.dh_lanczos_get_ground_state(self._handle, b.ptr))
+        b.finish()
+        return out
+
+    def counters(self):
+        m = ctypes.c_int64(0)
+        r = ctypes.c_int(0)
+        _check(_lib.dh_lanczos_get_counters(self._handle, ctypes.byref(m), ctypes.byref(r)))
+        return m.value, r.value
+
+    def solve(self, max_iter=500, graph_batch=16):
+        """Driver loop of QHEOnSphereMainTask.cc:732-753 on the device."""
+        eig = np.zeros(self.nbr_eigenvalue, np.float64)
+        it = ctypes.c_int(0)
+        conv = ctypes.c_int(0)
+        _check(_lib.dh_lanczos_solve(self._handle, max_iter, graph_batch, eig.ctypes.data, ctypes.byref(it),
+                                     ctypes.byref(conv)))
+        return dict(eigenvalues=eig, iterations=it.value, converged=bool(conv.value))
+
+    def solve_refined(self, max_iter=500, precision=1e-12):
+        """FP32-product Lanczos, then FP64 refinement of the ground state."""
+        out = np.zeros(5, np.float64)
+        _check(_lib.dh_lanczos_solve_refined(self._handle, max_iter, float(precision), out.ctypes.data))
+        return dict(energy=out[0], energy_fp32=out[1], residual=out[2], fp32_matvecs=int(out[3]),
+                    fp64_matvecs=int(out[4]))
+
+    def __del__(self):
+        if self._handle and _lib is not None:
+            _lib.dh_lanczos_destroy(self._handle)
+            self._handle = None
+
+
+class BasicLanczosAlgorithm(_Lanczos):
+    ALGORITHM = DH_LANCZOS_BASIC
+
+
+class FullReorthogonalizedLanczosAlgorithm(_Lanczos):
+    ALGORITHM = DH_LANCZOS_FULL_REORTHOGONALIZED
+
+
+class BasicLanczosAlgorithmWithGroundState(_Lanczos):
+    ALGORITHM = DH_LANCZOS_WITH_GROUND_STATE
+
+
+def coulomb_pseudopotentials(nbr_flux):
+    """EvaluatePseudopotentials(nbrFlux, 0, 0.0): LLL Coulomb V_0..V_nbrFlux on the sphere."""
+    load()
+    v = np.zeros(nbr_flux + 1, np.float64)
+    _check(_lib.dh_coulomb_pseudopotentials(nbr_flux, v.ctypes.data))
+    return v
+
+
+def clebsch_gordan(j1, m1, j2, m2, j):
+    load()
+    out = ctypes.c_double(0.0)
+    _check(_lib.dh_clebsch_gordan(j1, m1, j2, m2, j, ctypes.byref(out)))
+    return out.value

@@ -1,0 +1,531 @@
+// C ABI: Lanczos algorithms on the GPU (see include/diagham_b200.h for the contract).
+//
+// Vectors stay in device memory in FP64.  The recurrence is the reference's
+// (BasicLanczosAlgorithm.cc:148-216): alpha_i = <v_i|H v_i>, beta_i = <v_{i-1}|H v_i>, the new
+// vector normalised explicitly.  Its scalars live on the device and are only copied to the host to
+// diagonalise the tridiagonal matrix, as AbstractLanczosAlgorithm::Diagonalize does after every
+// RunLanczosAlgorithm call (AbstractLanczosAlgorithm.cc:136).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <new>
+#include <vector>
+
+#include "dh_internal.h"
+#include "dh_objects.h"
+
+using namespace dh;
+
+struct dh_lanczos_s {
+  dh_hamiltonian_s* h = nullptr;
+  int algorithm = DH_LANCZOS_BASIC;
+  int nev = 1;
+  int block = 1;
+  int max_iter = 0;
+  double precision = 1e-14;  // MACHINE_PRECISION (src/config.h:49)
+  int64_t dim = 0;
+  cudaStream_t stream = 0;
+  int cap = 0;  // capacity of the scalar arrays (tridiagonal rows)
+  DevBuf vec, x32, scal, red_storage, krylov, initial, coef, ground;
+  Reducer red;
+  LanczosDev st = {};
+  int krylov_cap = 0;
+  bool initialized = false;
+  bool ground_valid = false;
+  int index = 0;   // reference "Index": the newest vector is v_{index + 1}
+  int rows = 0;    // tridiagonal rows
+  double prev_last = 0.0;
+  std::vector<double> prev_wanted;
+  std::vector<double> alpha, beta, ritz;
+  int64_t matvecs = 0;
+  cudaGraphExec_t graph3 = nullptr;  // three iterations starting at phase 0
+  ~dh_lanczos_s() {
+    if (graph3) cudaGraphExecDestroy(graph3);
+  }
+};
+
+namespace {
+
+int lz_matvec(dh_lanczos_s* l, int src_slot, int dst_slot) {
+  double* x = l->st.vec + (size_t)src_slot * l->dim;
+  double* y = l->st.vec + (size_t)dst_slot * l->dim;
+  ++l->matvecs;
+  return hamiltonian_apply(l->h, x, y, 1, 0, l->dim, 0, l->st.x32, l->stream);
+}
+
+// one iteration: v_{i+1} from H v_i, then H v_{i+1} and the two new scalars (i = index)
+int lz_iteration(dh_lanczos_s* l, int i) {
+  const int phase = i % 3;
+  int rc;
+  if ((rc = launch_lz_update(l->st, phase, l->stream)) != DH_OK) return rc;
+  if (l->algorithm == DH_LANCZOS_FULL_REORTHOGONALIZED && i + 1 >= 3) {
+    // FullReorthogonalizedLanczosAlgorithm.cc:230-243: classical Gram-Schmidt of the new vector
+    // against v_0 .. v_{i-2} (v_{i-1}, v_i are handled by the recurrence), before normalisation
+    double* w = l->st.vec + (size_t)((phase + 1) % 3) * l->dim;
+    const int m = i - 1;
+    if ((rc = launch_strided_dots(l->st.krylov, m, l->dim, w, l->dim, l->coef.as<double>(), l->red, l->stream)) != DH_OK)
+      return rc;
+    if ((rc = launch_combine(l->st.krylov, m, l->dim, l->coef.as<double>(), -1.0, w, 1, l->dim, l->stream)) != DH_OK)
+      return rc;
+    // the norm of the re-orthogonalised vector
+    const double* vs[1] = {w};
+    if ((rc = launch_multi_dot(vs, 1, w, l->dim, l->st.norm + i + 1, l->red, l->stream)) != DH_OK) return rc;
+    if ((rc = launch_sqrt_inplace(l->st.norm + i + 1, l->stream)) != DH_OK) return rc;
+  }
+  if ((rc = launch_lz_scale(l->st, phase, l->stream)) != DH_OK) return rc;
+  if ((rc = lz_matvec(l, (phase + 1) % 3, (phase + 2) % 3)) != DH_OK) return rc;
+  return launch_lz_dots(l->st, phase, l->stream);
+}
+
+int lz_first_steps(dh_lanczos_s* l) {
+  // v_0 in slot 0 (normalised by initialize); H v_0 -> slot 1; alpha_0 = <v_0|H v_0>
+  int rc;
+  if (l->st.x32 && (rc = launch_convert_f32(l->st.vec, l->st.x32, l->dim, l->stream)) != DH_OK) return rc;
+  if (l->st.krylov)
+    DH_CUDA(cudaMemcpyAsync(l->st.krylov, l->st.vec, l->dim * sizeof(double), cudaMemcpyDeviceToDevice, l->stream));
+  if ((rc = lz_matvec(l, 0, 1)) != DH_OK) return rc;
+  const double* vs[1] = {l->st.vec};
+  if ((rc = launch_multi_dot(vs, 1, l->st.vec + l->dim, l->dim, l->st.alpha, l->red, l->stream)) != DH_OK) return rc;
+  DH_CUDA(cudaMemsetAsync(l->st.cursor, 0, sizeof(int), l->stream));
+  return lz_iteration(l, 0);
+}
+
+// copy the scalars, diagonalise the tridiagonal matrix, update the previous-eigenvalue bookkeeping
+// exactly as BasicLanczosAlgorithm.cc:200-214 does after each RunLanczosAlgorithm call
+int lz_finish_call(dh_lanczos_s* l) {
+  l->alpha.resize(l->rows);
+  l->beta.resize(std::max(l->rows - 1, 0));
+  DH_CUDA(cudaMemcpyAsync(l->alpha.data(), l->st.alpha, l->rows * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
+  if (l->rows > 1)
+    DH_CUDA(cudaMemcpyAsync(l->beta.data(), l->st.beta, (l->rows - 1) * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
+  DH_CUDA(cudaStreamSynchronize(l->stream));
+  const int nev = std::min(l->nev, l->rows);
+  std::vector<double> eig(l->rows);
+  if (l->prev_last != 0.0) {
+    l->prev_last = l->ritz[nev - 1];
+    for (int i = 0; i < nev; ++i) l->prev_wanted[i] = l->ritz[i];
+    int rc = tridiagonal_eigen(l->rows, l->alpha.data(), l->beta.data(), eig.data(), nullptr);
+    if (rc != DH_OK) return rc;
+  } else {
+    int rc = tridiagonal_eigen(l->rows, l->alpha.data(), l->beta.data(), eig.data(), nullptr);
+    if (rc != DH_OK) return rc;
+    l->prev_last = 2.0 * eig[nev - 1];
+    for (int i = 0; i < nev; ++i) l->prev_wanted[i] = 2.0 * eig[i];
+  }
+  l->ritz.swap(eig);
+  l->ground_valid = false;
+  return DH_OK;
+}
+
+// BasicLanczosAlgorithm::TestConvergence (:220): |lambda_{nev-1} - previous| < precision |lambda_{nev-1}|
+bool lz_converged(const dh_lanczos_s* l) {
+  if ((int)l->ritz.size() < l->nev) return false;
+  const double e = l->ritz[l->nev - 1];
+  return fabs(e - l->prev_last) < l->precision * fabs(e);
+}
+
+int lz_run(dh_lanczos_s* l, int nbr_iter) {
+  DH_CHECK(l->initialized, DH_ERR_STATE, "RunLanczosAlgorithm before InitializeLanczosAlgorithm");
+  int target;
+  int rc;
+  if (l->rows == 0) {
+    target = std::max(nbr_iter, 2);
+    DH_CHECK(target <= l->cap, DH_ERR_ARGUMENT, "more Lanczos rows (%d) than max_iter allows (%d)", target, l->cap);
+    if ((rc = lz_first_steps(l)) != DH_OK) return rc;
+    l->index = 0;
+    l->rows = 2;
+  } else {
+    target = l->rows + nbr_iter;
+    DH_CHECK(target <= l->cap, DH_ERR_ARGUMENT, "more Lanczos rows (%d) than max_iter allows (%d)", target, l->cap);
+  }
+  while (l->rows < target) {
+    if ((rc = lz_iteration(l, l->index + 1)) != DH_OK) return rc;
+    ++l->index;
+    ++l->rows;
+  }
+  return lz_finish_call(l);
+}
+
+// Ritz vector of the lowest Ritz value: from the Krylov store when kept, otherwise by replaying the
+// recurrence from the start vector (BasicLanczosAlgorithmWithGroundState.cc:256-335)
+int lz_ground_state(dh_lanczos_s* l) {
+  if (l->ground_valid) return DH_OK;
+  DH_CHECK(l->rows >= 2, DH_ERR_STATE, "no Lanczos iteration has been run");
+  const int n = l->rows;
+  std::vector<double> eig(n), z((size_t)n * n);
+  int rc = tridiagonal_eigen(n, l->alpha.data(), l->beta.data(), eig.data(), z.data());
+  if (rc != DH_OK) return rc;
+  std::vector<double> c(z.begin(), z.begin() + n);  // column 0 (column-major)
+  if ((rc = ensure_buffer(l->ground, l->dim * sizeof(double))) != DH_OK) return rc;
+  if ((rc = ensure_buffer(l->coef, (size_t)std::max(n, l->cap + 8) * sizeof(double))) != DH_OK) return rc;
+  double* g = l->ground.as<double>();
+  if (l->st.krylov && n <= l->krylov_cap) {
+    DH_CUDA(cudaMemcpyAsync(l->coef.ptr, c.data(), n * sizeof(double), cudaMemcpyHostToDevice, l->stream));
+    if ((rc = launch_combine(l->st.krylov, n, l->dim, l->coef.as<double>(), 1.0, g, 0, l->dim, l->stream)) != DH_OK)
+      return rc;
+  } else {
+    // replay: v_0 = start vector, v_{j+1} = (H v_j - alpha_j v_j - beta_{j-1} v_{j-1}) / |.|
+    double* v[3] = {l->st.vec, l->st.vec + l->dim, l->st.vec + 2 * l->dim};
+    DH_CUDA(cudaMemcpyAsync(v[0], l->initial.ptr, l->dim * sizeof(double), cudaMemcpyDeviceToDevice, l->stream));
+    DH_CUDA(cudaMemsetAsync(g, 0, l->dim * sizeof(double), l->stream));
+    if ((rc = launch_axpy_scalar(g, v[0], c[0], l->dim, l->stream)) != DH_OK) return rc;
+    double* nrm = l->coef.as<double>();
+    for (int j = 0; j + 1 < n; ++j) {
+      double* cur = v[j % 3];
+      double* prev = v[(j + 2) % 3];
+      double* next = v[(j + 1) % 3];
+      if ((rc = hamiltonian_apply(l->h, cur, next, 1, 0, l->dim, 0, nullptr, l->stream)) != DH_OK) return rc;
+      ++l->matvecs;
+      if ((rc = launch_lanczos_update(next, next, cur, j > 0 ? prev : nullptr, l->st.alpha + j,
+                                      j > 0 ? l->st.beta + j - 1 : nullptr, l->dim, nrm, l->red, l->stream)) != DH_OK)
+        return rc;
+      if ((rc = launch_scale_convert(next, nullptr, nrm, l->dim, l->stream)) != DH_OK) return rc;
+      if ((rc = launch_axpy_scalar(g, next, c[j + 1], l->dim, l->stream)) != DH_OK) return rc;
+    }
+    // the three work vectors were overwritten: the algorithm cannot continue from here
+    l->initialized = false;
+  }
+  // normalise
+  const double* vs[1] = {g};
+  double* nrm = l->coef.as<double>();
+  if ((rc = launch_multi_dot(vs, 1, g, l->dim, nrm, l->red, l->stream)) != DH_OK) return rc;
+  if ((rc = launch_sqrt_inplace(nrm, l->stream)) != DH_OK) return rc;
+  if ((rc = launch_scale_convert(g, nullptr, nrm, l->dim, l->stream)) != DH_OK) return rc;
+  DH_CUDA(cudaStreamSynchronize(l->stream));
+  l->ground_valid = true;
+  return DH_OK;
+}
+
+int lz_initialize_device(dh_lanczos_s* l) {
+  // normalise slot 0 and keep a copy of the start vector for a replay
+  const double* vs[1] = {l->st.vec};
+  int rc;
+  if ((rc = launch_multi_dot(vs, 1, l->st.vec, l->dim, l->st.norm, l->red, l->stream)) != DH_OK) return rc;
+  if ((rc = launch_sqrt_inplace(l->st.norm, l->stream)) != DH_OK) return rc;
+  if ((rc = launch_scale_convert(l->st.vec, nullptr, l->st.norm, l->dim, l->stream)) != DH_OK) return rc;
+  DH_CUDA(cudaMemcpyAsync(l->initial.ptr, l->st.vec, l->dim * sizeof(double), cudaMemcpyDeviceToDevice, l->stream));
+  DH_CUDA(cudaStreamSynchronize(l->stream));
+  l->initialized = true;
+  l->ground_valid = false;
+  l->rows = 0;
+  l->index = 0;
+  l->prev_last = 0.0;
+  std::fill(l->prev_wanted.begin(), l->prev_wanted.end(), 0.0);
+  l->ritz.clear();
+  return DH_OK;
+}
+
+// Three consecutive iterations (phases 0, 1, 2) captured once as a CUDA graph; the device cursor
+// selects the scalars, so the same graph serves every batch that starts at a multiple of three.
+int lz_graph3(dh_lanczos_s* l) {
+  if (l->graph3) return DH_OK;
+  DH_CHECK(l->stream != 0, DH_ERR_STATE, "graph capture needs a non-default stream");
+  cudaGraph_t g;
+  DH_CUDA(cudaStreamBeginCapture(l->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = DH_OK;
+  int64_t saved = l->matvecs;
+  for (int p = 0; p < 3 && rc == DH_OK; ++p) rc = lz_iteration(l, 3 + p);
+  l->matvecs = saved;
+  cudaError_t e = cudaStreamEndCapture(l->stream, &g);
+  if (rc != DH_OK) return rc;
+  DH_CUDA(e);
+  e = cudaGraphInstantiate(&l->graph3, g, 0);
+  cudaGraphDestroy(g);
+  DH_CUDA(e);
+  return DH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dh_lanczos_create(dh_hamiltonian_t h, int algorithm, int nbr_eigenvalue, int block_size, int max_iter,
+                      dh_lanczos_t* out) {
+  DH_CHECK(out, DH_ERR_ARGUMENT, "null output handle");
+  *out = nullptr;
+  DH_CHECK(h, DH_ERR_ARGUMENT, "null hamiltonian");
+  DH_CHECK(algorithm == DH_LANCZOS_BASIC || algorithm == DH_LANCZOS_FULL_REORTHOGONALIZED ||
+               algorithm == DH_LANCZOS_WITH_GROUND_STATE,
+           DH_ERR_UNSUPPORTED, "algorithm %d: use dh_block_lanczos_* for block Lanczos", algorithm);
+  DH_CHECK(nbr_eigenvalue >= 1, DH_ERR_ARGUMENT, "nbr_eigenvalue must be >= 1");
+  DH_CHECK(max_iter >= nbr_eigenvalue + 3, DH_ERR_ARGUMENT, "max_iter must be >= nbr_eigenvalue + 3");
+  (void)block_size;
+  dh_lanczos_s* l = new (std::nothrow) dh_lanczos_s();
+  DH_CHECK(l, DH_ERR_MEMORY, "out of host memory");
+  l->h = h;
+  l->algorithm = algorithm;
+  l->nev = nbr_eigenvalue;
+  l->max_iter = max_iter;
+  l->dim = h->space->dim;
+  l->cap = max_iter + 2;
+  l->prev_wanted.assign(nbr_eigenvalue, 0.0);
+  int rc;
+  const size_t vb = (size_t)l->dim * sizeof(double);
+  if ((rc = l->vec.alloc(3 * vb)) != DH_OK || (rc = l->initial.alloc(vb)) != DH_OK ||
+      (rc = l->scal.alloc((size_t)3 * (l->cap + 2) * sizeof(double) + 64)) != DH_OK ||
+      (rc = l->coef.alloc((size_t)(l->cap + 8) * sizeof(double))) != DH_OK ||
+      (rc = reducer_init(l->red, l->red_storage, 16)) != DH_OK) {
+    delete l;
+    return rc;
+  }
+  if (h->precision == DH_PRECISION_FP32 && (rc = l->x32.alloc((size_t)l->dim * sizeof(float))) != DH_OK) {
+    delete l;
+    return rc;
+  }
+  // keep the Krylov basis on the device when it fits in half of the free memory (needed by the full
+  // re-orthogonalisation; spares the ground-state replay otherwise)
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  const size_t kb = (size_t)l->cap * vb;
+  if (algorithm == DH_LANCZOS_FULL_REORTHOGONALIZED || kb < free_b / 2) {
+    if (l->krylov.alloc(kb) == DH_OK) l->krylov_cap = l->cap;
+    else cudaGetLastError();
+  }
+  DH_CHECK(algorithm != DH_LANCZOS_FULL_REORTHOGONALIZED || l->krylov_cap > 0, DH_ERR_MEMORY,
+           "full re-orthogonalisation needs %zu bytes for its vectors", kb);
+  if (cudaStreamCreateWithFlags(&l->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete l;
+    return cuda_fail(cudaGetLastError(), "cudaStreamCreate", __FILE__, __LINE__);
+  }
+  double* sc = l->scal.as<double>();
+  l->st.vec = l->vec.as<double>();
+  l->st.dim = l->dim;
+  l->st.x32 = l->x32.as<float>();
+  l->st.krylov = l->krylov.as<double>();
+  l->st.krylov_cap = l->krylov_cap;
+  l->st.alpha = sc;
+  l->st.beta = sc + (l->cap + 2);
+  l->st.norm = sc + 2 * (l->cap + 2);
+  l->st.cursor = reinterpret_cast<int*>(sc + 3 * (l->cap + 2));
+  l->st.partial = l->red.partial;
+  l->st.ticket = l->red.ticket;
+  l->st.nblocks = l->red.nblocks;
+  *out = l;
+  return DH_OK;
+}
+
+int dh_lanczos_destroy(dh_lanczos_t l) {
+  if (l) {
+    if (l->stream) cudaStreamSynchronize(l->stream);
+    cudaStream_t s = l->stream;
+    delete l;
+    if (s) cudaStreamDestroy(s);
+  }
+  return DH_OK;
+}
+
+int dh_lanczos_set_eigenvalue_precision(dh_lanczos_t l, double precision) {
+  DH_CHECK(l && precision > 0.0, DH_ERR_ARGUMENT, "bad argument");
+  l->precision = precision;
+  return DH_OK;
+}
+
+int dh_lanczos_initialize(dh_lanczos_t l, const double* vectors, int nbr_vectors) {
+  DH_CHECK(l && vectors && nbr_vectors >= 1, DH_ERR_ARGUMENT, "bad argument");
+  const cudaMemcpyKind kind = is_device_pointer(vectors) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  DH_CUDA(cudaMemcpyAsync(l->st.vec, vectors, l->dim * sizeof(double), kind, l->stream));
+  return lz_initialize_device(l);
+}
+
+int dh_lanczos_initialize_random(dh_lanczos_t l, uint64_t seed) {
+  DH_CHECK(l, DH_ERR_ARGUMENT, "null lanczos");
+  int rc = launch_random_vector(l->st.vec, l->dim, seed, l->stream);
+  if (rc != DH_OK) return rc;
+  return lz_initialize_device(l);
+}
+
+int dh_lanczos_run(dh_lanczos_t l, int nbr_iter) {
+  DH_CHECK(l && nbr_iter >= 1, DH_ERR_ARGUMENT, "bad argument");
+  return lz_run(l, nbr_iter);
+}
+
+int dh_lanczos_test_convergence(dh_lanczos_t l, int* converged) {
+  DH_CHECK(l && converged, DH_ERR_ARGUMENT, "null argument");
+  *converged = lz_converged(l) ? 1 : 0;
+  return DH_OK;
+}
+
+int dh_lanczos_get_eigenvalues(dh_lanczos_t l, double* eigenvalues, int n) {
+  DH_CHECK(l && eigenvalues, DH_ERR_ARGUMENT, "null argument");
+  DH_CHECK(n >= 0 && n <= (int)l->ritz.size(), DH_ERR_ARGUMENT, "only %d Ritz values", (int)l->ritz.size());
+  for (int i = 0; i < n; ++i) eigenvalues[i] = l->ritz[i];
+  return DH_OK;
+}
+
+int dh_lanczos_get_ground_state_energy(dh_lanczos_t l, double* energy) {
+  DH_CHECK(l && energy, DH_ERR_ARGUMENT, "null argument");
+  DH_CHECK(!l->ritz.empty(), DH_ERR_STATE, "no Lanczos iteration has been run");
+  *energy = l->ritz[0];
+  return DH_OK;
+}
+
+int dh_lanczos_get_ground_state(dh_lanczos_t l, double* vec) {
+  DH_CHECK(l && vec, DH_ERR_ARGUMENT, "null argument");
+  int rc = lz_ground_state(l);
+  if (rc != DH_OK) return rc;
+  const cudaMemcpyKind kind = is_device_pointer(vec) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  DH_CUDA(cudaMemcpyAsync(vec, l->ground.ptr, l->dim * sizeof(double), kind, l->stream));
+  DH_CUDA(cudaStreamSynchronize(l->stream));
+  return DH_OK;
+}
+
+int dh_lanczos_get_counters(dh_lanczos_t l, int64_t* matvecs, int* rows) {
+  DH_CHECK(l, DH_ERR_ARGUMENT, "null lanczos");
+  if (matvecs) *matvecs = l->matvecs;
+  if (rows) *rows = l->rows;
+  return DH_OK;
+}
+
+int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eigenvalues, int* iterations,
+                     int* converged) {
+  DH_CHECK(l && eigenvalues && iterations && converged, DH_ERR_ARGUMENT, "null argument");
+  DH_CHECK(l->initialized, DH_ERR_STATE, "solve before InitializeLanczosAlgorithm");
+  if (max_iter > l->max_iter) max_iter = l->max_iter;
+  int rc;
+  // QHEOnSphereMainTask.cc:732-753: RunLanczosAlgorithm(nev + 2), counter = nev + 3
+  if ((rc = lz_run(l, l->nev + 2)) != DH_OK) return rc;
+  int count = l->nev + 3;
+  const bool use_graph = graph_batch > 1 && l->algorithm != DH_LANCZOS_FULL_REORTHOGONALIZED;
+  while (!lz_converged(l) && count < max_iter) {
+    if (!use_graph) {
+      ++count;
+      if ((rc = lz_run(l, 1)) != DH_OK) return rc;
+      continue;
+    }
+    // issue iterations on the device without a host round trip until the next multiple of three,
+    // then whole captured triples, then replay the per-iteration convergence test on the host
+    int todo = std::min(graph_batch, max_iter - count);
+    todo = std::min(todo, l->cap - l->rows);
+    if (todo <= 0) break;
+    const int start_rows = l->rows;
+    int issued = 0;
+    while (issued < todo && ((l->index + 1) % 3) != 0) {
+      if ((rc = lz_iteration(l, l->index + 1)) != DH_OK) break;
+      ++l->index;
+      ++l->rows;
+      ++issued;
+    }
+    if (rc == DH_OK && todo - issued >= 3 && (rc = lz_graph3(l)) == DH_OK) {
+      while (todo - issued >= 3) {
+        cudaError_t e = cudaGraphLaunch(l->graph3, l->stream);
+        if (e != cudaSuccess) {
+          rc = cuda_fail(e, "cudaGraphLaunch", __FILE__, __LINE__);
+          break;
+        }
+        l->index += 3;
+        l->rows += 3;
+        l->matvecs += 3;
+        issued += 3;
+      }
+    }
+    while (rc == DH_OK && issued < todo) {
+      if ((rc = lz_iteration(l, l->index + 1)) != DH_OK) break;
+      ++l->index;
+      ++l->rows;
+      ++issued;
+    }
+    if (rc != DH_OK) return rc;
+    // host side: one RunLanczosAlgorithm(1) bookkeeping step per issued iteration
+    const int end_rows = l->rows;
+    std::vector<double> a(end_rows), b(end_rows);
+    DH_CUDA(cudaMemcpyAsync(a.data(), l->st.alpha, end_rows * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
+    DH_CUDA(cudaMemcpyAsync(b.data(), l->st.beta, (end_rows - 1) * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
+    DH_CUDA(cudaStreamSynchronize(l->stream));
+    for (int r = start_rows + 1; r <= end_rows; ++r) {
+      ++count;
+      l->rows = r;
+      if ((rc = lz_finish_call(l)) != DH_OK) return rc;
+      if (lz_converged(l) || count >= max_iter) break;
+    }
+    if (l->rows < end_rows) {
+      // converged before the end of the batch: the extra iterations are discarded; the Krylov
+      // vectors beyond l->rows are unused, so the algorithm cannot be continued
+      l->index = l->rows - 2;
+      l->initialized = false;
+    }
+  }
+  *iterations = count;
+  *converged = lz_converged(l) ? 1 : 0;
+  for (int i = 0; i < l->nev && i < (int)l->ritz.size(); ++i) eigenvalues[i] = l->ritz[i];
+  return DH_OK;
+}
+
+int dh_lanczos_solve_refined(dh_lanczos_t l, int max_iter, double precision, double* out) {
+  DH_CHECK(l && out, DH_ERR_ARGUMENT, "null argument");
+  DH_CHECK(l->initialized, DH_ERR_STATE, "solve before InitializeLanczosAlgorithm");
+  DH_CHECK(precision > 0.0, DH_ERR_ARGUMENT, "precision must be > 0");
+  dh_hamiltonian_s* h = l->h;
+  const int saved_precision = h->precision;
+  const double saved_lz_precision = l->precision;
+  int rc;
+  if (!l->st.x32) {
+    if ((rc = l->x32.alloc((size_t)l->dim * sizeof(float))) != DH_OK) return rc;
+    l->st.x32 = l->x32.as<float>();
+    if (l->graph3) {
+      cudaGraphExecDestroy(l->graph3);
+      l->graph3 = nullptr;
+    }
+  }
+  // phase 1: FP32 products, FP64 recurrence, converged to the FP32 resolution of the Ritz value
+  h->precision = DH_PRECISION_FP32;
+  l->precision = std::max(precision, 1e-9);
+  double e32 = 0.0;
+  int iters = 0, conv = 0;
+  rc = dh_lanczos_solve(l, max_iter, 16, &e32, &iters, &conv);
+  const int64_t fp32_matvecs = l->matvecs;
+  if (rc == DH_OK) rc = lz_ground_state(l);
+  // phase 2: FP64 Rayleigh quotient and residual of the Ritz vector
+  h->precision = DH_PRECISION_FP64;
+  double energy = e32, rnorm = 0.0;
+  double* sc = l->coef.as<double>();
+  if (rc == DH_OK) {
+    double* psi = l->ground.as<double>();
+    double* hpsi = l->st.vec;
+    double* res = l->st.vec + l->dim;
+    rc = hamiltonian_apply(h, psi, hpsi, 1, 0, l->dim, 0, nullptr, l->stream);
+    const double* vs[1] = {psi};
+    if (rc == DH_OK) rc = launch_multi_dot(vs, 1, hpsi, l->dim, sc, l->red, l->stream);
+    if (rc == DH_OK) rc = launch_lanczos_update(res, hpsi, psi, nullptr, sc, nullptr, l->dim, sc + 1, l->red, l->stream);
+    double host[2] = {0.0, 0.0};
+    if (rc == DH_OK && cudaMemcpyAsync(host, sc, 2 * sizeof(double), cudaMemcpyDeviceToHost, l->stream) != cudaSuccess)
+      rc = cuda_fail(cudaGetLastError(), "copy", __FILE__, __LINE__);
+    if (rc == DH_OK && cudaStreamSynchronize(l->stream) != cudaSuccess)
+      rc = cuda_fail(cudaGetLastError(), "sync", __FILE__, __LINE__);
+    energy = host[0];
+    rnorm = host[1];
+  }
+  int64_t fp64_matvecs = 1;
+  // the Rayleigh-quotient error is bounded by |r|^2 / gap: when that may exceed the target, restart
+  // an FP64 Lanczos from the Ritz vector (it converges in a few steps from there)
+  if (rc == DH_OK && rnorm * rnorm > precision * std::max(fabs(energy), 1e-300)) {
+    DH_CUDA(cudaMemcpyAsync(l->st.vec, l->ground.ptr, l->dim * sizeof(double), cudaMemcpyDeviceToDevice, l->stream));
+    if (l->graph3) {
+      cudaGraphExecDestroy(l->graph3);
+      l->graph3 = nullptr;
+    }
+    float* keep32 = l->st.x32;
+    l->st.x32 = nullptr;
+    rc = lz_initialize_device(l);
+    l->precision = precision;
+    const int64_t before = l->matvecs;
+    double e64 = 0.0;
+    if (rc == DH_OK) rc = dh_lanczos_solve(l, std::min(max_iter, 60), 1, &e64, &iters, &conv);
+    fp64_matvecs += l->matvecs - before;
+    if (rc == DH_OK) energy = e64;
+    l->st.x32 = keep32;
+  }
+  h->precision = saved_precision;
+  l->precision = saved_lz_precision;
+  if (rc != DH_OK) return rc;
+  out[0] = energy;
+  out[1] = e32;
+  out[2] = rnorm;
+  out[3] = (double)fp32_matvecs;
+  out[4] = (double)fp64_matvecs;
+  return DH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,651 @@
+// C ABI: Hilbert spaces and Hamiltonians (see include/diagham_b200.h for the contract).
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <new>
+#include <vector>
+
+#include "dh_internal.h"
+#include "dh_objects.h"
+
+using namespace dh;
+
+namespace dh {
+
+const char* last_error();
+
+bool is_device_pointer(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes attr;
+  cudaError_t e = cudaPointerGetAttributes(&attr, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+// FermionOnSphere set-up: orbital-sum counts, the two rank tables and the basis words
+static int build_fermion_space(dh_space_s* sp) {
+  const int N = sp->nbr_fermions, L = sp->lz_max, K = sp->total_sum;
+  const int O = L + 2;  // orbital counts 0 .. L+1
+  // counts[n][o][s]: n fermions in orbitals 0..o-1 with orbital-index sum s
+  std::vector<int64_t> counts((size_t)(N + 1) * O * (K + 1), 0);
+  auto C = [&](int n, int o, int s) -> int64_t& { return counts[((size_t)n * O + o) * (K + 1) + s]; };
+  for (int o = 0; o < O; ++o) C(0, o, 0) = 1;
+  for (int n = 1; n <= N; ++n)
+    for (int o = 1; o < O; ++o)
+      for (int s = 0; s <= K; ++s) {
+        int64_t v = C(n, o - 1, s);
+        if (s - (o - 1) >= 0) v += C(n - 1, o - 1, s - (o - 1));
+        C(n, o, s) = v;
+      }
+  const int64_t dim = C(N, L + 1, K);
+  DH_CHECK(dim > 0, DH_ERR_ARGUMENT, "FermionOnSphere(%d, %d, %d): empty sector", N, sp->total_lz, L);
+  DH_CHECK(dim < (1ll << 31), DH_ERR_UNSUPPORTED, "FermionOnSphere: dimension %lld >= 2^31", (long long)dim);
+  sp->dim = dim;
+
+  // rank tables: index(w) = high_offset[w >> LB] + low_rank[w & (2^LB - 1)]
+  FermionRankTables& t = sp->rank;
+  t.low_bits = (L + 2) / 2;
+  t.high_bits = L + 1 - t.low_bits;
+  const int LB = t.low_bits, HB = t.high_bits;
+  const int maxsum = LB * (LB - 1) / 2;
+  std::vector<int> counter((size_t)(LB + 1) * (maxsum + 1), 0);
+  t.low_rank.assign((size_t)1 << LB, 0);
+  for (int64_t l = ((int64_t)1 << LB) - 1; l >= 0; --l) {
+    int pc = __builtin_popcountll((unsigned long long)l), ws = 0;
+    for (int b = 0; b < LB; ++b)
+      if ((l >> b) & 1) ws += b;
+    int& c = counter[(size_t)pc * (maxsum + 1) + ws];
+    DH_CHECK(c < 65535, DH_ERR_UNSUPPORTED, "FermionOnSphere: rank class too large for 16-bit ranks");
+    t.low_rank[l] = (uint16_t)c++;
+  }
+  t.high_offset.assign((size_t)1 << HB, -1);
+  int64_t running = 0;
+  for (int64_t h = ((int64_t)1 << HB) - 1; h >= 0; --h) {
+    int nh = __builtin_popcountll((unsigned long long)h), sh = 0;
+    for (int b = 0; b < HB; ++b)
+      if ((h >> b) & 1) sh += b + LB;
+    int nl = N - nh, sl = K - sh;
+    if (nl < 0 || nl > LB || sl < 0 || sl > maxsum) continue;
+    int64_t c = C(nl, LB, sl);
+    if (c == 0) continue;
+    t.high_offset[h] = (int32_t)running;
+    running += c;
+  }
+  DH_CHECK(running == dim, DH_ERR_STATE, "FermionOnSphere: rank tables cover %lld of %lld states", (long long)running,
+           (long long)dim);
+
+  int rc;
+  DevBuf dcounts;
+  if ((rc = dcounts.alloc(counts.size() * sizeof(int64_t))) != DH_OK) return rc;
+  if ((rc = sp->words.alloc((size_t)dim * sizeof(uint64_t))) != DH_OK) return rc;
+  if ((rc = sp->low_rank.alloc(t.low_rank.size() * sizeof(uint16_t))) != DH_OK) return rc;
+  if ((rc = sp->high_offset.alloc(t.high_offset.size() * sizeof(int32_t))) != DH_OK) return rc;
+  DH_CUDA(cudaMemcpy(dcounts.ptr, counts.data(), counts.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+  DH_CUDA(cudaMemcpy(sp->low_rank.ptr, t.low_rank.data(), t.low_rank.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+  DH_CUDA(cudaMemcpy(sp->high_offset.ptr, t.high_offset.data(), t.high_offset.size() * sizeof(int32_t),
+                     cudaMemcpyHostToDevice));
+  rc = launch_fqhe_unrank(N, L, K, dim, sp->words.as<uint64_t>(), dcounts.as<int64_t>(), O * (K + 1), K + 1, 0);
+  if (rc != DH_OK) return rc;
+  DH_CUDA(cudaDeviceSynchronize());
+  return DH_OK;
+}
+
+// DiagHam's highest-bit lookup table (FermionOnSphere::GenerateLookUpTable, FermionOnSphere.cc:1659):
+// for each highest orbital l, table[l][v] = first index of the block of states with highest orbital l
+// whose prefix (word >> shift[l]) is below v, the block start for v above every prefix and the block
+// end (next block start, dim - 1 for the last block) for v at or below every prefix.
+int build_lookup(dh_space_s* sp) {
+  if (sp->lookup.ptr) return DH_OK;
+  const int L = sp->lz_max;
+  // DiagHam's width from the memory budget, capped to what stays in shared memory
+  unsigned long mem = sp->memory / (sizeof(int*) * (unsigned long)(L + 1));
+  int bits = 1;
+  while (mem > 0) {
+    mem >>= 1;
+    ++bits;
+  }
+  if (bits > L + 1) bits = L + 1;
+  while (bits > 1 && (size_t)(L + 1) * (((size_t)1 << bits) + 1) * sizeof(int) > (size_t)DH_LOOKUP_SMEM_BYTES) --bits;
+  sp->lookup_bits = bits;
+  const int64_t dim = sp->dim;
+  std::vector<uint64_t> w(dim);
+  DH_CUDA(cudaMemcpy(w.data(), sp->words.ptr, dim * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  const int64_t width = ((int64_t)1 << bits) + 1;
+  std::vector<int32_t> table((size_t)(L + 1) * width, -1), shift(L + 1);
+  for (int l = 0; l <= L; ++l) shift[l] = (l < bits) ? 0 : l + 1 - bits;
+  int64_t start = 0;
+  while (start < dim) {
+    const int l = 63 - __builtin_clzll(w[start] | 1ull);
+    int64_t end = start;
+    while (end < dim && (63 - __builtin_clzll(w[end] | 1ull)) == l) ++end;
+    const int64_t block_end = (end < dim) ? end : dim - 1;
+    int64_t idx = start;
+    for (int64_t v = width - 1; v >= 0; --v) {
+      while (idx < end && (int64_t)(w[idx] >> shift[l]) >= v) ++idx;
+      table[(size_t)l * width + v] = (int32_t)((idx < end) ? idx : block_end);
+    }
+    start = end;
+  }
+  int rc;
+  if ((rc = sp->lookup.alloc(table.size() * sizeof(int32_t))) != DH_OK) return rc;
+  if ((rc = sp->lookup_shift.alloc(shift.size() * sizeof(int32_t))) != DH_OK) return rc;
+  DH_CUDA(cudaMemcpy(sp->lookup.ptr, table.data(), table.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  DH_CUDA(cudaMemcpy(sp->lookup_shift.ptr, shift.data(), shift.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  return DH_OK;
+}
+
+FqheDevice fqhe_device(const dh_space_s* sp, const dh_hamiltonian_s* h, int precision) {
+  FqheDevice f = {};
+  f.words = sp->words.as<uint64_t>();
+  f.low_rank = sp->low_rank.as<uint16_t>();
+  f.high_offset = sp->high_offset.as<int32_t>();
+  f.lookup = sp->lookup.as<int32_t>();
+  f.lookup_shift = sp->lookup_shift.as<int32_t>();
+  f.dim = sp->dim;
+  f.lz_max = sp->lz_max;
+  f.low_bits = sp->rank.low_bits;
+  f.lookup_bits = sp->lookup_bits;
+  f.index_mode = sp->index_mode;
+  if (h) {
+    f.pair_offset = h->pair_offset.as<int32_t>();
+    f.factors = (precision == DH_PRECISION_FP32) ? h->factors32.ptr : h->factors64.ptr;
+    f.nbr_pairs = h->tabs.nbr_pairs;
+    f.nbr_factors = h->tabs.nbr_factors;
+  }
+  return f;
+}
+
+SpinDevice spin_device(const dh_space_s* sp, const dh_hamiltonian_s* h) {
+  SpinDevice s = {};
+  s.words = sp->words.as<uint32_t>();
+  s.dim = sp->dim;
+  s.length = sp->length;
+  s.nbr_up = sp->nbr_up;
+  if (h) {
+    s.j1 = h->j1;
+    s.j2 = h->j2;
+  }
+  return s;
+}
+
+int upload_factors(dh_hamiltonian_s* h) {
+  const InteractionTables& t = h->tabs;
+  std::vector<float> f32(t.nbr_factors);
+  for (int i = 0; i < t.nbr_factors; ++i) f32[i] = (float)t.factors[i];
+  DH_CUDA(cudaMemcpyAsync(h->factors64.ptr, t.factors.data(), t.nbr_factors * sizeof(double), cudaMemcpyHostToDevice,
+                          h->stream));
+  DH_CUDA(cudaMemcpyAsync(h->factors32.ptr, f32.data(), t.nbr_factors * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+  DH_CUDA(cudaStreamSynchronize(h->stream));
+  return DH_OK;
+}
+
+int ensure_buffer(DevBuf& b, size_t bytes) {
+  if (b.ptr && b.bytes >= bytes) return DH_OK;
+  return b.alloc(bytes);
+}
+
+// y (+)= H x for nvec vectors stored one after the other (stride dim); x, y device pointers.
+// In FP32 mode x is converted to FP32 first and the diagonal (shift) term uses the FP64 x.
+int hamiltonian_apply(dh_hamiltonian_s* h, const double* x, double* y, int nvec, int64_t first, int64_t nbr,
+                      int accumulate, const float* x32_ready, cudaStream_t stream) {
+  dh_space_s* sp = h->space;
+  const int64_t dim = sp->dim;
+  MatvecArgs a = {};
+  a.y = y;
+  a.ld = 1;
+  a.vstride = dim;
+  a.ld_y = 1;
+  a.vstride_y = dim;
+  a.nbr_vectors = nvec;
+  a.shift = h->shift;
+  a.col_first = first;
+  a.col_last = first + nbr;
+  a.row_first = first;
+  a.row_last = first + nbr;
+  a.accumulate = accumulate;
+  int rc;
+  if (h->precision == DH_PRECISION_FP32) {
+    const float* x32 = x32_ready;
+    if (!x32) {
+      if ((rc = ensure_buffer(h->x32, (size_t)dim * nvec * sizeof(float))) != DH_OK) return rc;
+      if ((rc = launch_convert_f32(x, h->x32.as<float>(), dim * nvec, stream)) != DH_OK) return rc;
+      x32 = h->x32.as<float>();
+    }
+    a.x = x32;
+    a.xdiag = x;
+  } else {
+    a.x = x;
+    a.xdiag = nullptr;
+  }
+  if (sp->kind == SPACE_FERMION) {
+    if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
+    return launch_fqhe_matvec(fqhe_device(sp, h, h->precision), a, h->precision, stream);
+  }
+  return launch_spin_matvec(spin_device(sp, h), a, h->precision, stream);
+}
+
+}  // namespace dh
+
+// ===================================================================== C ABI
+
+extern "C" {
+
+const char* dh_last_error(void) { return dh::last_error(); }
+
+const char* dh_version(void) { return "diagham_b200 0.1 (sm_100a)"; }
+
+int dh_device_count(int* count) {
+  DH_CHECK(count, DH_ERR_ARGUMENT, "null count");
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    n = 0;
+  }
+  *count = n;
+  return DH_OK;
+}
+
+int dh_fermion_on_sphere_create(int nbr_fermions, int total_lz, int lz_max, unsigned long memory, dh_space_t* out) {
+  DH_CHECK(out, DH_ERR_ARGUMENT, "null output handle");
+  *out = nullptr;
+  DH_CHECK(nbr_fermions >= 1, DH_ERR_ARGUMENT, "FermionOnSphere: nbr_fermions must be >= 1");
+  DH_CHECK(lz_max >= nbr_fermions - 1, DH_ERR_ARGUMENT, "FermionOnSphere: %d fermions do not fit in %d orbitals",
+           nbr_fermions, lz_max + 1);
+  DH_CHECK(lz_max <= 40, DH_ERR_UNSUPPORTED, "FermionOnSphere: lz_max = %d > 40 is not supported", lz_max);
+  const int twice = total_lz + nbr_fermions * lz_max;
+  DH_CHECK(twice >= 0 && (twice & 1) == 0, DH_ERR_ARGUMENT,
+           "FermionOnSphere: total_lz = %d is not reachable by %d fermions with lz_max = %d", total_lz, nbr_fermions,
+           lz_max);
+  dh_space_s* sp = new (std::nothrow) dh_space_s();
+  DH_CHECK(sp, DH_ERR_MEMORY, "out of host memory");
+  sp->kind = SPACE_FERMION;
+  sp->nbr_fermions = nbr_fermions;
+  sp->lz_max = lz_max;
+  sp->total_lz = total_lz;
+  sp->total_sum = twice / 2;
+  sp->memory = memory;
+  sp->index_mode = DH_INDEX_RANK;
+  int rc = build_fermion_space(sp);
+  if (rc != DH_OK) {
+    delete sp;
+    return rc;
+  }
+  *out = sp;
+  return DH_OK;
+}
+
+int dh_spin12_chain_create(int chain_length, int sz, int memory, dh_space_t* out) {
+  DH_CHECK(out, DH_ERR_ARGUMENT, "null output handle");
+  *out = nullptr;
+  (void)memory;
+  DH_CHECK(chain_length >= 1 && chain_length <= 32, DH_ERR_UNSUPPORTED, "Spin1_2Chain: chain length %d not in 1..32",
+           chain_length);
+  DH_CHECK(((chain_length + sz) & 1) == 0 && sz >= -chain_length && sz <= chain_length, DH_ERR_ARGUMENT,
+           "Spin1_2Chain: sz = %d is not reachable with %d spins", sz, chain_length);
+  dh_space_s* sp = new (std::nothrow) dh_space_s();
+  DH_CHECK(sp, DH_ERR_MEMORY, "out of host memory");
+  sp->kind = SPACE_SPIN12;
+  sp->length = chain_length;
+  sp->sz = sz;
+  sp->nbr_up = (chain_length + sz) / 2;
+  long long c = 1;
+  for (int q = 1; q <= sp->nbr_up; ++q) c = c * (chain_length - sp->nbr_up + q) / q;
+  sp->dim = c;
+  sp->index_mode = DH_INDEX_RANK;
+  int rc = sp->words.alloc((size_t)sp->dim * sizeof(uint32_t));
+  if (rc == DH_OK) rc = launch_spin_unrank(chain_length, sp->nbr_up, sp->dim, sp->words.as<uint32_t>(), 0);
+  if (rc == DH_OK && cudaDeviceSynchronize() != cudaSuccess) rc = cuda_fail(cudaGetLastError(), "unrank", __FILE__, __LINE__);
+  if (rc != DH_OK) {
+    delete sp;
+    return rc;
+  }
+  *out = sp;
+  return DH_OK;
+}
+
+int dh_space_destroy(dh_space_t space) {
+  delete space;
+  return DH_OK;
+}
+
+int dh_space_get_dimension(dh_space_t space, int64_t* dim) {
+  DH_CHECK(space && dim, DH_ERR_ARGUMENT, "null argument");
+  *dim = space->dim;
+  return DH_OK;
+}
+
+int dh_space_get_states(dh_space_t sp, uint64_t* words, int* lz_max, int64_t first, int64_t n) {
+  DH_CHECK(sp && words, DH_ERR_ARGUMENT, "null argument");
+  DH_CHECK(first >= 0 && n >= 0 && first + n <= sp->dim, DH_ERR_ARGUMENT, "state range out of bounds");
+  if (n == 0) return DH_OK;
+  if (sp->kind == SPACE_FERMION) {
+    DH_CUDA(cudaMemcpy(words, sp->words.as<uint64_t>() + first, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    if (lz_max)
+      for (int64_t i = 0; i < n; ++i) lz_max[i] = words[i] ? 63 - __builtin_clzll(words[i]) : 0;
+  } else {
+    std::vector<uint32_t> w(n);
+    DH_CUDA(cudaMemcpy(w.data(), sp->words.as<uint32_t>() + first, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    // the reference starts from 0xffffffff, so sites L..31 stay set (Spin1_2Chain.cc:137-138)
+    const uint64_t high = (sp->length < 32) ? (0xffffffffull & ~((1ull << sp->length) - 1ull)) : 0ull;
+    for (int64_t i = 0; i < n; ++i) words[i] = (uint64_t)w[i] | high;
+    if (lz_max)
+      for (int64_t i = 0; i < n; ++i) lz_max[i] = 0;
+  }
+  return DH_OK;
+}
+
+int dh_space_set_index_mode(dh_space_t sp, int mode) {
+  DH_CHECK(sp, DH_ERR_ARGUMENT, "null space");
+  DH_CHECK(mode == DH_INDEX_RANK || mode == DH_INDEX_LOOKUP, DH_ERR_ARGUMENT, "unknown index mode %d", mode);
+  DH_CHECK(sp->kind == SPACE_FERMION || mode == DH_INDEX_RANK, DH_ERR_UNSUPPORTED,
+           "the spin chain uses its closed-form rank only");
+  if (mode == DH_INDEX_LOOKUP) {
+    int rc = build_lookup(sp);
+    if (rc != DH_OK) return rc;
+  }
+  sp->index_mode = mode;
+  return DH_OK;
+}
+
+int dh_space_find_state_index(dh_space_t sp, const uint64_t* words, int64_t n, int64_t* indices) {
+  DH_CHECK(sp && words && indices, DH_ERR_ARGUMENT, "null argument");
+  if (n <= 0) return DH_OK;
+  DevBuf dw, di;
+  const uint64_t* w = words;
+  int64_t* out = indices;
+  const bool in_dev = is_device_pointer(words), out_dev = is_device_pointer(indices);
+  int rc;
+  if (!in_dev) {
+    if ((rc = dw.alloc(n * sizeof(uint64_t))) != DH_OK) return rc;
+    DH_CUDA(cudaMemcpy(dw.ptr, words, n * sizeof(uint64_t), cudaMemcpyHostToDevice));
+    w = dw.as<uint64_t>();
+  }
+  if (!out_dev) {
+    if ((rc = di.alloc(n * sizeof(int64_t))) != DH_OK) return rc;
+    out = di.as<int64_t>();
+  }
+  if (sp->kind == SPACE_FERMION) {
+    if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
+    rc = launch_fqhe_find(fqhe_device(sp, nullptr, 0), w, n, reinterpret_cast<long long*>(out), 0);
+  } else {
+    rc = launch_spin_find(spin_device(sp, nullptr), w, n, reinterpret_cast<long long*>(out), 0);
+  }
+  if (rc != DH_OK) return rc;
+  DH_CUDA(cudaDeviceSynchronize());
+  if (!out_dev) DH_CUDA(cudaMemcpy(indices, out, n * sizeof(int64_t), cudaMemcpyDeviceToHost));
+  return DH_OK;
+}
+
+// ----------------------------------------------------------- Hamiltonians
+
+int dh_particle_on_sphere_generic_hamiltonian_create(dh_space_t sp, int nbr_particles, int lz_max,
+                                                     const double* pseudopotentials, double l2_factor,
+                                                     dh_hamiltonian_t* out) {
+  DH_CHECK(out, DH_ERR_ARGUMENT, "null output handle");
+  *out = nullptr;
+  DH_CHECK(sp && pseudopotentials, DH_ERR_ARGUMENT, "null argument");
+  DH_CHECK(sp->kind == SPACE_FERMION, DH_ERR_ARGUMENT, "ParticleOnSphereGenericHamiltonian needs a FermionOnSphere space");
+  DH_CHECK(nbr_particles == sp->nbr_fermions && lz_max == sp->lz_max, DH_ERR_ARGUMENT,
+           "Hamiltonian (N = %d, lz_max = %d) does not match its space (N = %d, lz_max = %d)", nbr_particles, lz_max,
+           sp->nbr_fermions, sp->lz_max);
+  DH_CHECK(l2_factor == 0.0, DH_ERR_UNSUPPORTED, "an L^2 term (l2_factor != 0) is not supported");
+  dh_hamiltonian_s* h = new (std::nothrow) dh_hamiltonian_s();
+  DH_CHECK(h, DH_ERR_MEMORY, "out of host memory");
+  h->space = sp;
+  h->kind = SPACE_FERMION;
+  h->tabs.build(lz_max);
+  h->v.assign(pseudopotentials, pseudopotentials + lz_max + 1);
+  h->tabs.set_pseudopotentials(h->v.data());
+  int rc;
+  if ((rc = h->pair_offset.alloc(h->tabs.pair_offset.size() * sizeof(int32_t))) != DH_OK ||
+      (rc = h->factors64.alloc(h->tabs.nbr_factors * sizeof(double))) != DH_OK ||
+      (rc = h->factors32.alloc(h->tabs.nbr_factors * sizeof(float))) != DH_OK ||
+      (rc = reducer_init(h->red, h->red_storage, 16)) != DH_OK) {
+    delete h;
+    return rc;
+  }
+  if (cudaMemcpy(h->pair_offset.ptr, h->tabs.pair_offset.data(), h->tabs.pair_offset.size() * sizeof(int32_t),
+                 cudaMemcpyHostToDevice) != cudaSuccess) {
+    delete h;
+    return cuda_fail(cudaGetLastError(), "upload pair offsets", __FILE__, __LINE__);
+  }
+  if ((rc = upload_factors(h)) != DH_OK) {
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return DH_OK;
+}
+
+int dh_spin_chain_j1j2_hamiltonian_create(dh_space_t sp, double j1, double j2, dh_hamiltonian_t* out) {
+  DH_CHECK(out, DH_ERR_ARGUMENT, "null output handle");
+  *out = nullptr;
+  DH_CHECK(sp && sp->kind == SPACE_SPIN12, DH_ERR_ARGUMENT, "the J1-J2 chain needs a Spin1_2Chain space");
+  DH_CHECK(sp->length >= 3, DH_ERR_UNSUPPORTED, "the periodic J1-J2 chain needs at least 3 sites");
+  dh_hamiltonian_s* h = new (std::nothrow) dh_hamiltonian_s();
+  DH_CHECK(h, DH_ERR_MEMORY, "out of host memory");
+  h->space = sp;
+  h->kind = SPACE_SPIN12;
+  h->j1 = j1;
+  h->j2 = j2;
+  int rc = reducer_init(h->red, h->red_storage, 16);
+  if (rc != DH_OK) {
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return DH_OK;
+}
+
+int dh_hamiltonian_destroy(dh_hamiltonian_t h) {
+  delete h;
+  return DH_OK;
+}
+
+int dh_hamiltonian_get_dimension(dh_hamiltonian_t h, int64_t* dim) {
+  DH_CHECK(h && dim, DH_ERR_ARGUMENT, "null argument");
+  *dim = h->space->dim;
+  return DH_OK;
+}
+
+int dh_hamiltonian_shift(dh_hamiltonian_t h, double shift) {
+  DH_CHECK(h, DH_ERR_ARGUMENT, "null hamiltonian");
+  h->shift = shift;
+  return DH_OK;
+}
+
+int dh_hamiltonian_set_precision(dh_hamiltonian_t h, int precision) {
+  DH_CHECK(h, DH_ERR_ARGUMENT, "null hamiltonian");
+  DH_CHECK(precision == DH_PRECISION_FP64 || precision == DH_PRECISION_FP32, DH_ERR_ARGUMENT, "unknown precision %d",
+           precision);
+  h->precision = precision;
+  return DH_OK;
+}
+
+int dh_hamiltonian_set_pseudopotentials(dh_hamiltonian_t h, const double* v) {
+  DH_CHECK(h && v, DH_ERR_ARGUMENT, "null argument");
+  DH_CHECK(h->kind == SPACE_FERMION, DH_ERR_ARGUMENT, "pseudopotentials only apply to FQHE Hamiltonians");
+  h->v.assign(v, v + h->tabs.lz_max + 1);
+  h->tabs.set_pseudopotentials(h->v.data());
+  return upload_factors(h);
+}
+
+int dh_hamiltonian_set_stream(dh_hamiltonian_t h, void* stream) {
+  DH_CHECK(h, DH_ERR_ARGUMENT, "null hamiltonian");
+  h->stream = static_cast<cudaStream_t>(stream);
+  return DH_OK;
+}
+
+static int multiply_common(dh_hamiltonian_t h, const double* src, double* dst, int nvec, int64_t first, int64_t nbr,
+                           int accumulate) {
+  DH_CHECK(h && src && dst, DH_ERR_ARGUMENT, "null argument");
+  const int64_t dim = h->space->dim;
+  if (nbr < 0) nbr = dim - first;
+  DH_CHECK(first >= 0 && first + nbr <= dim, DH_ERR_ARGUMENT, "component range [%lld, %lld) outside [0, %lld)",
+           (long long)first, (long long)(first + nbr), (long long)dim);
+  DH_CHECK(nvec >= 1, DH_ERR_ARGUMENT, "nbr_vectors must be >= 1");
+  const size_t bytes = (size_t)dim * nvec * sizeof(double);
+  const bool src_dev = is_device_pointer(src), dst_dev = is_device_pointer(dst);
+  const double* x = src;
+  double* y = dst;
+  int rc;
+  if (!src_dev) {
+    if ((rc = ensure_buffer(h->stage_x, bytes)) != DH_OK) return rc;
+    DH_CUDA(cudaMemcpyAsync(h->stage_x.ptr, src, bytes, cudaMemcpyHostToDevice, h->stream));
+    x = h->stage_x.as<double>();
+  }
+  if (!dst_dev) {
+    if ((rc = ensure_buffer(h->stage_y, bytes)) != DH_OK) return rc;
+    if (accumulate) DH_CUDA(cudaMemcpyAsync(h->stage_y.ptr, dst, bytes, cudaMemcpyHostToDevice, h->stream));
+    y = h->stage_y.as<double>();
+  }
+  if (!accumulate) {
+    // LowLevelMultiply clears the destination, then adds (AbstractHamiltonian.cc:475-476)
+    DH_CUDA(cudaMemsetAsync(y, 0, bytes, h->stream));
+  }
+  if (nbr > 0 && (rc = hamiltonian_apply(h, x, y, nvec, first, nbr, 1, nullptr, h->stream)) != DH_OK) return rc;
+  if (!dst_dev) DH_CUDA(cudaMemcpyAsync(dst, y, bytes, cudaMemcpyDeviceToHost, h->stream));
+  DH_CUDA(cudaStreamSynchronize(h->stream));
+  return DH_OK;
+}
+
+int dh_hamiltonian_low_level_add_multiply(dh_hamiltonian_t h, const double* src, double* dst, int64_t first,
+                                          int64_t nbr) {
+  return multiply_common(h, src, dst, 1, first, nbr, 1);
+}
+
+int dh_hamiltonian_low_level_multiply(dh_hamiltonian_t h, const double* src, double* dst, int64_t first, int64_t nbr) {
+  return multiply_common(h, src, dst, 1, first, nbr, 0);
+}
+
+int dh_hamiltonian_low_level_multiple_add_multiply(dh_hamiltonian_t h, const double* srcs, double* dsts,
+                                                   int nbr_vectors, int64_t first, int64_t nbr) {
+  return multiply_common(h, srcs, dsts, nbr_vectors, first, nbr, 1);
+}
+
+int dh_hamiltonian_matrix_element(dh_hamiltonian_t h, const double* v1, const double* v2, double* out) {
+  DH_CHECK(h && v1 && v2 && out, DH_ERR_ARGUMENT, "null argument");
+  const int64_t dim = h->space->dim;
+  const size_t bytes = (size_t)dim * sizeof(double);
+  int rc;
+  if ((rc = ensure_buffer(h->stage_y, bytes)) != DH_OK) return rc;
+  if ((rc = ensure_buffer(h->stage_v, 2 * bytes + 64)) != DH_OK) return rc;
+  const double* a = v1;
+  const double* b = v2;
+  double* tmp_a = h->stage_v.as<double>();
+  double* tmp_b = tmp_a + dim;
+  if (!is_device_pointer(v1)) {
+    DH_CUDA(cudaMemcpyAsync(tmp_a, v1, bytes, cudaMemcpyHostToDevice, h->stream));
+    a = tmp_a;
+  }
+  if (!is_device_pointer(v2)) {
+    DH_CUDA(cudaMemcpyAsync(tmp_b, v2, bytes, cudaMemcpyHostToDevice, h->stream));
+    b = tmp_b;
+  }
+  double* y = h->stage_y.as<double>();
+  if ((rc = hamiltonian_apply(h, b, y, 1, 0, dim, 0, nullptr, h->stream)) != DH_OK) return rc;
+  double* res = reinterpret_cast<double*>(h->stage_v.as<char>() + 2 * bytes);
+  const double* vs[1] = {a};
+  if ((rc = launch_multi_dot(vs, 1, y, dim, res, h->red, h->stream)) != DH_OK) return rc;
+  DH_CUDA(cudaMemcpyAsync(out, res, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  DH_CUDA(cudaStreamSynchronize(h->stream));
+  return DH_OK;
+}
+
+int dh_hamiltonian_row_elements(dh_hamiltonian_t h, int64_t row, int* targets, int* signs, int* factor_index, int cap,
+                                int* count) {
+  DH_CHECK(h && count && (cap == 0 || (targets && signs && factor_index)), DH_ERR_ARGUMENT, "null argument");
+  DH_CHECK(h->kind == SPACE_FERMION, DH_ERR_UNSUPPORTED, "row elements are only available for FQHE Hamiltonians");
+  DH_CHECK(row >= 0 && row < h->space->dim, DH_ERR_ARGUMENT, "row %lld out of range", (long long)row);
+  dh_space_s* sp = h->space;
+  int rc;
+  if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
+  DevBuf buf;
+  const int c = cap > 0 ? cap : 1;
+  if ((rc = buf.alloc((size_t)3 * c * sizeof(int) + 16)) != DH_OK) return rc;
+  int* dt = buf.as<int>();
+  int* ds = dt + c;
+  int* df = ds + c;
+  int* dc = df + c;
+  if ((rc = launch_fqhe_row_elements(fqhe_device(sp, h, DH_PRECISION_FP64), row, dt, ds, df, cap, dc, h->stream)) != DH_OK)
+    return rc;
+  DH_CUDA(cudaStreamSynchronize(h->stream));
+  DH_CUDA(cudaMemcpy(count, dc, sizeof(int), cudaMemcpyDeviceToHost));
+  const int n = std::min(*count, cap);
+  if (n > 0) {
+    DH_CUDA(cudaMemcpy(targets, dt, n * sizeof(int), cudaMemcpyDeviceToHost));
+    DH_CUDA(cudaMemcpy(signs, ds, n * sizeof(int), cudaMemcpyDeviceToHost));
+    DH_CUDA(cudaMemcpy(factor_index, df, n * sizeof(int), cudaMemcpyDeviceToHost));
+  }
+  return DH_OK;
+}
+
+int dh_hamiltonian_get_interaction_factors(dh_hamiltonian_t h, double* factors, int cap, int* count) {
+  DH_CHECK(h && count, DH_ERR_ARGUMENT, "null argument");
+  DH_CHECK(h->kind == SPACE_FERMION, DH_ERR_UNSUPPORTED, "interaction factors only exist for FQHE Hamiltonians");
+  *count = h->tabs.nbr_factors;
+  const int n = std::min(cap, h->tabs.nbr_factors);
+  if (factors && n > 0) memcpy(factors, h->tabs.factors.data(), n * sizeof(double));
+  return DH_OK;
+}
+
+int dh_hamiltonian_pseudopotential_adjoint(dh_hamiltonian_t h, const double* u, const double* v, double* out) {
+  DH_CHECK(h && u && v && out, DH_ERR_ARGUMENT, "null argument");
+  DH_CHECK(h->kind == SPACE_FERMION, DH_ERR_UNSUPPORTED, "the pseudopotential adjoint needs an FQHE Hamiltonian");
+  dh_space_s* sp = h->space;
+  const int64_t dim = sp->dim;
+  const size_t bytes = (size_t)dim * sizeof(double);
+  int rc;
+  if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
+  if ((rc = ensure_buffer(h->stage_v, 2 * bytes + 64)) != DH_OK) return rc;
+  const double* du = u;
+  const double* dv = v;
+  if (!is_device_pointer(u)) {
+    DH_CUDA(cudaMemcpyAsync(h->stage_v.ptr, u, bytes, cudaMemcpyHostToDevice, h->stream));
+    du = h->stage_v.as<double>();
+  }
+  if (!is_device_pointer(v)) {
+    DH_CUDA(cudaMemcpyAsync(h->stage_v.as<double>() + dim, v, bytes, cudaMemcpyHostToDevice, h->stream));
+    dv = h->stage_v.as<double>() + dim;
+  }
+  int dev = 0, sms = 0;
+  DH_CUDA(cudaGetDevice(&dev));
+  DH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int nblocks = sms * 2;
+  const int nf = h->tabs.nbr_factors;
+  if ((rc = ensure_buffer(h->bins_partial, (size_t)nblocks * nf * sizeof(double))) != DH_OK) return rc;
+  if ((rc = ensure_buffer(h->bins, (size_t)nf * sizeof(double))) != DH_OK) return rc;
+  if ((rc = launch_fqhe_bins(fqhe_device(sp, h, DH_PRECISION_FP64), du, dv, h->bins_partial.as<double>(), nblocks,
+                             h->bins.as<double>(), h->stream)) != DH_OK)
+    return rc;
+  std::vector<double> bins(nf);
+  DH_CUDA(cudaMemcpyAsync(bins.data(), h->bins.ptr, nf * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  DH_CUDA(cudaStreamSynchronize(h->stream));
+  const int nlz = h->tabs.lz_max + 1;
+  for (int m = 0; m < nlz; ++m) {
+    double acc = 0.0;
+    for (int f = 0; f < nf; ++f) acc += bins[f] * h->tabs.dfactor[(size_t)f * nlz + m];
+    out[m] = acc;
+  }
+  return DH_OK;
+}
+
+int dh_coulomb_pseudopotentials(int nbr_flux, double* v) {
+  DH_CHECK(v && nbr_flux >= 1 && nbr_flux <= 60, DH_ERR_ARGUMENT, "nbr_flux must be in 1..60");
+  coulomb_pseudopotentials(nbr_flux, v);
+  return DH_OK;
+}
+
+int dh_clebsch_gordan(int j1, int m1, int j2, int m2, int j, double* out) {
+  DH_CHECK(out, DH_ERR_ARGUMENT, "null output");
+  DH_CHECK(j1 >= 0 && j2 >= 0 && j >= 0 && j1 + j2 + j < 300, DH_ERR_ARGUMENT, "angular momenta out of range");
+  *out = clebsch_gordan(j1, m1, j2, m2, j);
+  return DH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,176 @@
+// Internal declarations of the diagham_b200 library (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/diagham_b200.h"
+
+namespace dh {
+
+// ---------------------------------------------------------------- errors
+void set_error(const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
+
+#define DH_CUDA(expr)                                                   \
+  do {                                                                  \
+    cudaError_t _e = (expr);                                            \
+    if (_e != cudaSuccess) return ::dh::cuda_fail(_e, #expr, __FILE__, __LINE__); \
+  } while (0)
+
+#define DH_CHECK(cond, code, ...)      \
+  do {                                 \
+    if (!(cond)) {                     \
+      ::dh::set_error(__VA_ARGS__);    \
+      return (code);                   \
+    }                                  \
+  } while (0)
+
+// ------------------------------------------------------- device buffers
+// A device allocation owned by a handle.  Freed in the destructor.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  int alloc(size_t n);
+  void release();
+  template <typename T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// ------------------------------------------------------ host-side maths
+// Clebsch-Gordan <j1/2 m1/2; j2/2 m2/2 | j/2 (m1+m2)/2>, every argument doubled.
+double clebsch_gordan(int j1, int m1, int j2, int m2, int j);
+// LLL Coulomb pseudopotentials V_0..V_nbrFlux on the sphere (FP64).
+void coulomb_pseudopotentials(int nbr_flux, double* v);
+
+// Interaction tables of the two-body Hamiltonian on lz_max+1 orbitals.
+struct InteractionTables {
+  int lz_max = 0;
+  int nbr_pairs = 0;                // (m1 > m2) pairs, m1 ascending then m2 ascending
+  int nbr_factors = 0;              // (pair, m3) entries with 2 m3 > m1 + m2
+  std::vector<int> pair_offset;     // first factor of each pair
+  std::vector<double> dfactor;      // [factor][m]: d factor / d V_m (factors are linear in V)
+  std::vector<double> factors;      // current factors for the current V
+  void build(int lz_max);
+  void set_pseudopotentials(const double* v);
+};
+
+// Symmetric tridiagonal eigenvalues (ascending) by implicit QL; optional eigenvectors
+// (column-major n x n) when z != nullptr.
+int tridiagonal_eigen(int n, const double* diag, const double* off, double* eig, double* z);
+// Dense symmetric eigen-decomposition (row-major a, destroyed), eigenvalues ascending, optional
+// eigenvectors (columns of z, row-major n x n).
+int symmetric_eigen(int n, double* a, double* eig, double* z);
+
+// ------------------------------------------------------------- spaces
+enum SpaceKind { SPACE_FERMION = 1, SPACE_SPIN12 = 2 };
+
+struct FermionRankTables {
+  int low_bits = 0;                 // LB: rank = high_offset[w >> LB] + low_rank[w & (2^LB - 1)]
+  int high_bits = 0;
+  std::vector<uint16_t> low_rank;   // rank among LB-bit words with equal popcount and weighted sum
+  std::vector<int32_t> high_offset; // first index of the block of states sharing the high part, -1 if none
+};
+
+// ------------------------------------------------------ kernel launchers
+struct FqheDevice {
+  const uint64_t* words;
+  const uint16_t* low_rank;
+  const int32_t* high_offset;
+  const int32_t* lookup;       // [lz_max+1][2^lookup_shift + 1] (lookup-table search mode)
+  const int32_t* lookup_shift; // per highest orbital
+  const int32_t* pair_offset;  // [nbr_pairs]
+  const void* factors;         // FP64 or FP32 [nbr_factors]
+  long long dim;
+  int lz_max;
+  int low_bits;
+  int lookup_bits;
+  int nbr_pairs;
+  int nbr_factors;
+  int index_mode;              // DH_INDEX_RANK or DH_INDEX_LOOKUP
+};
+
+struct MatvecArgs {
+  const void* x;       // gather source: element (i, j) at x[i * ld + j * vstride]
+  void* y;             // output: element (i, j) at y[i * ld_y + j * vstride_y]
+  const double* xdiag; // optional FP64 source for the diagonal (shift) term (same layout as x); null = x
+  long long ld, vstride, ld_y, vstride_y;
+  int nbr_vectors;
+  double shift;
+  long long col_first, col_last; // only columns (targets) in [col_first, col_last) contribute
+  long long row_first, row_last; // rows that receive the diagonal (shift) contribution
+  int accumulate;                // y += H x (1) or y = H x (0)
+};
+
+int launch_fqhe_unrank(int nbr_fermions, int lz_max, int total_sum, long long dim, uint64_t* words,
+                       const int64_t* counts_dev, int count_stride_o, int count_stride_s, cudaStream_t s);
+int launch_fqhe_matvec(const FqheDevice& f, const MatvecArgs& a, int precision, cudaStream_t s);
+int launch_fqhe_row_elements(const FqheDevice& f, long long row, int* targets, int* signs, int* factor_index,
+                             int cap, int* count, cudaStream_t s);
+int launch_fqhe_bins(const FqheDevice& f, const double* u, const double* v, double* partial_bins, int nblocks,
+                     double* bins, cudaStream_t s);
+int launch_fqhe_find(const FqheDevice& f, const uint64_t* words, long long n, long long* out, cudaStream_t s);
+
+struct SpinDevice {
+  const uint32_t* words;
+  long long dim;
+  int length;
+  int nbr_up;
+  double j1, j2;
+};
+int launch_spin_unrank(int length, int nbr_up, long long dim, uint32_t* words, cudaStream_t s);
+int launch_spin_matvec(const SpinDevice& sp, const MatvecArgs& a, int precision, cudaStream_t s);
+int launch_spin_find(const SpinDevice& sp, const uint64_t* words, long long n, long long* out, cudaStream_t s);
+
+// BLAS-1 style kernels on FP64 vectors (device-resident scalars)
+struct Reducer {
+  double* partial = nullptr;   // [nblocks * width]
+  unsigned int* ticket = nullptr;
+  int nblocks = 0;
+  int width = 0;
+};
+int reducer_init(Reducer& r, DevBuf& storage, int width);
+int launch_multi_dot(const double* const* vs, int m, const double* y, long long n, double* out, Reducer& r,
+                     cudaStream_t s);
+int launch_lanczos_update(double* w, const double* y, const double* a, const double* b, const double* ca,
+                          const double* cb, long long n, double* norm_out, Reducer& r, cudaStream_t s);
+int launch_scale_convert(double* v, float* v32, const double* norm, long long n, cudaStream_t s);
+int launch_axpy_scalar(double* y, const double* x, double a, long long n, cudaStream_t s);
+int launch_random_vector(double* x, long long n, uint64_t seed, cudaStream_t s);
+int launch_convert_f32(const double* v, float* v32, long long n, cudaStream_t s);
+int launch_gemm_tall(const double* v, long long n, int k, const double* c, int m, double* out, int accumulate,
+                     cudaStream_t s);
+int launch_gram(const double* a, int ka, const double* b, int kb, long long n, double* out, Reducer& r,
+                cudaStream_t s);
+
+// Device view of a Lanczos run (three rotating FP64 vectors, device scalars, optional store).
+struct LanczosDev {
+  double* vec;        // 3 * dim, slot q at vec + q * dim
+  long long dim;
+  float* x32;         // FP32 copy of the newest vector (null in FP64 mode)
+  double* krylov;     // Krylov store (null if not kept); vector j at krylov + j * dim
+  int krylov_cap;
+  double* alpha;
+  double* beta;
+  double* norm;
+  int* cursor;
+  double* partial;
+  unsigned int* ticket;
+  int nblocks;
+};
+int launch_sqrt_inplace(double* x, cudaStream_t s);
+int launch_lz_update(const LanczosDev& st, int phase, cudaStream_t s);
+int launch_lz_scale(const LanczosDev& st, int phase, cudaStream_t s);
+int launch_lz_dots(const LanczosDev& st, int phase, cudaStream_t s);
+int launch_combine(const double* vs, int m, long long ld, const double* coef, double sign, double* out, int accumulate,
+                   long long n, cudaStream_t s);
+int launch_strided_dots(const double* vs, int m, long long ld, const double* y, long long n, double* out, Reducer& r,
+                        cudaStream_t s);
+
+}  // namespace dh

@@ -1,0 +1,357 @@
+// Host-side set-up maths of the engine: Clebsch-Gordan coefficients, Coulomb pseudopotentials,
+// the interaction-factor tables of ParticleOnSphereGenericHamiltonian, and the small FP64
+// eigensolvers used on the Lanczos tridiagonal / band matrices.
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "dh_internal.h"
+
+namespace dh {
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_last_error;
+
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+}
+
+const char* last_error() { return g_last_error.c_str(); }
+
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
+  set_error("CUDA error %d (%s) in %s at %s:%d", (int)e, cudaGetErrorString(e), what, file, line);
+  return e == cudaErrorMemoryAllocation ? DH_ERR_MEMORY : DH_ERR_CUDA;
+}
+
+int DevBuf::alloc(size_t n) {
+  release();
+  if (n == 0) n = 16;
+  cudaError_t e = cudaMalloc(&ptr, n);
+  if (e != cudaSuccess) {
+    ptr = nullptr;
+    return cuda_fail(e, "cudaMalloc", __FILE__, __LINE__);
+  }
+  bytes = n;
+  return DH_OK;
+}
+
+void DevBuf::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+// ---------------------------------------------- double-double arithmetic
+// Two doubles hi + lo carry ~32 significant digits; Racah's alternating sum for the
+// Clebsch-Gordan coefficients cancels up to ~10 digits at 2S = 33, so it is summed in this format.
+namespace {
+struct DD {
+  double hi, lo;
+};
+inline DD dd(double a) { return {a, 0.0}; }
+inline DD quick_two_sum(double a, double b) {
+  double s = a + b;
+  return {s, b - (s - a)};
+}
+inline DD two_sum(double a, double b) {
+  double s = a + b, v = s - a;
+  return {s, (a - (s - v)) + (b - v)};
+}
+inline DD operator+(DD a, DD b) {
+  DD s = two_sum(a.hi, b.hi), t = two_sum(a.lo, b.lo);
+  s.lo += t.hi;
+  s = quick_two_sum(s.hi, s.lo);
+  s.lo += t.lo;
+  return quick_two_sum(s.hi, s.lo);
+}
+inline DD operator-(DD a) { return {-a.hi, -a.lo}; }
+inline DD operator*(DD a, DD b) {
+  double p = a.hi * b.hi;
+  double e = fma(a.hi, b.hi, -p) + (a.hi * b.lo + a.lo * b.hi);
+  return quick_two_sum(p, e);
+}
+inline DD operator/(DD a, DD b) {
+  double q1 = a.hi / b.hi;
+  DD r = a + (-(dd(q1) * b));
+  double q2 = r.hi / b.hi;
+  r = r + (-(dd(q2) * b));
+  double q3 = r.hi / b.hi;
+  return quick_two_sum(q1, q2) + dd(q3);
+}
+inline DD dd_sqrt(DD a) {
+  if (a.hi <= 0.0) return dd(0.0);
+  double x = sqrt(a.hi);
+  DD r = a + (-(dd(x) * dd(x)));
+  return quick_two_sum(x, r.hi / (2.0 * x));
+}
+
+constexpr int kMaxFactorial = 170;
+const std::vector<DD>& factorials() {
+  static std::vector<DD> f;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    f.resize(kMaxFactorial + 1);
+    f[0] = dd(1.0);
+    for (int n = 1; n <= kMaxFactorial; ++n) f[n] = f[n - 1] * dd((double)n);
+  });
+  return f;
+}
+}  // namespace
+
+// Racah's formula for <j1 m1; j2 m2 | j m1+m2>, Condon-Shortley phase; doubled arguments.
+double clebsch_gordan(int j1, int m1, int j2, int m2, int j) {
+  const std::vector<DD>& F = factorials();
+  int m = m1 + m2;
+  if (abs(m1) > j1 || abs(m2) > j2 || abs(m) > j) return 0.0;
+  if (((j1 + m1) | (j2 + m2) | (j + m) | (j1 + j2 + j)) & 1) return 0.0;
+  if (j < abs(j1 - j2) || j > j1 + j2) return 0.0;
+  if ((j1 + j2 + j) / 2 + 1 > kMaxFactorial) return NAN;
+  const int a = (j1 + j2 - j) / 2, b = (j1 - j2 + j) / 2, c = (j2 - j1 + j) / 2, d = (j1 + j2 + j) / 2 + 1;
+  const int jm1 = (j1 - m1) / 2, jp1 = (j1 + m1) / 2, jm2 = (j2 - m2) / 2, jp2 = (j2 + m2) / 2;
+  const int Jm = (j - m) / 2, Jp = (j + m) / 2;
+  const int e1 = (j - j2 + m1) / 2, e2 = (j - j1 - m2) / 2;
+  DD norm2 = dd((double)(j + 1)) * F[a] * F[b] * F[c] / F[d];
+  norm2 = norm2 * (F[Jp] * F[Jm] * F[jm1] * F[jp1] * F[jm2] * F[jp2]);
+  int kmin = std::max(0, std::max(-e1, -e2));
+  int kmax = std::min(a, std::min(jm1, jp2));
+  DD sum = dd(0.0);
+  for (int k = kmin; k <= kmax; ++k) {
+    DD t = dd(1.0) / (F[k] * F[a - k] * F[jm1 - k] * F[jp2 - k] * F[e1 + k] * F[e2 + k]);
+    sum = (k & 1) ? sum + (-t) : sum + t;
+  }
+  DD r = dd_sqrt(norm2) * sum;
+  return r.hi + r.lo;
+}
+
+// Lowest-Landau-level Coulomb pseudopotentials on the sphere: the multipole expansion of
+// PseudoPotentials.cc:35-85 (landau level 0, zero layer separation, so all form factors are 1).
+void coulomb_pseudopotentials(int nbr_flux, double* v) {
+  const int mm = nbr_flux, n = nbr_flux + 1;
+  std::vector<double> cg_pair(n * n), cg_j((size_t)n * n * n), cg_top(n);
+  for (int l = 0; l < n; ++l)
+    for (int i = 0; i < n; ++i) cg_pair[l * n + i] = clebsch_gordan(mm, 2 * i - mm, mm, mm - 2 * i, 2 * l);
+  for (int j = 0; j < n; ++j) {
+    cg_top[j] = clebsch_gordan(mm, mm, 2 * j, 0, mm);
+    for (int i1 = 0; i1 < n; ++i1)
+      for (int i2 = 0; i2 < n; ++i2)
+        cg_j[((size_t)j * n + i1) * n + i2] = clebsch_gordan(mm, 2 * i1 - mm, 2 * j, 2 * (i2 - i1), mm);
+  }
+  // inner[i1][i2] = sum_{j >= |m1 - m2|} (-1)^(j - jmin) (<S m1; j m2-m1|S m2> <S S; j 0|S S>)^2
+  std::vector<double> inner((size_t)n * n);
+  for (int i1 = 0; i1 < n; ++i1)
+    for (int i2 = 0; i2 < n; ++i2) {
+      double acc = 0.0, sgn = 1.0;
+      for (int j = abs(i1 - i2); j <= mm; ++j) {
+        double t = cg_j[((size_t)j * n + i1) * n + i2] * cg_top[j];
+        acc += sgn * t * t;
+        sgn = -sgn;
+      }
+      inner[(size_t)i1 * n + i2] = acc;
+    }
+  for (int l = 0; l < n; ++l) {
+    double total = 0.0;
+    for (int i1 = 0; i1 < n; ++i1)
+      for (int i2 = 0; i2 < n; ++i2) total += cg_pair[l * n + i1] * cg_pair[l * n + i2] * inner[(size_t)i1 * n + i2];
+    v[mm - l] = total / sqrt(0.5 * nbr_flux);
+  }
+}
+
+// ------------------------------------------------------ interaction tables
+// Pair (m1 > m2) order: m1 ascending, then m2 ascending (pair index m1 (m1 - 1) / 2 + m2); per pair the
+// m3 with 2 m3 > m1 + m2 and m4 = m1 + m2 - m3 >= 0 ascending (m3 = floor(M / 2) + 1 .. min(M, lzmax)).
+// The factor of (m1, m2, m3) is -4 sum_J V_{lzmax - J/2} <m1 m2|J> <m3 m4|J> over odd relative
+// angular momentum (ParticleOnSphereGenericHamiltonian.cc:509-606); it is linear in V, so the
+// table stores d factor / d V_m and the factors of any V are one contraction away.
+void InteractionTables::build(int lzmax) {
+  lz_max = lzmax;
+  const int nlz = lzmax + 1;
+  const int parity = (lzmax & 1) ? 0 : 1;
+  nbr_pairs = nlz * lzmax / 2;
+  pair_offset.assign(nbr_pairs + 1, 0);
+  int nf = 0;
+  for (int m1 = 0; m1 < nlz; ++m1)
+    for (int m2 = 0; m2 < m1; ++m2) {
+      int p = m1 * (m1 - 1) / 2 + m2;
+      pair_offset[p] = nf;
+      int M = m1 + m2;
+      nf += std::min(M, lzmax) - (M / 2 + 1) + 1;
+    }
+  pair_offset[nbr_pairs] = nf;
+  nbr_factors = nf;
+  dfactor.assign((size_t)nf * nlz, 0.0);
+  // CG table over the pair's doubled projections: cg[(i1 * nlz + i2) * nlz + J/2]
+  std::vector<double> cg((size_t)nlz * nlz * nlz, 0.0);
+  for (int i1 = 0; i1 < nlz; ++i1)
+    for (int i2 = 0; i2 < nlz; ++i2)
+      for (int J = 0; J <= 2 * lzmax; J += 2)
+        cg[((size_t)i1 * nlz + i2) * nlz + J / 2] = clebsch_gordan(lzmax, 2 * i1 - lzmax, lzmax, 2 * i2 - lzmax, J);
+  for (int m1 = 0; m1 < nlz; ++m1)
+    for (int m2 = 0; m2 < m1; ++m2) {
+      int M = m1 + m2;
+      int f = pair_offset[m1 * (m1 - 1) / 2 + m2];
+      for (int m3 = M / 2 + 1; m3 <= std::min(M, lzmax); ++m3, ++f) {
+        int m4 = M - m3;
+        for (int J = abs(2 * M - 2 * lzmax); J <= 2 * lzmax; J += 2) {
+          if (((J >> 1) & 1) != parity) continue;
+          double c12 = cg[((size_t)m1 * nlz + m2) * nlz + J / 2];
+          double c34 = cg[((size_t)m3 * nlz + m4) * nlz + J / 2];
+          dfactor[(size_t)f * nlz + (lzmax - J / 2)] = -4.0 * c12 * c34;
+        }
+      }
+    }
+  factors.assign(nf, 0.0);
+}
+
+void InteractionTables::set_pseudopotentials(const double* v) {
+  const int nlz = lz_max + 1;
+  // J ascending (m descending), as the reference accumulates its Clebsch-Gordan sum
+  for (int f = 0; f < nbr_factors; ++f) {
+    double acc = 0.0;
+    for (int m = lz_max; m >= 0; --m) acc += v[m] * dfactor[(size_t)f * nlz + m];
+    factors[f] = acc;
+  }
+}
+
+// ------------------------------------------------------------ eigensolvers
+// Implicit QL with Wilkinson shifts on a symmetric tridiagonal matrix; eigenvectors are the
+// accumulated rotations (z column-major n x n, columns = eigenvectors), sorted ascending.
+int tridiagonal_eigen(int n, const double* diag, const double* off, double* eig, double* z) {
+  std::vector<double> d(diag, diag + n), e(n + 1, 0.0);
+  for (int i = 0; i + 1 < n; ++i) e[i] = off[i];
+  if (z) {
+    std::fill(z, z + (size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) z[(size_t)i * n + i] = 1.0;
+  }
+  for (int l = 0; l < n; ++l) {
+    int iter = 0;
+    for (;;) {
+      int m = l;
+      for (; m + 1 < n; ++m) {
+        double s = fabs(d[m]) + fabs(d[m + 1]);
+        if (fabs(e[m]) <= 2.220446049250313e-16 * s || fabs(e[m]) < 1e-300) break;
+      }
+      if (m == l) break;
+      if (++iter > 300) {
+        set_error("tridiagonal QL did not converge");
+        return DH_ERR_NOT_CONVERGED;
+      }
+      double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+      double r = hypot(g, 1.0);
+      g = d[m] - d[l] + e[l] / (g + (g >= 0 ? r : -r));
+      double s = 1.0, c = 1.0, p = 0.0;
+      int i = m - 1;
+      bool deflated = false;
+      for (; i >= l; --i) {
+        double f = s * e[i], b = c * e[i];
+        r = hypot(f, g);
+        e[i + 1] = r;
+        if (r == 0.0) {
+          d[i + 1] -= p;
+          e[m] = 0.0;
+          deflated = true;
+          break;
+        }
+        s = f / r;
+        c = g / r;
+        g = d[i + 1] - p;
+        r = (d[i] - g) * s + 2.0 * c * b;
+        p = s * r;
+        d[i + 1] = g + p;
+        g = c * r - b;
+        if (z) {
+          double* zi = z + (size_t)i * n;
+          double* zi1 = z + (size_t)(i + 1) * n;
+          for (int k = 0; k < n; ++k) {
+            double t = zi1[k];
+            zi1[k] = s * zi[k] + c * t;
+            zi[k] = c * zi[k] - s * t;
+          }
+        }
+      }
+      if (deflated) continue;
+      d[l] -= p;
+      e[l] = g;
+      e[m] = 0.0;
+    }
+  }
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return d[a] < d[b]; });
+  for (int i = 0; i < n; ++i) eig[i] = d[order[i]];
+  if (z) {
+    std::vector<double> tmp((size_t)n * n);
+    for (int i = 0; i < n; ++i) memcpy(&tmp[(size_t)i * n], z + (size_t)order[i] * n, sizeof(double) * n);
+    memcpy(z, tmp.data(), sizeof(double) * n * n);
+  }
+  return DH_OK;
+}
+
+// Householder reduction of a dense symmetric matrix to tridiagonal form, then implicit QL.
+// a (row-major n x n) is overwritten; z (row-major, columns = eigenvectors) optional.
+int symmetric_eigen(int n, double* a, double* eig, double* z) {
+  if (n == 0) return DH_OK;
+  std::vector<double> hv((size_t)n * n, 0.0), hnorm(n, 0.0), v(n), p(n);
+  for (int k = 0; k + 2 < n; ++k) {
+    double alpha = 0.0;
+    for (int i = k + 1; i < n; ++i) alpha += a[(size_t)i * n + k] * a[(size_t)i * n + k];
+    alpha = sqrt(alpha);
+    if (alpha == 0.0) continue;
+    double x0 = a[(size_t)(k + 1) * n + k];
+    if (x0 > 0) alpha = -alpha;
+    std::fill(v.begin(), v.end(), 0.0);
+    v[k + 1] = x0 - alpha;
+    for (int i = k + 2; i < n; ++i) v[i] = a[(size_t)i * n + k];
+    double vn2 = 0.0;
+    for (int i = k + 1; i < n; ++i) vn2 += v[i] * v[i];
+    if (vn2 == 0.0) continue;
+    // A <- H A H, H = I - 2 v v^T / |v|^2, as A - v w^T - w v^T
+    for (int i = 0; i < n; ++i) {
+      double s = 0.0;
+      for (int j = k + 1; j < n; ++j) s += a[(size_t)i * n + j] * v[j];
+      p[i] = 2.0 * s / vn2;
+    }
+    double K = 0.0;
+    for (int i = k + 1; i < n; ++i) K += v[i] * p[i];
+    K /= vn2;
+    for (int i = 0; i < n; ++i) p[i] -= K * v[i];
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) a[(size_t)i * n + j] -= v[i] * p[j] + p[i] * v[j];
+    memcpy(&hv[(size_t)k * n], v.data(), sizeof(double) * n);
+    hnorm[k] = vn2;
+  }
+  std::vector<double> d(n), off(n > 1 ? n - 1 : 1, 0.0);
+  for (int k = 0; k < n; ++k) d[k] = a[(size_t)k * n + k];
+  for (int k = 0; k + 1 < n; ++k) off[k] = a[(size_t)(k + 1) * n + k];
+  std::vector<double> zt;
+  if (z) zt.resize((size_t)n * n);
+  int rc = tridiagonal_eigen(n, d.data(), off.data(), eig, z ? zt.data() : nullptr);
+  if (rc != DH_OK || !z) return rc;
+  // eigenvectors of A = H_0 H_1 ... H_{n-3} (eigenvectors of T)
+  for (int c = 0; c < n; ++c)
+    for (int r = 0; r < n; ++r) z[(size_t)r * n + c] = zt[(size_t)c * n + r];
+  for (int k = n - 3; k >= 0; --k) {
+    if (hnorm[k] == 0.0) continue;
+    const double* hk = &hv[(size_t)k * n];
+    for (int c = 0; c < n; ++c) {
+      double s = 0.0;
+      for (int i = k + 1; i < n; ++i) s += hk[i] * z[(size_t)i * n + c];
+      s = 2.0 * s / hnorm[k];
+      for (int i = k + 1; i < n; ++i) z[(size_t)i * n + c] -= s * hk[i];
+    }
+  }
+  return DH_OK;
+}
+
+}  // namespace dh

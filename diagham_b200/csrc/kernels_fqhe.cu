@@ -1,0 +1,460 @@
+// Pull-form, atomic-free H.x for spin-polarised fermions on the sphere (sm_100a).
+//
+// One thread owns one basis row r; the 32 lanes of a warp own 32 consecutive rows, so rows that
+// share their high orbitals (most of a warp) walk the same (m1, m2) pairs in lock-step and the
+// gathers of moves confined to high orbitals land on consecutive x entries (coalesced).
+//
+// Per row (FermionOnSphere word s, bit m = orbital m):
+//   for every occupied pair m1 > m2 (descending), a = s - m1 - m2, M = m1 + m2:
+//     the admissible creations m3 > m4 = M - m3 (both empty in a) are the set bits of
+//       e & mirror_M(e) & [m3 > M/2],  e = empty orbitals of a,  mirror_M(e) bit p = e bit (M - p)
+//     sign = (-1)^(1 + |s in (m2, m1)| + |a in (m4, m3)|)  -- the AA * AdAd sign of
+//            FermionOnSphere::AA (FermionOnSphere.cc:790) and ::AdAd (:949), from popcounts
+//     target t = a + m3 + m4, index(t) = high_offset[t >> LB] + low_rank[t & (2^LB - 1)]
+//            (or DiagHam's lookup table + binary search, FermionOnSphere.cc:1431)
+//     y[r] += sign * factor(m1, m2, m3) * x[index(t)]
+// H is real symmetric, so this pull form equals the reference's push form
+// (AbstractQHEOnSphereHamiltonian.cc:456-488) up to FP rounding.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dh_internal.h"
+
+namespace dh {
+
+namespace {
+
+constexpr int kMatvecThreads = 256;
+
+__device__ __forceinline__ uint64_t between_mask(int lo, int hi) {
+  // bits strictly between lo and hi (lo < hi <= 63)
+  return ((1ull << hi) - 1ull) & ~((2ull << lo) - 1ull);
+}
+
+__device__ __forceinline__ uint64_t mirror_bits(uint64_t e, int M) {
+  // bit p of the result = bit (M - p) of e (0 when M - p is outside 0..63)
+  uint64_t r = __brevll(e);
+  return (M <= 63) ? (r >> (63 - M)) : (r << (M - 63));
+}
+
+struct SmemLayout {
+  int factor_bytes;
+  int pair_bytes;
+  int lookup_bytes;
+  int total;
+};
+
+__host__ __device__ inline int align16(int x) { return (x + 15) & ~15; }
+
+inline SmemLayout smem_layout(const FqheDevice& f, int elem) {
+  SmemLayout s;
+  s.factor_bytes = align16(f.nbr_factors * elem);
+  s.pair_bytes = align16(f.nbr_pairs * (int)sizeof(int));
+  s.lookup_bytes = 0;
+  if (f.index_mode == DH_INDEX_LOOKUP)
+    s.lookup_bytes = align16((f.lz_max + 1) * ((1 << f.lookup_bits) + 1) * (int)sizeof(int)) +
+                     align16((f.lz_max + 1) * (int)sizeof(int));
+  s.total = s.factor_bytes + s.pair_bytes + s.lookup_bytes;
+  return s;
+}
+
+template <int MODE>
+__device__ __forceinline__ long long target_index(const FqheDevice& f, uint64_t t, const int* slookup,
+                                                  const int* sshift) {
+  if (MODE == DH_INDEX_RANK) {
+    const int lb = f.low_bits;
+    return (long long)__ldg(f.high_offset + (t >> lb)) + (long long)__ldg(f.low_rank + (t & ((1ull << lb) - 1ull)));
+  } else {
+    // FermionOnSphere::FindStateIndex: the highest-bit table brackets a binary search on the
+    // descending word array (bracket [t[v + 1], t[v]], FermionOnSphere.cc:1431-1455)
+    const int l = 63 - __clzll(t);
+    const int width = (1 << f.lookup_bits) + 1;
+    const long long v = (long long)(t >> sshift[l]);
+    long long lo = slookup[l * width + v + 1];
+    long long hi = slookup[l * width + v];
+    while (hi - lo > 1) {
+      long long mid = (lo + hi) >> 1;
+      if (__ldg(f.words + mid) > t)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    return (__ldg(f.words + lo) == t) ? lo : hi;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T load_x(const T* p) {
+  return __ldg(p);
+}
+
+template <typename TG, int K, int MODE, bool RANGE>
+__global__ void __launch_bounds__(kMatvecThreads) fqhe_matvec_kernel(FqheDevice f, MatvecArgs a, SmemLayout lay) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  TG* sfac = reinterpret_cast<TG*>(smem);
+  int* spair = reinterpret_cast<int*>(smem + lay.factor_bytes);
+  int* slookup = reinterpret_cast<int*>(smem + lay.factor_bytes + lay.pair_bytes);
+  int* sshift = slookup + ((MODE == DH_INDEX_LOOKUP) ? (f.lz_max + 1) * ((1 << f.lookup_bits) + 1) : 0);
+
+  const TG* gfac = static_cast<const TG*>(f.factors);
+  for (int i = threadIdx.x; i < f.nbr_factors; i += blockDim.x) sfac[i] = gfac[i];
+  for (int i = threadIdx.x; i < f.nbr_pairs; i += blockDim.x) spair[i] = f.pair_offset[i];
+  if (MODE == DH_INDEX_LOOKUP) {
+    const int n = (f.lz_max + 1) * ((1 << f.lookup_bits) + 1);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) slookup[i] = f.lookup[i];
+    for (int i = threadIdx.x; i <= f.lz_max; i += blockDim.x) sshift[i] = f.lookup_shift[i];
+  }
+  __syncthreads();
+
+  const TG* x = static_cast<const TG*>(a.x);
+  const uint64_t full = (f.lz_max >= 63) ? ~0ull : ((1ull << (f.lz_max + 1)) - 1ull);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+    const uint64_t s = __ldg(f.words + r);
+    TG acc[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) acc[j] = TG(0);
+    uint64_t rem1 = s;
+    while (rem1) {
+      const int m1 = 63 - __clzll(rem1);
+      rem1 &= ~(1ull << m1);
+      uint64_t rem2 = rem1;
+      const int pbase = m1 * (m1 - 1) / 2;
+      while (rem2) {
+        const int m2 = 63 - __clzll(rem2);
+        rem2 &= ~(1ull << m2);
+        const uint64_t an = s & ~((1ull << m1) | (1ull << m2));
+        const int M = m1 + m2;
+        const int paa = 1 + __popcll(s & between_mask(m2, m1));
+        const uint64_t e = ~an & full;
+        uint64_t valid = e & mirror_bits(e, M) & (~0ull << (M / 2 + 1));
+        const TG* fp = sfac + (spair[pbase + m2] - (M / 2 + 1));
+        while (valid) {
+          const int m3 = __ffsll(valid) - 1;
+          valid &= valid - 1ull;
+          const int m4 = M - m3;
+          const uint64_t t = an | (1ull << m3) | (1ull << m4);
+          const int par = paa + __popcll(an & between_mask(m4, m3));
+          const long long idx = target_index<MODE>(f, t, slookup, sshift);
+          if (RANGE && (idx < a.col_first || idx >= a.col_last)) continue;
+          TG fct = fp[m3];
+          if (par & 1) fct = -fct;
+          const TG* xp = x + idx * a.ld;
+#pragma unroll
+          for (int j = 0; j < K; ++j) acc[j] += fct * load_x(xp + j * a.vstride);
+        }
+      }
+    }
+    const bool diag = (r >= a.row_first && r < a.row_last);
+    double* y = static_cast<double*>(a.y);
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      double v = (double)acc[j];
+      if (diag && a.shift != 0.0) {
+        double xd = a.xdiag ? a.xdiag[r * a.ld + j * a.vstride] : (double)x[r * a.ld + j * a.vstride];
+        v += a.shift * xd;
+      }
+      double* yp = y + r * a.ld_y + j * a.vstride_y;
+      *yp = a.accumulate ? (*yp + v) : v;
+    }
+  }
+}
+
+template <typename TG, int K, int MODE, bool RANGE>
+int launch_one(const FqheDevice& f, const MatvecArgs& a, cudaStream_t s) {
+  SmemLayout lay = smem_layout(f, sizeof(TG));
+  auto kern = fqhe_matvec_kernel<TG, K, MODE, RANGE>;
+  if (lay.total > 48 * 1024) DH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total));
+  int dev = 0, sms = 0, per_sm = 0;
+  DH_CUDA(cudaGetDevice(&dev));
+  DH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  DH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kMatvecThreads, lay.total));
+  if (per_sm < 1) {
+    set_error("fqhe matvec: %d bytes of shared memory per block do not fit", lay.total);
+    return DH_ERR_UNSUPPORTED;
+  }
+  long long need = (f.dim + kMatvecThreads - 1) / kMatvecThreads;
+  long long grid = (long long)sms * per_sm;
+  if (need < grid) grid = need;
+  if (grid < 1) grid = 1;
+  kern<<<(unsigned)grid, kMatvecThreads, lay.total, s>>>(f, a, lay);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+template <typename TG, int K>
+int dispatch_mode(const FqheDevice& f, const MatvecArgs& a, cudaStream_t s) {
+  const bool range = (a.col_first > 0 || a.col_last < f.dim);
+  if (f.index_mode == DH_INDEX_LOOKUP)
+    return range ? launch_one<TG, K, DH_INDEX_LOOKUP, true>(f, a, s) : launch_one<TG, K, DH_INDEX_LOOKUP, false>(f, a, s);
+  return range ? launch_one<TG, K, DH_INDEX_RANK, true>(f, a, s) : launch_one<TG, K, DH_INDEX_RANK, false>(f, a, s);
+}
+
+template <typename TG>
+int dispatch_k(const FqheDevice& f, MatvecArgs a, cudaStream_t s) {
+  // vectors are processed in groups of 4, 2 and 1 sharing one enumeration
+  int left = a.nbr_vectors;
+  const char* x0 = static_cast<const char*>(a.x);
+  char* y0 = static_cast<char*>(a.y);
+  const double* xd0 = a.xdiag;
+  int done = 0;
+  while (left > 0) {
+    int k = left >= 4 ? 4 : (left >= 2 ? 2 : 1);
+    MatvecArgs b = a;
+    b.x = x0 + (size_t)done * a.vstride * sizeof(TG);
+    b.y = y0 + (size_t)done * a.vstride_y * sizeof(double);
+    b.xdiag = xd0 ? xd0 + (size_t)done * a.vstride : nullptr;
+    b.nbr_vectors = k;
+    int rc = (k == 4) ? dispatch_mode<TG, 4>(f, b, s) : (k == 2 ? dispatch_mode<TG, 2>(f, b, s) : dispatch_mode<TG, 1>(f, b, s));
+    if (rc != DH_OK) return rc;
+    left -= k;
+    done += k;
+  }
+  return DH_OK;
+}
+
+// ------------------------------------------------------------- unranking
+// Word of basis index i: orbitals from the top down; with n fermions and orbital-sum s still to
+// place, the states occupying orbital p come first (descending order), and there are
+// counts[n-1][p][s-p] of them.
+__global__ void fqhe_unrank_kernel(int nbr_fermions, int lz_max, int total_sum, long long dim, uint64_t* words,
+                                   const int64_t* counts, int so, int ss) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= dim) return;
+  long long rest = i;
+  int n = nbr_fermions, sum = total_sum;
+  uint64_t w = 0;
+  for (int p = lz_max; p >= 0 && n > 0; --p) {
+    long long c = 0;
+    if (sum - p >= 0) c = counts[(size_t)(n - 1) * so + (size_t)p * ss + (sum - p)];
+    if (rest < c) {
+      w |= 1ull << p;
+      --n;
+      sum -= p;
+    } else {
+      rest -= c;
+    }
+  }
+  words[i] = w;
+}
+
+// ------------------------------------------------------ per-row dump
+// The reference enumeration order of AbstractQHEOnSphereHamiltonian::LowLevelAddMultiply
+// (:456-488): pairs m1 ascending then m2 ascending (M1Value/M2Value), m3 ascending (M3Values).
+template <int MODE>
+__global__ void fqhe_row_kernel(FqheDevice f, long long row, int* targets, int* signs, int* fidx, int cap,
+                                int* count) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int width = (1 << f.lookup_bits) + 1;
+  (void)width;
+  const uint64_t s = f.words[row];
+  const uint64_t full = (f.lz_max >= 63) ? ~0ull : ((1ull << (f.lz_max + 1)) - 1ull);
+  int n = 0;
+  for (int m1 = 1; m1 <= f.lz_max; ++m1) {
+    if (!((s >> m1) & 1)) continue;
+    for (int m2 = 0; m2 < m1; ++m2) {
+      if (!((s >> m2) & 1)) continue;
+      const uint64_t an = s & ~((1ull << m1) | (1ull << m2));
+      const int M = m1 + m2;
+      const int paa = 1 + __popcll(s & between_mask(m2, m1));
+      const uint64_t e = ~an & full;
+      uint64_t valid = e & mirror_bits(e, M) & (~0ull << (M / 2 + 1));
+      const int fb = f.pair_offset[m1 * (m1 - 1) / 2 + m2] - (M / 2 + 1);
+      while (valid) {
+        const int m3 = __ffsll(valid) - 1;
+        valid &= valid - 1ull;
+        const int m4 = M - m3;
+        const uint64_t t = an | (1ull << m3) | (1ull << m4);
+        const int par = paa + __popcll(an & between_mask(m4, m3));
+        long long idx;
+        if (MODE == DH_INDEX_RANK) {
+          idx = (long long)f.high_offset[t >> f.low_bits] + f.low_rank[t & ((1ull << f.low_bits) - 1ull)];
+        } else {
+          const int l = 63 - __clzll(t);
+          const int wdt = (1 << f.lookup_bits) + 1;
+          const long long v = (long long)(t >> f.lookup_shift[l]);
+          long long lo = f.lookup[l * wdt + v + 1], hi = f.lookup[l * wdt + v];
+          while (hi - lo > 1) {
+            long long mid = (lo + hi) >> 1;
+            if (f.words[mid] > t) lo = mid; else hi = mid;
+          }
+          idx = (f.words[lo] == t) ? lo : hi;
+        }
+        if (n < cap) {
+          targets[n] = (int)idx;
+          signs[n] = (par & 1) ? -1 : 1;
+          fidx[n] = fb + m3;
+        }
+        ++n;
+      }
+    }
+  }
+  *count = n;
+}
+
+// ----------------------------------------------------- adjoint bins
+// bins[f] = sum over rows r and elements (r -> t) of factor f of u[r] * sign * v[t].  Each block
+// accumulates into shared-memory bins and writes its partial row of a [blocks][factors] scratch
+// array; a second kernel sums the partials in block order (deterministic, no global atomics).
+constexpr int kBinThreads = 256;
+
+template <int MODE>
+__global__ void __launch_bounds__(kBinThreads) fqhe_bins_kernel(FqheDevice f, const double* u, const double* v,
+                                                                double* partial, SmemLayout lay) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double* sbins = reinterpret_cast<double*>(smem);
+  int* spair = reinterpret_cast<int*>(smem + align16(f.nbr_factors * (int)sizeof(double)));
+  int* slookup = spair + align16(f.nbr_pairs * (int)sizeof(int)) / (int)sizeof(int);
+  int* sshift = slookup + ((MODE == DH_INDEX_LOOKUP) ? (f.lz_max + 1) * ((1 << f.lookup_bits) + 1) : 0);
+  for (int i = threadIdx.x; i < f.nbr_factors; i += blockDim.x) sbins[i] = 0.0;
+  for (int i = threadIdx.x; i < f.nbr_pairs; i += blockDim.x) spair[i] = f.pair_offset[i];
+  if (MODE == DH_INDEX_LOOKUP) {
+    const int n = (f.lz_max + 1) * ((1 << f.lookup_bits) + 1);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) slookup[i] = f.lookup[i];
+    for (int i = threadIdx.x; i <= f.lz_max; i += blockDim.x) sshift[i] = f.lookup_shift[i];
+  }
+  __syncthreads();
+  const uint64_t full = (f.lz_max >= 63) ? ~0ull : ((1ull << (f.lz_max + 1)) - 1ull);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+    const uint64_t s = __ldg(f.words + r);
+    const double ur = u[r];
+    if (ur == 0.0) continue;
+    uint64_t rem1 = s;
+    while (rem1) {
+      const int m1 = 63 - __clzll(rem1);
+      rem1 &= ~(1ull << m1);
+      uint64_t rem2 = rem1;
+      const int pbase = m1 * (m1 - 1) / 2;
+      while (rem2) {
+        const int m2 = 63 - __clzll(rem2);
+        rem2 &= ~(1ull << m2);
+        const uint64_t an = s & ~((1ull << m1) | (1ull << m2));
+        const int M = m1 + m2;
+        const int paa = 1 + __popcll(s & between_mask(m2, m1));
+        const uint64_t e = ~an & full;
+        uint64_t valid = e & mirror_bits(e, M) & (~0ull << (M / 2 + 1));
+        const int fb = spair[pbase + m2] - (M / 2 + 1);
+        while (valid) {
+          const int m3 = __ffsll(valid) - 1;
+          valid &= valid - 1ull;
+          const int m4 = M - m3;
+          const uint64_t t = an | (1ull << m3) | (1ull << m4);
+          const int par = paa + __popcll(an & between_mask(m4, m3));
+          const long long idx = target_index<MODE>(f, t, slookup, sshift);
+          const double c = ur * __ldg(v + idx);
+          atomicAdd(sbins + fb + m3, (par & 1) ? -c : c);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  double* out = partial + (size_t)blockIdx.x * f.nbr_factors;
+  for (int i = threadIdx.x; i < f.nbr_factors; i += blockDim.x) out[i] = sbins[i];
+}
+
+__global__ void sum_partial_bins(const double* partial, int nblocks, int nbins, double* bins) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nbins) return;
+  double acc = 0.0;
+  for (int b = 0; b < nblocks; ++b) acc += partial[(size_t)b * nbins + i];
+  bins[i] = acc;
+}
+
+template <int MODE>
+__global__ void fqhe_find_kernel(FqheDevice f, const uint64_t* words, long long n, long long* out) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t t = words[i];
+  if (MODE == DH_INDEX_RANK) {
+    const long long hi = t >> f.low_bits;
+    if (hi >= (1ll << (f.lz_max + 1 - f.low_bits))) {
+      out[i] = -1;
+      return;
+    }
+    const int off = f.high_offset[hi];
+    out[i] = (off < 0) ? -1 : (long long)off + f.low_rank[t & ((1ull << f.low_bits) - 1ull)];
+    if (out[i] >= 0 && (out[i] >= f.dim || f.words[out[i]] != t)) out[i] = -1;
+  } else {
+    if (t == 0 || (63 - __clzll(t)) > f.lz_max) {
+      out[i] = -1;
+      return;
+    }
+    const int l = 63 - __clzll(t);
+    const int wdt = (1 << f.lookup_bits) + 1;
+    const long long v = (long long)(t >> f.lookup_shift[l]);
+    long long lo = f.lookup[l * wdt + v + 1], hi = f.lookup[l * wdt + v];
+    if (lo < 0 || hi < 0) {
+      out[i] = -1;
+      return;
+    }
+    while (hi - lo > 1) {
+      long long mid = (lo + hi) >> 1;
+      if (f.words[mid] > t) lo = mid; else hi = mid;
+    }
+    long long r = (f.words[lo] == t) ? lo : hi;
+    out[i] = (f.words[r] == t) ? r : -1;
+  }
+}
+
+}  // namespace
+
+int launch_fqhe_unrank(int nbr_fermions, int lz_max, int total_sum, long long dim, uint64_t* words,
+                       const int64_t* counts_dev, int count_stride_o, int count_stride_s, cudaStream_t s) {
+  if (dim <= 0) return DH_OK;
+  unsigned grid = (unsigned)((dim + 255) / 256);
+  fqhe_unrank_kernel<<<grid, 256, 0, s>>>(nbr_fermions, lz_max, total_sum, dim, words, counts_dev,
+                                          count_stride_o, count_stride_s);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_fqhe_matvec(const FqheDevice& f, const MatvecArgs& a, int precision, cudaStream_t s) {
+  if (f.dim <= 0) return DH_OK;
+  if (precision == DH_PRECISION_FP32) return dispatch_k<float>(f, a, s);
+  return dispatch_k<double>(f, a, s);
+}
+
+int launch_fqhe_row_elements(const FqheDevice& f, long long row, int* targets, int* signs, int* factor_index,
+                             int cap, int* count, cudaStream_t s) {
+  if (f.index_mode == DH_INDEX_LOOKUP)
+    fqhe_row_kernel<DH_INDEX_LOOKUP><<<1, 32, 0, s>>>(f, row, targets, signs, factor_index, cap, count);
+  else
+    fqhe_row_kernel<DH_INDEX_RANK><<<1, 32, 0, s>>>(f, row, targets, signs, factor_index, cap, count);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_fqhe_bins(const FqheDevice& f, const double* u, const double* v, double* partial_bins, int nblocks,
+                     double* bins, cudaStream_t s) {
+  SmemLayout lay = smem_layout(f, sizeof(double));
+  if (f.dim > 0) {
+    if (f.index_mode == DH_INDEX_LOOKUP) {
+      auto kern = fqhe_bins_kernel<DH_INDEX_LOOKUP>;
+      if (lay.total > 48 * 1024) DH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total));
+      kern<<<nblocks, kBinThreads, lay.total, s>>>(f, u, v, partial_bins, lay);
+    } else {
+      auto kern = fqhe_bins_kernel<DH_INDEX_RANK>;
+      if (lay.total > 48 * 1024) DH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total));
+      kern<<<nblocks, kBinThreads, lay.total, s>>>(f, u, v, partial_bins, lay);
+    }
+    DH_CUDA(cudaGetLastError());
+  }
+  sum_partial_bins<<<(f.nbr_factors + 255) / 256, 256, 0, s>>>(partial_bins, f.dim > 0 ? nblocks : 0, f.nbr_factors,
+                                                                 bins);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_fqhe_find(const FqheDevice& f, const uint64_t* words, long long n, long long* out, cudaStream_t s) {
+  if (n <= 0) return DH_OK;
+  unsigned grid = (unsigned)((n + 255) / 256);
+  if (f.index_mode == DH_INDEX_LOOKUP)
+    fqhe_find_kernel<DH_INDEX_LOOKUP><<<grid, 256, 0, s>>>(f, words, n, out);
+  else
+    fqhe_find_kernel<DH_INDEX_RANK><<<grid, 256, 0, s>>>(f, words, n, out);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+}  // namespace dh

@@ -1,0 +1,230 @@
+/* diagham_b200.h -- C ABI of the B200 engine for DiagHam's on-the-fly H.v + Lanczos path.
+ *
+ * Plain C: opaque handles, pointers and sizes, int status codes (0 = success, < 0 = error,
+ * message from dh_last_error()).  No function aborts the process or throws.
+ *
+ * Vectors are FP64 arrays of the Hilbert-space dimension, exactly like DiagHam's RealVector
+ * components (src/Vector/RealVector.h:108).  Every vector argument may be a host pointer (the
+ * call copies it to and from the GPU) or a device pointer on the library's device (used in
+ * place); the kind is detected per pointer.  Calls are ordered on the handle's CUDA stream
+ * (default: the legacy default stream, see dh_hamiltonian_set_stream) and return once their
+ * results are complete.
+ *
+ * Handles are not thread-safe: use one handle per host thread, as DiagHam clones Hilbert spaces
+ * per thread (FQHE/src/Hamiltonian/AbstractQHEOnSphereHamiltonian.cc:425).
+ */
+#ifndef DIAGHAM_B200_H
+#define DIAGHAM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status codes */
+#define DH_OK 0
+#define DH_ERR_ARGUMENT -1
+#define DH_ERR_CUDA -2
+#define DH_ERR_MEMORY -3
+#define DH_ERR_UNSUPPORTED -4
+#define DH_ERR_NOT_CONVERGED -5
+#define DH_ERR_STATE -6
+
+/* index search modes of the target-index lookup inside the matvec kernels */
+#define DH_INDEX_RANK 0   /* two-table combinatorial rank (default) */
+#define DH_INDEX_LOOKUP 1 /* DiagHam's highest-bit lookup table + binary search */
+
+/* arithmetic of the matrix-element generation and gather */
+#define DH_PRECISION_FP64 0
+#define DH_PRECISION_FP32 1 /* FP32 elements and FP32 per-row accumulation, FP64 output */
+
+/* Lanczos algorithms (src/LanczosAlgorithm/) */
+#define DH_LANCZOS_BASIC 0              /* BasicLanczosAlgorithm.cc */
+#define DH_LANCZOS_FULL_REORTHOGONALIZED 1 /* FullReorthogonalizedLanczosAlgorithm.cc */
+#define DH_LANCZOS_BLOCK 2              /* BasicBlockLanczosAlgorithm.cc */
+#define DH_LANCZOS_WITH_GROUND_STATE 3  /* BasicLanczosAlgorithmWithGroundState.cc */
+
+typedef struct dh_space_s* dh_space_t;
+typedef struct dh_hamiltonian_s* dh_hamiltonian_t;
+typedef struct dh_lanczos_s* dh_lanczos_t;
+
+/* Last error message of the calling thread ("" if none). */
+const char* dh_last_error(void);
+/* Library version string. */
+const char* dh_version(void);
+/* Number of CUDA devices visible (0 if none, never an error). */
+int dh_device_count(int* count);
+
+/* ================================================================ Hilbert spaces */
+
+/* FermionOnSphere(nbrFermions, totalLz, lzMax, memory):
+ * FQHE/src/HilbertSpace/FermionOnSphere.cc:75-130.  total_lz is twice the total Lz, lz_max is 2S.
+ * memory sizes DiagHam's lookup table (FermionOnSphere.cc:1659); it only matters for the
+ * DH_INDEX_LOOKUP search mode, which stages a table of at most DH_LOOKUP_SMEM_BYTES in shared
+ * memory.  Rejects lz_max > 40 and sectors of odd (total_lz + nbr_fermions * lz_max). */
+int dh_fermion_on_sphere_create(int nbr_fermions, int total_lz, int lz_max, unsigned long memory, dh_space_t* out);
+
+/* Spin1_2Chain(chainLength, sz, memorySize): Spin/src/HilbertSpace/Spin1_2Chain.cc:113-142.
+ * sz is twice the total Sz.  chain_length <= 32. */
+int dh_spin12_chain_create(int chain_length, int sz, int memory, dh_space_t* out);
+
+int dh_space_destroy(dh_space_t space);
+
+/* AbstractHilbertSpace::GetHilbertSpaceDimension (src/HilbertSpace/AbstractHilbertSpace.h). */
+int dh_space_get_dimension(dh_space_t space, int64_t* dim);
+
+/* StateDescription[first .. first+n) and, for fermions, StateLzMax (FermionOnSphere.h:166-168,
+ * Spin1_2Chain.h:64) copied to host arrays, in the reference's own order and bit layout.
+ * lz_max may be NULL. */
+int dh_space_get_states(dh_space_t space, uint64_t* words, int* lz_max, int64_t first, int64_t n);
+
+/* FindStateIndex for n words (FermionOnSphere.cc:1431, Spin1_2Chain.cc:1002), computed on the GPU
+ * with the space's current index mode; host or device arrays. */
+int dh_space_find_state_index(dh_space_t space, const uint64_t* words, int64_t n, int64_t* indices);
+
+/* Selects DH_INDEX_RANK or DH_INDEX_LOOKUP for every kernel that uses this space. */
+int dh_space_set_index_mode(dh_space_t space, int mode);
+
+/* ================================================================ Hamiltonians */
+
+/* ParticleOnSphereGenericHamiltonian(particles, nbrParticles, lzmax, pseudoPotential, l2Factor, ...):
+ * FQHE/src/Hamiltonian/ParticleOnSphereGenericHamiltonian.cc:66-140, interaction factors
+ * :493-612, on-the-fly multiplication (memory = 0).  pseudopotentials = V_0..V_lzmax, V_0 being
+ * the delta interaction.  l2_factor must be 0 (the L^2 term is not on this path).  The
+ * Hamiltonian does not own the space (FQHESphereFermionsTwoBodyGeneric.cc:395-396). */
+int dh_particle_on_sphere_generic_hamiltonian_create(dh_space_t space, int nbr_particles, int lz_max,
+                                                     const double* pseudopotentials, double l2_factor,
+                                                     dh_hamiltonian_t* out);
+
+/* Periodic J1-J2 spin-1/2 chain on a plain Spin1_2Chain: the element pattern of
+ * Spin/src/Hamiltonian/SpinChainJ1J2RealHamiltonianWithTranslations.cc:94-192 (flips J/2) and
+ * :335-352 (diagonal J Sz_i Sz_j) behind the SpinChainHamiltonian API (SpinChainHamiltonian.cc:257). */
+int dh_spin_chain_j1j2_hamiltonian_create(dh_space_t space, double j1, double j2, dh_hamiltonian_t* out);
+
+int dh_hamiltonian_destroy(dh_hamiltonian_t h);
+
+/* AbstractHamiltonian::GetHilbertSpaceDimension (src/Hamiltonian/AbstractHamiltonian.h:96). */
+int dh_hamiltonian_get_dimension(dh_hamiltonian_t h, int64_t* dim);
+
+/* AbstractQHEOnSphereHamiltonian::ShiftHamiltonian (AbstractQHEOnSphereHamiltonian.cc:144):
+ * H + shift * 1 in every product. */
+int dh_hamiltonian_shift(dh_hamiltonian_t h, double shift);
+
+/* DH_PRECISION_FP64 (default) or DH_PRECISION_FP32 for every following product. */
+int dh_hamiltonian_set_precision(dh_hamiltonian_t h, int precision);
+
+/* Replaces V_0..V_lzmax (rebuilds the interaction factors; FQHE Hamiltonians only). */
+int dh_hamiltonian_set_pseudopotentials(dh_hamiltonian_t h, const double* pseudopotentials);
+
+/* CUDA stream (a cudaStream_t passed as void*) the handle's work is ordered on. */
+int dh_hamiltonian_set_stream(dh_hamiltonian_t h, void* stream);
+
+/* AbstractHamiltonian::LowLevelAddMultiply(vSource, vDestination, firstComponent, nbrComponent)
+ * (src/Hamiltonian/AbstractHamiltonian.h:265, FQHE implementation
+ * AbstractQHEOnSphereHamiltonian.cc:410): dst += H[:, first:first+nbr] src[first:first+nbr], i.e.
+ * the reference's push-form semantics (columns first..first+nbr-1, destination accumulated),
+ * computed in pull form with no atomics.  nbr < 0 means "to the end". */
+int dh_hamiltonian_low_level_add_multiply(dh_hamiltonian_t h, const double* src, double* dst, int64_t first,
+                                          int64_t nbr);
+
+/* AbstractHamiltonian::LowLevelMultiply (AbstractHamiltonian.cc:448-476): clear dst then add. */
+int dh_hamiltonian_low_level_multiply(dh_hamiltonian_t h, const double* src, double* dst, int64_t first,
+                                      int64_t nbr);
+
+/* AbstractHamiltonian::LowLevelMultipleAddMultiply(vSources, vDestinations, nbrVectors, first, nbr)
+ * (AbstractHamiltonian.h:344, AbstractQHEOnSphereHamiltonian.cc:1217): srcs and dsts hold
+ * nbr_vectors vectors of the full dimension one after the other (the RealVector array). */
+int dh_hamiltonian_low_level_multiple_add_multiply(dh_hamiltonian_t h, const double* srcs, double* dsts,
+                                                   int nbr_vectors, int64_t first, int64_t nbr);
+
+/* AbstractHamiltonian::MatrixElement(V1, V2) (AbstractQHEOnSphereHamiltonian.cc:380): <v1|H|v2>. */
+int dh_hamiltonian_matrix_element(dh_hamiltonian_t h, const double* v1, const double* v2, double* out);
+
+/* Per-row element list of the on-the-fly product, the contract of
+ * AbstractQHEOnSphereHamiltonian::EvaluateMNTwoBodyFastMultiplicationComponent (.h:531):
+ * target index, sign (+1/-1) of AA*AdAd and interaction-factor index for every generated element
+ * of `row`, in the reference enumeration order.  *count receives the total; at most cap entries
+ * are written.  FQHE Hamiltonians only. */
+int dh_hamiltonian_row_elements(dh_hamiltonian_t h, int64_t row, int* targets, int* signs, int* factor_index,
+                                int cap, int* count);
+
+/* Adjoint of the pseudopotentials (Hellmann-Feynman / bilinear VJP): out[m] = <u| dH/dV_m |v> for
+ * m = 0..lz_max.  With u = v = normalised ground state this is dE0/dV_m; with u = upstream gradient
+ * and v = x it is the V part of the vector-Jacobian product of H(V) x.  FQHE Hamiltonians only. */
+int dh_hamiltonian_pseudopotential_adjoint(dh_hamiltonian_t h, const double* u, const double* v, double* out);
+
+/* Interaction factors of the current V (flattened in the reference order,
+ * ParticleOnSphereGenericHamiltonian.cc:566-606) and their count. */
+int dh_hamiltonian_get_interaction_factors(dh_hamiltonian_t h, double* factors, int cap, int* count);
+
+/* ================================================================ Lanczos */
+
+/* Creates one of the reference's Lanczos algorithms on the GPU: AbstractLanczosAlgorithm
+ * (src/LanczosAlgorithm/AbstractLanczosAlgorithm.h:45-120) with the recurrence of
+ * BasicLanczosAlgorithm.cc:148-216, FullReorthogonalizedLanczosAlgorithm.cc:209-323,
+ * BasicBlockLanczosAlgorithm.cc:524-697 or BasicLanczosAlgorithmWithGroundState.cc:256-335.
+ * Lanczos vectors stay in FP64 in device memory. */
+int dh_lanczos_create(dh_hamiltonian_t h, int algorithm, int nbr_eigenvalue, int block_size, int max_iter,
+                      dh_lanczos_t* out);
+int dh_lanczos_destroy(dh_lanczos_t l);
+
+/* SetEigenvaluePrecision (AbstractLanczosAlgorithm.h); default 1e-14 = MACHINE_PRECISION. */
+int dh_lanczos_set_eigenvalue_precision(dh_lanczos_t l, double precision);
+
+/* InitializeLanczosAlgorithm(vector) / (vectors, nbrVectors): nbr_vectors vectors one after the
+ * other (host or device).  Block algorithms orthonormalise the block; others use vectors[0]. */
+int dh_lanczos_initialize(dh_lanczos_t l, const double* vectors, int nbr_vectors);
+
+/* InitializeLanczosAlgorithm() with a reproducible start: component i of vector b is the
+ * (i+1)-th splitmix64 output of seed + b mapped to [-1, 1), then normalised. */
+int dh_lanczos_initialize_random(dh_lanczos_t l, uint64_t seed);
+
+/* RunLanczosAlgorithm(nbrIter) (BasicLanczosAlgorithm.cc:148). */
+int dh_lanczos_run(dh_lanczos_t l, int nbr_iter);
+
+/* TestConvergence (BasicLanczosAlgorithm.cc:220, BasicBlockLanczosAlgorithm.cc:731). */
+int dh_lanczos_test_convergence(dh_lanczos_t l, int* converged);
+
+/* Lowest n Ritz values, ascending (GetDiagonalizedMatrix + SortMatrixUpOrder). */
+int dh_lanczos_get_eigenvalues(dh_lanczos_t l, double* eigenvalues, int n);
+
+/* GetGroundStateEnergy (AbstractLanczosAlgorithm.cc:136-150). */
+int dh_lanczos_get_ground_state_energy(dh_lanczos_t l, double* energy);
+
+/* GetGroundState (BasicLanczosAlgorithmWithGroundState.cc:256-335): normalised Ritz vector of the
+ * lowest Ritz value, written to vec (host or device). */
+int dh_lanczos_get_ground_state(dh_lanczos_t l, double* vec);
+
+/* Number of matrix-vector products and tridiagonal rows so far. */
+int dh_lanczos_get_counters(dh_lanczos_t l, int64_t* matvecs, int* rows);
+
+/* Whole driver loop of QHEOnSphereMainTask.cc:732-753: RunLanczosAlgorithm(nbrEigenvalue + 2), then
+ * RunLanczosAlgorithm(1) until TestConvergence() or max_iter iterations, issued as CUDA-graph
+ * batches of `graph_batch` iterations (>= 1) whose extra iterations past convergence are discarded
+ * from the reported result.  *iterations follows the reference's iteration counter. */
+int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eigenvalues, int* iterations,
+                     int* converged);
+
+/* FP32-matvec Lanczos with FP64 recurrence followed by FP64 refinement of the ground state:
+ * the Ritz vector is rebuilt from the stored Krylov basis, its FP64 Rayleigh quotient and residual
+ * are taken with an FP64 product, and, while the residual bound exceeds `precision` * |E|, a short
+ * FP64 Lanczos restarted from it polishes the energy.  out[0] = refined E0, out[1] = FP32-phase E0,
+ * out[2] = residual norm, out[3] = FP32 matvecs, out[4] = FP64 matvecs. */
+int dh_lanczos_solve_refined(dh_lanczos_t l, int max_iter, double precision, double* out);
+
+/* ================================================================ setup helpers */
+
+/* EvaluatePseudopotentials(nbrFlux, 0, 0.0) (FQHE/src/Tools/FQHESpectrum/PseudoPotentials.cc:35):
+ * lowest-Landau-level Coulomb V_0..V_nbrFlux on the sphere, FP64 on the host. */
+int dh_coulomb_pseudopotentials(int nbr_flux, double* v);
+
+/* ClebschGordanCoefficients::GetCoefficient (src/MathTools/ClebschGordanCoefficients.cc:136),
+ * every argument doubled. */
+int dh_clebsch_gordan(int j1, int m1, int j2, int m2, int j, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,274 @@
+"""ctypes view of liboracle.so, the CPU restatement of DiagHam's H.v + Lanczos path.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline leg of bench.py, and there only as the checker.  The product
+package (diagham_b200) never imports this module.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_f64p = ctypes.POINTER(ctypes.c_double)
+
+
+def build():
+    """Compile liboracle.so in place (plain gcc, seconds)."""
+    subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        src = os.path.join(_HERE, "oracle.c")
+        if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+            build()
+        L = ctypes.CDLL(path)
+        L.orc_fermion_dimension.restype = ctypes.c_long
+        L.orc_fermion_dimension.argtypes = [ctypes.c_int] * 3
+        L.orc_fermion_basis.restype = ctypes.c_long
+        L.orc_fermion_basis.argtypes = [ctypes.c_int] * 3 + [_u64p, _i32p]
+        L.orc_lookup_shift_from_memory.restype = ctypes.c_int
+        L.orc_lookup_shift_from_memory.argtypes = [ctypes.c_int, ctypes.c_ulong]
+        L.orc_fermion_lookup_table.restype = None
+        L.orc_fermion_lookup_table.argtypes = [_u64p, _i32p, ctypes.c_long, ctypes.c_int, ctypes.c_int, _i32p, _i32p]
+        L.orc_fermion_find_state_index.restype = ctypes.c_long
+        L.orc_fermion_find_state_index.argtypes = [_u64p, ctypes.c_long, _i32p, _i32p, ctypes.c_int,
+                                                   ctypes.c_uint64, ctypes.c_int]
+        L.orc_fermion_aa.restype = ctypes.c_double
+        L.orc_fermion_aa.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, _u64p]
+        L.orc_fermion_adad.restype = ctypes.c_double
+        L.orc_fermion_adad.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, _u64p]
+        L.orc_clebsch_gordan.restype = ctypes.c_double
+        L.orc_clebsch_gordan.argtypes = [ctypes.c_int] * 5
+        L.orc_nbr_pairs.restype = ctypes.c_int
+        L.orc_nbr_pairs.argtypes = [ctypes.c_int]
+        L.orc_interaction_tables.restype = ctypes.c_int
+        L.orc_interaction_tables.argtypes = [ctypes.c_int, _f64p, _i32p, _i32p, _i32p, _i32p, _i32p, _f64p]
+        L.orc_interaction_derivatives.restype = ctypes.c_int
+        L.orc_interaction_derivatives.argtypes = [ctypes.c_int, _f64p]
+        L.orc_coulomb_pseudopotentials.restype = None
+        L.orc_coulomb_pseudopotentials.argtypes = [ctypes.c_int, _f64p]
+        L.orc_fqhe_push_add_multiply.restype = None
+        L.orc_fqhe_push_add_multiply.argtypes = [ctypes.c_void_p, _f64p, _f64p, ctypes.c_long, ctypes.c_long]
+        L.orc_fqhe_pull_multiply.restype = None
+        L.orc_fqhe_pull_multiply.argtypes = [ctypes.c_void_p, _f64p, _f64p]
+        L.orc_fqhe_row_elements.restype = ctypes.c_long
+        L.orc_fqhe_row_elements.argtypes = [ctypes.c_void_p, ctypes.c_long, _i32p, _i32p, _i32p, ctypes.c_long]
+        L.orc_fqhe_expectation_bins.restype = None
+        L.orc_fqhe_expectation_bins.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p]
+        L.orc_spin_dimension.restype = ctypes.c_long
+        L.orc_spin_dimension.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.orc_spin_basis.restype = ctypes.c_long
+        L.orc_spin_basis.argtypes = [ctypes.c_int, ctypes.c_int, _u64p]
+        L.orc_spin_find_state_index.restype = ctypes.c_long
+        L.orc_spin_find_state_index.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_uint64]
+        L.orc_spin_j1j2_multiply.restype = None
+        L.orc_spin_j1j2_multiply.argtypes = [ctypes.c_int, ctypes.c_int, _u64p, ctypes.c_long, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_double, _f64p, _f64p]
+        L.orc_random_vector.restype = None
+        L.orc_random_vector.argtypes = [ctypes.c_uint64, ctypes.c_long, _f64p]
+        L.orc_tridiagonal_eigenvalues.restype = ctypes.c_int
+        L.orc_tridiagonal_eigenvalues.argtypes = [ctypes.c_int, _f64p, _f64p, _f64p]
+        L.orc_symmetric_eigen.restype = ctypes.c_int
+        L.orc_symmetric_eigen.argtypes = [ctypes.c_int, _f64p, _f64p, _f64p]
+        L.orc_basic_lanczos.restype = ctypes.c_int
+        L.orc_basic_lanczos.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long, _f64p, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_double, _f64p, _i32p, _f64p, _f64p]
+        _LIB = L
+    return _LIB
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def fermion_basis(n, two_s, total_lz):
+    L = lib()
+    dim = L.orc_fermion_dimension(n, total_lz, two_s)
+    if dim <= 0:
+        raise ValueError("empty or invalid sector N=%d 2S=%d 2Lz=%d" % (n, two_s, total_lz))
+    words = np.zeros(max(dim, 1), np.uint64)
+    lz = np.zeros(max(dim, 1), np.int32)
+    got = L.orc_fermion_basis(n, total_lz, two_s, _p(words, _u64p), _p(lz, _i32p))
+    assert got == dim
+    return words[:dim], lz[:dim]
+
+
+def lookup_table(words, lzmax, two_s, max_shift):
+    L = lib()
+    width = (1 << max_shift) + 1
+    table = np.zeros((two_s + 1) * width, np.int32)
+    shifts = np.zeros(two_s + 1, np.int32)
+    L.orc_fermion_lookup_table(_p(words, _u64p), _p(lzmax, _i32p), len(words), two_s, max_shift,
+                               _p(table, _i32p), _p(shifts, _i32p))
+    return table.reshape(two_s + 1, width), shifts
+
+
+def interaction_tables(two_s, v):
+    L = lib()
+    v = np.ascontiguousarray(v, np.float64)
+    npairs = L.orc_nbr_pairs(two_s)
+    cap = npairs * (two_s + 1)
+    m1 = np.zeros(npairs, np.int32)
+    m2 = np.zeros(npairs, np.int32)
+    nm3 = np.zeros(npairs, np.int32)
+    off = np.zeros(npairs, np.int32)
+    m3 = np.zeros(cap, np.int32)
+    fac = np.zeros(cap, np.float64)
+    nf = L.orc_interaction_tables(two_s, _p(v, _f64p), _p(m1, _i32p), _p(m2, _i32p), _p(nm3, _i32p),
+                                  _p(off, _i32p), _p(m3, _i32p), _p(fac, _f64p))
+    return dict(m1=m1, m2=m2, nbr_m3=nm3, m3_offset=off, m3=m3[:nf], factors=fac[:nf])
+
+
+def interaction_derivatives(two_s):
+    L = lib()
+    nf = L.orc_interaction_tables(two_s, None, None, None, None, None, None, None)
+    d = np.zeros(nf * (two_s + 1), np.float64)
+    L.orc_interaction_derivatives(two_s, _p(d, _f64p))
+    return d.reshape(nf, two_s + 1)
+
+
+def coulomb_pseudopotentials(two_s):
+    v = np.zeros(two_s + 1, np.float64)
+    lib().orc_coulomb_pseudopotentials(two_s, _p(v, _f64p))
+    return v
+
+
+def clebsch_gordan(j1, m1, j2, m2, j):
+    return lib().orc_clebsch_gordan(j1, m1, j2, m2, j)
+
+
+class _FqheStruct(ctypes.Structure):
+    _fields_ = [("nbr_fermions", ctypes.c_int), ("lz_max", ctypes.c_int), ("total_lz", ctypes.c_int),
+                ("dim", ctypes.c_long), ("words", _u64p), ("state_lz_max", _i32p), ("table", _i32p),
+                ("table_shift", _i32p), ("max_shift", ctypes.c_int), ("nbr_pairs", ctypes.c_int),
+                ("m1v", _i32p), ("m2v", _i32p), ("nbr_m3", _i32p), ("m3_offset", _i32p), ("m3v", _i32p),
+                ("factors", _f64p), ("shift", ctypes.c_double)]
+
+
+class FQHE:
+    """The full FQHE sector of the oracle: basis, lookup table, interaction tables."""
+
+    def __init__(self, n, two_s, total_lz, v, shift=0.0, max_shift=None):
+        self.n, self.two_s, self.total_lz = n, two_s, total_lz
+        self.words, self.lzmax = fermion_basis(n, two_s, total_lz)
+        self.dim = len(self.words)
+        if max_shift is None:
+            max_shift = lib().orc_lookup_shift_from_memory(two_s, 9 << 20)
+        self.max_shift = max_shift
+        self.table, self.table_shift = lookup_table(self.words, self.lzmax, two_s, max_shift)
+        self.v = np.ascontiguousarray(v, np.float64)
+        self.tabs = interaction_tables(two_s, self.v)
+        self.shift = shift
+        t = self.tabs
+        self._keep = [self.words, self.lzmax, self.table, self.table_shift, t["m1"], t["m2"], t["nbr_m3"],
+                      t["m3_offset"], t["m3"], t["factors"]]
+        self.s = _FqheStruct(n, two_s, total_lz, self.dim, _p(self.words, _u64p), _p(self.lzmax, _i32p),
+                             _p(self.table, _i32p), _p(self.table_shift, _i32p), max_shift, len(t["m1"]),
+                             _p(t["m1"], _i32p), _p(t["m2"], _i32p), _p(t["nbr_m3"], _i32p),
+                             _p(t["m3_offset"], _i32p), _p(t["m3"], _i32p), _p(t["factors"], _f64p), shift)
+
+    def find(self, word):
+        w = int(word)
+        lz = w.bit_length() - 1 if w else 0
+        return lib().orc_fermion_find_state_index(_p(self.words, _u64p), self.dim, _p(self.table, _i32p),
+                                                  _p(self.table_shift, _i32p), self.max_shift, w, lz)
+
+    def pull(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros(self.dim, np.float64)
+        lib().orc_fqhe_pull_multiply(ctypes.byref(self.s), _p(x, _f64p), _p(y, _f64p))
+        return y
+
+    def push(self, x, first=0, nbr=None):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros(self.dim, np.float64)
+        nbr = self.dim - first if nbr is None else nbr
+        lib().orc_fqhe_push_add_multiply(ctypes.byref(self.s), _p(x, _f64p), _p(y, _f64p), first, nbr)
+        return y
+
+    def row(self, r):
+        cap = 4096
+        t = np.zeros(cap, np.int32)
+        s = np.zeros(cap, np.int32)
+        f = np.zeros(cap, np.int32)
+        n = lib().orc_fqhe_row_elements(ctypes.byref(self.s), r, _p(t, _i32p), _p(s, _i32p), _p(f, _i32p), cap)
+        assert n <= cap
+        return t[:n], s[:n], f[:n]
+
+    def bins(self, u, v):
+        u = np.ascontiguousarray(u, np.float64)
+        v = np.ascontiguousarray(v, np.float64)
+        b = np.zeros(len(self.tabs["factors"]), np.float64)
+        lib().orc_fqhe_expectation_bins(ctypes.byref(self.s), _p(u, _f64p), _p(v, _f64p), _p(b, _f64p))
+        return b
+
+    def lanczos(self, v0, nev=1, max_iter=200, precision=1e-14):
+        return basic_lanczos(lib().orc_fqhe_matvec_cb, ctypes.byref(self.s), self.dim, v0, nev, max_iter, precision)
+
+
+def spin_basis(length, sz):
+    L = lib()
+    dim = L.orc_spin_dimension(length, sz)
+    w = np.zeros(dim, np.uint64)
+    L.orc_spin_basis(length, sz, _p(w, _u64p))
+    return w
+
+
+def spin_find(length, sz, word):
+    return lib().orc_spin_find_state_index(length, sz, int(word))
+
+
+def spin_j1j2_multiply(length, sz, words, j1, j2, x, shift=0.0):
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.zeros(len(words), np.float64)
+    lib().orc_spin_j1j2_multiply(length, sz, _p(words, _u64p), len(words), j1, j2, shift, _p(x, _f64p), _p(y, _f64p))
+    return y
+
+
+def random_vector(seed, dim):
+    x = np.zeros(dim, np.float64)
+    lib().orc_random_vector(seed, dim, _p(x, _f64p))
+    return x
+
+
+def tridiagonal_eigenvalues(diag, off):
+    d = np.ascontiguousarray(diag, np.float64)
+    e = np.ascontiguousarray(off, np.float64)
+    out = np.zeros(len(d), np.float64)
+    assert lib().orc_tridiagonal_eigenvalues(len(d), _p(d, _f64p), _p(e, _f64p), _p(out, _f64p)) == 0
+    return out
+
+
+_MATVEC_CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p, _f64p, _f64p)
+
+
+def basic_lanczos(fn, ctx, dim, v0, nev=1, max_iter=200, precision=1e-14):
+    v0 = np.ascontiguousarray(v0, np.float64)
+    eig = np.zeros(nev, np.float64)
+    it = np.zeros(1, np.int32)
+    alpha = np.zeros(max_iter + 8, np.float64)
+    beta = np.zeros(max_iter + 8, np.float64)
+    conv = lib().orc_basic_lanczos(ctypes.cast(fn, ctypes.c_void_p), ctx, dim, _p(v0, _f64p), nev, max_iter,
+                                   precision, _p(eig, _f64p), _p(it, _i32p), _p(alpha, _f64p), _p(beta, _f64p))
+    return dict(eigenvalues=eig, iterations=int(it[0]), converged=bool(conv))
+
+
+def python_lanczos(matvec, dim, v0, nev=1, max_iter=200, precision=1e-14):
+    """Basic Lanczos with a Python matvec callable (for the spin chain)."""
+    @_MATVEC_CB
+    def cb(ctx, x, y):
+        xa = np.ctypeslib.as_array(x, shape=(dim,))
+        ya = np.ctypeslib.as_array(y, shape=(dim,))
+        ya[:] = matvec(xa)
+    r = basic_lanczos(cb, None, dim, v0, nev, max_iter, precision)
+    return r

@@ -1,0 +1,635 @@
+// ref_tool: a thin command-line driver over DiagHam's own classes.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is compiled (by oracle/Makefile) against
+// the reference sources and linked into oracle/_ref/ref_tool.  It is used to
+// generate the golden fixtures under tests/golden/ and, in bench.py, to time the
+// reference CPU implementation of the hot path.  No product code links it.
+//
+// Every command calls only reference classes:
+//   FermionOnSphere                      FQHE/src/HilbertSpace/FermionOnSphere.cc:75
+//   ParticleOnSphereGenericHamiltonian   FQHE/src/Hamiltonian/ParticleOnSphereGenericHamiltonian.cc:66
+//   AbstractQHEOnSphereHamiltonian::LowLevelAddMultiply   .../AbstractQHEOnSphereHamiltonian.cc:410
+//   Spin1_2Chain                         Spin/src/HilbertSpace/Spin1_2Chain.cc:113
+//   BasicLanczosAlgorithm / FullReorthogonalizedLanczosAlgorithm / BasicBlockLanczosAlgorithm
+//   EvaluatePseudopotentials             FQHE/src/Tools/FQHESpectrum/PseudoPotentials.cc:35
+//   VectorHamiltonianMultiplyOperation on SMPArchitecture (the reference SMP path)
+//
+// The J1-J2 chain on a plain Spin1_2Chain has no reference Hamiltonian class,
+// so J1J2ChainHarness below applies the element pattern of
+// SpinChainJ1J2RealHamiltonianWithTranslations.cc:94-192 / :335-352 through the
+// API model of SpinChainHamiltonian.cc:257-298, calling the reference
+// Spin1_2Chain::SmiSpj / SziSzj / FindStateIndex for every element.
+//
+// Binary outputs are little-endian raw arrays; tests/golden/make_golden.py
+// documents each layout and converts them to .npz fixtures.
+
+#include "config.h"
+#include "HilbertSpace/FermionOnSphere.h"
+#include "HilbertSpace/Spin1_2Chain.h"
+#include "Hamiltonian/ParticleOnSphereGenericHamiltonian.h"
+#include "Hamiltonian/AbstractHamiltonian.h"
+#include "Architecture/MonoProcessorArchitecture.h"
+#include "Architecture/SMPArchitecture.h"
+#include "Architecture/ArchitectureOperation/VectorHamiltonianMultiplyOperation.h"
+#include "LanczosAlgorithm/BasicLanczosAlgorithm.h"
+#include "LanczosAlgorithm/FullReorthogonalizedLanczosAlgorithm.h"
+#include "LanczosAlgorithm/BasicBlockLanczosAlgorithm.h"
+#include "LanczosAlgorithm/BasicLanczosAlgorithmWithGroundState.h"
+#include "Matrix/RealTriDiagonalSymmetricMatrix.h"
+#include "Tools/FQHESpectrum/PseudoPotentials.h"
+#include "Vector/RealVector.h"
+#include "MathTools/Complex.h"
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <vector>
+#include <sys/time.h>
+#include <iostream>
+
+using std::cout;
+using std::endl;
+
+static double Now()
+{
+  timeval t;
+  gettimeofday(&t, 0);
+  return t.tv_sec + 1e-6 * t.tv_usec;
+}
+
+static FILE* OpenOut(const char* name)
+{
+  FILE* f = fopen(name, "wb");
+  if (f == 0)
+    {
+      fprintf(stderr, "cannot open %s\n", name);
+      exit(2);
+    }
+  return f;
+}
+
+// pseudopotentials are read from a raw file of (2S+1) doubles (V_0 .. V_2S)
+static double* ReadDoubles(const char* name, long n)
+{
+  double* v = new double[n];
+  FILE* f = fopen(name, "rb");
+  if ((f == 0) || (fread(v, sizeof(double), n, f) != (size_t) n))
+    {
+      fprintf(stderr, "cannot read %ld doubles from %s\n", n, name);
+      exit(2);
+    }
+  fclose(f);
+  return v;
+}
+
+static int* ReadInts(const char* name, long& n)
+{
+  FILE* f = fopen(name, "rb");
+  if (f == 0)
+    {
+      fprintf(stderr, "cannot read %s\n", name);
+      exit(2);
+    }
+  fseek(f, 0, SEEK_END);
+  n = ftell(f) / sizeof(int);
+  fseek(f, 0, SEEK_SET);
+  int* v = new int[n];
+  if (fread(v, sizeof(int), n, f) != (size_t) n)
+    exit(2);
+  fclose(f);
+  return v;
+}
+
+// exposes the protected basis arrays of the reference Hilbert spaces
+class ExposedFermionOnSphere : public FermionOnSphere
+{
+ public:
+  ExposedFermionOnSphere(int nbrFermions, int totalLz, int lzMax, unsigned long memory)
+    : FermionOnSphere(nbrFermions, totalLz, lzMax, memory)
+  {
+  }
+  unsigned long Word(long i) { return this->StateDescription[i]; }
+  int WordLzMax(long i) { return this->StateLzMax[i]; }
+  int Find(unsigned long w, int lzmax) { return this->FindStateIndex(w, lzmax); }
+};
+
+class ExposedSpin1_2Chain : public Spin1_2Chain
+{
+ public:
+  ExposedSpin1_2Chain(int chainLength, int sz, int memory) : Spin1_2Chain(chainLength, sz, memory)
+  {
+  }
+  unsigned long Word(long i) { return this->StateDescription[i]; }
+  int Find(unsigned long w) { return this->FindStateIndex(w); }
+};
+
+// exposes the protected interaction tables of the reference Hamiltonian
+class ExposedGenericHamiltonian : public ParticleOnSphereGenericHamiltonian
+{
+ public:
+  ExposedGenericHamiltonian(ParticleOnSphere* particles, int nbrParticles, int lzmax, double* pseudo,
+			    AbstractArchitecture* arch, bool hermitian)
+    : ParticleOnSphereGenericHamiltonian(particles, nbrParticles, lzmax, pseudo, 0.0, arch, 0, false, 0, hermitian)
+  {
+  }
+  int GetNbrM12() { return this->NbrM12Indices; }
+  int M1(int i) { return this->M1Value[i]; }
+  int M2(int i) { return this->M2Value[i]; }
+  int NbrM3(int i) { return this->NbrM3Values[i]; }
+  int M3(int i, int j) { return this->M3Values[i][j]; }
+  int NbrFactors() { return this->NbrInteractionFactors; }
+  double Factor(int i) { return this->InteractionFactors[i]; }
+};
+
+// J1-J2 periodic chain on a plain Spin1_2Chain (see file header)
+class J1J2ChainHarness : public AbstractHamiltonian
+{
+ protected:
+  Spin1_2Chain* Chain;
+  int NbrSpin;
+  double J1;
+  double J2;
+  double Shift;
+  double* SzSzContributions;
+
+ public:
+  J1J2ChainHarness(Spin1_2Chain* chain, int nbrSpin, double j1, double j2)
+  {
+    this->Chain = chain;
+    this->NbrSpin = nbrSpin;
+    this->J1 = j1;
+    this->J2 = j2;
+    this->Shift = 0.0;
+    int Dim = this->Chain->GetHilbertSpaceDimension();
+    this->SzSzContributions = new double[Dim];
+    for (int i = 0; i < Dim; ++i)
+      {
+	double Tmp = 0.0;
+	for (int j = 0; j < this->NbrSpin; ++j)
+	  {
+	    Tmp += this->J1 * this->Chain->SziSzj(j, (j + 1) % this->NbrSpin, i);
+	    Tmp += this->J2 * this->Chain->SziSzj(j, (j + 2) % this->NbrSpin, i);
+	  }
+	this->SzSzContributions[i] = Tmp;
+      }
+  }
+  ~J1J2ChainHarness() { delete[] this->SzSzContributions; }
+  void SetHilbertSpace(AbstractHilbertSpace* hilbertSpace) { this->Chain = (Spin1_2Chain*) hilbertSpace; }
+  AbstractHilbertSpace* GetHilbertSpace() { return this->Chain; }
+  int GetHilbertSpaceDimension() { return this->Chain->GetHilbertSpaceDimension(); }
+  void ShiftHamiltonian(double shift) { this->Shift = shift; }
+  bool IsHermitian() { return false; }
+
+  RealVector& LowLevelAddMultiply(RealVector& vSource, RealVector& vDestination, int firstComponent, int nbrComponent)
+  {
+    int Last = firstComponent + nbrComponent;
+    int Dim = this->Chain->GetHilbertSpaceDimension();
+    double HalfJ1 = 0.5 * this->J1;
+    double HalfJ2 = 0.5 * this->J2;
+    double Coef;
+    int Pos;
+    for (int i = firstComponent; i < Last; ++i)
+      {
+	double TmpValue = vSource[i];
+	vDestination[i] += (this->SzSzContributions[i] + this->Shift) * TmpValue;
+	for (int j = 0; j < this->NbrSpin; ++j)
+	  {
+	    int j1 = (j + 1) % this->NbrSpin;
+	    int j2 = (j + 2) % this->NbrSpin;
+	    Pos = this->Chain->SmiSpj(j, j1, i, Coef);
+	    if (Pos != Dim)
+	      vDestination[Pos] += HalfJ1 * Coef * TmpValue;
+	    Pos = this->Chain->SmiSpj(j1, j, i, Coef);
+	    if (Pos != Dim)
+	      vDestination[Pos] += HalfJ1 * Coef * TmpValue;
+	    Pos = this->Chain->SmiSpj(j, j2, i, Coef);
+	    if (Pos != Dim)
+	      vDestination[Pos] += HalfJ2 * Coef * TmpValue;
+	    Pos = this->Chain->SmiSpj(j2, j, i, Coef);
+	    if (Pos != Dim)
+	      vDestination[Pos] += HalfJ2 * Coef * TmpValue;
+	  }
+      }
+    return vDestination;
+  }
+};
+
+static void WriteEigenvalues(FILE* f, AbstractLanczosAlgorithm* Lanczos, int nev)
+{
+  RealTriDiagonalSymmetricMatrix TmpMatrix;
+  TmpMatrix.Copy(Lanczos->GetDiagonalizedMatrix());
+  TmpMatrix.SortMatrixUpOrder();
+  for (int i = 0; i < nev; ++i)
+    {
+      double e = TmpMatrix.DiagonalElement(i);
+      fwrite(&e, sizeof(double), 1, f);
+    }
+}
+
+// the driver loop of QHEOnSphereMainTask.cc:732-753 / GenericRealMainTask.cc:790-808
+static void RunLanczosLoop(AbstractHamiltonian* H, AbstractArchitecture* Arch, const char* algo, int nev,
+			   int blockSize, int maxIter, double precision, RealVector* initial, int nbrInitial,
+			   const char* outName, const char* groundStateName)
+{
+  AbstractLanczosAlgorithm* Lanczos;
+  bool Block = false;
+  if (strcmp(algo, "basic") == 0)
+    Lanczos = new BasicLanczosAlgorithm(Arch, nev, maxIter);
+  else if (strcmp(algo, "full") == 0)
+    Lanczos = new FullReorthogonalizedLanczosAlgorithm(Arch, nev, maxIter);
+  else if (strcmp(algo, "ground") == 0)
+    Lanczos = new BasicLanczosAlgorithmWithGroundState(Arch, maxIter);
+  else
+    {
+      Lanczos = new BasicBlockLanczosAlgorithm(Arch, nev, blockSize, maxIter);
+      Block = true;
+    }
+  if (precision != 0.0)
+    Lanczos->SetEigenvaluePrecision(precision);
+  Lanczos->SetHamiltonian(H);
+  if (Block)
+    Lanczos->InitializeLanczosAlgorithm(initial, nbrInitial);
+  else
+    Lanczos->InitializeLanczosAlgorithm(initial[0]);
+  double t0 = Now();
+  int CurrentNbrIter;
+  Lanczos->RunLanczosAlgorithm(nev + 2);
+  if (Block)
+    CurrentNbrIter = (nev + 3) * blockSize;
+  else
+    CurrentNbrIter = nev + 3;
+  std::vector<double> History;
+  while ((Lanczos->TestConvergence() == false) && (CurrentNbrIter < maxIter))
+    {
+      if (Block)
+	CurrentNbrIter += blockSize;
+      else
+	++CurrentNbrIter;
+      Lanczos->RunLanczosAlgorithm(1);
+      RealTriDiagonalSymmetricMatrix TmpMatrix;
+      TmpMatrix.Copy(Lanczos->GetDiagonalizedMatrix());
+      TmpMatrix.SortMatrixUpOrder();
+      History.push_back(TmpMatrix.DiagonalElement(0));
+    }
+  double t1 = Now();
+  int Converged = Lanczos->TestConvergence() ? 1 : 0;
+  FILE* f = OpenOut(outName);
+  // layout: int32 nev, int32 iterations, int32 converged, double seconds, nev doubles (sorted lowest
+  // Ritz values), int32 nbr history, history doubles (lowest Ritz value after each extra step)
+  fwrite(&nev, sizeof(int), 1, f);
+  fwrite(&CurrentNbrIter, sizeof(int), 1, f);
+  fwrite(&Converged, sizeof(int), 1, f);
+  double Seconds = t1 - t0;
+  fwrite(&Seconds, sizeof(double), 1, f);
+  WriteEigenvalues(f, Lanczos, nev);
+  int NbrHistory = (int) History.size();
+  fwrite(&NbrHistory, sizeof(int), 1, f);
+  if (NbrHistory > 0)
+    fwrite(&History[0], sizeof(double), NbrHistory, f);
+  fclose(f);
+  if ((groundStateName != 0) && (strcmp(algo, "ground") == 0))
+    {
+      RealVector& GS = (RealVector&) Lanczos->GetGroundState();
+      GS.WriteVector(groundStateName);
+    }
+  delete Lanczos;
+}
+
+// REF_THREADS=P (environment) runs the Lanczos commands on SMPArchitecture(P) instead of the
+// mono-processor architecture, as the reference programs do with -S --processors P
+static AbstractArchitecture* MakeArchitecture()
+{
+  const char* Env = getenv("REF_THREADS");
+  int P = (Env != 0) ? atoi(Env) : 1;
+  if (P > 1)
+    return new SMPArchitecture(P);
+  return new MonoProcessorArchitecture;
+}
+
+static void Usage()
+{
+  fprintf(stderr,
+	  "ref_tool commands (all outputs little-endian binary):\n"
+	  "  fqhe_basis N 2S 2Lz out\n"
+	  "  fqhe_factors N 2S vfile out\n"
+	  "  fqhe_rows N 2S 2Lz vfile rowsfile out\n"
+	  "  fqhe_matvec N 2S 2Lz vfile xfile shift out\n"
+	  "  fqhe_lanczos N 2S 2Lz vfile algo nev block maxiter precision out gsout x0 [x1 ...]\n"
+	  "  fqhe_expect N 2S 2Lz vfile psifile out\n"
+	  "  pseudopotentials 2S out\n"
+	  "  spin_basis L 2Sz out\n"
+	  "  spin_matvec L 2Sz J1 J2 xfile out\n"
+	  "  spin_lanczos L 2Sz J1 J2 algo nev block maxiter precision out x0 [x1 ...]\n"
+	  "  bench_fqhe N 2S 2Lz vfile threads reps hermitian\n"
+	  "  bench_spin L 2Sz J1 J2 threads reps 0\n");
+  exit(1);
+}
+
+int main(int argc, char** argv)
+{
+  if (argc < 2)
+    Usage();
+  const char* Cmd = argv[1];
+  cout.precision(17);
+  if (strcmp(Cmd, "fqhe_basis") == 0 && argc == 6)
+    {
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      ExposedFermionOnSphere Space(N, TotalLz, LzMax, 1ul << 20);
+      long Dim = Space.GetHilbertSpaceDimension();
+      FILE* f = OpenOut(argv[5]);
+      fwrite(&Dim, sizeof(long), 1, f);
+      for (long i = 0; i < Dim; ++i)
+	{
+	  unsigned long w = Space.Word(i);
+	  fwrite(&w, sizeof(unsigned long), 1, f);
+	}
+      for (long i = 0; i < Dim; ++i)
+	{
+	  int l = Space.WordLzMax(i);
+	  fwrite(&l, sizeof(int), 1, f);
+	}
+      // FindStateIndex of every basis word (the TestFindAllStates invariant)
+      for (long i = 0; i < Dim; ++i)
+	{
+	  int idx = Space.Find(Space.Word(i), Space.WordLzMax(i));
+	  fwrite(&idx, sizeof(int), 1, f);
+	}
+      fclose(f);
+      return 0;
+    }
+  if (strcmp(Cmd, "fqhe_factors") == 0 && argc == 6)
+    {
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]);
+      double* V = ReadDoubles(argv[4], LzMax + 1);
+      FermionOnSphere Space(N, (N & 1) ? 1 : 0, LzMax, 1ul << 20);
+      MonoProcessorArchitecture Arch;
+      ExposedGenericHamiltonian H(&Space, N, LzMax, V, &Arch, false);
+      FILE* f = OpenOut(argv[5]);
+      // layout: int32 nbrM12, then per pair int32 (m1, m2, nbrM3, m3[nbrM3]); int32 nbrFactors; doubles
+      int P = H.GetNbrM12();
+      fwrite(&P, sizeof(int), 1, f);
+      for (int i = 0; i < P; ++i)
+	{
+	  int a[3] = {H.M1(i), H.M2(i), H.NbrM3(i)};
+	  fwrite(a, sizeof(int), 3, f);
+	  for (int j = 0; j < a[2]; ++j)
+	    {
+	      int m3 = H.M3(i, j);
+	      fwrite(&m3, sizeof(int), 1, f);
+	    }
+	}
+      int F = H.NbrFactors();
+      fwrite(&F, sizeof(int), 1, f);
+      for (int i = 0; i < F; ++i)
+	{
+	  double x = H.Factor(i);
+	  fwrite(&x, sizeof(double), 1, f);
+	}
+      fclose(f);
+      return 0;
+    }
+  if (strcmp(Cmd, "fqhe_rows") == 0 && argc == 8)
+    {
+      // the inner loops of AbstractQHEOnSphereHamiltonian::LowLevelAddMultiply (:456-488), one
+      // (target, AA sign * AdAd sign, factor index) triple per generated element, in the
+      // reference's own enumeration order
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      double* V = ReadDoubles(argv[5], LzMax + 1);
+      long NbrRows;
+      int* Rows = ReadInts(argv[6], NbrRows);
+      FermionOnSphere Space(N, TotalLz, LzMax, 1ul << 20);
+      MonoProcessorArchitecture Arch;
+      ExposedGenericHamiltonian H(&Space, N, LzMax, V, &Arch, false);
+      int Dim = Space.GetHilbertSpaceDimension();
+      FILE* f = OpenOut(argv[7]);
+      // layout: per requested row: int32 row, int32 count, count x (int32 target, int32 sign, int32 factor)
+      for (long r = 0; r < NbrRows; ++r)
+	{
+	  int i = Rows[r];
+	  std::vector<int> Out;
+	  int FactorIndex = 0;
+	  for (int p = 0; p < H.GetNbrM12(); ++p)
+	    {
+	      double C1 = Space.AA(i, H.M1(p), H.M2(p));
+	      if (C1 != 0.0)
+		{
+		  int Sum = H.M1(p) + H.M2(p);
+		  for (int q = 0; q < H.NbrM3(p); ++q)
+		    {
+		      double C2;
+		      int m3 = H.M3(p, q);
+		      int Index = Space.AdAd(m3, Sum - m3, C2);
+		      if (Index < Dim)
+			{
+			  Out.push_back(Index);
+			  Out.push_back((C1 * C2) > 0.0 ? 1 : -1);
+			  Out.push_back(FactorIndex);
+			}
+		      ++FactorIndex;
+		    }
+		}
+	      else
+		FactorIndex += H.NbrM3(p);
+	    }
+	  int Count = (int) Out.size() / 3;
+	  fwrite(&i, sizeof(int), 1, f);
+	  fwrite(&Count, sizeof(int), 1, f);
+	  if (Count > 0)
+	    fwrite(&Out[0], sizeof(int), Out.size(), f);
+	}
+      fclose(f);
+      return 0;
+    }
+  if (strcmp(Cmd, "fqhe_matvec") == 0 && argc == 9)
+    {
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      double* V = ReadDoubles(argv[5], LzMax + 1);
+      FermionOnSphere Space(N, TotalLz, LzMax, 1ul << 20);
+      MonoProcessorArchitecture Arch;
+      ParticleOnSphereGenericHamiltonian H(&Space, N, LzMax, V, 0.0, &Arch, 0, false, 0, false);
+      H.ShiftHamiltonian(atof(argv[7]));
+      RealVector X;
+      X.ReadVector(argv[6]);
+      RealVector Y(Space.GetHilbertSpaceDimension(), true);
+      H.LowLevelMultiply(X, Y);
+      Y.WriteVector(argv[8]);
+      return 0;
+    }
+  if (strcmp(Cmd, "fqhe_lanczos") == 0 && argc >= 14)
+    {
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      double* V = ReadDoubles(argv[5], LzMax + 1);
+      const char* Algo = argv[6];
+      int Nev = atoi(argv[7]), Block = atoi(argv[8]), MaxIter = atoi(argv[9]);
+      double Precision = atof(argv[10]);
+      FermionOnSphere Space(N, TotalLz, LzMax, 9ul << 20);
+      AbstractArchitecture* Arch = MakeArchitecture();
+      Arch->SetDimension(Space.GetHilbertSpaceDimension());
+      ParticleOnSphereGenericHamiltonian H(&Space, N, LzMax, V, 0.0, Arch, 0, false, 0, false);
+      int NbrInitial = argc - 13;
+      RealVector* Init = new RealVector[NbrInitial];
+      for (int i = 0; i < NbrInitial; ++i)
+	Init[i].ReadVector(argv[13 + i]);
+      RunLanczosLoop(&H, Arch, Algo, Nev, Block, MaxIter, Precision, Init, NbrInitial, argv[11],
+		     strcmp(argv[12], "-") == 0 ? 0 : argv[12]);
+      return 0;
+    }
+  if (strcmp(Cmd, "fqhe_expect") == 0 && argc == 8)
+    {
+      // <psi|H_m|psi> for every m, with H_m the generic Hamiltonian of V = e_m (linearity of
+      // EvaluateInteractionFactors in V), followed by <psi|H(V)|psi> for the given V
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      double* V = ReadDoubles(argv[5], LzMax + 1);
+      FermionOnSphere Space(N, TotalLz, LzMax, 1ul << 20);
+      MonoProcessorArchitecture Arch;
+      RealVector Psi;
+      Psi.ReadVector(argv[6]);
+      RealVector Tmp(Space.GetHilbertSpaceDimension(), true);
+      FILE* f = OpenOut(argv[7]);
+      double* E = new double[LzMax + 1];
+      for (int m = 0; m <= LzMax; ++m)
+	{
+	  for (int k = 0; k <= LzMax; ++k)
+	    E[k] = (k == m) ? 1.0 : 0.0;
+	  ParticleOnSphereGenericHamiltonian Hm(&Space, N, LzMax, E, 0.0, &Arch, 0, false, 0, false);
+	  Hm.LowLevelMultiply(Psi, Tmp);
+	  double x = (Psi * Tmp) / (Psi * Psi);
+	  fwrite(&x, sizeof(double), 1, f);
+	}
+      ParticleOnSphereGenericHamiltonian H(&Space, N, LzMax, V, 0.0, &Arch, 0, false, 0, false);
+      H.LowLevelMultiply(Psi, Tmp);
+      double x = (Psi * Tmp) / (Psi * Psi);
+      fwrite(&x, sizeof(double), 1, f);
+      fclose(f);
+      return 0;
+    }
+  if (strcmp(Cmd, "pseudopotentials") == 0 && argc == 4)
+    {
+      int NbrFlux = atoi(argv[2]);
+      double* V = EvaluatePseudopotentials(NbrFlux, 0, 0.0, true);
+      FILE* f = OpenOut(argv[3]);
+      fwrite(V, sizeof(double), NbrFlux + 1, f);
+      fclose(f);
+      return 0;
+    }
+  if (strcmp(Cmd, "spin_basis") == 0 && argc == 5)
+    {
+      int L = atoi(argv[2]), Sz = atoi(argv[3]);
+      ExposedSpin1_2Chain Chain(L, Sz, 1 << 20);
+      long Dim = Chain.GetHilbertSpaceDimension();
+      FILE* f = OpenOut(argv[4]);
+      fwrite(&Dim, sizeof(long), 1, f);
+      for (long i = 0; i < Dim; ++i)
+	{
+	  unsigned long w = Chain.Word(i);
+	  fwrite(&w, sizeof(unsigned long), 1, f);
+	}
+      for (long i = 0; i < Dim; ++i)
+	{
+	  int idx = Chain.Find(Chain.Word(i));
+	  fwrite(&idx, sizeof(int), 1, f);
+	}
+      fclose(f);
+      return 0;
+    }
+  if (strcmp(Cmd, "spin_matvec") == 0 && argc == 8)
+    {
+      int L = atoi(argv[2]), Sz = atoi(argv[3]);
+      Spin1_2Chain Chain(L, Sz, 1 << 20);
+      J1J2ChainHarness H(&Chain, L, atof(argv[4]), atof(argv[5]));
+      RealVector X;
+      X.ReadVector(argv[6]);
+      RealVector Y(Chain.GetHilbertSpaceDimension(), true);
+      H.LowLevelMultiply(X, Y);
+      Y.WriteVector(argv[7]);
+      return 0;
+    }
+  if (strcmp(Cmd, "spin_lanczos") == 0 && argc >= 13)
+    {
+      int L = atoi(argv[2]), Sz = atoi(argv[3]);
+      Spin1_2Chain Chain(L, Sz, 1 << 20);
+      J1J2ChainHarness H(&Chain, L, atof(argv[4]), atof(argv[5]));
+      AbstractArchitecture* Arch = MakeArchitecture();
+      Arch->SetDimension(Chain.GetHilbertSpaceDimension());
+      const char* Algo = argv[6];
+      int Nev = atoi(argv[7]), Block = atoi(argv[8]), MaxIter = atoi(argv[9]);
+      double Precision = atof(argv[10]);
+      int NbrInitial = argc - 12;
+      RealVector* Init = new RealVector[NbrInitial];
+      for (int i = 0; i < NbrInitial; ++i)
+	Init[i].ReadVector(argv[12 + i]);
+      RunLanczosLoop(&H, Arch, Algo, Nev, Block, MaxIter, Precision, Init, NbrInitial, argv[11], 0);
+      return 0;
+    }
+  if (strcmp(Cmd, "bench_fqhe") == 0 && argc == 9)
+    {
+      // times the reference SMP matvec: VectorHamiltonianMultiplyOperation on SMPArchitecture
+      // (VectorHamiltonianMultiplyOperation.cc:241-320), on-the-fly (memory 0) as with -m 0
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      double* V = ReadDoubles(argv[5], LzMax + 1);
+      int Threads = atoi(argv[6]);
+      int Reps = atoi(argv[7]);
+      bool Hermitian = atoi(argv[8]) != 0;
+      double ts = Now();
+      FermionOnSphere Space(N, TotalLz, LzMax, 9ul << 20);
+      SMPArchitecture Arch(Threads);
+      Arch.SetDimension(Space.GetHilbertSpaceDimension());
+      ParticleOnSphereGenericHamiltonian H(&Space, N, LzMax, V, 0.0, &Arch, 0, false, 0, Hermitian);
+      double tsetup = Now() - ts;
+      long Dim = Space.GetHilbertSpaceDimension();
+      RealVector X(Dim, true), Y(Dim, true);
+      for (long i = 0; i < Dim; ++i)
+	X[i] = 1.0 / sqrt((double) Dim);
+      double Best = 1e30, Total = 0.0, Check = 0.0;
+      for (int r = 0; r < Reps; ++r)
+	{
+	  VectorHamiltonianMultiplyOperation Op(&H, &X, &Y);
+	  double t0 = Now();
+	  Op.ApplyOperation(&Arch);
+	  double t = Now() - t0;
+	  Total += t;
+	  if (t < Best)
+	    Best = t;
+	  Check = X * Y;
+	}
+      printf("{\"dim\": %ld, \"threads\": %d, \"reps\": %d, \"best_s\": %.6e, \"mean_s\": %.6e, "
+	     "\"setup_s\": %.3f, \"hermitian\": %d, \"xHx\": %.15e}\n", Dim, Threads, Reps, Best, Total / Reps,
+	     tsetup, Hermitian ? 1 : 0, Check);
+      return 0;
+    }
+  if (strcmp(Cmd, "bench_spin") == 0 && argc == 9)
+    {
+      int L = atoi(argv[2]), Sz = atoi(argv[3]);
+      int Threads = atoi(argv[6]);
+      int Reps = atoi(argv[7]);
+      (void) argv[8];
+      double ts = Now();
+      Spin1_2Chain Chain(L, Sz, 1 << 26);
+      J1J2ChainHarness H(&Chain, L, atof(argv[4]), atof(argv[5]));
+      SMPArchitecture Arch(Threads);
+      Arch.SetDimension(Chain.GetHilbertSpaceDimension());
+      double tsetup = Now() - ts;
+      long Dim = Chain.GetHilbertSpaceDimension();
+      RealVector X(Dim, true), Y(Dim, true);
+      for (long i = 0; i < Dim; ++i)
+	X[i] = 1.0 / sqrt((double) Dim);
+      double Best = 1e30, Total = 0.0, Check = 0.0;
+      for (int r = 0; r < Reps; ++r)
+	{
+	  VectorHamiltonianMultiplyOperation Op(&H, &X, &Y);
+	  double t0 = Now();
+	  Op.ApplyOperation(&Arch);
+	  double t = Now() - t0;
+	  Total += t;
+	  if (t < Best)
+	    Best = t;
+	  Check = X * Y;
+	}
+      printf("{\"dim\": %ld, \"threads\": %d, \"reps\": %d, \"best_s\": %.6e, \"mean_s\": %.6e, "
+	     "\"setup_s\": %.3f, \"xHx\": %.15e}\n", Dim, Threads, Reps, Best, Total / Reps, tsetup, Check);
+      return 0;
+    }
+  Usage();
+  return 1;
+}

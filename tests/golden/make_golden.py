@@ -1,0 +1,290 @@
+"""Generates the golden fixtures of the parity tests by running the reference itself.
+
+Every fixture in this directory is produced by oracle/_ref/ref_tool (the reference compiled from
+its own sources by `make -C oracle ref`; see oracle/ref_harness/ref_tool.cc for what each command
+calls).  This script needs the reference checkout (default /root/reference, or $DIAGHAM_REF) and is
+run by hand; the tests only read the .npz files it writes.
+
+    python tests/golden/make_golden.py            # all small fixtures (about a minute)
+    python tests/golden/make_golden.py --slow     # adds the long N=12, 2S=33 reference Lanczos run
+
+Binary layouts written by ref_tool are documented next to each reader below.  Start vectors are
+the repository's splitmix64 vectors (component i = (i+1)-th splitmix64 output of the seed mapped to
+[-1, 1), normalised), written in DiagHam's vector format (int32 dimension + little-endian doubles,
+RealVector::WriteVector, src/Vector/RealVector.cc:3669).
+"""
+import argparse
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+TOOL = os.path.join(ROOT, "oracle", "_ref", "ref_tool")
+
+
+def splitmix_vector(seed, dim):
+    i = np.arange(1, dim + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + i * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    x = (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0) * 2.0 - 1.0
+    return x / np.sqrt(np.dot(x, x))
+
+
+def uniform(seed, n, lo, hi):
+    """n values uniform in [lo, hi) from splitmix64(seed), the same stream as splitmix_vector."""
+    i = np.arange(1, n + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + i * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return lo + (hi - lo) * (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def write_vector(path, x):
+    with open(path, "wb") as f:
+        f.write(np.int32(len(x)).tobytes())
+        f.write(np.ascontiguousarray(x, np.float64).tobytes())
+
+
+def read_vector(path):
+    b = open(path, "rb").read()
+    d = int(np.frombuffer(b[:4], np.int32)[0])
+    return np.frombuffer(b[4:4 + 8 * d], np.float64).copy()
+
+
+def run(*args, env=None):
+    cmd = [TOOL] + [str(a) for a in args]
+    e = dict(os.environ)
+    if env:
+        e.update(env)
+    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, env=e)
+    return " ".join(["ref_tool"] + [str(a) for a in args[:-1]])
+
+
+def read_basis(path):
+    # int64 dim, dim uint64 words, dim int32 lzmax (fermions only), dim int32 FindStateIndex
+    b = open(path, "rb").read()
+    d = int(np.frombuffer(b[:8], np.int64)[0])
+    w = np.frombuffer(b[8:8 + 8 * d], np.uint64).copy()
+    rest = np.frombuffer(b[8 + 8 * d:], np.int32).copy()
+    return d, w, rest
+
+
+def read_factors(path):
+    # int32 nbrM12, per pair int32 (m1, m2, nbrM3, m3...), int32 nbrFactors, doubles
+    b = np.fromfile(path, np.int32)
+    p = int(b[0])
+    i = 1
+    m1, m2, nm3, m3 = [], [], [], []
+    for _ in range(p):
+        m1.append(b[i]); m2.append(b[i + 1]); nm3.append(b[i + 2])
+        m3.extend(b[i + 3:i + 3 + b[i + 2]])
+        i += 3 + b[i + 2]
+    nf = int(b[i])
+    fac = np.frombuffer(b[i + 1:].tobytes(), np.float64)[:nf].copy()
+    return dict(m1=np.array(m1, np.int32), m2=np.array(m2, np.int32), nbr_m3=np.array(nm3, np.int32),
+                m3=np.array(m3, np.int32), factors=fac)
+
+
+def read_lanczos(path):
+    # int32 nev, int32 iterations, int32 converged, double seconds, nev doubles, int32 nhist, nhist doubles
+    b = open(path, "rb").read()
+    nev, it, conv = np.frombuffer(b[:12], np.int32)
+    eig = np.frombuffer(b[20:20 + 8 * nev], np.float64).copy()
+    o = 20 + 8 * nev
+    nh = int(np.frombuffer(b[o:o + 4], np.int32)[0])
+    hist = np.frombuffer(b[o + 4:o + 4 + 8 * nh], np.float64).copy()
+    return dict(nev=int(nev), iterations=int(it), converged=int(conv), eigenvalues=eig, history=hist)
+
+
+def read_rows(path):
+    # per row: int32 row, int32 count, count x (int32 target, int32 sign, int32 factor)
+    b = np.fromfile(path, np.int32)
+    i = 0
+    rows, offs, trip = [], [0], []
+    while i < len(b):
+        r, c = b[i], b[i + 1]
+        rows.append(r)
+        trip.append(b[i + 2:i + 2 + 3 * c].reshape(c, 3))
+        offs.append(offs[-1] + c)
+        i += 2 + 3 * c
+    t = np.concatenate(trip) if trip else np.zeros((0, 3), np.int32)
+    return dict(rows=np.array(rows, np.int32), offsets=np.array(offs, np.int64), targets=t[:, 0].copy(),
+                signs=t[:, 1].copy(), factor_index=t[:, 2].copy())
+
+
+def coulomb_odd(two_s, tmp):
+    p = os.path.join(tmp, "pp.bin")
+    run("pseudopotentials", two_s, p)
+    v = np.fromfile(p, np.float64)
+    v[0::2] = 0.0
+    return v
+
+
+def save(name, cmd, **arrays):
+    np.savez_compressed(os.path.join(HERE, name), command=np.array(cmd), **arrays)
+    print("wrote", name)
+
+
+def fermion_fixtures(tmp):
+    for (n, s, lz) in [(4, 8, 2), (8, 21, 0), (5, 13, 1), (6, 15, 8), (3, 9, -3), (7, 18, 4)]:
+        p = os.path.join(tmp, "b.bin")
+        cmd = run("fqhe_basis", n, s, lz, p)
+        d, w, rest = read_basis(p)
+        save("fqhe_basis_n%d_2s%d_lz%d.npz" % (n, s, lz), cmd, words=w, lzmax=rest[:d], find=rest[d:2 * d])
+    for s in (8, 21, 27, 33):
+        p = os.path.join(tmp, "v.bin")
+        cmd = run("pseudopotentials", s, p)
+        save("pseudopotentials_2s%d.npz" % s, cmd, v=np.fromfile(p, np.float64))
+    for (s, kind) in [(21, "v1"), (27, "coulomb"), (33, "coulomb")]:
+        if kind == "v1":
+            v = np.zeros(s + 1)
+            v[1] = 1.0
+        else:
+            v = coulomb_odd(s, tmp)
+        vf = os.path.join(tmp, "vv.bin")
+        v.tofile(vf)
+        p = os.path.join(tmp, "f.bin")
+        cmd = run("fqhe_factors", 8, s, vf, p)
+        save("factors_2s%d_%s.npz" % (s, kind), cmd, v=v, **read_factors(p))
+
+
+def fqhe_sector_fixtures(tmp, n, s, lz, kind, rows_sample, lanczos=True, algos=("basic",)):
+    if kind == "v1":
+        v = np.zeros(s + 1)
+        v[1] = 1.0
+    else:
+        v = coulomb_odd(s, tmp)
+    vf = os.path.join(tmp, "vv.bin")
+    v.tofile(vf)
+    tag = "n%d_2s%d_lz%d_%s" % (n, s, lz, kind)
+    rows = np.asarray(rows_sample, np.int32)
+    rf = os.path.join(tmp, "rows.bin")
+    rows.tofile(rf)
+    p = os.path.join(tmp, "rows.out")
+    cmd = run("fqhe_rows", n, s, lz, vf, rf, p)
+    save("rows_%s.npz" % tag, cmd, v=v, **read_rows(p))
+    if not lanczos:
+        return
+    from math import comb  # noqa: F401  (dimension comes from the basis fixture / oracle)
+    dfile = os.path.join(tmp, "b.bin")
+    run("fqhe_basis", n, s, lz, dfile)
+    dim, _, _ = read_basis(dfile)
+    x = splitmix_vector(0, dim)
+    xf = os.path.join(tmp, "x0.vec")
+    write_vector(xf, x)
+    for shift in (0.0, 0.37):
+        yf = os.path.join(tmp, "y.vec")
+        cmd = run("fqhe_matvec", n, s, lz, vf, xf, shift, yf)
+        save("matvec_%s_shift%g.npz" % (tag, shift), cmd, v=v, seed=0, shift=shift, y=read_vector(yf))
+    for algo in algos:
+        lf = os.path.join(tmp, "l.out")
+        gf = os.path.join(tmp, "gs.vec")
+        cmd = run("fqhe_lanczos", n, s, lz, vf, algo, 1, 1, 200, 0, lf, gf if algo == "ground" else "-", xf)
+        extra = {}
+        if algo == "ground":
+            psi = read_vector(gf)
+            ef = os.path.join(tmp, "expect.bin")
+            run("fqhe_expect", n, s, lz, vf, gf, ef)
+            e = np.fromfile(ef, np.float64)
+            extra = dict(expectation=e[:-1], energy_expectation=e[-1], psi_norm=np.linalg.norm(psi))
+        save("lanczos_%s_%s.npz" % (tag, algo), cmd, v=v, seed=0, max_iter=200, **read_lanczos(lf), **extra)
+
+
+def block_fixture(tmp, n, s, lz, k):
+    v = coulomb_odd(s, tmp)
+    vf = os.path.join(tmp, "vv.bin")
+    v.tofile(vf)
+    dfile = os.path.join(tmp, "b.bin")
+    run("fqhe_basis", n, s, lz, dfile)
+    dim, _, _ = read_basis(dfile)
+    files = []
+    for b in range(k):
+        xf = os.path.join(tmp, "xb%d.vec" % b)
+        write_vector(xf, splitmix_vector(100 + b, dim))
+        files.append(xf)
+    lf = os.path.join(tmp, "l.out")
+    cmd = run("fqhe_lanczos", n, s, lz, vf, "block", 2, k, 400, 0, lf, "-", *files)
+    save("lanczos_n%d_2s%d_lz%d_coulomb_block%d.npz" % (n, s, lz, k), cmd, v=v, seeds=np.arange(100, 100 + k),
+         **read_lanczos(lf))
+
+
+def spin_fixtures(tmp):
+    for (L, sz) in [(10, 0), (9, 1), (12, 0), (12, -4), (32, 30)]:
+        p = os.path.join(tmp, "sb.bin")
+        cmd = run("spin_basis", L, sz, p)
+        d, w, rest = read_basis(p)
+        save("spin_basis_L%d_sz%d.npz" % (L, sz), cmd, words=w, find=rest[:d])
+    for (L, sz, j1, j2) in [(12, 0, 1.0, 0.5), (11, 1, 1.0, 0.3), (10, 2, 0.7, -0.4)]:
+        p = os.path.join(tmp, "sb.bin")
+        run("spin_basis", L, sz, p)
+        d, _, _ = read_basis(p)
+        xf = os.path.join(tmp, "sx.vec")
+        write_vector(xf, splitmix_vector(3, d))
+        yf = os.path.join(tmp, "sy.vec")
+        cmd = run("spin_matvec", L, sz, j1, j2, xf, yf)
+        save("spin_matvec_L%d_sz%d_j%g_%g.npz" % (L, sz, j1, j2), cmd, seed=3, y=read_vector(yf))
+    for (L, sz, j1, j2) in [(16, 0, 1.0, 0.5), (14, 0, 1.0, 0.2), (13, 1, 1.0, 0.5)]:
+        p = os.path.join(tmp, "sb.bin")
+        run("spin_basis", L, sz, p)
+        d, _, _ = read_basis(p)
+        xf = os.path.join(tmp, "sx.vec")
+        write_vector(xf, splitmix_vector(0, d))
+        lf = os.path.join(tmp, "sl.out")
+        cmd = run("spin_lanczos", L, sz, j1, j2, "basic", 1, 1, 400, 0, lf, xf)
+        save("spin_lanczos_L%d_sz%d_j%g_%g.npz" % (L, sz, j1, j2), cmd, seed=0, **read_lanczos(lf))
+
+
+def slow_fixtures(tmp):
+    # the precision workload: N = 12, 2S = 33, Lz = 0, LLL Coulomb (odd m), start vector seed 0
+    v = coulomb_odd(33, tmp)
+    vf = os.path.join(tmp, "vv.bin")
+    v.tofile(vf)
+    dim = 7764392
+    xf = os.path.join(tmp, "x0.vec")
+    write_vector(xf, splitmix_vector(0, dim))
+    lf = os.path.join(tmp, "l.out")
+    threads = os.cpu_count() or 1
+    cmd = run("fqhe_lanczos", 12, 33, 0, vf, "basic", 1, 1, 400, 1e-13, lf, "-", xf, env={"REF_THREADS": str(threads)})
+    save("lanczos_n12_2s33_lz0_coulomb_basic.npz", cmd + " (REF_THREADS=%d)" % threads, v=v, seed=0, precision=1e-13,
+         **read_lanczos(lf))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--slow", action="store_true")
+    ap.add_argument("--only", default=None)
+    args = ap.parse_args()
+    if not os.path.exists(TOOL):
+        sys.exit("build the reference first: make -C oracle ref")
+    with tempfile.TemporaryDirectory() as tmp:
+        if args.only in (None, "fermion"):
+            fermion_fixtures(tmp)
+        if args.only in (None, "sectors"):
+            fqhe_sector_fixtures(tmp, 8, 21, 0, "v1", [0, 1, 2, 77, 4000, 8511])
+            fqhe_sector_fixtures(tmp, 8, 21, 0, "coulomb", [0, 5, 100, 2222, 8000, 8511],
+                                 algos=("basic", "full", "ground"))
+            fqhe_sector_fixtures(tmp, 7, 18, 2, "coulomb", [0, 3, 500, 1000], algos=("basic",))
+            rng = np.random.default_rng(12)
+            big = np.concatenate([[0, 1, 7764391], rng.integers(0, 7764392, 13)]).astype(np.int32)
+            fqhe_sector_fixtures(tmp, 12, 33, 0, "coulomb", big, lanczos=False)
+            mid = np.concatenate([[0, 246447], rng.integers(0, 246448, 10)]).astype(np.int32)
+            fqhe_sector_fixtures(tmp, 10, 27, 0, "coulomb", mid, lanczos=False)
+        if args.only in (None, "block"):
+            block_fixture(tmp, 6, 15, 0, 4)
+        if args.only in (None, "spin"):
+            spin_fixtures(tmp)
+        if args.slow:
+            slow_fixtures(tmp)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,163 @@
+"""The oracle (CPU restatement of the reference path) pinned against the reference's own outputs.
+
+Every fixture was produced by the reference compiled from its sources (tests/golden/make_golden.py);
+the oracle must reproduce integer results bit for bit and FP64 results to rounding.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden, parse_sector
+
+
+@pytest.mark.parametrize("name", sorted(os.path.basename(f) for f in glob.glob(os.path.join(GOLDEN, "fqhe_basis_*.npz"))))
+def test_fermion_basis_bit_exact(orc, name):
+    z = golden(name)
+    n, s, lz = parse_sector(name)
+    words, lzmax = orc.fermion_basis(n, s, lz)
+    assert np.array_equal(words, z["words"])
+    assert np.array_equal(lzmax, z["lzmax"])
+    # TestFindAllStates invariant of the reference (AbstractHilbertSpace.h:127)
+    assert np.array_equal(z["find"], np.arange(len(words)))
+
+
+def test_documented_basis_order(orc):
+    # FQHE/docs/DataFormat/FermionOnSphere.xml:19-40: N = 4, S = 4, Lz = 1, first and last states
+    words, _ = orc.fermion_basis(4, 8, 2)
+    assert len(words) == 11
+    assert int(words[0]) == 0b110000101 and int(words[-1]) == 0b001110100
+
+
+def test_lookup_table_find_state_index(orc):
+    z = golden("fqhe_basis_n8_2s21_lz0.npz")
+    for shift in (17, 9, 4, 1):
+        H = orc.FQHE(8, 21, 0, np.eye(22)[1], max_shift=shift)
+        for i in range(0, H.dim, 37):
+            assert H.find(z["words"][i]) == i
+
+
+@pytest.mark.parametrize("two_s", [8, 21, 27, 33])
+def test_coulomb_pseudopotentials(orc, two_s):
+    v = orc.coulomb_pseudopotentials(two_s)
+    ref = golden("pseudopotentials_2s%d.npz" % two_s)["v"]
+    assert np.max(np.abs(v - ref) / np.abs(ref)) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["factors_2s21_v1.npz", "factors_2s27_coulomb.npz", "factors_2s33_coulomb.npz"])
+def test_interaction_factors(orc, name):
+    z = golden(name)
+    two_s = int(name.split("_")[1][2:])
+    t = orc.interaction_tables(two_s, z["v"])
+    assert np.array_equal(t["m1"], z["m1"]) and np.array_equal(t["m2"], z["m2"])
+    assert np.array_equal(t["nbr_m3"], z["nbr_m3"]) and np.array_equal(t["m3"], z["m3"])
+    scale = np.max(np.abs(z["factors"]))
+    assert np.max(np.abs(t["factors"] - z["factors"])) < 1e-13 * scale
+
+
+def test_interaction_derivatives_linear(orc):
+    z = golden("factors_2s27_coulomb.npz")
+    d = orc.interaction_derivatives(27)
+    assert np.max(np.abs(d @ z["v"] - z["factors"])) < 1e-13 * np.max(np.abs(z["factors"]))
+
+
+def test_clebsch_gordan_orthonormal(orc):
+    # sum_J <j1 m1 j2 m2|J M><j1 m1' j2 m2'|J M> = delta for j1 = j2 = 33/2 (doubled projections)
+    j = 33
+    for M in (2, 14):
+        ms = [m for m in range(-j, j + 1, 2) if abs(M - m) <= j]
+        Js = list(range(abs(M), 2 * j + 1, 2))
+        C = np.array([[orc.clebsch_gordan(j, m, j, M - m, J) for J in Js] for m in ms])
+        assert np.max(np.abs(C @ C.T - np.eye(len(ms)))) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["rows_n8_2s21_lz0_v1.npz", "rows_n8_2s21_lz0_coulomb.npz",
+                                  "rows_n7_2s18_lz2_coulomb.npz", "rows_n10_2s27_lz0_coulomb.npz"])
+def test_row_elements_bit_exact(orc, name):
+    z = golden(name)
+    n, s, lz = parse_sector(name)
+    H = orc.FQHE(n, s, lz, z["v"])
+    for k, r in enumerate(z["rows"]):
+        a, b = z["offsets"][k], z["offsets"][k + 1]
+        t, sg, f = H.row(int(r))
+        assert np.array_equal(t, z["targets"][a:b])
+        assert np.array_equal(sg, z["signs"][a:b])
+        assert np.array_equal(f, z["factor_index"][a:b])
+
+
+@pytest.mark.parametrize("tag", ["n8_2s21_lz0_v1", "n8_2s21_lz0_coulomb", "n7_2s18_lz2_coulomb"])
+@pytest.mark.parametrize("shift", [0.0, 0.37])
+def test_matvec_push_and_pull(orc, tag, shift):
+    z = golden("matvec_%s_shift%g.npz" % (tag, shift))
+    n, s, lz = parse_sector(tag)
+    H = orc.FQHE(n, s, lz, z["v"], shift=shift)
+    x = orc.random_vector(0, H.dim)
+    tol = 1e-13 * max(1.0, np.max(np.abs(z["y"])))
+    assert np.max(np.abs(H.push(x) - z["y"])) < tol
+    assert np.max(np.abs(H.pull(x) - z["y"])) < tol
+
+
+@pytest.mark.parametrize("tag,algo", [("n8_2s21_lz0_coulomb", "basic"), ("n8_2s21_lz0_v1", "basic"),
+                                      ("n7_2s18_lz2_coulomb", "basic")])
+def test_lanczos_energy_and_iterations(orc, tag, algo):
+    z = golden("lanczos_%s_%s.npz" % (tag, algo))
+    n, s, lz = parse_sector(tag)
+    H = orc.FQHE(n, s, lz, z["v"])
+    r = H.lanczos(orc.random_vector(0, H.dim), 1, int(z["max_iter"]), 1e-14)
+    e_ref = float(z["eigenvalues"][0])
+    assert abs(r["eigenvalues"][0] - e_ref) <= 1e-10 * max(abs(e_ref), 1.0)
+    assert r["iterations"] == int(z["iterations"]) and r["converged"] == bool(z["converged"])
+
+
+def test_laughlin_exact_zero(orc):
+    z = golden("lanczos_n8_2s21_lz0_v1_basic.npz")
+    assert abs(float(z["eigenvalues"][0])) < 1e-10
+
+
+def test_hellmann_feynman_expectation(orc):
+    # <psi|H_m|psi> of the reference ground state, from the oracle's per-factor bins
+    z = golden("lanczos_n8_2s21_lz0_coulomb_ground.npz")
+    H = orc.FQHE(8, 21, 0, z["v"])
+    r = H.lanczos(orc.random_vector(0, H.dim), 1, 200, 1e-14)
+    assert abs(r["eigenvalues"][0] - z["energy_expectation"]) < 1e-10
+
+
+@pytest.mark.parametrize("name", sorted(os.path.basename(f) for f in glob.glob(os.path.join(GOLDEN, "spin_basis_*.npz"))))
+def test_spin_basis_bit_exact(orc, name):
+    z = golden(name)
+    L = int(name.split("_")[2][1:])
+    sz = int(name.split("_")[3][2:-4])
+    w = orc.spin_basis(L, sz)
+    assert np.array_equal(w, z["words"])
+    assert np.array_equal(z["find"], np.arange(len(w)))
+    for i in range(0, len(w), max(1, len(w) // 50)):
+        assert orc.spin_find(L, sz, w[i]) == i
+
+
+@pytest.mark.parametrize("name", sorted(os.path.basename(f) for f in glob.glob(os.path.join(GOLDEN, "spin_matvec_*.npz"))))
+def test_spin_matvec(orc, name):
+    z = golden(name)
+    parts = name[:-4].split("_")
+    L, sz = int(parts[2][1:]), int(parts[3][2:])
+    j1, j2 = float(parts[4][1:]), float(parts[5])
+    w = orc.spin_basis(L, sz)
+    x = orc.random_vector(3, len(w))
+    y = orc.spin_j1j2_multiply(L, sz, w, j1, j2, x)
+    assert np.max(np.abs(y - z["y"])) < 1e-13
+
+
+def test_spin_majumdar_ghosh(orc):
+    z = golden("spin_lanczos_L16_sz0_j1_0.5.npz")
+    assert abs(float(z["eigenvalues"][0]) + 6.0) < 1e-10  # E0 = -3L/8
+    w = orc.spin_basis(16, 0)
+    r = orc.python_lanczos(lambda v: orc.spin_j1j2_multiply(16, 0, w, 1.0, 0.5, v), len(w),
+                           orc.random_vector(0, len(w)), 1, 400, 1e-14)
+    assert abs(r["eigenvalues"][0] + 6.0) < 1e-10
+
+
+def test_random_vector_matches_fixture_generator(orc):
+    from golden.make_golden import splitmix_vector
+    a = orc.random_vector(7, 1000)
+    b = splitmix_vector(7, 1000)
+    assert np.max(np.abs(a - b)) < 1e-15
