@@ -61,9 +61,11 @@ SIGNATURES = {
     "dh_hamiltonian_row_elements": ([_vp, _c_i64, _vp, _vp, _vp, _c_int, _ip], _c_int),
     "dh_hamiltonian_pseudopotential_adjoint": ([_vp, _vp, _vp, _vp], _c_int),
     "dh_hamiltonian_get_interaction_factors": ([_vp, _vp, _c_int, _ip], _c_int),
+    "dh_hamiltonian_count_elements": ([_vp, _i64p], _c_int),
     "dh_lanczos_create": ([_vp, _c_int, _c_int, _c_int, _c_int, _vp], _c_int),
     "dh_lanczos_destroy": ([_vp], _c_int),
     "dh_lanczos_set_eigenvalue_precision": ([_vp, _c_dbl], _c_int),
+    "dh_lanczos_set_vector_storage": ([_vp, _c_int], _c_int),
     "dh_lanczos_initialize": ([_vp, _vp, _c_int], _c_int),
     "dh_lanczos_initialize_random": ([_vp, _c_u64], _c_int),
     "dh_lanczos_run": ([_vp, _c_int], _c_int),
@@ -253,6 +255,12 @@ class _Hamiltonian:
         d.finish()
         return dsts
 
+    def count_elements(self):
+        """Elements one product generates (moves incl. diagonal ones; spin flips)."""
+        t = ctypes.c_int64(0)
+        _check(_lib.dh_hamiltonian_count_elements(self._handle, ctypes.byref(t)))
+        return t.value
+
     def MatrixElement(self, v1, v2):
         a, b = _Buf(v1), _Buf(v2)
         out = ctypes.c_double(0.0)
@@ -334,6 +342,9 @@ class _Lanczos:
         _check(_lib.dh_lanczos_create(hamiltonian._handle, self.ALGORITHM, nbr_eigenvalue, block_size, max_iter,
                                       ctypes.byref(h)))
         self._handle = h
+
+    def set_vector_storage(self, keep):
+        _check(_lib.dh_lanczos_set_vector_storage(self._handle, 1 if keep else 0))
 
     def SetEigenvaluePrecision(self, precision):
         _check(_lib.dh_lanczos_set_eigenvalue_precision(self._handle, float(precision)))

@@ -317,6 +317,28 @@ int dh_lanczos_destroy(dh_lanczos_t l) {
   return DH_OK;
 }
 
+int dh_lanczos_set_vector_storage(dh_lanczos_t l, int keep) {
+  DH_CHECK(l, DH_ERR_ARGUMENT, "null lanczos");
+  DH_CHECK(l->algorithm != DH_LANCZOS_FULL_REORTHOGONALIZED || keep, DH_ERR_ARGUMENT,
+           "full re-orthogonalisation needs its vectors");
+  if (!keep) {
+    l->krylov.release();
+    l->krylov_cap = 0;
+  } else if (!l->krylov.ptr) {
+    int rc = l->krylov.alloc((size_t)l->cap * l->dim * sizeof(double));
+    if (rc != DH_OK) return rc;
+    l->krylov_cap = l->cap;
+  }
+  l->st.krylov = l->krylov.as<double>();
+  l->st.krylov_cap = l->krylov_cap;
+  if (l->graph3) {
+    cudaGraphExecDestroy(l->graph3);
+    l->graph3 = nullptr;
+  }
+  l->initialized = false;
+  return DH_OK;
+}
+
 int dh_lanczos_set_eigenvalue_precision(dh_lanczos_t l, double precision) {
   DH_CHECK(l && precision > 0.0, DH_ERR_ARGUMENT, "bad argument");
   l->precision = precision;

@@ -3,6 +3,8 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <math.h>
+
 #include <algorithm>
 #include <new>
 #include <vector>
@@ -504,11 +506,9 @@ static int multiply_common(dh_hamiltonian_t h, const double* src, double* dst, i
     if (accumulate) DH_CUDA(cudaMemcpyAsync(h->stage_y.ptr, dst, bytes, cudaMemcpyHostToDevice, h->stream));
     y = h->stage_y.as<double>();
   }
-  if (!accumulate) {
-    // LowLevelMultiply clears the destination, then adds (AbstractHamiltonian.cc:475-476)
-    DH_CUDA(cudaMemsetAsync(y, 0, bytes, h->stream));
-  }
-  if (nbr > 0 && (rc = hamiltonian_apply(h, x, y, nvec, first, nbr, 1, nullptr, h->stream)) != DH_OK) return rc;
+  // LowLevelMultiply clears the destination, then adds (AbstractHamiltonian.cc:475-476); the pull
+  // kernels write every row, so "clear then add" is a plain store (accumulate = 0)
+  if ((rc = hamiltonian_apply(h, x, y, nvec, first, nbr, accumulate, nullptr, h->stream)) != DH_OK) return rc;
   if (!dst_dev) DH_CUDA(cudaMemcpyAsync(dst, y, bytes, cudaMemcpyDeviceToHost, h->stream));
   DH_CUDA(cudaStreamSynchronize(h->stream));
   return DH_OK;
@@ -632,6 +632,29 @@ int dh_hamiltonian_pseudopotential_adjoint(dh_hamiltonian_t h, const double* u, 
     for (int f = 0; f < nf; ++f) acc += bins[f] * h->tabs.dfactor[(size_t)f * nlz + m];
     out[m] = acc;
   }
+  return DH_OK;
+}
+
+int dh_hamiltonian_count_elements(dh_hamiltonian_t h, int64_t* total) {
+  DH_CHECK(h && total, DH_ERR_ARGUMENT, "null argument");
+  dh_space_s* sp = h->space;
+  if (h->kind == SPACE_SPIN12) {
+    // every antiparallel bond is one flip: sum over the basis of #antiparallel bonds equals
+    // (#bonds) * (fraction of states in which a given bond is antiparallel) * dim
+    const long long L = sp->length, n = sp->nbr_up;
+    const double frac = (L >= 2) ? 2.0 * (double)n * (double)(L - n) / ((double)L * (double)(L - 1)) : 0.0;
+    *total = (int64_t)llround(2.0 * (double)L * frac * (double)sp->dim);
+    return DH_OK;
+  }
+  DevBuf t;
+  int rc;
+  if ((rc = t.alloc(sizeof(unsigned long long))) != DH_OK) return rc;
+  if ((rc = launch_fqhe_count(fqhe_device(sp, h, DH_PRECISION_FP64), t.as<unsigned long long>(), h->stream)) != DH_OK)
+    return rc;
+  unsigned long long v = 0;
+  DH_CUDA(cudaMemcpyAsync(&v, t.ptr, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+  DH_CUDA(cudaStreamSynchronize(h->stream));
+  *total = (int64_t)v;
   return DH_OK;
 }
 

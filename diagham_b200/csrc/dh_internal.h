@@ -115,6 +115,7 @@ int launch_fqhe_row_elements(const FqheDevice& f, long long row, int* targets, i
                              int cap, int* count, cudaStream_t s);
 int launch_fqhe_bins(const FqheDevice& f, const double* u, const double* v, double* partial_bins, int nblocks,
                      double* bins, cudaStream_t s);
+int launch_fqhe_count(const FqheDevice& f, unsigned long long* total, cudaStream_t s);
 int launch_fqhe_find(const FqheDevice& f, const uint64_t* words, long long n, long long* out, cudaStream_t s);
 
 struct SpinDevice {

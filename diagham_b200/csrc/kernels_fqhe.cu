@@ -361,6 +361,36 @@ __global__ void sum_partial_bins(const double* partial, int nblocks, int nbins, 
   bins[i] = acc;
 }
 
+// number of generated elements (moves) of all rows, block partials then one atomic per block
+__global__ void fqhe_count_kernel(FqheDevice f, unsigned long long* total) {
+  __shared__ unsigned long long acc;
+  if (threadIdx.x == 0) acc = 0;
+  __syncthreads();
+  const uint64_t full = (f.lz_max >= 63) ? ~0ull : ((1ull << (f.lz_max + 1)) - 1ull);
+  unsigned long long mine = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+    const uint64_t s = f.words[r];
+    uint64_t rem1 = s;
+    while (rem1) {
+      const int m1 = 63 - __clzll(rem1);
+      rem1 &= ~(1ull << m1);
+      uint64_t rem2 = rem1;
+      while (rem2) {
+        const int m2 = 63 - __clzll(rem2);
+        rem2 &= ~(1ull << m2);
+        const uint64_t an = s & ~((1ull << m1) | (1ull << m2));
+        const uint64_t e = ~an & full;
+        const int M = m1 + m2;
+        mine += __popcll(e & mirror_bits(e, M) & (~0ull << (M / 2 + 1)));
+      }
+    }
+  }
+  atomicAdd(&acc, mine);
+  __syncthreads();
+  if (threadIdx.x == 0) atomicAdd(total, acc);
+}
+
 template <int MODE>
 __global__ void fqhe_find_kernel(FqheDevice f, const uint64_t* words, long long n, long long* out) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -442,6 +472,16 @@ int launch_fqhe_bins(const FqheDevice& f, const double* u, const double* v, doub
   }
   sum_partial_bins<<<(f.nbr_factors + 255) / 256, 256, 0, s>>>(partial_bins, f.dim > 0 ? nblocks : 0, f.nbr_factors,
                                                                  bins);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_fqhe_count(const FqheDevice& f, unsigned long long* total, cudaStream_t s) {
+  DH_CUDA(cudaMemsetAsync(total, 0, sizeof(unsigned long long), s));
+  if (f.dim <= 0) return DH_OK;
+  long long g = (f.dim + 255) / 256;
+  if (g > 148 * 16) g = 148 * 16;
+  fqhe_count_kernel<<<(unsigned)g, 256, 0, s>>>(f, total);
   DH_CUDA(cudaGetLastError());
   return DH_OK;
 }

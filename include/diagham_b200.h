@@ -155,6 +155,10 @@ int dh_hamiltonian_row_elements(dh_hamiltonian_t h, int64_t row, int* targets, i
  * and v = x it is the V part of the vector-Jacobian product of H(V) x.  FQHE Hamiltonians only. */
 int dh_hamiltonian_pseudopotential_adjoint(dh_hamiltonian_t h, const double* u, const double* v, double* out);
 
+/* Number of elements (a+a+aa moves, diagonal ones included; spin flips for the chain) that one
+ * product generates over all rows, counted on the GPU. */
+int dh_hamiltonian_count_elements(dh_hamiltonian_t h, int64_t* total);
+
 /* Interaction factors of the current V (flattened in the reference order,
  * ParticleOnSphereGenericHamiltonian.cc:566-606) and their count. */
 int dh_hamiltonian_get_interaction_factors(dh_hamiltonian_t h, double* factors, int cap, int* count);
@@ -169,6 +173,12 @@ int dh_hamiltonian_get_interaction_factors(dh_hamiltonian_t h, double* factors, 
 int dh_lanczos_create(dh_hamiltonian_t h, int algorithm, int nbr_eigenvalue, int block_size, int max_iter,
                       dh_lanczos_t* out);
 int dh_lanczos_destroy(dh_lanczos_t l);
+
+/* Keep every Lanczos vector in device memory (keep = 1, default when it fits in half of the free
+ * memory) or only three and rebuild the ground state by a second pass (keep = 0), the store-or-
+ * recompute choice of BasicLanczosAlgorithmWithGroundState (DiskFlag, .cc:256-335).  Call before
+ * dh_lanczos_initialize. */
+int dh_lanczos_set_vector_storage(dh_lanczos_t l, int keep);
 
 /* SetEigenvaluePrecision (AbstractLanczosAlgorithm.h); default 1e-14 = MACHINE_PRECISION. */
 int dh_lanczos_set_eigenvalue_precision(dh_lanczos_t l, double precision);

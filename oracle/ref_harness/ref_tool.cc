@@ -321,7 +321,7 @@ static void Usage()
 	  "  spin_basis L 2Sz out\n"
 	  "  spin_matvec L 2Sz J1 J2 xfile out\n"
 	  "  spin_lanczos L 2Sz J1 J2 algo nev block maxiter precision out x0 [x1 ...]\n"
-	  "  bench_fqhe N 2S 2Lz vfile threads reps hermitian\n"
+	  "  bench_fqhe N 2S 2Lz vfile threads reps hermitian [rows]\n"
 	  "  bench_spin L 2Sz J1 J2 threads reps 0\n");
   exit(1);
 }
@@ -562,10 +562,13 @@ int main(int argc, char** argv)
       RunLanczosLoop(&H, Arch, Algo, Nev, Block, MaxIter, Precision, Init, NbrInitial, argv[11], 0);
       return 0;
     }
-  if (strcmp(Cmd, "bench_fqhe") == 0 && argc == 9)
+  if (strcmp(Cmd, "bench_fqhe") == 0 && (argc == 9 || argc == 10))
     {
       // times the reference SMP matvec: VectorHamiltonianMultiplyOperation on SMPArchitecture
-      // (VectorHamiltonianMultiplyOperation.cc:241-320), on-the-fly (memory 0) as with -m 0
+      // (VectorHamiltonianMultiplyOperation.cc:241-320), on-the-fly (memory 0) as with -m 0.
+      // An optional row count bounds the sample: the architecture's typical range (the rows the
+      // SMP operation splits between its threads, AbstractArchitecture.cc:65) is set to the first
+      // `rows` rows instead of the whole space.
       int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
       double* V = ReadDoubles(argv[5], LzMax + 1);
       int Threads = atoi(argv[6]);
@@ -574,10 +577,13 @@ int main(int argc, char** argv)
       double ts = Now();
       FermionOnSphere Space(N, TotalLz, LzMax, 9ul << 20);
       SMPArchitecture Arch(Threads);
-      Arch.SetDimension(Space.GetHilbertSpaceDimension());
+      long Dim = Space.GetHilbertSpaceDimension();
+      long Rows = (argc == 10) ? atol(argv[9]) : Dim;
+      if (Rows <= 0 || Rows > Dim)
+	Rows = Dim;
+      Arch.SetDimension(Rows);
       ParticleOnSphereGenericHamiltonian H(&Space, N, LzMax, V, 0.0, &Arch, 0, false, 0, Hermitian);
       double tsetup = Now() - ts;
-      long Dim = Space.GetHilbertSpaceDimension();
       RealVector X(Dim, true), Y(Dim, true);
       for (long i = 0; i < Dim; ++i)
 	X[i] = 1.0 / sqrt((double) Dim);
@@ -593,8 +599,8 @@ int main(int argc, char** argv)
 	    Best = t;
 	  Check = X * Y;
 	}
-      printf("{\"dim\": %ld, \"threads\": %d, \"reps\": %d, \"best_s\": %.6e, \"mean_s\": %.6e, "
-	     "\"setup_s\": %.3f, \"hermitian\": %d, \"xHx\": %.15e}\n", Dim, Threads, Reps, Best, Total / Reps,
+      printf("{\"dim\": %ld, \"rows\": %ld, \"threads\": %d, \"reps\": %d, \"best_s\": %.6e, \"mean_s\": %.6e, "
+	     "\"setup_s\": %.3f, \"hermitian\": %d, \"xHx\": %.15e}\n", Dim, Rows, Threads, Reps, Best, Total / Reps,
 	     tsetup, Hermitian ? 1 : 0, Check);
       return 0;
     }
