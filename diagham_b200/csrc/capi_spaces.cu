@@ -1,6 +1,7 @@
 // C ABI: Hilbert spaces and Hamiltonians (see include/diagham_b200.h for the contract).
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <math.h>
@@ -52,6 +53,11 @@ static int build_fermion_space(dh_space_s* sp) {
   // rank tables: index(w) = high_offset[w >> LB] + low_rank[w & (2^LB - 1)]
   FermionRankTables& t = sp->rank;
   t.low_bits = (L + 2) / 2;
+  if (sp->requested_low_bits > 0) t.low_bits = sp->requested_low_bits;
+  if (sp->kernel_variant == 2 && t.low_bits > 15) t.low_bits = 15;
+  if (t.low_bits < 3) t.low_bits = 3;
+  if (t.low_bits > L) t.low_bits = L;
+  if (L + 1 - t.low_bits > 26) t.low_bits = L + 1 - 26;
   t.high_bits = L + 1 - t.low_bits;
   const int LB = t.low_bits, HB = t.high_bits;
   const int maxsum = LB * (LB - 1) / 2;
@@ -153,6 +159,7 @@ FqheDevice fqhe_device(const dh_space_s* sp, const dh_hamiltonian_s* h, int prec
   f.low_bits = sp->rank.low_bits;
   f.lookup_bits = sp->lookup_bits;
   f.index_mode = sp->index_mode;
+  f.kernel_variant = sp->kernel_variant;
   if (h) {
     f.pair_offset = h->pair_offset.as<int32_t>();
     f.factors = (precision == DH_PRECISION_FP32) ? h->factors32.ptr : h->factors64.ptr;
@@ -272,6 +279,15 @@ int dh_fermion_on_sphere_create(int nbr_fermions, int total_lz, int lz_max, unsi
   sp->total_sum = twice / 2;
   sp->memory = memory;
   sp->index_mode = DH_INDEX_RANK;
+  // product kernel of the rank mode: split-word (default) or the generic one (DH_FQHE_KERNEL=generic)
+  // DH_FQHE_LOW_BITS sets the split of the rank tables; "smem" stages the low-rank table in shared
+  // memory (the split is then lowered until the table fits in 64 KiB)
+  const char* kv = getenv("DH_FQHE_KERNEL");
+  sp->kernel_variant = 0;
+  if (kv && strcmp(kv, "generic") == 0) sp->kernel_variant = 1;
+  if (kv && strcmp(kv, "smem") == 0) sp->kernel_variant = 2;
+  const char* lb = getenv("DH_FQHE_LOW_BITS");
+  sp->requested_low_bits = lb ? atoi(lb) : 0;
   int rc = build_fermion_space(sp);
   if (rc != DH_OK) {
     delete sp;

@@ -94,6 +94,7 @@ struct FqheDevice {
   int nbr_pairs;
   int nbr_factors;
   int index_mode;              // DH_INDEX_RANK or DH_INDEX_LOOKUP
+  int kernel_variant;          // 0: split-word rank kernel, 1: generic kernel (rank mode)
 };
 
 struct MatvecArgs {

@@ -15,6 +15,8 @@ struct dh_space_s {
   int kind = 0;
   int64_t dim = 0;
   int index_mode = DH_INDEX_RANK;
+  int kernel_variant = 0;  // product kernel of the rank mode (0 split-word, 1 generic, 2 split + smem table)
+  int requested_low_bits = 0;
   dh::DevBuf words;  // uint64 FermionOnSphere words, uint32 spin words (chain bits only)
   // FermionOnSphere
   int nbr_fermions = 0, lz_max = 0, total_lz = 0, total_sum = 0;

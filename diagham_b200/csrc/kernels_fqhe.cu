@@ -51,6 +51,7 @@ inline SmemLayout smem_layout(const FqheDevice& f, int elem) {
   s.factor_bytes = align16(f.nbr_factors * elem);
   s.pair_bytes = align16(f.nbr_pairs * (int)sizeof(int));
   s.lookup_bytes = 0;
+  if (f.index_mode == DH_INDEX_RANK && f.kernel_variant == 2) s.lookup_bytes = align16((1 << f.low_bits) * 2);
   if (f.index_mode == DH_INDEX_LOOKUP)
     s.lookup_bytes = align16((f.lz_max + 1) * ((1 << f.lookup_bits) + 1) * (int)sizeof(int)) +
                      align16((f.lz_max + 1) * (int)sizeof(int));
@@ -160,10 +161,209 @@ __global__ void __launch_bounds__(kMatvecThreads) fqhe_matvec_kernel(FqheDevice 
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Rank-mode product, split-word form.  The word is handled as a low half (orbitals 0..LB-1) and a
+// high half (LB..lz_max), the two halves of the rank tables: index(t) = HO[t_high] + LR[t_low].
+// Per row, HO of the row's own high half is loaded once and LR of its low half is r - HO.  Per
+// annihilated pair, whichever half the pair leaves untouched keeps the row's table value, so
+//   creations in the low half only  (m4 < m3 < LB):  one LR load,
+//   creations in the high half only (LB <= m4 < m3): one HO load,
+//   mixed creations (m4 < LB <= m3):                 one LR and one HO load,
+// all in 32-bit arithmetic.  Two creations are processed per iteration so that two independent
+// table-load -> gather chains are in flight per thread.
+__device__ __forceinline__ uint32_t between32(int lo, int hi) {
+  // bits strictly between lo and hi, 0 <= lo < hi <= 32
+  const uint32_t upto = (hi >= 32) ? 0xffffffffu : ((1u << hi) - 1u);
+  return upto & ~((2u << lo) - 1u);
+}
+
+template <typename TG, int K, bool RANGE>
+__device__ __forceinline__ void accumulate2(TG (&acc)[K], const TG* x, const MatvecArgs& a, int ia, TG fa, int ib,
+                                            TG fb) {
+  if (RANGE) {
+    if (ia < a.col_first || ia >= a.col_last) fa = TG(0);
+    if (ib < a.col_first || ib >= a.col_last) fb = TG(0);
+  }
+  if (K == 1 && a.ld == 1) {
+    acc[0] += fa * __ldg(x + ia) + fb * __ldg(x + ib);
+    return;
+  }
+  const TG* pa = x + (long long)ia * a.ld;
+  const TG* pb = x + (long long)ib * a.ld;
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    const TG xa = __ldg(pa + j * a.vstride);
+    const TG xb = __ldg(pb + j * a.vstride);
+    acc[j] += fa * xa + fb * xb;
+  }
+}
+
+template <typename TG, int K, bool RANGE, bool LR_SMEM>
+__global__ void __launch_bounds__(kMatvecThreads) fqhe_split_kernel(FqheDevice f, MatvecArgs a, SmemLayout lay) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  TG* sfac = reinterpret_cast<TG*>(smem);
+  int* spair = reinterpret_cast<int*>(smem + lay.factor_bytes);
+  const TG* gfac = static_cast<const TG*>(f.factors);
+  for (int i = threadIdx.x; i < f.nbr_factors; i += blockDim.x) sfac[i] = gfac[i];
+  for (int i = threadIdx.x; i < f.nbr_pairs; i += blockDim.x) spair[i] = f.pair_offset[i];
+  const int LB = f.low_bits;
+  const uint16_t* __restrict__ LR = f.low_rank;
+  if (LR_SMEM) {
+    uint16_t* slr = reinterpret_cast<uint16_t*>(smem + lay.factor_bytes + lay.pair_bytes);
+    const uint4* src = reinterpret_cast<const uint4*>(f.low_rank);
+    uint4* dst = reinterpret_cast<uint4*>(slr);
+    for (int i = threadIdx.x; i < (1 << LB) / 8; i += blockDim.x) dst[i] = src[i];
+    LR = slr;
+  }
+  __syncthreads();
+
+  const uint32_t lmask = (1u << LB) - 1u;
+  const int32_t* __restrict__ HO = f.high_offset;
+  const TG* x = static_cast<const TG*>(a.x);
+  const uint64_t full = (f.lz_max >= 63) ? ~0ull : ((1ull << (f.lz_max + 1)) - 1ull);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+    const uint64_t s = __ldg(f.words + r);
+    const uint32_t sl = (uint32_t)s & lmask;
+    const uint32_t sh = (uint32_t)(s >> LB);
+    const int ho_row = __ldg(HO + sh);
+    const int lr_row = (int)(r - ho_row);
+    // a non-diagonal creation pair is empty in the row itself, so its admissible m3 for the sum M
+    // are E & mirror_M(E) above M/2; the bit reversal of E is taken once per row
+    const uint64_t E = ~s & full;
+    const uint64_t RE = __brevll(E);
+    // exclusive prefix parity of s: bit k = parity of the occupied orbitals below k
+    uint64_t pp = s;
+    pp ^= pp << 1;
+    pp ^= pp << 2;
+    pp ^= pp << 4;
+    pp ^= pp << 8;
+    pp ^= pp << 16;
+    pp ^= pp << 32;
+    pp <<= 1;
+    TG acc[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) acc[j] = TG(0);
+    // diagonal elements: (m3, m4) = (m1, m2) is admissible for every occupied pair and its
+    // AA * AdAd sign is -1, so they add -sum(factor(m1, m2, m1)) * x[r]
+    TG dsum = TG(0);
+    uint64_t rem1 = s;
+    while (rem1) {
+      const int m1 = 63 - __clzll(rem1);
+      rem1 &= ~(1ull << m1);
+      uint64_t rem2 = rem1;
+      const int pbase = m1 * (m1 - 1) / 2;
+      const int p1 = (int)(pp >> m1) & 1;
+      while (rem2) {
+        const int m2 = 63 - __clzll(rem2);
+        rem2 &= ~(1ull << m2);
+        const int M = m1 + m2;
+        const TG* fp = sfac + (spair[pbase + m2] - (M / 2 + 1));
+        dsum -= fp[m1];
+        const uint64_t mir = (M <= 63) ? (RE >> (63 - M)) : (RE << (M - 63));
+        const uint64_t valid = E & mir & (~0ull << (M / 2 + 1));
+        if (!valid) continue;
+        // AA sign parity: 1 + occupied orbitals strictly between m2 and m1
+        const int paa = 1 ^ p1 ^ ((int)(pp >> (m2 + 1)) & 1);
+        const uint32_t anl = sl & ~((m1 < LB ? (1u << m1) : 0u) | (m2 < LB ? (1u << m2) : 0u));
+        const uint32_t anh = sh & ~((m1 >= LB ? (1u << (m1 - LB)) : 0u) | (m2 >= LB ? (1u << (m2 - LB)) : 0u));
+        // split the admissible m3 into three 32-bit masks:
+        //   vl: m3 < LB (creations in the low half), bit m3
+        //   vh: m4 = M - m3 >= LB (creations in the high half), bit m3 - LB
+        //   vm: m4 < LB <= m3 (mixed), bit m3 - LB
+        uint32_t vl = (uint32_t)valid & lmask;
+        const uint64_t hv = valid >> LB;
+        const int hcut = M - 2 * LB;  // relative m3 - LB <= M - 2 LB  <=>  m4 >= LB
+        const uint64_t hkeep = (hcut < 0) ? 0ull : ((hcut >= 63) ? ~0ull : ((2ull << hcut) - 1ull));
+        uint32_t vh = (uint32_t)(hv & hkeep);
+        uint32_t vm = (uint32_t)(hv & ~hkeep);
+        if (vl) {
+          const int base = (m1 < LB) ? ho_row : __ldg(HO + anh);
+          while (vl) {
+            const int m3a = __ffs(vl) - 1;
+            vl &= vl - 1u;
+            const bool two = vl != 0u;
+            const int m3b = two ? __ffs(vl) - 1 : m3a;
+            vl &= vl - 1u;
+            const int m4a = M - m3a, m4b = M - m3b;
+            const int ia = base + LR[anl | (1u << m3a) | (1u << m4a)];
+            const int ib = base + LR[anl | (1u << m3b) | (1u << m4b)];
+            TG fa = fp[m3a], fb = two ? fp[m3b] : TG(0);
+            if ((paa + __popc(anl & between32(m4a, m3a))) & 1) fa = -fa;
+            if ((paa + __popc(anl & between32(m4b, m3b))) & 1) fb = -fb;
+            accumulate2<TG, K, RANGE>(acc, x, a, ia, fa, ib, fb);
+          }
+        }
+        if (vh) {
+          const int base = (m2 >= LB) ? lr_row : LR[anl];
+          const TG* fph = fp + LB;
+          const int MH = M - 2 * LB;
+          while (vh) {
+            const int ha3 = __ffs(vh) - 1;
+            vh &= vh - 1u;
+            const bool two = vh != 0u;
+            const int hb3 = two ? __ffs(vh) - 1 : ha3;
+            vh &= vh - 1u;
+            const int ha4 = MH - ha3, hb4 = MH - hb3;
+            const int ia = base + __ldg(HO + (anh | (1u << ha3) | (1u << ha4)));
+            const int ib = base + __ldg(HO + (anh | (1u << hb3) | (1u << hb4)));
+            TG fa = fph[ha3], fb = two ? fph[hb3] : TG(0);
+            if ((paa + __popc(anh & between32(ha4, ha3))) & 1) fa = -fa;
+            if ((paa + __popc(anh & between32(hb4, hb3))) & 1) fb = -fb;
+            accumulate2<TG, K, RANGE>(acc, x, a, ia, fa, ib, fb);
+          }
+        }
+        if (vm) {
+          // m4 < LB <= m3: the orbitals between them are the low ones above m4 and the high ones below m3
+          const TG* fph = fp + LB;
+          const int ML = M - LB;
+          while (vm) {
+            const int ha3 = __ffs(vm) - 1;
+            vm &= vm - 1u;
+            const bool two = vm != 0u;
+            const int hb3 = two ? __ffs(vm) - 1 : ha3;
+            vm &= vm - 1u;
+            const int m4a = ML - ha3, m4b = ML - hb3;
+            const int ia = __ldg(HO + (anh | (1u << ha3))) + LR[anl | (1u << m4a)];
+            const int ib = __ldg(HO + (anh | (1u << hb3))) + LR[anl | (1u << m4b)];
+            TG fa = fph[ha3], fb = two ? fph[hb3] : TG(0);
+            const int pa = __popc(anl & between32(m4a, LB)) + __popc(anh & ((1u << ha3) - 1u));
+            const int pb = __popc(anl & between32(m4b, LB)) + __popc(anh & ((1u << hb3) - 1u));
+            if ((paa + pa) & 1) fa = -fa;
+            if ((paa + pb) & 1) fb = -fb;
+            accumulate2<TG, K, RANGE>(acc, x, a, ia, fa, ib, fb);
+          }
+        }
+      }
+    }
+    if (!RANGE || (r >= a.col_first && r < a.col_last)) {
+      const TG* xr = x + r * a.ld;
+#pragma unroll
+      for (int j = 0; j < K; ++j) acc[j] += dsum * xr[j * a.vstride];
+    }
+    const bool diag = (r >= a.row_first && r < a.row_last);
+    double* y = static_cast<double*>(a.y);
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      double v = (double)acc[j];
+      if (diag && a.shift != 0.0) {
+        double xd = a.xdiag ? a.xdiag[r * a.ld + j * a.vstride] : (double)x[r * a.ld + j * a.vstride];
+        v += a.shift * xd;
+      }
+      double* yp = y + r * a.ld_y + j * a.vstride_y;
+      *yp = a.accumulate ? (*yp + v) : v;
+    }
+  }
+}
+
 template <typename TG, int K, int MODE, bool RANGE>
 int launch_one(const FqheDevice& f, const MatvecArgs& a, cudaStream_t s) {
   SmemLayout lay = smem_layout(f, sizeof(TG));
   auto kern = fqhe_matvec_kernel<TG, K, MODE, RANGE>;
+  // the split-word form needs both halves of a word in 32 bits; variant 2 stages the low-rank table
+  // in shared memory
+  if (MODE == DH_INDEX_RANK && f.kernel_variant != 1 && f.low_bits <= 31 && f.lz_max + 1 - f.low_bits <= 31)
+    kern = (f.kernel_variant == 2) ? fqhe_split_kernel<TG, K, RANGE, true> : fqhe_split_kernel<TG, K, RANGE, false>;
   if (lay.total > 48 * 1024) DH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total));
   int dev = 0, sms = 0, per_sm = 0;
   DH_CUDA(cudaGetDevice(&dev));

@@ -11,7 +11,23 @@ from conftest import GOLDEN, golden, parse_sector
 
 pytestmark = pytest.mark.gpu
 
-MODES = ["rank", "lookup"]
+MODES = ["rank", "lookup", "rank-generic", "rank-smem"]
+
+
+def make_space(gpu, n, lz, s, mode):
+    """A FermionOnSphere in one of the index modes; rank-generic is the rank mode on the generic
+    (non split-word) product kernel."""
+    import os
+    if mode in ("rank-generic", "rank-smem"):
+        os.environ["DH_FQHE_KERNEL"] = mode.split("-")[1]
+        try:
+            sp = gpu.FermionOnSphere(n, lz, s)
+        finally:
+            del os.environ["DH_FQHE_KERNEL"]
+        return sp
+    sp = gpu.FermionOnSphere(n, lz, s)
+    sp.set_index_mode(mode)
+    return sp
 
 
 @pytest.mark.parametrize("name", sorted(os.path.basename(f) for f in glob.glob(os.path.join(GOLDEN, "fqhe_basis_*.npz"))))
@@ -25,8 +41,7 @@ def test_basis_words_bit_exact(gpu, name):
 
 @pytest.mark.parametrize("mode", MODES)
 def test_find_state_index(gpu, orc, mode):
-    sp = gpu.FermionOnSphere(8, 0, 21)
-    sp.set_index_mode(mode)
+    sp = make_space(gpu, 8, 0, 21, mode)
     words, _ = sp.states()
     assert np.array_equal(sp.FindStateIndex(words), np.arange(len(words)))
     # words outside the sector are reported as -1
@@ -41,8 +56,7 @@ def test_find_state_index(gpu, orc, mode):
 def test_row_elements_bit_exact(gpu, name, mode):
     z = golden(name)
     n, s, lz = parse_sector(name)
-    sp = gpu.FermionOnSphere(n, lz, s)
-    sp.set_index_mode(mode)
+    sp = make_space(gpu, n, lz, s, mode)
     H = gpu.ParticleOnSphereGenericHamiltonian(sp, n, s, z["v"])
     for k, r in enumerate(z["rows"]):
         a, b = z["offsets"][k], z["offsets"][k + 1]
@@ -68,8 +82,7 @@ def test_interaction_factors(gpu, name):
 def test_matvec_fp64_vs_reference(gpu, orc, tag, shift, mode):
     z = golden("matvec_%s_shift%g.npz" % (tag, shift))
     n, s, lz = parse_sector(tag)
-    sp = gpu.FermionOnSphere(n, lz, s)
-    sp.set_index_mode(mode)
+    sp = make_space(gpu, n, lz, s, mode)
     H = gpu.ParticleOnSphereGenericHamiltonian(sp, n, s, z["v"])
     H.ShiftHamiltonian(shift)
     x = orc.random_vector(0, sp.dim)
@@ -77,9 +90,10 @@ def test_matvec_fp64_vs_reference(gpu, orc, tag, shift, mode):
     assert np.max(np.abs(y - z["y"])) <= 1e-12 * max(1.0, np.max(np.abs(z["y"])))
 
 
-def test_matvec_fp32_vs_fp64(gpu, orc):
+@pytest.mark.parametrize("mode", MODES)
+def test_matvec_fp32_vs_fp64(gpu, orc, mode):
     z = golden("matvec_n8_2s21_lz0_coulomb_shift0.37.npz")
-    sp = gpu.FermionOnSphere(8, 0, 21)
+    sp = make_space(gpu, 8, 0, 21, mode)
     H = gpu.ParticleOnSphereGenericHamiltonian(sp, 8, 21, z["v"])
     H.ShiftHamiltonian(0.37)
     H.set_precision("fp32")
@@ -87,13 +101,14 @@ def test_matvec_fp32_vs_fp64(gpu, orc):
     assert np.max(np.abs(y - z["y"])) <= 2e-6 * np.max(np.abs(z["y"]))
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("first,nbr", [(0, 100), (1234, 3000), (8000, 512), (4000, -1)])
-def test_low_level_add_multiply_column_range(gpu, orc, first, nbr):
+def test_low_level_add_multiply_column_range(gpu, orc, first, nbr, mode):
     # push-form contract: dst += H[:, first:first+nbr] src[first:first+nbr], dst accumulated
     z = golden("factors_2s21_v1.npz")
     v = golden("matvec_n8_2s21_lz0_coulomb_shift0.npz")["v"]
     O = orc.FQHE(8, 21, 0, v, shift=0.25)
-    sp = gpu.FermionOnSphere(8, 0, 21)
+    sp = make_space(gpu, 8, 0, 21, mode)
     H = gpu.ParticleOnSphereGenericHamiltonian(sp, 8, 21, v)
     H.ShiftHamiltonian(0.25)
     x = orc.random_vector(1, sp.dim)
@@ -106,9 +121,10 @@ def test_low_level_add_multiply_column_range(gpu, orc, first, nbr):
     del z
 
 
-def test_multiple_add_multiply(gpu, orc):
+@pytest.mark.parametrize("mode", MODES)
+def test_multiple_add_multiply(gpu, orc, mode):
     v = golden("matvec_n8_2s21_lz0_coulomb_shift0.npz")["v"]
-    sp = gpu.FermionOnSphere(8, 0, 21)
+    sp = make_space(gpu, 8, 0, 21, mode)
     H = gpu.ParticleOnSphereGenericHamiltonian(sp, 8, 21, v)
     for k in (1, 2, 3, 4, 7):
         xs = np.stack([orc.random_vector(10 + j, sp.dim) for j in range(k)])
@@ -141,8 +157,7 @@ def test_matrix_element_and_device_pointers(gpu, orc):
 def test_precision_workload_symmetry_and_rows(gpu, orc, mode):
     """N = 12, 2S = 33, Lz = 0 (dimension 7,764,392): size-independent properties of the product."""
     z = golden("rows_n12_2s33_lz0_coulomb.npz")
-    sp = gpu.FermionOnSphere(12, 0, 33)
-    sp.set_index_mode(mode)
+    sp = make_space(gpu, 12, 0, 33, mode)
     assert sp.dim == 7764392
     H = gpu.ParticleOnSphereGenericHamiltonian(sp, 12, 33, z["v"])
     x, y = orc.random_vector(5, sp.dim), orc.random_vector(6, sp.dim)
