@@ -61,6 +61,7 @@ SIGNATURES = {
     "dh_hamiltonian_row_elements": ([_vp, _c_i64, _vp, _vp, _vp, _c_int, _ip], _c_int),
     "dh_hamiltonian_pseudopotential_adjoint": ([_vp, _vp, _vp, _vp], _c_int),
     "dh_hamiltonian_get_interaction_factors": ([_vp, _vp, _c_int, _ip], _c_int),
+    "dh_hamiltonian_pseudopotential_adjoint_static": ([_vp, _vp, _vp, _vp], _c_int),
     "dh_hamiltonian_count_elements": ([_vp, _i64p], _c_int),
     "dh_lanczos_create": ([_vp, _c_int, _c_int, _c_int, _c_int, _vp], _c_int),
     "dh_lanczos_destroy": ([_vp], _c_int),
@@ -316,6 +317,15 @@ class ParticleOnSphereGenericHamiltonian(_Hamiltonian):
         a, b = _Buf(u), _Buf(v)
         out = np.zeros(self.lz_max + 1, np.float64)
         _check(_lib.dh_hamiltonian_pseudopotential_adjoint(self._handle, a.ptr, b.ptr, out.ctypes.data))
+        return out
+
+
+    def pseudopotential_adjoint_static(self, u, v):
+        """pseudopotential_adjoint without any device allocation (u, v must be CUDA tensors); its
+        scratch is a static device array shared by all calls, so concurrent calls race."""
+        a, b = _Buf(u), _Buf(v)
+        out = np.zeros(self.lz_max + 1, np.float64)
+        _check(_lib.dh_hamiltonian_pseudopotential_adjoint_static(self._handle, a.ptr, b.ptr, out.ctypes.data))
         return out
 
 
