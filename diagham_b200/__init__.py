@@ -77,6 +77,8 @@ SIGNATURES = {
     "dh_lanczos_get_counters": ([_vp, _i64p, _ip], _c_int),
     "dh_lanczos_solve": ([_vp, _c_int, _c_int, _vp, _ip, _ip], _c_int),
     "dh_lanczos_solve_refined": ([_vp, _c_int, _c_dbl, _vp], _c_int),
+    "dh_fqhe_sectors_block_lanczos": ([_c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _c_dbl, _c_int, _c_int,
+                                       _c_u64, _vp, _vp, _vp], _c_int),
     "dh_coulomb_pseudopotentials": ([_c_int, _vp], _c_int),
     "dh_clebsch_gordan": ([_c_int, _c_int, _c_int, _c_int, _c_int, _vp], _c_int),
 }
@@ -447,3 +449,22 @@ def clebsch_gordan(j1, m1, j2, m2, j):
     out = ctypes.c_double(0.0)
     _check(_lib.dh_clebsch_gordan(j1, m1, j2, m2, j, ctypes.byref(out)))
     return out.value
+
+
+def fqhe_sectors_block_lanczos(nbr_fermions, lz_max, total_lz, pseudopotentials, block_size=4, max_iter=400,
+                               precision=1e-14, fp32=False, full_diag_limit=200, seed=100):
+    """Lowest energy of every requested Lz sector: block Lanczos over all sectors in lockstep, one
+    launch per block product (BasicBlockLanczosAlgorithm + QHEOnSphereMainTask's loop per sector)."""
+    load()
+    tl = np.ascontiguousarray(total_lz, np.int32)
+    v = np.ascontiguousarray(pseudopotentials, np.float64)
+    ns = tl.size
+    e = np.zeros(ns, np.float64)
+    it = np.zeros(ns, np.int32)
+    secs = np.zeros(4, np.float64)
+    _check(_lib.dh_fqhe_sectors_block_lanczos(nbr_fermions, lz_max, tl.ctypes.data, ns, v.ctypes.data, block_size,
+                                              max_iter, float(precision),
+                                              DH_PRECISION_FP32 if fp32 else DH_PRECISION_FP64, full_diag_limit, seed,
+                                              e.ctypes.data, it.ctypes.data, secs.ctypes.data))
+    return dict(energies=e, iterations=it, setup_seconds=secs[0], solve_seconds=secs[1], product_seconds=secs[2],
+                block_products=int(secs[3]))

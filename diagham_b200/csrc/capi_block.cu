@@ -1,0 +1,554 @@
+// Block Lanczos on the GPU, for one Hamiltonian or for all Lz sectors of a system in lockstep.
+//
+// Recurrence (the block form of BasicBlockLanczosAlgorithm.cc:524-697, k = block size):
+//     W = H V_i;  A_i = V_i^T W;  W -= V_i A_i + V_{i-1} B_i^T;  W = V_{i+1} B_{i+1}  (QR)
+// with every block stored k-interleaved ([row][k], FP64) so that one product enumerates each row's
+// elements once for the k vectors.  The QR is CholQR2 (Gram matrix, Cholesky, triangular solve,
+// twice), the role of ReorthogonalizeVectors (:771-799).  The band matrix of the A_i and B_i is
+// diagonalised on the host after every step (band -> tridiagonal -> QL, the reference's
+// RealBandDiagonalSymmetricMatrix::Tridiagonalize + Diagonalize), and each sector follows the
+// reference's convergence bookkeeping (:683-697, TestConvergence :731).  A sector whose block
+// Krylov space is exhausted (Cholesky breakdown) is exact and stops; sectors of dimension at most
+// full_diag_limit are diagonalised densely, as QHEOnSphereMainTask does below --full-diag (:397).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <functional>
+#include <new>
+#include <thread>
+#include <vector>
+
+#include "dh_internal.h"
+#include "dh_objects.h"
+
+using namespace dh;
+
+namespace dh {
+
+constexpr long long kTileRows = 4096;
+
+struct BlockSector {
+  long long dim = 0;
+  bool active = true;     // still iterating
+  bool converged = false;
+  bool exhausted = false; // Krylov space exhausted: the band matrix is exact
+  int blocks = 0;         // A blocks recorded
+  std::vector<double> A, B;  // A_j (k x k) for j < blocks, B_j (k x k) for 1 <= j <= blocks (B[0] unused)
+  double prev_last = 0.0;
+  std::vector<double> ritz;
+  int count = 0;          // the reference driver's iteration counter (in vectors)
+  int steps = 0;
+};
+
+struct BlockEngine {
+  int k = 4, nsec = 0, nev = 1, precision = DH_PRECISION_FP64;
+  double eig_precision = 1e-14;
+  int max_iter = 400;  // in vectors, as the reference's --iter-max
+  long long total = 0;
+  std::vector<long long> off;
+  cudaStream_t stream = 0;
+  DevBuf tiles_buf, vec, x32, partial, small, offs_dev;
+  TileSetDevice tiles = {};
+  const long long* row_offset_dev = nullptr;  // [nsec + 1] concatenated row offsets on the device
+  int slot_cur = 0;
+  double* slot[3] = {nullptr, nullptr, nullptr};
+  bool have_prev = false;
+  std::vector<BlockSector> sec;
+  std::vector<double> bt_host;  // B_i^T of every sector for the next update
+  std::function<int(const double*, const float*, double*)> product;
+  double product_ms = 0.0;
+  long long products = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  ~BlockEngine() {
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+  }
+};
+
+namespace {
+
+int engine_setup(BlockEngine& e, const std::vector<long long>& dims) {
+  e.nsec = (int)dims.size();
+  e.off.assign(e.nsec + 1, 0);
+  e.sec.assign(e.nsec, BlockSector());
+  for (int s = 0; s < e.nsec; ++s) {
+    e.off[s + 1] = e.off[s] + dims[s];
+    e.sec[s].dim = dims[s];
+  }
+  e.total = e.off[e.nsec];
+  std::vector<int> tsec, first(e.nsec + 1, 0);
+  std::vector<long long> tb, te;
+  for (int s = 0; s < e.nsec; ++s) {
+    first[s] = (int)tsec.size();
+    for (long long r = e.off[s]; r < e.off[s + 1]; r += kTileRows) {
+      tsec.push_back(s);
+      tb.push_back(r);
+      te.push_back(std::min(r + kTileRows, e.off[s + 1]));
+    }
+  }
+  first[e.nsec] = (int)tsec.size();
+  const int nt = (int)tsec.size();
+  const size_t bytes = nt * (sizeof(int) + 2 * sizeof(long long)) + (e.nsec + 1) * (sizeof(int) + sizeof(long long)) + 64;
+  int rc;
+  if ((rc = e.tiles_buf.alloc(bytes)) != DH_OK) return rc;
+  char* p = e.tiles_buf.as<char>();
+  long long* d_tb = reinterpret_cast<long long*>(p);
+  long long* d_te = d_tb + nt;
+  long long* d_off = d_te + nt;
+  int* d_ts = reinterpret_cast<int*>(d_off + e.nsec + 1);
+  int* d_first = d_ts + nt;
+  DH_CUDA(cudaMemcpy(d_tb, tb.data(), nt * sizeof(long long), cudaMemcpyHostToDevice));
+  DH_CUDA(cudaMemcpy(d_te, te.data(), nt * sizeof(long long), cudaMemcpyHostToDevice));
+  DH_CUDA(cudaMemcpy(d_off, e.off.data(), (e.nsec + 1) * sizeof(long long), cudaMemcpyHostToDevice));
+  DH_CUDA(cudaMemcpy(d_ts, tsec.data(), nt * sizeof(int), cudaMemcpyHostToDevice));
+  DH_CUDA(cudaMemcpy(d_first, first.data(), (e.nsec + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  e.tiles.tile_sector = d_ts;
+  e.tiles.tile_begin = d_tb;
+  e.tiles.tile_end = d_te;
+  e.tiles.sector_tile_first = d_first;
+  e.tiles.nbr_tiles = nt;
+  e.tiles.nbr_sectors = e.nsec;
+  e.row_offset_dev = d_off;
+  const size_t vb = (size_t)e.total * e.k * sizeof(double);
+  if ((rc = e.vec.alloc(3 * vb)) != DH_OK) return rc;
+  if (e.precision == DH_PRECISION_FP32 && (rc = e.x32.alloc((size_t)e.total * e.k * sizeof(float))) != DH_OK) return rc;
+  if ((rc = e.partial.alloc((size_t)std::max(nt, 1) * e.k * e.k * sizeof(double))) != DH_OK) return rc;
+  if ((rc = e.small.alloc((size_t)e.nsec * e.k * e.k * 4 * sizeof(double) + 64)) != DH_OK) return rc;
+  DH_CUDA(cudaMemset(e.vec.ptr, 0, 3 * vb));
+  for (int q = 0; q < 3; ++q) e.slot[q] = e.vec.as<double>() + (size_t)q * e.total * e.k;
+  e.bt_host.assign((size_t)e.nsec * e.k * e.k, 0.0);
+  if (!e.ev0) {
+    DH_CUDA(cudaEventCreate(&e.ev0));
+    DH_CUDA(cudaEventCreate(&e.ev1));
+  }
+  return DH_OK;
+}
+
+// G[s] = X_s^T Y_s for every sector, copied to the host
+int engine_gram(BlockEngine& e, const double* x, const double* y, std::vector<double>& g) {
+  const int kk = e.k * e.k;
+  double* dg = e.small.as<double>();
+  int rc = launch_seg_gram(x, y, e.k, e.tiles, e.partial.as<double>(), dg, e.stream);
+  if (rc != DH_OK) return rc;
+  g.resize((size_t)e.nsec * kk);
+  DH_CUDA(cudaMemcpyAsync(g.data(), dg, g.size() * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+  DH_CUDA(cudaStreamSynchronize(e.stream));
+  return DH_OK;
+}
+
+// Cholesky G = R^T R (R upper); returns false on breakdown.  Rinv = R^{-1} (upper).
+bool cholesky_inverse(int k, const double* G, double* R, double* Rinv) {
+  double trace = 0.0;
+  for (int i = 0; i < k; ++i) trace += fabs(G[i * k + i]);
+  for (int i = 0; i < k * k; ++i) R[i] = Rinv[i] = 0.0;
+  for (int j = 0; j < k; ++j) {
+    double d = G[j * k + j];
+    for (int p = 0; p < j; ++p) d -= R[p * k + j] * R[p * k + j];
+    if (!(d > 1e-26 * std::max(trace, 1e-300))) return false;
+    const double rjj = sqrt(d);
+    R[j * k + j] = rjj;
+    for (int c = j + 1; c < k; ++c) {
+      double v = 0.5 * (G[j * k + c] + G[c * k + j]);
+      for (int p = 0; p < j; ++p) v -= R[p * k + j] * R[p * k + c];
+      R[j * k + c] = v / rjj;
+    }
+  }
+  for (int c = 0; c < k; ++c) {  // R Rinv = I, column by column (back substitution)
+    for (int i = c; i >= 0; --i) {
+      double v = (i == c) ? 1.0 : 0.0;
+      for (int p = i + 1; p <= c; ++p) v -= R[i * k + p] * Rinv[p * k + c];
+      Rinv[i * k + c] = v / R[i * k + i];
+    }
+  }
+  return true;
+}
+
+// X = X Q with X = V B (CholQR2): writes B (k x k per sector, upper) and leaves X orthonormal.
+// A sector whose block is numerically zero against its scale (|X|_F^2 < 1e-24 scale[s], scale =
+// |A|^2 + |B|^2 of the step: the block Krylov space is complete) or whose Gram matrix breaks down
+// gets a zero block and is marked exhausted.
+int engine_qr(BlockEngine& e, double* x, std::vector<double>& B, float* x32, const std::vector<double>* scale) {
+  const int k = e.k, kk = k * k;
+  std::vector<double> g, R1((size_t)e.nsec * kk), R2((size_t)e.nsec * kk), inv((size_t)e.nsec * kk);
+  std::vector<char> broke(e.nsec, 0);
+  double* dM = e.small.as<double>() + (size_t)e.nsec * kk;
+  int rc;
+  for (int pass = 0; pass < 2; ++pass) {
+    if ((rc = engine_gram(e, x, x, g)) != DH_OK) return rc;
+    std::vector<double>& R = pass ? R2 : R1;
+    if (pass == 0 && scale)
+      for (int s = 0; s < e.nsec; ++s) {
+        double tr = 0.0;
+        for (int i = 0; i < k; ++i) tr += g[(size_t)s * kk + i * k + i];
+        if (!(tr > 1e-24 * (*scale)[s])) broke[s] = 1;
+      }
+    for (int s = 0; s < e.nsec; ++s) {
+      if (broke[s] || !cholesky_inverse(k, &g[(size_t)s * kk], &R[(size_t)s * kk], &inv[(size_t)s * kk])) {
+        broke[s] = 1;
+        std::fill(&R[(size_t)s * kk], &R[(size_t)s * kk] + kk, 0.0);
+        std::fill(&inv[(size_t)s * kk], &inv[(size_t)s * kk] + kk, 0.0);
+      }
+    }
+    DH_CUDA(cudaMemcpyAsync(dM, inv.data(), inv.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+    if ((rc = launch_seg_rmul(x, dM, k, e.tiles, pass ? x32 : nullptr, e.stream)) != DH_OK) return rc;
+  }
+  B.assign((size_t)e.nsec * kk, 0.0);
+  for (int s = 0; s < e.nsec; ++s) {
+    if (broke[s]) {
+      e.sec[s].exhausted = true;
+      continue;
+    }
+    const double* a = &R2[(size_t)s * kk];
+    const double* b = &R1[(size_t)s * kk];
+    for (int i = 0; i < k; ++i)
+      for (int j = 0; j < k; ++j) {
+        double v = 0.0;
+        for (int p = 0; p < k; ++p) v += a[i * k + p] * b[p * k + j];
+        B[(size_t)s * kk + i * k + j] = v;
+      }
+  }
+  return DH_OK;
+}
+
+int engine_product(BlockEngine& e, const double* x, double* y) {
+  const float* x32 = e.precision == DH_PRECISION_FP32 ? e.x32.as<float>() : nullptr;
+  DH_CUDA(cudaEventRecord(e.ev0, e.stream));
+  int rc = e.product(x, x32, y);
+  if (rc != DH_OK) return rc;
+  DH_CUDA(cudaEventRecord(e.ev1, e.stream));
+  DH_CUDA(cudaEventSynchronize(e.ev1));
+  float ms = 0.0f;
+  DH_CUDA(cudaEventElapsedTime(&ms, e.ev0, e.ev1));
+  e.product_ms += ms;
+  ++e.products;
+  return DH_OK;
+}
+
+// orthonormalise the start block (slot 0) and prepare its FP32 copy
+int engine_start(BlockEngine& e) {
+  std::vector<double> B;
+  e.slot_cur = 0;
+  e.have_prev = false;
+  int rc = engine_qr(e, e.slot[0], B, e.x32.as<float>(), nullptr);
+  if (rc != DH_OK) return rc;
+  for (int s = 0; s < e.nsec; ++s) {
+    BlockSector& b = e.sec[s];
+    b.blocks = 0;
+    b.steps = 0;
+    b.A.clear();
+    b.B.assign((size_t)e.k * e.k, 0.0);
+    b.prev_last = 0.0;
+    b.ritz.clear();
+    b.converged = false;
+    b.active = !b.exhausted;
+  }
+  return DH_OK;
+}
+
+// one block step for every sector (results recorded for the active ones)
+int engine_step(BlockEngine& e) {
+  const int k = e.k, kk = k * k;
+  double* V = e.slot[e.slot_cur];
+  double* W = e.slot[(e.slot_cur + 1) % 3];
+  double* Vp = e.slot[(e.slot_cur + 2) % 3];
+  int rc;
+  if ((rc = engine_product(e, V, W)) != DH_OK) return rc;
+  std::vector<double> A;
+  if ((rc = engine_gram(e, V, W, A)) != DH_OK) return rc;
+  for (int s = 0; s < e.nsec; ++s)
+    for (int i = 0; i < k; ++i)
+      for (int j = i + 1; j < k; ++j) {
+        const double m = 0.5 * (A[(size_t)s * kk + i * k + j] + A[(size_t)s * kk + j * k + i]);
+        A[(size_t)s * kk + i * k + j] = A[(size_t)s * kk + j * k + i] = m;
+      }
+  double* dA = e.small.as<double>() + 2 * (size_t)e.nsec * kk;
+  double* dBt = dA + (size_t)e.nsec * kk;
+  DH_CUDA(cudaMemcpyAsync(dA, A.data(), A.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+  DH_CUDA(cudaMemcpyAsync(dBt, e.bt_host.data(), e.bt_host.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+  if ((rc = launch_seg_update(W, V, dA, e.have_prev ? Vp : nullptr, e.have_prev ? dBt : nullptr, k, e.tiles, e.stream)) !=
+      DH_OK)
+    return rc;
+  std::vector<double> B, scale(e.nsec, 0.0);
+  std::vector<char> was_exhausted(e.nsec);
+  for (int s = 0; s < e.nsec; ++s) {
+    was_exhausted[s] = e.sec[s].exhausted;
+    for (int i = 0; i < kk; ++i)
+      scale[s] += A[(size_t)s * kk + i] * A[(size_t)s * kk + i] + e.bt_host[(size_t)s * kk + i] * e.bt_host[(size_t)s * kk + i];
+  }
+  if ((rc = engine_qr(e, W, B, e.x32.as<float>(), &scale)) != DH_OK) return rc;
+  for (int s = 0; s < e.nsec; ++s) {
+    BlockSector& b = e.sec[s];
+    if (!b.active) continue;
+    b.A.insert(b.A.end(), A.begin() + (size_t)s * kk, A.begin() + (size_t)(s + 1) * kk);
+    b.B.insert(b.B.end(), B.begin() + (size_t)s * kk, B.begin() + (size_t)(s + 1) * kk);
+    ++b.blocks;
+    ++b.steps;
+    if (b.exhausted && !was_exhausted[s]) b.converged = true;  // exact: the Krylov space is complete
+  }
+  for (int s = 0; s < e.nsec; ++s)
+    for (int i = 0; i < k; ++i)
+      for (int j = 0; j < k; ++j) e.bt_host[(size_t)s * kk + i * k + j] = B[(size_t)s * kk + j * k + i];
+  e.have_prev = true;
+  e.slot_cur = (e.slot_cur + 1) % 3;
+  return DH_OK;
+}
+
+// eigenvalues of the band matrix of sector s (blocks A_0..A_{m-1}, B_1..B_{m-1})
+int sector_eigenvalues(const BlockEngine& e, const BlockSector& b, std::vector<double>& eig) {
+  const int k = e.k, kk = k * k, m = b.blocks, n = m * k;
+  std::vector<double> t((size_t)n * n, 0.0);
+  for (int j = 0; j < m; ++j) {
+    for (int p = 0; p < k; ++p)
+      for (int q = 0; q < k; ++q) t[(size_t)(j * k + p) * n + j * k + q] = b.A[(size_t)j * kk + p * k + q];
+    if (j + 1 < m)
+      for (int p = 0; p < k; ++p)
+        for (int q = 0; q < k; ++q) {
+          const double v = b.B[(size_t)(j + 1) * kk + p * k + q];
+          t[(size_t)((j + 1) * k + p) * n + j * k + q] = v;
+          t[(size_t)(j * k + q) * n + (j + 1) * k + p] = v;
+        }
+  }
+  eig.assign(n, 0.0);
+  return band_eigenvalues(n, std::max(1, 2 * k - 1), t.data(), eig.data());
+}
+
+// the reference's per-call bookkeeping (BasicBlockLanczosAlgorithm.cc:683-697) and TestConvergence
+// (:731): first evaluation sets previous = 2 * lambda, later ones the previous lambda
+int sector_evaluate(const BlockEngine& e, BlockSector& b) {
+  std::vector<double> eig;
+  int rc = sector_eigenvalues(e, b, eig);
+  if (rc != DH_OK) return rc;
+  const int nev = std::min(e.nev, (int)eig.size());
+  if (b.prev_last != 0.0 && !b.ritz.empty())
+    b.prev_last = b.ritz[std::min(nev, (int)b.ritz.size()) - 1];
+  else
+    b.prev_last = 2.0 * eig[nev - 1];
+  b.ritz.swap(eig);
+  if ((int)b.ritz.size() > e.nev) {
+    const double l = b.ritz[e.nev - 1];
+    if (fabs(l - b.prev_last) < e.eig_precision * fabs(l)) b.converged = true;
+  }
+  return DH_OK;
+}
+
+// run every active sector until converged, exhausted or at the iteration limit; the driver loop of
+// QHEOnSphereMainTask.cc:732-753 per sector (first call nev + 2 block steps, counter (nev + 3) k)
+int engine_solve(BlockEngine& e) {
+  const int first = e.nev + 2;
+  for (;;) {
+    bool any = false;
+    for (auto& b : e.sec) any |= b.active;
+    if (!any) break;
+    int rc = engine_step(e);
+    if (rc != DH_OK) return rc;
+    std::vector<int> eval;
+    for (int s = 0; s < e.nsec; ++s) {
+      BlockSector& b = e.sec[s];
+      if (!b.active) continue;
+      if (b.steps == first) {
+        b.count = (e.nev + 3) * e.k;
+        eval.push_back(s);
+      } else if (b.steps > first || b.exhausted) {
+        b.count += e.k;
+        eval.push_back(s);
+      }
+    }
+    // band eigenvalues of the sectors due, spread over host threads
+    std::vector<int> status(eval.size(), DH_OK);
+    const int nthreads = std::max(1, std::min((int)eval.size(), (int)std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthreads; ++t)
+      pool.emplace_back([&, t] {
+        for (size_t i = t; i < eval.size(); i += nthreads) status[i] = sector_evaluate(e, e.sec[eval[i]]);
+      });
+    for (auto& th : pool) th.join();
+    for (size_t i = 0; i < eval.size(); ++i) {
+      if (status[i] != DH_OK) return status[i];
+      BlockSector& b = e.sec[eval[i]];
+      if (b.converged || b.exhausted || b.count >= e.max_iter) b.active = false;
+    }
+  }
+  return DH_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ batched FQHE sectors
+
+struct SectorBatchHost {
+  std::vector<dh_space_s*> spaces;
+  DevBuf ptrs;  // words and HO pointer arrays + row offsets
+  DevBuf pair_offset, f64, f32;
+  InteractionTables tabs;
+  ~SectorBatchHost() {
+    for (auto* s : spaces) delete s;
+  }
+};
+
+int dense_lowest(dh_space_s* sp, const SectorBatchHost& hb, int nev, std::vector<double>& out, cudaStream_t stream) {
+  // H on the unit vectors, four columns per launch (one-sector batch, k = 4, FP64), then a dense
+  // symmetric eigensolve on the host
+  const long long d = sp->dim;
+  const int k = 4;
+  DevBuf x, y, ptrs;
+  int rc;
+  if ((rc = x.alloc((size_t)d * k * sizeof(double))) != DH_OK || (rc = y.alloc((size_t)d * k * sizeof(double))) != DH_OK ||
+      (rc = ptrs.alloc(2 * sizeof(void*) + 2 * sizeof(long long))) != DH_OK)
+    return rc;
+  const void* hp[2] = {sp->words.ptr, sp->high_offset.ptr};
+  long long ho[2] = {0, d};
+  DH_CUDA(cudaMemcpy(ptrs.ptr, hp, 2 * sizeof(void*), cudaMemcpyHostToDevice));
+  DH_CUDA(cudaMemcpy(ptrs.as<char>() + 2 * sizeof(void*), ho, 2 * sizeof(long long), cudaMemcpyHostToDevice));
+  SectorBatchDevice b = {};
+  b.words = reinterpret_cast<const uint64_t* const*>(ptrs.ptr);
+  b.high_offset = reinterpret_cast<const int32_t* const*>(ptrs.as<char>() + sizeof(void*));
+  b.row_offset = reinterpret_cast<const long long*>(ptrs.as<char>() + 2 * sizeof(void*));
+  b.low_rank = sp->low_rank.as<uint16_t>();
+  b.pair_offset = hb.pair_offset.as<int32_t>();
+  b.factors = hb.f64.ptr;
+  b.x = x.ptr;
+  b.y = y.as<double>();
+  b.total_rows = d;
+  b.nbr_sectors = 1;
+  b.block = k;
+  b.lz_max = sp->lz_max;
+  b.low_bits = sp->rank.low_bits;
+  b.nbr_pairs = hb.tabs.nbr_pairs;
+  b.nbr_factors = hb.tabs.nbr_factors;
+  std::vector<double> H((size_t)d * d), xin((size_t)d * k), yout((size_t)d * k);
+  for (long long c0 = 0; c0 < d; c0 += k) {
+    std::fill(xin.begin(), xin.end(), 0.0);
+    for (int j = 0; j < k && c0 + j < d; ++j) xin[(size_t)(c0 + j) * k + j] = 1.0;
+    DH_CUDA(cudaMemcpyAsync(x.ptr, xin.data(), xin.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+    if ((rc = launch_fqhe_sectors(b, DH_PRECISION_FP64, stream)) != DH_OK) return rc;
+    DH_CUDA(cudaMemcpyAsync(yout.data(), y.ptr, yout.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    DH_CUDA(cudaStreamSynchronize(stream));
+    for (int j = 0; j < k && c0 + j < d; ++j)
+      for (long long r = 0; r < d; ++r) H[(size_t)r * d + c0 + j] = yout[(size_t)r * k + j];
+  }
+  out.assign(d, 0.0);
+  rc = symmetric_eigen((int)d, H.data(), out.data(), nullptr);
+  out.resize(std::min<long long>(d, std::max(nev, 1)));
+  return rc;
+}
+
+}  // namespace dh
+
+extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const int* total_lz, int nbr_sectors,
+                                             const double* pseudopotentials, int block_size, int max_iter,
+                                             double precision_target, int precision, int full_diag_limit,
+                                             uint64_t seed, double* energies, int* iterations, double* seconds) {
+  using clk = std::chrono::steady_clock;
+  const auto t0 = clk::now();
+  DH_CHECK(total_lz && pseudopotentials && energies && iterations && nbr_sectors >= 1, DH_ERR_ARGUMENT, "bad argument");
+  DH_CHECK(block_size == 1 || block_size == 2 || block_size == 4, DH_ERR_UNSUPPORTED, "block size must be 1, 2 or 4");
+  DH_CHECK(precision == DH_PRECISION_FP64 || precision == DH_PRECISION_FP32, DH_ERR_ARGUMENT, "unknown precision");
+  SectorBatchHost hb;
+  BlockEngine e;
+  e.k = block_size;
+  e.nev = 1;
+  e.precision = precision;
+  e.eig_precision = precision_target > 0.0 ? precision_target : 1e-14;
+  e.max_iter = max_iter;
+  int rc;
+  // spaces (each builds its words and rank tables on the device)
+  std::vector<int> lanczos_sectors, dense_sectors;
+  std::vector<long long> dims;
+  for (int s = 0; s < nbr_sectors; ++s) {
+    dh_space_t sp = nullptr;
+    rc = dh_fermion_on_sphere_create(nbr_fermions, total_lz[s], lz_max, 9ul << 20, &sp);
+    if (rc != DH_OK) return rc;
+    hb.spaces.push_back(sp);
+    DH_CHECK(sp->rank.low_bits == hb.spaces[0]->rank.low_bits, DH_ERR_STATE, "sectors disagree on the table split");
+    if (sp->dim <= full_diag_limit || sp->dim <= 2 * block_size)
+      dense_sectors.push_back(s);
+    else {
+      lanczos_sectors.push_back(s);
+      dims.push_back(sp->dim);
+    }
+  }
+  hb.tabs.build(lz_max);
+  std::vector<double> v(pseudopotentials, pseudopotentials + lz_max + 1);
+  hb.tabs.set_pseudopotentials(v.data());
+  std::vector<float> f32(hb.tabs.nbr_factors);
+  for (int i = 0; i < hb.tabs.nbr_factors; ++i) f32[i] = (float)hb.tabs.factors[i];
+  if ((rc = hb.pair_offset.alloc(hb.tabs.pair_offset.size() * sizeof(int32_t))) != DH_OK ||
+      (rc = hb.f64.alloc(hb.tabs.nbr_factors * sizeof(double))) != DH_OK ||
+      (rc = hb.f32.alloc(hb.tabs.nbr_factors * sizeof(float))) != DH_OK)
+    return rc;
+  DH_CUDA(cudaMemcpy(hb.pair_offset.ptr, hb.tabs.pair_offset.data(), hb.tabs.pair_offset.size() * sizeof(int32_t),
+                     cudaMemcpyHostToDevice));
+  DH_CUDA(cudaMemcpy(hb.f64.ptr, hb.tabs.factors.data(), hb.tabs.nbr_factors * sizeof(double), cudaMemcpyHostToDevice));
+  DH_CUDA(cudaMemcpy(hb.f32.ptr, f32.data(), hb.tabs.nbr_factors * sizeof(float), cudaMemcpyHostToDevice));
+  DH_CUDA(cudaStreamCreateWithFlags(&e.stream, cudaStreamNonBlocking));
+  struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() {
+      if (s) cudaStreamDestroy(s);
+    }
+  } guard{e.stream};
+  const auto t1 = clk::now();
+  // dense sectors
+  for (int s : dense_sectors) {
+    std::vector<double> ev;
+    if ((rc = dense_lowest(hb.spaces[s], hb, 1, ev, e.stream)) != DH_OK) return rc;
+    energies[s] = ev[0];
+    iterations[s] = 0;
+  }
+  if (!lanczos_sectors.empty()) {
+    if ((rc = engine_setup(e, dims)) != DH_OK) return rc;
+    // the one-launch product over every Lanczos sector
+    const int ns = (int)lanczos_sectors.size();
+    if ((rc = hb.ptrs.alloc(2 * ns * sizeof(void*))) != DH_OK) return rc;
+    std::vector<const void*> hp(2 * ns);
+    for (int i = 0; i < ns; ++i) {
+      hp[i] = hb.spaces[lanczos_sectors[i]]->words.ptr;
+      hp[ns + i] = hb.spaces[lanczos_sectors[i]]->high_offset.ptr;
+    }
+    DH_CUDA(cudaMemcpy(hb.ptrs.ptr, hp.data(), hp.size() * sizeof(void*), cudaMemcpyHostToDevice));
+    SectorBatchDevice b = {};
+    b.words = reinterpret_cast<const uint64_t* const*>(hb.ptrs.ptr);
+    b.high_offset = reinterpret_cast<const int32_t* const*>(hb.ptrs.as<char>() + ns * sizeof(void*));
+    b.row_offset = e.row_offset_dev;
+    b.low_rank = hb.spaces[lanczos_sectors[0]]->low_rank.as<uint16_t>();
+    b.pair_offset = hb.pair_offset.as<int32_t>();
+    b.factors = (precision == DH_PRECISION_FP32) ? hb.f32.ptr : hb.f64.ptr;
+    b.total_rows = e.total;
+    b.nbr_sectors = ns;
+    b.block = e.k;
+    b.lz_max = lz_max;
+    b.low_bits = hb.spaces[lanczos_sectors[0]]->rank.low_bits;
+    b.nbr_pairs = hb.tabs.nbr_pairs;
+    b.nbr_factors = hb.tabs.nbr_factors;
+    e.product = [b, &e](const double* x64, const float* x32, double* y) mutable {
+      b.x = x32 ? static_cast<const void*>(x32) : static_cast<const void*>(x64);
+      b.xdiag = x32 ? x64 : nullptr;
+      b.y = y;
+      return launch_fqhe_sectors(b, e.precision, e.stream);
+    };
+    // start block: splitmix64 vectors per sector (seed + j for vector j)
+    DevBuf base;
+    if ((rc = base.alloc(ns * sizeof(long long))) != DH_OK) return rc;
+    DH_CUDA(cudaMemcpy(base.ptr, e.off.data(), ns * sizeof(long long), cudaMemcpyHostToDevice));
+    if ((rc = launch_random_block(e.slot[0], e.total, e.k, base.as<long long>(), e.tiles, seed, e.stream)) != DH_OK)
+      return rc;
+    if ((rc = engine_start(e)) != DH_OK) return rc;
+    if ((rc = engine_solve(e)) != DH_OK) return rc;
+    for (int i = 0; i < ns; ++i) {
+      const BlockSector& bs = e.sec[i];
+      energies[lanczos_sectors[i]] = bs.ritz.empty() ? NAN : bs.ritz[0];
+      iterations[lanczos_sectors[i]] = bs.count;
+    }
+  }
+  const auto t2 = clk::now();
+  if (seconds) {
+    seconds[0] = std::chrono::duration<double>(t1 - t0).count();
+    seconds[1] = std::chrono::duration<double>(t2 - t1).count();
+    seconds[2] = e.product_ms / 1000.0;
+    seconds[3] = (double)e.products;
+  }
+  return DH_OK;
+}

@@ -109,6 +109,46 @@ struct MatvecArgs {
   int accumulate;                // y += H x (1) or y = H x (0)
 };
 
+// Every Lz sector of one system in one launch (rows concatenated, vectors K-interleaved).
+struct SectorBatchDevice {
+  const uint64_t* const* words;       // [nbr_sectors] device pointers (array in device memory)
+  const int32_t* const* high_offset;  // [nbr_sectors] device pointers (array in device memory)
+  const long long* row_offset;        // [nbr_sectors + 1] in device memory
+  const uint16_t* low_rank;           // shared: depends on the split only
+  const int32_t* pair_offset;
+  const void* factors;                // FP64 or FP32
+  const void* x;                      // [total_rows][block]
+  const double* xdiag;                // optional FP64 copy of x for the shift term
+  double* y;                          // [total_rows][block]
+  long long total_rows;
+  double shift;
+  int nbr_sectors, block, lz_max, low_bits, nbr_pairs, nbr_factors;
+};
+int launch_fqhe_sectors(const SectorBatchDevice& b, int precision, cudaStream_t s);
+
+// Tiles of the concatenated rows of several sectors (a tile never straddles two sectors).
+struct TileSetDevice {
+  const int* tile_sector;        // [nbr_tiles]
+  const long long* tile_begin;   // [nbr_tiles] first concatenated row
+  const long long* tile_end;     // [nbr_tiles] one past the last
+  const int* sector_tile_first;  // [nbr_sectors + 1]
+  int nbr_tiles;
+  int nbr_sectors;
+};
+int launch_seg_gram(const double* a, const double* b, int k, const TileSetDevice& t, double* partial, double* g,
+                    cudaStream_t s);
+int launch_seg_update(double* w, const double* v, const double* A, const double* vp, const double* Bt, int k,
+                      const TileSetDevice& t, cudaStream_t s);
+int launch_seg_rmul(double* w, const double* M, int k, const TileSetDevice& t, float* w32, cudaStream_t s);
+int launch_seg_combine_blocks(const double* blocks, int nb, long long stride, const double* C, int cstride, int k,
+                              const TileSetDevice& t, double* out, cudaStream_t s);
+int launch_random_block(double* x, long long rows, int k, const long long* row_sector_base, const TileSetDevice& t,
+                        uint64_t seed, cudaStream_t s);
+int launch_f32_copy(const double* x, float* y, long long n, cudaStream_t s);
+// eigenvalues (ascending) of a symmetric band matrix of half-bandwidth b stored densely (row-major,
+// destroyed): Givens reduction to tridiagonal form touching only the band, then implicit QL
+int band_eigenvalues(int n, int b, double* a, double* eig);
+
 int launch_fqhe_unrank(int nbr_fermions, int lz_max, int total_sum, long long dim, uint64_t* words,
                        const int64_t* counts_dev, int count_stride_o, int count_stride_s, cudaStream_t s);
 int launch_fqhe_matvec(const FqheDevice& f, const MatvecArgs& a, int precision, cudaStream_t s);

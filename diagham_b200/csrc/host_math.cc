@@ -354,4 +354,54 @@ int symmetric_eigen(int n, double* a, double* eig, double* z) {
   return DH_OK;
 }
 
+// Symmetric band matrix (half-bandwidth b, dense row-major storage) to tridiagonal form by Givens
+// rotations with bulge chasing (Schwarz's algorithm; the role of
+// RealBandDiagonalSymmetricMatrix::Tridiagonalize, RealBandDiagonalSymmetricMatrix.cc:847), then the
+// implicit QL of tridiagonal_eigen.  Each rotation touches O(b) entries: O(n^2 b) work overall.
+namespace {
+void band_rotate(double* a, int n, int b, int p, int q, double c, double s) {
+  const int lo = std::max(0, p - b - 2), hi = std::min(n - 1, q + b + 1);
+  for (int col = lo; col <= hi; ++col) {
+    if (col == p || col == q) continue;
+    const double x = a[(size_t)p * n + col], y = a[(size_t)q * n + col];
+    const double xp = c * x + s * y, yq = -s * x + c * y;
+    a[(size_t)p * n + col] = xp;
+    a[(size_t)col * n + p] = xp;
+    a[(size_t)q * n + col] = yq;
+    a[(size_t)col * n + q] = yq;
+  }
+  const double app = a[(size_t)p * n + p], aqq = a[(size_t)q * n + q], apq = a[(size_t)p * n + q];
+  a[(size_t)p * n + p] = c * c * app + 2.0 * c * s * apq + s * s * aqq;
+  a[(size_t)q * n + q] = s * s * app - 2.0 * c * s * apq + c * c * aqq;
+  const double off = (c * c - s * s) * apq + c * s * (aqq - app);
+  a[(size_t)p * n + q] = off;
+  a[(size_t)q * n + p] = off;
+}
+
+// zero a[q][j] against a[p][j] (j < p = q - 1) with a rotation in the (p, q) plane
+void band_annihilate(double* a, int n, int b, int p, int q, int j) {
+  const double x = a[(size_t)p * n + j], y = a[(size_t)q * n + j];
+  if (y == 0.0) return;
+  const double r = hypot(x, y);
+  band_rotate(a, n, b, p, q, x / r, y / r);
+  a[(size_t)q * n + j] = 0.0;
+  a[(size_t)j * n + q] = 0.0;
+}
+}  // namespace
+
+int band_eigenvalues(int n, int b, double* a, double* eig) {
+  if (n <= 0) return DH_OK;
+  for (int j = 0; j + 2 < n; ++j) {
+    for (int i = std::min(j + b, n - 1); i >= j + 2; --i) {
+      band_annihilate(a, n, b, i - 1, i, j);
+      // the rotation leaves a bulge at (i + b, i - 1); chase it down the band
+      for (int k = i; k + b < n; k += b) band_annihilate(a, n, b, k + b - 1, k + b, k - 1);
+    }
+  }
+  std::vector<double> d(n), e(n > 1 ? n - 1 : 1, 0.0);
+  for (int i = 0; i < n; ++i) d[i] = a[(size_t)i * n + i];
+  for (int i = 0; i + 1 < n; ++i) e[i] = a[(size_t)(i + 1) * n + i];
+  return tridiagonal_eigen(n, d.data(), e.data(), eig, nullptr);
+}
+
 }  // namespace dh

@@ -1,0 +1,266 @@
+// Block (k-vector) kernels of the batched block Lanczos: every sector's block is a tall-skinny
+// [rows][k] FP64 array inside one concatenated vector, and every kernel works sector by sector
+// through a tile list (tile = up to kTileRows rows of one sector), so all sectors advance in one
+// launch.  The small k x k matrices (Gram, recurrence and QR coefficients) are per sector.
+// Reductions are two-level and deterministic: tile partials, then a per-sector sum in tile order.
+// This is the device side of BasicBlockLanczosAlgorithm's MultipleRealScalarProductOperation /
+// AddRealLinearCombinationOperation / ReorthogonalizeVectors (BasicBlockLanczosAlgorithm.cc:524-799).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dh_internal.h"
+
+namespace dh {
+namespace {
+
+constexpr int kThreads = 256;
+
+template <int W>
+__device__ __forceinline__ void block_sum(double (&acc)[W], double (&out)[W]) {
+  __shared__ double red[W][kThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < W; ++j) {
+    double v = acc[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) red[j][warp] = v;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < W; ++j) {
+    double v = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) v += red[j][w];
+    out[j] = v;
+  }
+}
+
+// partial[tile][p * K + q] = sum over the tile's rows of a[r][p] * b[r][q]
+template <int K>
+__global__ void __launch_bounds__(kThreads) seg_gram_kernel(const double* a, const double* b, TileSetDevice t,
+                                                            double* partial) {
+  const int tile = blockIdx.x;
+  const long long r0 = t.tile_begin[tile], r1 = t.tile_end[tile];
+  double acc[K * K];
+#pragma unroll
+  for (int j = 0; j < K * K; ++j) acc[j] = 0.0;
+  for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+    double av[K], bv[K];
+#pragma unroll
+    for (int p = 0; p < K; ++p) av[p] = a[r * K + p];
+#pragma unroll
+    for (int q = 0; q < K; ++q) bv[q] = b[r * K + q];
+#pragma unroll
+    for (int p = 0; p < K; ++p)
+#pragma unroll
+      for (int q = 0; q < K; ++q) acc[p * K + q] += av[p] * bv[q];
+  }
+  double tot[K * K];
+  block_sum<K * K>(acc, tot);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int j = 0; j < K * K; ++j) partial[(size_t)tile * K * K + j] = tot[j];
+  }
+}
+
+// g[s][j] = sum over the tiles of sector s (in tile order) of partial[tile][j]
+template <int K>
+__global__ void seg_gram_reduce_kernel(const double* partial, TileSetDevice t, double* g) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= t.nbr_sectors * K * K) return;
+  const int s = i / (K * K), j = i % (K * K);
+  double acc = 0.0;
+  for (int tile = t.sector_tile_first[s]; tile < t.sector_tile_first[s + 1]; ++tile) acc += partial[(size_t)tile * K * K + j];
+  g[i] = acc;
+}
+
+// w[r] -= v[r] * A_s + vp[r] * Bt_s   (A, Bt: [sector][K][K] row-major; vp / Bt may be null)
+template <int K>
+__global__ void __launch_bounds__(kThreads) seg_update_kernel(double* w, const double* v, const double* A,
+                                                              const double* vp, const double* Bt, TileSetDevice t) {
+  const int tile = blockIdx.x;
+  const int s = t.tile_sector[tile];
+  __shared__ double sA[K * K], sB[K * K];
+  if (threadIdx.x < K * K) {
+    sA[threadIdx.x] = A[(size_t)s * K * K + threadIdx.x];
+    sB[threadIdx.x] = (vp && Bt) ? Bt[(size_t)s * K * K + threadIdx.x] : 0.0;
+  }
+  __syncthreads();
+  const long long r0 = t.tile_begin[tile], r1 = t.tile_end[tile];
+  for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+    double vr[K], pr[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      vr[j] = v[r * K + j];
+      pr[j] = vp ? vp[r * K + j] : 0.0;
+    }
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+      double acc = w[r * K + c];
+#pragma unroll
+      for (int j = 0; j < K; ++j) acc -= vr[j] * sA[j * K + c] + pr[j] * sB[j * K + c];
+      w[r * K + c] = acc;
+    }
+  }
+}
+
+// w[r] = w[r] * M_s in place (M: [sector][K][K] row-major), optional FP32 copy of the result
+template <int K>
+__global__ void __launch_bounds__(kThreads) seg_rmul_kernel(double* w, const double* M, TileSetDevice t, float* w32) {
+  const int tile = blockIdx.x;
+  const int s = t.tile_sector[tile];
+  __shared__ double sM[K * K];
+  if (threadIdx.x < K * K) sM[threadIdx.x] = M[(size_t)s * K * K + threadIdx.x];
+  __syncthreads();
+  const long long r0 = t.tile_begin[tile], r1 = t.tile_end[tile];
+  for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+    double in[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) in[j] = w[r * K + j];
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+      double acc = 0.0;
+#pragma unroll
+      for (int j = 0; j < K; ++j) acc += in[j] * sM[j * K + c];
+      w[r * K + c] = acc;
+      if (w32) w32[r * K + c] = (float)acc;
+    }
+  }
+}
+
+// out[r] (+)= sum_b blocks[b][r] * C_s[b] (Ritz vectors: nb stored blocks of K vectors, C per sector
+// [nb * K][K]); writes the K Ritz vectors of every sector
+template <int K>
+__global__ void __launch_bounds__(kThreads) seg_combine_blocks_kernel(const double* blocks, int nb, long long stride,
+                                                                      const double* C, int cstride, TileSetDevice t,
+                                                                      double* out) {
+  const int tile = blockIdx.x;
+  const int s = t.tile_sector[tile];
+  const double* Cs = C + (size_t)s * cstride;
+  const long long r0 = t.tile_begin[tile], r1 = t.tile_end[tile];
+  for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+    double acc[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) acc[c] = 0.0;
+    for (int b = 0; b < nb; ++b) {
+      const double* vb = blocks + (size_t)b * stride + r * K;
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
+        const double x = vb[j];
+#pragma unroll
+        for (int c = 0; c < K; ++c) acc[c] += x * Cs[(b * K + j) * K + c];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < K; ++c) out[r * K + c] = acc[c];
+  }
+}
+
+__global__ void random_block_kernel(double* x, long long rows, int k, const long long* row_sector_base,
+                                    TileSetDevice t, uint64_t seed) {
+  const int tile = blockIdx.x;
+  const int s = t.tile_sector[tile];
+  const long long base = row_sector_base[s];
+  const long long r0 = t.tile_begin[tile], r1 = t.tile_end[tile];
+  for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+    for (int j = 0; j < k; ++j) {
+      // vector j of sector s: component i = (i+1)-th splitmix64 output of seed + j
+      const uint64_t i = (uint64_t)(r - base);
+      uint64_t z = seed + (uint64_t)j + (i + 1) * 0x9E3779B97F4A7C15ull;
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+      z = z ^ (z >> 31);
+      x[r * k + j] = (double)(z >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+    }
+  }
+  (void)rows;
+}
+
+__global__ void f32_copy_kernel(const double* x, float* y, long long n) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) y[i] = (float)x[i];
+}
+
+}  // namespace
+
+int launch_seg_gram(const double* a, const double* b, int k, const TileSetDevice& t, double* partial, double* g,
+                    cudaStream_t s) {
+  if (t.nbr_tiles <= 0) return DH_OK;
+  const int n = t.nbr_sectors * k * k;
+  switch (k) {
+    case 1:
+      seg_gram_kernel<1><<<t.nbr_tiles, kThreads, 0, s>>>(a, b, t, partial);
+      seg_gram_reduce_kernel<1><<<(n + 255) / 256, 256, 0, s>>>(partial, t, g);
+      break;
+    case 2:
+      seg_gram_kernel<2><<<t.nbr_tiles, kThreads, 0, s>>>(a, b, t, partial);
+      seg_gram_reduce_kernel<2><<<(n + 255) / 256, 256, 0, s>>>(partial, t, g);
+      break;
+    case 4:
+      seg_gram_kernel<4><<<t.nbr_tiles, kThreads, 0, s>>>(a, b, t, partial);
+      seg_gram_reduce_kernel<4><<<(n + 255) / 256, 256, 0, s>>>(partial, t, g);
+      break;
+    default:
+      set_error("block size %d not in {1, 2, 4}", k);
+      return DH_ERR_UNSUPPORTED;
+  }
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_seg_update(double* w, const double* v, const double* A, const double* vp, const double* Bt, int k,
+                      const TileSetDevice& t, cudaStream_t s) {
+  if (t.nbr_tiles <= 0) return DH_OK;
+  switch (k) {
+    case 1: seg_update_kernel<1><<<t.nbr_tiles, kThreads, 0, s>>>(w, v, A, vp, Bt, t); break;
+    case 2: seg_update_kernel<2><<<t.nbr_tiles, kThreads, 0, s>>>(w, v, A, vp, Bt, t); break;
+    case 4: seg_update_kernel<4><<<t.nbr_tiles, kThreads, 0, s>>>(w, v, A, vp, Bt, t); break;
+    default: set_error("block size %d not in {1, 2, 4}", k); return DH_ERR_UNSUPPORTED;
+  }
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_seg_rmul(double* w, const double* M, int k, const TileSetDevice& t, float* w32, cudaStream_t s) {
+  if (t.nbr_tiles <= 0) return DH_OK;
+  switch (k) {
+    case 1: seg_rmul_kernel<1><<<t.nbr_tiles, kThreads, 0, s>>>(w, M, t, w32); break;
+    case 2: seg_rmul_kernel<2><<<t.nbr_tiles, kThreads, 0, s>>>(w, M, t, w32); break;
+    case 4: seg_rmul_kernel<4><<<t.nbr_tiles, kThreads, 0, s>>>(w, M, t, w32); break;
+    default: set_error("block size %d not in {1, 2, 4}", k); return DH_ERR_UNSUPPORTED;
+  }
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_seg_combine_blocks(const double* blocks, int nb, long long stride, const double* C, int cstride, int k,
+                              const TileSetDevice& t, double* out, cudaStream_t s) {
+  if (t.nbr_tiles <= 0) return DH_OK;
+  switch (k) {
+    case 1: seg_combine_blocks_kernel<1><<<t.nbr_tiles, kThreads, 0, s>>>(blocks, nb, stride, C, cstride, t, out); break;
+    case 2: seg_combine_blocks_kernel<2><<<t.nbr_tiles, kThreads, 0, s>>>(blocks, nb, stride, C, cstride, t, out); break;
+    case 4: seg_combine_blocks_kernel<4><<<t.nbr_tiles, kThreads, 0, s>>>(blocks, nb, stride, C, cstride, t, out); break;
+    default: set_error("block size %d not in {1, 2, 4}", k); return DH_ERR_UNSUPPORTED;
+  }
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_random_block(double* x, long long rows, int k, const long long* row_sector_base, const TileSetDevice& t,
+                        uint64_t seed, cudaStream_t s) {
+  if (t.nbr_tiles <= 0) return DH_OK;
+  random_block_kernel<<<t.nbr_tiles, kThreads, 0, s>>>(x, rows, k, row_sector_base, t, seed);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_f32_copy(const double* x, float* y, long long n, cudaStream_t s) {
+  long long g = (n + 255) / 256;
+  if (g > 148 * 16) g = 148 * 16;
+  if (g < 1) g = 1;
+  f32_copy_kernel<<<(unsigned)g, 256, 0, s>>>(x, y, n);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+}  // namespace dh

@@ -177,24 +177,183 @@ __device__ __forceinline__ uint32_t between32(int lo, int hi) {
   return upto & ~((2u << lo) - 1u);
 }
 
-template <typename TG, int K, bool RANGE>
+// K gathered values of target row idx: interleaved blocks ([row][K], IL) load them as one vector
+template <typename TG, int K, bool IL>
+__device__ __forceinline__ void load_row(const TG* x, const MatvecArgs& a, int idx, TG (&v)[K]) {
+  if (IL) {
+    const TG* p = x + (long long)idx * K;
+    if (sizeof(TG) == 4 && K == 4) {
+      const float4 q = __ldg(reinterpret_cast<const float4*>(p));
+      v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+      return;
+    }
+    if (sizeof(TG) == 4 && K == 2) {
+      const float2 q = __ldg(reinterpret_cast<const float2*>(p));
+      v[0] = q.x; v[1] = q.y;
+      return;
+    }
+    if (sizeof(TG) == 8 && (K == 2 || K == 4)) {
+#pragma unroll
+      for (int j = 0; j < K; j += 2) {
+        const double2 q = __ldg(reinterpret_cast<const double2*>(p) + j / 2);
+        v[j] = q.x;
+        v[j + 1] = q.y;
+      }
+      return;
+    }
+#pragma unroll
+    for (int j = 0; j < K; ++j) v[j] = __ldg(p + j);
+    return;
+  }
+  if (K == 1 && a.ld == 1) {
+    v[0] = __ldg(x + idx);
+    return;
+  }
+  const TG* p = x + (long long)idx * a.ld;
+#pragma unroll
+  for (int j = 0; j < K; ++j) v[j] = __ldg(p + j * a.vstride);
+}
+
+template <typename TG, int K, bool RANGE, bool IL>
 __device__ __forceinline__ void accumulate2(TG (&acc)[K], const TG* x, const MatvecArgs& a, int ia, TG fa, int ib,
                                             TG fb) {
   if (RANGE) {
     if (ia < a.col_first || ia >= a.col_last) fa = TG(0);
     if (ib < a.col_first || ib >= a.col_last) fb = TG(0);
   }
-  if (K == 1 && a.ld == 1) {
-    acc[0] += fa * __ldg(x + ia) + fb * __ldg(x + ib);
-    return;
-  }
-  const TG* pa = x + (long long)ia * a.ld;
-  const TG* pb = x + (long long)ib * a.ld;
+  TG xa[K], xb[K];
+  load_row<TG, K, IL>(x, a, ia, xa);
+  load_row<TG, K, IL>(x, a, ib, xb);
 #pragma unroll
-  for (int j = 0; j < K; ++j) {
-    const TG xa = __ldg(pa + j * a.vstride);
-    const TG xb = __ldg(pb + j * a.vstride);
-    acc[j] += fa * xa + fb * xb;
+  for (int j = 0; j < K; ++j) acc[j] += fa * xa[j] + fb * xb[j];
+}
+
+// the rank tables and words of one sector
+struct SplitTables {
+  const uint64_t* words;
+  const int32_t* HO;
+  const uint16_t* LR;
+  int LB;
+  uint64_t full;
+};
+
+// Off-diagonal elements of row r accumulated into acc (K vectors) and the sum of its diagonal
+// factors into dsum; the caller adds dsum * x[r] and the shift.
+template <typename TG, int K, bool RANGE, bool IL>
+__device__ __forceinline__ void split_row(const SplitTables& t, const TG* sfac, const int* spair, long long r,
+                                          const TG* x, const MatvecArgs& a, TG (&acc)[K], TG& dsum) {
+  const int LB = t.LB;
+  const uint32_t lmask = (1u << LB) - 1u;
+  const int32_t* __restrict__ HO = t.HO;
+  const uint16_t* __restrict__ LR = t.LR;
+  const uint64_t s = __ldg(t.words + r);
+  const uint32_t sl = (uint32_t)s & lmask;
+  const uint32_t sh = (uint32_t)(s >> LB);
+  const int ho_row = __ldg(HO + sh);
+  const int lr_row = (int)(r - ho_row);
+  // a non-diagonal creation pair is empty in the row itself, so its admissible m3 for the sum M
+  // are E & mirror_M(E) above M/2; the bit reversal of E is taken once per row
+  const uint64_t E = ~s & t.full;
+  const uint64_t RE = __brevll(E);
+  // exclusive prefix parity of s: bit k = parity of the occupied orbitals below k
+  uint64_t pp = s;
+  pp ^= pp << 1;
+  pp ^= pp << 2;
+  pp ^= pp << 4;
+  pp ^= pp << 8;
+  pp ^= pp << 16;
+  pp ^= pp << 32;
+  pp <<= 1;
+  // diagonal elements: (m3, m4) = (m1, m2) is admissible for every occupied pair and its
+  // AA * AdAd sign is -1, so they add -sum(factor(m1, m2, m1)) * x[r]
+  uint64_t rem1 = s;
+  while (rem1) {
+    const int m1 = 63 - __clzll(rem1);
+    rem1 &= ~(1ull << m1);
+    uint64_t rem2 = rem1;
+    const int pbase = m1 * (m1 - 1) / 2;
+    const int p1 = (int)(pp >> m1) & 1;
+    while (rem2) {
+      const int m2 = 63 - __clzll(rem2);
+      rem2 &= ~(1ull << m2);
+      const int M = m1 + m2;
+      const TG* fp = sfac + (spair[pbase + m2] - (M / 2 + 1));
+      dsum -= fp[m1];
+      const uint64_t mir = (M <= 63) ? (RE >> (63 - M)) : (RE << (M - 63));
+      const uint64_t valid = E & mir & (~0ull << (M / 2 + 1));
+      if (!valid) continue;
+      // AA sign parity: 1 + occupied orbitals strictly between m2 and m1
+      const int paa = 1 ^ p1 ^ ((int)(pp >> (m2 + 1)) & 1);
+      const uint32_t anl = sl & ~((m1 < LB ? (1u << m1) : 0u) | (m2 < LB ? (1u << m2) : 0u));
+      const uint32_t anh = sh & ~((m1 >= LB ? (1u << (m1 - LB)) : 0u) | (m2 >= LB ? (1u << (m2 - LB)) : 0u));
+      // split the admissible m3 into three 32-bit masks:
+      //   vl: m3 < LB (creations in the low half), bit m3
+      //   vh: m4 = M - m3 >= LB (creations in the high half), bit m3 - LB
+      //   vm: m4 < LB <= m3 (mixed), bit m3 - LB
+      uint32_t vl = (uint32_t)valid & lmask;
+      const uint64_t hv = valid >> LB;
+      const int hcut = M - 2 * LB;  // relative m3 - LB <= M - 2 LB  <=>  m4 >= LB
+      const uint64_t hkeep = (hcut < 0) ? 0ull : ((hcut >= 63) ? ~0ull : ((2ull << hcut) - 1ull));
+      uint32_t vh = (uint32_t)(hv & hkeep);
+      uint32_t vm = (uint32_t)(hv & ~hkeep);
+      if (vl) {
+        const int base = (m1 < LB) ? ho_row : __ldg(HO + anh);
+        while (vl) {
+          const int m3a = __ffs(vl) - 1;
+          vl &= vl - 1u;
+          const bool two = vl != 0u;
+          const int m3b = two ? __ffs(vl) - 1 : m3a;
+          vl &= vl - 1u;
+          const int m4a = M - m3a, m4b = M - m3b;
+          const int ia = base + LR[anl | (1u << m3a) | (1u << m4a)];
+          const int ib = base + LR[anl | (1u << m3b) | (1u << m4b)];
+          TG fa = fp[m3a], fb = two ? fp[m3b] : TG(0);
+          if ((paa + __popc(anl & between32(m4a, m3a))) & 1) fa = -fa;
+          if ((paa + __popc(anl & between32(m4b, m3b))) & 1) fb = -fb;
+          accumulate2<TG, K, RANGE, IL>(acc, x, a, ia, fa, ib, fb);
+        }
+      }
+      if (vh) {
+        const int base = (m2 >= LB) ? lr_row : LR[anl];
+        const TG* fph = fp + LB;
+        const int MH = M - 2 * LB;
+        while (vh) {
+          const int ha3 = __ffs(vh) - 1;
+          vh &= vh - 1u;
+          const bool two = vh != 0u;
+          const int hb3 = two ? __ffs(vh) - 1 : ha3;
+          vh &= vh - 1u;
+          const int ha4 = MH - ha3, hb4 = MH - hb3;
+          const int ia = base + __ldg(HO + (anh | (1u << ha3) | (1u << ha4)));
+          const int ib = base + __ldg(HO + (anh | (1u << hb3) | (1u << hb4)));
+          TG fa = fph[ha3], fb = two ? fph[hb3] : TG(0);
+          if ((paa + __popc(anh & between32(ha4, ha3))) & 1) fa = -fa;
+          if ((paa + __popc(anh & between32(hb4, hb3))) & 1) fb = -fb;
+          accumulate2<TG, K, RANGE, IL>(acc, x, a, ia, fa, ib, fb);
+        }
+      }
+      if (vm) {
+        // m4 < LB <= m3: the orbitals between them are the low ones above m4 and the high ones below m3
+        const TG* fph = fp + LB;
+        const int ML = M - LB;
+        while (vm) {
+          const int ha3 = __ffs(vm) - 1;
+          vm &= vm - 1u;
+          const bool two = vm != 0u;
+          const int hb3 = two ? __ffs(vm) - 1 : ha3;
+          vm &= vm - 1u;
+          const int m4a = ML - ha3, m4b = ML - hb3;
+          const int ia = __ldg(HO + (anh | (1u << ha3))) + LR[anl | (1u << m4a)];
+          const int ib = __ldg(HO + (anh | (1u << hb3))) + LR[anl | (1u << m4b)];
+          TG fa = fph[ha3], fb = two ? fph[hb3] : TG(0);
+          const int pa = __popc(anl & between32(m4a, LB)) + __popc(anh & ((1u << ha3) - 1u));
+          const int pb = __popc(anl & between32(m4b, LB)) + __popc(anh & ((1u << hb3) - 1u));
+          if ((paa + pa) & 1) fa = -fa;
+          if ((paa + pb) & 1) fb = -fb;
+          accumulate2<TG, K, RANGE, IL>(acc, x, a, ia, fa, ib, fb);
+        }
+      }
+    }
   }
 }
 
@@ -206,136 +365,28 @@ __global__ void __launch_bounds__(kMatvecThreads) fqhe_split_kernel(FqheDevice f
   const TG* gfac = static_cast<const TG*>(f.factors);
   for (int i = threadIdx.x; i < f.nbr_factors; i += blockDim.x) sfac[i] = gfac[i];
   for (int i = threadIdx.x; i < f.nbr_pairs; i += blockDim.x) spair[i] = f.pair_offset[i];
-  const int LB = f.low_bits;
-  const uint16_t* __restrict__ LR = f.low_rank;
+  SplitTables t;
+  t.words = f.words;
+  t.HO = f.high_offset;
+  t.LR = f.low_rank;
+  t.LB = f.low_bits;
+  t.full = (f.lz_max >= 63) ? ~0ull : ((1ull << (f.lz_max + 1)) - 1ull);
   if (LR_SMEM) {
     uint16_t* slr = reinterpret_cast<uint16_t*>(smem + lay.factor_bytes + lay.pair_bytes);
     const uint4* src = reinterpret_cast<const uint4*>(f.low_rank);
     uint4* dst = reinterpret_cast<uint4*>(slr);
-    for (int i = threadIdx.x; i < (1 << LB) / 8; i += blockDim.x) dst[i] = src[i];
-    LR = slr;
+    for (int i = threadIdx.x; i < (1 << t.LB) / 8; i += blockDim.x) dst[i] = src[i];
+    t.LR = slr;
   }
   __syncthreads();
-
-  const uint32_t lmask = (1u << LB) - 1u;
-  const int32_t* __restrict__ HO = f.high_offset;
   const TG* x = static_cast<const TG*>(a.x);
-  const uint64_t full = (f.lz_max >= 63) ? ~0ull : ((1ull << (f.lz_max + 1)) - 1ull);
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
-    const uint64_t s = __ldg(f.words + r);
-    const uint32_t sl = (uint32_t)s & lmask;
-    const uint32_t sh = (uint32_t)(s >> LB);
-    const int ho_row = __ldg(HO + sh);
-    const int lr_row = (int)(r - ho_row);
-    // a non-diagonal creation pair is empty in the row itself, so its admissible m3 for the sum M
-    // are E & mirror_M(E) above M/2; the bit reversal of E is taken once per row
-    const uint64_t E = ~s & full;
-    const uint64_t RE = __brevll(E);
-    // exclusive prefix parity of s: bit k = parity of the occupied orbitals below k
-    uint64_t pp = s;
-    pp ^= pp << 1;
-    pp ^= pp << 2;
-    pp ^= pp << 4;
-    pp ^= pp << 8;
-    pp ^= pp << 16;
-    pp ^= pp << 32;
-    pp <<= 1;
     TG acc[K];
 #pragma unroll
     for (int j = 0; j < K; ++j) acc[j] = TG(0);
-    // diagonal elements: (m3, m4) = (m1, m2) is admissible for every occupied pair and its
-    // AA * AdAd sign is -1, so they add -sum(factor(m1, m2, m1)) * x[r]
     TG dsum = TG(0);
-    uint64_t rem1 = s;
-    while (rem1) {
-      const int m1 = 63 - __clzll(rem1);
-      rem1 &= ~(1ull << m1);
-      uint64_t rem2 = rem1;
-      const int pbase = m1 * (m1 - 1) / 2;
-      const int p1 = (int)(pp >> m1) & 1;
-      while (rem2) {
-        const int m2 = 63 - __clzll(rem2);
-        rem2 &= ~(1ull << m2);
-        const int M = m1 + m2;
-        const TG* fp = sfac + (spair[pbase + m2] - (M / 2 + 1));
-        dsum -= fp[m1];
-        const uint64_t mir = (M <= 63) ? (RE >> (63 - M)) : (RE << (M - 63));
-        const uint64_t valid = E & mir & (~0ull << (M / 2 + 1));
-        if (!valid) continue;
-        // AA sign parity: 1 + occupied orbitals strictly between m2 and m1
-        const int paa = 1 ^ p1 ^ ((int)(pp >> (m2 + 1)) & 1);
-        const uint32_t anl = sl & ~((m1 < LB ? (1u << m1) : 0u) | (m2 < LB ? (1u << m2) : 0u));
-        const uint32_t anh = sh & ~((m1 >= LB ? (1u << (m1 - LB)) : 0u) | (m2 >= LB ? (1u << (m2 - LB)) : 0u));
-        // split the admissible m3 into three 32-bit masks:
-        //   vl: m3 < LB (creations in the low half), bit m3
-        //   vh: m4 = M - m3 >= LB (creations in the high half), bit m3 - LB
-        //   vm: m4 < LB <= m3 (mixed), bit m3 - LB
-        uint32_t vl = (uint32_t)valid & lmask;
-        const uint64_t hv = valid >> LB;
-        const int hcut = M - 2 * LB;  // relative m3 - LB <= M - 2 LB  <=>  m4 >= LB
-        const uint64_t hkeep = (hcut < 0) ? 0ull : ((hcut >= 63) ? ~0ull : ((2ull << hcut) - 1ull));
-        uint32_t vh = (uint32_t)(hv & hkeep);
-        uint32_t vm = (uint32_t)(hv & ~hkeep);
-        if (vl) {
-          const int base = (m1 < LB) ? ho_row : __ldg(HO + anh);
-          while (vl) {
-            const int m3a = __ffs(vl) - 1;
-            vl &= vl - 1u;
-            const bool two = vl != 0u;
-            const int m3b = two ? __ffs(vl) - 1 : m3a;
-            vl &= vl - 1u;
-            const int m4a = M - m3a, m4b = M - m3b;
-            const int ia = base + LR[anl | (1u << m3a) | (1u << m4a)];
-            const int ib = base + LR[anl | (1u << m3b) | (1u << m4b)];
-            TG fa = fp[m3a], fb = two ? fp[m3b] : TG(0);
-            if ((paa + __popc(anl & between32(m4a, m3a))) & 1) fa = -fa;
-            if ((paa + __popc(anl & between32(m4b, m3b))) & 1) fb = -fb;
-            accumulate2<TG, K, RANGE>(acc, x, a, ia, fa, ib, fb);
-          }
-        }
-        if (vh) {
-          const int base = (m2 >= LB) ? lr_row : LR[anl];
-          const TG* fph = fp + LB;
-          const int MH = M - 2 * LB;
-          while (vh) {
-            const int ha3 = __ffs(vh) - 1;
-            vh &= vh - 1u;
-            const bool two = vh != 0u;
-            const int hb3 = two ? __ffs(vh) - 1 : ha3;
-            vh &= vh - 1u;
-            const int ha4 = MH - ha3, hb4 = MH - hb3;
-            const int ia = base + __ldg(HO + (anh | (1u << ha3) | (1u << ha4)));
-            const int ib = base + __ldg(HO + (anh | (1u << hb3) | (1u << hb4)));
-            TG fa = fph[ha3], fb = two ? fph[hb3] : TG(0);
-            if ((paa + __popc(anh & between32(ha4, ha3))) & 1) fa = -fa;
-            if ((paa + __popc(anh & between32(hb4, hb3))) & 1) fb = -fb;
-            accumulate2<TG, K, RANGE>(acc, x, a, ia, fa, ib, fb);
-          }
-        }
-        if (vm) {
-          // m4 < LB <= m3: the orbitals between them are the low ones above m4 and the high ones below m3
-          const TG* fph = fp + LB;
-          const int ML = M - LB;
-          while (vm) {
-            const int ha3 = __ffs(vm) - 1;
-            vm &= vm - 1u;
-            const bool two = vm != 0u;
-            const int hb3 = two ? __ffs(vm) - 1 : ha3;
-            vm &= vm - 1u;
-            const int m4a = ML - ha3, m4b = ML - hb3;
-            const int ia = __ldg(HO + (anh | (1u << ha3))) + LR[anl | (1u << m4a)];
-            const int ib = __ldg(HO + (anh | (1u << hb3))) + LR[anl | (1u << m4b)];
-            TG fa = fph[ha3], fb = two ? fph[hb3] : TG(0);
-            const int pa = __popc(anl & between32(m4a, LB)) + __popc(anh & ((1u << ha3) - 1u));
-            const int pb = __popc(anl & between32(m4b, LB)) + __popc(anh & ((1u << hb3) - 1u));
-            if ((paa + pa) & 1) fa = -fa;
-            if ((paa + pb) & 1) fb = -fb;
-            accumulate2<TG, K, RANGE>(acc, x, a, ia, fa, ib, fb);
-          }
-        }
-      }
-    }
+    split_row<TG, K, RANGE, false>(t, sfac, spair, r, x, a, acc, dsum);
     if (!RANGE || (r >= a.col_first && r < a.col_last)) {
       const TG* xr = x + r * a.ld;
 #pragma unroll
@@ -352,6 +403,61 @@ __global__ void __launch_bounds__(kMatvecThreads) fqhe_split_kernel(FqheDevice f
       }
       double* yp = y + r * a.ld_y + j * a.vstride_y;
       *yp = a.accumulate ? (*yp + v) : v;
+    }
+  }
+}
+
+// All Lz sectors of one system in one launch: rows of every sector are concatenated (sector s owns
+// rows [row_offset[s], row_offset[s+1])), vectors are K-interleaved ([row][K]) over the
+// concatenated rows, and the factors (same 2S and V for every sector) are staged once per block.
+// A thread finds its sector by a binary search over the offsets kept in shared memory.
+template <typename TG, int K>
+__global__ void __launch_bounds__(kMatvecThreads) fqhe_sectors_kernel(SectorBatchDevice b, SmemLayout lay) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  TG* sfac = reinterpret_cast<TG*>(smem);
+  int* spair = reinterpret_cast<int*>(smem + lay.factor_bytes);
+  long long* soff = reinterpret_cast<long long*>(smem + lay.factor_bytes + lay.pair_bytes);
+  const TG* gfac = static_cast<const TG*>(b.factors);
+  for (int i = threadIdx.x; i < b.nbr_factors; i += blockDim.x) sfac[i] = gfac[i];
+  for (int i = threadIdx.x; i < b.nbr_pairs; i += blockDim.x) spair[i] = b.pair_offset[i];
+  for (int i = threadIdx.x; i <= b.nbr_sectors; i += blockDim.x) soff[i] = b.row_offset[i];
+  __syncthreads();
+  const uint64_t full = (b.lz_max >= 63) ? ~0ull : ((1ull << (b.lz_max + 1)) - 1ull);
+  const TG* xall = static_cast<const TG*>(b.x);
+  MatvecArgs a = {};
+  a.ld = K;
+  a.vstride = 1;
+  const long long total = soff[b.nbr_sectors];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += stride) {
+    int lo = 0, hi = b.nbr_sectors;  // soff[lo] <= g < soff[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (soff[mid] <= g) lo = mid; else hi = mid;
+    }
+    const long long off = soff[lo];
+    const long long r = g - off;
+    SplitTables t;
+    t.words = b.words[lo];
+    t.HO = b.high_offset[lo];
+    t.LR = b.low_rank;
+    t.LB = b.low_bits;
+    t.full = full;
+    const TG* x = xall + off * K;
+    TG acc[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) acc[j] = TG(0);
+    TG dsum = TG(0);
+    split_row<TG, K, false, true>(t, sfac, spair, r, x, a, acc, dsum);
+    TG xr[K];
+    load_row<TG, K, true>(x, a, (int)r, xr);
+    double* y = b.y + g * K;
+    const double* xd = b.xdiag ? b.xdiag + g * K : nullptr;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      double v = (double)(acc[j] + dsum * xr[j]);
+      if (b.shift != 0.0) v += b.shift * (xd ? xd[j] : (double)xr[j]);
+      y[j] = v;
     }
   }
 }
@@ -643,6 +749,49 @@ int launch_fqhe_matvec(const FqheDevice& f, const MatvecArgs& a, int precision, 
   if (f.dim <= 0) return DH_OK;
   if (precision == DH_PRECISION_FP32) return dispatch_k<float>(f, a, s);
   return dispatch_k<double>(f, a, s);
+}
+
+template <typename TG, int K>
+static int launch_sectors_typed(const SectorBatchDevice& b, cudaStream_t s) {
+  SmemLayout lay;
+  lay.factor_bytes = align16(b.nbr_factors * (int)sizeof(TG));
+  lay.pair_bytes = align16(b.nbr_pairs * (int)sizeof(int));
+  lay.lookup_bytes = align16((b.nbr_sectors + 1) * (int)sizeof(long long));
+  lay.total = lay.factor_bytes + lay.pair_bytes + lay.lookup_bytes;
+  auto kern = fqhe_sectors_kernel<TG, K>;
+  if (lay.total > 48 * 1024) DH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total));
+  int dev = 0, sms = 0, per_sm = 0;
+  DH_CUDA(cudaGetDevice(&dev));
+  DH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  DH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kMatvecThreads, lay.total));
+  DH_CHECK(per_sm >= 1, DH_ERR_UNSUPPORTED, "sector kernel: %d bytes of shared memory per block do not fit", lay.total);
+  long long need = (b.total_rows + kMatvecThreads - 1) / kMatvecThreads;
+  long long grid = (long long)sms * per_sm;
+  if (need < grid) grid = need;
+  if (grid < 1) grid = 1;
+  kern<<<(unsigned)grid, kMatvecThreads, lay.total, s>>>(b, lay);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_fqhe_sectors(const SectorBatchDevice& b, int precision, cudaStream_t s) {
+  if (b.total_rows <= 0) return DH_OK;
+  DH_CHECK(b.low_bits <= 31 && b.lz_max + 1 - b.low_bits <= 31, DH_ERR_UNSUPPORTED, "lz_max too large for the sector kernel");
+  if (precision == DH_PRECISION_FP32) {
+    switch (b.block) {
+      case 1: return launch_sectors_typed<float, 1>(b, s);
+      case 2: return launch_sectors_typed<float, 2>(b, s);
+      case 4: return launch_sectors_typed<float, 4>(b, s);
+    }
+  } else {
+    switch (b.block) {
+      case 1: return launch_sectors_typed<double, 1>(b, s);
+      case 2: return launch_sectors_typed<double, 2>(b, s);
+      case 4: return launch_sectors_typed<double, 4>(b, s);
+    }
+  }
+  set_error("sector kernel: block size %d not in {1, 2, 4}", b.block);
+  return DH_ERR_UNSUPPORTED;
 }
 
 int launch_fqhe_row_elements(const FqheDevice& f, long long row, int* targets, int* signs, int* factor_index,

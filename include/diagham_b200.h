@@ -239,6 +239,23 @@ int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eige
  * out[2] = residual norm, out[3] = FP32 matvecs, out[4] = FP64 matvecs. */
 int dh_lanczos_solve_refined(dh_lanczos_t l, int max_iter, double precision, double* out);
 
+/* ================================================================ batched sectors */
+
+/* All requested Lz sectors of N fermions in 2S+1 orbitals with one two-body interaction, solved by
+ * block Lanczos (block_size vectors per sector, BasicBlockLanczosAlgorithm.cc:524-697) in lockstep:
+ * each block product is one launch over every sector, and the block recurrence runs on every
+ * sector at once.  Each sector follows the reference's driver loop and convergence test
+ * (QHEOnSphereMainTask.cc:732-753, precision_target = the Lanczos precision, max_iter in vectors).
+ * Sectors of dimension <= full_diag_limit (or <= 2 block_size) are diagonalised densely, as
+ * QHEOnSphereMainTask does below --full-diag (:397).  FP32 products with FP64 recurrence when
+ * precision == DH_PRECISION_FP32.  energies[s] = lowest eigenvalue of sector s, iterations[s] =
+ * the driver's counter (0 for dense sectors); seconds (optional, 4 values) = set-up seconds, solve
+ * seconds, device time of the block products, number of block products. */
+int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const int* total_lz, int nbr_sectors,
+                                  const double* pseudopotentials, int block_size, int max_iter,
+                                  double precision_target, int precision, int full_diag_limit,
+                                  uint64_t seed, double* energies, int* iterations, double* seconds);
+
 /* ================================================================ setup helpers */
 
 /* EvaluatePseudopotentials(nbrFlux, 0, 0.0) (FQHE/src/Tools/FQHESpectrum/PseudoPotentials.cc:35):

@@ -206,10 +206,13 @@ def block_fixture(tmp, n, s, lz, k):
     dfile = os.path.join(tmp, "b.bin")
     run("fqhe_basis", n, s, lz, dfile)
     dim, _, _ = read_basis(dfile)
+    # BasicBlockLanczosAlgorithm uses given start vectors as they are (InitializeLanczosAlgorithm,
+    # BasicBlockLanczosAlgorithm.cc:262-300), so the block is orthonormalised here first
+    block, _ = np.linalg.qr(np.stack([splitmix_vector(100 + b, dim) for b in range(k)], axis=1))
     files = []
     for b in range(k):
         xf = os.path.join(tmp, "xb%d.vec" % b)
-        write_vector(xf, splitmix_vector(100 + b, dim))
+        write_vector(xf, block[:, b])
         files.append(xf)
     lf = os.path.join(tmp, "l.out")
     cmd = run("fqhe_lanczos", n, s, lz, vf, "block", 2, k, 400, 0, lf, "-", *files)

@@ -161,3 +161,14 @@ def test_random_vector_matches_fixture_generator(orc):
     a = orc.random_vector(7, 1000)
     b = splitmix_vector(7, 1000)
     assert np.max(np.abs(a - b)) < 1e-15
+
+
+def test_block_lanczos_fixture_against_dense(orc):
+    # the reference's BasicBlockLanczosAlgorithm (k = 4) against a dense diagonalisation of the
+    # oracle's Hamiltonian for N = 6, 2S = 15, Lz = 0 (dimension 338)
+    z = golden("lanczos_n6_2s15_lz0_coulomb_block4.npz")
+    H = orc.FQHE(6, 15, 0, z["v"])
+    M = np.stack([H.pull(np.eye(H.dim)[j]) for j in range(H.dim)], axis=1)
+    w = np.linalg.eigvalsh(0.5 * (M + M.T))
+    assert abs(w[0] - float(z["eigenvalues"][0])) < 1e-10 * abs(w[0])
+    assert bool(z["converged"])
