@@ -74,6 +74,7 @@ SIGNATURES = {
     "dh_lanczos_get_eigenvalues": ([_vp, _vp, _c_int], _c_int),
     "dh_lanczos_get_ground_state_energy": ([_vp, _vp], _c_int),
     "dh_lanczos_get_ground_state": ([_vp, _vp], _c_int),
+    "dh_lanczos_get_eigenstates": ([_vp, _c_int, _vp], _c_int),
     "dh_lanczos_get_counters": ([_vp, _i64p, _ip], _c_int),
     "dh_lanczos_solve": ([_vp, _c_int, _c_int, _vp, _ip, _ip], _c_int),
     "dh_lanczos_solve_refined": ([_vp, _c_int, _c_dbl, _vp], _c_int),
@@ -362,11 +363,15 @@ class _Lanczos:
         _check(_lib.dh_lanczos_set_eigenvalue_precision(self._handle, float(precision)))
 
     def InitializeLanczosAlgorithm(self, vector=None, seed=0):
+        """No vector: a reproducible random start from seed.  A vector (dim,) or vectors
+        (nbr, dim) (numpy or torch CUDA): the start vector(s); block algorithms complete and
+        orthonormalise the block."""
         if vector is None:
             _check(_lib.dh_lanczos_initialize_random(self._handle, seed))
         else:
             b = _Buf(vector)
-            _check(_lib.dh_lanczos_initialize(self._handle, b.ptr, 1))
+            nbr = 1 if len(vector.shape) == 1 else int(vector.shape[0])
+            _check(_lib.dh_lanczos_initialize(self._handle, b.ptr, nbr))
 
     def RunLanczosAlgorithm(self, nbr_iter):
         _check(_lib.dh_lanczos_run(self._handle, nbr_iter))
@@ -393,6 +398,16 @@ class _Lanczos:
             out = np.zeros(dim, np.float64)
         b = _Buf(out, writable=True)
         _check(_lib.dh_lanczos_get_ground_state(self._handle, b.ptr))
+        b.finish()
+        return out
+
+    def GetEigenstates(self, n, out=None):
+        """The n lowest Ritz vectors, normalised, as an (n, dim) array (or into out)."""
+        dim = self.hamiltonian.dim
+        if out is None:
+            out = np.zeros((n, dim), np.float64)
+        b = _Buf(out, writable=True)
+        _check(_lib.dh_lanczos_get_eigenstates(self._handle, n, b.ptr))
         b.finish()
         return out
 
@@ -434,6 +449,16 @@ class FullReorthogonalizedLanczosAlgorithm(_Lanczos):
 
 class BasicLanczosAlgorithmWithGroundState(_Lanczos):
     ALGORITHM = DH_LANCZOS_WITH_GROUND_STATE
+
+
+class BasicBlockLanczosAlgorithm(_Lanczos):
+    """BasicBlockLanczosAlgorithm(architecture, nbrEigenvalue, blockSize, maxIter): block_size 1, 2
+    or 4 vectors per step, one product per block step for the whole block."""
+    ALGORITHM = DH_LANCZOS_BLOCK
+
+    def __init__(self, hamiltonian, nbr_eigenvalue=1, max_iter=500, block_size=2):
+        super().__init__(hamiltonian, nbr_eigenvalue, max_iter, block_size)
+        self.block_size = block_size
 
 
 def coulomb_pseudopotentials(nbr_flux):

@@ -43,6 +43,13 @@ struct BlockSector {
   int steps = 0;
 };
 
+// coefficients of one block step for every sector, enough to replay it exactly (every kernel is
+// deterministic): the symmetrised A, the B^T used by the update, and the two CholQR inverses
+struct StepRecord {
+  std::vector<double> A, Bt, inv1, inv2;
+  bool have_prev = false;
+};
+
 struct BlockEngine {
   int k = 4, nsec = 0, nev = 1, precision = DH_PRECISION_FP64;
   double eig_precision = 1e-14;
@@ -61,6 +68,10 @@ struct BlockEngine {
   std::function<int(const double*, const float*, double*)> product;
   double product_ms = 0.0;
   long long products = 0;
+  std::vector<StepRecord> history;
+  DevBuf start_block;    // the orthonormal start block, for replays
+  DevBuf store;          // every block when keep_blocks (store_cap blocks of total * k)
+  int store_cap = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   ~BlockEngine() {
     if (ev0) cudaEventDestroy(ev0);
@@ -170,7 +181,8 @@ bool cholesky_inverse(int k, const double* G, double* R, double* Rinv) {
 // A sector whose block is numerically zero against its scale (|X|_F^2 < 1e-24 scale[s], scale =
 // |A|^2 + |B|^2 of the step: the block Krylov space is complete) or whose Gram matrix breaks down
 // gets a zero block and is marked exhausted.
-int engine_qr(BlockEngine& e, double* x, std::vector<double>& B, float* x32, const std::vector<double>* scale) {
+int engine_qr(BlockEngine& e, double* x, std::vector<double>& B, float* x32, const std::vector<double>* scale,
+              std::vector<double>* inv1 = nullptr, std::vector<double>* inv2 = nullptr) {
   const int k = e.k, kk = k * k;
   std::vector<double> g, R1((size_t)e.nsec * kk), R2((size_t)e.nsec * kk), inv((size_t)e.nsec * kk);
   std::vector<char> broke(e.nsec, 0);
@@ -194,6 +206,9 @@ int engine_qr(BlockEngine& e, double* x, std::vector<double>& B, float* x32, con
     }
     DH_CUDA(cudaMemcpyAsync(dM, inv.data(), inv.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
     if ((rc = launch_seg_rmul(x, dM, k, e.tiles, pass ? x32 : nullptr, e.stream)) != DH_OK) return rc;
+    if (pass == 0 && inv1) *inv1 = inv;
+    if (pass == 1 && inv2) *inv2 = inv;
+    DH_CUDA(cudaStreamSynchronize(e.stream));  // inv is reused by the next pass
   }
   B.assign((size_t)e.nsec * kk, 0.0);
   for (int s = 0; s < e.nsec; ++s) {
@@ -234,6 +249,11 @@ int engine_start(BlockEngine& e) {
   e.have_prev = false;
   int rc = engine_qr(e, e.slot[0], B, e.x32.as<float>(), nullptr);
   if (rc != DH_OK) return rc;
+  const size_t vb = (size_t)e.total * e.k * sizeof(double);
+  if ((rc = ensure_buffer(e.start_block, vb)) != DH_OK) return rc;
+  DH_CUDA(cudaMemcpyAsync(e.start_block.ptr, e.slot[0], vb, cudaMemcpyDeviceToDevice, e.stream));
+  if (e.store_cap > 0) DH_CUDA(cudaMemcpyAsync(e.store.ptr, e.slot[0], vb, cudaMemcpyDeviceToDevice, e.stream));
+  e.history.clear();
   for (int s = 0; s < e.nsec; ++s) {
     BlockSector& b = e.sec[s];
     b.blocks = 0;
@@ -278,7 +298,16 @@ int engine_step(BlockEngine& e) {
     for (int i = 0; i < kk; ++i)
       scale[s] += A[(size_t)s * kk + i] * A[(size_t)s * kk + i] + e.bt_host[(size_t)s * kk + i] * e.bt_host[(size_t)s * kk + i];
   }
-  if ((rc = engine_qr(e, W, B, e.x32.as<float>(), &scale)) != DH_OK) return rc;
+  StepRecord rec;
+  rec.A = A;
+  rec.Bt = e.bt_host;
+  rec.have_prev = e.have_prev;
+  if ((rc = engine_qr(e, W, B, e.x32.as<float>(), &scale, &rec.inv1, &rec.inv2)) != DH_OK) return rc;
+  e.history.push_back(std::move(rec));
+  const int nb = (int)e.history.size();  // W now holds block nb
+  if (nb < e.store_cap)
+    DH_CUDA(cudaMemcpyAsync(e.store.as<double>() + (size_t)nb * e.total * e.k, W, (size_t)e.total * e.k * sizeof(double),
+                            cudaMemcpyDeviceToDevice, e.stream));
   for (int s = 0; s < e.nsec; ++s) {
     BlockSector& b = e.sec[s];
     if (!b.active) continue;
@@ -313,6 +342,106 @@ int sector_eigenvalues(const BlockEngine& e, const BlockSector& b, std::vector<d
   }
   eig.assign(n, 0.0);
   return band_eigenvalues(n, std::max(1, 2 * k - 1), t.data(), eig.data());
+}
+
+// the nvec lowest eigenpairs of sector s's band matrix; C[(b * k + j) * nvec + c] = component
+// (b k + j) of eigenvector c (the coefficients of the Ritz vectors in the Lanczos blocks)
+int sector_ritz_coefficients(const BlockEngine& e, const BlockSector& b, int nvec, std::vector<double>& C,
+                             std::vector<double>& vals) {
+  const int k = e.k, kk = k * k, m = b.blocks, n = m * k;
+  std::vector<double> t((size_t)n * n, 0.0);
+  for (int j = 0; j < m; ++j) {
+    for (int p = 0; p < k; ++p)
+      for (int q = 0; q < k; ++q) t[(size_t)(j * k + p) * n + j * k + q] = b.A[(size_t)j * kk + p * k + q];
+    if (j + 1 < m)
+      for (int p = 0; p < k; ++p)
+        for (int q = 0; q < k; ++q) {
+          const double v = b.B[(size_t)(j + 1) * kk + p * k + q];
+          t[(size_t)((j + 1) * k + p) * n + j * k + q] = v;
+          t[(size_t)(j * k + q) * n + (j + 1) * k + p] = v;
+        }
+  }
+  std::vector<double> z((size_t)n * n);
+  vals.assign(n, 0.0);
+  int rc = symmetric_eigen(n, t.data(), vals.data(), z.data());
+  if (rc != DH_OK) return rc;
+  C.assign((size_t)n * nvec, 0.0);
+  for (int r = 0; r < n; ++r)
+    for (int c = 0; c < nvec && c < n; ++c) C[(size_t)r * nvec + c] = z[(size_t)r * n + c];
+  return DH_OK;
+}
+
+// out = the k lowest Ritz vectors of every sector (k-interleaved like the blocks): from the stored
+// blocks when they were kept, otherwise by replaying the recorded steps from the start block.
+// After a replay the engine's work vectors hold the replayed state.
+int engine_ritz(BlockEngine& e, double* out) {
+  const int k = e.k, kk = k * k;
+  int nb = 0;
+  for (auto& b : e.sec) nb = std::max(nb, b.blocks);
+  DH_CHECK(nb >= 1, DH_ERR_STATE, "no block step has been run");
+  // per-sector coefficient matrices, padded to nb blocks: Cs[(b * k + j) * k + c]
+  std::vector<double> C((size_t)e.nsec * nb * kk, 0.0);
+  for (int s = 0; s < e.nsec; ++s) {
+    const BlockSector& b = e.sec[s];
+    if (b.blocks == 0) continue;
+    std::vector<double> cs, vals;
+    int rc = sector_ritz_coefficients(e, b, k, cs, vals);
+    if (rc != DH_OK) return rc;
+    std::copy(cs.begin(), cs.end(), C.begin() + (size_t)s * nb * kk);
+  }
+  DevBuf dC;
+  int rc;
+  if ((rc = dC.alloc(C.size() * sizeof(double))) != DH_OK) return rc;
+  DH_CUDA(cudaMemcpyAsync(dC.ptr, C.data(), C.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+  const long long stride = e.total * k;
+  if (nb <= e.store_cap) {
+    rc = launch_seg_combine_blocks(e.store.as<double>(), nb, stride, dC.as<double>(), nb * kk, k, e.tiles, out, e.stream);
+    if (rc != DH_OK) return rc;
+    DH_CUDA(cudaStreamSynchronize(e.stream));
+    return DH_OK;
+  }
+  // replay: V_0 = start block; V_{j+1} = (H V_j - V_j A_j - V_{j-1} B_j^T) inv1_j inv2_j
+  DH_CUDA(cudaMemsetAsync(out, 0, (size_t)stride * sizeof(double), e.stream));
+  double* V = e.slot[0];
+  double* W = e.slot[1];
+  double* Vp = e.slot[2];
+  DH_CUDA(cudaMemcpyAsync(V, e.start_block.ptr, (size_t)stride * sizeof(double), cudaMemcpyDeviceToDevice, e.stream));
+  if (e.precision == DH_PRECISION_FP32 && (rc = launch_f32_copy(V, e.x32.as<float>(), stride, e.stream)) != DH_OK)
+    return rc;
+  DevBuf dm;
+  if ((rc = dm.alloc((size_t)e.nsec * kk * 4 * sizeof(double))) != DH_OK) return rc;
+  double* dNegC = dm.as<double>();
+  double* dA = dNegC + (size_t)e.nsec * kk;
+  double* dBt = dA + (size_t)e.nsec * kk;
+  double* dInv = dBt + (size_t)e.nsec * kk;
+  std::vector<double> negc((size_t)e.nsec * kk);
+  for (int j = 0; j < nb; ++j) {
+    // out += V_j C_j   (seg_update subtracts V * M, so M = -C_j)
+    for (int s = 0; s < e.nsec; ++s)
+      for (int i = 0; i < kk; ++i) negc[(size_t)s * kk + i] = -C[(size_t)s * nb * kk + (size_t)j * kk + i];
+    DH_CUDA(cudaMemcpyAsync(dNegC, negc.data(), negc.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+    if ((rc = launch_seg_update(out, V, dNegC, nullptr, nullptr, k, e.tiles, e.stream)) != DH_OK) return rc;
+    if (j + 1 == nb) break;
+    const StepRecord& h = e.history[j];
+    if ((rc = engine_product(e, V, W)) != DH_OK) return rc;
+    DH_CUDA(cudaMemcpyAsync(dA, h.A.data(), h.A.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+    DH_CUDA(cudaMemcpyAsync(dBt, h.Bt.data(), h.Bt.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+    if ((rc = launch_seg_update(W, V, dA, h.have_prev ? Vp : nullptr, h.have_prev ? dBt : nullptr, k, e.tiles,
+                                e.stream)) != DH_OK)
+      return rc;
+    DH_CUDA(cudaMemcpyAsync(dInv, h.inv1.data(), h.inv1.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+    if ((rc = launch_seg_rmul(W, dInv, k, e.tiles, nullptr, e.stream)) != DH_OK) return rc;
+    DH_CUDA(cudaStreamSynchronize(e.stream));
+    DH_CUDA(cudaMemcpyAsync(dInv, h.inv2.data(), h.inv2.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+    if ((rc = launch_seg_rmul(W, dInv, k, e.tiles, e.x32.as<float>(), e.stream)) != DH_OK) return rc;
+    DH_CUDA(cudaStreamSynchronize(e.stream));
+    double* t = Vp;
+    Vp = V;
+    V = W;
+    W = t;
+  }
+  DH_CUDA(cudaStreamSynchronize(e.stream));
+  return DH_OK;
 }
 
 // the reference's per-call bookkeeping (BasicBlockLanczosAlgorithm.cc:683-697) and TestConvergence
@@ -433,6 +562,279 @@ int dense_lowest(dh_space_s* sp, const SectorBatchHost& hb, int nev, std::vector
   rc = symmetric_eigen((int)d, H.data(), out.data(), nullptr);
   out.resize(std::min<long long>(d, std::max(nev, 1)));
   return rc;
+}
+
+
+// ------------------------------------------------------------------ one Hamiltonian
+
+// BasicBlockLanczosAlgorithm on one Hamiltonian: the engine with a single sector spanning the
+// whole space, products through the Hamiltonian's own kernels on [dim][k] blocks.
+struct BlockLanczos {
+  dh_hamiltonian_s* h = nullptr;
+  BlockEngine e;
+  int nev = 1, k = 1, max_iter = 0;
+  bool initialized = false;
+  bool keep = true;        // keep every block on the device when they fit
+  bool ritz_valid = false;
+  DevBuf ritz;             // the k lowest Ritz vectors, [dim][k]
+  DevBuf stage;            // one vector, for host input and output
+  ~BlockLanczos() {
+    if (e.stream) {
+      cudaStreamSynchronize(e.stream);
+      cudaStreamDestroy(e.stream);
+    }
+  }
+};
+
+namespace {
+
+int bl_ensure_x32(BlockLanczos* b) {
+  BlockEngine& e = b->e;
+  return ensure_buffer(e.x32, (size_t)e.total * e.k * sizeof(float));
+}
+
+int bl_allocate_store(BlockLanczos* b) {
+  BlockEngine& e = b->e;
+  e.store.release();
+  e.store_cap = 0;
+  if (!b->keep) return DH_OK;
+  const int cap = b->max_iter / b->k + 3;
+  const size_t bytes = (size_t)cap * e.total * e.k * sizeof(double);
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  if (bytes < free_b / 2) {
+    if (e.store.alloc(bytes) == DH_OK) e.store_cap = cap;
+    else cudaGetLastError();
+  }
+  return DH_OK;
+}
+
+// the reference's TestConvergence (BasicBlockLanczosAlgorithm.cc:731), or an exhausted Krylov space
+bool bl_converged(const BlockLanczos* b) {
+  const BlockSector& s = b->e.sec[0];
+  if (s.exhausted && s.blocks > 0) return true;
+  if ((int)s.ritz.size() <= b->nev) return false;
+  const double l = s.ritz[b->nev - 1];
+  return fabs(l - s.prev_last) < b->e.eig_precision * fabs(l);
+}
+
+int bl_ritz_block(BlockLanczos* b) {
+  if (b->ritz_valid) return DH_OK;
+  BlockEngine& e = b->e;
+  int rc;
+  if ((rc = ensure_buffer(b->ritz, (size_t)e.total * e.k * sizeof(double))) != DH_OK) return rc;
+  const bool replay = e.sec[0].blocks > e.store_cap;
+  if ((rc = engine_ritz(e, b->ritz.as<double>())) != DH_OK) return rc;
+  if (replay) b->initialized = false;  // the replay overwrote the work blocks
+  b->ritz_valid = true;
+  return DH_OK;
+}
+
+}  // namespace
+
+int block_lanczos_create(dh_hamiltonian_s* h, int nev, int k, int max_iter, BlockLanczos** out) {
+  *out = nullptr;
+  DH_CHECK(k == 1 || k == 2 || k == 4, DH_ERR_UNSUPPORTED, "block size %d not in {1, 2, 4}", k);
+  BlockLanczos* b = new (std::nothrow) BlockLanczos();
+  DH_CHECK(b, DH_ERR_MEMORY, "out of host memory");
+  b->h = h;
+  b->nev = nev;
+  b->k = k;
+  b->max_iter = max_iter;
+  BlockEngine& e = b->e;
+  e.k = k;
+  e.nev = nev;
+  e.max_iter = max_iter;
+  e.precision = h->precision;
+  int rc = DH_OK;
+  if (cudaStreamCreateWithFlags(&e.stream, cudaStreamNonBlocking) != cudaSuccess) {
+    e.stream = 0;
+    rc = cuda_fail(cudaGetLastError(), "cudaStreamCreate", __FILE__, __LINE__);
+  }
+  if (rc == DH_OK) rc = engine_setup(e, std::vector<long long>{(long long)h->space->dim});
+  if (rc == DH_OK) rc = bl_allocate_store(b);
+  if (rc != DH_OK) {
+    delete b;
+    return rc;
+  }
+  e.product = [b](const double* x64, const float* x32, double* y) {
+    return hamiltonian_apply_block(b->h, x64, x32, y, b->k, b->e.precision, b->e.stream);
+  };
+  *out = b;
+  return DH_OK;
+}
+
+void block_lanczos_destroy(BlockLanczos* b) { delete b; }
+
+int block_lanczos_set_storage(BlockLanczos* b, int keep) {
+  b->keep = keep != 0;
+  b->initialized = false;
+  b->ritz_valid = false;
+  return bl_allocate_store(b);
+}
+
+void block_lanczos_set_precision(BlockLanczos* b, double precision) { b->e.eig_precision = precision; }
+
+int block_lanczos_initialize(BlockLanczos* b, const double* vectors, int nbr_vectors, uint64_t seed) {
+  BlockEngine& e = b->e;
+  const long long dim = e.total;
+  int rc;
+  e.precision = b->h->precision;
+  if (e.precision == DH_PRECISION_FP32 && (rc = bl_ensure_x32(b)) != DH_OK) return rc;
+  if ((rc = launch_random_block(e.slot[0], dim, e.k, e.row_offset_dev, e.tiles, seed, e.stream)) != DH_OK) return rc;
+  const int given = vectors ? std::min(nbr_vectors, e.k) : 0;
+  for (int j = 0; j < given; ++j) {
+    const double* src = vectors + (size_t)j * dim;
+    if (!is_device_pointer(vectors)) {
+      if ((rc = ensure_buffer(b->stage, (size_t)dim * sizeof(double))) != DH_OK) return rc;
+      DH_CUDA(cudaMemcpyAsync(b->stage.ptr, src, (size_t)dim * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+      src = b->stage.as<double>();
+    }
+    if ((rc = launch_put_column(src, dim, e.k, j, e.slot[0], e.stream)) != DH_OK) return rc;
+  }
+  e.sec[0].exhausted = false;
+  if ((rc = engine_start(e)) != DH_OK) return rc;
+  DH_CHECK(!e.sec[0].exhausted, DH_ERR_ARGUMENT, "the start block is linearly dependent");
+  b->initialized = true;
+  b->ritz_valid = false;
+  return DH_OK;
+}
+
+// RunLanczosAlgorithm(nbrIter) (BasicBlockLanczosAlgorithm.cc:524-697): nbrIter block steps, at least
+// two on the first call, then the band matrix is diagonalised with the reference's bookkeeping
+int block_lanczos_run(BlockLanczos* b, int nbr_iter) {
+  DH_CHECK(b->initialized, DH_ERR_STATE, "RunLanczosAlgorithm before InitializeLanczosAlgorithm");
+  BlockEngine& e = b->e;
+  BlockSector& s = e.sec[0];
+  DH_CHECK(!(s.exhausted && s.blocks > 0), DH_ERR_STATE, "the block Krylov space is exhausted (the result is exact)");
+  if (e.precision == DH_PRECISION_FP32) DH_CHECK(e.x32.ptr, DH_ERR_STATE, "FP32 copy missing");
+  int n = s.blocks == 0 ? std::max(nbr_iter, 2) : nbr_iter;
+  int rc;
+  for (int i = 0; i < n; ++i) {
+    if ((rc = engine_step(e)) != DH_OK) return rc;
+    if (s.exhausted) {
+      s.active = false;
+      break;
+    }
+  }
+  b->ritz_valid = false;
+  return sector_evaluate(e, s);
+}
+
+bool block_lanczos_converged(const BlockLanczos* b) { return bl_converged(b); }
+
+const std::vector<double>& block_lanczos_ritz(const BlockLanczos* b) { return b->e.sec[0].ritz; }
+
+int block_lanczos_eigenstates(BlockLanczos* b, int n, double* out) {
+  BlockEngine& e = b->e;
+  DH_CHECK(n >= 1 && n <= e.k, DH_ERR_ARGUMENT, "%d eigenstates asked of a block of %d", n, e.k);
+  DH_CHECK(e.sec[0].blocks >= 1, DH_ERR_STATE, "no Lanczos iteration has been run");
+  int rc;
+  if ((rc = bl_ritz_block(b)) != DH_OK) return rc;
+  std::vector<double> g;
+  if ((rc = engine_gram(e, b->ritz.as<double>(), b->ritz.as<double>(), g)) != DH_OK) return rc;
+  const long long dim = e.total;
+  const bool dev = is_device_pointer(out);
+  if (!dev && (rc = ensure_buffer(b->stage, (size_t)dim * sizeof(double))) != DH_OK) return rc;
+  for (int c = 0; c < n; ++c) {
+    const double nrm = sqrt(g[(size_t)c * e.k + c]);
+    DH_CHECK(nrm > 0.0, DH_ERR_STATE, "Ritz vector %d vanishes", c);
+    double* dst = dev ? out + (size_t)c * dim : b->stage.as<double>();
+    if ((rc = launch_get_column(b->ritz.as<double>(), dim, e.k, c, 1.0 / nrm, dst, e.stream)) != DH_OK) return rc;
+    if (!dev)
+      DH_CUDA(cudaMemcpyAsync(out + (size_t)c * dim, dst, (size_t)dim * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+    DH_CUDA(cudaStreamSynchronize(e.stream));
+  }
+  return DH_OK;
+}
+
+void block_lanczos_counters(const BlockLanczos* b, int64_t* products, int* rows) {
+  if (products) *products = b->e.products * b->k;
+  if (rows) *rows = b->e.sec[0].blocks * b->k;
+}
+
+// the driver loop of QHEOnSphereMainTask.cc:732-753 with a block algorithm: RunLanczosAlgorithm
+// (nev + 2), counter (nev + 3) k, then RunLanczosAlgorithm(1) and k more until converged
+int block_lanczos_solve(BlockLanczos* b, int max_iter, double* eigenvalues, int* iterations, int* converged) {
+  DH_CHECK(b->initialized, DH_ERR_STATE, "solve before InitializeLanczosAlgorithm");
+  if (max_iter > b->max_iter) max_iter = b->max_iter;
+  int rc = block_lanczos_run(b, b->nev + 2);
+  if (rc != DH_OK) return rc;
+  int count = (b->nev + 3) * b->k;
+  while (!bl_converged(b) && count < max_iter) {
+    count += b->k;
+    if ((rc = block_lanczos_run(b, 1)) != DH_OK) return rc;
+  }
+  const std::vector<double>& r = b->e.sec[0].ritz;
+  for (int i = 0; i < b->nev; ++i) eigenvalues[i] = i < (int)r.size() ? r[i] : NAN;
+  *iterations = count;
+  *converged = bl_converged(b) ? 1 : 0;
+  return DH_OK;
+}
+
+// FP32 products with the FP64 block recurrence to the FP32 resolution of the Ritz values, then the
+// Ritz block's FP64 Rayleigh quotients and residuals; while |r_0|^2 > precision |E_0| an FP64 block
+// Lanczos restarted from the Ritz block polishes the energy.
+int block_lanczos_solve_refined(BlockLanczos* b, int max_iter, double precision, double* out) {
+  BlockEngine& e = b->e;
+  DH_CHECK(b->initialized && e.sec[0].blocks == 0, DH_ERR_STATE, "refined solve needs a freshly initialised algorithm");
+  const double saved_precision = e.eig_precision;
+  const long long dim = e.total;
+  const int k = e.k;
+  int rc;
+  if ((rc = bl_ensure_x32(b)) != DH_OK) return rc;
+  e.precision = DH_PRECISION_FP32;
+  if ((rc = launch_f32_copy(e.slot[e.slot_cur], e.x32.as<float>(), dim * k, e.stream)) != DH_OK) return rc;
+  e.eig_precision = std::max(precision, 1e-9);
+  std::vector<double> eig(b->nev);
+  int iters = 0, conv = 0;
+  rc = block_lanczos_solve(b, max_iter, eig.data(), &iters, &conv);
+  const long long fp32_products = e.products;
+  const double e32 = eig[0];
+  if (rc == DH_OK) rc = bl_ritz_block(b);
+  e.precision = DH_PRECISION_FP64;
+  double energy = e32, rnorm = 0.0;
+  if (rc == DH_OK) {
+    // H X in FP64, E_c = <x_c|H x_c> / <x_c|x_c>, R = H X - X diag(E), |r_0| / |x_0|
+    double* X = b->ritz.as<double>();
+    double* Y = e.slot[(e.slot_cur + 1) % 3];
+    std::vector<double> g, a, rr;
+    rc = engine_product(e, X, Y);
+    if (rc == DH_OK) rc = engine_gram(e, X, X, g);
+    if (rc == DH_OK) rc = engine_gram(e, X, Y, a);
+    if (rc == DH_OK) {
+      std::vector<double> d((size_t)k * k, 0.0);
+      for (int c = 0; c < k; ++c) d[(size_t)c * k + c] = a[(size_t)c * k + c] / g[(size_t)c * k + c];
+      energy = d[0];
+      double* dA = e.small.as<double>() + 2 * (size_t)e.nsec * k * k;
+      if (cudaMemcpyAsync(dA, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream) != cudaSuccess)
+        rc = cuda_fail(cudaGetLastError(), "copy", __FILE__, __LINE__);
+      if (rc == DH_OK) rc = launch_seg_update(Y, X, dA, nullptr, nullptr, k, e.tiles, e.stream);
+      if (rc == DH_OK) rc = engine_gram(e, Y, Y, rr);
+      if (rc == DH_OK) rnorm = sqrt(std::max(rr[0], 0.0) / g[0]);
+    }
+  }
+  if (rc == DH_OK && rnorm * rnorm > precision * std::max(fabs(energy), 1e-300)) {
+    DH_CUDA(cudaMemcpyAsync(e.slot[0], b->ritz.ptr, (size_t)dim * k * sizeof(double), cudaMemcpyDeviceToDevice, e.stream));
+    e.sec[0].exhausted = false;
+    rc = engine_start(e);
+    if (rc == DH_OK) {
+      b->initialized = true;
+      b->ritz_valid = false;
+      e.eig_precision = precision;
+      rc = block_lanczos_solve(b, std::min(max_iter, 60 * k), eig.data(), &iters, &conv);
+      if (rc == DH_OK) energy = eig[0];
+    }
+  }
+  e.precision = b->h->precision;
+  e.eig_precision = saved_precision;
+  if (rc != DH_OK) return rc;
+  out[0] = energy;
+  out[1] = e32;
+  out[2] = rnorm;
+  out[3] = (double)(fp32_products * k);
+  out[4] = (double)((e.products - fp32_products) * k);
+  return DH_OK;
 }
 
 }  // namespace dh

@@ -42,8 +42,10 @@ struct dh_lanczos_s {
   std::vector<double> alpha, beta, ritz;
   int64_t matvecs = 0;
   cudaGraphExec_t graph3 = nullptr;  // three iterations starting at phase 0
+  dh::BlockLanczos* blk = nullptr;   // DH_LANCZOS_BLOCK: everything runs in the block engine
   ~dh_lanczos_s() {
     if (graph3) cudaGraphExecDestroy(graph3);
+    if (blk) dh::block_lanczos_destroy(blk);
   }
 };
 
@@ -248,13 +250,27 @@ int dh_lanczos_create(dh_hamiltonian_t h, int algorithm, int nbr_eigenvalue, int
   *out = nullptr;
   DH_CHECK(h, DH_ERR_ARGUMENT, "null hamiltonian");
   DH_CHECK(algorithm == DH_LANCZOS_BASIC || algorithm == DH_LANCZOS_FULL_REORTHOGONALIZED ||
-               algorithm == DH_LANCZOS_WITH_GROUND_STATE,
-           DH_ERR_UNSUPPORTED, "algorithm %d: use dh_block_lanczos_* for block Lanczos", algorithm);
+               algorithm == DH_LANCZOS_WITH_GROUND_STATE || algorithm == DH_LANCZOS_BLOCK,
+           DH_ERR_UNSUPPORTED, "unknown algorithm %d", algorithm);
   DH_CHECK(nbr_eigenvalue >= 1, DH_ERR_ARGUMENT, "nbr_eigenvalue must be >= 1");
   DH_CHECK(max_iter >= nbr_eigenvalue + 3, DH_ERR_ARGUMENT, "max_iter must be >= nbr_eigenvalue + 3");
-  (void)block_size;
   dh_lanczos_s* l = new (std::nothrow) dh_lanczos_s();
   DH_CHECK(l, DH_ERR_MEMORY, "out of host memory");
+  if (algorithm == DH_LANCZOS_BLOCK) {
+    l->h = h;
+    l->algorithm = algorithm;
+    l->nev = nbr_eigenvalue;
+    l->block = block_size;
+    l->max_iter = max_iter;
+    l->dim = h->space->dim;
+    int rc = block_lanczos_create(h, nbr_eigenvalue, block_size, max_iter, &l->blk);
+    if (rc != DH_OK) {
+      delete l;
+      return rc;
+    }
+    *out = l;
+    return DH_OK;
+  }
   l->h = h;
   l->algorithm = algorithm;
   l->nev = nbr_eigenvalue;
@@ -319,6 +335,7 @@ int dh_lanczos_destroy(dh_lanczos_t l) {
 
 int dh_lanczos_set_vector_storage(dh_lanczos_t l, int keep) {
   DH_CHECK(l, DH_ERR_ARGUMENT, "null lanczos");
+  if (l->blk) return block_lanczos_set_storage(l->blk, keep);
   DH_CHECK(l->algorithm != DH_LANCZOS_FULL_REORTHOGONALIZED || keep, DH_ERR_ARGUMENT,
            "full re-orthogonalisation needs its vectors");
   if (!keep) {
@@ -342,11 +359,13 @@ int dh_lanczos_set_vector_storage(dh_lanczos_t l, int keep) {
 int dh_lanczos_set_eigenvalue_precision(dh_lanczos_t l, double precision) {
   DH_CHECK(l && precision > 0.0, DH_ERR_ARGUMENT, "bad argument");
   l->precision = precision;
+  if (l->blk) block_lanczos_set_precision(l->blk, precision);
   return DH_OK;
 }
 
 int dh_lanczos_initialize(dh_lanczos_t l, const double* vectors, int nbr_vectors) {
   DH_CHECK(l && vectors && nbr_vectors >= 1, DH_ERR_ARGUMENT, "bad argument");
+  if (l->blk) return block_lanczos_initialize(l->blk, vectors, nbr_vectors, 0);
   const cudaMemcpyKind kind = is_device_pointer(vectors) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   DH_CUDA(cudaMemcpyAsync(l->st.vec, vectors, l->dim * sizeof(double), kind, l->stream));
   return lz_initialize_device(l);
@@ -354,6 +373,7 @@ int dh_lanczos_initialize(dh_lanczos_t l, const double* vectors, int nbr_vectors
 
 int dh_lanczos_initialize_random(dh_lanczos_t l, uint64_t seed) {
   DH_CHECK(l, DH_ERR_ARGUMENT, "null lanczos");
+  if (l->blk) return block_lanczos_initialize(l->blk, nullptr, 0, seed);
   int rc = launch_random_vector(l->st.vec, l->dim, seed, l->stream);
   if (rc != DH_OK) return rc;
   return lz_initialize_device(l);
@@ -361,31 +381,35 @@ int dh_lanczos_initialize_random(dh_lanczos_t l, uint64_t seed) {
 
 int dh_lanczos_run(dh_lanczos_t l, int nbr_iter) {
   DH_CHECK(l && nbr_iter >= 1, DH_ERR_ARGUMENT, "bad argument");
+  if (l->blk) return block_lanczos_run(l->blk, nbr_iter);
   return lz_run(l, nbr_iter);
 }
 
 int dh_lanczos_test_convergence(dh_lanczos_t l, int* converged) {
   DH_CHECK(l && converged, DH_ERR_ARGUMENT, "null argument");
-  *converged = lz_converged(l) ? 1 : 0;
+  *converged = (l->blk ? block_lanczos_converged(l->blk) : lz_converged(l)) ? 1 : 0;
   return DH_OK;
 }
 
 int dh_lanczos_get_eigenvalues(dh_lanczos_t l, double* eigenvalues, int n) {
   DH_CHECK(l && eigenvalues, DH_ERR_ARGUMENT, "null argument");
-  DH_CHECK(n >= 0 && n <= (int)l->ritz.size(), DH_ERR_ARGUMENT, "only %d Ritz values", (int)l->ritz.size());
-  for (int i = 0; i < n; ++i) eigenvalues[i] = l->ritz[i];
+  const std::vector<double>& ritz = l->blk ? block_lanczos_ritz(l->blk) : l->ritz;
+  DH_CHECK(n >= 0 && n <= (int)ritz.size(), DH_ERR_ARGUMENT, "only %d Ritz values", (int)ritz.size());
+  for (int i = 0; i < n; ++i) eigenvalues[i] = ritz[i];
   return DH_OK;
 }
 
 int dh_lanczos_get_ground_state_energy(dh_lanczos_t l, double* energy) {
   DH_CHECK(l && energy, DH_ERR_ARGUMENT, "null argument");
-  DH_CHECK(!l->ritz.empty(), DH_ERR_STATE, "no Lanczos iteration has been run");
-  *energy = l->ritz[0];
+  const std::vector<double>& ritz = l->blk ? block_lanczos_ritz(l->blk) : l->ritz;
+  DH_CHECK(!ritz.empty(), DH_ERR_STATE, "no Lanczos iteration has been run");
+  *energy = ritz[0];
   return DH_OK;
 }
 
 int dh_lanczos_get_ground_state(dh_lanczos_t l, double* vec) {
   DH_CHECK(l && vec, DH_ERR_ARGUMENT, "null argument");
+  if (l->blk) return block_lanczos_eigenstates(l->blk, 1, vec);
   int rc = lz_ground_state(l);
   if (rc != DH_OK) return rc;
   const cudaMemcpyKind kind = is_device_pointer(vec) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
@@ -394,8 +418,45 @@ int dh_lanczos_get_ground_state(dh_lanczos_t l, double* vec) {
   return DH_OK;
 }
 
+int dh_lanczos_get_eigenstates(dh_lanczos_t l, int n, double* vecs) {
+  DH_CHECK(l && vecs, DH_ERR_ARGUMENT, "null argument");
+  if (l->blk) return block_lanczos_eigenstates(l->blk, n, vecs);
+  DH_CHECK(n >= 1 && n <= l->rows, DH_ERR_ARGUMENT, "%d eigenstates asked of %d Lanczos rows", n, l->rows);
+  if (n == 1) return dh_lanczos_get_ground_state(l, vecs);
+  DH_CHECK(l->st.krylov && l->rows <= l->krylov_cap, DH_ERR_UNSUPPORTED,
+           "more than one eigenstate needs the stored Krylov vectors");
+  const int m = l->rows;
+  std::vector<double> eig(m), z((size_t)m * m);
+  int rc = tridiagonal_eigen(m, l->alpha.data(), l->beta.data(), eig.data(), z.data());
+  if (rc != DH_OK) return rc;
+  if ((rc = ensure_buffer(l->ground, l->dim * sizeof(double))) != DH_OK) return rc;
+  if ((rc = ensure_buffer(l->coef, (size_t)std::max(m, l->cap + 8) * sizeof(double))) != DH_OK) return rc;
+  const bool dev = is_device_pointer(vecs);
+  double* g = l->ground.as<double>();
+  for (int c = 0; c < n; ++c) {
+    double* dst = dev ? vecs + (size_t)c * l->dim : g;
+    DH_CUDA(cudaMemcpyAsync(l->coef.ptr, z.data() + (size_t)c * m, m * sizeof(double), cudaMemcpyHostToDevice, l->stream));
+    if ((rc = launch_combine(l->st.krylov, m, l->dim, l->coef.as<double>(), 1.0, dst, 0, l->dim, l->stream)) != DH_OK)
+      return rc;
+    const double* vs[1] = {dst};
+    double* nrm = l->coef.as<double>() + m;
+    if ((rc = launch_multi_dot(vs, 1, dst, l->dim, nrm, l->red, l->stream)) != DH_OK) return rc;
+    if ((rc = launch_sqrt_inplace(nrm, l->stream)) != DH_OK) return rc;
+    if ((rc = launch_scale_convert(dst, nullptr, nrm, l->dim, l->stream)) != DH_OK) return rc;
+    if (!dev)
+      DH_CUDA(cudaMemcpyAsync(vecs + (size_t)c * l->dim, dst, l->dim * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
+    DH_CUDA(cudaStreamSynchronize(l->stream));
+  }
+  l->ground_valid = false;  // the ground-state buffer now holds the last vector
+  return DH_OK;
+}
+
 int dh_lanczos_get_counters(dh_lanczos_t l, int64_t* matvecs, int* rows) {
   DH_CHECK(l, DH_ERR_ARGUMENT, "null lanczos");
+  if (l->blk) {
+    block_lanczos_counters(l->blk, matvecs, rows);
+    return DH_OK;
+  }
   if (matvecs) *matvecs = l->matvecs;
   if (rows) *rows = l->rows;
   return DH_OK;
@@ -404,6 +465,7 @@ int dh_lanczos_get_counters(dh_lanczos_t l, int64_t* matvecs, int* rows) {
 int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eigenvalues, int* iterations,
                      int* converged) {
   DH_CHECK(l && eigenvalues && iterations && converged, DH_ERR_ARGUMENT, "null argument");
+  if (l->blk) return block_lanczos_solve(l->blk, max_iter, eigenvalues, iterations, converged);
   DH_CHECK(l->initialized, DH_ERR_STATE, "solve before InitializeLanczosAlgorithm");
   if (max_iter > l->max_iter) max_iter = l->max_iter;
   int rc;
@@ -477,8 +539,9 @@ int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eige
 
 int dh_lanczos_solve_refined(dh_lanczos_t l, int max_iter, double precision, double* out) {
   DH_CHECK(l && out, DH_ERR_ARGUMENT, "null argument");
-  DH_CHECK(l->initialized, DH_ERR_STATE, "solve before InitializeLanczosAlgorithm");
   DH_CHECK(precision > 0.0, DH_ERR_ARGUMENT, "precision must be > 0");
+  if (l->blk) return block_lanczos_solve_refined(l->blk, max_iter, precision, out);
+  DH_CHECK(l->initialized, DH_ERR_STATE, "solve before InitializeLanczosAlgorithm");
   dh_hamiltonian_s* h = l->h;
   const int saved_precision = h->precision;
   const double saved_lz_precision = l->precision;

@@ -238,6 +238,38 @@ int hamiltonian_apply(dh_hamiltonian_s* h, const double* x, double* y, int nvec,
   return launch_spin_matvec(spin_device(sp, h), a, h->precision, stream);
 }
 
+int hamiltonian_apply_block(dh_hamiltonian_s* h, const double* x64, const float* x32, double* y, int k, int precision,
+                            cudaStream_t stream) {
+  dh_space_s* sp = h->space;
+  MatvecArgs a = {};
+  a.y = y;
+  a.ld = k;
+  a.vstride = 1;
+  a.ld_y = k;
+  a.vstride_y = 1;
+  a.nbr_vectors = k;
+  a.shift = h->shift;
+  a.col_first = 0;
+  a.col_last = sp->dim;
+  a.row_first = 0;
+  a.row_last = sp->dim;
+  a.accumulate = 0;
+  if (precision == DH_PRECISION_FP32) {
+    DH_CHECK(x32, DH_ERR_STATE, "FP32 product without an FP32 copy of the block");
+    a.x = x32;
+    a.xdiag = x64;
+  } else {
+    a.x = x64;
+    a.xdiag = nullptr;
+  }
+  int rc;
+  if (sp->kind == SPACE_FERMION) {
+    if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
+    return launch_fqhe_matvec(fqhe_device(sp, h, precision), a, precision, stream);
+  }
+  return launch_spin_matvec(spin_device(sp, h), a, precision, stream);
+}
+
 }  // namespace dh
 
 // ===================================================================== C ABI

@@ -145,6 +145,9 @@ int launch_seg_combine_blocks(const double* blocks, int nb, long long stride, co
 int launch_random_block(double* x, long long rows, int k, const long long* row_sector_base, const TileSetDevice& t,
                         uint64_t seed, cudaStream_t s);
 int launch_f32_copy(const double* x, float* y, long long n, cudaStream_t s);
+// x[i][col] = v[i] and v[i] = scale * x[i][col] for a [n][k] block x
+int launch_put_column(const double* v, long long n, int k, int col, double* x, cudaStream_t s);
+int launch_get_column(const double* x, long long n, int k, int col, double scale, double* v, cudaStream_t s);
 // eigenvalues (ascending) of a symmetric band matrix of half-bandwidth b stored densely (row-major,
 // destroyed): Givens reduction to tridiagonal form touching only the band, then implicit QL
 int band_eigenvalues(int n, int b, double* a, double* eig);

@@ -57,4 +57,25 @@ int upload_factors(dh_hamiltonian_s* h);
 // y (+)= H x for nvec vectors stored one after the other; x32_ready: FP32 copy of x if already made
 int hamiltonian_apply(dh_hamiltonian_s* h, const double* x, double* y, int nvec, int64_t first, int64_t nbr,
                       int accumulate, const float* x32_ready, cudaStream_t stream);
+// y = H x for a [dim][k] block (x64 FP64; x32 its FP32 copy, used when precision is FP32)
+int hamiltonian_apply_block(dh_hamiltonian_s* h, const double* x64, const float* x32, double* y, int k, int precision,
+                            cudaStream_t stream);
+
+// block Lanczos on one Hamiltonian (the engine of the batched sectors with a single sector)
+struct BlockLanczos;
+int block_lanczos_create(dh_hamiltonian_s* h, int nev, int k, int max_iter, BlockLanczos** out);
+void block_lanczos_destroy(BlockLanczos* b);
+int block_lanczos_set_storage(BlockLanczos* b, int keep);
+void block_lanczos_set_precision(BlockLanczos* b, double precision);
+// vectors: nbr_vectors vectors one after the other (host or device), the rest of the block random
+// from seed; vectors == nullptr: the whole block random
+int block_lanczos_initialize(BlockLanczos* b, const double* vectors, int nbr_vectors, uint64_t seed);
+int block_lanczos_run(BlockLanczos* b, int nbr_iter);
+bool block_lanczos_converged(const BlockLanczos* b);
+const std::vector<double>& block_lanczos_ritz(const BlockLanczos* b);
+// the n lowest Ritz vectors (n <= k), normalised, one after the other (host or device)
+int block_lanczos_eigenstates(BlockLanczos* b, int n, double* out);
+void block_lanczos_counters(const BlockLanczos* b, int64_t* products, int* rows);
+int block_lanczos_solve(BlockLanczos* b, int max_iter, double* eigenvalues, int* iterations, int* converged);
+int block_lanczos_solve_refined(BlockLanczos* b, int max_iter, double precision, double* out);
 }  // namespace dh

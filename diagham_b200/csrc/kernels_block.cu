@@ -176,6 +176,17 @@ __global__ void random_block_kernel(double* x, long long rows, int k, const long
   (void)rows;
 }
 
+// column col of a [n][k] block from / to a contiguous vector (scaled on the way out)
+__global__ void put_column_kernel(const double* v, long long n, int k, int col, double* x) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) x[i * k + col] = v[i];
+}
+
+__global__ void get_column_kernel(const double* x, long long n, int k, int col, double scale, double* v) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) v[i] = scale * x[i * k + col];
+}
+
 __global__ void f32_copy_kernel(const double* x, float* y, long long n) {
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) y[i] = (float)x[i];
@@ -250,6 +261,27 @@ int launch_random_block(double* x, long long rows, int k, const long long* row_s
                         uint64_t seed, cudaStream_t s) {
   if (t.nbr_tiles <= 0) return DH_OK;
   random_block_kernel<<<t.nbr_tiles, kThreads, 0, s>>>(x, rows, k, row_sector_base, t, seed);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+static unsigned stream_grid(long long n) {
+  long long g = (n + 255) / 256;
+  if (g > 148 * 16) g = 148 * 16;
+  if (g < 1) g = 1;
+  return (unsigned)g;
+}
+
+int launch_put_column(const double* v, long long n, int k, int col, double* x, cudaStream_t s) {
+  if (n <= 0) return DH_OK;
+  put_column_kernel<<<stream_grid(n), 256, 0, s>>>(v, n, k, col, x);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_get_column(const double* x, long long n, int k, int col, double scale, double* v, cudaStream_t s) {
+  if (n <= 0) return DH_OK;
+  get_column_kernel<<<stream_grid(n), 256, 0, s>>>(x, n, k, col, scale, v);
   DH_CUDA(cudaGetLastError());
   return DH_OK;
 }

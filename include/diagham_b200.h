@@ -184,7 +184,12 @@ int dh_hamiltonian_get_interaction_factors(dh_hamiltonian_t h, double* factors, 
  * (src/LanczosAlgorithm/AbstractLanczosAlgorithm.h:45-120) with the recurrence of
  * BasicLanczosAlgorithm.cc:148-216, FullReorthogonalizedLanczosAlgorithm.cc:209-323,
  * BasicBlockLanczosAlgorithm.cc:524-697 or BasicLanczosAlgorithmWithGroundState.cc:256-335.
- * Lanczos vectors stay in FP64 in device memory. */
+ * Lanczos vectors stay in FP64 in device memory.  block_size (1, 2 or 4) is used by
+ * DH_LANCZOS_BLOCK only: the block is stored row-interleaved and one product enumerates each row's
+ * matrix elements once for the whole block; max_iter counts vectors, as the reference's --iter-max,
+ * and RunLanczosAlgorithm counts block steps.  The block algorithm keeps every block when they fit
+ * in half of the free device memory, otherwise it rebuilds Ritz vectors by replaying its recorded
+ * steps. */
 int dh_lanczos_create(dh_hamiltonian_t h, int algorithm, int nbr_eigenvalue, int block_size, int max_iter,
                       dh_lanczos_t* out);
 int dh_lanczos_destroy(dh_lanczos_t l);
@@ -222,13 +227,21 @@ int dh_lanczos_get_ground_state_energy(dh_lanczos_t l, double* energy);
  * lowest Ritz value, written to vec (host or device). */
 int dh_lanczos_get_ground_state(dh_lanczos_t l, double* vec);
 
+/* GetEigenstates(nbrEigenstates) (BasicBlockLanczosAlgorithm.cc:380-500,
+ * BasicLanczosAlgorithmWithGroundState.cc:256-335): the n lowest normalised Ritz vectors, one after
+ * the other in vecs (host or device).  Block algorithms give up to block_size of them; the others
+ * need the stored Krylov vectors for n > 1. */
+int dh_lanczos_get_eigenstates(dh_lanczos_t l, int n, double* vecs);
+
 /* Number of matrix-vector products and tridiagonal rows so far. */
 int dh_lanczos_get_counters(dh_lanczos_t l, int64_t* matvecs, int* rows);
 
 /* Whole driver loop of QHEOnSphereMainTask.cc:732-753: RunLanczosAlgorithm(nbrEigenvalue + 2), then
  * RunLanczosAlgorithm(1) until TestConvergence() or max_iter iterations, issued as CUDA-graph
  * batches of `graph_batch` iterations (>= 1) whose extra iterations past convergence are discarded
- * from the reported result.  *iterations follows the reference's iteration counter. */
+ * from the reported result.  *iterations follows the reference's iteration counter (in vectors:
+ * (nbrEigenvalue + 3) block_size after the first call, + block_size per step for DH_LANCZOS_BLOCK,
+ * whose steps are never graph-batched). */
 int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eigenvalues, int* iterations,
                      int* converged);
 
@@ -236,7 +249,9 @@ int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eige
  * the Ritz vector is rebuilt from the stored Krylov basis, its FP64 Rayleigh quotient and residual
  * are taken with an FP64 product, and, while the residual bound exceeds `precision` * |E|, a short
  * FP64 Lanczos restarted from it polishes the energy.  out[0] = refined E0, out[1] = FP32-phase E0,
- * out[2] = residual norm, out[3] = FP32 matvecs, out[4] = FP64 matvecs. */
+ * out[2] = residual norm, out[3] = FP32 matvecs, out[4] = FP64 matvecs.  With DH_LANCZOS_BLOCK the
+ * whole block of Ritz vectors is refined and the FP64 restart is a block Lanczos from it; the
+ * algorithm must be freshly initialised. */
 int dh_lanczos_solve_refined(dh_lanczos_t l, int max_iter, double precision, double* out);
 
 /* ================================================================ batched sectors */

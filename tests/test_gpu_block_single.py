@@ -1,0 +1,121 @@
+"""Block Lanczos on one Hamiltonian (DH_LANCZOS_BLOCK through the Lanczos handle) against the
+reference's BasicBlockLanczosAlgorithm run (same start block), dense diagonalisation of the oracle's
+Hamiltonian and the exact Majumdar-Ghosh energy -3L/8 of the J1-J2 chain at J2 = J1/2.
+Eigenvalues within 1e-10 relative; iteration counters within two block steps of the reference
+(FP64 reduction order differs); Ritz vectors orthonormal to 1e-10."""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _fqhe(gpu, v, n=6, s=15, lz=0):
+    sp = gpu.FermionOnSphere(n, lz, s)
+    return sp, gpu.ParticleOnSphereGenericHamiltonian(sp, n, s, v)
+
+
+def _reference_block(orc, dim, k):
+    # the fixture's start block: splitmix vectors from seeds 100.. orthonormalised
+    q, _ = np.linalg.qr(np.stack([orc.random_vector(100 + b, dim) for b in range(k)], axis=1))
+    return np.ascontiguousarray(q.T)
+
+
+def test_run_loop_matches_reference(gpu, orc):
+    z = golden("lanczos_n6_2s15_lz0_coulomb_block4.npz")
+    nev, k = int(z["nev"]), 4
+    sp, H = _fqhe(gpu, z["v"])
+    lz = gpu.BasicBlockLanczosAlgorithm(H, nev, 400, block_size=k)
+    lz.InitializeLanczosAlgorithm(_reference_block(orc, sp.dim, k))
+    # the reference harness's loop (QHEOnSphereMainTask.cc:732-753 with a block algorithm)
+    lz.RunLanczosAlgorithm(nev + 2)
+    count = (nev + 3) * k
+    hist = []
+    while not lz.TestConvergence() and count < 400:
+        count += k
+        lz.RunLanczosAlgorithm(1)
+        hist.append(lz.GetEigenvalues(1)[0])
+    e, e_ref = lz.GetEigenvalues(nev), z["eigenvalues"]
+    assert np.max(np.abs(e - e_ref) / np.abs(e_ref)) < 1e-10, (e, e_ref)
+    assert abs(count - int(z["iterations"])) <= 2 * k
+    n = min(12, len(hist), len(z["history"]))
+    assert np.max(np.abs(np.array(hist[:n]) - z["history"][:n]) / np.abs(z["history"][:n])) < 1e-9
+    m, rows = lz.counters()
+    assert rows % k == 0 and m == rows
+
+
+@pytest.mark.parametrize("k", [1, 2, 4])
+def test_solve_against_dense(gpu, orc, k):
+    from test_gpu_block import dense_e0
+    v = golden("lanczos_n6_2s15_lz0_coulomb_block4.npz")["v"]
+    sp, H = _fqhe(gpu, v, lz=2)
+    lz = gpu.BasicBlockLanczosAlgorithm(H, 1, 600, block_size=k)
+    lz.InitializeLanczosAlgorithm(seed=7)
+    r = lz.solve(600)
+    ref = dense_e0(orc, 6, 15, 2, v)
+    assert r["converged"]
+    assert abs(r["eigenvalues"][0] - ref) < 1e-10 * abs(ref), (r, ref)
+
+
+@pytest.mark.parametrize("keep", [True, False])
+def test_eigenstates_stored_or_replayed(gpu, orc, keep):
+    v = golden("lanczos_n6_2s15_lz0_coulomb_block4.npz")["v"]
+    sp, H = _fqhe(gpu, v)
+    lz = gpu.BasicBlockLanczosAlgorithm(H, 2, 400, block_size=2)
+    lz.set_vector_storage(keep)
+    lz.InitializeLanczosAlgorithm(seed=3)
+    r = lz.solve(400)
+    psi = lz.GetEigenstates(2)
+    assert np.max(np.abs(psi @ psi.T - np.eye(2))) < 1e-10
+    O = orc.FQHE(6, 15, 0, v)
+    for c in range(2):
+        hpsi = O.pull(psi[c])
+        e = float(psi[c] @ hpsi)
+        assert abs(e - r["eigenvalues"][c]) < 1e-9 * abs(e)
+        assert np.linalg.norm(hpsi - e * psi[c]) < 1e-5
+    g = lz.GetGroundState()
+    assert abs(abs(float(g @ psi[0])) - 1.0) < 1e-12
+
+
+def test_stored_and_replayed_ritz_vectors_agree(gpu):
+    v = golden("lanczos_n6_2s15_lz0_coulomb_block4.npz")["v"]
+    out = []
+    for keep in (True, False):
+        sp, H = _fqhe(gpu, v)
+        lz = gpu.BasicBlockLanczosAlgorithm(H, 1, 400, block_size=4)
+        lz.set_vector_storage(keep)
+        lz.InitializeLanczosAlgorithm(seed=11)
+        lz.solve(400)
+        out.append(lz.GetGroundState())
+    assert abs(abs(float(out[0] @ out[1])) - 1.0) < 1e-12
+
+
+def test_majumdar_ghosh_chain_fp64_and_fp32_refined(gpu):
+    z = golden("spin_lanczos_L16_sz0_j1_0.5.npz")
+    exact = -3.0 * 16 / 8
+    assert abs(float(z["eigenvalues"][0]) - exact) < 1e-12
+    chain = gpu.Spin1_2Chain(16, 0)
+    H = gpu.SpinChainJ1J2Hamiltonian(chain, 1.0, 0.5)
+    lz = gpu.BasicBlockLanczosAlgorithm(H, 1, 800, block_size=2)
+    lz.InitializeLanczosAlgorithm(seed=0)
+    r = lz.solve(800)
+    assert abs(r["eigenvalues"][0] - exact) < 1e-10 * abs(exact), r
+    H.set_precision("fp32")
+    lz32 = gpu.BasicBlockLanczosAlgorithm(H, 1, 800, block_size=2)
+    lz32.InitializeLanczosAlgorithm(seed=0)
+    q = lz32.solve_refined(800, precision=1e-12)
+    assert abs(q["energy"] - exact) < 1e-10 * abs(exact), q
+    assert q["fp32_matvecs"] > 0 and q["fp64_matvecs"] > 0
+
+
+def test_fqhe_fp32_refined_block(gpu):
+    z = golden("lanczos_n8_2s21_lz0_coulomb_basic.npz")
+    sp, H = _fqhe(gpu, z["v"], 8, 21, 0)
+    H.set_precision("fp32")
+    lz = gpu.BasicBlockLanczosAlgorithm(H, 1, 800, block_size=4)
+    lz.InitializeLanczosAlgorithm(seed=0)
+    q = lz.solve_refined(800, precision=1e-12)
+    e_ref = float(z["eigenvalues"][0])
+    assert abs(q["energy"] - e_ref) < 1e-10 * abs(e_ref), q
+    assert abs(q["energy_fp32"] - e_ref) < 1e-6 * abs(e_ref)
