@@ -479,17 +479,19 @@ def clebsch_gordan(j1, m1, j2, m2, j):
 def fqhe_sectors_block_lanczos(nbr_fermions, lz_max, total_lz, pseudopotentials, block_size=4, max_iter=400,
                                precision=1e-14, fp32=False, full_diag_limit=200, seed=100):
     """Lowest energy of every requested Lz sector: block Lanczos over all sectors in lockstep, one
-    launch per block product (BasicBlockLanczosAlgorithm + QHEOnSphereMainTask's loop per sector)."""
+    launch per block product (BasicBlockLanczosAlgorithm + QHEOnSphereMainTask's loop per sector).
+    fp32=True: FP32 products, then FP64 refinement of every sector to `precision`."""
     load()
     tl = np.ascontiguousarray(total_lz, np.int32)
     v = np.ascontiguousarray(pseudopotentials, np.float64)
     ns = tl.size
     e = np.zeros(ns, np.float64)
     it = np.zeros(ns, np.int32)
-    secs = np.zeros(4, np.float64)
+    secs = np.zeros(8, np.float64)
     _check(_lib.dh_fqhe_sectors_block_lanczos(nbr_fermions, lz_max, tl.ctypes.data, ns, v.ctypes.data, block_size,
                                               max_iter, float(precision),
                                               DH_PRECISION_FP32 if fp32 else DH_PRECISION_FP64, full_diag_limit, seed,
                                               e.ctypes.data, it.ctypes.data, secs.ctypes.data))
     return dict(energies=e, iterations=it, setup_seconds=secs[0], solve_seconds=secs[1], product_seconds=secs[2],
-                block_products=int(secs[3]))
+                block_products=int(secs[3]), fp32_seconds=secs[4], refine_seconds=secs[5],
+                refined_sectors=int(secs[6]), max_refine_shift=secs[7])

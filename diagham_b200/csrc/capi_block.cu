@@ -8,8 +8,11 @@
 // diagonalised on the host after every step (band -> tridiagonal -> QL, the reference's
 // RealBandDiagonalSymmetricMatrix::Tridiagonalize + Diagonalize), and each sector follows the
 // reference's convergence bookkeeping (:683-697, TestConvergence :731).  A sector whose block
-// Krylov space is exhausted (Cholesky breakdown) is exact and stops; sectors of dimension at most
-// full_diag_limit are diagonalised densely, as QHEOnSphereMainTask does below --full-diag (:397).
+// Krylov space is exhausted stops: its band matrix is exact when the whole new block vanished with
+// FP64 products; when the block only lost rank (dimension not a multiple of k) or the products were
+// FP32, the space is small (at most the vectors built so far) and is diagonalised densely in FP64.
+// Sectors of dimension at most full_diag_limit are diagonalised densely from the start, as
+// QHEOnSphereMainTask does below --full-diag (:397).
 #include <cuda_runtime.h>
 #include <math.h>
 #include <string.h>
@@ -29,12 +32,15 @@ using namespace dh;
 namespace dh {
 
 constexpr long long kTileRows = 4096;
+// largest exhausted space diagonalised densely on the host when its band matrix is not exact
+constexpr long long kDenseFallbackLimit = 2048;
 
 struct BlockSector {
   long long dim = 0;
   bool active = true;     // still iterating
   bool converged = false;
-  bool exhausted = false; // Krylov space exhausted: the band matrix is exact
+  bool exhausted = false; // Krylov space exhausted: the band matrix is exact ...
+  bool partial = false;   // ... unless the last block only lost rank (dimension not a multiple of k)
   int blocks = 0;         // A blocks recorded
   std::vector<double> A, B;  // A_j (k x k) for j < blocks, B_j (k x k) for 1 <= j <= blocks (B[0] unused)
   double prev_last = 0.0;
@@ -150,15 +156,16 @@ int engine_gram(BlockEngine& e, const double* x, const double* y, std::vector<do
   return DH_OK;
 }
 
-// Cholesky G = R^T R (R upper); returns false on breakdown.  Rinv = R^{-1} (upper).
-bool cholesky_inverse(int k, const double* G, double* R, double* Rinv) {
+// Cholesky G = R^T R (R upper); returns false on breakdown (a pivot below tol trace(G)).
+// Rinv = R^{-1} (upper).
+bool cholesky_inverse(int k, const double* G, double* R, double* Rinv, double tol) {
   double trace = 0.0;
   for (int i = 0; i < k; ++i) trace += fabs(G[i * k + i]);
   for (int i = 0; i < k * k; ++i) R[i] = Rinv[i] = 0.0;
   for (int j = 0; j < k; ++j) {
     double d = G[j * k + j];
     for (int p = 0; p < j; ++p) d -= R[p * k + j] * R[p * k + j];
-    if (!(d > 1e-26 * std::max(trace, 1e-300))) return false;
+    if (!(d > tol * std::max(trace, 1e-300))) return false;
     const double rjj = sqrt(d);
     R[j * k + j] = rjj;
     for (int c = j + 1; c < k; ++c) {
@@ -178,27 +185,34 @@ bool cholesky_inverse(int k, const double* G, double* R, double* Rinv) {
 }
 
 // X = X Q with X = V B (CholQR2): writes B (k x k per sector, upper) and leaves X orthonormal.
-// A sector whose block is numerically zero against its scale (|X|_F^2 < 1e-24 scale[s], scale =
-// |A|^2 + |B|^2 of the step: the block Krylov space is complete) or whose Gram matrix breaks down
-// gets a zero block and is marked exhausted.
+// A sector whose block is numerically zero against its scale (|X|_F^2 < tol scale[s], scale =
+// |A|^2 + |B|^2 of the step, tol = 1e-24 with FP64 products and 4e-12, about (32 u_FP32)^2, with
+// FP32 ones: the block Krylov space is complete) or whose Gram matrix breaks down gets a zero
+// block and is marked exhausted.
 int engine_qr(BlockEngine& e, double* x, std::vector<double>& B, float* x32, const std::vector<double>* scale,
               std::vector<double>* inv1 = nullptr, std::vector<double>* inv2 = nullptr) {
   const int k = e.k, kk = k * k;
   std::vector<double> g, R1((size_t)e.nsec * kk), R2((size_t)e.nsec * kk), inv((size_t)e.nsec * kk);
-  std::vector<char> broke(e.nsec, 0);
+  std::vector<char> broke(e.nsec, 0), vanished(e.nsec, 0);
   double* dM = e.small.as<double>() + (size_t)e.nsec * kk;
   int rc;
   for (int pass = 0; pass < 2; ++pass) {
     if ((rc = engine_gram(e, x, x, g)) != DH_OK) return rc;
     std::vector<double>& R = pass ? R2 : R1;
-    if (pass == 0 && scale)
+    // with FP32 products an exhausted Krylov space leaves FP32 rounding noise, not zero: the
+    // vanishing and pivot thresholds are about (32 u)^2 of the product's precision
+    const bool f32 = e.precision == DH_PRECISION_FP32;
+    const double pivot_tol = f32 ? 4e-12 : 1e-26;
+    if (pass == 0 && scale) {
+      const double tol = f32 ? 4e-12 : 1e-24;
       for (int s = 0; s < e.nsec; ++s) {
         double tr = 0.0;
         for (int i = 0; i < k; ++i) tr += g[(size_t)s * kk + i * k + i];
-        if (!(tr > 1e-24 * (*scale)[s])) broke[s] = 1;
+        if (!(tr > tol * (*scale)[s])) broke[s] = vanished[s] = 1;
       }
+    }
     for (int s = 0; s < e.nsec; ++s) {
-      if (broke[s] || !cholesky_inverse(k, &g[(size_t)s * kk], &R[(size_t)s * kk], &inv[(size_t)s * kk])) {
+      if (broke[s] || !cholesky_inverse(k, &g[(size_t)s * kk], &R[(size_t)s * kk], &inv[(size_t)s * kk], pivot_tol)) {
         broke[s] = 1;
         std::fill(&R[(size_t)s * kk], &R[(size_t)s * kk] + kk, 0.0);
         std::fill(&inv[(size_t)s * kk], &inv[(size_t)s * kk] + kk, 0.0);
@@ -213,6 +227,7 @@ int engine_qr(BlockEngine& e, double* x, std::vector<double>& B, float* x32, con
   B.assign((size_t)e.nsec * kk, 0.0);
   for (int s = 0; s < e.nsec; ++s) {
     if (broke[s]) {
+      if (!e.sec[s].exhausted) e.sec[s].partial = !vanished[s];
       e.sec[s].exhausted = true;
       continue;
     }
@@ -315,7 +330,13 @@ int engine_step(BlockEngine& e) {
     b.B.insert(b.B.end(), B.begin() + (size_t)s * kk, B.begin() + (size_t)(s + 1) * kk);
     ++b.blocks;
     ++b.steps;
-    if (b.exhausted && !was_exhausted[s]) b.converged = true;  // exact: the Krylov space is complete
+    // counting rule: once the blocks would outnumber the dimension the Krylov space is complete
+    // (exact band matrix) or the new block has lost rank, whatever the rounding noise says
+    if (!b.exhausted && (long long)(b.blocks + 1) * k > b.dim) {
+      b.exhausted = true;
+      b.partial = (long long)b.blocks * k < b.dim;
+    }
+    if (b.exhausted && !was_exhausted[s]) b.converged = true;  // the Krylov space is complete
   }
   for (int s = 0; s < e.nsec; ++s)
     for (int i = 0; i < k; ++i)
@@ -517,16 +538,47 @@ struct SectorBatchHost {
   }
 };
 
-int dense_lowest(dh_space_s* sp, const SectorBatchHost& hb, int nev, std::vector<double>& out, cudaStream_t stream) {
-  // H on the unit vectors, four columns per launch (one-sector batch, k = 4, FP64), then a dense
-  // symmetric eigensolve on the host
-  const long long d = sp->dim;
+// Dense FP64 spectrum of a small d x d Hamiltonian: H on the unit vectors, four columns per
+// product (product4: y = H x on [d][4] device blocks), then a dense symmetric eigensolve on the
+// host.  vals: all eigenvalues ascending; vecs (optional): the lowest nvec eigenvectors, [d][nvec].
+int dense_spectrum(long long d, const std::function<int(const double*, double*)>& product4, int nvec,
+                   std::vector<double>& vals, std::vector<double>* vecs, cudaStream_t stream) {
   const int k = 4;
-  DevBuf x, y, ptrs;
+  DevBuf x, y;
   int rc;
-  if ((rc = x.alloc((size_t)d * k * sizeof(double))) != DH_OK || (rc = y.alloc((size_t)d * k * sizeof(double))) != DH_OK ||
-      (rc = ptrs.alloc(2 * sizeof(void*) + 2 * sizeof(long long))) != DH_OK)
+  if ((rc = x.alloc((size_t)d * k * sizeof(double))) != DH_OK || (rc = y.alloc((size_t)d * k * sizeof(double))) != DH_OK)
     return rc;
+  std::vector<double> H((size_t)d * d), xin((size_t)d * k), yout((size_t)d * k);
+  for (long long c0 = 0; c0 < d; c0 += k) {
+    std::fill(xin.begin(), xin.end(), 0.0);
+    for (int j = 0; j < k && c0 + j < d; ++j) xin[(size_t)(c0 + j) * k + j] = 1.0;
+    DH_CUDA(cudaMemcpyAsync(x.ptr, xin.data(), xin.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+    if ((rc = product4(x.as<double>(), y.as<double>())) != DH_OK) return rc;
+    DH_CUDA(cudaMemcpyAsync(yout.data(), y.ptr, yout.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    DH_CUDA(cudaStreamSynchronize(stream));
+    for (int j = 0; j < k && c0 + j < d; ++j)
+      for (long long r = 0; r < d; ++r) H[(size_t)r * d + c0 + j] = yout[(size_t)r * k + j];
+  }
+  for (long long r = 0; r < d; ++r)  // symmetrise the rounding of the two triangles
+    for (long long c = r + 1; c < d; ++c) H[(size_t)r * d + c] = H[(size_t)c * d + r] = 0.5 * (H[(size_t)r * d + c] + H[(size_t)c * d + r]);
+  vals.assign(d, 0.0);
+  std::vector<double> z;
+  if (vecs) z.resize((size_t)d * d);
+  if ((rc = symmetric_eigen((int)d, H.data(), vals.data(), vecs ? z.data() : nullptr)) != DH_OK) return rc;
+  if (vecs) {
+    vecs->assign((size_t)d * nvec, 0.0);
+    for (long long r = 0; r < d; ++r)
+      for (int c = 0; c < nvec && c < d; ++c) (*vecs)[(size_t)r * nvec + c] = z[(size_t)r * d + c];
+  }
+  return DH_OK;
+}
+
+// the one-sector FP64 product of a batch's space, for dense_spectrum
+int dense_lowest(dh_space_s* sp, const SectorBatchHost& hb, int nev, std::vector<double>& out, cudaStream_t stream) {
+  const long long d = sp->dim;
+  DevBuf ptrs;
+  int rc;
+  if ((rc = ptrs.alloc(2 * sizeof(void*) + 2 * sizeof(long long))) != DH_OK) return rc;
   const void* hp[2] = {sp->words.ptr, sp->high_offset.ptr};
   long long ho[2] = {0, d};
   DH_CUDA(cudaMemcpy(ptrs.ptr, hp, 2 * sizeof(void*), cudaMemcpyHostToDevice));
@@ -538,32 +590,24 @@ int dense_lowest(dh_space_s* sp, const SectorBatchHost& hb, int nev, std::vector
   b.low_rank = sp->low_rank.as<uint16_t>();
   b.pair_offset = hb.pair_offset.as<int32_t>();
   b.factors = hb.f64.ptr;
-  b.x = x.ptr;
-  b.y = y.as<double>();
   b.total_rows = d;
   b.nbr_sectors = 1;
-  b.block = k;
+  b.block = 4;
   b.lz_max = sp->lz_max;
   b.low_bits = sp->rank.low_bits;
   b.nbr_pairs = hb.tabs.nbr_pairs;
   b.nbr_factors = hb.tabs.nbr_factors;
-  std::vector<double> H((size_t)d * d), xin((size_t)d * k), yout((size_t)d * k);
-  for (long long c0 = 0; c0 < d; c0 += k) {
-    std::fill(xin.begin(), xin.end(), 0.0);
-    for (int j = 0; j < k && c0 + j < d; ++j) xin[(size_t)(c0 + j) * k + j] = 1.0;
-    DH_CUDA(cudaMemcpyAsync(x.ptr, xin.data(), xin.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
-    if ((rc = launch_fqhe_sectors(b, DH_PRECISION_FP64, stream)) != DH_OK) return rc;
-    DH_CUDA(cudaMemcpyAsync(yout.data(), y.ptr, yout.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
-    DH_CUDA(cudaStreamSynchronize(stream));
-    for (int j = 0; j < k && c0 + j < d; ++j)
-      for (long long r = 0; r < d; ++r) H[(size_t)r * d + c0 + j] = yout[(size_t)r * k + j];
-  }
-  out.assign(d, 0.0);
-  rc = symmetric_eigen((int)d, H.data(), out.data(), nullptr);
-  out.resize(std::min<long long>(d, std::max(nev, 1)));
-  return rc;
+  auto product4 = [&b, stream](const double* x, double* y) {
+    SectorBatchDevice c = b;
+    c.x = x;
+    c.y = y;
+    return launch_fqhe_sectors(c, DH_PRECISION_FP64, stream);
+  };
+  std::vector<double> vals;
+  if ((rc = dense_spectrum(d, product4, 0, vals, nullptr, stream)) != DH_OK) return rc;
+  out.assign(vals.begin(), vals.begin() + std::min<long long>(d, std::max(nev, 1)));
+  return DH_OK;
 }
-
 
 // ------------------------------------------------------------------ one Hamiltonian
 
@@ -692,7 +736,7 @@ int block_lanczos_initialize(BlockLanczos* b, const double* vectors, int nbr_vec
     }
     if ((rc = launch_put_column(src, dim, e.k, j, e.slot[0], e.stream)) != DH_OK) return rc;
   }
-  e.sec[0].exhausted = false;
+  e.sec[0].exhausted = e.sec[0].partial = false;
   if ((rc = engine_start(e)) != DH_OK) return rc;
   DH_CHECK(!e.sec[0].exhausted, DH_ERR_ARGUMENT, "the start block is linearly dependent");
   b->initialized = true;
@@ -718,7 +762,26 @@ int block_lanczos_run(BlockLanczos* b, int nbr_iter) {
     }
   }
   b->ritz_valid = false;
-  return sector_evaluate(e, s);
+  if ((rc = sector_evaluate(e, s)) != DH_OK) return rc;
+  // an exhausted space is at most (blocks + 1) k vectors: when its band matrix is not exact (the
+  // last block only lost rank, or the products were FP32) diagonalise H densely in FP64
+  if (s.exhausted && (s.partial || e.precision == DH_PRECISION_FP32) && e.total <= kDenseFallbackLimit) {
+    dh_hamiltonian_s* h = b->h;
+    cudaStream_t st = e.stream;
+    auto product4 = [h, st](const double* x, double* y) {
+      return hamiltonian_apply_block(h, x, nullptr, y, 4, DH_PRECISION_FP64, st);
+    };
+    std::vector<double> vals, vecs;
+    if ((rc = dense_spectrum(e.total, product4, e.k, vals, &vecs, st)) != DH_OK) return rc;
+    if ((rc = ensure_buffer(b->ritz, (size_t)e.total * e.k * sizeof(double))) != DH_OK) return rc;
+    DH_CUDA(cudaMemcpyAsync(b->ritz.ptr, vecs.data(), vecs.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    DH_CUDA(cudaStreamSynchronize(st));
+    b->ritz_valid = true;
+    s.prev_last = s.ritz.empty() ? 0.0 : s.ritz[std::min(b->nev, (int)s.ritz.size()) - 1];
+    s.ritz = vals;
+    s.converged = true;
+  }
+  return DH_OK;
 }
 
 bool block_lanczos_converged(const BlockLanczos* b) { return bl_converged(b); }
@@ -815,8 +878,10 @@ int block_lanczos_solve_refined(BlockLanczos* b, int max_iter, double precision,
     }
   }
   if (rc == DH_OK && rnorm * rnorm > precision * std::max(fabs(energy), 1e-300)) {
+    // restart block: the lowest Ritz vector and fresh random vectors
     DH_CUDA(cudaMemcpyAsync(e.slot[0], b->ritz.ptr, (size_t)dim * k * sizeof(double), cudaMemcpyDeviceToDevice, e.stream));
-    e.sec[0].exhausted = false;
+    if ((rc = launch_random_block(e.slot[0], dim, k, e.row_offset_dev, e.tiles, 1000, e.stream, 1)) != DH_OK) return rc;
+    e.sec[0].exhausted = e.sec[0].partial = false;
     rc = engine_start(e);
     if (rc == DH_OK) {
       b->initialized = true;
@@ -837,12 +902,70 @@ int block_lanczos_solve_refined(BlockLanczos* b, int max_iter, double precision,
   return DH_OK;
 }
 
+
+// The one-launch product over a list of sectors of hb (their rows concatenated in list order); the
+// factor table follows the engine's current precision.
+struct SectorProduct {
+  DevBuf ptrs;
+  SectorBatchDevice b = {};
+};
+
+int bind_sector_product(SectorBatchHost& hb, const std::vector<int>& sectors, BlockEngine& e, SectorProduct& sp) {
+  const int ns = (int)sectors.size();
+  int rc;
+  if ((rc = sp.ptrs.alloc(2 * ns * sizeof(void*))) != DH_OK) return rc;
+  std::vector<const void*> hp(2 * ns);
+  for (int i = 0; i < ns; ++i) {
+    hp[i] = hb.spaces[sectors[i]]->words.ptr;
+    hp[ns + i] = hb.spaces[sectors[i]]->high_offset.ptr;
+  }
+  DH_CUDA(cudaMemcpy(sp.ptrs.ptr, hp.data(), hp.size() * sizeof(void*), cudaMemcpyHostToDevice));
+  SectorBatchDevice& b = sp.b;
+  b.words = reinterpret_cast<const uint64_t* const*>(sp.ptrs.ptr);
+  b.high_offset = reinterpret_cast<const int32_t* const*>(sp.ptrs.as<char>() + ns * sizeof(void*));
+  b.row_offset = e.row_offset_dev;
+  b.low_rank = hb.spaces[sectors[0]]->low_rank.as<uint16_t>();
+  b.pair_offset = hb.pair_offset.as<int32_t>();
+  b.total_rows = e.total;
+  b.nbr_sectors = ns;
+  b.block = e.k;
+  b.lz_max = hb.spaces[sectors[0]]->lz_max;
+  b.low_bits = hb.spaces[sectors[0]]->rank.low_bits;
+  b.nbr_pairs = hb.tabs.nbr_pairs;
+  b.nbr_factors = hb.tabs.nbr_factors;
+  SectorBatchDevice* bp = &sp.b;
+  SectorBatchHost* hbp = &hb;
+  BlockEngine* ep = &e;
+  e.product = [bp, hbp, ep](const double* x64, const float* x32, double* y) {
+    SectorBatchDevice c = *bp;
+    const bool f32 = ep->precision == DH_PRECISION_FP32;
+    c.factors = f32 ? hbp->f32.ptr : hbp->f64.ptr;
+    c.x = f32 ? static_cast<const void*>(x32) : static_cast<const void*>(x64);
+    c.xdiag = f32 ? x64 : nullptr;
+    c.y = y;
+    return launch_fqhe_sectors(c, ep->precision, ep->stream);
+  };
+  return DH_OK;
+}
+
+// keep every block on the device when the store fits in half of the free memory
+void engine_store_if_fits(BlockEngine& e) {
+  const int cap = e.max_iter / e.k + 3;
+  const size_t bytes = (size_t)cap * e.total * e.k * sizeof(double);
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  if (bytes < free_b / 2) {
+    if (e.store.alloc(bytes) == DH_OK) e.store_cap = cap;
+    else cudaGetLastError();
+  }
+}
+
 }  // namespace dh
 
 extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const int* total_lz, int nbr_sectors,
                                              const double* pseudopotentials, int block_size, int max_iter,
                                              double precision_target, int precision, int full_diag_limit,
-                                             uint64_t seed, double* energies, int* iterations, double* seconds) {
+                                             uint64_t seed, double* energies, int* iterations, double* stats) {
   using clk = std::chrono::steady_clock;
   const auto t0 = clk::now();
   DH_CHECK(total_lz && pseudopotentials && energies && iterations && nbr_sectors >= 1, DH_ERR_ARGUMENT, "bad argument");
@@ -900,42 +1023,20 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
     energies[s] = ev[0];
     iterations[s] = 0;
   }
+  double fp32_seconds = 0.0, refine_seconds = 0.0, max_shift = 0.0;
+  int refined = 0;
+  long long products = 0;
+  double product_ms = 0.0;
   if (!lanczos_sectors.empty()) {
+    const auto ta = clk::now();
+    e.eig_precision = precision == DH_PRECISION_FP32 ? std::max(e.eig_precision, 1e-9) : e.eig_precision;
     if ((rc = engine_setup(e, dims)) != DH_OK) return rc;
-    // the one-launch product over every Lanczos sector
+    if (precision == DH_PRECISION_FP32) engine_store_if_fits(e);
+    SectorProduct prod;
+    if ((rc = bind_sector_product(hb, lanczos_sectors, e, prod)) != DH_OK) return rc;
     const int ns = (int)lanczos_sectors.size();
-    if ((rc = hb.ptrs.alloc(2 * ns * sizeof(void*))) != DH_OK) return rc;
-    std::vector<const void*> hp(2 * ns);
-    for (int i = 0; i < ns; ++i) {
-      hp[i] = hb.spaces[lanczos_sectors[i]]->words.ptr;
-      hp[ns + i] = hb.spaces[lanczos_sectors[i]]->high_offset.ptr;
-    }
-    DH_CUDA(cudaMemcpy(hb.ptrs.ptr, hp.data(), hp.size() * sizeof(void*), cudaMemcpyHostToDevice));
-    SectorBatchDevice b = {};
-    b.words = reinterpret_cast<const uint64_t* const*>(hb.ptrs.ptr);
-    b.high_offset = reinterpret_cast<const int32_t* const*>(hb.ptrs.as<char>() + ns * sizeof(void*));
-    b.row_offset = e.row_offset_dev;
-    b.low_rank = hb.spaces[lanczos_sectors[0]]->low_rank.as<uint16_t>();
-    b.pair_offset = hb.pair_offset.as<int32_t>();
-    b.factors = (precision == DH_PRECISION_FP32) ? hb.f32.ptr : hb.f64.ptr;
-    b.total_rows = e.total;
-    b.nbr_sectors = ns;
-    b.block = e.k;
-    b.lz_max = lz_max;
-    b.low_bits = hb.spaces[lanczos_sectors[0]]->rank.low_bits;
-    b.nbr_pairs = hb.tabs.nbr_pairs;
-    b.nbr_factors = hb.tabs.nbr_factors;
-    e.product = [b, &e](const double* x64, const float* x32, double* y) mutable {
-      b.x = x32 ? static_cast<const void*>(x32) : static_cast<const void*>(x64);
-      b.xdiag = x32 ? x64 : nullptr;
-      b.y = y;
-      return launch_fqhe_sectors(b, e.precision, e.stream);
-    };
     // start block: splitmix64 vectors per sector (seed + j for vector j)
-    DevBuf base;
-    if ((rc = base.alloc(ns * sizeof(long long))) != DH_OK) return rc;
-    DH_CUDA(cudaMemcpy(base.ptr, e.off.data(), ns * sizeof(long long), cudaMemcpyHostToDevice));
-    if ((rc = launch_random_block(e.slot[0], e.total, e.k, base.as<long long>(), e.tiles, seed, e.stream)) != DH_OK)
+    if ((rc = launch_random_block(e.slot[0], e.total, e.k, e.row_offset_dev, e.tiles, seed, e.stream)) != DH_OK)
       return rc;
     if ((rc = engine_start(e)) != DH_OK) return rc;
     if ((rc = engine_solve(e)) != DH_OK) return rc;
@@ -944,13 +1045,109 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
       energies[lanczos_sectors[i]] = bs.ritz.empty() ? NAN : bs.ritz[0];
       iterations[lanczos_sectors[i]] = bs.count;
     }
+    products += e.products;
+    product_ms += e.product_ms;
+    // exhausted sectors whose band matrix is not exact (rank lost in the last block, or FP32
+    // products) are small: they are diagonalised densely in FP64 at the end
+    std::vector<char> need_dense(ns, 0);
+    for (int i = 0; i < ns; ++i)
+      need_dense[i] = e.sec[i].exhausted && (e.sec[i].partial || precision == DH_PRECISION_FP32) &&
+                      e.sec[i].dim <= kDenseFallbackLimit;
+    const auto tb = clk::now();
+    fp32_seconds = precision == DH_PRECISION_FP32 ? std::chrono::duration<double>(tb - ta).count() : 0.0;
+    if (precision == DH_PRECISION_FP32) {
+      // refinement: FP64 Rayleigh quotient and residual of every sector's lowest Ritz vector
+      const int k = e.k, kk = k * k;
+      DevBuf R;
+      if ((rc = R.alloc((size_t)e.total * k * sizeof(double))) != DH_OK) return rc;
+      if ((rc = engine_ritz(e, R.as<double>())) != DH_OK) return rc;
+      e.precision = DH_PRECISION_FP64;
+      double* Y = e.slot[0];
+      std::vector<double> g, a, rr;
+      if ((rc = engine_product(e, R.as<double>(), Y)) != DH_OK) return rc;
+      if ((rc = engine_gram(e, R.as<double>(), R.as<double>(), g)) != DH_OK) return rc;
+      if ((rc = engine_gram(e, R.as<double>(), Y, a)) != DH_OK) return rc;
+      std::vector<double> d((size_t)ns * kk, 0.0), e_rq(ns);
+      for (int i = 0; i < ns; ++i) {
+        for (int c = 0; c < k; ++c)
+          d[(size_t)i * kk + c * k + c] = a[(size_t)i * kk + c * k + c] / g[(size_t)i * kk + c * k + c];
+        e_rq[i] = d[(size_t)i * kk];
+      }
+      double* dA = e.small.as<double>() + 2 * (size_t)e.nsec * kk;
+      DH_CUDA(cudaMemcpyAsync(dA, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+      if ((rc = launch_seg_update(Y, R.as<double>(), dA, nullptr, nullptr, k, e.tiles, e.stream)) != DH_OK) return rc;
+      if ((rc = engine_gram(e, Y, Y, rr)) != DH_OK) return rc;
+      products = e.products;
+      product_ms = e.product_ms;
+      std::vector<int> redo;  // positions in lanczos_sectors
+      for (int i = 0; i < ns; ++i) {
+        const double r2 = std::max(rr[(size_t)i * kk], 0.0) / g[(size_t)i * kk];
+        const int s = lanczos_sectors[i];
+        max_shift = std::max(max_shift, fabs(e_rq[i] - energies[s]));
+        energies[s] = e_rq[i];
+        if (need_dense[i]) continue;
+        if (r2 > precision_target * std::max(fabs(e_rq[i]), 1e-300)) redo.push_back(i);
+      }
+      refined = (int)redo.size();
+      if (!redo.empty()) {
+        // FP64 block Lanczos restarted from the Ritz blocks of those sectors, in lockstep
+        BlockEngine f;
+        f.k = k;
+        f.nev = 1;
+        f.precision = DH_PRECISION_FP64;
+        f.eig_precision = precision_target > 0.0 ? precision_target : 1e-14;
+        f.max_iter = std::min(max_iter, 60 * k);
+        f.stream = e.stream;
+        std::vector<long long> rdims;
+        std::vector<int> rsec;
+        for (int i : redo) {
+          rdims.push_back(e.sec[i].dim);
+          rsec.push_back(lanczos_sectors[i]);
+        }
+        if ((rc = engine_setup(f, rdims)) != DH_OK) return rc;
+        for (size_t j = 0; j < redo.size(); ++j)
+          DH_CUDA(cudaMemcpyAsync(f.slot[0] + (size_t)f.off[j] * k, R.as<double>() + (size_t)e.off[redo[j]] * k,
+                                  (size_t)rdims[j] * k * sizeof(double), cudaMemcpyDeviceToDevice, f.stream));
+        // the lowest Ritz vector and fresh random vectors: the other Ritz vectors of a sector whose
+        // FP32 basis lost orthogonality can be nearly dependent on it
+        if ((rc = launch_random_block(f.slot[0], f.total, k, f.row_offset_dev, f.tiles, seed + 1000, f.stream, 1)) !=
+            DH_OK)
+          return rc;
+        SectorProduct fprod;
+        if ((rc = bind_sector_product(hb, rsec, f, fprod)) != DH_OK) return rc;
+        if ((rc = engine_start(f)) != DH_OK) return rc;
+        if ((rc = engine_solve(f)) != DH_OK) return rc;
+        for (size_t j = 0; j < redo.size(); ++j) {
+          const BlockSector& bs = f.sec[j];
+          if (!bs.ritz.empty()) energies[rsec[j]] = bs.ritz[0];
+          iterations[rsec[j]] += bs.count;
+          max_shift = std::max(max_shift, fabs(energies[rsec[j]] - e_rq[redo[j]]));
+          if (bs.exhausted && bs.partial && bs.dim <= kDenseFallbackLimit) need_dense[redo[j]] = 1;
+        }
+        products += f.products;
+        product_ms += f.product_ms;
+      }
+      refine_seconds = std::chrono::duration<double>(clk::now() - tb).count();
+    }
+    for (int i = 0; i < ns; ++i) {
+      if (!need_dense[i]) continue;
+      const int s = lanczos_sectors[i];
+      std::vector<double> ev;
+      if ((rc = dense_lowest(hb.spaces[s], hb, 1, ev, e.stream)) != DH_OK) return rc;
+      if (precision == DH_PRECISION_FP32) max_shift = std::max(max_shift, fabs(ev[0] - energies[s]));
+      energies[s] = ev[0];
+    }
   }
   const auto t2 = clk::now();
-  if (seconds) {
-    seconds[0] = std::chrono::duration<double>(t1 - t0).count();
-    seconds[1] = std::chrono::duration<double>(t2 - t1).count();
-    seconds[2] = e.product_ms / 1000.0;
-    seconds[3] = (double)e.products;
+  if (stats) {
+    stats[0] = std::chrono::duration<double>(t1 - t0).count();
+    stats[1] = std::chrono::duration<double>(t2 - t1).count();
+    stats[2] = product_ms / 1000.0;
+    stats[3] = (double)products;
+    stats[4] = fp32_seconds;
+    stats[5] = refine_seconds;
+    stats[6] = (double)refined;
+    stats[7] = max_shift;
   }
   return DH_OK;
 }

@@ -142,8 +142,10 @@ int launch_seg_update(double* w, const double* v, const double* A, const double*
 int launch_seg_rmul(double* w, const double* M, int k, const TileSetDevice& t, float* w32, cudaStream_t s);
 int launch_seg_combine_blocks(const double* blocks, int nb, long long stride, const double* C, int cstride, int k,
                               const TileSetDevice& t, double* out, cudaStream_t s);
+// vectors first_col .. k-1 of every sector's [rows][k] block: component i of vector j is the
+// (i+1)-th splitmix64 output of seed + j, mapped to [-1, 1)
 int launch_random_block(double* x, long long rows, int k, const long long* row_sector_base, const TileSetDevice& t,
-                        uint64_t seed, cudaStream_t s);
+                        uint64_t seed, cudaStream_t s, int first_col = 0);
 int launch_f32_copy(const double* x, float* y, long long n, cudaStream_t s);
 // x[i][col] = v[i] and v[i] = scale * x[i][col] for a [n][k] block x
 int launch_put_column(const double* v, long long n, int k, int col, double* x, cudaStream_t s);

@@ -156,14 +156,14 @@ __global__ void __launch_bounds__(kThreads) seg_combine_blocks_kernel(const doub
   }
 }
 
-__global__ void random_block_kernel(double* x, long long rows, int k, const long long* row_sector_base,
+__global__ void random_block_kernel(double* x, long long rows, int k, int first_col, const long long* row_sector_base,
                                     TileSetDevice t, uint64_t seed) {
   const int tile = blockIdx.x;
   const int s = t.tile_sector[tile];
   const long long base = row_sector_base[s];
   const long long r0 = t.tile_begin[tile], r1 = t.tile_end[tile];
   for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
-    for (int j = 0; j < k; ++j) {
+    for (int j = first_col; j < k; ++j) {
       // vector j of sector s: component i = (i+1)-th splitmix64 output of seed + j
       const uint64_t i = (uint64_t)(r - base);
       uint64_t z = seed + (uint64_t)j + (i + 1) * 0x9E3779B97F4A7C15ull;
@@ -258,9 +258,9 @@ int launch_seg_combine_blocks(const double* blocks, int nb, long long stride, co
 }
 
 int launch_random_block(double* x, long long rows, int k, const long long* row_sector_base, const TileSetDevice& t,
-                        uint64_t seed, cudaStream_t s) {
-  if (t.nbr_tiles <= 0) return DH_OK;
-  random_block_kernel<<<t.nbr_tiles, kThreads, 0, s>>>(x, rows, k, row_sector_base, t, seed);
+                        uint64_t seed, cudaStream_t s, int first_col) {
+  if (t.nbr_tiles <= 0 || first_col >= k) return DH_OK;
+  random_block_kernel<<<t.nbr_tiles, kThreads, 0, s>>>(x, rows, k, first_col, row_sector_base, t, seed);
   DH_CUDA(cudaGetLastError());
   return DH_OK;
 }

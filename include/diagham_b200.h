@@ -262,14 +262,21 @@ int dh_lanczos_solve_refined(dh_lanczos_t l, int max_iter, double precision, dou
  * sector at once.  Each sector follows the reference's driver loop and convergence test
  * (QHEOnSphereMainTask.cc:732-753, precision_target = the Lanczos precision, max_iter in vectors).
  * Sectors of dimension <= full_diag_limit (or <= 2 block_size) are diagonalised densely, as
- * QHEOnSphereMainTask does below --full-diag (:397).  FP32 products with FP64 recurrence when
- * precision == DH_PRECISION_FP32.  energies[s] = lowest eigenvalue of sector s, iterations[s] =
- * the driver's counter (0 for dense sectors); seconds (optional, 4 values) = set-up seconds, solve
- * seconds, device time of the block products, number of block products. */
+ * QHEOnSphereMainTask does below --full-diag (:397); so are sectors whose block Krylov space runs
+ * out with a band matrix that is not exact (a last block that only lost rank, or FP32 products).
+ * precision == DH_PRECISION_FP32: FP32 products with the FP64 recurrence until the Ritz values
+ * settle to max(precision_target, 1e-9); then every sector's lowest Ritz vector gets an FP64
+ * Rayleigh quotient and residual, and the sectors whose |r|^2 > precision_target |E| are polished
+ * by an FP64 block Lanczos restarted from their Ritz blocks, all of them in lockstep.
+ * energies[s] = lowest eigenvalue of sector s, iterations[s] = the driver's counter (both phases;
+ * 0 for dense sectors); stats (optional, DH_SECTOR_STATS values): set-up seconds, solve seconds,
+ * device time of the block products, number of block products, FP32-phase seconds, refinement
+ * seconds, number of sectors restarted in FP64, largest |E_refined - E_FP32| over the sectors. */
+#define DH_SECTOR_STATS 8
 int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const int* total_lz, int nbr_sectors,
                                   const double* pseudopotentials, int block_size, int max_iter,
                                   double precision_target, int precision, int full_diag_limit,
-                                  uint64_t seed, double* energies, int* iterations, double* seconds);
+                                  uint64_t seed, double* energies, int* iterations, double* stats);
 
 /* ================================================================ setup helpers */
 

@@ -37,12 +37,25 @@ def test_all_sectors_against_dense(gpu, orc, k):
         assert abs(e - ref) < 1e-10 * max(1.0, abs(ref)), (lz, e, ref)
 
 
-def test_fp32_products_then_fp64(gpu, orc):
+def test_fp32_products_refined_to_fp64(gpu, orc):
     v = golden("lanczos_n8_2s21_lz0_coulomb_basic.npz")["v"]
     sectors = [0, 2, 4, 6]
     r64 = gpu.fqhe_sectors_block_lanczos(8, 21, sectors, v, block_size=4, max_iter=800)
-    r32 = gpu.fqhe_sectors_block_lanczos(8, 21, sectors, v, block_size=4, max_iter=800, fp32=True, precision=1e-9)
+    r32 = gpu.fqhe_sectors_block_lanczos(8, 21, sectors, v, block_size=4, max_iter=800, fp32=True, precision=1e-12)
     e_basic = float(golden("lanczos_n8_2s21_lz0_coulomb_basic.npz")["eigenvalues"][0])
     assert abs(r64["energies"][0] - e_basic) < 1e-10 * abs(e_basic)
-    assert np.max(np.abs(r32["energies"] - r64["energies"]) / np.abs(r64["energies"])) < 1e-6
-    assert r64["block_products"] > 0 and r64["product_seconds"] > 0
+    assert np.max(np.abs(r32["energies"] - r64["energies"]) / np.abs(r64["energies"])) < 1e-10, (r32, r64)
+    assert r32["refined_sectors"] >= 1 and 0 < r32["max_refine_shift"] < 1e-5
+    assert r64["block_products"] > 0 and r64["product_seconds"] > 0 and r64["refined_sectors"] == 0
+
+
+@pytest.mark.parametrize("k", [2, 4])
+def test_every_sector_fp32_refined_against_dense(gpu, orc, k):
+    # all 31 sectors 2Lz = 0 .. 60 of N = 6, 2S = 15, dimensions 1 .. 1242
+    v = golden("lanczos_n6_2s15_lz0_coulomb_block4.npz")["v"]
+    sectors = list(range(0, 61, 2))
+    r = gpu.fqhe_sectors_block_lanczos(6, 15, sectors, v, block_size=k, max_iter=600, fp32=True, precision=1e-13,
+                                       full_diag_limit=16)
+    for lz, e in zip(sectors, r["energies"]):
+        ref = dense_e0(orc, 6, 15, lz, v)
+        assert abs(e - ref) < 1e-10 * max(1.0, abs(ref)), (lz, e, ref)

@@ -119,3 +119,21 @@ def test_fqhe_fp32_refined_block(gpu):
     e_ref = float(z["eigenvalues"][0])
     assert abs(q["energy"] - e_ref) < 1e-10 * abs(e_ref), q
     assert abs(q["energy_fp32"] - e_ref) < 1e-6 * abs(e_ref)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_exhausted_space_falls_back_to_dense(gpu, orc, prec):
+    # 2Lz = 42 of N = 6, 2S = 15 has dimension 26: with k = 4 the last block only has rank 2
+    from test_gpu_block import dense_e0
+    v = golden("lanczos_n6_2s15_lz0_coulomb_block4.npz")["v"]
+    sp, H = _fqhe(gpu, v, lz=42)
+    assert sp.dim == 26
+    H.set_precision(prec)
+    lz = gpu.BasicBlockLanczosAlgorithm(H, 1, 400, block_size=4)
+    lz.InitializeLanczosAlgorithm(seed=5)
+    r = lz.solve(400)
+    ref = dense_e0(orc, 6, 15, 42, v)
+    assert r["converged"] and abs(r["eigenvalues"][0] - ref) < 1e-10 * abs(ref), (r, ref)
+    psi = lz.GetGroundState()
+    hpsi = orc.FQHE(6, 15, 42, v).pull(psi)
+    assert np.linalg.norm(hpsi - ref * psi) < 1e-10
