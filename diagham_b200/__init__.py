@@ -57,6 +57,7 @@ SIGNATURES = {
     "dh_hamiltonian_low_level_add_multiply": ([_vp, _vp, _vp, _c_i64, _c_i64], _c_int),
     "dh_hamiltonian_low_level_multiply": ([_vp, _vp, _vp, _c_i64, _c_i64], _c_int),
     "dh_hamiltonian_low_level_multiple_add_multiply": ([_vp, _vp, _vp, _c_int, _c_i64, _c_i64], _c_int),
+    "dh_hamiltonian_block_multiply": ([_vp, _vp, _vp, _c_int], _c_int),
     "dh_hamiltonian_matrix_element": ([_vp, _vp, _vp, _vp], _c_int),
     "dh_hamiltonian_row_elements": ([_vp, _c_i64, _vp, _vp, _vp, _c_int, _ip], _c_int),
     "dh_hamiltonian_pseudopotential_adjoint": ([_vp, _vp, _vp, _vp], _c_int),
@@ -258,6 +259,16 @@ class _Hamiltonian:
         _check(_lib.dh_hamiltonian_low_level_multiple_add_multiply(self._handle, s.ptr, d.ptr, k, first, nbr))
         d.finish()
         return dsts
+
+    def block_multiply(self, x, y=None):
+        """y = H x for a row-interleaved block x of shape (dim, k) (numpy or torch CUDA)."""
+        k = 1 if len(x.shape) == 1 else int(x.shape[1])
+        if y is None:
+            y = np.zeros((self.dim, k), np.float64) if isinstance(x, np.ndarray) else x.new_empty(x.shape)
+        s, d = _Buf(x), _Buf(y, writable=True)
+        _check(_lib.dh_hamiltonian_block_multiply(self._handle, s.ptr, d.ptr, k))
+        d.finish()
+        return y
 
     def count_elements(self):
         """Elements one product generates (moves incl. diagonal ones; spin flips)."""

@@ -562,6 +562,36 @@ static int multiply_common(dh_hamiltonian_t h, const double* src, double* dst, i
   return DH_OK;
 }
 
+int dh_hamiltonian_block_multiply(dh_hamiltonian_t h, const double* x, double* y, int k) {
+  DH_CHECK(h && x && y, DH_ERR_ARGUMENT, "null argument");
+  DH_CHECK(k >= 1, DH_ERR_ARGUMENT, "k must be >= 1");
+  const int64_t dim = h->space->dim;
+  const size_t bytes = (size_t)dim * k * sizeof(double);
+  const bool src_dev = is_device_pointer(x), dst_dev = is_device_pointer(y);
+  const double* xd = x;
+  double* yd = y;
+  int rc;
+  if (!src_dev) {
+    if ((rc = ensure_buffer(h->stage_x, bytes)) != DH_OK) return rc;
+    DH_CUDA(cudaMemcpyAsync(h->stage_x.ptr, x, bytes, cudaMemcpyHostToDevice, h->stream));
+    xd = h->stage_x.as<double>();
+  }
+  if (!dst_dev) {
+    if ((rc = ensure_buffer(h->stage_y, bytes)) != DH_OK) return rc;
+    yd = h->stage_y.as<double>();
+  }
+  const float* x32 = nullptr;
+  if (h->precision == DH_PRECISION_FP32) {
+    if ((rc = ensure_buffer(h->x32, (size_t)dim * k * sizeof(float))) != DH_OK) return rc;
+    if ((rc = launch_convert_f32(xd, h->x32.as<float>(), dim * k, h->stream)) != DH_OK) return rc;
+    x32 = h->x32.as<float>();
+  }
+  if ((rc = hamiltonian_apply_block(h, xd, x32, yd, k, h->precision, h->stream)) != DH_OK) return rc;
+  if (!dst_dev) DH_CUDA(cudaMemcpyAsync(y, yd, bytes, cudaMemcpyDeviceToHost, h->stream));
+  DH_CUDA(cudaStreamSynchronize(h->stream));
+  return DH_OK;
+}
+
 int dh_hamiltonian_low_level_add_multiply(dh_hamiltonian_t h, const double* src, double* dst, int64_t first,
                                           int64_t nbr) {
   return multiply_common(h, src, dst, 1, first, nbr, 1);

@@ -180,38 +180,34 @@ __device__ __forceinline__ uint32_t between32(int lo, int hi) {
 // K gathered values of target row idx: interleaved blocks ([row][K], IL) load them as one vector
 template <typename TG, int K, bool IL>
 __device__ __forceinline__ void load_row(const TG* x, const MatvecArgs& a, int idx, TG (&v)[K]) {
-  if (IL) {
+  if constexpr (IL) {
     const TG* p = x + (long long)idx * K;
-    if (sizeof(TG) == 4 && K == 4) {
+    if constexpr (sizeof(TG) == 4 && K == 4) {
       const float4 q = __ldg(reinterpret_cast<const float4*>(p));
       v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
-      return;
-    }
-    if (sizeof(TG) == 4 && K == 2) {
+    } else if constexpr (sizeof(TG) == 4 && K == 2) {
       const float2 q = __ldg(reinterpret_cast<const float2*>(p));
       v[0] = q.x; v[1] = q.y;
-      return;
-    }
-    if (sizeof(TG) == 8 && (K == 2 || K == 4)) {
+    } else if constexpr (sizeof(TG) == 8 && (K == 2 || K == 4)) {
 #pragma unroll
       for (int j = 0; j < K; j += 2) {
         const double2 q = __ldg(reinterpret_cast<const double2*>(p) + j / 2);
         v[j] = q.x;
         v[j + 1] = q.y;
       }
+    } else {
+#pragma unroll
+      for (int j = 0; j < K; ++j) v[j] = __ldg(p + j);
+    }
+  } else {
+    if (K == 1 && a.ld == 1) {
+      v[0] = __ldg(x + idx);
       return;
     }
+    const TG* p = x + (long long)idx * a.ld;
 #pragma unroll
-    for (int j = 0; j < K; ++j) v[j] = __ldg(p + j);
-    return;
+    for (int j = 0; j < K; ++j) v[j] = __ldg(p + j * a.vstride);
   }
-  if (K == 1 && a.ld == 1) {
-    v[0] = __ldg(x + idx);
-    return;
-  }
-  const TG* p = x + (long long)idx * a.ld;
-#pragma unroll
-  for (int j = 0; j < K; ++j) v[j] = __ldg(p + j * a.vstride);
 }
 
 template <typename TG, int K, bool RANGE, bool IL>
@@ -357,8 +353,14 @@ __device__ __forceinline__ void split_row(const SplitTables& t, const TG* sfac, 
   }
 }
 
-template <typename TG, int K, bool RANGE, bool LR_SMEM>
-__global__ void __launch_bounds__(kMatvecThreads) fqhe_split_kernel(FqheDevice f, MatvecArgs a, SmemLayout lay) {
+// four resident blocks per SM: at most 64 registers per thread (a tighter bound of 48 registers for
+// the FP32 single-vector form measured slower)
+constexpr int kSplitMinBlocks = 4;
+
+// IL: the K vectors are row-interleaved ([row][K], ld = K, vstride = 1 for x and y)
+template <typename TG, int K, bool RANGE, bool LR_SMEM, bool IL>
+__global__ void __launch_bounds__(kMatvecThreads, kSplitMinBlocks)
+    fqhe_split_kernel(FqheDevice f, MatvecArgs a, SmemLayout lay) {
   extern __shared__ __align__(16) unsigned char smem[];
   TG* sfac = reinterpret_cast<TG*>(smem);
   int* spair = reinterpret_cast<int*>(smem + lay.factor_bytes);
@@ -386,22 +388,24 @@ __global__ void __launch_bounds__(kMatvecThreads) fqhe_split_kernel(FqheDevice f
 #pragma unroll
     for (int j = 0; j < K; ++j) acc[j] = TG(0);
     TG dsum = TG(0);
-    split_row<TG, K, RANGE, false>(t, sfac, spair, r, x, a, acc, dsum);
+    split_row<TG, K, RANGE, IL>(t, sfac, spair, r, x, a, acc, dsum);
     if (!RANGE || (r >= a.col_first && r < a.col_last)) {
-      const TG* xr = x + r * a.ld;
+      TG xr[K];
+      load_row<TG, K, IL>(x, a, (int)r, xr);
 #pragma unroll
-      for (int j = 0; j < K; ++j) acc[j] += dsum * xr[j * a.vstride];
+      for (int j = 0; j < K; ++j) acc[j] += dsum * xr[j];
     }
     const bool diag = (r >= a.row_first && r < a.row_last);
     double* y = static_cast<double*>(a.y);
 #pragma unroll
     for (int j = 0; j < K; ++j) {
       double v = (double)acc[j];
+      const long long xo = IL ? r * K + j : r * a.ld + j * a.vstride;
       if (diag && a.shift != 0.0) {
-        double xd = a.xdiag ? a.xdiag[r * a.ld + j * a.vstride] : (double)x[r * a.ld + j * a.vstride];
+        double xd = a.xdiag ? a.xdiag[xo] : (double)x[xo];
         v += a.shift * xd;
       }
-      double* yp = y + r * a.ld_y + j * a.vstride_y;
+      double* yp = y + (IL ? r * K + j : r * a.ld_y + j * a.vstride_y);
       *yp = a.accumulate ? (*yp + v) : v;
     }
   }
@@ -468,8 +472,15 @@ int launch_one(const FqheDevice& f, const MatvecArgs& a, cudaStream_t s) {
   auto kern = fqhe_matvec_kernel<TG, K, MODE, RANGE>;
   // the split-word form needs both halves of a word in 32 bits; variant 2 stages the low-rank table
   // in shared memory
-  if (MODE == DH_INDEX_RANK && f.kernel_variant != 1 && f.low_bits <= 31 && f.lz_max + 1 - f.low_bits <= 31)
-    kern = (f.kernel_variant == 2) ? fqhe_split_kernel<TG, K, RANGE, true> : fqhe_split_kernel<TG, K, RANGE, false>;
+  if (MODE == DH_INDEX_RANK && f.kernel_variant != 1 && f.low_bits <= 31 && f.lz_max + 1 - f.low_bits <= 31) {
+    kern = (f.kernel_variant == 2) ? fqhe_split_kernel<TG, K, RANGE, true, false>
+                                   : fqhe_split_kernel<TG, K, RANGE, false, false>;
+    if constexpr (!RANGE && K > 1) {
+      // row-interleaved blocks (block Lanczos): vector loads of the K values of a target row
+      if (f.kernel_variant != 2 && a.ld == K && a.vstride == 1 && a.ld_y == K && a.vstride_y == 1)
+        kern = fqhe_split_kernel<TG, K, false, false, true>;
+    }
+  }
   if (lay.total > 48 * 1024) DH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total));
   int dev = 0, sms = 0, per_sm = 0;
   DH_CUDA(cudaGetDevice(&dev));

@@ -139,6 +139,13 @@ int dh_hamiltonian_low_level_multiply(dh_hamiltonian_t h, const double* src, dou
 int dh_hamiltonian_low_level_multiple_add_multiply(dh_hamiltonian_t h, const double* srcs, double* dsts,
                                                    int nbr_vectors, int64_t first, int64_t nbr);
 
+/* y = H x for a block of k vectors stored row-interleaved (x[i * k + j] = component i of vector j,
+ * a row-major (dim, k) array), host or device pointers.  One enumeration of each row's matrix
+ * elements serves the whole block, with vector loads for k = 2 and 4.  No reference counterpart:
+ * LowLevelMultipleAddMultiply (AbstractHamiltonian.h) takes k separate vectors; this is its form
+ * for blocks kept interleaved, as the block Lanczos and (dim, k) torch tensors keep them. */
+int dh_hamiltonian_block_multiply(dh_hamiltonian_t h, const double* x, double* y, int k);
+
 /* AbstractHamiltonian::MatrixElement(V1, V2) (AbstractQHEOnSphereHamiltonian.cc:380): <v1|H|v2>. */
 int dh_hamiltonian_matrix_element(dh_hamiltonian_t h, const double* v1, const double* v2, double* out);
 

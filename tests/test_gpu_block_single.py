@@ -137,3 +137,33 @@ def test_exhausted_space_falls_back_to_dense(gpu, orc, prec):
     psi = lz.GetGroundState()
     hpsi = orc.FQHE(6, 15, 42, v).pull(psi)
     assert np.linalg.norm(hpsi - ref * psi) < 1e-10
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-13), ("fp32", 2e-6)])
+@pytest.mark.parametrize("k", [1, 2, 3, 4])
+def test_block_multiply_matches_oracle(gpu, orc, prec, tol, k):
+    v = golden("lanczos_n8_2s21_lz0_coulomb_basic.npz")["v"]
+    sp, H = _fqhe(gpu, v, 8, 21, 0)
+    H.set_precision(prec)
+    H.ShiftHamiltonian(0.37)
+    x = np.random.default_rng(k).uniform(-1.0, 1.0, (sp.dim, k))
+    y = H.block_multiply(x)
+    O = orc.FQHE(8, 21, 0, v)
+    for j in range(k):
+        ref = O.pull(np.ascontiguousarray(x[:, j])) + 0.37 * x[:, j]
+        assert np.max(np.abs(y[:, j] - ref)) <= tol * np.max(np.abs(ref)), (j, prec)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-13), ("fp32", 2e-6)])
+@pytest.mark.parametrize("k", [2, 4])
+def test_spin_block_multiply_matches_oracle(gpu, orc, prec, tol, k):
+    L, sz = 14, 0
+    chain = gpu.Spin1_2Chain(L, sz)
+    H = gpu.SpinChainJ1J2Hamiltonian(chain, 1.0, 0.5)
+    H.set_precision(prec)
+    words = orc.spin_basis(L, sz)
+    x = np.random.default_rng(k).uniform(-1.0, 1.0, (chain.dim, k))
+    y = H.block_multiply(x)
+    for j in range(k):
+        ref = orc.spin_j1j2_multiply(L, sz, words, 1.0, 0.5, x[:, j])
+        assert np.max(np.abs(y[:, j] - ref)) <= tol * np.max(np.abs(ref)), (j, prec)
