@@ -3,9 +3,12 @@
 
 Workload (the precision configuration): N = 12 spin-polarised fermions on the sphere, 2S = 33,
 total Lz = 0 (dimension 7,764,392), lowest-Landau-level Coulomb pseudopotentials V_m (odd m),
-synthetic start vectors from splitmix64.  One step = one H.v through the C ABI with the input
-already in HBM: FP32 matrix elements and FP32 per-row accumulation, FP64 in and out (the product
-the FP32+refine Lanczos runs).  L2 is flushed (a 256 MiB write) before every step.
+synthetic inputs.  One step = one block product H X of 4 vectors (4 H.v) through the C ABI with the
+input already in HBM, the batched form of the block Lanczos: FP32 matrix elements and FP32 per-row
+accumulation, FP64 in and out.  L2 is flushed (a 256 MiB write) before every step.  The line also
+carries the single-vector FP64 / FP32 rates, the time to E0 of the sector (plain FP64 against FP32
+products + FP64 refinement), of all 91 sectors of N = 10, 2S = 27 (batched against sector by
+sector), and the L = 32 J1-J2 chain product with its roofline.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -32,11 +35,12 @@ METRIC = "H·v/sec and time-to-E0 (1e-10) FP32+refine batched vs plain FP64, one
 UNIT = "H·v/s"
 REF_TOOL = os.path.join(ROOT, "oracle", "_ref", "ref_tool")
 FLUSH_BYTES = 256 << 20
+BLOCK = 4  # vectors per product in the measured step (the batched form)
 
 
 def workload_name():
-    return ("FermionOnSphere N=12 2S=33 2Lz=0 (dim 7764392), LLL Coulomb V_m odd m, on-the-fly H.v, "
-            "FP32 elements + FP32 row accumulation, FP64 vectors")
+    return ("FermionOnSphere N=12 2S=33 2Lz=0 (dim 7764392), LLL Coulomb V_m odd m, on-the-fly H.v on "
+            "row-interleaved blocks of 4 vectors, FP32 elements + FP32 row accumulation, FP64 vectors")
 
 
 def pseudopotentials(dh):
@@ -55,8 +59,8 @@ def peaks():
 
 
 def profile_traffic():
-    """DRAM bytes per launch of the FP32 product from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "fqhe_matvec_fp32_n12_2s33.md")
+    """DRAM bytes per launch of the measured block product from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "fqhe_block4_fp32_n12_2s33.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -221,45 +225,158 @@ def run_reference_arm(args, world, rank):
 
 # ------------------------------------------------------------------ B200 arm
 
-def time_to_e0(dh, H, dim, max_iter=400):
-    """Plain FP64 Lanczos to |dE| < 1e-13 |E| against FP32-product Lanczos + FP64 refinement, same start."""
+def _median_run(fn, runs):
     import torch
-    res = {}
+    out = []
+    for _ in range(runs):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        out.append((time.perf_counter() - t0, r))
+    out.sort(key=lambda t: t[0])
+    return out[len(out) // 2]
+
+
+def time_to_e0_single_sector(dh, H, runs=3, max_iter=600, precision=1e-13):
+    """The N=12, 2S=33 sector: plain FP64 single-vector Lanczos (CUDA-graph batches) against the
+    FP32-product forms with FP64 refinement (single vector, and block k = 2, 4), same seeded start,
+    the reference's convergence test at `precision`; median wall time of `runs` runs each."""
+    res = {"precision": precision, "runs": runs}
     H.set_precision("fp64")
-    lz = dh.BasicLanczosAlgorithm(H, 1, max_iter)
-    lz.SetEigenvaluePrecision(1e-13)
-    lz.InitializeLanczosAlgorithm(seed=0)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    r64 = lz.solve(max_iter, graph_batch=16)
-    torch.cuda.synchronize()
-    t64 = time.perf_counter() - t0
-    m64, _ = lz.counters()
-    del lz
-    lz = dh.BasicLanczosAlgorithm(H, 1, max_iter)
-    lz.InitializeLanczosAlgorithm(seed=0)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    r32 = lz.solve_refined(max_iter, precision=1e-13)
-    torch.cuda.synchronize()
-    t32 = time.perf_counter() - t0
-    del lz
-    e64 = float(r64["eigenvalues"][0])
-    res = {"fp64": {"seconds": t64, "e0": e64, "iterations": r64["iterations"], "matvecs": m64,
-                    "converged": r64["converged"]},
-           "fp32_refined": {"seconds": t32, "e0": r32["energy"], "e0_fp32_phase": r32["energy_fp32"],
-                            "residual": r32["residual"], "fp32_matvecs": r32["fp32_matvecs"],
-                            "fp64_matvecs": r32["fp64_matvecs"]},
-           "abs_e_minus_e_fp64": abs(r32["energy"] - e64),
-           "rel_e_minus_e_fp64": abs(r32["energy"] - e64) / abs(e64),
-           "speedup": t64 / t32 if t32 > 0 else None}
+
+    def plain():
+        lz = dh.BasicLanczosAlgorithm(H, 1, max_iter)
+        lz.SetEigenvaluePrecision(precision)
+        lz.InitializeLanczosAlgorithm(seed=0)
+        r = lz.solve(max_iter, graph_batch=16)
+        return float(r["eigenvalues"][0]), r["iterations"], lz.counters()[0]
+
+    t64, (e64, it64, mv64) = _median_run(plain, runs)
+    res["plain_fp64"] = {"seconds": t64, "e0": e64, "iterations": it64, "matvecs": mv64}
+    H.set_precision("fp32")
+    for k in (1, 2, 4):
+        def refined():
+            if k == 1:
+                lz = dh.BasicLanczosAlgorithm(H, 1, max_iter)
+            else:
+                lz = dh.BasicBlockLanczosAlgorithm(H, 1, max_iter, block_size=k)
+            lz.InitializeLanczosAlgorithm(seed=0)
+            return lz.solve_refined(max_iter, precision=precision)
+
+        t, r = _median_run(refined, runs)
+        res["fp32_refined_k%d" % k] = {"seconds": t, "e0": r["energy"], "e0_fp32_phase": r["energy_fp32"],
+                                       "abs_e_minus_e_fp64": abs(r["energy"] - e64),
+                                       "fp32_matvecs": r["fp32_matvecs"], "fp64_matvecs": r["fp64_matvecs"],
+                                       "speedup_vs_plain_fp64": t64 / t}
+    H.set_precision("fp32")
     ref = os.path.join(ROOT, "tests", "golden", "lanczos_n12_2s33_lz0_coulomb_basic.npz")
     if os.path.exists(ref):
         e_ref = float(np.load(ref)["eigenvalues"][0])
         res["reference_e0"] = e_ref
-        res["rel_e_minus_reference"] = {"fp64": abs(e64 - e_ref) / abs(e_ref),
-                                        "fp32_refined": abs(r32["energy"] - e_ref) / abs(e_ref)}
+        res["rel_e_minus_reference"] = {k: abs(v["e0"] - e_ref) / abs(e_ref) for k, v in res.items()
+                                        if isinstance(v, dict) and "e0" in v}
     return res
+
+
+def splitmix_uniform(seed, n, lo, hi):
+    i = np.arange(1, n + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + i * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return lo + (hi - lo) * (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def time_to_e0_all_sectors(dh, precision=1e-13, k=2):
+    """Every Lz sector of N=10, 2S=27 (2Lz = 0..180, 91 sectors) with V1 = 1 and V3, V5, V7 uniform
+    in [0, 0.5) from splitmix64 seed 1: the batched block form (FP32 products, FP64 refinement; and
+    FP64) against plain FP64 single-vector Lanczos run sector after sector (sectors of dimension
+    <= 200 go through the same dense path in both)."""
+    import torch
+    n, s = 10, 27
+    v = np.zeros(s + 1)
+    v[1] = 1.0
+    v[[3, 5, 7]] = splitmix_uniform(1, 3, 0.0, 0.5)
+    sectors = list(range(0, 181, 2))
+    dims = [dh.FermionOnSphere(n, lz, s).dim for lz in sectors]
+    res = {"sectors": len(sectors), "total_rows": int(sum(dims)), "largest": int(max(dims)), "block": k,
+           "precision": precision}
+    dh.fqhe_sectors_block_lanczos(n, s, sectors[-12:], v, block_size=k, max_iter=400)  # warm-up
+    for fp32 in (True, False):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = dh.fqhe_sectors_block_lanczos(n, s, sectors, v, block_size=k, max_iter=800, precision=precision,
+                                         fp32=fp32, full_diag_limit=200)
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        res["batched_%s" % ("fp32_refined" if fp32 else "fp64")] = {
+            "seconds": t, "energies": r["energies"], "block_products": r["block_products"],
+            "product_seconds": r["product_seconds"], "fp32_seconds": r["fp32_seconds"],
+            "refine_seconds": r["refine_seconds"], "refined_sectors": r["refined_sectors"]}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    dense = [lz for lz, d in zip(sectors, dims) if d <= 200]
+    plain = dict(zip(dense, dh.fqhe_sectors_block_lanczos(n, s, dense, v, block_size=4, max_iter=800,
+                                                          full_diag_limit=200)["energies"]))
+    for lz, d in zip(sectors, dims):
+        if d <= 200:
+            continue
+        space = dh.FermionOnSphere(n, lz, s)
+        H = dh.ParticleOnSphereGenericHamiltonian(space, n, s, v)
+        lzz = dh.BasicLanczosAlgorithm(H, 1, 800)
+        lzz.SetEigenvaluePrecision(precision)
+        lzz.InitializeLanczosAlgorithm(seed=100)
+        plain[lz] = float(lzz.solve(800, graph_batch=16)["eigenvalues"][0])
+        del lzz, H, space
+    torch.cuda.synchronize()
+    tp = time.perf_counter() - t0
+    e_plain = np.array([plain[lz] for lz in sectors])
+    res["plain_fp64_per_sector"] = {"seconds": tp}
+    for key in ("batched_fp32_refined", "batched_fp64"):
+        e = np.asarray(res[key].pop("energies"))
+        res[key]["max_abs_e_minus_plain_fp64"] = float(np.max(np.abs(e - e_plain)))
+        res[key]["speedup_vs_plain_fp64"] = tp / res[key]["seconds"]
+    res["ground_state"] = {"two_lz": int(sectors[int(np.argmin(e_plain))]), "e0": float(np.min(e_plain))}
+    return res
+
+
+def spin_chain_product(dh, flush, steps=5, k=2):
+    """The periodic J1-J2 chain, L = 32, Sz = 0 (dimension 601,080,390): FP32 block products of k
+    vectors (the config whose x and basis do not fit in L2), with their algorithmic bytes."""
+    import torch
+    t0 = time.perf_counter()
+    chain = dh.Spin1_2Chain(32, 0)
+    H = dh.SpinChainJ1J2Hamiltonian(chain, 1.0, 0.5)
+    H.set_precision("fp32")
+    dim = chain.dim
+    setup = time.perf_counter() - t0
+    x = torch.empty(dim, k, dtype=torch.float64, device="cuda")
+    x.uniform_(-1.0, 1.0)
+    y = torch.empty_like(x)
+    for _ in range(2):
+        H.block_multiply(x, y)
+    ms = []
+    for _ in range(steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        H.block_multiply(x, y)
+        b.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    flips = H.count_elements()
+    alg = dim * 4 + k * dim * 8 + k * (flips + dim) * 4
+    mean_s = statistics.mean(ms) / 1000.0
+    peak, kind = peaks()
+    del x, y, H, chain
+    torch.cuda.empty_cache()
+    return {"workload": "Spin1_2Chain L=32 Sz=0 periodic J1=1 J2=0.5 (dim %d), FP32 block k=%d" % (dim, k),
+            "setup_seconds": setup, "mean_launch_ms": mean_s * 1000.0, "hv_per_s": k / mean_s,
+            "off_diagonal_flips": flips, "algorithmic_bytes_per_launch": alg,
+            "roofline": {"bound": "hbm", "achieved": alg / mean_s / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / mean_s / 1e9 / peak, "peak_kind": kind}}
 
 
 def run_b200(args, world, rank, local):
@@ -276,17 +393,18 @@ def run_b200(args, world, rank, local):
     moves = H.count_elements()
     g = torch.Generator(device="cuda")
     g.manual_seed(0)
-    x = torch.rand(dim, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
-    x /= torch.linalg.vector_norm(x)
-    y = torch.empty_like(x)
+    xb = torch.rand(dim, BLOCK, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    yb = torch.empty_like(xb)
+    x1 = xb[:, 0].contiguous()
+    y1 = torch.empty_like(x1)
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
-    # FP64 product rate (for the record), then the FP32 product (the measured step)
-    def timed(precision, steps, warmup):
+    def timed(precision, k, steps, warmup):
         H.set_precision(precision)
+        x, y = (x1, y1) if k == 1 else (xb, yb)
         for _ in range(warmup):
             flush.zero_()
-            H.LowLevelMultiply(x, y)
+            H.block_multiply(x, y)
         starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
         ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -296,78 +414,89 @@ def run_b200(args, world, rank, local):
         for i in range(steps):
             flush.zero_()
             starts[i].record(stream)
-            H.LowLevelMultiply(x, y)
+            H.block_multiply(x, y)
             ends[i].record(stream)
         e1.record(stream)
         torch.cuda.synchronize()
         barrier(world)
-        total_ms = e0.elapsed_time(e1)
-        launch_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-        return total_ms, launch_ms
+        return e0.elapsed_time(e1), [s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)]
 
     if args.kernel_only:
-        total_ms, launch_ms = timed("fp32", args.steps, args.warmup)
+        total_ms, launch_ms = timed("fp32", BLOCK, args.steps, args.warmup)
         if rank == 0:
-            print(json.dumps({"kernel_only": True, "dim": dim, "elements_per_product": moves, "steps": args.steps,
-                              "mean_launch_ms": statistics.mean(launch_ms), "ms_per_step": total_ms / args.steps}))
+            print(json.dumps({"kernel_only": True, "dim": dim, "block": BLOCK, "elements_per_product": moves,
+                              "steps": args.steps, "mean_launch_ms": statistics.mean(launch_ms),
+                              "ms_per_step": total_ms / args.steps}))
         return
-    fp64_ms, fp64_launch = timed("fp64", max(5, args.steps // 10), 2)
+    # single-vector rates for the record (the plain FP64 form and the FP32 single-vector form)
+    singles = {}
+    for prec in ("fp64", "fp32"):
+        t_ms, l_ms = timed(prec, 1, max(5, args.steps // 10), 3)
+        singles[prec] = {"hv_per_s": len(l_ms) / (t_ms / 1000.0), "mean_launch_ms": statistics.mean(l_ms)}
+    t_ms, l_ms = timed("fp64", BLOCK, max(5, args.steps // 10), 3)
+    singles["fp64_block%d" % BLOCK] = {"hv_per_s": BLOCK * len(l_ms) / (t_ms / 1000.0),
+                                       "mean_launch_ms": statistics.mean(l_ms)}
     with ClockSampler(local) as clocks:
-        total_ms, launch_ms = timed("fp32", args.steps, args.warmup)
+        total_ms, launch_ms = timed("fp32", BLOCK, args.steps, args.warmup)
     total_ms = reduce_max(total_ms, world)
-    value = world * args.steps / (total_ms / 1000.0)
+    value = world * BLOCK * args.steps / (total_ms / 1000.0)
 
-    # roofline of the FP32 product: algorithmic bytes per launch (basis word + FP64 y + FP32 x per
-    # off-diagonal element and for the row itself), over the mean device time of one C-ABI call
-    # (FP64->FP32 conversion of x included)
+    # roofline of the block product: algorithmic bytes per launch (basis word and k FP64 outputs per
+    # row, k FP32 inputs per off-diagonal element and for the row itself) over the mean device time
+    # of one C-ABI call (the FP64 -> FP32 conversion of x included)
     c_n2 = N_FERMIONS * (N_FERMIONS - 1) // 2
     nnz_off = moves - c_n2 * dim
-    alg_bytes = dim * 8 + dim * 8 + (nnz_off + dim) * 4
+    alg_bytes = dim * 8 + BLOCK * dim * 8 + BLOCK * (nnz_off + dim) * 4
     launch_mean = statistics.mean(launch_ms) / 1000.0
     peak, peak_kind = peaks()
     achieved = alg_bytes / launch_mean / 1e9
     traffic = profile_traffic()
 
     # end to end through the public API with pinned host buffers (H2D of x, D2H of y every step)
-    hx = torch.empty(dim, dtype=torch.float64, pin_memory=True)
-    hy = torch.empty(dim, dtype=torch.float64, pin_memory=True)
-    hx.copy_(x.cpu())
+    hx = torch.empty(dim, BLOCK, dtype=torch.float64, pin_memory=True)
+    hy = torch.empty(dim, BLOCK, dtype=torch.float64, pin_memory=True)
+    hx.copy_(xb.cpu())
     hxn, hyn = hx.numpy(), hy.numpy()
     H.set_precision("fp32")
     e2e_steps = max(3, min(args.steps, 40))
     for _ in range(2):
-        H.LowLevelMultiply(hxn, hyn)
+        H.block_multiply(hxn, hyn)
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        H.LowLevelMultiply(hxn, hyn)
+        H.block_multiply(hxn, hyn)
     torch.cuda.synchronize()
     e2e_s = reduce_max(time.perf_counter() - t0, world)
-    e2e_value = world * e2e_steps / e2e_s
+    e2e_value = world * BLOCK * e2e_steps / e2e_s
 
-    tte = None
+    tte = tte_c = spin = None
     if not args.no_solve:
-        tte = time_to_e0(dh, H, dim)
+        tte = time_to_e0_single_sector(dh, H)
+        tte_c = time_to_e0_all_sectors(dh)
+        del xb, yb, hx, hy
+        torch.cuda.empty_cache()
+        spin = spin_chain_product(dh, flush)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload_name(), "dim": dim, "elements_per_product": moves,
-                       "l2": "flushed: 256 MiB write before every step",
+            "config": {"workload": workload_name(), "dim": dim, "block": BLOCK, "elements_per_product": moves,
+                       "hv_per_step": BLOCK, "l2": "flushed: 256 MiB write before every step",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "gpu_launches": 2 * args.steps,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": dim * 8, "d2h_bytes_per_step": dim * 8,
-                    "steps": e2e_steps, "buffers": "pinned host"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": dim * BLOCK * 8,
+                    "d2h_bytes_per_step": dim * BLOCK * 8, "steps": e2e_steps, "buffers": "pinned host"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes,
-                         "kernel": "fqhe_matvec_kernel<float> (+ x FP64->FP32 conversion)",
+                         "kernel": "fqhe_split_kernel<float, 4, RANGE=0, LR_SMEM=0, IL=1> (+ x FP64->FP32 conversion)",
                          "mean_launch_ms": launch_mean * 1000.0},
-            "fp64_product": {"value": len(fp64_launch) / (fp64_ms / 1000.0), "unit": UNIT,
-                             "mean_launch_ms": statistics.mean(fp64_launch)},
+            "single_vector": singles,
             "clocks": clocks.summary(),
-            "time_to_e0": tte}
+            "time_to_e0": tte,
+            "time_to_e0_all_sectors": tte_c,
+            "spin_chain_l32": spin}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if rank == 0:
