@@ -8,7 +8,8 @@ input already in HBM, the batched form of the block Lanczos: FP32 matrix element
 accumulation, FP64 in and out.  L2 is flushed (a 256 MiB write) before every step.  The line also
 carries the single-vector FP64 / FP32 rates, the time to E0 of the sector (plain FP64 against FP32
 products + FP64 refinement), of all 91 sectors of N = 10, 2S = 27 (batched against sector by
-sector), and the L = 32 J1-J2 chain product with its roofline.
+sector), the adjoint gradients of N = 10, 2S = 27 against the reference's and finite differences,
+and the L = 32 J1-J2 chain product with its roofline.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -379,6 +380,52 @@ def spin_chain_product(dh, flush, steps=5, k=2):
                          "frac": alg / mean_s / 1e9 / peak, "peak_kind": kind}}
 
 
+def gradients_two_sectors(dh, h=1e-6):
+    """dE0/dV_m and d(neutral gap)/dV_m, odd m = 1..27, for N=10, 2S=27, Lz = 0 and 1 (Coulomb V_m
+    plus uniform [-0.05, 0.05) noise from splitmix64 seed 2) by the adjoint kernel (Hellmann-Feynman
+    on the GPU ground states), against the reference's FP64 gradient (committed fixture) and
+    central finite differences of the GPU E0 with step h."""
+    import torch
+    from diagham_b200.autograd import ground_state_energy, neutral_gap
+    fx = [np.load(os.path.join(ROOT, "tests", "golden", "gradient_n10_2s27_lz%d.npz" % lz)) for lz in (0, 2)]
+    v = fx[0]["v"]
+    odd = np.arange(1, 28, 2)
+    hs = []
+    for lz in (0, 2):
+        sp = dh.FermionOnSphere(10, lz, 27)
+        hs.append((sp, dh.ParticleOnSphereGenericHamiltonian(sp, 10, 27, v)))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    V = torch.tensor(v, dtype=torch.float64, requires_grad=True)
+    gap = neutral_gap(V, hs[0][1], hs[1][1])
+    gap.backward()
+    torch.cuda.synchronize()
+    t_gap = time.perf_counter() - t0
+    g_gap = V.grad.numpy()[odd].copy()
+    res = {"workload": "FermionOnSphere N=10 2S=27 2Lz=0,2 (dims %d, %d), Coulomb + U[-0.05,0.05) seed 2"
+                       % (hs[0][0].dim, hs[1][0].dim),
+           "gap_and_gradient_seconds": t_gap, "gap": float(gap.detach()),
+           "gap_reference": float(fx[1]["eigenvalues"][0] - fx[0]["eigenvalues"][0]),
+           "max_abs_dgap_minus_reference": float(np.max(np.abs(
+               g_gap - (fx[1]["expectation"][odd] - fx[0]["expectation"][odd]))))}
+    worst_ref = worst_fd = 0.0
+    for (sp, H), z in zip(hs, fx):
+        V = torch.tensor(v, dtype=torch.float64, requires_grad=True)
+        ground_state_energy(V, H).backward()
+        g = V.grad.numpy()[odd]
+        worst_ref = max(worst_ref, float(np.max(np.abs(g - z["expectation"][odd]))))
+        for i, m in enumerate(odd):
+            vp, vm = v.copy(), v.copy()
+            vp[m] += h
+            vm[m] -= h
+            fd = (float(ground_state_energy(torch.tensor(vp), H)) - float(ground_state_energy(torch.tensor(vm), H))) / (2 * h)
+            worst_fd = max(worst_fd, abs(fd - g[i]))
+    res["max_abs_de0_minus_reference"] = worst_ref
+    res["max_abs_de0_minus_central_difference"] = worst_fd
+    res["finite_difference_step"] = h
+    return res
+
+
 def run_b200(args, world, rank, local):
     import torch
     import diagham_b200 as dh
@@ -470,10 +517,11 @@ def run_b200(args, world, rank, local):
     e2e_s = reduce_max(time.perf_counter() - t0, world)
     e2e_value = world * BLOCK * e2e_steps / e2e_s
 
-    tte = tte_c = spin = None
+    tte = tte_c = spin = grads = None
     if not args.no_solve:
         tte = time_to_e0_single_sector(dh, H)
         tte_c = time_to_e0_all_sectors(dh)
+        grads = gradients_two_sectors(dh)
         del xb, yb, hx, hy
         torch.cuda.empty_cache()
         spin = spin_chain_product(dh, flush)
@@ -496,6 +544,7 @@ def run_b200(args, world, rank, local):
             "clocks": clocks.summary(),
             "time_to_e0": tte,
             "time_to_e0_all_sectors": tte_c,
+            "gradients": grads,
             "spin_chain_l32": spin}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()

@@ -261,6 +261,33 @@ def slow_fixtures(tmp):
          **read_lanczos(lf))
 
 
+def gradient_fixtures(tmp):
+    # the differentiation workload: N = 10, 2S = 27, 2Lz = 0 and 2 (Lz = 0, 1); LLL Coulomb V_m
+    # (every m) plus uniform [-0.05, 0.05) noise from splitmix64 seed 2.  The reference's
+    # BasicLanczosAlgorithmWithGroundState (precision 1e-14, start vector seed 0) gives E0 and psi;
+    # ParticleOnSphereGenericHamiltonian(V = e_m).MatrixElement(psi, psi) for every m is the FP64
+    # reference gradient dE0/dV_m (Hellmann-Feynman; the interaction factors are linear in V)
+    p = os.path.join(tmp, "pp.bin")
+    run("pseudopotentials", 27, p)
+    v = np.fromfile(p, np.float64) + uniform(2, 28, -0.05, 0.05)
+    vf = os.path.join(tmp, "vg.bin")
+    v.tofile(vf)
+    threads = os.cpu_count() or 1
+    for lz in (0, 2):
+        bf = os.path.join(tmp, "b.bin")
+        run("fqhe_basis", 10, 27, lz, bf)
+        dim, _, _ = read_basis(bf)
+        xf = os.path.join(tmp, "xg.vec")
+        write_vector(xf, splitmix_vector(0, dim))
+        lf, gf, ef = (os.path.join(tmp, n) for n in ("lg.out", "gg.vec", "eg.bin"))
+        cmd = run("fqhe_lanczos", 10, 27, lz, vf, "ground", 1, 1, 600, 1e-14, lf, gf, xf,
+                  env={"REF_THREADS": str(threads)})
+        run("fqhe_expect", 10, 27, lz, vf, gf, ef)
+        e = np.fromfile(ef, np.float64)
+        save("gradient_n10_2s27_lz%d.npz" % lz, cmd + " (REF_THREADS=%d)" % threads, v=v, seed=0, precision=1e-14,
+             dim=dim, expectation=e[:-1], energy_expectation=e[-1], **read_lanczos(lf))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--slow", action="store_true")
@@ -285,6 +312,8 @@ def main():
             block_fixture(tmp, 6, 15, 0, 4)
         if args.only in (None, "spin"):
             spin_fixtures(tmp)
+        if args.only in (None, "gradient"):
+            gradient_fixtures(tmp)
         if args.slow:
             slow_fixtures(tmp)
 
