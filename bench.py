@@ -343,12 +343,12 @@ def time_to_e0_all_sectors(dh, precision=1e-13, k=2):
     return res
 
 
-def spin_chain_product(dh, flush, steps=5, k=2):
+def spin_chain_product(dh, flush, steps=5, k=2, length=32, warmup=2):
     """The periodic J1-J2 chain, L = 32, Sz = 0 (dimension 601,080,390): FP32 block products of k
     vectors (the config whose x and basis do not fit in L2), with their algorithmic bytes."""
     import torch
     t0 = time.perf_counter()
-    chain = dh.Spin1_2Chain(32, 0)
+    chain = dh.Spin1_2Chain(length, 0)
     H = dh.SpinChainJ1J2Hamiltonian(chain, 1.0, 0.5)
     H.set_precision("fp32")
     dim = chain.dim
@@ -356,7 +356,8 @@ def spin_chain_product(dh, flush, steps=5, k=2):
     x = torch.empty(dim, k, dtype=torch.float64, device="cuda")
     x.uniform_(-1.0, 1.0)
     y = torch.empty_like(x)
-    for _ in range(2):
+    for _ in range(warmup):
+        flush.zero_()
         H.block_multiply(x, y)
     ms = []
     for _ in range(steps):
@@ -373,7 +374,7 @@ def spin_chain_product(dh, flush, steps=5, k=2):
     peak, kind = peaks()
     del x, y, H, chain
     torch.cuda.empty_cache()
-    return {"workload": "Spin1_2Chain L=32 Sz=0 periodic J1=1 J2=0.5 (dim %d), FP32 block k=%d" % (dim, k),
+    return {"workload": "Spin1_2Chain L=%d Sz=0 periodic J1=1 J2=0.5 (dim %d), FP32 block k=%d" % (length, dim, k),
             "setup_seconds": setup, "mean_launch_ms": mean_s * 1000.0, "hv_per_s": k / mean_s,
             "off_diagonal_flips": flips, "algorithmic_bytes_per_launch": alg,
             "roofline": {"bound": "hbm", "achieved": alg / mean_s / 1e9, "peak": peak, "unit": "GB/s",
@@ -433,6 +434,12 @@ def run_b200(args, world, rank, local):
     _build.build()
     torch.cuda.set_device(local)
     stream = torch.cuda.current_stream()
+    if args.kernel_only and args.chain_length:
+        flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+        r = spin_chain_product(dh, flush, steps=args.steps, length=args.chain_length, warmup=args.warmup)
+        if rank == 0:
+            print(json.dumps(dict(kernel_only=True, **r)))
+        return
     space = dh.FermionOnSphere(N_FERMIONS, TWO_LZ, TWO_S)
     dim = space.dim
     H = dh.ParticleOnSphereGenericHamiltonian(space, N_FERMIONS, TWO_S, pseudopotentials(dh))
@@ -562,6 +569,8 @@ def main():
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only the timed FP32 products (the short command used for ncu captures)")
+    ap.add_argument("--chain-length", type=int, default=0,
+                    help="with --kernel-only: time the J1-J2 chain block product (k = 2) at this length instead")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

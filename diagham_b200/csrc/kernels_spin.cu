@@ -31,25 +31,111 @@ __device__ __forceinline__ long long spin_full_index(uint32_t t, int L, long lon
   return D - 1 - rank;
 }
 
-template <typename TG, int K>
-__global__ void __launch_bounds__(kSpinThreads) spin_j1j2_kernel(SpinDevice sp, MatvecArgs a) {
-  __shared__ int binom[33 * 33];  // binom[n * 33 + k] = C(n, k), n, k <= 32
+// the K values of target row idx: one vector load when the block is row-interleaved (IL)
+template <typename TG, int K, bool IL>
+__device__ __forceinline__ void spin_gather(const TG* x, const MatvecArgs& a, long long idx, TG (&v)[K]) {
+  if constexpr (IL && sizeof(TG) == 4 && K == 4) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(x + idx * 4));
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+  } else if constexpr (IL && sizeof(TG) == 4 && K == 2) {
+    const float2 q = __ldg(reinterpret_cast<const float2*>(x + idx * 2));
+    v[0] = q.x; v[1] = q.y;
+  } else if constexpr (IL && sizeof(TG) == 8 && (K == 2 || K == 4)) {
+#pragma unroll
+    for (int j = 0; j < K; j += 2) {
+      const double2 q = __ldg(reinterpret_cast<const double2*>(x + idx * K) + j / 2);
+      v[j] = q.x;
+      v[j + 1] = q.y;
+    }
+  } else {
+    const TG* p = x + idx * a.ld;
+#pragma unroll
+    for (int q = 0; q < K; ++q) v[q] = __ldg(p + q * a.vstride);
+  }
+}
+
+template <typename TG, int K, bool IL>
+__device__ __forceinline__ void spin_add(TG (&acc)[K], TG h, const TG* x, const MatvecArgs& a, long long idx) {
+  TG v[K];
+  spin_gather<TG, K, IL>(x, a, idx, v);
+#pragma unroll
+  for (int q = 0; q < K; ++q) acc[q] += h * v[q];
+}
+
+// Shared tables of the product kernel (every entry an int: C(32, 16) = 601,080,390 < 2^31).
+//   j1[(j << 5) | kk]            J1 flip (j, j+1) index step: C(L-2-j, kk), kk = up spins at sites > j+1
+//   j2[(mid << 10) | (j << 5) | kk]  J2 flip (j, j+2) step, kk = up spins at sites > j+2, mid = spin j+1:
+//                                  mid = 0: C(p-1, kk) + C(p-2, kk); mid = 1: 2 C(p-1, kk+1) - C(p-2, kk+1), p = L-1-j
+//   nib[(n * 33 + c) * 16 + v]  rank contribution of nibble n (positions p = 4n..4n+3 of the
+//                                  bit-reversed word) holding v, with c up spins at lower positions:
+//                                  sum over bits i of v (ascending) of C(4n+i, c + (bits of v below i) + 1)
+struct SpinTables {
+  int binom[33 * 33];
+  int j1[32 * 32];
+  int j2[2 * 32 * 32];
+  int nib[8 * 33 * 16];
+};
+
+__device__ void build_spin_tables(SpinTables& t, int L) {
   for (int i = threadIdx.x; i < 33 * 33; i += blockDim.x) {
     const int n = i / 33, k = i % 33;
     long long c = 1;
     if (k > n) c = 0;
     else
       for (int q = 1; q <= k; ++q) c = c * (n - k + q) / q;
-    binom[i] = (int)c;
+    t.binom[i] = (int)c;
   }
   __syncthreads();
+  auto C = [&](int n, int k) { return (n < 0 || k < 0 || k > n) ? 0 : t.binom[n * 33 + k]; };
+  for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) {
+    const int j = i >> 5, kk = i & 31;
+    t.j1[i] = (j <= L - 2) ? C(L - 2 - j, kk) : 0;
+    const int p = L - 1 - j;
+    t.j2[i] = (j <= L - 3) ? C(p - 1, kk) + C(p - 2, kk) : 0;
+    t.j2[1024 + i] = (j <= L - 3) ? 2 * C(p - 1, kk + 1) - C(p - 2, kk + 1) : 0;
+  }
+  for (int i = threadIdx.x; i < 8 * 33 * 16; i += blockDim.x) {
+    const int v = i & 15, c = (i >> 4) % 33, n = (i >> 4) / 33;
+    int sum = 0, below = 0;
+    for (int b = 0; b < 4; ++b)
+      if ((v >> b) & 1) {
+        sum += C(4 * n + b, c + below + 1);
+        ++below;
+      }
+    t.nib[i] = sum;
+  }
+  __syncthreads();
+}
+
+// index of word t (chain bits only): D - 1 - sum_k C(p_k, k) over the up spins at p = L-1-site in
+// ascending order, summed nibble by nibble of the bit-reversed word
+__device__ __forceinline__ int spin_rank_index(const SpinTables& tb, uint32_t t, int L, int D) {
+  const uint32_t tr = __brev(t) >> (32 - L);
+  int rank = 0, c = 0;
+#pragma unroll
+  for (int n = 0; n < 8; ++n) {
+    const uint32_t v = (tr >> (4 * n)) & 15u;
+    rank += tb.nib[(n * 33 + c) * 16 + v];
+    c += __popc(v);
+  }
+  return D - 1 - rank;
+}
+
+// IL: x, y (and xdiag) are row-interleaved [row][K] blocks (ld = K, vstride = 1).  Rows and
+// indices are 32-bit (a 32-site chain has at most C(32, 16) < 2^31 states); lanes own consecutive
+// rows, which share their low sites and so mostly the same index step for a given bond: the
+// gathers of a warp coalesce.  Flips are taken two at a time so that two gathers are in flight.
+template <typename TG, int K, bool IL>
+__global__ void __launch_bounds__(kSpinThreads) spin_j1j2_kernel(SpinDevice sp, MatvecArgs a) {
+  __shared__ SpinTables tb;
   const int L = sp.length;
-  const long long D = sp.dim;
+  build_spin_tables(tb, L);
+  const int D = (int)sp.dim;
   const uint32_t maskL = (L == 32) ? 0xffffffffu : ((1u << L) - 1u);
   const TG hj1 = (TG)(0.5 * sp.j1), hj2 = (TG)(0.5 * sp.j2);
   const TG* x = static_cast<const TG*>(a.x);
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < D; r += stride) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < D; r += stride) {
     const uint32_t w = __ldg(sp.words + r);
     const uint32_t rot1 = ((w >> 1) | (w << (L - 1))) & maskL;  // bit j = spin j+1 (mod L)
     const uint32_t rot2 = ((w >> 2) | (w << (L - 2))) & maskL;  // bit j = spin j+2 (mod L)
@@ -57,68 +143,85 @@ __global__ void __launch_bounds__(kSpinThreads) spin_j1j2_kernel(SpinDevice sp, 
     TG acc[K];
 #pragma unroll
     for (int j = 0; j < K; ++j) acc[j] = TG(0);
-    // J1 bonds (j, j+1), j = 0 .. L-2
-    uint32_t f1 = d1 & (maskL >> 1);
-    while (f1) {
-      const int j = __ffs(f1) - 1;
-      f1 &= f1 - 1u;
-      const int kk = __popcll((uint64_t)w >> (j + 2));  // j + 2 may equal 32
-      const long long delta = binom[(L - 2 - j) * 33 + kk];
-      const long long idx = ((w >> j) & 1u) ? r + delta : r - delta;
-      const TG* xp = x + idx * a.ld;
+    // J1 bonds (j, j+1), j = 0 .. L-2: the up spin moves one site; up at j moves the index forward
+    uint32_t f = d1 & (maskL >> 1);
+    while (f) {
+      const int ja = __ffs(f) - 1;
+      f &= f - 1u;
+      const bool two = f != 0u;
+      const int jb = two ? __ffs(f) - 1 : ja;
+      f &= f - 1u;
+      const int da = tb.j1[(ja << 5) | __popc(__funnelshift_rc(w, 0u, ja + 2))];
+      const int db = tb.j1[(jb << 5) | __popc(__funnelshift_rc(w, 0u, jb + 2))];
+      const int ia = ((w >> ja) & 1u) ? r + da : r - da;
+      const int ib = ((w >> jb) & 1u) ? r + db : r - db;
+      TG xa[K], xb[K];
+      spin_gather<TG, K, IL>(x, a, ia, xa);
+      spin_gather<TG, K, IL>(x, a, ib, xb);
+      const TG hb = two ? hj1 : TG(0);
 #pragma unroll
-      for (int q = 0; q < K; ++q) acc[q] += hj1 * __ldg(xp + q * a.vstride);
+      for (int q = 0; q < K; ++q) acc[q] += hj1 * xa[q] + hb * xb[q];
     }
     // J2 bonds (j, j+2), j = 0 .. L-3
-    uint32_t f2 = d2 & (maskL >> 2);
-    while (f2) {
-      const int j = __ffs(f2) - 1;
-      f2 &= f2 - 1u;
-      const int kk = __popcll((uint64_t)w >> (j + 3));  // j + 3 may equal 32
-      const int p = L - 1 - j;
-      long long delta;
-      if (!((w >> (j + 1)) & 1u))
-        delta = (long long)binom[(p - 1) * 33 + kk] + binom[(p - 2) * 33 + kk];
-      else
-        delta = 2ll * binom[(p - 1) * 33 + kk + 1] - binom[(p - 2) * 33 + kk + 1];
-      const long long idx = ((w >> j) & 1u) ? r + delta : r - delta;
-      const TG* xp = x + idx * a.ld;
+    f = d2 & (maskL >> 2);
+    while (f) {
+      const int ja = __ffs(f) - 1;
+      f &= f - 1u;
+      const bool two = f != 0u;
+      const int jb = two ? __ffs(f) - 1 : ja;
+      f &= f - 1u;
+      const int da = tb.j2[(((w >> (ja + 1)) & 1u) << 10) | (ja << 5) | __popc(__funnelshift_rc(w, 0u, ja + 3))];
+      const int db = tb.j2[(((w >> (jb + 1)) & 1u) << 10) | (jb << 5) | __popc(__funnelshift_rc(w, 0u, jb + 3))];
+      const int ia = ((w >> ja) & 1u) ? r + da : r - da;
+      const int ib = ((w >> jb) & 1u) ? r + db : r - db;
+      TG xa[K], xb[K];
+      spin_gather<TG, K, IL>(x, a, ia, xa);
+      spin_gather<TG, K, IL>(x, a, ib, xb);
+      const TG hb = two ? hj2 : TG(0);
 #pragma unroll
-      for (int q = 0; q < K; ++q) acc[q] += hj2 * __ldg(xp + q * a.vstride);
+      for (int q = 0; q < K; ++q) acc[q] += hj2 * xa[q] + hb * xb[q];
     }
-    // bonds that wrap: J1 (L-1, 0), J2 (L-2, 0) and (L-1, 1)
-    if ((d1 >> (L - 1)) & 1u) {
-      const long long idx = spin_full_index<TG>(w ^ (1u | (1u << (L - 1))), L, D, binom);
-      const TG* xp = x + idx * a.ld;
-#pragma unroll
-      for (int q = 0; q < K; ++q) acc[q] += hj1 * __ldg(xp + q * a.vstride);
-    }
-    if ((d2 >> (L - 2)) & 1u) {
-      const long long idx = spin_full_index<TG>(w ^ (1u | (1u << (L - 2))), L, D, binom);
-      const TG* xp = x + idx * a.ld;
-#pragma unroll
-      for (int q = 0; q < K; ++q) acc[q] += hj2 * __ldg(xp + q * a.vstride);
-    }
-    if ((d2 >> (L - 1)) & 1u) {
-      const long long idx = spin_full_index<TG>(w ^ (2u | (1u << (L - 1))), L, D, binom);
-      const TG* xp = x + idx * a.ld;
-#pragma unroll
-      for (int q = 0; q < K; ++q) acc[q] += hj2 * __ldg(xp + q * a.vstride);
-    }
+    // bonds that wrap: J1 (L-1, 0), J2 (L-2, 0) and (L-1, 1): the moved spin passes the others
+    if ((d1 >> (L - 1)) & 1u)
+      spin_add<TG, K, IL>(acc, hj1, x, a, spin_rank_index(tb, w ^ (1u | (1u << (L - 1))), L, D));
+    if ((d2 >> (L - 2)) & 1u)
+      spin_add<TG, K, IL>(acc, hj2, x, a, spin_rank_index(tb, w ^ (1u | (1u << (L - 2))), L, D));
+    if ((d2 >> (L - 1)) & 1u)
+      spin_add<TG, K, IL>(acc, hj2, x, a, spin_rank_index(tb, w ^ (2u | (1u << (L - 1))), L, D));
     // diagonal: sum over bonds of J Sz_i Sz_j = J/4 (L - 2 * #antiparallel bonds), plus the shift
     const double diag = 0.25 * sp.j1 * (double)(L - 2 * __popc(d1)) + 0.25 * sp.j2 * (double)(L - 2 * __popc(d2)) +
                         a.shift;
     const bool on_diag = (r >= a.row_first && r < a.row_last);
     double* y = static_cast<double*>(a.y);
+    double out[K];
 #pragma unroll
     for (int q = 0; q < K; ++q) {
       double v = (double)acc[q];
       if (on_diag) {
-        const double xd = a.xdiag ? a.xdiag[r * a.ld + q * a.vstride] : (double)x[r * a.ld + q * a.vstride];
+        const long long xo = IL ? (long long)r * K + q : r * a.ld + q * a.vstride;
+        const double xd = a.xdiag ? a.xdiag[xo] : (double)x[xo];
         v += diag * xd;
       }
-      double* yp = y + r * a.ld_y + q * a.vstride_y;
-      *yp = a.accumulate ? (*yp + v) : v;
+      out[q] = v;
+    }
+    if constexpr (IL && K % 2 == 0) {
+      double2* yp = reinterpret_cast<double2*>(y + (long long)r * K);
+#pragma unroll
+      for (int q = 0; q < K; q += 2) {
+        double2 o = make_double2(out[q], out[q + 1]);
+        if (a.accumulate) {
+          const double2 old = yp[q / 2];
+          o.x += old.x;
+          o.y += old.y;
+        }
+        yp[q / 2] = o;
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < K; ++q) {
+        double* yp = y + r * a.ld_y + q * a.vstride_y;
+        *yp = a.accumulate ? (*yp + out[q]) : out[q];
+      }
     }
   }
 }
@@ -235,6 +338,19 @@ int launch_spin_typed(const SpinDevice& sp, MatvecArgs a, cudaStream_t s) {
     DH_CUDA(cudaGetLastError());
     return DH_OK;
   }
+  const int nv = a.nbr_vectors;
+  if ((nv == 2 || nv == 4) && a.ld == nv && a.vstride == 1 && a.ld_y == nv && a.vstride_y == 1) {
+    // row-interleaved block: one launch with vector gathers and stores
+    auto kern = (nv == 4) ? spin_j1j2_kernel<TG, 4, true> : spin_j1j2_kernel<TG, 2, true>;
+    int per_sm = 0;
+    DH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSpinThreads, 0));
+    long long grid = (long long)sms * (per_sm > 0 ? per_sm : 1);
+    if (need < grid) grid = need;
+    if (grid < 1) grid = 1;
+    kern<<<(unsigned)grid, kSpinThreads, 0, s>>>(sp, a);
+    DH_CUDA(cudaGetLastError());
+    return DH_OK;
+  }
   int left = a.nbr_vectors, done = 0;
   while (left > 0) {
     int k = left >= 2 ? 2 : 1;
@@ -245,16 +361,16 @@ int launch_spin_typed(const SpinDevice& sp, MatvecArgs a, cudaStream_t s) {
     b.nbr_vectors = k;
     int per_sm = 0;
     if (k == 2)
-      DH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spin_j1j2_kernel<TG, 2>, kSpinThreads, 0));
+      DH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spin_j1j2_kernel<TG, 2, false>, kSpinThreads, 0));
     else
-      DH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spin_j1j2_kernel<TG, 1>, kSpinThreads, 0));
+      DH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spin_j1j2_kernel<TG, 1, false>, kSpinThreads, 0));
     long long grid = (long long)sms * (per_sm > 0 ? per_sm : 1);
     if (need < grid) grid = need;
     if (grid < 1) grid = 1;
     if (k == 2)
-      spin_j1j2_kernel<TG, 2><<<(unsigned)grid, kSpinThreads, 0, s>>>(sp, b);
+      spin_j1j2_kernel<TG, 2, false><<<(unsigned)grid, kSpinThreads, 0, s>>>(sp, b);
     else
-      spin_j1j2_kernel<TG, 1><<<(unsigned)grid, kSpinThreads, 0, s>>>(sp, b);
+      spin_j1j2_kernel<TG, 1, false><<<(unsigned)grid, kSpinThreads, 0, s>>>(sp, b);
     DH_CUDA(cudaGetLastError());
     left -= k;
     done += k;
