@@ -58,6 +58,7 @@ SIGNATURES = {
     "dh_hamiltonian_low_level_multiply": ([_vp, _vp, _vp, _c_i64, _c_i64], _c_int),
     "dh_hamiltonian_low_level_multiple_add_multiply": ([_vp, _vp, _vp, _c_int, _c_i64, _c_i64], _c_int),
     "dh_hamiltonian_block_multiply": ([_vp, _vp, _vp, _c_int], _c_int),
+    "dh_hamiltonian_autotune": ([_vp, _c_int, _c_int, _vp], _c_int),
     "dh_hamiltonian_matrix_element": ([_vp, _vp, _vp, _vp], _c_int),
     "dh_hamiltonian_row_elements": ([_vp, _c_i64, _vp, _vp, _vp, _c_int, _ip], _c_int),
     "dh_hamiltonian_pseudopotential_adjoint": ([_vp, _vp, _vp, _vp], _c_int),
@@ -269,6 +270,13 @@ class _Hamiltonian:
         _check(_lib.dh_hamiltonian_block_multiply(self._handle, s.ptr, d.ptr, k))
         d.finish()
         return y
+
+    def autotune(self, block_size=1, repeats=3):
+        """Time the product's kernel forms on this Hamiltonian and keep the fastest one."""
+        out = np.zeros(7, np.float64)
+        _check(_lib.dh_hamiltonian_autotune(self._handle, block_size, repeats, out.ctypes.data))
+        return dict(best_ms=out[0], kernel_variant={0: "split", 1: "generic", 2: "split+smem"}[int(out[1])],
+                    low_bits=int(out[2]), ms_k1=out[3], ms_k2=out[4], ms_k4=out[5], candidates=int(out[6]))
 
     def count_elements(self):
         """Elements one product generates (moves incl. diagonal ones; spin flips)."""

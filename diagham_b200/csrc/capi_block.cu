@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <chrono>
 #include <functional>
+#include <memory>
 #include <new>
 #include <thread>
 #include <vector>
@@ -53,12 +54,17 @@ struct BlockSector {
 // deterministic): the symmetrised A, the B^T used by the update, and the two CholQR inverses
 struct StepRecord {
   std::vector<double> A, Bt, inv1, inv2;
+  std::vector<double> lock;  // start-block projection coefficients (empty when not locked)
   bool have_prev = false;
 };
 
 struct BlockEngine {
   int k = 4, nsec = 0, nev = 1, precision = DH_PRECISION_FP64;
   double eig_precision = 1e-14;
+  // > 0: converge on the lowest Ritz vector's residual instead, |r|^2 < residual_target |lambda|
+  // (|r| = |B_m s_last| from the band matrix), used by the mixed-precision restarts whose Ritz
+  // values move at the FP32 rounding level long after the vector is accurate enough
+  double residual_target = 0.0;
   int max_iter = 400;  // in vectors, as the reference's --iter-max
   long long total = 0;
   std::vector<long long> off;
@@ -74,8 +80,13 @@ struct BlockEngine {
   std::function<int(const double*, const float*, double*)> product;
   double product_ms = 0.0;
   long long products = 0;
+  long long fp64_products = 0;
   std::vector<StepRecord> history;
-  DevBuf start_block;    // the orthonormal start block, for replays
+  // mixed-precision restart from a Ritz block: the start block's product in FP64, the following
+  // ones in the engine's precision, every new block projected against the start block
+  bool fp64_first_product = false;
+  bool lock_start = false;
+  DevBuf start_block;    // the orthonormal start block, for replays and the projection
   DevBuf store;          // every block when keep_blocks (store_cap blocks of total * k)
   int store_cap = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -243,10 +254,15 @@ int engine_qr(BlockEngine& e, double* x, std::vector<double>& B, float* x32, con
   return DH_OK;
 }
 
-int engine_product(BlockEngine& e, const double* x, double* y) {
+// y = H x; step = the block step the product belongs to (-1: outside the recurrence)
+int engine_product(BlockEngine& e, const double* x, double* y, int step = -1) {
+  const int saved = e.precision;
+  if (step == 0 && e.fp64_first_product) e.precision = DH_PRECISION_FP64;
   const float* x32 = e.precision == DH_PRECISION_FP32 ? e.x32.as<float>() : nullptr;
+  if (e.precision == DH_PRECISION_FP64) ++e.fp64_products;
   DH_CUDA(cudaEventRecord(e.ev0, e.stream));
   int rc = e.product(x, x32, y);
+  e.precision = saved;
   if (rc != DH_OK) return rc;
   DH_CUDA(cudaEventRecord(e.ev1, e.stream));
   DH_CUDA(cudaEventSynchronize(e.ev1));
@@ -283,6 +299,55 @@ int engine_start(BlockEngine& e) {
   return DH_OK;
 }
 
+// FP64 check of a block X holding each sector's Ritz vectors: Y = H X with FP64 products,
+// E[s] = <x0|H x0> / <x0|x0> and r2[s] = |H x0 - E x0|^2 / |x0|^2 for the lowest vector x0 of every
+// sector.  Y is left holding the residual block.
+int engine_fp64_check(BlockEngine& e, const double* X, double* Y, std::vector<double>& E, std::vector<double>& r2) {
+  const int k = e.k, kk = k * k;
+  const int saved = e.precision;
+  e.precision = DH_PRECISION_FP64;
+  int rc = engine_product(e, X, Y);
+  e.precision = saved;
+  if (rc != DH_OK) return rc;
+  std::vector<double> g, a, rr;
+  if ((rc = engine_gram(e, X, X, g)) != DH_OK) return rc;
+  if ((rc = engine_gram(e, X, Y, a)) != DH_OK) return rc;
+  std::vector<double> d((size_t)e.nsec * kk, 0.0);
+  for (int s = 0; s < e.nsec; ++s)
+    for (int c = 0; c < k; ++c)
+      d[(size_t)s * kk + c * k + c] = a[(size_t)s * kk + c * k + c] / std::max(g[(size_t)s * kk + c * k + c], 1e-300);
+  double* dA = e.small.as<double>() + 2 * (size_t)e.nsec * kk;
+  DH_CUDA(cudaMemcpyAsync(dA, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+  if ((rc = launch_seg_update(Y, X, dA, nullptr, nullptr, k, e.tiles, e.stream)) != DH_OK) return rc;
+  if ((rc = engine_gram(e, Y, Y, rr)) != DH_OK) return rc;
+  E.assign(e.nsec, 0.0);
+  r2.assign(e.nsec, 0.0);
+  for (int s = 0; s < e.nsec; ++s) {
+    E[s] = d[(size_t)s * kk];
+    r2[s] = std::max(rr[(size_t)s * kk], 0.0) / std::max(g[(size_t)s * kk], 1e-300);
+  }
+  return DH_OK;
+}
+
+// Mixed-precision restart: the engine's start block becomes (lowest Ritz vector, fresh random
+// vectors) per sector (already copied into slot 0 by the caller); its product is FP64, the
+// following ones FP32, and every new block is projected against it.  The Krylov space is the one
+// an FP64 restart would build; the FP32 products only touch directions whose coefficients in the
+// refined ground state are of the order of the Ritz vector's residual.
+int engine_mixed_restart(BlockEngine& e, uint64_t seed) {
+  int rc;
+  if ((rc = launch_random_block(e.slot[0], e.total, e.k, e.row_offset_dev, e.tiles, seed, e.stream, 1)) != DH_OK)
+    return rc;
+  e.precision = DH_PRECISION_FP32;
+  e.fp64_first_product = true;
+  e.lock_start = true;
+  for (auto& b : e.sec) b.exhausted = b.partial = false;
+  return engine_start(e);
+}
+
+// the residual target of a mixed restart aiming at |r|^2 <= precision |E| after the FP64 check
+inline double restart_residual_target(double precision) { return 0.1 * precision; }
+
 // one block step for every sector (results recorded for the active ones)
 int engine_step(BlockEngine& e) {
   const int k = e.k, kk = k * k;
@@ -290,7 +355,8 @@ int engine_step(BlockEngine& e) {
   double* W = e.slot[(e.slot_cur + 1) % 3];
   double* Vp = e.slot[(e.slot_cur + 2) % 3];
   int rc;
-  if ((rc = engine_product(e, V, W)) != DH_OK) return rc;
+  const int step = (int)e.history.size();
+  if ((rc = engine_product(e, V, W, step)) != DH_OK) return rc;
   std::vector<double> A;
   if ((rc = engine_gram(e, V, W, A)) != DH_OK) return rc;
   for (int s = 0; s < e.nsec; ++s)
@@ -317,6 +383,16 @@ int engine_step(BlockEngine& e) {
   rec.A = A;
   rec.Bt = e.bt_host;
   rec.have_prev = e.have_prev;
+  if (e.lock_start && step >= 1) {
+    // W -= S (S^T W) with S the start block: the FP32 products of the later blocks leave components
+    // along S of the order of their rounding, which the recurrence alone would keep
+    if ((rc = engine_gram(e, e.start_block.as<double>(), W, rec.lock)) != DH_OK) return rc;
+    double* dL = e.small.as<double>() + 2 * (size_t)e.nsec * kk;  // dA is free again after the update
+    DH_CUDA(cudaMemcpyAsync(dL, rec.lock.data(), rec.lock.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+    if ((rc = launch_seg_update(W, e.start_block.as<double>(), dL, nullptr, nullptr, k, e.tiles, e.stream)) != DH_OK)
+      return rc;
+    DH_CUDA(cudaStreamSynchronize(e.stream));
+  }
   if ((rc = engine_qr(e, W, B, e.x32.as<float>(), &scale, &rec.inv1, &rec.inv2)) != DH_OK) return rc;
   e.history.push_back(std::move(rec));
   const int nb = (int)e.history.size();  // W now holds block nb
@@ -444,12 +520,18 @@ int engine_ritz(BlockEngine& e, double* out) {
     if ((rc = launch_seg_update(out, V, dNegC, nullptr, nullptr, k, e.tiles, e.stream)) != DH_OK) return rc;
     if (j + 1 == nb) break;
     const StepRecord& h = e.history[j];
-    if ((rc = engine_product(e, V, W)) != DH_OK) return rc;
+    if ((rc = engine_product(e, V, W, j)) != DH_OK) return rc;
     DH_CUDA(cudaMemcpyAsync(dA, h.A.data(), h.A.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
     DH_CUDA(cudaMemcpyAsync(dBt, h.Bt.data(), h.Bt.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
     if ((rc = launch_seg_update(W, V, dA, h.have_prev ? Vp : nullptr, h.have_prev ? dBt : nullptr, k, e.tiles,
                                 e.stream)) != DH_OK)
       return rc;
+    if (!h.lock.empty()) {
+      DH_CUDA(cudaStreamSynchronize(e.stream));
+      DH_CUDA(cudaMemcpyAsync(dA, h.lock.data(), h.lock.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+      if ((rc = launch_seg_update(W, e.start_block.as<double>(), dA, nullptr, nullptr, k, e.tiles, e.stream)) != DH_OK)
+        return rc;
+    }
     DH_CUDA(cudaMemcpyAsync(dInv, h.inv1.data(), h.inv1.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
     if ((rc = launch_seg_rmul(W, dInv, k, e.tiles, nullptr, e.stream)) != DH_OK) return rc;
     DH_CUDA(cudaStreamSynchronize(e.stream));
@@ -477,6 +559,20 @@ int sector_evaluate(const BlockEngine& e, BlockSector& b) {
   else
     b.prev_last = 2.0 * eig[nev - 1];
   b.ritz.swap(eig);
+  if (e.residual_target > 0.0) {
+    std::vector<double> C, vals;
+    if ((rc = sector_ritz_coefficients(e, b, 1, C, vals)) != DH_OK) return rc;
+    const int k = e.k, m = b.blocks;
+    const double* Bm = &b.B[(size_t)m * k * k];  // X_m = V_m B_m: the block after the last A
+    double r2 = 0.0;
+    for (int i = 0; i < k; ++i) {
+      double v = 0.0;
+      for (int j = 0; j < k; ++j) v += Bm[i * k + j] * C[(size_t)((m - 1) * k + j)];
+      r2 += v * v;
+    }
+    if (r2 < e.residual_target * fabs(b.ritz[0])) b.converged = true;
+    return DH_OK;
+  }
   if ((int)b.ritz.size() > e.nev) {
     const double l = b.ritz[e.nev - 1];
     if (fabs(l - b.prev_last) < e.eig_precision * fabs(l)) b.converged = true;
@@ -657,6 +753,7 @@ int bl_allocate_store(BlockLanczos* b) {
 bool bl_converged(const BlockLanczos* b) {
   const BlockSector& s = b->e.sec[0];
   if (s.exhausted && s.blocks > 0) return true;
+  if (b->e.residual_target > 0.0) return s.converged;  // residual test of sector_evaluate
   if ((int)s.ritz.size() <= b->nev) return false;
   const double l = s.ritz[b->nev - 1];
   return fabs(l - s.prev_last) < b->e.eig_precision * fabs(l);
@@ -847,58 +944,42 @@ int block_lanczos_solve_refined(BlockLanczos* b, int max_iter, double precision,
   int rc;
   if ((rc = bl_ensure_x32(b)) != DH_OK) return rc;
   e.precision = DH_PRECISION_FP32;
+  e.fp64_first_product = e.lock_start = false;
+  const long long products0 = e.products, fp64_0 = e.fp64_products;
   if ((rc = launch_f32_copy(e.slot[e.slot_cur], e.x32.as<float>(), dim * k, e.stream)) != DH_OK) return rc;
   e.eig_precision = std::max(precision, 1e-9);
   std::vector<double> eig(b->nev);
   int iters = 0, conv = 0;
   rc = block_lanczos_solve(b, max_iter, eig.data(), &iters, &conv);
-  const long long fp32_products = e.products;
   const double e32 = eig[0];
   if (rc == DH_OK) rc = bl_ritz_block(b);
-  e.precision = DH_PRECISION_FP64;
   double energy = e32, rnorm = 0.0;
-  if (rc == DH_OK) {
-    // H X in FP64, E_c = <x_c|H x_c> / <x_c|x_c>, R = H X - X diag(E), |r_0| / |x_0|
-    double* X = b->ritz.as<double>();
-    double* Y = e.slot[(e.slot_cur + 1) % 3];
-    std::vector<double> g, a, rr;
-    rc = engine_product(e, X, Y);
-    if (rc == DH_OK) rc = engine_gram(e, X, X, g);
-    if (rc == DH_OK) rc = engine_gram(e, X, Y, a);
-    if (rc == DH_OK) {
-      std::vector<double> d((size_t)k * k, 0.0);
-      for (int c = 0; c < k; ++c) d[(size_t)c * k + c] = a[(size_t)c * k + c] / g[(size_t)c * k + c];
-      energy = d[0];
-      double* dA = e.small.as<double>() + 2 * (size_t)e.nsec * k * k;
-      if (cudaMemcpyAsync(dA, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream) != cudaSuccess)
-        rc = cuda_fail(cudaGetLastError(), "copy", __FILE__, __LINE__);
-      if (rc == DH_OK) rc = launch_seg_update(Y, X, dA, nullptr, nullptr, k, e.tiles, e.stream);
-      if (rc == DH_OK) rc = engine_gram(e, Y, Y, rr);
-      if (rc == DH_OK) rnorm = sqrt(std::max(rr[0], 0.0) / g[0]);
-    }
-  }
-  if (rc == DH_OK && rnorm * rnorm > precision * std::max(fabs(energy), 1e-300)) {
-    // restart block: the lowest Ritz vector and fresh random vectors
+  std::vector<double> E, r2;
+  for (int round = 0; rc == DH_OK; ++round) {
+    // FP64 Rayleigh quotient and residual of the lowest Ritz vector
+    if ((rc = engine_fp64_check(e, b->ritz.as<double>(), e.slot[(e.slot_cur + 1) % 3], E, r2)) != DH_OK) break;
+    energy = E[0];
+    rnorm = sqrt(r2[0]);
+    if (r2[0] <= precision * std::max(fabs(energy), 1e-300) || round == 3) break;
     DH_CUDA(cudaMemcpyAsync(e.slot[0], b->ritz.ptr, (size_t)dim * k * sizeof(double), cudaMemcpyDeviceToDevice, e.stream));
-    if ((rc = launch_random_block(e.slot[0], dim, k, e.row_offset_dev, e.tiles, 1000, e.stream, 1)) != DH_OK) return rc;
-    e.sec[0].exhausted = e.sec[0].partial = false;
-    rc = engine_start(e);
-    if (rc == DH_OK) {
-      b->initialized = true;
-      b->ritz_valid = false;
-      e.eig_precision = precision;
-      rc = block_lanczos_solve(b, std::min(max_iter, 60 * k), eig.data(), &iters, &conv);
-      if (rc == DH_OK) energy = eig[0];
-    }
+    if ((rc = engine_mixed_restart(e, 1000 + round)) != DH_OK) break;
+    b->initialized = true;
+    b->ritz_valid = false;
+    e.eig_precision = precision;
+    e.residual_target = restart_residual_target(precision);
+    if ((rc = block_lanczos_solve(b, std::min(max_iter, 100 * k), eig.data(), &iters, &conv)) != DH_OK) break;
+    rc = bl_ritz_block(b);
   }
+  e.fp64_first_product = e.lock_start = false;
+  e.residual_target = 0.0;
   e.precision = b->h->precision;
   e.eig_precision = saved_precision;
   if (rc != DH_OK) return rc;
   out[0] = energy;
   out[1] = e32;
   out[2] = rnorm;
-  out[3] = (double)(fp32_products * k);
-  out[4] = (double)((e.products - fp32_products) * k);
+  out[3] = (double)((e.products - products0 - (e.fp64_products - fp64_0)) * k);
+  out[4] = (double)((e.fp64_products - fp64_0) * k);
   return DH_OK;
 }
 
@@ -1056,76 +1137,77 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
     const auto tb = clk::now();
     fp32_seconds = precision == DH_PRECISION_FP32 ? std::chrono::duration<double>(tb - ta).count() : 0.0;
     if (precision == DH_PRECISION_FP32) {
-      // refinement: FP64 Rayleigh quotient and residual of every sector's lowest Ritz vector
-      const int k = e.k, kk = k * k;
-      DevBuf R;
-      if ((rc = R.alloc((size_t)e.total * k * sizeof(double))) != DH_OK) return rc;
-      if ((rc = engine_ritz(e, R.as<double>())) != DH_OK) return rc;
-      e.precision = DH_PRECISION_FP64;
-      double* Y = e.slot[0];
-      std::vector<double> g, a, rr;
-      if ((rc = engine_product(e, R.as<double>(), Y)) != DH_OK) return rc;
-      if ((rc = engine_gram(e, R.as<double>(), R.as<double>(), g)) != DH_OK) return rc;
-      if ((rc = engine_gram(e, R.as<double>(), Y, a)) != DH_OK) return rc;
-      std::vector<double> d((size_t)ns * kk, 0.0), e_rq(ns);
-      for (int i = 0; i < ns; ++i) {
-        for (int c = 0; c < k; ++c)
-          d[(size_t)i * kk + c * k + c] = a[(size_t)i * kk + c * k + c] / g[(size_t)i * kk + c * k + c];
-        e_rq[i] = d[(size_t)i * kk];
-      }
-      double* dA = e.small.as<double>() + 2 * (size_t)e.nsec * kk;
-      DH_CUDA(cudaMemcpyAsync(dA, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
-      if ((rc = launch_seg_update(Y, R.as<double>(), dA, nullptr, nullptr, k, e.tiles, e.stream)) != DH_OK) return rc;
-      if ((rc = engine_gram(e, Y, Y, rr)) != DH_OK) return rc;
+      // refinement rounds: FP64 Rayleigh quotient and residual of every pending sector's lowest
+      // Ritz vector; the sectors above the target restart (mixed precision) from it, in lockstep
+      const int k = e.k;
       products = e.products;
       product_ms = e.product_ms;
-      std::vector<int> redo;  // positions in lanczos_sectors
-      for (int i = 0; i < ns; ++i) {
-        const double r2 = std::max(rr[(size_t)i * kk], 0.0) / g[(size_t)i * kk];
-        const int s = lanczos_sectors[i];
-        max_shift = std::max(max_shift, fabs(e_rq[i] - energies[s]));
-        energies[s] = e_rq[i];
-        if (need_dense[i]) continue;
-        if (r2 > precision_target * std::max(fabs(e_rq[i]), 1e-300)) redo.push_back(i);
-      }
-      refined = (int)redo.size();
-      if (!redo.empty()) {
-        // FP64 block Lanczos restarted from the Ritz blocks of those sectors, in lockstep
-        BlockEngine f;
-        f.k = k;
-        f.nev = 1;
-        f.precision = DH_PRECISION_FP64;
-        f.eig_precision = precision_target > 0.0 ? precision_target : 1e-14;
-        f.max_iter = std::min(max_iter, 60 * k);
-        f.stream = e.stream;
+      std::vector<int> pending;  // positions in lanczos_sectors
+      for (int i = 0; i < ns; ++i)
+        if (!need_dense[i]) pending.push_back(i);
+      BlockEngine* src = &e;            // engine holding the pending sectors' Ritz blocks
+      std::vector<int> src_pos(ns, -1);  // position of a lanczos sector inside src
+      for (int i = 0; i < ns; ++i) src_pos[i] = i;
+      std::unique_ptr<BlockEngine> cur;
+      std::unique_ptr<SectorProduct> cur_prod;
+      DevBuf R;
+      for (int round = 0; !pending.empty(); ++round) {
+        if ((rc = ensure_buffer(R, (size_t)src->total * k * sizeof(double))) != DH_OK) return rc;
+        if ((rc = engine_ritz(*src, R.as<double>())) != DH_OK) return rc;
+        std::vector<double> E, r2;
+        if ((rc = engine_fp64_check(*src, R.as<double>(), src->slot[0], E, r2)) != DH_OK) return rc;
+        std::vector<int> redo;
+        for (int i : pending) {
+          const int p = src_pos[i];
+          const int s = lanczos_sectors[i];
+          max_shift = std::max(max_shift, fabs(E[p] - energies[s]));
+          energies[s] = E[p];
+          if (r2[p] > precision_target * std::max(fabs(E[p]), 1e-300)) redo.push_back(i);
+        }
+        if (src != &e) {
+          products += src->products;
+          product_ms += src->product_ms;
+        } else {
+          products = e.products;
+          product_ms = e.product_ms;
+        }
+        if (round == 0) refined = (int)redo.size();
+        if (redo.empty() || round == 3) break;
+        auto f = std::make_unique<BlockEngine>();
+        f->k = k;
+        f->nev = 1;
+        f->precision = DH_PRECISION_FP32;
+        f->eig_precision = precision_target > 0.0 ? precision_target : 1e-14;
+        f->residual_target = restart_residual_target(f->eig_precision);
+        f->max_iter = std::min(max_iter, 100 * k);
+        f->stream = e.stream;
         std::vector<long long> rdims;
         std::vector<int> rsec;
         for (int i : redo) {
           rdims.push_back(e.sec[i].dim);
           rsec.push_back(lanczos_sectors[i]);
         }
-        if ((rc = engine_setup(f, rdims)) != DH_OK) return rc;
-        for (size_t j = 0; j < redo.size(); ++j)
-          DH_CUDA(cudaMemcpyAsync(f.slot[0] + (size_t)f.off[j] * k, R.as<double>() + (size_t)e.off[redo[j]] * k,
-                                  (size_t)rdims[j] * k * sizeof(double), cudaMemcpyDeviceToDevice, f.stream));
-        // the lowest Ritz vector and fresh random vectors: the other Ritz vectors of a sector whose
-        // FP32 basis lost orthogonality can be nearly dependent on it
-        if ((rc = launch_random_block(f.slot[0], f.total, k, f.row_offset_dev, f.tiles, seed + 1000, f.stream, 1)) !=
-            DH_OK)
-          return rc;
-        SectorProduct fprod;
-        if ((rc = bind_sector_product(hb, rsec, f, fprod)) != DH_OK) return rc;
-        if ((rc = engine_start(f)) != DH_OK) return rc;
-        if ((rc = engine_solve(f)) != DH_OK) return rc;
-        for (size_t j = 0; j < redo.size(); ++j) {
-          const BlockSector& bs = f.sec[j];
-          if (!bs.ritz.empty()) energies[rsec[j]] = bs.ritz[0];
-          iterations[rsec[j]] += bs.count;
-          max_shift = std::max(max_shift, fabs(energies[rsec[j]] - e_rq[redo[j]]));
-          if (bs.exhausted && bs.partial && bs.dim <= kDenseFallbackLimit) need_dense[redo[j]] = 1;
+        if ((rc = engine_setup(*f, rdims)) != DH_OK) return rc;
+        engine_store_if_fits(*f);
+        for (size_t jj = 0; jj < redo.size(); ++jj)
+          DH_CUDA(cudaMemcpyAsync(f->slot[0] + (size_t)f->off[jj] * k, R.as<double>() + (size_t)src->off[src_pos[redo[jj]]] * k,
+                                  (size_t)rdims[jj] * k * sizeof(double), cudaMemcpyDeviceToDevice, f->stream));
+        auto fprod = std::make_unique<SectorProduct>();
+        if ((rc = bind_sector_product(hb, rsec, *f, *fprod)) != DH_OK) return rc;
+        if ((rc = engine_mixed_restart(*f, seed + 1000 + round)) != DH_OK) return rc;
+        if ((rc = engine_solve(*f)) != DH_OK) return rc;
+        for (size_t jj = 0; jj < redo.size(); ++jj) {
+          const BlockSector& bs = f->sec[jj];
+          iterations[rsec[jj]] += bs.count;
+          if (bs.exhausted && bs.partial && bs.dim <= kDenseFallbackLimit) need_dense[redo[jj]] = 1;
+          src_pos[redo[jj]] = (int)jj;
         }
-        products += f.products;
-        product_ms += f.product_ms;
+        pending.clear();
+        for (int i : redo)
+          if (!need_dense[i]) pending.push_back(i);
+        cur_prod = std::move(fprod);  // the product binding must outlive the engine using it
+        cur = std::move(f);
+        src = cur.get();
       }
       refine_seconds = std::chrono::duration<double>(clk::now() - tb).count();
     }

@@ -41,6 +41,14 @@ struct dh_lanczos_s {
   std::vector<double> prev_wanted;
   std::vector<double> alpha, beta, ritz;
   int64_t matvecs = 0;
+  int64_t fp64_matvecs = 0;
+  // mixed-precision restart: the start vector's product in FP64, the following ones in the
+  // Hamiltonian's precision, every new vector projected against the start vector
+  bool fp64_first = false;
+  bool lock_v0 = false;
+  // > 0: converged when the lowest Ritz vector's residual estimate beta |s_last| (of the matrix one
+  // row short, whose next beta is known) satisfies |r|^2 < residual_target |lambda|
+  double residual_target = 0.0;
   cudaGraphExec_t graph3 = nullptr;  // three iterations starting at phase 0
   dh::BlockLanczos* blk = nullptr;   // DH_LANCZOS_BLOCK: everything runs in the block engine
   ~dh_lanczos_s() {
@@ -55,7 +63,9 @@ int lz_matvec(dh_lanczos_s* l, int src_slot, int dst_slot) {
   double* x = l->st.vec + (size_t)src_slot * l->dim;
   double* y = l->st.vec + (size_t)dst_slot * l->dim;
   ++l->matvecs;
-  return hamiltonian_apply(l->h, x, y, 1, 0, l->dim, 0, l->st.x32, l->stream);
+  if (l->h->precision == DH_PRECISION_FP64) ++l->fp64_matvecs;
+  return hamiltonian_apply(l->h, x, y, 1, 0, l->dim, 0, l->h->precision == DH_PRECISION_FP32 ? l->st.x32 : nullptr,
+                           l->stream);
 }
 
 // one iteration: v_{i+1} from H v_i, then H v_{i+1} and the two new scalars (i = index)
@@ -77,6 +87,19 @@ int lz_iteration(dh_lanczos_s* l, int i) {
     if ((rc = launch_multi_dot(vs, 1, w, l->dim, l->st.norm + i + 1, l->red, l->stream)) != DH_OK) return rc;
     if ((rc = launch_sqrt_inplace(l->st.norm + i + 1, l->stream)) != DH_OK) return rc;
   }
+  if (l->lock_v0 && i + 1 >= 2) {
+    // project the new vector against the start vector (the FP32 products leave components along it
+    // of the order of their rounding), then take its norm again
+    double* w = l->st.vec + (size_t)((phase + 1) % 3) * l->dim;
+    const double* v0 = l->initial.as<double>();
+    double* c = l->coef.as<double>() + l->cap + 4;
+    const double* vs[1] = {v0};
+    if ((rc = launch_multi_dot(vs, 1, w, l->dim, c, l->red, l->stream)) != DH_OK) return rc;
+    if ((rc = launch_combine(v0, 1, l->dim, c, -1.0, w, 1, l->dim, l->stream)) != DH_OK) return rc;
+    const double* ws[1] = {w};
+    if ((rc = launch_multi_dot(ws, 1, w, l->dim, l->st.norm + i + 1, l->red, l->stream)) != DH_OK) return rc;
+    if ((rc = launch_sqrt_inplace(l->st.norm + i + 1, l->stream)) != DH_OK) return rc;
+  }
   if ((rc = launch_lz_scale(l->st, phase, l->stream)) != DH_OK) return rc;
   if ((rc = lz_matvec(l, (phase + 1) % 3, (phase + 2) % 3)) != DH_OK) return rc;
   return launch_lz_dots(l->st, phase, l->stream);
@@ -88,7 +111,11 @@ int lz_first_steps(dh_lanczos_s* l) {
   if (l->st.x32 && (rc = launch_convert_f32(l->st.vec, l->st.x32, l->dim, l->stream)) != DH_OK) return rc;
   if (l->st.krylov)
     DH_CUDA(cudaMemcpyAsync(l->st.krylov, l->st.vec, l->dim * sizeof(double), cudaMemcpyDeviceToDevice, l->stream));
-  if ((rc = lz_matvec(l, 0, 1)) != DH_OK) return rc;
+  const int saved = l->h->precision;
+  if (l->fp64_first) l->h->precision = DH_PRECISION_FP64;
+  rc = lz_matvec(l, 0, 1);
+  l->h->precision = saved;
+  if (rc != DH_OK) return rc;
   const double* vs[1] = {l->st.vec};
   if ((rc = launch_multi_dot(vs, 1, l->st.vec + l->dim, l->dim, l->st.alpha, l->red, l->stream)) != DH_OK) return rc;
   DH_CUDA(cudaMemsetAsync(l->st.cursor, 0, sizeof(int), l->stream));
@@ -124,6 +151,14 @@ int lz_finish_call(dh_lanczos_s* l) {
 
 // BasicLanczosAlgorithm::TestConvergence (:220): |lambda_{nev-1} - previous| < precision |lambda_{nev-1}|
 bool lz_converged(const dh_lanczos_s* l) {
+  if (l->residual_target > 0.0) {
+    const int n = l->rows - 1;
+    if (n < 2 || (int)l->beta.size() < n) return false;
+    std::vector<double> eig(n), z((size_t)n * n);
+    if (tridiagonal_eigen(n, l->alpha.data(), l->beta.data(), eig.data(), z.data()) != DH_OK) return false;
+    const double r = l->beta[n - 1] * z[n - 1];  // column 0, last component
+    return r * r < l->residual_target * fabs(eig[0]);
+  }
   if ((int)l->ritz.size() < l->nev) return false;
   const double e = l->ritz[l->nev - 1];
   return fabs(e - l->prev_last) < l->precision * fabs(e);
@@ -472,7 +507,8 @@ int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eige
   // QHEOnSphereMainTask.cc:732-753: RunLanczosAlgorithm(nev + 2), counter = nev + 3
   if ((rc = lz_run(l, l->nev + 2)) != DH_OK) return rc;
   int count = l->nev + 3;
-  const bool use_graph = graph_batch > 1 && l->algorithm != DH_LANCZOS_FULL_REORTHOGONALIZED;
+  // the start-vector projection indexes its norm from the host: no graph batches with it
+  const bool use_graph = graph_batch > 1 && l->algorithm != DH_LANCZOS_FULL_REORTHOGONALIZED && !l->lock_v0;
   while (!lz_converged(l) && count < max_iter) {
     if (!use_graph) {
       ++count;
@@ -545,62 +581,79 @@ int dh_lanczos_solve_refined(dh_lanczos_t l, int max_iter, double precision, dou
   dh_hamiltonian_s* h = l->h;
   const int saved_precision = h->precision;
   const double saved_lz_precision = l->precision;
+  const int64_t matvecs0 = l->matvecs, fp64_0 = l->fp64_matvecs;
   int rc;
-  if (!l->st.x32) {
-    if ((rc = l->x32.alloc((size_t)l->dim * sizeof(float))) != DH_OK) return rc;
-    l->st.x32 = l->x32.as<float>();
+  auto drop_graph = [&]() {
     if (l->graph3) {
       cudaGraphExecDestroy(l->graph3);
       l->graph3 = nullptr;
     }
+  };
+  if (!l->st.x32) {
+    if ((rc = l->x32.alloc((size_t)l->dim * sizeof(float))) != DH_OK) return rc;
+    l->st.x32 = l->x32.as<float>();
+    drop_graph();
   }
+  l->fp64_first = l->lock_v0 = false;
   // phase 1: FP32 products, FP64 recurrence, converged to the FP32 resolution of the Ritz value
   h->precision = DH_PRECISION_FP32;
   l->precision = std::max(precision, 1e-9);
   double e32 = 0.0;
   int iters = 0, conv = 0;
   rc = dh_lanczos_solve(l, max_iter, 16, &e32, &iters, &conv);
-  const int64_t fp32_matvecs = l->matvecs;
   if (rc == DH_OK) rc = lz_ground_state(l);
-  // phase 2: FP64 Rayleigh quotient and residual of the Ritz vector
-  h->precision = DH_PRECISION_FP64;
   double energy = e32, rnorm = 0.0;
   double* sc = l->coef.as<double>();
-  if (rc == DH_OK) {
+  // FP64 Rayleigh quotient and residual of the Ritz vector
+  auto fp64_check = [&]() -> int {
     double* psi = l->ground.as<double>();
     double* hpsi = l->st.vec;
     double* res = l->st.vec + l->dim;
-    rc = hamiltonian_apply(h, psi, hpsi, 1, 0, l->dim, 0, nullptr, l->stream);
+    const int saved = h->precision;
+    h->precision = DH_PRECISION_FP64;
+    int r = hamiltonian_apply(h, psi, hpsi, 1, 0, l->dim, 0, nullptr, l->stream);
+    h->precision = saved;
+    ++l->matvecs;
+    ++l->fp64_matvecs;
     const double* vs[1] = {psi};
-    if (rc == DH_OK) rc = launch_multi_dot(vs, 1, hpsi, l->dim, sc, l->red, l->stream);
-    if (rc == DH_OK) rc = launch_lanczos_update(res, hpsi, psi, nullptr, sc, nullptr, l->dim, sc + 1, l->red, l->stream);
+    if (r == DH_OK) r = launch_multi_dot(vs, 1, hpsi, l->dim, sc, l->red, l->stream);
+    if (r == DH_OK) r = launch_lanczos_update(res, hpsi, psi, nullptr, sc, nullptr, l->dim, sc + 1, l->red, l->stream);
     double host[2] = {0.0, 0.0};
-    if (rc == DH_OK && cudaMemcpyAsync(host, sc, 2 * sizeof(double), cudaMemcpyDeviceToHost, l->stream) != cudaSuccess)
-      rc = cuda_fail(cudaGetLastError(), "copy", __FILE__, __LINE__);
-    if (rc == DH_OK && cudaStreamSynchronize(l->stream) != cudaSuccess)
-      rc = cuda_fail(cudaGetLastError(), "sync", __FILE__, __LINE__);
+    if (r == DH_OK && cudaMemcpyAsync(host, sc, 2 * sizeof(double), cudaMemcpyDeviceToHost, l->stream) != cudaSuccess)
+      r = cuda_fail(cudaGetLastError(), "copy", __FILE__, __LINE__);
+    if (r == DH_OK && cudaStreamSynchronize(l->stream) != cudaSuccess)
+      r = cuda_fail(cudaGetLastError(), "sync", __FILE__, __LINE__);
     energy = host[0];
     rnorm = host[1];
-  }
-  int64_t fp64_matvecs = 1;
-  // the Rayleigh-quotient error is bounded by |r|^2 / gap: when that may exceed the target, restart
-  // an FP64 Lanczos from the Ritz vector (it converges in a few steps from there)
-  if (rc == DH_OK && rnorm * rnorm > precision * std::max(fabs(energy), 1e-300)) {
+    return r;
+  };
+  // the Rayleigh-quotient error is bounded by |r|^2 / gap: while that may exceed the target, restart
+  // from the Ritz vector.  With the Krylov vectors stored the restart is mixed precision (the Ritz
+  // vector's product in FP64, the correction directions' products in FP32); otherwise it is FP64.
+  for (int round = 0; rc == DH_OK; ++round) {
+    if ((rc = fp64_check()) != DH_OK) break;
+    if (rnorm * rnorm <= precision * std::max(fabs(energy), 1e-300) || round == 3) break;
     DH_CUDA(cudaMemcpyAsync(l->st.vec, l->ground.ptr, l->dim * sizeof(double), cudaMemcpyDeviceToDevice, l->stream));
-    if (l->graph3) {
-      cudaGraphExecDestroy(l->graph3);
-      l->graph3 = nullptr;
-    }
+    drop_graph();
+    const bool mixed = l->krylov_cap > 0;
     float* keep32 = l->st.x32;
-    l->st.x32 = nullptr;
+    if (mixed) {
+      l->fp64_first = l->lock_v0 = true;
+      l->residual_target = 0.1 * precision;
+      h->precision = DH_PRECISION_FP32;
+    } else {
+      l->st.x32 = nullptr;
+      h->precision = DH_PRECISION_FP64;
+    }
     rc = lz_initialize_device(l);
     l->precision = precision;
-    const int64_t before = l->matvecs;
-    double e64 = 0.0;
-    if (rc == DH_OK) rc = dh_lanczos_solve(l, std::min(max_iter, 60), 1, &e64, &iters, &conv);
-    fp64_matvecs += l->matvecs - before;
-    if (rc == DH_OK) energy = e64;
+    double e2 = 0.0;
+    if (rc == DH_OK) rc = dh_lanczos_solve(l, std::min(max_iter, 200), mixed ? 16 : 1, &e2, &iters, &conv);
+    if (rc == DH_OK) rc = lz_ground_state(l);
     l->st.x32 = keep32;
+    l->fp64_first = l->lock_v0 = false;
+    l->residual_target = 0.0;
+    drop_graph();
   }
   h->precision = saved_precision;
   l->precision = saved_lz_precision;
@@ -608,8 +661,8 @@ int dh_lanczos_solve_refined(dh_lanczos_t l, int max_iter, double precision, dou
   out[0] = energy;
   out[1] = e32;
   out[2] = rnorm;
-  out[3] = (double)fp32_matvecs;
-  out[4] = (double)fp64_matvecs;
+  out[3] = (double)((l->matvecs - matvecs0) - (l->fp64_matvecs - fp64_0));
+  out[4] = (double)(l->fp64_matvecs - fp64_0);
   return DH_OK;
 }
 

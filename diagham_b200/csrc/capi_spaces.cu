@@ -31,29 +31,15 @@ bool is_device_pointer(const void* p) {
 }
 
 // FermionOnSphere set-up: orbital-sum counts, the two rank tables and the basis words
-static int build_fermion_space(dh_space_s* sp) {
+int build_rank_tables(dh_space_s* sp, int low_bits) {
   const int N = sp->nbr_fermions, L = sp->lz_max, K = sp->total_sum;
-  const int O = L + 2;  // orbital counts 0 .. L+1
-  // counts[n][o][s]: n fermions in orbitals 0..o-1 with orbital-index sum s
-  std::vector<int64_t> counts((size_t)(N + 1) * O * (K + 1), 0);
-  auto C = [&](int n, int o, int s) -> int64_t& { return counts[((size_t)n * O + o) * (K + 1) + s]; };
-  for (int o = 0; o < O; ++o) C(0, o, 0) = 1;
-  for (int n = 1; n <= N; ++n)
-    for (int o = 1; o < O; ++o)
-      for (int s = 0; s <= K; ++s) {
-        int64_t v = C(n, o - 1, s);
-        if (s - (o - 1) >= 0) v += C(n - 1, o - 1, s - (o - 1));
-        C(n, o, s) = v;
-      }
-  const int64_t dim = C(N, L + 1, K);
-  DH_CHECK(dim > 0, DH_ERR_ARGUMENT, "FermionOnSphere(%d, %d, %d): empty sector", N, sp->total_lz, L);
-  DH_CHECK(dim < (1ll << 31), DH_ERR_UNSUPPORTED, "FermionOnSphere: dimension %lld >= 2^31", (long long)dim);
-  sp->dim = dim;
-
+  const int O = L + 2;
+  auto C = [&](int n, int o, int s) -> int64_t { return sp->counts[((size_t)n * O + o) * (K + 1) + s]; };
   // rank tables: index(w) = high_offset[w >> LB] + low_rank[w & (2^LB - 1)]
   FermionRankTables& t = sp->rank;
   t.low_bits = (L + 2) / 2;
   if (sp->requested_low_bits > 0) t.low_bits = sp->requested_low_bits;
+  if (low_bits > 0) t.low_bits = low_bits;
   if (sp->kernel_variant == 2 && t.low_bits > 15) t.low_bits = 15;
   if (t.low_bits < 3) t.low_bits = 3;
   if (t.low_bits > L) t.low_bits = L;
@@ -84,19 +70,43 @@ static int build_fermion_space(dh_space_s* sp) {
     t.high_offset[h] = (int32_t)running;
     running += c;
   }
-  DH_CHECK(running == dim, DH_ERR_STATE, "FermionOnSphere: rank tables cover %lld of %lld states", (long long)running,
-           (long long)dim);
-
+  DH_CHECK(running == sp->dim, DH_ERR_STATE, "FermionOnSphere: rank tables cover %lld of %lld states",
+           (long long)running, (long long)sp->dim);
   int rc;
-  DevBuf dcounts;
-  if ((rc = dcounts.alloc(counts.size() * sizeof(int64_t))) != DH_OK) return rc;
-  if ((rc = sp->words.alloc((size_t)dim * sizeof(uint64_t))) != DH_OK) return rc;
+  sp->low_rank.release();
+  sp->high_offset.release();
   if ((rc = sp->low_rank.alloc(t.low_rank.size() * sizeof(uint16_t))) != DH_OK) return rc;
   if ((rc = sp->high_offset.alloc(t.high_offset.size() * sizeof(int32_t))) != DH_OK) return rc;
-  DH_CUDA(cudaMemcpy(dcounts.ptr, counts.data(), counts.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
   DH_CUDA(cudaMemcpy(sp->low_rank.ptr, t.low_rank.data(), t.low_rank.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
   DH_CUDA(cudaMemcpy(sp->high_offset.ptr, t.high_offset.data(), t.high_offset.size() * sizeof(int32_t),
                      cudaMemcpyHostToDevice));
+  return DH_OK;
+}
+
+static int build_fermion_space(dh_space_s* sp) {
+  const int N = sp->nbr_fermions, L = sp->lz_max, K = sp->total_sum;
+  const int O = L + 2;  // orbital counts 0 .. L+1
+  // counts[n][o][s]: n fermions in orbitals 0..o-1 with orbital-index sum s
+  sp->counts.assign((size_t)(N + 1) * O * (K + 1), 0);
+  auto C = [&](int n, int o, int s) -> int64_t& { return sp->counts[((size_t)n * O + o) * (K + 1) + s]; };
+  for (int o = 0; o < O; ++o) C(0, o, 0) = 1;
+  for (int n = 1; n <= N; ++n)
+    for (int o = 1; o < O; ++o)
+      for (int s = 0; s <= K; ++s) {
+        int64_t v = C(n, o - 1, s);
+        if (s - (o - 1) >= 0) v += C(n - 1, o - 1, s - (o - 1));
+        C(n, o, s) = v;
+      }
+  const int64_t dim = C(N, L + 1, K);
+  DH_CHECK(dim > 0, DH_ERR_ARGUMENT, "FermionOnSphere(%d, %d, %d): empty sector", N, sp->total_lz, L);
+  DH_CHECK(dim < (1ll << 31), DH_ERR_UNSUPPORTED, "FermionOnSphere: dimension %lld >= 2^31", (long long)dim);
+  sp->dim = dim;
+  int rc = build_rank_tables(sp, 0);
+  if (rc != DH_OK) return rc;
+  DevBuf dcounts;
+  if ((rc = dcounts.alloc(sp->counts.size() * sizeof(int64_t))) != DH_OK) return rc;
+  if ((rc = sp->words.alloc((size_t)dim * sizeof(uint64_t))) != DH_OK) return rc;
+  DH_CUDA(cudaMemcpy(dcounts.ptr, sp->counts.data(), sp->counts.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
   rc = launch_fqhe_unrank(N, L, K, dim, sp->words.as<uint64_t>(), dcounts.as<int64_t>(), O * (K + 1), K + 1, 0);
   if (rc != DH_OK) return rc;
   DH_CUDA(cudaDeviceSynchronize());
@@ -589,6 +599,95 @@ int dh_hamiltonian_block_multiply(dh_hamiltonian_t h, const double* x, double* y
   if ((rc = hamiltonian_apply_block(h, xd, x32, yd, k, h->precision, h->stream)) != DH_OK) return rc;
   if (!dst_dev) DH_CUDA(cudaMemcpyAsync(y, yd, bytes, cudaMemcpyDeviceToHost, h->stream));
   DH_CUDA(cudaStreamSynchronize(h->stream));
+  return DH_OK;
+}
+
+int dh_hamiltonian_autotune(dh_hamiltonian_t h, int block_size, int repeats, double* out) {
+  DH_CHECK(h, DH_ERR_ARGUMENT, "null hamiltonian");
+  DH_CHECK(block_size == 1 || block_size == 2 || block_size == 4, DH_ERR_ARGUMENT, "block size %d not in {1, 2, 4}",
+           block_size);
+  if (repeats < 1) repeats = 3;
+  dh_space_s* sp = h->space;
+  const int64_t dim = sp->dim;
+  const int kmax = 4;
+  DevBuf x, x32, y;
+  int rc;
+  if ((rc = x.alloc((size_t)dim * kmax * sizeof(double))) != DH_OK ||
+      (rc = x32.alloc((size_t)dim * kmax * sizeof(float))) != DH_OK ||
+      (rc = y.alloc((size_t)dim * kmax * sizeof(double))) != DH_OK)
+    return rc;
+  cudaStream_t st = h->stream;
+  if ((rc = launch_random_vector(x.as<double>(), dim * kmax, 12345, st)) != DH_OK) return rc;
+  if ((rc = launch_convert_f32(x.as<double>(), x32.as<float>(), dim * kmax, st)) != DH_OK) return rc;
+  if (sp->kind == SPACE_FERMION && sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
+  cudaEvent_t e0, e1;
+  DH_CUDA(cudaEventCreate(&e0));
+  DH_CUDA(cudaEventCreate(&e1));
+  struct Events {
+    cudaEvent_t a, b;
+    ~Events() {
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+    }
+  } guard{e0, e1};
+  // median device time of one product of a k-vector block (one untimed call first)
+  auto time_one = [&](int k, double* ms_out) -> int {
+    int r = hamiltonian_apply_block(h, x.as<double>(), x32.as<float>(), y.as<double>(), k, h->precision, st);
+    if (r != DH_OK) return r;
+    std::vector<float> ms(repeats);
+    for (int i = 0; i < repeats; ++i) {
+      DH_CUDA(cudaEventRecord(e0, st));
+      if ((r = hamiltonian_apply_block(h, x.as<double>(), x32.as<float>(), y.as<double>(), k, h->precision, st)) != DH_OK)
+        return r;
+      DH_CUDA(cudaEventRecord(e1, st));
+      DH_CUDA(cudaEventSynchronize(e1));
+      DH_CUDA(cudaEventElapsedTime(&ms[i], e0, e1));
+    }
+    std::sort(ms.begin(), ms.end());
+    *ms_out = ms[repeats / 2];
+    return DH_OK;
+  };
+  double best = 1e300;
+  int best_variant = sp->kernel_variant, best_lb = sp->rank.low_bits, tried = 0;
+  if (sp->kind == SPACE_FERMION && sp->index_mode == DH_INDEX_RANK) {
+    const int L = sp->lz_max;
+    const int lb0 = (L + 2) / 2;
+    for (int variant : {0, 2, 1}) {
+      for (int lb = lb0 - 2; lb <= lb0 + 2; ++lb) {
+        if (variant == 1 && lb != lb0) continue;  // the generic kernel does not read the tables' split
+        if (lb < 3 || lb > L || L + 1 - lb > 24) continue;
+        if (variant == 2 && lb > 15) continue;    // the staged low-rank table must fit in 64 KiB
+        sp->kernel_variant = variant;
+        if ((rc = build_rank_tables(sp, lb)) != DH_OK) return rc;
+        double ms = 0.0;
+        if ((rc = time_one(block_size, &ms)) != DH_OK) return rc;
+        ++tried;
+        if (ms < best) {
+          best = ms;
+          best_variant = variant;
+          best_lb = sp->rank.low_bits;
+        }
+      }
+    }
+    sp->kernel_variant = best_variant;
+    if ((rc = build_rank_tables(sp, best_lb)) != DH_OK) return rc;
+  } else {
+    if ((rc = time_one(block_size, &best)) != DH_OK) return rc;
+    tried = 1;
+  }
+  double per_k[3] = {0.0, 0.0, 0.0};
+  const int ks[3] = {1, 2, 4};
+  for (int i = 0; i < 3; ++i)
+    if ((rc = time_one(ks[i], &per_k[i])) != DH_OK) return rc;
+  if (out) {
+    out[0] = best;
+    out[1] = sp->kind == SPACE_FERMION ? sp->kernel_variant : 0;
+    out[2] = sp->kind == SPACE_FERMION ? sp->rank.low_bits : 0;
+    out[3] = per_k[0];
+    out[4] = per_k[1];
+    out[5] = per_k[2];
+    out[6] = tried;
+  }
   return DH_OK;
 }
 

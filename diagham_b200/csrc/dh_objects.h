@@ -17,6 +17,7 @@ struct dh_space_s {
   int index_mode = DH_INDEX_RANK;
   int kernel_variant = 0;  // product kernel of the rank mode (0 split-word, 1 generic, 2 split + smem table)
   int requested_low_bits = 0;
+  std::vector<int64_t> counts;  // [n][o][s]: n fermions in orbitals 0..o-1 with orbital-index sum s
   dh::DevBuf words;  // uint64 FermionOnSphere words, uint32 spin words (chain bits only)
   // FermionOnSphere
   int nbr_fermions = 0, lz_max = 0, total_lz = 0, total_sum = 0;
@@ -54,6 +55,9 @@ int build_lookup(dh_space_s* sp);
 FqheDevice fqhe_device(const dh_space_s* sp, const dh_hamiltonian_s* h, int precision);
 SpinDevice spin_device(const dh_space_s* sp, const dh_hamiltonian_s* h);
 int upload_factors(dh_hamiltonian_s* h);
+// (re)build the split-word rank tables of a FermionOnSphere space for a split of low_bits (0: the
+// default, or the space's requested split) and upload them
+int build_rank_tables(dh_space_s* sp, int low_bits);
 // y (+)= H x for nvec vectors stored one after the other; x32_ready: FP32 copy of x if already made
 int hamiltonian_apply(dh_hamiltonian_s* h, const double* x, double* y, int nvec, int64_t first, int64_t nbr,
                       int accumulate, const float* x32_ready, cudaStream_t stream);

@@ -146,6 +146,18 @@ int dh_hamiltonian_low_level_multiple_add_multiply(dh_hamiltonian_t h, const dou
  * for blocks kept interleaved, as the block Lanczos and (dim, k) torch tensors keep them. */
 int dh_hamiltonian_block_multiply(dh_hamiltonian_t h, const double* x, double* y, int k);
 
+/* Autotuner of the product (no reference counterpart): times this Hamiltonian's product on random
+ * blocks of block_size vectors (1, 2 or 4; the precision currently set), median of `repeats`
+ * CUDA-event timings per candidate, and keeps the fastest FQHE kernel form: split-word rank tables
+ * read through L1, split-word with the low-rank table staged in shared memory, or the generic
+ * kernel, over rank-table splits LB = default - 2 .. default + 2.  Every candidate computes the
+ * same product (the rank function does not depend on the split).  Spin chains have one form.
+ * out (optional, DH_TUNE_RESULTS doubles): best ms per product, kernel variant (0 split-word,
+ * 1 generic, 2 staged table), LB, ms per product of blocks of 1, 2 and 4 vectors with the chosen
+ * form, number of candidates timed. */
+#define DH_TUNE_RESULTS 7
+int dh_hamiltonian_autotune(dh_hamiltonian_t h, int block_size, int repeats, double* out);
+
 /* AbstractHamiltonian::MatrixElement(V1, V2) (AbstractQHEOnSphereHamiltonian.cc:380): <v1|H|v2>. */
 int dh_hamiltonian_matrix_element(dh_hamiltonian_t h, const double* v1, const double* v2, double* out);
 

@@ -188,3 +188,21 @@ def test_pseudopotential_adjoint_vs_oracle(gpu, orc):
     assert np.max(np.abs(got - ref)) < 1e-12
     # linearity in V: sum_m V_m <u|dH/dV_m|w> = <u|H|w>
     assert abs(got @ v - u @ O.pull(w)) < 1e-12
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_autotune_keeps_parity(gpu, orc, prec):
+    # every candidate form computes the same product: after tuning the product still matches the
+    # oracle, and the tuner reports the form it kept
+    z = golden("lanczos_n8_2s21_lz0_coulomb_basic.npz")
+    sp = gpu.FermionOnSphere(8, 0, 21)
+    H = gpu.ParticleOnSphereGenericHamiltonian(sp, 8, 21, z["v"])
+    H.set_precision(prec)
+    x = orc.random_vector(5, sp.dim)
+    ref = orc.FQHE(8, 21, 0, z["v"]).pull(x)
+    tol = 1e-13 if prec == "fp64" else 2e-6
+    r = H.autotune(block_size=2, repeats=2)
+    assert r["candidates"] >= 5 and r["best_ms"] > 0 and r["kernel_variant"] in ("split", "generic", "split+smem")
+    assert 0 < r["ms_k1"] and 0 < r["ms_k4"]
+    y = H.LowLevelMultiply(x)
+    assert np.max(np.abs(y - ref)) <= tol * np.max(np.abs(ref))
