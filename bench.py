@@ -393,6 +393,41 @@ def spin_chain_product(dh, flush, steps=5, k=2, length=32, warmup=2):
 
 
 
+def stored_elements(dh, H, flush, dim):
+    """The stored-element (fast multiplication) form of the sector's product: build time and size,
+    device time per product next to the on-the-fly form, and the autotuner's choice between them."""
+    import torch
+    res = {}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    on, nbytes = H.EnableFastMultiplication()
+    torch.cuda.synchronize()
+    res.update(built=on, bytes=nbytes, build_seconds=time.perf_counter() - t0)
+    if not on:
+        return res
+    for prec, k in (("fp64", 1), ("fp32", 1), ("fp32", BLOCK)):
+        H.set_precision(prec)
+        x = torch.rand(dim, k, dtype=torch.float64, device="cuda") - 0.5
+        y = torch.empty_like(x)
+        H.block_multiply(x, y)
+        ms = []
+        for _ in range(5):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            H.block_multiply(x, y)
+            b.record()
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        res["%s_k%d_ms" % (prec, k)] = statistics.median(ms)
+    H.set_precision("fp32")
+    t = H.autotune(block_size=BLOCK, repeats=3)
+    res["autotuned_k%d" % BLOCK] = {"stored_ms": t["stored_ms"], "best_ms": t["best_ms"],
+                                   "stored_in_use": t["stored_in_use"]}
+    H.DisableFastMultiplication()
+    return res
+
+
 def gradients_two_sectors(dh, h=1e-6):
     """dE0/dV_m and d(neutral gap)/dV_m, odd m = 1..27, for N=10, 2S=27, Lz = 0 and 1 (Coulomb V_m
     plus uniform [-0.05, 0.05) noise from splitmix64 seed 2) by the adjoint kernel (Hellmann-Feynman
@@ -539,8 +574,10 @@ def run_b200(args, world, rank, local):
     e2e_s = reduce_max(time.perf_counter() - t0, world)
     e2e_value = world * BLOCK * e2e_steps / e2e_s
 
-    tte = tte_c = spin = grads = None
+    tte = tte_c = spin = grads = stored = None
     if not args.no_solve:
+        stored = stored_elements(dh, H, flush, dim)
+        H.autotune(block_size=BLOCK, repeats=3)
         tte = time_to_e0_single_sector(dh, H)
         tte_c = time_to_e0_all_sectors(dh)
         grads = gradients_two_sectors(dh)
@@ -568,6 +605,7 @@ def run_b200(args, world, rank, local):
             "time_to_e0": tte,
             "time_to_e0_all_sectors": tte_c,
             "gradients": grads,
+            "stored_elements": stored,
             "spin_chain_l32": spin}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()

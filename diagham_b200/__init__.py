@@ -59,6 +59,8 @@ SIGNATURES = {
     "dh_hamiltonian_low_level_multiple_add_multiply": ([_vp, _vp, _vp, _c_int, _c_i64, _c_i64], _c_int),
     "dh_hamiltonian_block_multiply": ([_vp, _vp, _vp, _c_int], _c_int),
     "dh_hamiltonian_autotune": ([_vp, _c_int, _c_int, _vp], _c_int),
+    "dh_hamiltonian_enable_fast_multiplication": ([_vp, _c_i64, _ip, _i64p], _c_int),
+    "dh_hamiltonian_disable_fast_multiplication": ([_vp], _c_int),
     "dh_hamiltonian_matrix_element": ([_vp, _vp, _vp, _vp], _c_int),
     "dh_hamiltonian_row_elements": ([_vp, _c_i64, _vp, _vp, _vp, _c_int, _ip], _c_int),
     "dh_hamiltonian_pseudopotential_adjoint": ([_vp, _vp, _vp, _vp], _c_int),
@@ -271,12 +273,25 @@ class _Hamiltonian:
         d.finish()
         return y
 
+    def EnableFastMultiplication(self, allowed_memory=-1):
+        """Store every row's elements in device memory if they fit in allowed_memory bytes (< 0: no
+        budget).  Returns (enabled, bytes needed)."""
+        en = ctypes.c_int(0)
+        nb = ctypes.c_int64(0)
+        _check(_lib.dh_hamiltonian_enable_fast_multiplication(self._handle, int(allowed_memory), ctypes.byref(en),
+                                                              ctypes.byref(nb)))
+        return bool(en.value), nb.value
+
+    def DisableFastMultiplication(self):
+        _check(_lib.dh_hamiltonian_disable_fast_multiplication(self._handle))
+
     def autotune(self, block_size=1, repeats=3):
         """Time the product's kernel forms on this Hamiltonian and keep the fastest one."""
-        out = np.zeros(7, np.float64)
+        out = np.zeros(9, np.float64)
         _check(_lib.dh_hamiltonian_autotune(self._handle, block_size, repeats, out.ctypes.data))
         return dict(best_ms=out[0], kernel_variant={0: "split", 1: "generic", 2: "split+smem"}[int(out[1])],
-                    low_bits=int(out[2]), ms_k1=out[3], ms_k2=out[4], ms_k4=out[5], candidates=int(out[6]))
+                    low_bits=int(out[2]), ms_k1=out[3], ms_k2=out[4], ms_k4=out[5], candidates=int(out[6]),
+                    stored_ms=out[7], stored_in_use=bool(out[8]))
 
     def count_elements(self):
         """Elements one product generates (moves incl. diagonal ones; spin flips)."""

@@ -208,6 +208,28 @@ int ensure_buffer(DevBuf& b, size_t bytes) {
   return b.alloc(bytes);
 }
 
+EllDevice ell_device(const dh_hamiltonian_s* h, int precision) {
+  EllDevice e = {};
+  e.slice_ptr = h->ell_slice_ptr.as<long long>();
+  e.slice_len = h->ell_slice_len.as<int>();
+  e.cols = h->ell_cols.as<int>();
+  e.coef = h->ell_coef.as<uint16_t>();
+  e.diag = precision == DH_PRECISION_FP32 ? h->diag32.ptr : h->diag64.ptr;
+  e.factors = precision == DH_PRECISION_FP32 ? h->factors32.ptr : h->factors64.ptr;
+  e.dim = h->space->dim;
+  e.nbr_factors = h->tabs.nbr_factors;
+  return e;
+}
+
+int refresh_fast_diagonal(dh_hamiltonian_s* h) {
+  if (!h->fast) return DH_OK;
+  int rc = launch_fqhe_diag(fqhe_device(h->space, h, DH_PRECISION_FP64), h->factors64.as<double>(),
+                            h->diag64.as<double>(), h->diag32.as<float>(), h->stream);
+  if (rc != DH_OK) return rc;
+  DH_CUDA(cudaStreamSynchronize(h->stream));
+  return DH_OK;
+}
+
 // y (+)= H x for nvec vectors stored one after the other (stride dim); x, y device pointers.
 // In FP32 mode x is converted to FP32 first and the diagonal (shift) term uses the FP64 x.
 int hamiltonian_apply(dh_hamiltonian_s* h, const double* x, double* y, int nvec, int64_t first, int64_t nbr,
@@ -242,6 +264,7 @@ int hamiltonian_apply(dh_hamiltonian_s* h, const double* x, double* y, int nvec,
     a.xdiag = nullptr;
   }
   if (sp->kind == SPACE_FERMION) {
+    if (h->fast && h->fast_use && first == 0 && nbr == dim) return launch_ell_product(ell_device(h, h->precision), a, h->precision, stream);
     if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
     return launch_fqhe_matvec(fqhe_device(sp, h, h->precision), a, h->precision, stream);
   }
@@ -274,6 +297,7 @@ int hamiltonian_apply_block(dh_hamiltonian_s* h, const double* x64, const float*
   }
   int rc;
   if (sp->kind == SPACE_FERMION) {
+    if (h->fast && h->fast_use) return launch_ell_product(ell_device(h, precision), a, precision, stream);
     if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
     return launch_fqhe_matvec(fqhe_device(sp, h, precision), a, precision, stream);
   }
@@ -532,7 +556,91 @@ int dh_hamiltonian_set_pseudopotentials(dh_hamiltonian_t h, const double* v) {
   DH_CHECK(h->kind == SPACE_FERMION, DH_ERR_ARGUMENT, "pseudopotentials only apply to FQHE Hamiltonians");
   h->v.assign(v, v + h->tabs.lz_max + 1);
   h->tabs.set_pseudopotentials(h->v.data());
-  return upload_factors(h);
+  int rc = upload_factors(h);
+  if (rc != DH_OK) return rc;
+  return refresh_fast_diagonal(h);  // the stored elements hold factor indices: only the diagonal changes
+}
+
+int dh_hamiltonian_enable_fast_multiplication(dh_hamiltonian_t h, int64_t allowed_memory, int* enabled,
+                                              int64_t* bytes) {
+  DH_CHECK(h, DH_ERR_ARGUMENT, "null hamiltonian");
+  if (enabled) *enabled = 0;
+  if (bytes) *bytes = 0;
+  DH_CHECK(h->kind == SPACE_FERMION, DH_ERR_UNSUPPORTED, "stored elements are available for FQHE Hamiltonians");
+  DH_CHECK(h->tabs.nbr_factors < 0x8000, DH_ERR_UNSUPPORTED, "%d interaction factors do not fit 15-bit indices",
+           h->tabs.nbr_factors);
+  if (h->fast) {
+    if (enabled) *enabled = 1;
+    if (bytes) *bytes = (int64_t)h->fast_bytes;
+    return DH_OK;
+  }
+  dh_space_s* sp = h->space;
+  const long long dim = sp->dim;
+  const FqheDevice f = fqhe_device(sp, h, DH_PRECISION_FP64);
+  int rc;
+  // per-row element counts, then the slices (32 rows, padded to the longest) and their offsets
+  std::vector<int> counts(dim);
+  {
+    DevBuf dcounts;
+    if ((rc = dcounts.alloc((size_t)dim * sizeof(int))) != DH_OK) return rc;
+    if ((rc = launch_fqhe_row_counts(f, dcounts.as<int>(), h->stream)) != DH_OK) return rc;
+    DH_CUDA(cudaMemcpyAsync(counts.data(), dcounts.ptr, (size_t)dim * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    DH_CUDA(cudaStreamSynchronize(h->stream));
+  }
+  const long long nslices = (dim + 31) / 32;
+  std::vector<long long> slice_ptr(nslices);
+  std::vector<int> slice_len(nslices);
+  long long total = 0;
+  for (long long sl = 0; sl < nslices; ++sl) {
+    int mx = 0;
+    for (long long r = sl * 32; r < std::min(dim, sl * 32 + 32); ++r) mx = std::max(mx, counts[r]);
+    slice_ptr[sl] = total;
+    slice_len[sl] = mx;
+    total += 32ll * mx;
+  }
+  const size_t need = (size_t)total * (sizeof(int) + sizeof(uint16_t)) + (size_t)nslices * (sizeof(long long) + sizeof(int)) +
+                      (size_t)dim * (sizeof(double) + sizeof(float));
+  if (bytes) *bytes = (int64_t)need;
+  if (allowed_memory >= 0 && need > (size_t)allowed_memory) return DH_OK;  // the caller's memory budget
+  size_t free_b = 0, total_b = 0;
+  DH_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  if (need > free_b / 10 * 9) return DH_OK;
+  if ((rc = h->ell_slice_ptr.alloc((size_t)nslices * sizeof(long long))) != DH_OK ||
+      (rc = h->ell_slice_len.alloc((size_t)nslices * sizeof(int))) != DH_OK ||
+      (rc = h->ell_cols.alloc((size_t)total * sizeof(int))) != DH_OK ||
+      (rc = h->ell_coef.alloc((size_t)total * sizeof(uint16_t))) != DH_OK ||
+      (rc = h->diag64.alloc((size_t)dim * sizeof(double))) != DH_OK ||
+      (rc = h->diag32.alloc((size_t)dim * sizeof(float))) != DH_OK)
+    return rc;
+  DH_CUDA(cudaMemcpyAsync(h->ell_slice_ptr.ptr, slice_ptr.data(), slice_ptr.size() * sizeof(long long),
+                          cudaMemcpyHostToDevice, h->stream));
+  DH_CUDA(cudaMemcpyAsync(h->ell_slice_len.ptr, slice_len.data(), slice_len.size() * sizeof(int), cudaMemcpyHostToDevice,
+                          h->stream));
+  if ((rc = launch_fqhe_ell_fill(f, h->ell_slice_ptr.as<long long>(), h->ell_slice_len.as<int>(), h->ell_cols.as<int>(),
+                                 h->ell_coef.as<uint16_t>(), h->stream)) != DH_OK)
+    return rc;
+  h->fast = true;
+  h->fast_use = true;
+  h->fast_elements = total;
+  h->fast_bytes = need;
+  if ((rc = refresh_fast_diagonal(h)) != DH_OK) return rc;
+  if (enabled) *enabled = 1;
+  return DH_OK;
+}
+
+int dh_hamiltonian_disable_fast_multiplication(dh_hamiltonian_t h) {
+  DH_CHECK(h, DH_ERR_ARGUMENT, "null hamiltonian");
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  h->fast = false;
+  h->fast_elements = 0;
+  h->fast_bytes = 0;
+  h->ell_slice_ptr.release();
+  h->ell_slice_len.release();
+  h->ell_cols.release();
+  h->ell_coef.release();
+  h->diag64.release();
+  h->diag32.release();
+  return DH_OK;
 }
 
 int dh_hamiltonian_set_stream(dh_hamiltonian_t h, void* stream) {
@@ -649,6 +757,7 @@ int dh_hamiltonian_autotune(dh_hamiltonian_t h, int block_size, int repeats, dou
   };
   double best = 1e300;
   int best_variant = sp->kernel_variant, best_lb = sp->rank.low_bits, tried = 0;
+  h->fast_use = false;  // the on-the-fly forms first
   if (sp->kind == SPACE_FERMION && sp->index_mode == DH_INDEX_RANK) {
     const int L = sp->lz_max;
     const int lb0 = (L + 2) / 2;
@@ -675,11 +784,22 @@ int dh_hamiltonian_autotune(dh_hamiltonian_t h, int block_size, int repeats, dou
     if ((rc = time_one(block_size, &best)) != DH_OK) return rc;
     tried = 1;
   }
+  // stored elements, when built: kept in use only if they beat the best on-the-fly form
+  double stored_ms = 0.0;
+  if (h->fast) {
+    h->fast_use = true;
+    if ((rc = time_one(block_size, &stored_ms)) != DH_OK) return rc;
+    ++tried;
+    if (stored_ms < best) best = stored_ms;
+    else h->fast_use = false;
+  }
   double per_k[3] = {0.0, 0.0, 0.0};
   const int ks[3] = {1, 2, 4};
   for (int i = 0; i < 3; ++i)
     if ((rc = time_one(ks[i], &per_k[i])) != DH_OK) return rc;
   if (out) {
+    out[7] = stored_ms;
+    out[8] = (h->fast && h->fast_use) ? 1.0 : 0.0;
     out[0] = best;
     out[1] = sp->kind == SPACE_FERMION ? sp->kernel_variant : 0;
     out[2] = sp->kind == SPACE_FERMION ? sp->rank.low_bits : 0;

@@ -164,6 +164,23 @@ int launch_fqhe_bins(const FqheDevice& f, const double* u, const double* v, doub
 int launch_fqhe_count(const FqheDevice& f, unsigned long long* total, cudaStream_t s);
 int launch_fqhe_find(const FqheDevice& f, const uint64_t* words, long long n, long long* out, cudaStream_t s);
 
+// Stored elements of an FQHE Hamiltonian (sliced ELL, 32-row slices; see kernels_fast.cu)
+struct EllDevice {
+  const long long* slice_ptr;  // [nslices] first element of each slice
+  const int* slice_len;        // [nslices] elements per row of the slice (padded)
+  const int* cols;             // target index of each element
+  const uint16_t* coef;        // factor index | sign << 15; padding holds nbr_factors (a zero factor)
+  const void* diag;            // [dim] diagonal, FP64 or FP32 like the factors
+  const void* factors;         // [nbr_factors] FP64 or FP32
+  long long dim;
+  int nbr_factors;
+};
+int launch_fqhe_row_counts(const FqheDevice& f, int* counts, cudaStream_t s);
+int launch_fqhe_ell_fill(const FqheDevice& f, const long long* slice_ptr, const int* slice_len, int* cols,
+                         uint16_t* coef, cudaStream_t s);
+int launch_fqhe_diag(const FqheDevice& f, const double* factors64, double* diag64, float* diag32, cudaStream_t s);
+int launch_ell_product(const EllDevice& e, const MatvecArgs& a, int precision, cudaStream_t s);
+
 struct SpinDevice {
   const uint32_t* words;
   long long dim;

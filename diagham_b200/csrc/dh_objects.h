@@ -42,6 +42,12 @@ struct dh_hamiltonian_s {
   dh::DevBuf pair_offset, factors64, factors32;
   // J1-J2 chain
   double j1 = 0.0, j2 = 0.0;
+  // stored elements (fast multiplication): built by dh_hamiltonian_enable_fast_multiplication
+  bool fast = false;
+  bool fast_use = true;  // products read the stored elements (the autotuner may prefer the on-the-fly form)
+  long long fast_elements = 0;  // stored elements, padding included
+  size_t fast_bytes = 0;
+  dh::DevBuf ell_slice_ptr, ell_slice_len, ell_cols, ell_coef, diag64, diag32;
   // staging / scratch
   dh::DevBuf stage_x, stage_y, stage_v, x32, bins_partial, bins;
   dh::Reducer red;
@@ -58,6 +64,10 @@ int upload_factors(dh_hamiltonian_s* h);
 // (re)build the split-word rank tables of a FermionOnSphere space for a split of low_bits (0: the
 // default, or the space's requested split) and upload them
 int build_rank_tables(dh_space_s* sp, int low_bits);
+// the stored-element view of an FQHE Hamiltonian whose fast multiplication is enabled
+EllDevice ell_device(const dh_hamiltonian_s* h, int precision);
+// recompute the stored diagonal after the factors changed
+int refresh_fast_diagonal(dh_hamiltonian_s* h);
 // y (+)= H x for nvec vectors stored one after the other; x32_ready: FP32 copy of x if already made
 int hamiltonian_apply(dh_hamiltonian_s* h, const double* x, double* y, int nvec, int64_t first, int64_t nbr,
                       int accumulate, const float* x32_ready, cudaStream_t stream);

@@ -1,0 +1,303 @@
+// Stored-element ("fast multiplication") form of the two-body FQHE product on sm_100a.
+//
+// The reference can precompute, for every row, the list of (target index, interaction-factor
+// index) of its matrix elements and multiply from those lists afterwards
+// (AbstractQHEOnSphereHamiltonian::EnableFastMultiplication / FastMultiplicationMemory,
+// AbstractQHEOnSphereHamiltonian.cc:3625,3814; QHEParticlePrecalculationOperation.cc:95).  Here the
+// lists are kept in device memory as sliced ELL: rows are grouped in slices of 32 consecutive rows
+// (one warp), every row of a slice is padded to the slice's longest row, and element j of the
+// slice's 32 rows is stored contiguously, so that a warp reads one coalesced run per element.
+// Each element is an int32 target and a uint16 factor index with the fermionic sign in bit 15; the
+// structure does not depend on the pseudopotentials.  Diagonal moves are summed per row into a
+// separate diagonal array, recomputed when the pseudopotentials change.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dh_internal.h"
+
+namespace dh {
+namespace {
+
+constexpr int kFastThreads = 256;
+
+__device__ __forceinline__ uint64_t bits_between(int lo, int hi) {
+  // bits strictly between lo and hi (lo < hi <= 63)
+  return ((1ull << hi) - 1ull) & ~((2ull << lo) - 1ull);
+}
+
+__device__ __forceinline__ uint64_t mirror_of(uint64_t e, int M) {
+  // bit p of the result = bit (M - p) of e (0 when M - p is outside 0..63)
+  const uint64_t r = __brevll(e);
+  return (M <= 63) ? (r >> (63 - M)) : (r << (M - 63));
+}
+
+// Visits the off-diagonal elements of row word s (moves whose two created orbitals are both empty
+// in s): pairs m1 > m2 occupied, descending, then m3 ascending over E & mirror_M(E) above M/2.
+// visit(target, factor index, negative) is called for each; rank-table target indices.
+template <typename Visit>
+__device__ __forceinline__ void visit_row(const FqheDevice& f, uint64_t s, Visit&& visit) {
+  const uint64_t full = (f.lz_max >= 63) ? ~0ull : ((1ull << (f.lz_max + 1)) - 1ull);
+  const uint64_t E = ~s & full;
+  const uint64_t lmask = (1ull << f.low_bits) - 1ull;
+  uint64_t rem1 = s;
+  while (rem1) {
+    const int m1 = 63 - __clzll(rem1);
+    rem1 &= ~(1ull << m1);
+    uint64_t rem2 = rem1;
+    while (rem2) {
+      const int m2 = 63 - __clzll(rem2);
+      rem2 &= ~(1ull << m2);
+      const int M = m1 + m2;
+      uint64_t valid = E & mirror_of(E, M) & (~0ull << (M / 2 + 1));
+      if (!valid) continue;
+      const uint64_t an = s & ~((1ull << m1) | (1ull << m2));
+      const int paa = 1 + __popcll(s & bits_between(m2, m1));
+      const int fbase = __ldg(f.pair_offset + (m1 * (m1 - 1) / 2 + m2)) - (M / 2 + 1);
+      while (valid) {
+        const int m3 = __ffsll(valid) - 1;
+        valid &= valid - 1ull;
+        const int m4 = M - m3;
+        const uint64_t t = an | (1ull << m3) | (1ull << m4);
+        const int idx = __ldg(f.high_offset + (t >> f.low_bits)) + (int)__ldg(f.low_rank + (t & lmask));
+        const bool neg = (paa + __popcll(an & bits_between(m4, m3))) & 1;
+        visit(idx, fbase + m3, neg);
+      }
+    }
+  }
+}
+
+__global__ void row_counts_kernel(FqheDevice f, int* counts) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const uint64_t full = (f.lz_max >= 63) ? ~0ull : ((1ull << (f.lz_max + 1)) - 1ull);
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+    const uint64_t s = __ldg(f.words + r);
+    const uint64_t E = ~s & full;
+    int n = 0;
+    uint64_t rem1 = s;
+    while (rem1) {
+      const int m1 = 63 - __clzll(rem1);
+      rem1 &= ~(1ull << m1);
+      uint64_t rem2 = rem1;
+      while (rem2) {
+        const int m2 = 63 - __clzll(rem2);
+        rem2 &= ~(1ull << m2);
+        const int M = m1 + m2;
+        n += __popcll(E & mirror_of(E, M) & (~0ull << (M / 2 + 1)));
+      }
+    }
+    counts[r] = n;
+  }
+}
+
+__global__ void ell_fill_kernel(FqheDevice f, const long long* slice_ptr, const int* slice_len, int* cols,
+                                uint16_t* coef) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+    const long long sl = r >> 5;
+    const long long base = slice_ptr[sl] + (r & 31);
+    const int len = slice_len[sl];
+    int j = 0;
+    visit_row(f, __ldg(f.words + r), [&](int idx, int fidx, bool neg) {
+      cols[base + (long long)j * 32] = idx;
+      coef[base + (long long)j * 32] = (uint16_t)(fidx | (neg ? 0x8000 : 0));
+      ++j;
+    });
+    for (; j < len; ++j) {  // padding: the row itself times a zero factor
+      cols[base + (long long)j * 32] = (int)r;
+      coef[base + (long long)j * 32] = (uint16_t)f.nbr_factors;
+    }
+  }
+}
+
+// diagonal of every row: the (m3, m4) = (m1, m2) moves have sign -1, so d = -sum factor(m1, m2, m1)
+__global__ void diag_kernel(FqheDevice f, const double* factors, double* diag64, float* diag32) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+    const uint64_t s = __ldg(f.words + r);
+    double d = 0.0;
+    uint64_t rem1 = s;
+    while (rem1) {
+      const int m1 = 63 - __clzll(rem1);
+      rem1 &= ~(1ull << m1);
+      uint64_t rem2 = rem1;
+      while (rem2) {
+        const int m2 = 63 - __clzll(rem2);
+        rem2 &= ~(1ull << m2);
+        const int M = m1 + m2;
+        d -= factors[__ldg(f.pair_offset + (m1 * (m1 - 1) / 2 + m2)) - (M / 2 + 1) + m1];
+      }
+    }
+    diag64[r] = d;
+    diag32[r] = (float)d;
+  }
+}
+
+template <typename TG, int K, bool IL>
+__device__ __forceinline__ void gather(const TG* x, const MatvecArgs& a, long long idx, TG (&v)[K]) {
+  if constexpr (IL && sizeof(TG) == 4 && K == 4) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(x + idx * 4));
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+  } else if constexpr (IL && sizeof(TG) == 4 && K == 2) {
+    const float2 q = __ldg(reinterpret_cast<const float2*>(x + idx * 2));
+    v[0] = q.x; v[1] = q.y;
+  } else if constexpr (IL && sizeof(TG) == 8 && (K == 2 || K == 4)) {
+#pragma unroll
+    for (int j = 0; j < K; j += 2) {
+      const double2 q = __ldg(reinterpret_cast<const double2*>(x + idx * K) + j / 2);
+      v[j] = q.x;
+      v[j + 1] = q.y;
+    }
+  } else {
+    const TG* p = x + idx * a.ld;
+#pragma unroll
+    for (int q = 0; q < K; ++q) v[q] = __ldg(p + q * a.vstride);
+  }
+}
+
+// y = H x from the stored elements: lanes own the 32 rows of a slice; the element stream, the
+// diagonal and y go through L2 with streaming (evict-first) accesses so that the gathered x keeps
+// the cache
+template <typename TG, int K, bool IL>
+__global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, MatvecArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  TG* sfac = reinterpret_cast<TG*>(smem);
+  const TG* gfac = static_cast<const TG*>(e.factors);
+  for (int i = threadIdx.x; i < e.nbr_factors; i += blockDim.x) sfac[i] = gfac[i];
+  if (threadIdx.x == 0) sfac[e.nbr_factors] = TG(0);
+  __syncthreads();
+  const TG* x = static_cast<const TG*>(a.x);
+  const TG* diag = static_cast<const TG*>(e.diag);
+  const int lane = threadIdx.x & 31;
+  const long long nslices = (e.dim + 31) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long sl = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < nslices; sl += nwarps) {
+    const long long r = sl * 32 + lane;
+    if (r >= e.dim) continue;
+    const long long base = e.slice_ptr[sl] + lane;
+    const int len = e.slice_len[sl];
+    TG acc[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) acc[q] = TG(0);
+    int j = 0;
+    for (; j + 1 < len; j += 2) {
+      const long long pa = base + (long long)j * 32, pb = pa + 32;
+      const int ca = __ldcs(e.cols + pa), cb = __ldcs(e.cols + pb);
+      const unsigned short ka = __ldcs(e.coef + pa), kb = __ldcs(e.coef + pb);
+      TG fa = sfac[ka & 0x7fff], fb = sfac[kb & 0x7fff];
+      if (ka & 0x8000) fa = -fa;
+      if (kb & 0x8000) fb = -fb;
+      TG xa[K], xb[K];
+      gather<TG, K, IL>(x, a, ca, xa);
+      gather<TG, K, IL>(x, a, cb, xb);
+#pragma unroll
+      for (int q = 0; q < K; ++q) acc[q] += fa * xa[q] + fb * xb[q];
+    }
+    if (j < len) {
+      const long long pa = base + (long long)j * 32;
+      const int ca = __ldcs(e.cols + pa);
+      const unsigned short ka = __ldcs(e.coef + pa);
+      TG fa = sfac[ka & 0x7fff];
+      if (ka & 0x8000) fa = -fa;
+      TG xa[K];
+      gather<TG, K, IL>(x, a, ca, xa);
+#pragma unroll
+      for (int q = 0; q < K; ++q) acc[q] += fa * xa[q];
+    }
+    TG xr[K];
+    gather<TG, K, IL>(x, a, r, xr);
+    const TG d = __ldcs(diag + r);
+#pragma unroll
+    for (int q = 0; q < K; ++q) acc[q] += d * xr[q];
+    const bool on_diag = (r >= a.row_first && r < a.row_last);
+    double* y = static_cast<double*>(a.y);
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+      double v = (double)acc[q];
+      const long long xo = IL ? r * K + q : r * a.ld + q * a.vstride;
+      if (on_diag && a.shift != 0.0) v += a.shift * (a.xdiag ? a.xdiag[xo] : (double)x[xo]);
+      double* yp = y + (IL ? r * K + q : r * a.ld_y + q * a.vstride_y);
+      __stcs(yp, a.accumulate ? (__ldcs(yp) + v) : v);
+    }
+  }
+}
+
+unsigned grid_for(long long n) {
+  long long g = (n + 255) / 256;
+  if (g > 148 * 32) g = 148 * 32;
+  if (g < 1) g = 1;
+  return (unsigned)g;
+}
+
+template <typename TG, int K, bool IL>
+int launch_ell_typed(const EllDevice& e, const MatvecArgs& a, cudaStream_t s) {
+  auto kern = ell_product_kernel<TG, K, IL>;
+  const int smem = (e.nbr_factors + 1) * (int)sizeof(TG);
+  if (smem > 48 * 1024) DH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int dev = 0, sms = 0, per_sm = 0;
+  DH_CUDA(cudaGetDevice(&dev));
+  DH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  DH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFastThreads, smem));
+  DH_CHECK(per_sm >= 1, DH_ERR_UNSUPPORTED, "stored-element product: %d bytes of shared memory do not fit", smem);
+  long long need = ((e.dim + 31) / 32 * 32 + kFastThreads - 1) / kFastThreads;
+  long long grid = (long long)sms * per_sm;
+  if (need < grid) grid = need;
+  if (grid < 1) grid = 1;
+  kern<<<(unsigned)grid, kFastThreads, smem, s>>>(e, a);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+template <typename TG>
+int launch_ell_k(const EllDevice& e, MatvecArgs a, cudaStream_t s) {
+  const int nv = a.nbr_vectors;
+  if ((nv == 2 || nv == 4) && a.ld == nv && a.vstride == 1 && a.ld_y == nv && a.vstride_y == 1)
+    return nv == 4 ? launch_ell_typed<TG, 4, true>(e, a, s) : launch_ell_typed<TG, 2, true>(e, a, s);
+  // separate or strided vectors: groups of 4, 2 and 1 sharing one pass over the elements
+  int left = nv, done = 0;
+  while (left > 0) {
+    const int k = left >= 4 ? 4 : (left >= 2 ? 2 : 1);
+    MatvecArgs b = a;
+    b.x = static_cast<const TG*>(a.x) + (size_t)done * a.vstride;
+    b.y = static_cast<double*>(a.y) + (size_t)done * a.vstride_y;
+    b.xdiag = a.xdiag ? a.xdiag + (size_t)done * a.vstride : nullptr;
+    b.nbr_vectors = k;
+    const int rc = (k == 4) ? launch_ell_typed<TG, 4, false>(e, b, s)
+                            : (k == 2 ? launch_ell_typed<TG, 2, false>(e, b, s) : launch_ell_typed<TG, 1, false>(e, b, s));
+    if (rc != DH_OK) return rc;
+    left -= k;
+    done += k;
+  }
+  return DH_OK;
+}
+
+}  // namespace
+
+int launch_fqhe_row_counts(const FqheDevice& f, int* counts, cudaStream_t s) {
+  if (f.dim <= 0) return DH_OK;
+  row_counts_kernel<<<grid_for(f.dim), 256, 0, s>>>(f, counts);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_fqhe_ell_fill(const FqheDevice& f, const long long* slice_ptr, const int* slice_len, int* cols,
+                         uint16_t* coef, cudaStream_t s) {
+  if (f.dim <= 0) return DH_OK;
+  ell_fill_kernel<<<grid_for(f.dim), 256, 0, s>>>(f, slice_ptr, slice_len, cols, coef);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_fqhe_diag(const FqheDevice& f, const double* factors64, double* diag64, float* diag32, cudaStream_t s) {
+  if (f.dim <= 0) return DH_OK;
+  diag_kernel<<<grid_for(f.dim), 256, 0, s>>>(f, factors64, diag64, diag32);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_ell_product(const EllDevice& e, const MatvecArgs& a, int precision, cudaStream_t s) {
+  if (e.dim <= 0) return DH_OK;
+  if (precision == DH_PRECISION_FP32) return launch_ell_k<float>(e, a, s);
+  return launch_ell_k<double>(e, a, s);
+}
+
+}  // namespace dh

@@ -146,16 +146,32 @@ int dh_hamiltonian_low_level_multiple_add_multiply(dh_hamiltonian_t h, const dou
  * for blocks kept interleaved, as the block Lanczos and (dim, k) torch tensors keep them. */
 int dh_hamiltonian_block_multiply(dh_hamiltonian_t h, const double* x, double* y, int k);
 
+/* EnableFastMultiplication / FastMultiplicationMemory (AbstractQHEOnSphereHamiltonian.cc:3625,3814):
+ * precompute every row's matrix elements (target index, interaction-factor index and sign; the
+ * diagonal moves summed per row) in device memory, as sliced ELL (32-row slices padded to their
+ * longest row), when they take at most allowed_memory bytes (< 0: no budget) and fit in the free
+ * device memory; every later full product of this Hamiltonian then reads them instead of
+ * enumerating the moves.  *bytes = the memory the structure needs (set even when it is not built),
+ * *enabled = 1 if it was built.  The elements do not depend on the pseudopotentials: setting new
+ * ones only recomputes the diagonal.  FQHE Hamiltonians only; partial column ranges stay on the fly. */
+int dh_hamiltonian_enable_fast_multiplication(dh_hamiltonian_t h, int64_t allowed_memory, int* enabled,
+                                              int64_t* bytes);
+/* Frees the stored elements: products go back to the on-the-fly kernels. */
+int dh_hamiltonian_disable_fast_multiplication(dh_hamiltonian_t h);
+
 /* Autotuner of the product (no reference counterpart): times this Hamiltonian's product on random
  * blocks of block_size vectors (1, 2 or 4; the precision currently set), median of `repeats`
  * CUDA-event timings per candidate, and keeps the fastest FQHE kernel form: split-word rank tables
  * read through L1, split-word with the low-rank table staged in shared memory, or the generic
  * kernel, over rank-table splits LB = default - 2 .. default + 2.  Every candidate computes the
  * same product (the rank function does not depend on the split).  Spin chains have one form.
+ * When stored elements exist (dh_hamiltonian_enable_fast_multiplication) their product is timed too
+ * and stays in use only if it is the fastest.
  * out (optional, DH_TUNE_RESULTS doubles): best ms per product, kernel variant (0 split-word,
  * 1 generic, 2 staged table), LB, ms per product of blocks of 1, 2 and 4 vectors with the chosen
- * form, number of candidates timed. */
-#define DH_TUNE_RESULTS 7
+ * form, number of candidates timed, ms of the stored-element product (0: none), 1 if the stored
+ * elements are in use. */
+#define DH_TUNE_RESULTS 9
 int dh_hamiltonian_autotune(dh_hamiltonian_t h, int block_size, int repeats, double* out);
 
 /* AbstractHamiltonian::MatrixElement(V1, V2) (AbstractQHEOnSphereHamiltonian.cc:380): <v1|H|v2>. */
