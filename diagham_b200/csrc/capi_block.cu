@@ -348,6 +348,11 @@ int engine_mixed_restart(BlockEngine& e, uint64_t seed) {
 // the residual target of a mixed restart aiming at |r|^2 <= precision |E| after the FP64 check
 inline double restart_residual_target(double precision) { return 0.1 * precision; }
 
+// the FP32 phase converges on the Ritz vector's residual too, down to the FP32 rounding floor of the
+// products (|r| of a few 1e-6 relative): when the target lies above it, the FP64 check that follows
+// passes without a restart
+inline double fp32_phase_residual_target(double precision) { return std::max(0.1 * precision, 1e-11); }
+
 // one block step for every sector (results recorded for the active ones)
 int engine_step(BlockEngine& e) {
   const int k = e.k, kk = k * k;
@@ -559,7 +564,11 @@ int sector_evaluate(const BlockEngine& e, BlockSector& b) {
   else
     b.prev_last = 2.0 * eig[nev - 1];
   b.ritz.swap(eig);
-  if (e.residual_target > 0.0) {
+  if (e.residual_target > 0.0 && e.nev == 1) {
+    // the residual needs the band matrix's eigenvector (a dense eigensolve on the host): only once
+    // the Ritz value has settled to 1e-7, which any residual small enough to pass implies anyway
+    const double l0 = b.ritz[0];
+    if (!(fabs(l0 - b.prev_last) < 1e-7 * fabs(l0))) return DH_OK;
     std::vector<double> C, vals;
     if ((rc = sector_ritz_coefficients(e, b, 1, C, vals)) != DH_OK) return rc;
     const int k = e.k, m = b.blocks;
@@ -948,9 +957,11 @@ int block_lanczos_solve_refined(BlockLanczos* b, int max_iter, double precision,
   const long long products0 = e.products, fp64_0 = e.fp64_products;
   if ((rc = launch_f32_copy(e.slot[e.slot_cur], e.x32.as<float>(), dim * k, e.stream)) != DH_OK) return rc;
   e.eig_precision = std::max(precision, 1e-9);
+  e.residual_target = fp32_phase_residual_target(precision);
   std::vector<double> eig(b->nev);
   int iters = 0, conv = 0;
   rc = block_lanczos_solve(b, max_iter, eig.data(), &iters, &conv);
+  e.residual_target = 0.0;
   const double e32 = eig[0];
   if (rc == DH_OK) rc = bl_ritz_block(b);
   double energy = e32, rnorm = 0.0;

@@ -596,11 +596,15 @@ int dh_lanczos_solve_refined(dh_lanczos_t l, int max_iter, double precision, dou
   }
   l->fp64_first = l->lock_v0 = false;
   // phase 1: FP32 products, FP64 recurrence, converged to the FP32 resolution of the Ritz value
+  // (converged on the Ritz vector's residual down to the FP32 rounding floor of the products: when
+  // the target lies above it the FP64 check that follows passes without a restart)
   h->precision = DH_PRECISION_FP32;
   l->precision = std::max(precision, 1e-9);
+  l->residual_target = std::max(0.1 * precision, 1e-11);
   double e32 = 0.0;
   int iters = 0, conv = 0;
   rc = dh_lanczos_solve(l, max_iter, 16, &e32, &iters, &conv);
+  l->residual_target = 0.0;
   if (rc == DH_OK) rc = lz_ground_state(l);
   double energy = e32, rnorm = 0.0;
   double* sc = l->coef.as<double>();
