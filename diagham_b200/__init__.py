@@ -47,6 +47,7 @@ SIGNATURES = {
     "dh_space_find_state_index": ([_vp, _vp, _c_i64, _vp], _c_int),
     "dh_space_set_index_mode": ([_vp, _c_int], _c_int),
     "dh_particle_on_sphere_generic_hamiltonian_create": ([_vp, _c_int, _c_int, _vp, _c_dbl, _vp], _c_int),
+    "dh_particle_on_sphere_l2_hamiltonian_create": ([_vp, _c_int, _c_int, _c_int, _c_dbl, _vp], _c_int),
     "dh_spin_chain_j1j2_hamiltonian_create": ([_vp, _c_dbl, _c_dbl, _vp], _c_int),
     "dh_hamiltonian_destroy": ([_vp], _c_int),
     "dh_hamiltonian_get_dimension": ([_vp, _i64p], _c_int),
@@ -364,6 +365,27 @@ class ParticleOnSphereGenericHamiltonian(_Hamiltonian):
         out = np.zeros(self.lz_max + 1, np.float64)
         _check(_lib.dh_hamiltonian_pseudopotential_adjoint_static(self._handle, a.ptr, b.ptr, out.ctypes.data))
         return out
+
+
+class ParticleOnSphereL2Hamiltonian(_Hamiltonian):
+    """ParticleOnSphereL2Hamiltonian(particles, nbrParticles, lzmax, totalLz, l2Factor) with Lz fixed
+    by the sector: l2_factor L^2 (ParticleOnSphereL2Hamiltonian.cc:240-368)."""
+
+    def __init__(self, space, nbr_particles, lz_max, total_lz, l2_factor=1.0):
+        load()
+        self.space = space
+        self.lz_max = lz_max
+        h = ctypes.c_void_p()
+        _check(_lib.dh_particle_on_sphere_l2_hamiltonian_create(space._handle, nbr_particles, lz_max, total_lz,
+                                                                float(l2_factor), ctypes.byref(h)))
+        self._handle = h
+        self.l2_factor = l2_factor
+
+    def total_angular_momentum(self, psi):
+        """L with <psi|L^2|psi> / <psi|psi> = L (L + 1)."""
+        psi = np.asarray(psi.detach().cpu() if hasattr(psi, "detach") else psi, np.float64)
+        l2 = self.MatrixElement(psi, psi) / float(psi @ psi) / self.l2_factor
+        return 0.5 * (np.sqrt(1.0 + 4.0 * max(l2, 0.0)) - 1.0)
 
 
 class SpinChainJ1J2Hamiltonian(_Hamiltonian):

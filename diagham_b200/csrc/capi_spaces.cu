@@ -477,12 +477,20 @@ int dh_particle_on_sphere_generic_hamiltonian_create(dh_space_t sp, int nbr_part
   DH_CHECK(nbr_particles == sp->nbr_fermions && lz_max == sp->lz_max, DH_ERR_ARGUMENT,
            "Hamiltonian (N = %d, lz_max = %d) does not match its space (N = %d, lz_max = %d)", nbr_particles, lz_max,
            sp->nbr_fermions, sp->lz_max);
-  DH_CHECK(l2_factor == 0.0, DH_ERR_UNSUPPORTED, "an L^2 term (l2_factor != 0) is not supported");
+  DH_CHECK(l2_factor == 0.0 || nbr_particles >= 2, DH_ERR_UNSUPPORTED, "an L^2 term needs at least two particles");
   dh_hamiltonian_s* h = new (std::nothrow) dh_hamiltonian_s();
   DH_CHECK(h, DH_ERR_MEMORY, "out of host memory");
   h->space = sp;
   h->kind = SPACE_FERMION;
   h->tabs.build(lz_max);
+  if (l2_factor != 0.0) {
+    // ParticleOnSphereGenericHamiltonian adds l2Factor L^2 (its L2Operator): a two-body table on top
+    // of the interaction's, and the constant l2Factor (Lz^2 + Lz) in the shift
+    h->tabs.build_l2(nbr_particles);
+    h->tabs.l2_factor = l2_factor;
+    h->shift_base = l2_factor * l2_constant(sp->total_lz);
+    h->shift = h->shift_base;
+  }
   h->v.assign(pseudopotentials, pseudopotentials + lz_max + 1);
   h->tabs.set_pseudopotentials(h->v.data());
   int rc;
@@ -503,6 +511,20 @@ int dh_particle_on_sphere_generic_hamiltonian_create(dh_space_t sp, int nbr_part
     return rc;
   }
   *out = h;
+  return DH_OK;
+}
+
+int dh_particle_on_sphere_l2_hamiltonian_create(dh_space_t sp, int nbr_particles, int lz_max, int total_lz,
+                                                double l2_factor, dh_hamiltonian_t* out) {
+  DH_CHECK(out, DH_ERR_ARGUMENT, "null output handle");
+  *out = nullptr;
+  DH_CHECK(sp && sp->kind == SPACE_FERMION, DH_ERR_ARGUMENT, "ParticleOnSphereL2Hamiltonian needs a FermionOnSphere space");
+  DH_CHECK(total_lz == sp->total_lz, DH_ERR_ARGUMENT, "total_lz %d does not match the space's %d", total_lz, sp->total_lz);
+  DH_CHECK(l2_factor != 0.0, DH_ERR_ARGUMENT, "l2_factor must not be 0");
+  std::vector<double> zero(lz_max + 1, 0.0);
+  int rc = dh_particle_on_sphere_generic_hamiltonian_create(sp, nbr_particles, lz_max, zero.data(), l2_factor, out);
+  if (rc != DH_OK) return rc;
+  (*out)->l2_only = true;
   return DH_OK;
 }
 
@@ -539,7 +561,7 @@ int dh_hamiltonian_get_dimension(dh_hamiltonian_t h, int64_t* dim) {
 
 int dh_hamiltonian_shift(dh_hamiltonian_t h, double shift) {
   DH_CHECK(h, DH_ERR_ARGUMENT, "null hamiltonian");
-  h->shift = shift;
+  h->shift = shift + h->shift_base;
   return DH_OK;
 }
 
@@ -553,7 +575,8 @@ int dh_hamiltonian_set_precision(dh_hamiltonian_t h, int precision) {
 
 int dh_hamiltonian_set_pseudopotentials(dh_hamiltonian_t h, const double* v) {
   DH_CHECK(h && v, DH_ERR_ARGUMENT, "null argument");
-  DH_CHECK(h->kind == SPACE_FERMION, DH_ERR_ARGUMENT, "pseudopotentials only apply to FQHE Hamiltonians");
+  DH_CHECK(h->kind == SPACE_FERMION && !h->l2_only, DH_ERR_ARGUMENT,
+           "pseudopotentials only apply to FQHE interaction Hamiltonians");
   h->v.assign(v, v + h->tabs.lz_max + 1);
   h->tabs.set_pseudopotentials(h->v.data());
   int rc = upload_factors(h);
@@ -893,7 +916,8 @@ int dh_hamiltonian_get_interaction_factors(dh_hamiltonian_t h, double* factors, 
 
 int dh_hamiltonian_pseudopotential_adjoint(dh_hamiltonian_t h, const double* u, const double* v, double* out) {
   DH_CHECK(h && u && v && out, DH_ERR_ARGUMENT, "null argument");
-  DH_CHECK(h->kind == SPACE_FERMION, DH_ERR_UNSUPPORTED, "the pseudopotential adjoint needs an FQHE Hamiltonian");
+  DH_CHECK(h->kind == SPACE_FERMION && !h->l2_only, DH_ERR_UNSUPPORTED,
+           "the pseudopotential adjoint needs an FQHE interaction Hamiltonian");
   dh_space_s* sp = h->space;
   const int64_t dim = sp->dim;
   const size_t bytes = (size_t)dim * sizeof(double);

@@ -52,7 +52,8 @@ int scratch_address(double** out) {
 extern "C" int dh_hamiltonian_pseudopotential_adjoint_static(dh_hamiltonian_t h, const double* u, const double* v,
                                                              double* out) {
   DH_CHECK(h && u && v && out, DH_ERR_ARGUMENT, "null argument");
-  DH_CHECK(h->kind == SPACE_FERMION, DH_ERR_UNSUPPORTED, "the pseudopotential adjoint needs an FQHE Hamiltonian");
+  DH_CHECK(h->kind == SPACE_FERMION && !h->l2_only, DH_ERR_UNSUPPORTED,
+           "the pseudopotential adjoint needs an FQHE interaction Hamiltonian");
   DH_CHECK(is_device_pointer(u) && is_device_pointer(v), DH_ERR_ARGUMENT,
            "u and v must be device pointers: this entry point stages nothing");
   const int nf = h->tabs.nbr_factors;

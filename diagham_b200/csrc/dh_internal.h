@@ -56,10 +56,17 @@ struct InteractionTables {
   int nbr_factors = 0;              // (pair, m3) entries with 2 m3 > m1 + m2
   std::vector<int> pair_offset;     // first factor of each pair
   std::vector<double> dfactor;      // [factor][m]: d factor / d V_m (factors are linear in V)
-  std::vector<double> factors;      // current factors for the current V
+  std::vector<double> factors;      // current factors for the current V (+ l2_factor * l2_part)
+  std::vector<double> l2_part;      // [factor]: the two-body table of L^2 (empty: no L^2 term)
+  double l2_factor = 0.0;
   void build(int lz_max);
+  // L^2 of nbr_particles fermions as a two-body table (L^2 = L-L+ + Lz^2 + Lz; the constant part
+  // is returned by l2_constant)
+  void build_l2(int nbr_particles);
   void set_pseudopotentials(const double* v);
 };
+// Lz^2 + Lz of the sector 2 Lz = total_lz: the constant part of L^2
+double l2_constant(int total_lz);
 
 // Symmetric tridiagonal eigenvalues (ascending) by implicit QL; optional eigenvectors
 // (column-major n x n) when z != nullptr.

@@ -34,7 +34,9 @@ struct dh_hamiltonian_s {
   dh_space_s* space = nullptr;
   int kind = 0;
   int precision = DH_PRECISION_FP64;
-  double shift = 0.0;
+  double shift = 0.0;        // user shift + shift_base
+  double shift_base = 0.0;   // constant part of the operator itself (l2 factor x (Lz^2 + Lz))
+  bool l2_only = false;      // ParticleOnSphereL2Hamiltonian: no pseudopotentials
   cudaStream_t stream = 0;
   // FQHE
   dh::InteractionTables tabs;

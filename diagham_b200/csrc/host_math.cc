@@ -222,6 +222,57 @@ void InteractionTables::set_pseudopotentials(const double* v) {
     for (int m = lz_max; m >= 0; --m) acc += v[m] * dfactor[(size_t)f * nlz + m];
     factors[f] = acc;
   }
+  if (!l2_part.empty() && l2_factor != 0.0)
+    for (int f = 0; f < nbr_factors; ++f) factors[f] += l2_factor * l2_part[f];
+}
+
+// L^2 = L-L+ + Lz^2 + Lz, the operator of ParticleOnSphereL2Hamiltonian (ParticleOnSphereL2Hamiltonian.cc:
+// 240-368), written in this table's form: the element of move (m1, m2) -> (m3, m4) is
+// F(m1, m2, m3) <t| a+_m3 a+_m4 a_m1 a_m2 |s>.  With L+ = sum_m lam_m a+_{m+1} a_m,
+//   L-L+ = sum_m lam_m^2 n_m - sum_{m, m'} lam_m lam_m' a+_m' a+_{m+1} a_{m'+1} a_m,
+// each two-body term is reordered to (m3 > m4, m1 > m2) with its fermionic sign, and the one-body
+// part is folded into the diagonal pair factors: at fixed N, sum_m w_m n_m =
+// sum_{a > b} (w_a + w_b) / (N - 1) n_a n_b, and a diagonal factor F contributes -F n_a n_b.
+void InteractionTables::build_l2(int nbr_particles) {
+  const int S2 = lz_max;
+  std::vector<double> lam(S2 + 1, 0.0);
+  for (int m = 0; m <= S2; ++m) lam[m] = 0.5 * sqrt((double)(S2 * (S2 + 2) - (2 * m - S2) * (2 * m - S2 + 2)));
+  l2_part.assign(nbr_factors, 0.0);
+  auto slot = [&](int m1, int m2, int m3) -> double& {
+    const int M = m1 + m2;
+    return l2_part[pair_offset[m1 * (m1 - 1) / 2 + m2] + (m3 - (M / 2 + 1))];
+  };
+  for (int m = 0; m < S2; ++m)
+    for (int mp = 0; mp < S2; ++mp) {
+      if (mp == m + 1 || mp + 1 == m) continue;
+      int a, b, c, d;
+      double s = -lam[m] * lam[mp];
+      if (mp > m + 1) {
+        a = mp;
+        b = m + 1;
+      } else {
+        a = m + 1;
+        b = mp;
+        s = -s;
+      }
+      if (mp + 1 > m) {
+        c = mp + 1;
+        d = m;
+      } else {
+        c = m;
+        d = mp + 1;
+        s = -s;
+      }
+      (void)b;
+      slot(c, d, a) += s;
+    }
+  for (int a = 0; a <= S2; ++a)
+    for (int b = 0; b < a; ++b) slot(a, b, a) -= (lam[a] * lam[a] + lam[b] * lam[b]) / (nbr_particles - 1);
+}
+
+double l2_constant(int total_lz) {
+  const double lz = 0.5 * total_lz;
+  return lz * lz + lz;
 }
 
 // ------------------------------------------------------------ eigensolvers

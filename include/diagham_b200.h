@@ -92,11 +92,22 @@ int dh_space_set_index_mode(dh_space_t space, int mode);
 /* ParticleOnSphereGenericHamiltonian(particles, nbrParticles, lzmax, pseudoPotential, l2Factor, ...):
  * FQHE/src/Hamiltonian/ParticleOnSphereGenericHamiltonian.cc:66-140, interaction factors
  * :493-612, on-the-fly multiplication (memory = 0).  pseudopotentials = V_0..V_lzmax, V_0 being
- * the delta interaction.  l2_factor must be 0 (the L^2 term is not on this path).  The
- * Hamiltonian does not own the space (FQHESphereFermionsTwoBodyGeneric.cc:395-396). */
+ * the delta interaction.  l2_factor != 0 adds l2_factor L^2 (the reference's L2Operator,
+ * AbstractQHEOnSphereHamiltonian.cc:541-542), as a second two-body table plus the constant
+ * l2_factor (Lz^2 + Lz) in the shift (N >= 2).  The Hamiltonian does not own the space
+ * (FQHESphereFermionsTwoBodyGeneric.cc:395-396). */
 int dh_particle_on_sphere_generic_hamiltonian_create(dh_space_t space, int nbr_particles, int lz_max,
                                                      const double* pseudopotentials, double l2_factor,
                                                      dh_hamiltonian_t* out);
+
+/* ParticleOnSphereL2Hamiltonian(particles, nbrParticles, lzmax, totalLz, architecture, l2Factor, memory,
+ * fixedLz = true, ...) (FQHE/src/Hamiltonian/ParticleOnSphereL2Hamiltonian.cc:73-133, operator
+ * :240-368): l2_factor L^2 on the sector, with L^2 = L-L+ + Lz^2 + Lz written as a two-body table
+ * (the one-body part folded into the diagonal pairs at fixed N >= 2) and the constant in the shift,
+ * so every product form (on the fly, stored elements, blocks) applies it.  <psi|L^2|psi> =
+ * L (L + 1) identifies the total angular momentum of a state.  total_lz must be the space's. */
+int dh_particle_on_sphere_l2_hamiltonian_create(dh_space_t space, int nbr_particles, int lz_max, int total_lz,
+                                                double l2_factor, dh_hamiltonian_t* out);
 
 /* Periodic J1-J2 spin-1/2 chain on a plain Spin1_2Chain: the element pattern of
  * Spin/src/Hamiltonian/SpinChainJ1J2RealHamiltonianWithTranslations.cc:94-192 (flips J/2) and

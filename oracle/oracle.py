@@ -272,3 +272,55 @@ def python_lanczos(matvec, dim, v0, nev=1, max_iter=200, precision=1e-14):
         ya[:] = matvec(xa)
     r = basic_lanczos(cb, None, dim, v0, nev, max_iter, precision)
     return r
+
+
+def l2_factors(n, two_s, total_lz):
+    """L^2 = L-L+ + Lz^2 + Lz of N fermions in 2S+1 orbitals as a two-body table in the layout of
+    interaction_tables (pairs m1 > m2, creation m3 > M/2, element = F(m1, m2, m3) <t|a+_m3 a+_m4
+    a_m1 a_m2|s>, the operator the reference's ParticleOnSphereL2Hamiltonian applies,
+    ParticleOnSphereL2Hamiltonian.cc:240-368): L+ = sum_m lam_m a+_{m+1} a_m, so
+    L-L+ = sum_m lam_m^2 n_m - sum_{m,m'} lam_m lam_m' a+_m' a+_{m+1} a_{m'+1} a_m, each term put in
+    canonical order with its fermionic sign; the one-body part is folded into the diagonal pair
+    factors (sum_m w_m n_m = sum_{a>b} (w_a + w_b) / (N - 1) n_a n_b at fixed N).  Returns
+    (factors, constant) with constant = Lz^2 + Lz, Lz = total_lz / 2."""
+    t = interaction_tables(two_s, np.zeros(two_s + 1))
+    lam = [0.5 * np.sqrt(two_s * (two_s + 2) - (2 * m - two_s) * (2 * m - two_s + 2)) for m in range(two_s + 1)]
+    F = {}
+
+    def add(c, d, a, val):
+        F[(c, d, a)] = F.get((c, d, a), 0.0) + val
+
+    for m in range(two_s):
+        for mp in range(two_s):
+            if mp == m + 1 or mp + 1 == m:
+                continue
+            a_, b_, s1 = (mp, m + 1, 1.0) if mp > m + 1 else (m + 1, mp, -1.0)
+            c_, d_, s2 = (mp + 1, m, 1.0) if mp + 1 > m else (m, mp + 1, -1.0)
+            add(c_, d_, a_, -lam[m] * lam[mp] * s1 * s2)
+    w = [lam[m] ** 2 for m in range(two_s + 1)]
+    for a_ in range(two_s + 1):
+        for b_ in range(a_):
+            add(a_, b_, a_, -(w[a_] + w[b_]) / (n - 1))
+    f = np.zeros_like(t["factors"])
+    for p in range(len(t["m1"])):
+        m1, m2 = int(t["m1"][p]), int(t["m2"][p])
+        for q in range(int(t["nbr_m3"][p])):
+            f[t["m3_offset"][p] + q] = F.get((m1, m2, int(t["m3"][t["m3_offset"][p] + q])), 0.0)
+    lz = total_lz / 2.0
+    return f, lz * lz + lz
+
+
+def l2_raise(n, two_s, total_lz, x):
+    """L+ x from the sector 2Lz to 2Lz + 2: a+_{m+1} a_m hops with coefficient lam_m and sign +1
+    (no orbital lies between m and m + 1)."""
+    words, _ = fermion_basis(n, two_s, total_lz)
+    up, _ = fermion_basis(n, two_s, total_lz + 2)
+    index = {int(w): i for i, w in enumerate(up)}
+    y = np.zeros(len(up))
+    for i, w in enumerate(words):
+        w = int(w)
+        for m in range(two_s):
+            if (w >> m) & 1 and not (w >> (m + 1)) & 1:
+                lam = 0.5 * np.sqrt(two_s * (two_s + 2) - (2 * m - two_s) * (2 * m - two_s + 2))
+                y[index[w ^ (3 << m)]] += lam * x[i]
+    return y

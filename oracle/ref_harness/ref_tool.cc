@@ -27,6 +27,7 @@
 #include "HilbertSpace/FermionOnSphere.h"
 #include "HilbertSpace/Spin1_2Chain.h"
 #include "Hamiltonian/ParticleOnSphereGenericHamiltonian.h"
+#include "Hamiltonian/ParticleOnSphereL2Hamiltonian.h"
 #include "Hamiltonian/AbstractHamiltonian.h"
 #include "Architecture/MonoProcessorArchitecture.h"
 #include "Architecture/SMPArchitecture.h"
@@ -317,6 +318,7 @@ static void Usage()
 	  "  fqhe_matvec N 2S 2Lz vfile xfile shift out\n"
 	  "  fqhe_lanczos N 2S 2Lz vfile algo nev block maxiter precision out gsout x0 [x1 ...]\n"
 	  "  fqhe_expect N 2S 2Lz vfile psifile out\n"
+	  "  fqhe_l2 N 2S 2Lz xfile out\n"
 	  "  pseudopotentials 2S out\n"
 	  "  spin_basis L 2Sz out\n"
 	  "  spin_matvec L 2Sz J1 J2 xfile out\n"
@@ -502,6 +504,21 @@ int main(int argc, char** argv)
       double x = (Psi * Tmp) / (Psi * Psi);
       fwrite(&x, sizeof(double), 1, f);
       fclose(f);
+      return 0;
+    }
+  if (strcmp(Cmd, "fqhe_l2") == 0 && argc == 7)
+    {
+      // y = L^2 x with the reference's ParticleOnSphereL2Hamiltonian (l2Factor 1, Lz fixed by the
+      // sector, on the fly, hermitian symmetry off)
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      FermionOnSphere Space(N, TotalLz, LzMax, 1ul << 20);
+      MonoProcessorArchitecture Arch;
+      RealVector X;
+      X.ReadVector(argv[5]);
+      RealVector Y(Space.GetHilbertSpaceDimension(), true);
+      ParticleOnSphereL2Hamiltonian L2(&Space, N, LzMax, TotalLz, &Arch, 1.0, 0, true, false, 0, false);
+      L2.LowLevelMultiply(X, Y);
+      Y.WriteVector(argv[6]);
       return 0;
     }
   if (strcmp(Cmd, "pseudopotentials") == 0 && argc == 4)

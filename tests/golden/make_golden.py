@@ -288,6 +288,19 @@ def gradient_fixtures(tmp):
              dim=dim, expectation=e[:-1], energy_expectation=e[-1], **read_lanczos(lf))
 
 
+def l2_fixtures(tmp):
+    # y = L^2 x by the reference's ParticleOnSphereL2Hamiltonian (l2Factor 1, fixed Lz, on the fly,
+    # hermitian symmetry off) for x = the splitmix64 vector of seed 7
+    for (n, s, lz) in [(6, 15, 0), (6, 15, 4), (7, 18, 2), (8, 21, 0), (8, 21, 6)]:
+        bf = os.path.join(tmp, "b.bin")
+        run("fqhe_basis", n, s, lz, bf)
+        dim, _, _ = read_basis(bf)
+        xf, yf = os.path.join(tmp, "xl2.vec"), os.path.join(tmp, "yl2.vec")
+        write_vector(xf, splitmix_vector(7, dim))
+        cmd = run("fqhe_l2", n, s, lz, xf, yf)
+        save("l2_n%d_2s%d_lz%d.npz" % (n, s, lz), cmd, seed=7, y=read_vector(yf))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--slow", action="store_true")
@@ -314,6 +327,8 @@ def main():
             spin_fixtures(tmp)
         if args.only in (None, "gradient"):
             gradient_fixtures(tmp)
+        if args.only in (None, "l2"):
+            l2_fixtures(tmp)
         if args.slow:
             slow_fixtures(tmp)
 

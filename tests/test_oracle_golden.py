@@ -172,3 +172,20 @@ def test_block_lanczos_fixture_against_dense(orc):
     w = np.linalg.eigvalsh(0.5 * (M + M.T))
     assert abs(w[0] - float(z["eigenvalues"][0])) < 1e-10 * abs(w[0])
     assert bool(z["converged"])
+
+
+@pytest.mark.parametrize("tag", ["n6_2s15_lz0", "n6_2s15_lz4", "n7_2s18_lz2", "n8_2s21_lz0", "n8_2s21_lz6"])
+def test_l2_table_matches_reference(orc, tag):
+    # the oracle's two-body form of L^2 (plus its constant) against the reference's
+    # ParticleOnSphereL2Hamiltonian product, and <x|L^2|x> against |L+ x|^2 + Lz (Lz + 1)
+    z = golden("l2_%s.npz" % tag)
+    n, s, lz = parse_sector(tag)
+    O = orc.FQHE(n, s, lz, np.zeros(s + 1))
+    f, c = orc.l2_factors(n, s, lz)
+    O.tabs["factors"][:len(f)] = f
+    x = orc.random_vector(int(z["seed"]), O.dim)
+    y = O.pull(x) + c * x
+    assert np.max(np.abs(y - z["y"])) <= 1e-13 * np.max(np.abs(z["y"]))
+    if O.dim < 2000:
+        up = orc.l2_raise(n, s, lz, x)
+        assert abs(float(x @ y) - (float(up @ up) + c)) <= 1e-12 * abs(float(x @ y))
