@@ -7,8 +7,10 @@ diagham_b200/_build.py).  Class and method names follow the reference classes th
     Spin1_2Chain                        Spin/src/HilbertSpace/Spin1_2Chain.h
     ParticleOnSphereGenericHamiltonian  FQHE/src/Hamiltonian/ParticleOnSphereGenericHamiltonian.h
     SpinChainJ1J2Hamiltonian            (J1-J2 pattern of SpinChainJ1J2RealHamiltonianWithTranslations on a plain chain)
-    BasicLanczosAlgorithm, FullReorthogonalizedLanczosAlgorithm, BasicLanczosAlgorithmWithGroundState
+    BasicLanczosAlgorithm, FullReorthogonalizedLanczosAlgorithm, BasicLanczosAlgorithmWithGroundState,
+    BasicLanczosAlgorithmWithDiskStorage, BasicLanczosAlgorithmWithGroundStateDiskStorage
                                         src/LanczosAlgorithm/*.h
+    WriteVector, ReadVector             RealVector::WriteVector / ReadVector (src/Vector/RealVector.cc)
 
 Vectors are FP64 numpy arrays (host) or torch CUDA tensors (used in place).  Every call goes to
 the GPU; there is no CPU fallback: importing without the built library raises.
@@ -83,6 +85,12 @@ SIGNATURES = {
     "dh_lanczos_get_counters": ([_vp, _i64p, _ip], _c_int),
     "dh_lanczos_solve": ([_vp, _c_int, _c_int, _vp, _ip, _ip], _c_int),
     "dh_lanczos_solve_refined": ([_vp, _c_int, _c_dbl, _vp], _c_int),
+    "dh_lanczos_set_disk_storage": ([_vp, ctypes.c_char_p, _c_int], _c_int),
+    "dh_lanczos_write_state": ([_vp], _c_int),
+    "dh_lanczos_resume": ([_vp], _c_int),
+    "dh_vector_write": ([ctypes.c_char_p, _vp, _c_i64], _c_int),
+    "dh_vector_file_dimension": ([ctypes.c_char_p, _i64p], _c_int),
+    "dh_vector_read": ([ctypes.c_char_p, _vp, _c_i64], _c_int),
     "dh_fqhe_sectors_block_lanczos": ([_c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _c_dbl, _c_int, _c_int,
                                        _c_u64, _vp, _vp, _vp], _c_int),
     "dh_coulomb_pseudopotentials": ([_c_int, _vp], _c_int),
@@ -489,10 +497,42 @@ class _Lanczos:
         return dict(energy=out[0], energy_fp32=out[1], residual=out[2], fp32_matvecs=int(out[3]),
                     fp64_matvecs=int(out[4]))
 
+    def set_disk_storage(self, directory, interval=1):
+        """Checkpoint the state into `directory` in the reference's disk-storage format of this
+        algorithm, every `interval` rows and at the end of solve; None switches it off."""
+        d = None if directory is None else os.fsencode(directory)
+        _check(_lib.dh_lanczos_set_disk_storage(self._handle, d, int(interval)))
+
+    def WriteState(self):
+        _check(_lib.dh_lanczos_write_state(self._handle))
+
+    def ResumeLanczosAlgorithm(self):
+        _check(_lib.dh_lanczos_resume(self._handle))
+
     def __del__(self):
         if self._handle and _lib is not None:
             _lib.dh_lanczos_destroy(self._handle)
             self._handle = None
+
+
+class BasicLanczosAlgorithmWithDiskStorage(_Lanczos):
+    """BasicLanczosAlgorithmWithDiskStorage(architecture, nbrEigenvalue, maxIter): the basic algorithm
+    with its state in `directory` (lanczos.dat and three vector files) after every `interval` rows."""
+    ALGORITHM = DH_LANCZOS_BASIC
+
+    def __init__(self, hamiltonian, nbr_eigenvalue=1, max_iter=500, directory=".", interval=1):
+        super().__init__(hamiltonian, nbr_eigenvalue, max_iter)
+        self.set_disk_storage(directory, interval)
+
+
+class BasicLanczosAlgorithmWithGroundStateDiskStorage(_Lanczos):
+    """BasicLanczosAlgorithmWithGroundStateDiskStorage(architecture, nbrIter, maxIter): the ground-state
+    algorithm with its state in `directory` (lanczos.dat, vector.0 = start vector, vector.1-3)."""
+    ALGORITHM = DH_LANCZOS_WITH_GROUND_STATE
+
+    def __init__(self, hamiltonian, max_iter=500, directory=".", interval=1):
+        super().__init__(hamiltonian, 1, max_iter)
+        self.set_disk_storage(directory, interval)
 
 
 class BasicLanczosAlgorithm(_Lanczos):
@@ -551,3 +591,35 @@ def fqhe_sectors_block_lanczos(nbr_fermions, lz_max, total_lz, pseudopotentials,
     return dict(energies=e, iterations=it, setup_seconds=secs[0], solve_seconds=secs[1], product_seconds=secs[2],
                 block_products=int(secs[3]), fp32_seconds=secs[4], refine_seconds=secs[5],
                 refined_sectors=int(secs[6]), max_refine_shift=secs[7])
+
+
+def WriteVector(vec, file_name):
+    """RealVector::WriteVector: vec (numpy or torch CUDA, FP64) into file_name."""
+    b = _Buf(vec)
+    load()
+    _check(_lib.dh_vector_write(os.fsencode(file_name), b.ptr, b.n))
+
+
+def vector_file_dimension(file_name):
+    load()
+    d = ctypes.c_int64(0)
+    _check(_lib.dh_vector_file_dimension(os.fsencode(file_name), ctypes.byref(d)))
+    return d.value
+
+
+def ReadVector(file_name, out=None):
+    """RealVector::ReadVector: the vector stored in file_name (into out if given: numpy or torch
+    CUDA of the stored dimension)."""
+    dim = vector_file_dimension(file_name)
+    if out is None:
+        out = np.zeros(dim, np.float64)
+    b = _Buf(out, writable=True)
+    _check(_lib.dh_vector_read(os.fsencode(file_name), b.ptr, b.n))
+    b.finish()
+    return out
+
+
+def eigenstate_file_name(statistics, interaction_name, nbr_particles, lz_max, total_lz, index):
+    """<statistics>_<interaction>_n_<N>_2s_<2S>_lz_<2Lz>.<index>.vec, the eigenstate naming of
+    FQHE/docs/DataFormat/FermionOnSphere.xml:9-16 (statistics "fermions" or "bosons", total_lz = 2 Lz)."""
+    return "%s_%s_n_%d_2s_%d_lz_%d.%d.vec" % (statistics, interaction_name, nbr_particles, lz_max, total_lz, index)

@@ -12,12 +12,65 @@
 
 #include <algorithm>
 #include <new>
+#include <string>
+#include <thread>
 #include <vector>
 
+#include "dh_disk.h"
 #include "dh_internal.h"
 #include "dh_objects.h"
 
 using namespace dh;
+
+namespace {
+
+// Writes checkpoint files on a background thread: the vectors wait in pinned host memory while the
+// GPU carries on with the next iterations.  One job at a time; wait() joins it and re-raises its
+// error on the calling thread.
+struct DiskWriter {
+  double* staging = nullptr;  // pinned host copies of the vectors of the job in flight
+  size_t staging_doubles = 0;
+  std::thread worker;
+  int status = DH_OK;
+  std::string message;
+  DiskWriter() = default;
+  DiskWriter(const DiskWriter&) = delete;
+  DiskWriter& operator=(const DiskWriter&) = delete;
+  ~DiskWriter() {
+    if (worker.joinable()) worker.join();
+    if (staging) cudaFreeHost(staging);
+  }
+  int wait() {
+    if (worker.joinable()) worker.join();
+    const int rc = status;
+    status = DH_OK;
+    if (rc != DH_OK) set_error("%s", message.c_str());
+    return rc;
+  }
+  int reserve(size_t doubles) {
+    if (staging_doubles >= doubles) return DH_OK;
+    if (staging) cudaFreeHost(staging);
+    staging = nullptr;
+    staging_doubles = 0;
+    DH_CUDA(cudaMallocHost(&staging, doubles * sizeof(double)));
+    staging_doubles = doubles;
+    return DH_OK;
+  }
+  // job: the vectors staging[q * dim] to paths[q], then (if state_path is not empty) the state file
+  void start(std::vector<std::string> paths, int64_t dim, std::string state_path, int algorithm,
+             LanczosDiskState state) {
+    worker = std::thread([this, paths, dim, state_path, algorithm, state]() {
+      int rc = DH_OK;
+      for (size_t q = 0; q < paths.size() && rc == DH_OK; ++q)
+        rc = vector_file_write(paths[q], staging + q * dim, dim);
+      if (rc == DH_OK && !state_path.empty()) rc = lanczos_state_write(state_path, algorithm, state);
+      if (rc != DH_OK) message = dh_last_error();
+      status = rc;
+    });
+  }
+};
+
+}  // namespace
 
 struct dh_lanczos_s {
   dh_hamiltonian_s* h = nullptr;
@@ -51,6 +104,17 @@ struct dh_lanczos_s {
   double residual_target = 0.0;
   cudaGraphExec_t graph3 = nullptr;  // three iterations starting at phase 0
   dh::BlockLanczos* blk = nullptr;   // DH_LANCZOS_BLOCK: everything runs in the block engine
+  // disk storage in the reference's disk-storage formats
+  bool disk = false;
+  std::string disk_dir;
+  int disk_interval = 1;
+  int disk_rows = -1;        // rows of the checkpoint on disk (-1: none yet)
+  int disk_set = 1;          // basic format: name set of the last checkpoint (0: vector1-3, 1: vector4-6)
+  int pending = 0;           // rows a resumed mid-call state owes the next run call
+  bool resumed = false;      // the next solve continues the driver loop without its first call
+  bool start_known = true;   // `initial` holds the start vector
+  bool krylov_valid = true;  // the Krylov store holds v_0, v_1, ... (not after a resume)
+  DiskWriter writer;
   ~dh_lanczos_s() {
     if (graph3) cudaGraphExecDestroy(graph3);
     if (blk) dh::block_lanczos_destroy(blk);
@@ -153,7 +217,10 @@ int lz_finish_call(dh_lanczos_s* l) {
 bool lz_converged(const dh_lanczos_s* l) {
   if (l->residual_target > 0.0) {
     const int n = l->rows - 1;
-    if (n < 2 || (int)l->beta.size() < n) return false;
+    if (n < 2 || (int)l->beta.size() < n || l->ritz.empty()) return false;
+    // the residual (an O(n^3) eigenvector solve on the host) only once the Ritz value has settled:
+    // near the residual target its changes are orders of magnitude below this
+    if (fabs(l->ritz[0] - l->prev_last) > 1e-7 * fabs(l->ritz[0])) return false;
     std::vector<double> eig(n), z((size_t)n * n);
     if (tridiagonal_eigen(n, l->alpha.data(), l->beta.data(), eig.data(), z.data()) != DH_OK) return false;
     const double r = l->beta[n - 1] * z[n - 1];  // column 0, last component
@@ -162,6 +229,63 @@ bool lz_converged(const dh_lanczos_s* l) {
   if ((int)l->ritz.size() < l->nev) return false;
   const double e = l->ritz[l->nev - 1];
   return fabs(e - l->prev_last) < l->precision * fabs(e);
+}
+
+// ------------------------------------------------------------------ disk storage
+// Files of the state after a RunLanczosAlgorithm call: v_index (slot index % 3), v_{index+1} and
+// H v_{index+1} (the next two slots), with lanczos.dat in the format of the algorithm's disk-storage
+// class.  The copies to pinned memory are ordered on the stream; a background thread writes them.
+int lz_checkpoint(dh_lanczos_s* l) {
+  int rc = l->writer.wait();
+  if (rc != DH_OK) return rc;
+  DH_CHECK(l->initialized && l->rows >= 2, DH_ERR_STATE,
+           "no Lanczos state to write (not run yet, or its vectors were used to rebuild the ground state)");
+  const int64_t dim = l->dim;
+  if ((rc = l->writer.reserve((size_t)3 * dim)) != DH_OK) return rc;
+  for (int q = 0; q < 3; ++q)
+    DH_CUDA(cudaMemcpyAsync(l->writer.staging + (size_t)q * dim, l->st.vec + (size_t)((l->index + q) % 3) * dim,
+                            dim * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
+  DH_CUDA(cudaStreamSynchronize(l->stream));
+  LanczosDiskState s;
+  s.index = l->index;
+  s.prev_last = l->prev_last;
+  s.precision = l->precision;
+  s.nbr_eigenvalue = l->nev;
+  s.nbr_row = l->rows;
+  s.diag.assign(l->alpha.begin(), l->alpha.begin() + l->rows);
+  s.upper.assign(l->beta.begin(), l->beta.begin() + (l->rows - 1));
+  std::vector<std::string> paths;
+  if (l->algorithm == DH_LANCZOS_BASIC) {
+    // the other name set than the checkpoint on disk, which stays whole until lanczos.dat moves on
+    const int set = 1 - l->disk_set;
+    for (int q = 0; q < 3; ++q) {
+      snprintf(s.names[q], sizeof(s.names[q]), "vector%d", 3 * set + q + 1);
+      paths.push_back(join_path(l->disk_dir, s.names[q]));
+    }
+    l->disk_set = set;
+  } else {
+    for (int q = 0; q < 3; ++q) {
+      char name[16];
+      snprintf(name, sizeof(name), "vector.%d", q + 1);
+      paths.push_back(join_path(l->disk_dir, name));
+    }
+  }
+  l->writer.start(paths, dim, join_path(l->disk_dir, "lanczos.dat"), l->algorithm, s);
+  l->disk_rows = l->rows;
+  return DH_OK;
+}
+
+// vector.0 of the ground-state format: the (normalised) start vector
+int lz_write_start_vector(dh_lanczos_s* l) {
+  if (!l->disk || l->algorithm != DH_LANCZOS_WITH_GROUND_STATE) return DH_OK;
+  int rc = l->writer.wait();
+  if (rc != DH_OK) return rc;
+  if ((rc = l->writer.reserve((size_t)l->dim)) != DH_OK) return rc;
+  DH_CUDA(cudaMemcpyAsync(l->writer.staging, l->initial.ptr, l->dim * sizeof(double), cudaMemcpyDeviceToHost,
+                          l->stream));
+  DH_CUDA(cudaStreamSynchronize(l->stream));
+  l->writer.start({join_path(l->disk_dir, "vector.0")}, l->dim, std::string(), l->algorithm, LanczosDiskState());
+  return DH_OK;
 }
 
 int lz_run(dh_lanczos_s* l, int nbr_iter) {
@@ -175,15 +299,19 @@ int lz_run(dh_lanczos_s* l, int nbr_iter) {
     l->index = 0;
     l->rows = 2;
   } else {
-    target = l->rows + nbr_iter;
+    // a state resumed from the middle of a call first completes that call's rows
+    target = l->rows + l->pending + nbr_iter;
     DH_CHECK(target <= l->cap, DH_ERR_ARGUMENT, "more Lanczos rows (%d) than max_iter allows (%d)", target, l->cap);
   }
+  l->pending = 0;
   while (l->rows < target) {
     if ((rc = lz_iteration(l, l->index + 1)) != DH_OK) return rc;
     ++l->index;
     ++l->rows;
   }
-  return lz_finish_call(l);
+  if ((rc = lz_finish_call(l)) != DH_OK) return rc;
+  if (l->disk && l->rows - l->disk_rows >= l->disk_interval) return lz_checkpoint(l);
+  return DH_OK;
 }
 
 // Ritz vector of the lowest Ritz value: from the Krylov store when kept, otherwise by replaying the
@@ -199,12 +327,14 @@ int lz_ground_state(dh_lanczos_s* l) {
   if ((rc = ensure_buffer(l->ground, l->dim * sizeof(double))) != DH_OK) return rc;
   if ((rc = ensure_buffer(l->coef, (size_t)std::max(n, l->cap + 8) * sizeof(double))) != DH_OK) return rc;
   double* g = l->ground.as<double>();
-  if (l->st.krylov && n <= l->krylov_cap) {
+  if (l->st.krylov && l->krylov_valid && n <= l->krylov_cap) {
     DH_CUDA(cudaMemcpyAsync(l->coef.ptr, c.data(), n * sizeof(double), cudaMemcpyHostToDevice, l->stream));
     if ((rc = launch_combine(l->st.krylov, n, l->dim, l->coef.as<double>(), 1.0, g, 0, l->dim, l->stream)) != DH_OK)
       return rc;
   } else {
     // replay: v_0 = start vector, v_{j+1} = (H v_j - alpha_j v_j - beta_{j-1} v_{j-1}) / |.|
+    DH_CHECK(l->start_known, DH_ERR_STATE,
+             "the start vector is unknown (a state resumed from the basic disk format does not store it)");
     double* v[3] = {l->st.vec, l->st.vec + l->dim, l->st.vec + 2 * l->dim};
     DH_CUDA(cudaMemcpyAsync(v[0], l->initial.ptr, l->dim * sizeof(double), cudaMemcpyDeviceToDevice, l->stream));
     DH_CUDA(cudaMemsetAsync(g, 0, l->dim * sizeof(double), l->stream));
@@ -252,7 +382,12 @@ int lz_initialize_device(dh_lanczos_s* l) {
   l->prev_last = 0.0;
   std::fill(l->prev_wanted.begin(), l->prev_wanted.end(), 0.0);
   l->ritz.clear();
-  return DH_OK;
+  l->pending = 0;
+  l->resumed = false;
+  l->start_known = true;
+  l->krylov_valid = true;
+  l->disk_rows = -1;
+  return lz_write_start_vector(l);
 }
 
 // Three consecutive iterations (phases 0, 1, 2) captured once as a CUDA graph; the device cursor
@@ -458,8 +593,8 @@ int dh_lanczos_get_eigenstates(dh_lanczos_t l, int n, double* vecs) {
   if (l->blk) return block_lanczos_eigenstates(l->blk, n, vecs);
   DH_CHECK(n >= 1 && n <= l->rows, DH_ERR_ARGUMENT, "%d eigenstates asked of %d Lanczos rows", n, l->rows);
   if (n == 1) return dh_lanczos_get_ground_state(l, vecs);
-  DH_CHECK(l->st.krylov && l->rows <= l->krylov_cap, DH_ERR_UNSUPPORTED,
-           "more than one eigenstate needs the stored Krylov vectors");
+  DH_CHECK(l->st.krylov && l->krylov_valid && l->rows <= l->krylov_cap, DH_ERR_UNSUPPORTED,
+           "more than one eigenstate needs the stored Krylov vectors (of a run that was not resumed)");
   const int m = l->rows;
   std::vector<double> eig(m), z((size_t)m * m);
   int rc = tridiagonal_eigen(m, l->alpha.data(), l->beta.data(), eig.data(), z.data());
@@ -504,11 +639,18 @@ int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eige
   DH_CHECK(l->initialized, DH_ERR_STATE, "solve before InitializeLanczosAlgorithm");
   if (max_iter > l->max_iter) max_iter = l->max_iter;
   int rc;
-  // QHEOnSphereMainTask.cc:732-753: RunLanczosAlgorithm(nev + 2), counter = nev + 3
-  if ((rc = lz_run(l, l->nev + 2)) != DH_OK) return rc;
-  int count = l->nev + 3;
-  // the start-vector projection indexes its norm from the host: no graph batches with it
-  const bool use_graph = graph_batch > 1 && l->algorithm != DH_LANCZOS_FULL_REORTHOGONALIZED && !l->lock_v0;
+  // QHEOnSphereMainTask.cc:732-753: RunLanczosAlgorithm(nev + 2), counter = nev + 3; a resumed run
+  // (--resume, :730) skips that call and counts from 0
+  int count = 0;
+  if (!l->resumed) {
+    if ((rc = lz_run(l, l->nev + 2)) != DH_OK) return rc;
+    count = l->nev + 3;
+  }
+  l->resumed = false;
+  // the start-vector projection indexes its norm from the host, and checkpoints need the state of
+  // every call on the device: no graph batches with either
+  const bool use_graph =
+      graph_batch > 1 && l->algorithm != DH_LANCZOS_FULL_REORTHOGONALIZED && !l->lock_v0 && !l->disk;
   while (!lz_converged(l) && count < max_iter) {
     if (!use_graph) {
       ++count;
@@ -567,9 +709,103 @@ int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eige
       l->initialized = false;
     }
   }
+  if (l->disk) {
+    // the final state is on disk when the solve returns
+    if (l->rows != l->disk_rows && (rc = lz_checkpoint(l)) != DH_OK) return rc;
+    if ((rc = l->writer.wait()) != DH_OK) return rc;
+  }
   *iterations = count;
   *converged = lz_converged(l) ? 1 : 0;
   for (int i = 0; i < l->nev && i < (int)l->ritz.size(); ++i) eigenvalues[i] = l->ritz[i];
+  return DH_OK;
+}
+
+int dh_lanczos_set_disk_storage(dh_lanczos_t l, const char* directory, int interval) {
+  DH_CHECK(l, DH_ERR_ARGUMENT, "null lanczos");
+  DH_CHECK(!l->blk && (l->algorithm == DH_LANCZOS_BASIC || l->algorithm == DH_LANCZOS_WITH_GROUND_STATE),
+           DH_ERR_UNSUPPORTED, "disk storage is implemented for the basic and with-ground-state algorithms");
+  int rc = l->writer.wait();
+  if (rc != DH_OK) return rc;
+  if (!directory) {
+    l->disk = false;
+    l->disk_dir.clear();
+    return DH_OK;
+  }
+  DH_CHECK(interval >= 1, DH_ERR_ARGUMENT, "checkpoint interval must be >= 1");
+  l->disk = true;
+  l->disk_dir = directory;
+  l->disk_interval = interval;
+  l->disk_rows = -1;
+  // a start vector set before disk storage was switched on
+  if (l->initialized && l->start_known && l->rows == 0) return lz_write_start_vector(l);
+  return DH_OK;
+}
+
+int dh_lanczos_write_state(dh_lanczos_t l) {
+  DH_CHECK(l, DH_ERR_ARGUMENT, "null lanczos");
+  DH_CHECK(l->disk, DH_ERR_STATE, "WriteState needs disk storage (dh_lanczos_set_disk_storage)");
+  int rc = lz_checkpoint(l);
+  if (rc != DH_OK) return rc;
+  return l->writer.wait();
+}
+
+int dh_lanczos_resume(dh_lanczos_t l) {
+  DH_CHECK(l, DH_ERR_ARGUMENT, "null lanczos");
+  DH_CHECK(l->disk, DH_ERR_STATE, "ResumeLanczosAlgorithm needs disk storage (dh_lanczos_set_disk_storage)");
+  int rc = l->writer.wait();
+  if (rc != DH_OK) return rc;
+  LanczosDiskState s;
+  if ((rc = lanczos_state_read(join_path(l->disk_dir, "lanczos.dat"), l->algorithm, &s)) != DH_OK) return rc;
+  const bool ground = l->algorithm == DH_LANCZOS_WITH_GROUND_STATE;
+  // GroundStateEvaluationFlag 1: the run had finished and its ground state was being assembled
+  // (Index then counts assembly steps); every row of the matrix is valid
+  const bool finished = ground && s.ground_flag == 1;
+  const int rows = finished ? s.nbr_row : s.index + 2;
+  DH_CHECK(rows + (finished ? 0 : 1) <= l->cap, DH_ERR_ARGUMENT,
+           "the stored state has %d rows; this handle holds %d (max_iter + 2)", rows, l->cap);
+  const int64_t dim = l->dim;
+  if ((rc = l->writer.reserve((size_t)4 * dim)) != DH_OK) return rc;
+  double* host = l->writer.staging;
+  if (!finished) {
+    for (int q = 0; q < 3; ++q) {
+      char name[16];
+      if (ground) snprintf(name, sizeof(name), "vector.%d", q + 1);
+      const std::string path = join_path(l->disk_dir, ground ? name : s.names[q]);
+      if ((rc = vector_file_read(path, host + (size_t)q * dim, dim)) != DH_OK) return rc;
+    }
+  }
+  if (ground && (rc = vector_file_read(join_path(l->disk_dir, "vector.0"), host + (size_t)3 * dim, dim)) != DH_OK)
+    return rc;
+  std::vector<double> eig(rows);
+  if ((rc = tridiagonal_eigen(rows, s.diag.data(), s.upper.data(), eig.data(), nullptr)) != DH_OK) return rc;
+  // the device state: the three vectors in their slots, the scalars, the iteration cursor
+  if (!finished)
+    for (int q = 0; q < 3; ++q)
+      DH_CUDA(cudaMemcpyAsync(l->st.vec + (size_t)((s.index + q) % 3) * dim, host + (size_t)q * dim,
+                              dim * sizeof(double), cudaMemcpyHostToDevice, l->stream));
+  if (ground)
+    DH_CUDA(cudaMemcpyAsync(l->initial.ptr, host + (size_t)3 * dim, dim * sizeof(double), cudaMemcpyHostToDevice,
+                            l->stream));
+  DH_CUDA(cudaMemcpyAsync(l->st.alpha, s.diag.data(), rows * sizeof(double), cudaMemcpyHostToDevice, l->stream));
+  DH_CUDA(cudaMemcpyAsync(l->st.beta, s.upper.data(), (rows - 1) * sizeof(double), cudaMemcpyHostToDevice, l->stream));
+  const int cursor = rows - 1;
+  DH_CUDA(cudaMemcpyAsync(l->st.cursor, &cursor, sizeof(int), cudaMemcpyHostToDevice, l->stream));
+  DH_CUDA(cudaStreamSynchronize(l->stream));
+  l->alpha.assign(s.diag.begin(), s.diag.begin() + rows);
+  l->beta.assign(s.upper.begin(), s.upper.begin() + (rows - 1));
+  l->index = rows - 2;
+  l->rows = rows;
+  l->prev_last = s.prev_last;
+  l->precision = s.precision;
+  l->ritz.swap(eig);
+  l->pending = finished ? 0 : s.nbr_row - rows;
+  l->resumed = !finished;
+  l->initialized = !finished;
+  l->ground_valid = false;
+  l->start_known = ground;
+  l->krylov_valid = false;
+  l->disk_rows = rows;
+  l->disk_set = (!ground && s.names[0][6] >= '4') ? 1 : 0;
   return DH_OK;
 }
 
@@ -578,6 +814,7 @@ int dh_lanczos_solve_refined(dh_lanczos_t l, int max_iter, double precision, dou
   DH_CHECK(precision > 0.0, DH_ERR_ARGUMENT, "precision must be > 0");
   if (l->blk) return block_lanczos_solve_refined(l->blk, max_iter, precision, out);
   DH_CHECK(l->initialized, DH_ERR_STATE, "solve before InitializeLanczosAlgorithm");
+  DH_CHECK(!l->disk, DH_ERR_UNSUPPORTED, "the refined solve restarts its Lanczos runs: switch disk storage off");
   dh_hamiltonian_s* h = l->h;
   const int saved_precision = h->precision;
   const double saved_lz_precision = l->precision;

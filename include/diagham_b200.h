@@ -31,6 +31,7 @@ extern "C" {
 #define DH_ERR_UNSUPPORTED -4
 #define DH_ERR_NOT_CONVERGED -5
 #define DH_ERR_STATE -6
+#define DH_ERR_IO -7 /* a file could not be read or written, or does not hold what its format says */
 
 /* index search modes of the target-index lookup inside the matvec kernels */
 #define DH_INDEX_RANK 0   /* two-table combinatorial rank (default) */
@@ -299,6 +300,57 @@ int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eige
  * whole block of Ritz vectors is refined and the FP64 restart is a block Lanczos from it; the
  * algorithm must be freshly initialised. */
 int dh_lanczos_solve_refined(dh_lanczos_t l, int max_iter, double precision, double* out);
+
+/* Disk storage of the Lanczos state, in the files of the reference's disk-storage classes, so that an
+ * interrupted run resumes (here or in the reference) where it stopped:
+ *   DH_LANCZOS_BASIC             BasicLanczosAlgorithmWithDiskStorage (src/LanczosAlgorithm/
+ *                                BasicLanczosAlgorithmWithDiskStorage.cc:286-335): lanczos.dat and three
+ *                                vector files v_Index, v_Index+1, H v_Index+1 named in it;
+ *   DH_LANCZOS_WITH_GROUND_STATE BasicLanczosAlgorithmWithGroundStateDiskStorage (...WithGroundState
+ *                                DiskStorage.cc:399-453): lanczos.dat, vector.0 (the start vector,
+ *                                written by dh_lanczos_initialize*) and vector.1-3 (the same three).
+ * The files live in `directory` (the reference uses the working directory).  A checkpoint is written
+ * at the end of every RunLanczosAlgorithm call that has added `interval` (>= 1) or more rows since the
+ * last one, and at the end of dh_lanczos_solve; interval 1 is the reference's behaviour.  The vectors
+ * are copied to pinned host memory on the handle's stream and written by a background thread while
+ * the next iterations run; each file goes to a temporary name and is renamed into place, lanczos.dat
+ * last.  The basic format alternates between the names vector1-3 and vector4-6 (lanczos.dat names
+ * them), so the previous checkpoint stays whole until the new lanczos.dat replaces it.  directory =
+ * NULL switches disk storage off.  Other algorithms: DH_ERR_UNSUPPORTED.  Solves with disk storage
+ * run without CUDA-graph batches; dh_lanczos_solve_refined rejects it. */
+int dh_lanczos_set_disk_storage(dh_lanczos_t l, const char* directory, int interval);
+
+/* WriteState: a checkpoint of the current state now; returns once every file is written. */
+int dh_lanczos_write_state(dh_lanczos_t l);
+
+/* ResumeLanczosAlgorithm (BasicLanczosAlgorithmWithDiskStorage.cc:161,
+ * BasicLanczosAlgorithmWithGroundStateDiskStorage.cc:175): the state in the disk-storage directory
+ * replaces dh_lanczos_initialize*.  EigenvaluePrecision and PreviousLastWantedEigenvalue come from the
+ * file.  A state written in the middle of a reference RunLanczosAlgorithm call (NbrRow above Index +
+ * 2) owes its remaining rows to the next run call, which adds them before its own, as the reference
+ * does.  dh_lanczos_solve after a resume continues the driver loop without its first call and counts
+ * iterations from 0 (QHEOnSphereMainTask.cc:730-736 with --resume).  A ground-state-format state
+ * written during the reference's ground-state evaluation (GroundStateEvaluationFlag 1) holds a
+ * finished run: it resumes for dh_lanczos_get_ground_state only (rebuilt from vector.0 and the
+ * tridiagonal matrix).  The basic format does not store the start vector, so its resumed runs give
+ * eigenvalues but no ground state. */
+int dh_lanczos_resume(dh_lanczos_t l);
+
+/* ================================================================ vector files */
+
+/* RealVector::WriteVector (src/Vector/RealVector.cc:3669): little-endian int32 dimension (int32 -1
+ * and an int64 dimension from 2^31 on), then the components as little-endian doubles.  vec is a host
+ * or device pointer; the file is written under a temporary name and renamed into place.  Eigenstate
+ * files are named <prefix>.<index>.vec, prefix = statistics_interaction_n_N_2s_2S_lz_2Lz
+ * (FQHE/docs/DataFormat/FermionOnSphere.xml:9-16, QHEOnSphereMainTask.cc:891). */
+int dh_vector_write(const char* file_name, const double* vec, int64_t dim);
+
+/* The dimension of the vector stored in file_name (RealVector::ReadVector's header). */
+int dh_vector_file_dimension(const char* file_name, int64_t* dim);
+
+/* RealVector::ReadVector (src/Vector/RealVector.cc:3798) into vec (host or device) of dim doubles:
+ * the stored dimension must be dim and the file length must match it exactly (DH_ERR_IO otherwise). */
+int dh_vector_read(const char* file_name, double* vec, int64_t dim);
 
 /* ================================================================ batched sectors */
 

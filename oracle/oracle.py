@@ -324,3 +324,50 @@ def l2_raise(n, two_s, total_lz, x):
                 lam = 0.5 * np.sqrt(two_s * (two_s + 2) - (2 * m - two_s) * (2 * m - two_s + 2))
                 y[index[w ^ (3 << m)]] += lam * x[i]
     return y
+
+
+def read_vector_bytes(b):
+    """A vector file's bytes (RealVector::WriteVector, src/Vector/RealVector.cc:3669): int32
+    dimension, or int32 -1 and an int64 dimension, then little-endian doubles."""
+    d = int(np.frombuffer(b[:4], "<i4")[0])
+    off = 4
+    if d <= 0 and len(b) > 4:
+        d = int(np.frombuffer(b[4:12], "<i8")[0])
+        off = 12
+    assert len(b) == off + 8 * d, (len(b), d)
+    return np.frombuffer(b[off:], "<f8").copy()
+
+
+def read_lanczos_state(b, fmt):
+    """lanczos.dat bytes of the reference's disk-storage Lanczos classes.
+    fmt "basic": BasicLanczosAlgorithmWithDiskStorage::WriteState (BasicLanczosAlgorithmWithDiskStorage.cc:
+    286-308): int32 Index, f64 PreviousLastWantedEigenvalue, f64 EigenvaluePrecision, int32 NbrRow, three
+    NUL-terminated vector file names, Index+2 diagonal then Index+1 upper-diagonal elements.
+    fmt "ground": BasicLanczosAlgorithmWithGroundStateDiskStorage::WriteState (...GroundStateDiskStorage.cc:
+    399-423): int32 Index, int32 GroundStateEvaluationFlag, f64 PreviousLastWantedEigenvalue, f64
+    EigenvaluePrecision, int32 NbrEigenvalue, int32 NbrRow, NbrRow diagonal then NbrRow-1 upper-diagonal
+    elements."""
+    b = bytes(b)
+    if fmt == "basic":
+        index = int(np.frombuffer(b[0:4], "<i4")[0])
+        prev, prec = np.frombuffer(b[4:20], "<f8")
+        nbr_row = int(np.frombuffer(b[20:24], "<i4")[0])
+        names, o = [], 24
+        for _ in range(3):
+            e = b.index(b"\0", o)
+            names.append(b[o:e].decode())
+            o = e + 1
+        rows = index + 2
+        diag = np.frombuffer(b[o:o + 8 * rows], "<f8").copy()
+        upper = np.frombuffer(b[o + 8 * rows:o + 8 * (2 * rows - 1)], "<f8").copy()
+        assert len(b) == o + 8 * (2 * rows - 1)
+        return dict(index=index, prev_last=float(prev), precision=float(prec), nbr_row=nbr_row, names=names,
+                    diag=diag, upper=upper, ground_flag=0)
+    index, flag = (int(x) for x in np.frombuffer(b[0:8], "<i4"))
+    prev, prec = np.frombuffer(b[8:24], "<f8")
+    nev, nbr_row = (int(x) for x in np.frombuffer(b[24:32], "<i4"))
+    diag = np.frombuffer(b[32:32 + 8 * nbr_row], "<f8").copy()
+    upper = np.frombuffer(b[32 + 8 * nbr_row:], "<f8").copy()
+    assert upper.size == nbr_row - 1
+    return dict(index=index, ground_flag=flag, prev_last=float(prev), precision=float(prec), nbr_eigenvalue=nev,
+                nbr_row=nbr_row, diag=diag, upper=upper)

@@ -11,6 +11,7 @@
 //   AbstractQHEOnSphereHamiltonian::LowLevelAddMultiply   .../AbstractQHEOnSphereHamiltonian.cc:410
 //   Spin1_2Chain                         Spin/src/HilbertSpace/Spin1_2Chain.cc:113
 //   BasicLanczosAlgorithm / FullReorthogonalizedLanczosAlgorithm / BasicBlockLanczosAlgorithm
+//   BasicLanczosAlgorithmWithDiskStorage / BasicLanczosAlgorithmWithGroundStateDiskStorage
 //   EvaluatePseudopotentials             FQHE/src/Tools/FQHESpectrum/PseudoPotentials.cc:35
 //   VectorHamiltonianMultiplyOperation on SMPArchitecture (the reference SMP path)
 //
@@ -36,6 +37,8 @@
 #include "LanczosAlgorithm/FullReorthogonalizedLanczosAlgorithm.h"
 #include "LanczosAlgorithm/BasicBlockLanczosAlgorithm.h"
 #include "LanczosAlgorithm/BasicLanczosAlgorithmWithGroundState.h"
+#include "LanczosAlgorithm/BasicLanczosAlgorithmWithDiskStorage.h"
+#include "LanczosAlgorithm/BasicLanczosAlgorithmWithGroundStateDiskStorage.h"
 #include "Matrix/RealTriDiagonalSymmetricMatrix.h"
 #include "Tools/FQHESpectrum/PseudoPotentials.h"
 #include "Vector/RealVector.h"
@@ -47,7 +50,9 @@
 #include <cmath>
 #include <vector>
 #include <sys/time.h>
+#include <unistd.h>
 #include <iostream>
+#include <string>
 
 using std::cout;
 using std::endl;
@@ -297,6 +302,119 @@ static void RunLanczosLoop(AbstractHamiltonian* H, AbstractArchitecture* Arch, c
   delete Lanczos;
 }
 
+// the driver loop of QHEOnSphereMainTask.cc:671-753 with --disk: BasicLanczosAlgorithmWithDiskStorage
+// ("basic") or BasicLanczosAlgorithmWithGroundStateDiskStorage ("ground", ground-state assembly in
+// steps of groundIter) run in directory dir, which receives lanczos.dat and the vector files.  start
+// = "resume" resumes from dir (ResumeLanczosAlgorithm, no first call, counter from 0), otherwise it
+// is the start vector file.  nbrIter bounds the counter as --nbr-iter does in disk mode, so a small
+// value leaves an interrupted run on disk.  Output layout as RunLanczosLoop's.
+static void RunDiskLanczosLoop(AbstractHamiltonian* H, AbstractArchitecture* Arch, const char* algo, int nbrIter,
+			       double precision, const char* dir, const char* start, int groundIter,
+			       const char* outName, const char* groundStateName)
+{
+  AbstractLanczosAlgorithm* Lanczos;
+  bool Ground = (strcmp(algo, "ground") == 0);
+  // "block<k>": BasicBlockLanczosAlgorithm with --fast-disk (diskFlag), --resume-fastdisk for "resume"
+  int BlockSize = (strncmp(algo, "block", 5) == 0) ? atoi(algo + 5) : 0;
+  bool Resume = (strcmp(start, "resume") == 0);
+  if (Ground)
+    Lanczos = new BasicLanczosAlgorithmWithGroundStateDiskStorage(Arch, groundIter, 4000);
+  else if (BlockSize > 0)
+    Lanczos = new BasicBlockLanczosAlgorithm(Arch, 1, BlockSize, 4000, true, Resume, false, false);
+  else
+    Lanczos = new BasicLanczosAlgorithmWithDiskStorage(Arch, 1, 4000);
+  // start vectors: file names separated by commas (the block gets one per vector)
+  std::vector<RealVector> Initial;
+  if (!Resume)
+    {
+      std::string Names(start);
+      size_t Pos = 0;
+      while (Pos <= Names.size())
+	{
+	  size_t End = Names.find(',', Pos);
+	  if (End == std::string::npos)
+	    End = Names.size();
+	  RealVector V;
+	  V.ReadVector(Names.substr(Pos, End - Pos).c_str());
+	  Initial.push_back(V);
+	  Pos = End + 1;
+	}
+    }
+  // outputs are opened (or made absolute) before moving into dir
+  FILE* f = OpenOut(outName);
+  std::string GroundStatePath;
+  if (groundStateName != 0)
+    {
+      GroundStatePath = groundStateName;
+      if (groundStateName[0] != '/')
+	{
+	  char Cwd[4096];
+	  if (getcwd(Cwd, sizeof(Cwd)) == 0)
+	    exit(2);
+	  GroundStatePath = std::string(Cwd) + "/" + groundStateName;
+	}
+    }
+  if (chdir(dir) != 0)
+    {
+      fprintf(stderr, "cannot enter %s\n", dir);
+      exit(2);
+    }
+  if (precision != 0.0)
+    Lanczos->SetEigenvaluePrecision(precision);
+  Lanczos->SetHamiltonian(H);
+  int CurrentNbrIter = 0;
+  double t0 = Now();
+  if (BlockSize > 0)
+    {
+      // QHEOnSphereMainTask.cc:711-736 without --resume: the (resuming) initialisation, then the
+      // first call of nbrEigenvalue + 2 block steps
+      if (Resume)
+	Lanczos->InitializeLanczosAlgorithm();
+      else
+	Lanczos->InitializeLanczosAlgorithm(&Initial[0], (int) Initial.size());
+      Lanczos->RunLanczosAlgorithm(3);
+      CurrentNbrIter = 4 * BlockSize;
+    }
+  else if (Resume)
+    Lanczos->ResumeLanczosAlgorithm();
+  else
+    {
+      Lanczos->InitializeLanczosAlgorithm(Initial[0]);
+      Lanczos->RunLanczosAlgorithm(3);
+      CurrentNbrIter = 4;
+    }
+  std::vector<double> History;
+  while ((Lanczos->TestConvergence() == false) && (CurrentNbrIter < nbrIter))
+    {
+      CurrentNbrIter += (BlockSize > 0) ? BlockSize : 1;
+      Lanczos->RunLanczosAlgorithm(1);
+      RealTriDiagonalSymmetricMatrix TmpMatrix;
+      TmpMatrix.Copy(Lanczos->GetDiagonalizedMatrix());
+      TmpMatrix.SortMatrixUpOrder();
+      History.push_back(TmpMatrix.DiagonalElement(0));
+    }
+  double t1 = Now();
+  int Nev = 1;
+  int Converged = Lanczos->TestConvergence() ? 1 : 0;
+  fwrite(&Nev, sizeof(int), 1, f);
+  fwrite(&CurrentNbrIter, sizeof(int), 1, f);
+  fwrite(&Converged, sizeof(int), 1, f);
+  double Seconds = t1 - t0;
+  fwrite(&Seconds, sizeof(double), 1, f);
+  WriteEigenvalues(f, Lanczos, Nev);
+  int NbrHistory = (int) History.size();
+  fwrite(&NbrHistory, sizeof(int), 1, f);
+  if (NbrHistory > 0)
+    fwrite(&History[0], sizeof(double), NbrHistory, f);
+  fclose(f);
+  if (Ground && (groundStateName != 0))
+    {
+      RealVector& GS = (RealVector&) Lanczos->GetGroundState();
+      GS.WriteVector(GroundStatePath.c_str());
+    }
+  delete Lanczos;
+}
+
 // REF_THREADS=P (environment) runs the Lanczos commands on SMPArchitecture(P) instead of the
 // mono-processor architecture, as the reference programs do with -S --processors P
 static AbstractArchitecture* MakeArchitecture()
@@ -317,6 +435,7 @@ static void Usage()
 	  "  fqhe_rows N 2S 2Lz vfile rowsfile out\n"
 	  "  fqhe_matvec N 2S 2Lz vfile xfile shift out\n"
 	  "  fqhe_lanczos N 2S 2Lz vfile algo nev block maxiter precision out gsout x0 [x1 ...]\n"
+	  "  fqhe_lanczos_disk N 2S 2Lz vfile algo nbriter precision dir x0|resume gsiter out gsout\n"
 	  "  fqhe_expect N 2S 2Lz vfile psifile out\n"
 	  "  fqhe_l2 N 2S 2Lz xfile out\n"
 	  "  pseudopotentials 2S out\n"
@@ -475,6 +594,18 @@ int main(int argc, char** argv)
 	Init[i].ReadVector(argv[13 + i]);
       RunLanczosLoop(&H, Arch, Algo, Nev, Block, MaxIter, Precision, Init, NbrInitial, argv[11],
 		     strcmp(argv[12], "-") == 0 ? 0 : argv[12]);
+      return 0;
+    }
+  if (strcmp(Cmd, "fqhe_lanczos_disk") == 0 && argc == 14)
+    {
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      double* V = ReadDoubles(argv[5], LzMax + 1);
+      FermionOnSphere Space(N, TotalLz, LzMax, 9ul << 20);
+      AbstractArchitecture* Arch = MakeArchitecture();
+      Arch->SetDimension(Space.GetHilbertSpaceDimension());
+      ParticleOnSphereGenericHamiltonian H(&Space, N, LzMax, V, 0.0, Arch, 0, false, 0, false);
+      RunDiskLanczosLoop(&H, Arch, argv[6], atoi(argv[7]), atof(argv[8]), argv[9], argv[10], atoi(argv[11]),
+			 argv[12], strcmp(argv[13], "-") == 0 ? 0 : argv[13]);
       return 0;
     }
   if (strcmp(Cmd, "fqhe_expect") == 0 && argc == 8)

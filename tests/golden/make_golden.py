@@ -301,6 +301,58 @@ def l2_fixtures(tmp):
         save("l2_n%d_2s%d_lz%d.npz" % (n, s, lz), cmd, seed=7, y=read_vector(yf))
 
 
+def dir_files(d):
+    names = sorted(os.listdir(d))
+    return np.array(names), {"f%d" % i: np.frombuffer(open(os.path.join(d, f), "rb").read(), np.uint8)
+                             for i, f in enumerate(names)}
+
+
+def disk_fixtures(tmp):
+    # The disk-storage Lanczos classes (BasicLanczosAlgorithmWithDiskStorage = "basic",
+    # BasicLanczosAlgorithmWithGroundStateDiskStorage = "ground") on N=7 2S=18 2Lz=2, odd Coulomb
+    # pseudopotentials, start = splitmix64 vector of seed 0, precision MACHINE_PRECISION:
+    #   interrupted_*  the files of the run stopped at counter 14 (file names in interrupted_names,
+    #                  contents as raw bytes in interrupted_f<i>)
+    #   resumed        the driver loop resumed from those files (counter from 0)
+    #   full           the uninterrupted run (and its ground state psi for "ground")
+    #   assembly_*     ("ground") the files after the resumed run assembled its ground state for 5
+    #                  steps only (GroundStateEvaluationFlag 1)
+    import shutil
+    n, s, lz, stop = 7, 18, 2, 14
+    v = coulomb_odd(s, tmp)
+    vf = os.path.join(tmp, "vv.bin")
+    v.tofile(vf)
+    bf = os.path.join(tmp, "b.bin")
+    run("fqhe_basis", n, s, lz, bf)
+    dim, _, _ = read_basis(bf)
+    xf = os.path.join(tmp, "x0.vec")
+    write_vector(xf, splitmix_vector(0, dim))
+    lf = os.path.join(tmp, "l.out")
+    for algo in ("basic", "ground"):
+        d_full, d_int, d_res = (os.path.join(tmp, "%s_%s" % (algo, k)) for k in ("full", "int", "res"))
+        for d in (d_full, d_int):
+            os.makedirs(d)
+        gf = os.path.join(tmp, "gs_full.vec")
+        cmd = run("fqhe_lanczos_disk", n, s, lz, vf, algo, 400, 0, d_full, xf, 100000, lf,
+                  gf if algo == "ground" else "-")
+        full = read_lanczos(lf)
+        cmd_int = run("fqhe_lanczos_disk", n, s, lz, vf, algo, stop, 0, d_int, xf, 100000, lf, "-")
+        int_names, int_files = dir_files(d_int)
+        shutil.copytree(d_int, d_res)
+        cmd_res = run("fqhe_lanczos_disk", n, s, lz, vf, algo, 400, 0, d_res, "resume", 100000, lf, "-")
+        res = read_lanczos(lf)
+        extra = {}
+        if algo == "ground":
+            run("fqhe_lanczos_disk", n, s, lz, vf, algo, 400, 0, d_res, "resume", 5, lf, os.path.join(tmp, "gs5.vec"))
+            a_names, a_files = dir_files(d_res)
+            extra = dict(psi=read_vector(gf), assembly_names=a_names,
+                         **{"assembly_" + k: b for k, b in a_files.items()})
+        save("disk_%s_n%d_2s%d_lz%d.npz" % (algo, n, s, lz), "; ".join([cmd, cmd_int, cmd_res]), v=v, seed=0, stop=stop,
+             full_iterations=full["iterations"], full_eigenvalue=full["eigenvalues"][0],
+             resumed_iterations=res["iterations"], resumed_eigenvalue=res["eigenvalues"][0],
+             interrupted_names=int_names, **{"interrupted_" + k: b for k, b in int_files.items()}, **extra)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--slow", action="store_true")
@@ -329,6 +381,8 @@ def main():
             gradient_fixtures(tmp)
         if args.only in (None, "l2"):
             l2_fixtures(tmp)
+        if args.only in (None, "disk"):
+            disk_fixtures(tmp)
         if args.slow:
             slow_fixtures(tmp)
 

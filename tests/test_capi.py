@@ -57,3 +57,54 @@ def test_errors_are_codes_not_aborts(dh):
         dh.Spin1_2Chain(40, 0)
     msg = dh.load().dh_last_error().decode()
     assert "chain length" in msg
+
+
+def test_vector_files_match_the_reference_bytes(dh, orc, tmp_path):
+    # RealVector::WriteVector / ReadVector: the reference's files read back exactly, and the same
+    # components written by the library give the same bytes
+    z = golden("disk_ground_n7_2s18_lz2.npz")
+    for i, name in enumerate(z["interrupted_names"]):
+        if not str(name).startswith("vector"):
+            continue
+        ref = bytes(z["interrupted_f%d" % i])
+        p = tmp_path / str(name)
+        p.write_bytes(ref)
+        assert dh.vector_file_dimension(str(p)) == 1646
+        x = dh.ReadVector(str(p))
+        assert np.array_equal(x, orc.read_vector_bytes(ref))
+        q = tmp_path / ("copy_" + str(name))
+        dh.WriteVector(x, str(q))
+        assert q.read_bytes() == ref
+        assert not (tmp_path / ("copy_" + str(name) + ".tmp")).exists()
+
+
+def test_vector_file_forms_and_errors(dh, tmp_path):
+    x = np.random.default_rng(3).standard_normal(37)
+    # the int64 form (int32 -1, then the dimension) that the reference writes from 2^31 on
+    p = tmp_path / "large_form.vec"
+    p.write_bytes(np.int32(-1).tobytes() + np.int64(37).tobytes() + x.tobytes())
+    assert dh.vector_file_dimension(str(p)) == 37
+    assert np.array_equal(dh.ReadVector(str(p)), x)
+    # empty vector
+    e = tmp_path / "empty.vec"
+    dh.WriteVector(np.zeros(0), str(e))
+    assert e.read_bytes() == np.int32(0).tobytes() and dh.ReadVector(str(e)).size == 0
+    # missing, truncated, too long, wrong dimension for the buffer
+    with pytest.raises(dh.DiagHamError, match="error -7"):
+        dh.ReadVector(str(tmp_path / "missing.vec"))
+    t = tmp_path / "truncated.vec"
+    t.write_bytes(np.int32(37).tobytes() + x[:30].tobytes())
+    with pytest.raises(dh.DiagHamError, match="do not hold"):
+        dh.ReadVector(str(t))
+    t.write_bytes(np.int32(37).tobytes() + np.concatenate([x, x[:1]]).tobytes())
+    with pytest.raises(dh.DiagHamError, match="do not hold"):
+        dh.ReadVector(str(t))
+    with pytest.raises(dh.DiagHamError, match="expected 36"):
+        dh.ReadVector(str(p), out=np.zeros(36))
+    with pytest.raises(dh.DiagHamError, match="error -7"):
+        dh.WriteVector(x, str(tmp_path / "no_such_dir" / "x.vec"))
+
+
+def test_eigenstate_file_name(dh):
+    # FQHE/docs/DataFormat/FermionOnSphere.xml:9-16; QHEOnSphereMainTask.cc:891
+    assert dh.eigenstate_file_name("fermions", "coulomb", 8, 21, 0, 0) == "fermions_coulomb_n_8_2s_21_lz_0.0.vec"

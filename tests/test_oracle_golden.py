@@ -189,3 +189,40 @@ def test_l2_table_matches_reference(orc, tag):
     if O.dim < 2000:
         up = orc.l2_raise(n, s, lz, x)
         assert abs(float(x @ y) - (float(up @ up) + c)) <= 1e-12 * abs(float(x @ y))
+
+
+def disk_files(z, prefix):
+    return {str(n): bytes(z["%s_f%d" % (prefix, i)]) for i, n in enumerate(z["%s_names" % prefix])}
+
+
+@pytest.mark.parametrize("fmt", ["basic", "ground"])
+def test_disk_state_files_of_the_reference(orc, fmt):
+    # what the reference's disk-storage classes leave on disk after 14 iterations, read with the
+    # oracle's parsers: V1 = v_Index, V2 = v_Index+1 (normalised), V3 = H V2, the last tridiagonal
+    # elements are <V1|V3> and <V2|V3>, the first is <v0|H|v0>; the ground-state format also
+    # stores the start vector as vector.0
+    z = golden("disk_%s_n7_2s18_lz2.npz" % fmt)
+    files = disk_files(z, "interrupted")
+    st = orc.read_lanczos_state(files["lanczos.dat"], fmt)
+    O = orc.FQHE(7, 18, 2, z["v"])
+    names = st["names"] if fmt == "basic" else ["vector.1", "vector.2", "vector.3"]
+    v1, v2, v3 = (orc.read_vector_bytes(files[n]) for n in names)
+    i = st["index"]
+    assert i == int(z["stop"]) - 3 and st["nbr_row"] == i + 2 and st["precision"] == 1e-14
+    assert abs(v1 @ v1 - 1) < 1e-13 and abs(v2 @ v2 - 1) < 1e-13
+    hv2 = O.pull(v2)
+    assert np.max(np.abs(v3 - hv2)) <= 1e-13 * np.max(np.abs(hv2))
+    assert abs(st["upper"][i] - v1 @ v3) < 1e-12 and abs(st["diag"][i + 1] - v2 @ v3) < 1e-12
+    x0 = orc.random_vector(int(z["seed"]), O.dim)
+    assert abs(st["diag"][0] - x0 @ O.pull(x0)) < 1e-12
+    if fmt == "ground":
+        assert st["ground_flag"] == 0 and st["nbr_eigenvalue"] == 1
+        assert np.max(np.abs(orc.read_vector_bytes(files["vector.0"]) - x0)) < 1e-15
+        # the state left by an interrupted ground-state assembly: flag 1 and the finished run's matrix
+        a = orc.read_lanczos_state(disk_files(z, "assembly")["lanczos.dat"], fmt)
+        assert a["ground_flag"] == 1
+        e = orc.tridiagonal_eigenvalues(a["diag"], a["upper"])
+        assert abs(e.min() - float(z["full_eigenvalue"])) < 1e-13 * abs(float(z["full_eigenvalue"]))
+    # the resumed reference run ends where the uninterrupted one does
+    assert int(z["resumed_iterations"]) + int(z["stop"]) == int(z["full_iterations"])
+    assert float(z["resumed_eigenvalue"]) == float(z["full_eigenvalue"])
