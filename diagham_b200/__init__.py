@@ -4,6 +4,7 @@ Python view of the C ABI in include/diagham_b200.h (libdiagham_b200.so, built in
 diagham_b200/_build.py).  Class and method names follow the reference classes they replace:
 
     FermionOnSphere                     FQHE/src/HilbertSpace/FermionOnSphere.h
+    BosonOnSphereShort                  FQHE/src/HilbertSpace/BosonOnSphereShort.h
     Spin1_2Chain                        Spin/src/HilbertSpace/Spin1_2Chain.h
     ParticleOnSphereGenericHamiltonian  FQHE/src/Hamiltonian/ParticleOnSphereGenericHamiltonian.h
     SpinChainJ1J2Hamiltonian            (J1-J2 pattern of SpinChainJ1J2RealHamiltonianWithTranslations on a plain chain)
@@ -42,6 +43,7 @@ SIGNATURES = {
     "dh_version": ([], ctypes.c_char_p),
     "dh_device_count": ([_ip], _c_int),
     "dh_fermion_on_sphere_create": ([_c_int, _c_int, _c_int, ctypes.c_ulong, _vp], _c_int),
+    "dh_boson_on_sphere_create": ([_c_int, _c_int, _c_int, ctypes.c_ulong, _vp], _c_int),
     "dh_spin12_chain_create": ([_c_int, _c_int, _c_int, _vp], _c_int),
     "dh_space_destroy": ([_vp], _c_int),
     "dh_space_get_dimension": ([_vp, _i64p], _c_int),
@@ -215,6 +217,34 @@ class FermionOnSphere(_Space):
         _check(_lib.dh_fermion_on_sphere_create(nbr_fermions, total_lz, lz_max, memory, ctypes.byref(h)))
         self._handle = h
         self.nbr_fermions, self.total_lz, self.lz_max = nbr_fermions, total_lz, lz_max
+
+
+class BosonOnSphereShort(_Space):
+    """BosonOnSphereShort(nbrBosons, totalLz, lzMax): BosonOnSphereShort.cc:81.  states() and
+    FindStateIndex use the FermionOnSphere words of the occupations (n_0 ones, a zero, n_1 ones, ...)."""
+
+    def __init__(self, nbr_bosons, total_lz, lz_max, memory=0):
+        load()
+        h = ctypes.c_void_p()
+        _check(_lib.dh_boson_on_sphere_create(nbr_bosons, total_lz, lz_max, memory, ctypes.byref(h)))
+        self._handle = h
+        self.nbr_bosons, self.total_lz, self.lz_max = nbr_bosons, total_lz, lz_max
+
+    def occupations(self, words):
+        """Occupations n_0..n_lzmax of each word (rows of an (n, lz_max + 1) array)."""
+        words = np.asarray(words, np.uint64)
+        out = np.zeros((words.size, self.lz_max + 1), np.int32)
+        for i, w in enumerate(words):
+            w, m = int(w), 0
+            while m <= self.lz_max:
+                c = 0
+                while w & 1:
+                    c += 1
+                    w >>= 1
+                out[i, m] = c
+                w >>= 1
+                m += 1
+        return out
 
 
 class Spin1_2Chain(_Space):

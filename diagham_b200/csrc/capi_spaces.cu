@@ -170,6 +170,8 @@ FqheDevice fqhe_device(const dh_space_s* sp, const dh_hamiltonian_s* h, int prec
   f.lookup_bits = sp->lookup_bits;
   f.index_mode = sp->index_mode;
   f.kernel_variant = sp->kernel_variant;
+  f.boson_lz_max = sp->boson_lz_max;
+  f.nbr_bosons = (sp->kind == SPACE_BOSON) ? sp->nbr_fermions : 0;
   if (h) {
     f.pair_offset = h->pair_offset.as<int32_t>();
     f.factors = (precision == DH_PRECISION_FP32) ? h->factors32.ptr : h->factors64.ptr;
@@ -263,6 +265,7 @@ int hamiltonian_apply(dh_hamiltonian_s* h, const double* x, double* y, int nvec,
     a.x = x;
     a.xdiag = nullptr;
   }
+  if (sp->kind == SPACE_BOSON) return launch_boson_matvec(fqhe_device(sp, h, h->precision), a, h->precision, stream);
   if (sp->kind == SPACE_FERMION) {
     if (h->fast && h->fast_use && first == 0 && nbr == dim) return launch_ell_product(ell_device(h, h->precision), a, h->precision, stream);
     if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
@@ -296,6 +299,7 @@ int hamiltonian_apply_block(dh_hamiltonian_s* h, const double* x64, const float*
     a.xdiag = nullptr;
   }
   int rc;
+  if (sp->kind == SPACE_BOSON) return launch_boson_matvec(fqhe_device(sp, h, precision), a, precision, stream);
   if (sp->kind == SPACE_FERMION) {
     if (h->fast && h->fast_use) return launch_ell_product(ell_device(h, precision), a, precision, stream);
     if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
@@ -363,6 +367,40 @@ int dh_fermion_on_sphere_create(int nbr_fermions, int total_lz, int lz_max, unsi
   return DH_OK;
 }
 
+int dh_boson_on_sphere_create(int nbr_bosons, int total_lz, int lz_max, unsigned long memory, dh_space_t* out) {
+  DH_CHECK(out, DH_ERR_ARGUMENT, "null output handle");
+  *out = nullptr;
+  DH_CHECK(nbr_bosons >= 1, DH_ERR_ARGUMENT, "BosonOnSphereShort: nbr_bosons must be >= 1");
+  DH_CHECK(lz_max >= 0, DH_ERR_ARGUMENT, "BosonOnSphereShort: lz_max must be >= 0");
+  DH_CHECK(lz_max + nbr_bosons - 1 <= 40, DH_ERR_UNSUPPORTED,
+           "BosonOnSphereShort: lz_max + N - 1 = %d > 40 is not supported", lz_max + nbr_bosons - 1);
+  const int twice = total_lz + nbr_bosons * lz_max;
+  DH_CHECK(twice >= 0 && (twice & 1) == 0 && twice <= 2 * nbr_bosons * lz_max, DH_ERR_ARGUMENT,
+           "BosonOnSphereShort: total_lz = %d is not reachable by %d bosons with lz_max = %d", total_lz, nbr_bosons,
+           lz_max);
+  dh_space_s* sp = new (std::nothrow) dh_space_s();
+  DH_CHECK(sp, DH_ERR_MEMORY, "out of host memory");
+  // BosonOnSphereShort.cc:83-93: the basis is FermionOnSphere(N, totalLz, lzMax + N - 1)
+  sp->kind = SPACE_BOSON;
+  sp->nbr_fermions = nbr_bosons;
+  sp->lz_max = lz_max + nbr_bosons - 1;
+  sp->boson_lz_max = lz_max;
+  sp->total_lz = total_lz;
+  sp->total_sum = (total_lz + nbr_bosons * sp->lz_max) / 2;
+  sp->memory = memory;
+  sp->index_mode = DH_INDEX_RANK;
+  sp->kernel_variant = 1;
+  const char* lb = getenv("DH_FQHE_LOW_BITS");
+  sp->requested_low_bits = lb ? atoi(lb) : 0;
+  int rc = build_fermion_space(sp);
+  if (rc != DH_OK) {
+    delete sp;
+    return rc;
+  }
+  *out = sp;
+  return DH_OK;
+}
+
 int dh_spin12_chain_create(int chain_length, int sz, int memory, dh_space_t* out) {
   DH_CHECK(out, DH_ERR_ARGUMENT, "null output handle");
   *out = nullptr;
@@ -407,7 +445,7 @@ int dh_space_get_states(dh_space_t sp, uint64_t* words, int* lz_max, int64_t fir
   DH_CHECK(sp && words, DH_ERR_ARGUMENT, "null argument");
   DH_CHECK(first >= 0 && n >= 0 && first + n <= sp->dim, DH_ERR_ARGUMENT, "state range out of bounds");
   if (n == 0) return DH_OK;
-  if (sp->kind == SPACE_FERMION) {
+  if (sp->kind == SPACE_FERMION || sp->kind == SPACE_BOSON) {
     DH_CUDA(cudaMemcpy(words, sp->words.as<uint64_t>() + first, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
     if (lz_max)
       for (int64_t i = 0; i < n; ++i) lz_max[i] = words[i] ? 63 - __builtin_clzll(words[i]) : 0;
@@ -427,7 +465,7 @@ int dh_space_set_index_mode(dh_space_t sp, int mode) {
   DH_CHECK(sp, DH_ERR_ARGUMENT, "null space");
   DH_CHECK(mode == DH_INDEX_RANK || mode == DH_INDEX_LOOKUP, DH_ERR_ARGUMENT, "unknown index mode %d", mode);
   DH_CHECK(sp->kind == SPACE_FERMION || mode == DH_INDEX_RANK, DH_ERR_UNSUPPORTED,
-           "the spin chain uses its closed-form rank only");
+           "the spin chain and the boson space use their rank tables only");
   if (mode == DH_INDEX_LOOKUP) {
     int rc = build_lookup(sp);
     if (rc != DH_OK) return rc;
@@ -453,7 +491,7 @@ int dh_space_find_state_index(dh_space_t sp, const uint64_t* words, int64_t n, i
     if ((rc = di.alloc(n * sizeof(int64_t))) != DH_OK) return rc;
     out = di.as<int64_t>();
   }
-  if (sp->kind == SPACE_FERMION) {
+  if (sp->kind == SPACE_FERMION || sp->kind == SPACE_BOSON) {
     if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
     rc = launch_fqhe_find(fqhe_device(sp, nullptr, 0), w, n, reinterpret_cast<long long*>(out), 0);
   } else {
@@ -473,16 +511,25 @@ int dh_particle_on_sphere_generic_hamiltonian_create(dh_space_t sp, int nbr_part
   DH_CHECK(out, DH_ERR_ARGUMENT, "null output handle");
   *out = nullptr;
   DH_CHECK(sp && pseudopotentials, DH_ERR_ARGUMENT, "null argument");
-  DH_CHECK(sp->kind == SPACE_FERMION, DH_ERR_ARGUMENT, "ParticleOnSphereGenericHamiltonian needs a FermionOnSphere space");
-  DH_CHECK(nbr_particles == sp->nbr_fermions && lz_max == sp->lz_max, DH_ERR_ARGUMENT,
+  DH_CHECK(sp->kind == SPACE_FERMION || sp->kind == SPACE_BOSON, DH_ERR_ARGUMENT,
+           "ParticleOnSphereGenericHamiltonian needs a FermionOnSphere or BosonOnSphereShort space");
+  const bool bosons = sp->kind == SPACE_BOSON;
+  const int space_lz_max = bosons ? sp->boson_lz_max : sp->lz_max;
+  DH_CHECK(nbr_particles == sp->nbr_fermions && lz_max == space_lz_max, DH_ERR_ARGUMENT,
            "Hamiltonian (N = %d, lz_max = %d) does not match its space (N = %d, lz_max = %d)", nbr_particles, lz_max,
-           sp->nbr_fermions, sp->lz_max);
+           sp->nbr_fermions, space_lz_max);
   DH_CHECK(l2_factor == 0.0 || nbr_particles >= 2, DH_ERR_UNSUPPORTED, "an L^2 term needs at least two particles");
+  DH_CHECK(l2_factor == 0.0 || !bosons, DH_ERR_UNSUPPORTED, "the L^2 term is implemented for fermions");
   dh_hamiltonian_s* h = new (std::nothrow) dh_hamiltonian_s();
   DH_CHECK(h, DH_ERR_MEMORY, "out of host memory");
   h->space = sp;
-  h->kind = SPACE_FERMION;
-  h->tabs.build(lz_max);
+  h->kind = sp->kind;
+  // the particle statistics of the space select the factors, as Particles->GetParticleStatistic()
+  // does in EvaluateInteractionFactors (ParticleOnSphereGenericHamiltonian.cc:514)
+  if (bosons)
+    h->tabs.build_bosons(lz_max);
+  else
+    h->tabs.build(lz_max);
   if (l2_factor != 0.0) {
     // ParticleOnSphereGenericHamiltonian adds l2Factor L^2 (its L2Operator): a two-body table on top
     // of the interaction's, and the constant l2Factor (Lz^2 + Lz) in the shift
@@ -575,7 +622,7 @@ int dh_hamiltonian_set_precision(dh_hamiltonian_t h, int precision) {
 
 int dh_hamiltonian_set_pseudopotentials(dh_hamiltonian_t h, const double* v) {
   DH_CHECK(h && v, DH_ERR_ARGUMENT, "null argument");
-  DH_CHECK(h->kind == SPACE_FERMION && !h->l2_only, DH_ERR_ARGUMENT,
+  DH_CHECK((h->kind == SPACE_FERMION || h->kind == SPACE_BOSON) && !h->l2_only, DH_ERR_ARGUMENT,
            "pseudopotentials only apply to FQHE interaction Hamiltonians");
   h->v.assign(v, v + h->tabs.lz_max + 1);
   h->tabs.set_pseudopotentials(h->v.data());
@@ -907,7 +954,8 @@ int dh_hamiltonian_row_elements(dh_hamiltonian_t h, int64_t row, int* targets, i
 
 int dh_hamiltonian_get_interaction_factors(dh_hamiltonian_t h, double* factors, int cap, int* count) {
   DH_CHECK(h && count, DH_ERR_ARGUMENT, "null argument");
-  DH_CHECK(h->kind == SPACE_FERMION, DH_ERR_UNSUPPORTED, "interaction factors only exist for FQHE Hamiltonians");
+  DH_CHECK(h->kind == SPACE_FERMION || h->kind == SPACE_BOSON, DH_ERR_UNSUPPORTED,
+           "interaction factors only exist for FQHE Hamiltonians");
   *count = h->tabs.nbr_factors;
   const int n = std::min(cap, h->tabs.nbr_factors);
   if (factors && n > 0) memcpy(factors, h->tabs.factors.data(), n * sizeof(double));
@@ -967,6 +1015,7 @@ int dh_hamiltonian_count_elements(dh_hamiltonian_t h, int64_t* total) {
     *total = (int64_t)llround(2.0 * (double)L * frac * (double)sp->dim);
     return DH_OK;
   }
+  DH_CHECK(h->kind == SPACE_FERMION, DH_ERR_UNSUPPORTED, "element counts are implemented for fermions and spins");
   DevBuf t;
   int rc;
   if ((rc = t.alloc(sizeof(unsigned long long))) != DH_OK) return rc;

@@ -59,7 +59,11 @@ struct InteractionTables {
   std::vector<double> factors;      // current factors for the current V (+ l2_factor * l2_part)
   std::vector<double> l2_part;      // [factor]: the two-body table of L^2 (empty: no L^2 term)
   double l2_factor = 0.0;
+  bool bosonic = false;             // pair layout of build_bosons (m1 >= m2)
   void build(int lz_max);
+  // ParticleOnSphereGenericHamiltonian's bosonic factors (ParticleOnSphereGenericHamiltonian.cc:
+  // 620-806): pairs m1 >= m2 (pair m1 (m1 + 1) / 2 + m2), creations m3 >= m4, even relative momentum
+  void build_bosons(int lz_max);
   // L^2 of nbr_particles fermions as a two-body table (L^2 = L-L+ + Lz^2 + Lz; the constant part
   // is returned by l2_constant)
   void build_l2(int nbr_particles);
@@ -76,7 +80,7 @@ int tridiagonal_eigen(int n, const double* diag, const double* off, double* eig,
 int symmetric_eigen(int n, double* a, double* eig, double* z);
 
 // ------------------------------------------------------------- spaces
-enum SpaceKind { SPACE_FERMION = 1, SPACE_SPIN12 = 2 };
+enum SpaceKind { SPACE_FERMION = 1, SPACE_SPIN12 = 2, SPACE_BOSON = 3 };
 
 struct FermionRankTables {
   int low_bits = 0;                 // LB: rank = high_offset[w >> LB] + low_rank[w & (2^LB - 1)]
@@ -102,6 +106,8 @@ struct FqheDevice {
   int nbr_factors;
   int index_mode;              // DH_INDEX_RANK or DH_INDEX_LOOKUP
   int kernel_variant;          // 0: split-word rank kernel, 1: generic kernel (rank mode)
+  int boson_lz_max;            // BosonOnSphereShort: orbitals 0..boson_lz_max (words of lz_max + 1 bits)
+  int nbr_bosons;
 };
 
 struct MatvecArgs {
@@ -164,6 +170,8 @@ int band_eigenvalues(int n, int b, double* a, double* eig);
 int launch_fqhe_unrank(int nbr_fermions, int lz_max, int total_sum, long long dim, uint64_t* words,
                        const int64_t* counts_dev, int count_stride_o, int count_stride_s, cudaStream_t s);
 int launch_fqhe_matvec(const FqheDevice& f, const MatvecArgs& a, int precision, cudaStream_t s);
+// BosonOnSphereShort product (kernels_boson.cu), any vector layout, K = 1, 2, 4 (else in passes)
+int launch_boson_matvec(const FqheDevice& f, const MatvecArgs& a, int precision, cudaStream_t s);
 int launch_fqhe_row_elements(const FqheDevice& f, long long row, int* targets, int* signs, int* factor_index,
                              int cap, int* count, cudaStream_t s);
 int launch_fqhe_bins(const FqheDevice& f, const double* u, const double* v, double* partial_bins, int nblocks,

@@ -21,6 +21,9 @@ struct dh_space_s {
   dh::DevBuf words;  // uint64 FermionOnSphere words, uint32 spin words (chain bits only)
   // FermionOnSphere
   int nbr_fermions = 0, lz_max = 0, total_lz = 0, total_sum = 0;
+  // BosonOnSphereShort: N bosons in orbitals 0..boson_lz_max, stored as the FermionOnSphere words of
+  // N fermions in boson_lz_max + N orbitals (nbr_fermions = N, lz_max = boson_lz_max + N - 1)
+  int boson_lz_max = -1;
   unsigned long memory = 0;
   dh::FermionRankTables rank;
   dh::DevBuf low_rank, high_offset;

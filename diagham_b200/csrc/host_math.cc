@@ -214,6 +214,48 @@ void InteractionTables::build(int lzmax) {
   factors.assign(nf, 0.0);
 }
 
+void InteractionTables::build_bosons(int lzmax) {
+  lz_max = lzmax;
+  bosonic = true;
+  const int nlz = lzmax + 1;
+  // the reference keeps the pseudopotentials whose J / 2 has the parity opposite to the fermionic one
+  const int parity = (lzmax & 1) ? 0 : 1;
+  nbr_pairs = nlz * (nlz + 1) / 2;
+  pair_offset.assign(nbr_pairs + 1, 0);
+  int nf = 0;
+  for (int m1 = 0; m1 < nlz; ++m1)
+    for (int m2 = 0; m2 <= m1; ++m2) {
+      const int M = m1 + m2;
+      pair_offset[m1 * (m1 + 1) / 2 + m2] = nf;
+      nf += std::min(M, lzmax) - (M + 1) / 2 + 1;  // m3 = ceil(M / 2) .. min(M, lz_max)
+    }
+  pair_offset[nbr_pairs] = nf;
+  nbr_factors = nf;
+  dfactor.assign((size_t)nf * nlz, 0.0);
+  std::vector<double> cg((size_t)nlz * nlz * nlz, 0.0);
+  for (int i1 = 0; i1 < nlz; ++i1)
+    for (int i2 = 0; i2 < nlz; ++i2)
+      for (int J = 0; J <= 2 * lzmax; J += 2)
+        cg[((size_t)i1 * nlz + i2) * nlz + J / 2] = clebsch_gordan(lzmax, 2 * i1 - lzmax, lzmax, 2 * i2 - lzmax, J);
+  for (int m1 = 0; m1 < nlz; ++m1)
+    for (int m2 = 0; m2 <= m1; ++m2) {
+      const int M = m1 + m2;
+      int f = pair_offset[m1 * (m1 + 1) / 2 + m2];
+      for (int m3 = (M + 1) / 2; m3 <= std::min(M, lzmax); ++m3, ++f) {
+        const int m4 = M - m3;
+        // 4 for distinct pairs, halved for each pair of equal orbitals (the reference's weights)
+        const double w = 4.0 * ((m1 == m2) ? 0.5 : 1.0) * ((m3 == m4) ? 0.5 : 1.0);
+        for (int J = abs(2 * M - 2 * lzmax); J <= 2 * lzmax; J += 2) {
+          if (((J >> 1) & 1) == parity) continue;
+          const double c12 = cg[((size_t)m1 * nlz + m2) * nlz + J / 2];
+          const double c34 = cg[((size_t)m3 * nlz + m4) * nlz + J / 2];
+          dfactor[(size_t)f * nlz + (lzmax - J / 2)] = w * c12 * c34;
+        }
+      }
+    }
+  factors.assign(nf, 0.0);
+}
+
 void InteractionTables::set_pseudopotentials(const double* v) {
   const int nlz = lz_max + 1;
   // J ascending (m descending), as the reference accumulates its Clebsch-Gordan sum

@@ -67,6 +67,14 @@ int dh_device_count(int* count);
  * memory.  Rejects lz_max > 40 and sectors of odd (total_lz + nbr_fermions * lz_max). */
 int dh_fermion_on_sphere_create(int nbr_fermions, int total_lz, int lz_max, unsigned long memory, dh_space_t* out);
 
+/* BosonOnSphereShort(nbrBosons, totalLz, lzMax): FQHE/src/HilbertSpace/BosonOnSphereShort.cc:81-110.
+ * The states are stored, ordered and found as the FermionOnSphere(N, totalLz, lzMax + N - 1) words
+ * of their occupations (n_0 ones, a zero, n_1 ones, ...; BosonOnSphereShort.h:1231), so
+ * dh_space_get_states and dh_space_find_state_index take those words.  Rank index mode only;
+ * rejects lz_max + N - 1 > 40 (the reference switches to BosonOnSphere from lz_max + N - 1 = 63,
+ * ParticleOnSphereManager.cc:487).  memory is accepted for the signature and unused. */
+int dh_boson_on_sphere_create(int nbr_bosons, int total_lz, int lz_max, unsigned long memory, dh_space_t* out);
+
 /* Spin1_2Chain(chainLength, sz, memorySize): Spin/src/HilbertSpace/Spin1_2Chain.cc:113-142.
  * sz is twice the total Sz.  chain_length <= 32. */
 int dh_spin12_chain_create(int chain_length, int sz, int memory, dh_space_t* out);
@@ -96,7 +104,10 @@ int dh_space_set_index_mode(dh_space_t space, int mode);
  * the delta interaction.  l2_factor != 0 adds l2_factor L^2 (the reference's L2Operator,
  * AbstractQHEOnSphereHamiltonian.cc:541-542), as a second two-body table plus the constant
  * l2_factor (Lz^2 + Lz) in the shift (N >= 2).  The Hamiltonian does not own the space
- * (FQHESphereFermionsTwoBodyGeneric.cc:395-396). */
+ * (FQHESphereFermionsTwoBodyGeneric.cc:395-396).  On a BosonOnSphereShort space the factors are the
+ * reference's bosonic ones (:620-806: pairs m1 >= m2, even relative angular momenta, weights 4, 2 and
+ * 1) and the product applies AA / AdAd with their occupation square roots (BosonOnSphereShort.cc:
+ * 353, 431); bosonic Hamiltonians have no L^2 term, stored elements, element counts or adjoint. */
 int dh_particle_on_sphere_generic_hamiltonian_create(dh_space_t space, int nbr_particles, int lz_max,
                                                      const double* pseudopotentials, double l2_factor,
                                                      dh_hamiltonian_t* out);

@@ -955,3 +955,189 @@ int orc_basic_lanczos(orc_matvec_fn mv, void* ctx, long dim, const double* v0, i
   free(eig);
   return converged;
 }
+
+/* ===================================================================== */
+/* bosons: BosonOnSphereShort (FQHE/src/HilbertSpace/BosonOnSphereShort) */
+/* ===================================================================== */
+
+/* FermionToBoson / BosonToFermion (BosonOnSphereShort.h:1231-1290): occupations n_0..n_lzmax <->
+ * the fermionic word with, from bit 0 up, n_0 ones, a zero, n_1 ones, a zero, ... */
+void orc_boson_unpack(uint64_t w, int lz_max, int* n)
+{
+  for (int m = 0; m <= lz_max; ++m)
+    {
+      int c = 0;
+      while (w & 1ull)
+        {
+          ++c;
+          w >>= 1;
+        }
+      n[m] = c;
+      w >>= 1;
+    }
+}
+
+uint64_t orc_boson_pack(const int* n, int lz_max)
+{
+  uint64_t w = 0;
+  int shift = 0;
+  for (int m = 0; m <= lz_max; ++m)
+    {
+      w |= ((1ull << n[m]) - 1ull) << shift;
+      shift += n[m] + 1;
+    }
+  return w;
+}
+
+/* AA (BosonOnSphereShort.cc:353-375): annihilate n2 then n1 on a copy of the occupations, coefficient
+ * sqrt(n_n2 (n_n1 after the first)); 0 when either orbital is empty */
+double orc_boson_aa(const int* occ, int lz_max, int n1, int n2, int* out)
+{
+  for (int m = 0; m <= lz_max; ++m)
+    out[m] = occ[m];
+  if (out[n2] == 0)
+    return 0.0;
+  double c = out[n2];
+  --out[n2];
+  if (out[n1] == 0)
+    return 0.0;
+  c *= out[n1];
+  --out[n1];
+  return sqrt(c);
+}
+
+/* AdAd (BosonOnSphereShort.cc:431-451): create m2 then m1, coefficient sqrt((n_m2 + 1)(n_m1 + 1 after)) */
+double orc_boson_adad(const int* occ, int lz_max, int m1, int m2, uint64_t* out)
+{
+  int t[64];
+  for (int m = 0; m <= lz_max; ++m)
+    t[m] = occ[m];
+  ++t[m2];
+  double c = t[m2];
+  ++t[m1];
+  c *= t[m1];
+  *out = orc_boson_pack(t, lz_max);
+  return sqrt(c);
+}
+
+int orc_boson_nbr_pairs(int lz_max)
+{
+  return (lz_max + 1) * (lz_max + 2) / 2;
+}
+
+/* the bosonic branch of ParticleOnSphereGenericHamiltonian::EvaluateInteractionFactors (:620-806):
+ * pairs m1 ascending, m2 = 0..m1 (m2 = m1 last); per pair the m3 with 2 m3 >= m1 + m2 and m4 a valid
+ * orbital, ascending; factor = w sum_J V CG(m1 m2; J) CG(m3 m4; J) over the J with (J / 2) of the
+ * parity opposite to the fermionic one, w = 4, halved for m1 = m2 and again for m3 = m4 */
+int orc_boson_interaction_tables(int lz_max, const double* v, int* m1v, int* m2v, int* nbr_m3, int* m3_offset,
+                                 int* m3v, double* factors)
+{
+  int nlz = lz_max + 1;
+  int sign = (lz_max & 1) ? 0 : 1;
+  int pair = 0, nf = 0;
+  for (int m1 = 0; m1 < nlz; ++m1)
+    for (int m2 = 0; m2 <= m1; ++m2)
+      {
+        int lim = m1 + m2 > lz_max ? lz_max : m1 + m2;
+        int mn = m1 + m2 - lz_max < 0 ? 0 : m1 + m2 - lz_max;
+        if (m1v)
+          {
+            m1v[pair] = m1;
+            m2v[pair] = m2;
+            m3_offset[pair] = nf;
+          }
+        int cnt = 0;
+        int d1 = 2 * m1 - lz_max, d2 = 2 * m2 - lz_max;
+        for (int m3 = mn; m3 <= lim; ++m3)
+          {
+            if (2 * m3 < m1 + m2)
+              continue;
+            int m4 = m1 + m2 - m3;
+            int d3 = 2 * m3 - lz_max, d4 = 2 * m4 - lz_max;
+            if (m3v)
+              m3v[nf] = m3;
+            double acc = 0.0;
+            for (int J = abs(d1 + d2); J <= 2 * lz_max; J += 2)
+              {
+                if (((J >> 1) & 1) == sign)
+                  continue;
+                acc += v[lz_max - (J >> 1)] * orc_clebsch_gordan(lz_max, d1, lz_max, d2, J) *
+                       orc_clebsch_gordan(lz_max, d3, lz_max, d4, J);
+              }
+            double w = 4.0;
+            if (m1 == m2)
+              w *= 0.5;
+            if (m3 == m4)
+              w *= 0.5;
+            if (factors)
+              factors[nf] = w * acc;
+            ++nf;
+            ++cnt;
+          }
+        if (nbr_m3)
+          nbr_m3[pair] = cnt;
+        ++pair;
+      }
+  return nf;
+}
+
+/* the boson product through the same on-the-fly loop (AbstractQHEOnSphereHamiltonian.cc:456-488,
+ * push form; and its pull form, H being real symmetric); h holds the fermionic words of the
+ * BosonOnSphereShort basis (h->lz_max = lz_max + N - 1) and the bosonic tables */
+void orc_boson_push_add_multiply(const orc_fqhe_t* h, const double* x, double* y, long first, long nbr)
+{
+  int lz_max = h->lz_max - h->nbr_fermions + 1;
+  int occ[64], a[64];
+  for (long i = first; i < first + nbr; ++i)
+    {
+      orc_boson_unpack(h->words[i], lz_max, occ);
+      for (int p = 0; p < h->nbr_pairs; ++p)
+        {
+          double c = orc_boson_aa(occ, lz_max, h->m1v[p], h->m2v[p], a);
+          if (c == 0.0)
+            continue;
+          c *= x[i];
+          int sum = h->m1v[p] + h->m2v[p];
+          for (int q = 0; q < h->nbr_m3[p]; ++q)
+            {
+              int m3 = h->m3v[h->m3_offset[p] + q];
+              uint64_t t;
+              double c2 = orc_boson_adad(a, lz_max, m3, sum - m3, &t);
+              y[fqhe_index(h, t)] += c * h->factors[h->m3_offset[p] + q] * c2;
+            }
+        }
+    }
+  for (long i = first; i < first + nbr; ++i)
+    y[i] += h->shift * x[i];
+}
+
+void orc_boson_pull_multiply(const orc_fqhe_t* h, const double* x, double* y)
+{
+  int lz_max = h->lz_max - h->nbr_fermions + 1;
+  int occ[64], a[64];
+  for (long i = 0; i < h->dim; ++i)
+    {
+      orc_boson_unpack(h->words[i], lz_max, occ);
+      double acc = 0.0;
+      for (int p = 0; p < h->nbr_pairs; ++p)
+        {
+          double c = orc_boson_aa(occ, lz_max, h->m1v[p], h->m2v[p], a);
+          if (c == 0.0)
+            continue;
+          int sum = h->m1v[p] + h->m2v[p];
+          for (int q = 0; q < h->nbr_m3[p]; ++q)
+            {
+              int m3 = h->m3v[h->m3_offset[p] + q];
+              uint64_t t;
+              double c2 = orc_boson_adad(a, lz_max, m3, sum - m3, &t);
+              acc += c * c2 * h->factors[h->m3_offset[p] + q] * x[fqhe_index(h, t)];
+            }
+        }
+      y[i] = acc + h->shift * x[i];
+    }
+}
+
+void orc_boson_matvec_cb(void* ctx, const double* x, double* y)
+{
+  orc_boson_pull_multiply((const orc_fqhe_t*) ctx, x, y);
+}

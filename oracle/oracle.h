@@ -68,6 +68,19 @@ void orc_fqhe_pull_multiply(const orc_fqhe_t* h, const double* x, double* y);
 long orc_fqhe_row_elements(const orc_fqhe_t* h, long row, int* target, int* sign, int* factor_index, long cap);
 void orc_fqhe_expectation_bins(const orc_fqhe_t* h, const double* u, const double* v, double* bins);
 
+/* BosonOnSphereShort: occupations <-> fermionic words, AA / AdAd, the bosonic factors and the product
+ * (h holds the FermionOnSphere(N, 2Lz, lz_max + N - 1) words and the bosonic tables) */
+void orc_boson_unpack(uint64_t w, int lz_max, int* n);
+uint64_t orc_boson_pack(const int* n, int lz_max);
+double orc_boson_aa(const int* occ, int lz_max, int n1, int n2, int* out);
+double orc_boson_adad(const int* occ, int lz_max, int m1, int m2, uint64_t* out);
+int orc_boson_nbr_pairs(int lz_max);
+int orc_boson_interaction_tables(int lz_max, const double* v, int* m1v, int* m2v, int* nbr_m3, int* m3_offset,
+                                 int* m3v, double* factors);
+void orc_boson_push_add_multiply(const orc_fqhe_t* h, const double* x, double* y, long first, long nbr);
+void orc_boson_pull_multiply(const orc_fqhe_t* h, const double* x, double* y);
+void orc_boson_matvec_cb(void* ctx, const double* x, double* y);
+
 /* ---- spin-1/2 chain (Spin/src/HilbertSpace/Spin1_2Chain.cc) ---- */
 long orc_spin_dimension(int length, int sz);
 long orc_spin_basis(int length, int sz, uint64_t* words);

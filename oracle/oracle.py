@@ -83,6 +83,16 @@ def lib():
         L.orc_basic_lanczos.restype = ctypes.c_int
         L.orc_basic_lanczos.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long, _f64p, ctypes.c_int,
                                         ctypes.c_int, ctypes.c_double, _f64p, _i32p, _f64p, _f64p]
+        L.orc_boson_unpack.restype = None
+        L.orc_boson_unpack.argtypes = [ctypes.c_uint64, ctypes.c_int, _i32p]
+        L.orc_boson_nbr_pairs.restype = ctypes.c_int
+        L.orc_boson_nbr_pairs.argtypes = [ctypes.c_int]
+        L.orc_boson_interaction_tables.restype = ctypes.c_int
+        L.orc_boson_interaction_tables.argtypes = [ctypes.c_int, _f64p, _i32p, _i32p, _i32p, _i32p, _i32p, _f64p]
+        L.orc_boson_push_add_multiply.restype = None
+        L.orc_boson_push_add_multiply.argtypes = [ctypes.c_void_p, _f64p, _f64p, ctypes.c_long, ctypes.c_long]
+        L.orc_boson_pull_multiply.restype = None
+        L.orc_boson_pull_multiply.argtypes = [ctypes.c_void_p, _f64p, _f64p]
         _LIB = L
     return _LIB
 
@@ -214,6 +224,73 @@ class FQHE:
 
     def lanczos(self, v0, nev=1, max_iter=200, precision=1e-14):
         return basic_lanczos(lib().orc_fqhe_matvec_cb, ctypes.byref(self.s), self.dim, v0, nev, max_iter, precision)
+
+
+def boson_interaction_tables(two_s, v):
+    """The bosonic factors of ParticleOnSphereGenericHamiltonian (:620-806), layout of interaction_tables
+    with pairs m1 >= m2."""
+    L = lib()
+    v = np.ascontiguousarray(v, np.float64)
+    npairs = L.orc_boson_nbr_pairs(two_s)
+    cap = npairs * (two_s + 1)
+    m1 = np.zeros(npairs, np.int32)
+    m2 = np.zeros(npairs, np.int32)
+    nm3 = np.zeros(npairs, np.int32)
+    off = np.zeros(npairs, np.int32)
+    m3 = np.zeros(cap, np.int32)
+    fac = np.zeros(cap, np.float64)
+    nf = L.orc_boson_interaction_tables(two_s, _p(v, _f64p), _p(m1, _i32p), _p(m2, _i32p), _p(nm3, _i32p),
+                                        _p(off, _i32p), _p(m3, _i32p), _p(fac, _f64p))
+    return dict(m1=m1, m2=m2, nbr_m3=nm3, m3_offset=off, m3=m3[:nf], factors=fac[:nf])
+
+
+def boson_occupations(words, two_s):
+    out = np.zeros((len(words), two_s + 1), np.int32)
+    for i, w in enumerate(words):
+        lib().orc_boson_unpack(int(w), two_s, _p(out[i], _i32p))
+    return out
+
+
+class BosonFQHE(FQHE):
+    """N bosons in 2S + 1 orbitals at 2Lz, BosonOnSphereShort representation: the words and lookup
+    table of FermionOnSphere(N, 2Lz, 2S + N - 1) and the bosonic interaction tables."""
+
+    def __init__(self, n, two_s, total_lz, v, shift=0.0):
+        self.n, self.two_s, self.total_lz = n, two_s, total_lz
+        lzf = two_s + n - 1
+        self.words, self.lzmax = fermion_basis(n, lzf, total_lz)
+        self.dim = len(self.words)
+        self.max_shift = lib().orc_lookup_shift_from_memory(lzf, 9 << 20)
+        self.table, self.table_shift = lookup_table(self.words, self.lzmax, lzf, self.max_shift)
+        self.v = np.ascontiguousarray(v, np.float64)
+        self.tabs = boson_interaction_tables(two_s, self.v)
+        self.shift = shift
+        t = self.tabs
+        self._keep = [self.words, self.lzmax, self.table, self.table_shift, t["m1"], t["m2"], t["nbr_m3"],
+                      t["m3_offset"], t["m3"], t["factors"]]
+        self.s = _FqheStruct(n, lzf, total_lz, self.dim, _p(self.words, _u64p), _p(self.lzmax, _i32p),
+                             _p(self.table, _i32p), _p(self.table_shift, _i32p), self.max_shift, len(t["m1"]),
+                             _p(t["m1"], _i32p), _p(t["m2"], _i32p), _p(t["nbr_m3"], _i32p),
+                             _p(t["m3_offset"], _i32p), _p(t["m3"], _i32p), _p(t["factors"], _f64p), shift)
+
+    def occupations(self):
+        return boson_occupations(self.words, self.two_s)
+
+    def pull(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros(self.dim, np.float64)
+        lib().orc_boson_pull_multiply(ctypes.byref(self.s), _p(x, _f64p), _p(y, _f64p))
+        return y
+
+    def push(self, x, first=0, nbr=None):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros(self.dim, np.float64)
+        nbr = self.dim - first if nbr is None else nbr
+        lib().orc_boson_push_add_multiply(ctypes.byref(self.s), _p(x, _f64p), _p(y, _f64p), first, nbr)
+        return y
+
+    def lanczos(self, v0, nev=1, max_iter=200, precision=1e-14):
+        return basic_lanczos(lib().orc_boson_matvec_cb, ctypes.byref(self.s), self.dim, v0, nev, max_iter, precision)
 
 
 def spin_basis(length, sz):

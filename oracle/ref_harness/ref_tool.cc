@@ -7,6 +7,7 @@
 //
 // Every command calls only reference classes:
 //   FermionOnSphere                      FQHE/src/HilbertSpace/FermionOnSphere.cc:75
+//   BosonOnSphereShort                   FQHE/src/HilbertSpace/BosonOnSphereShort.cc:81 (bqhe_* commands)
 //   ParticleOnSphereGenericHamiltonian   FQHE/src/Hamiltonian/ParticleOnSphereGenericHamiltonian.cc:66
 //   AbstractQHEOnSphereHamiltonian::LowLevelAddMultiply   .../AbstractQHEOnSphereHamiltonian.cc:410
 //   Spin1_2Chain                         Spin/src/HilbertSpace/Spin1_2Chain.cc:113
@@ -26,6 +27,7 @@
 
 #include "config.h"
 #include "HilbertSpace/FermionOnSphere.h"
+#include "HilbertSpace/BosonOnSphereShort.h"
 #include "HilbertSpace/Spin1_2Chain.h"
 #include "Hamiltonian/ParticleOnSphereGenericHamiltonian.h"
 #include "Hamiltonian/ParticleOnSphereL2Hamiltonian.h"
@@ -53,6 +55,7 @@
 #include <unistd.h>
 #include <iostream>
 #include <string>
+#include <sstream>
 
 using std::cout;
 using std::endl;
@@ -437,6 +440,9 @@ static void Usage()
 	  "  fqhe_lanczos N 2S 2Lz vfile algo nev block maxiter precision out gsout x0 [x1 ...]\n"
 	  "  fqhe_lanczos_disk N 2S 2Lz vfile algo nbriter precision dir x0|resume gsiter out gsout\n"
 	  "  fqhe_expect N 2S 2Lz vfile psifile out\n"
+	  "  bqhe_basis N 2S 2Lz out\n"
+	  "  bqhe_matvec N 2S 2Lz vfile xfile shift out\n"
+	  "  bqhe_lanczos N 2S 2Lz vfile algo nev block maxiter precision out gsout x0 [x1 ...]\n"
 	  "  fqhe_l2 N 2S 2Lz xfile out\n"
 	  "  pseudopotentials 2S out\n"
 	  "  spin_basis L 2Sz out\n"
@@ -593,6 +599,62 @@ int main(int argc, char** argv)
       for (int i = 0; i < NbrInitial; ++i)
 	Init[i].ReadVector(argv[13 + i]);
       RunLanczosLoop(&H, Arch, Algo, Nev, Block, MaxIter, Precision, Init, NbrInitial, argv[11],
+		     strcmp(argv[12], "-") == 0 ? 0 : argv[12]);
+      return 0;
+    }
+  // bosons: BosonOnSphereShort with the same Hamiltonian class (its bosonic factors and AA / AdAd)
+  if (strcmp(Cmd, "bqhe_basis") == 0 && argc == 6)
+    {
+      // layout: int64 dimension, then per state the occupations n_0..n_2S as int32 (PrintState)
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      BosonOnSphereShort Space(N, TotalLz, LzMax);
+      long Dim = Space.GetHilbertSpaceDimension();
+      FILE* f = OpenOut(argv[5]);
+      fwrite(&Dim, sizeof(long), 1, f);
+      for (long i = 0; i < Dim; ++i)
+	{
+	  std::ostringstream Str;
+	  Space.PrintState(Str, (int) i);
+	  std::istringstream In(Str.str());
+	  for (int m = 0; m <= LzMax; ++m)
+	    {
+	      int Occupation = -1;
+	      In >> Occupation;
+	      fwrite(&Occupation, sizeof(int), 1, f);
+	    }
+	}
+      fclose(f);
+      return 0;
+    }
+  if (strcmp(Cmd, "bqhe_matvec") == 0 && argc == 9)
+    {
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      double* V = ReadDoubles(argv[5], LzMax + 1);
+      BosonOnSphereShort Space(N, TotalLz, LzMax);
+      MonoProcessorArchitecture Arch;
+      ParticleOnSphereGenericHamiltonian H(&Space, N, LzMax, V, 0.0, &Arch, 0, false, 0, false);
+      H.ShiftHamiltonian(atof(argv[7]));
+      RealVector X;
+      X.ReadVector(argv[6]);
+      RealVector Y(Space.GetHilbertSpaceDimension(), true);
+      H.LowLevelMultiply(X, Y);
+      Y.WriteVector(argv[8]);
+      return 0;
+    }
+  if (strcmp(Cmd, "bqhe_lanczos") == 0 && argc >= 14)
+    {
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      double* V = ReadDoubles(argv[5], LzMax + 1);
+      int Nev = atoi(argv[7]), Block = atoi(argv[8]), MaxIter = atoi(argv[9]);
+      BosonOnSphereShort Space(N, TotalLz, LzMax);
+      AbstractArchitecture* Arch = MakeArchitecture();
+      Arch->SetDimension(Space.GetHilbertSpaceDimension());
+      ParticleOnSphereGenericHamiltonian H(&Space, N, LzMax, V, 0.0, Arch, 0, false, 0, false);
+      int NbrInitial = argc - 13;
+      RealVector* Init = new RealVector[NbrInitial];
+      for (int i = 0; i < NbrInitial; ++i)
+	Init[i].ReadVector(argv[13 + i]);
+      RunLanczosLoop(&H, Arch, argv[6], Nev, Block, MaxIter, atof(argv[10]), Init, NbrInitial, argv[11],
 		     strcmp(argv[12], "-") == 0 ? 0 : argv[12]);
       return 0;
     }

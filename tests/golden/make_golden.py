@@ -301,6 +301,40 @@ def l2_fixtures(tmp):
         save("l2_n%d_2s%d_lz%d.npz" % (n, s, lz), cmd, seed=7, y=read_vector(yf))
 
 
+def boson_fixtures(tmp):
+    # BosonOnSphereShort with ParticleOnSphereGenericHamiltonian (on the fly, hermitian symmetry off):
+    # the basis as occupations (PrintState), y = H x for x = the splitmix64 vector of seed 0 (shift 0
+    # and 0.37), and the basic Lanczos run from that vector (precision MACHINE_PRECISION, 300 iterations
+    # at most).  "coulomb" = the LLL Coulomb V_m with the odd m set to zero, "v0" = the delta interaction.
+    for (n, s, lz, kind) in [(4, 6, 0, "v0"), (6, 10, 0, "v0"), (6, 10, 0, "coulomb"), (5, 9, 1, "coulomb"),
+                             (7, 12, 2, "coulomb"), (8, 8, 0, "coulomb"), (8, 14, 0, "coulomb")]:
+        p = os.path.join(tmp, "pp.bin")
+        run("pseudopotentials", s, p)
+        v = np.fromfile(p, np.float64)
+        v[1::2] = 0.0
+        if kind == "v0":
+            v = np.zeros(s + 1)
+            v[0] = 1.0
+        vf = os.path.join(tmp, "vb.bin")
+        v.tofile(vf)
+        bf = os.path.join(tmp, "bb.bin")
+        cmd = run("bqhe_basis", n, s, lz, bf)
+        b = open(bf, "rb").read()
+        dim = int(np.frombuffer(b[:8], np.int64)[0])
+        occ = np.frombuffer(b[8:], np.int32).reshape(dim, s + 1).copy()
+        xf = os.path.join(tmp, "xb.vec")
+        write_vector(xf, splitmix_vector(0, dim))
+        ys = {}
+        for shift in (0.0, 0.37):
+            yf = os.path.join(tmp, "yb.vec")
+            cmd2 = run("bqhe_matvec", n, s, lz, vf, xf, shift, yf)
+            ys["y_shift%g" % shift] = read_vector(yf)
+        lf = os.path.join(tmp, "lb.out")
+        cmd3 = run("bqhe_lanczos", n, s, lz, vf, "basic", 1, 1, 300, 0, lf, "-", xf)
+        save("boson_n%d_2s%d_lz%d_%s.npz" % (n, s, lz, kind), "; ".join([cmd, cmd2, cmd3]), v=v, seed=0,
+             occupations=occ, max_iter=300, **ys, **read_lanczos(lf))
+
+
 def dir_files(d):
     names = sorted(os.listdir(d))
     return np.array(names), {"f%d" % i: np.frombuffer(open(os.path.join(d, f), "rb").read(), np.uint8)
@@ -383,6 +417,8 @@ def main():
             l2_fixtures(tmp)
         if args.only in (None, "disk"):
             disk_fixtures(tmp)
+        if args.only in (None, "boson"):
+            boson_fixtures(tmp)
         if args.slow:
             slow_fixtures(tmp)
 

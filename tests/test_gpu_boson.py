@@ -1,0 +1,132 @@
+"""BosonOnSphereShort on the GPU against the reference's fixtures and the oracle:
+
+- the basis: the occupations of the stored words equal the reference's (PrintState) in order, and
+  FindStateIndex returns every state's own index;
+- the product (ParticleOnSphereGenericHamiltonian on bosons, on the fly): FP64 within 1e-13 and FP32
+  within 2e-6 of max|y|, shift 0 and 0.37, single vectors, blocks of 2, 3 and 4 vectors in both
+  layouts, and a column range against the oracle's push form;
+- Lanczos: the reference's E0 (1e-10 relative, iteration counter within 2) and E0 = 0 (1e-10
+  absolute) for the Laughlin state of the delta interaction; block Lanczos and the FP32 + FP64
+  refined solve reach the same energy;
+- what bosons do not offer is refused with an error."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden, parse_sector
+
+pytestmark = pytest.mark.gpu
+
+NAMES = sorted(os.path.basename(f) for f in glob.glob(os.path.join(GOLDEN, "boson_*.npz")))
+
+
+def _setup(gpu, name):
+    z = golden(name)
+    n, s, lz = parse_sector(name)
+    sp = gpu.BosonOnSphereShort(n, lz, s)
+    return z, sp, gpu.ParticleOnSphereGenericHamiltonian(sp, n, s, z["v"])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_boson_basis_matches_reference(gpu, name):
+    z, sp, _ = _setup(gpu, name)
+    assert sp.dim == z["occupations"].shape[0]
+    words, _ = sp.states()
+    assert np.array_equal(sp.occupations(words), z["occupations"])
+    assert np.array_equal(sp.FindStateIndex(words), np.arange(sp.dim))
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-13), ("fp32", 2e-6)])
+@pytest.mark.parametrize("name", NAMES)
+def test_boson_product_matches_reference(gpu, orc, name, prec, tol):
+    z, sp, H = _setup(gpu, name)
+    H.set_precision(prec)
+    x = orc.random_vector(int(z["seed"]), sp.dim)
+    for shift in (0.0, 0.37):
+        H.ShiftHamiltonian(shift)
+        ref = z["y_shift%g" % shift]
+        y = H.LowLevelMultiply(x)
+        assert np.max(np.abs(y - ref)) <= tol * np.max(np.abs(ref)), shift
+    H.ShiftHamiltonian(0.0)
+    ref = z["y_shift0"]
+    for k in (2, 3, 4):
+        X = np.stack([x * c for c in (1.0, -0.5, 2.0, 0.25)[:k]], axis=1)
+        Y = H.block_multiply(X)  # row-interleaved (dim, k)
+        for j in range(k):
+            c = X[0, j] / x[0]
+            assert np.max(np.abs(Y[:, j] - c * ref)) <= tol * abs(c) * np.max(np.abs(ref)), (k, j)
+        srcs = np.ascontiguousarray(X.T)
+        dsts = np.zeros_like(srcs)
+        H.LowLevelMultipleAddMultiply(srcs, dsts)  # vectors one after the other
+        for j in range(k):
+            c = X[0, j] / x[0]
+            assert np.max(np.abs(dsts[j] - c * ref)) <= tol * abs(c) * np.max(np.abs(ref)), (k, j)
+
+
+@pytest.mark.parametrize("name", ["boson_n7_2s12_lz2_coulomb.npz", "boson_n8_2s8_lz0_coulomb.npz"])
+def test_boson_column_range_matches_oracle_push(gpu, orc, name):
+    z, sp, H = _setup(gpu, name)
+    n, s, lz = parse_sector(name)
+    O = orc.BosonFQHE(n, s, lz, z["v"], shift=0.3)
+    H.ShiftHamiltonian(0.3)
+    x = orc.random_vector(3, sp.dim)
+    first, nbr = sp.dim // 5, sp.dim // 3
+    y = np.zeros(sp.dim)
+    H.LowLevelAddMultiply(x, y, first, nbr)
+    ref = O.push(x, first, nbr)
+    assert np.max(np.abs(y - ref)) <= 1e-13 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_boson_lanczos_matches_reference(gpu, orc, name):
+    z, sp, H = _setup(gpu, name)
+    lz = gpu.BasicLanczosAlgorithm(H, 1, 400)
+    lz.InitializeLanczosAlgorithm(orc.random_vector(int(z["seed"]), sp.dim))
+    r = lz.solve(int(z["max_iter"]))
+    e_ref = float(z["eigenvalues"][0])
+    if bool(z["converged"]):
+        assert abs(r["eigenvalues"][0] - e_ref) <= 1e-10 * abs(e_ref)
+        assert abs(r["iterations"] - int(z["iterations"])) <= 2
+    else:
+        assert abs(r["eigenvalues"][0]) < 1e-10  # Laughlin state of the delta interaction
+
+
+def test_boson_block_and_refined_solves(gpu, orc):
+    z, sp, H = _setup(gpu, "boson_n8_2s14_lz0_coulomb.npz")
+    e_ref = float(z["eigenvalues"][0])
+    b = gpu.BasicBlockLanczosAlgorithm(H, 1, 400, block_size=2)
+    b.InitializeLanczosAlgorithm(seed=4)
+    rb = b.solve(400)
+    assert abs(rb["eigenvalues"][0] - e_ref) <= 1e-10 * abs(e_ref)
+    H.set_precision("fp32")
+    lz = gpu.BasicLanczosAlgorithmWithGroundState(H, 1, 400)
+    lz.InitializeLanczosAlgorithm(seed=5)
+    r = lz.solve_refined(400, precision=1e-12)
+    assert abs(r["energy"] - e_ref) <= 1e-11 * abs(e_ref)
+    psi = lz.GetGroundState()
+    H.set_precision("fp64")
+    assert abs(H.MatrixElement(psi, psi) - e_ref) <= 1e-10 * abs(e_ref)
+
+
+def test_boson_errors(gpu, orc):
+    z, sp, H = _setup(gpu, "boson_n6_2s10_lz0_coulomb.npz")
+    with pytest.raises(gpu.DiagHamError, match="error -4"):
+        H.EnableFastMultiplication()
+    with pytest.raises(gpu.DiagHamError, match="error -4"):
+        H.pseudopotential_adjoint(np.ones(sp.dim), np.ones(sp.dim))
+    with pytest.raises(gpu.DiagHamError, match="error -4"):
+        gpu.ParticleOnSphereGenericHamiltonian(sp, 6, 10, z["v"], l2_factor=1.0)
+    with pytest.raises(gpu.DiagHamError, match="error -1"):
+        gpu.ParticleOnSphereL2Hamiltonian(sp, 6, 10, 0)
+    with pytest.raises(gpu.DiagHamError, match="error -4"):
+        sp.set_index_mode("lookup")
+    with pytest.raises(gpu.DiagHamError, match="not reachable"):
+        gpu.BosonOnSphereShort(5, 0, 9)
+    # new pseudopotentials are taken by the boson tables too
+    v2 = np.array(z["v"]) * 0.5
+    H.set_pseudopotentials(v2)
+    x = orc.random_vector(1, sp.dim)
+    ref = orc.BosonFQHE(6, 10, 0, v2).pull(x)
+    assert np.max(np.abs(H.LowLevelMultiply(x) - ref)) <= 1e-13 * np.max(np.abs(ref))

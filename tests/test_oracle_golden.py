@@ -226,3 +226,33 @@ def test_disk_state_files_of_the_reference(orc, fmt):
     # the resumed reference run ends where the uninterrupted one does
     assert int(z["resumed_iterations"]) + int(z["stop"]) == int(z["full_iterations"])
     assert float(z["resumed_eigenvalue"]) == float(z["full_eigenvalue"])
+
+
+BOSON_FIXTURES = sorted(os.path.basename(f) for f in glob.glob(os.path.join(GOLDEN, "boson_*.npz")))
+
+
+@pytest.mark.parametrize("name", BOSON_FIXTURES)
+def test_boson_oracle_matches_reference(orc, name):
+    # BosonOnSphereShort: the basis (occupations of the fermionic words, in the reference's order),
+    # the product at shift 0 and 0.37 (push and pull forms), and the Lanczos ground-state energy
+    z = golden(name)
+    n, s, lz = parse_sector(name)
+    O = orc.BosonFQHE(n, s, lz, z["v"])
+    assert O.dim == z["occupations"].shape[0]
+    assert np.array_equal(O.occupations(), z["occupations"])
+    x = orc.random_vector(int(z["seed"]), O.dim)
+    for shift in (0.0, 0.37):
+        O.s.shift = shift
+        ref = z["y_shift%g" % shift]
+        tol = 1e-13 * np.max(np.abs(ref))
+        assert np.max(np.abs(O.pull(x) - ref)) <= tol
+        assert np.max(np.abs(O.push(x) - ref)) <= tol
+    O.s.shift = 0.0
+    e_ref = float(z["eigenvalues"][0])
+    if bool(z["converged"]):
+        r = O.lanczos(x, max_iter=int(z["max_iter"]))
+        assert abs(r["eigenvalues"][0] - e_ref) <= 1e-10 * abs(e_ref)
+        assert abs(r["iterations"] - int(z["iterations"])) <= 2
+    else:
+        # the Laughlin state of the delta interaction at 2S = 2 (N - 1): E0 = 0
+        assert abs(e_ref) < 1e-12
