@@ -236,9 +236,17 @@ int refresh_fast_diagonal(dh_hamiltonian_s* h) {
 // In FP32 mode x is converted to FP32 first and the diagonal (shift) term uses the FP64 x.
 int hamiltonian_apply(dh_hamiltonian_s* h, const double* x, double* y, int nvec, int64_t first, int64_t nbr,
                       int accumulate, const float* x32_ready, cudaStream_t stream) {
+  return hamiltonian_apply_rows(h, x, y, nvec, first, nbr, accumulate, x32_ready, stream, 0, 0);
+}
+
+int hamiltonian_apply_rows(dh_hamiltonian_s* h, const double* x, double* y, int nvec, int64_t first, int64_t nbr,
+                           int accumulate, const float* x32_ready, cudaStream_t stream, int64_t out_first,
+                           int64_t out_last) {
   dh_space_s* sp = h->space;
   const int64_t dim = sp->dim;
   MatvecArgs a = {};
+  a.out_first = out_first;
+  a.out_last = out_last;
   a.y = y;
   a.ld = 1;
   a.vstride = dim;
@@ -276,8 +284,15 @@ int hamiltonian_apply(dh_hamiltonian_s* h, const double* x, double* y, int nvec,
 
 int hamiltonian_apply_block(dh_hamiltonian_s* h, const double* x64, const float* x32, double* y, int k, int precision,
                             cudaStream_t stream) {
+  return hamiltonian_apply_block_rows(h, x64, x32, y, k, precision, stream, 0, 0);
+}
+
+int hamiltonian_apply_block_rows(dh_hamiltonian_s* h, const double* x64, const float* x32, double* y, int k,
+                                 int precision, cudaStream_t stream, int64_t out_first, int64_t out_last) {
   dh_space_s* sp = h->space;
   MatvecArgs a = {};
+  a.out_first = out_first;
+  a.out_last = out_last;
   a.y = y;
   a.ld = k;
   a.vstride = 1;
@@ -719,6 +734,46 @@ int dh_hamiltonian_set_stream(dh_hamiltonian_t h, void* stream) {
   return DH_OK;
 }
 
+// A product whose result goes to host memory: the rows are computed in up to kCopyChunks chunks on
+// the handle's stream, and each chunk's rows are copied to the host on a second stream as soon as
+// they are done, so the copy of all but the last chunk overlaps the product.  run(r0, r1) enqueues
+// the product of rows [r0, r1) on h->stream; copy(r0, r1, s) enqueues their device-to-host copy on s.
+extern "C++" {
+template <typename Run, typename Copy>
+static int product_to_host(dh_hamiltonian_s* h, int64_t dim, Run run, Copy copy) {
+  // chunks of at least 2^18 rows, boundaries on multiples of 256 rows (slices of the stored form)
+  int chunks = (int)std::min<int64_t>(dh_hamiltonian_s::kCopyChunks, std::max<int64_t>(1, dim >> 18));
+  if (chunks > 1 && !h->copy_stream) {
+    if (cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      h->copy_stream = nullptr;
+    }
+    for (int c = 0; h->copy_stream && c < dh_hamiltonian_s::kCopyChunks; ++c)
+      DH_CUDA(cudaEventCreateWithFlags(&h->chunk_done[c], cudaEventDisableTiming));
+  }
+  if (!h->copy_stream) chunks = 1;
+  int rc;
+  if (chunks == 1) {
+    if ((rc = run(0, dim)) != DH_OK) return rc;
+    if ((rc = copy(0, dim, h->stream)) != DH_OK) return rc;
+    DH_CUDA(cudaStreamSynchronize(h->stream));
+    return DH_OK;
+  }
+  const int64_t step = ((dim + chunks - 1) / chunks + 255) & ~(int64_t)255;
+  for (int c = 0; c < chunks; ++c) {
+    const int64_t r0 = (int64_t)c * step, r1 = std::min(dim, r0 + step);
+    if (r0 >= r1) break;
+    if ((rc = run(r0, r1)) != DH_OK) return rc;
+    DH_CUDA(cudaEventRecord(h->chunk_done[c], h->stream));
+    DH_CUDA(cudaStreamWaitEvent(h->copy_stream, h->chunk_done[c], 0));
+    if ((rc = copy(r0, r1, h->copy_stream)) != DH_OK) return rc;
+  }
+  DH_CUDA(cudaStreamSynchronize(h->copy_stream));
+  DH_CUDA(cudaStreamSynchronize(h->stream));
+  return DH_OK;
+}
+}  // extern "C++"
+
 static int multiply_common(dh_hamiltonian_t h, const double* src, double* dst, int nvec, int64_t first, int64_t nbr,
                            int accumulate) {
   DH_CHECK(h && src && dst, DH_ERR_ARGUMENT, "null argument");
@@ -744,10 +799,29 @@ static int multiply_common(dh_hamiltonian_t h, const double* src, double* dst, i
   }
   // LowLevelMultiply clears the destination, then adds (AbstractHamiltonian.cc:475-476); the pull
   // kernels write every row, so "clear then add" is a plain store (accumulate = 0)
-  if ((rc = hamiltonian_apply(h, x, y, nvec, first, nbr, accumulate, nullptr, h->stream)) != DH_OK) return rc;
-  if (!dst_dev) DH_CUDA(cudaMemcpyAsync(dst, y, bytes, cudaMemcpyDeviceToHost, h->stream));
-  DH_CUDA(cudaStreamSynchronize(h->stream));
-  return DH_OK;
+  if (dst_dev) {
+    if ((rc = hamiltonian_apply(h, x, y, nvec, first, nbr, accumulate, nullptr, h->stream)) != DH_OK) return rc;
+    DH_CUDA(cudaStreamSynchronize(h->stream));
+    return DH_OK;
+  }
+  const float* x32 = nullptr;
+  if (h->precision == DH_PRECISION_FP32) {
+    if ((rc = ensure_buffer(h->x32, (size_t)dim * nvec * sizeof(float))) != DH_OK) return rc;
+    if ((rc = launch_convert_f32(x, h->x32.as<float>(), dim * nvec, h->stream)) != DH_OK) return rc;
+    x32 = h->x32.as<float>();
+  }
+  return product_to_host(
+      h, dim,
+      [&](int64_t r0, int64_t r1) {
+        return hamiltonian_apply_rows(h, x, y, nvec, first, nbr, accumulate, x32, h->stream, r0, r1);
+      },
+      [&](int64_t r0, int64_t r1, cudaStream_t cs) -> int {
+        // vector j of the result occupies [j dim, (j + 1) dim)
+        for (int j = 0; j < nvec; ++j)
+          DH_CUDA(cudaMemcpyAsync(dst + (size_t)j * dim + r0, y + (size_t)j * dim + r0, (size_t)(r1 - r0) * sizeof(double),
+                                  cudaMemcpyDeviceToHost, cs));
+        return DH_OK;
+      });
 }
 
 int dh_hamiltonian_block_multiply(dh_hamiltonian_t h, const double* x, double* y, int k) {
@@ -774,10 +848,22 @@ int dh_hamiltonian_block_multiply(dh_hamiltonian_t h, const double* x, double* y
     if ((rc = launch_convert_f32(xd, h->x32.as<float>(), dim * k, h->stream)) != DH_OK) return rc;
     x32 = h->x32.as<float>();
   }
-  if ((rc = hamiltonian_apply_block(h, xd, x32, yd, k, h->precision, h->stream)) != DH_OK) return rc;
-  if (!dst_dev) DH_CUDA(cudaMemcpyAsync(y, yd, bytes, cudaMemcpyDeviceToHost, h->stream));
-  DH_CUDA(cudaStreamSynchronize(h->stream));
-  return DH_OK;
+  if (dst_dev) {
+    if ((rc = hamiltonian_apply_block(h, xd, x32, yd, k, h->precision, h->stream)) != DH_OK) return rc;
+    DH_CUDA(cudaStreamSynchronize(h->stream));
+    return DH_OK;
+  }
+  return product_to_host(
+      h, dim,
+      [&](int64_t r0, int64_t r1) {
+        return hamiltonian_apply_block_rows(h, xd, x32, yd, k, h->precision, h->stream, r0, r1);
+      },
+      [&](int64_t r0, int64_t r1, cudaStream_t cs) -> int {
+        // rows are k-interleaved: rows [r0, r1) are one contiguous range
+        DH_CUDA(cudaMemcpyAsync(y + (size_t)r0 * k, yd + (size_t)r0 * k, (size_t)(r1 - r0) * k * sizeof(double),
+                                cudaMemcpyDeviceToHost, cs));
+        return DH_OK;
+      });
 }
 
 int dh_hamiltonian_autotune(dh_hamiltonian_t h, int block_size, int repeats, double* out) {

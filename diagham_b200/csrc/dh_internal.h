@@ -120,6 +120,7 @@ struct MatvecArgs {
   long long col_first, col_last; // only columns (targets) in [col_first, col_last) contribute
   long long row_first, row_last; // rows that receive the diagonal (shift) contribution
   int accumulate;                // y += H x (1) or y = H x (0)
+  long long out_first, out_last; // rows computed: [out_first, out_last); out_last = 0: every row
 };
 
 // Every Lz sector of one system in one launch (rows concatenated, vectors K-interleaved).

@@ -57,6 +57,19 @@ struct dh_hamiltonian_s {
   dh::DevBuf stage_x, stage_y, stage_v, x32, bins_partial, bins;
   dh::Reducer red;
   dh::DevBuf red_storage;
+  // products into host memory: a second stream carries finished row chunks back while the next
+  // chunks are computed (created on first use)
+  static const int kCopyChunks = 8;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t chunk_done[kCopyChunks] = {};
+  ~dh_hamiltonian_s() {
+    if (copy_stream) {
+      cudaStreamSynchronize(copy_stream);
+      cudaStreamDestroy(copy_stream);
+    }
+    for (cudaEvent_t e : chunk_done)
+      if (e) cudaEventDestroy(e);
+  }
 };
 
 namespace dh {
@@ -64,6 +77,12 @@ bool is_device_pointer(const void* p);
 int ensure_buffer(DevBuf& b, size_t bytes);
 int build_lookup(dh_space_s* sp);
 FqheDevice fqhe_device(const dh_space_s* sp, const dh_hamiltonian_s* h, int precision);
+// the product restricted to output rows [out_first, out_last) (out_last = 0: every row)
+int hamiltonian_apply_rows(dh_hamiltonian_s* h, const double* x, double* y, int nvec, int64_t first, int64_t nbr,
+                           int accumulate, const float* x32_ready, cudaStream_t stream, int64_t out_first,
+                           int64_t out_last);
+int hamiltonian_apply_block_rows(dh_hamiltonian_s* h, const double* x64, const float* x32, double* y, int k,
+                                 int precision, cudaStream_t stream, int64_t out_first, int64_t out_last);
 SpinDevice spin_device(const dh_space_s* sp, const dh_hamiltonian_s* h);
 int upload_factors(dh_hamiltonian_s* h);
 // (re)build the split-word rank tables of a FermionOnSphere space for a split of low_bits (0: the

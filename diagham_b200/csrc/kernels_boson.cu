@@ -67,7 +67,8 @@ __global__ void __launch_bounds__(kBosonThreads) boson_matvec_kernel(FqheDevice 
   const TG* x = static_cast<const TG*>(a.x);
   double* y = static_cast<double*>(a.y);
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+  const long long r_end = a.out_last > 0 ? a.out_last : f.dim;
+  for (long long r = a.out_first + (long long)blockIdx.x * blockDim.x + threadIdx.x; r < r_end; r += stride) {
     const uint64_t s = __ldg(f.words + r);
     // occupations and group starts of the row
     uint8_t n[64], P[64];
@@ -137,7 +138,8 @@ int launch_typed(const FqheDevice& f, const MatvecArgs& a, cudaStream_t s) {
   int sms = 148;
   int dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  long long blocks = (f.dim + kBosonThreads - 1) / kBosonThreads;
+  const long long rows = (a.out_last > 0 ? a.out_last : f.dim) - a.out_first;
+  long long blocks = (rows + kBosonThreads - 1) / kBosonThreads;
   const long long cap = (long long)sms * 16;
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;

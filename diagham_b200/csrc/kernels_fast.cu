@@ -168,11 +168,14 @@ __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, 
   const TG* x = static_cast<const TG*>(a.x);
   const TG* diag = static_cast<const TG*>(e.diag);
   const int lane = threadIdx.x & 31;
-  const long long nslices = (e.dim + 31) >> 5;
+  // a row range starts on a slice boundary (callers split at multiples of 32 rows)
+  const long long r_end = a.out_last > 0 ? a.out_last : e.dim;
+  const long long nslices = (r_end + 31) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long sl = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < nslices; sl += nwarps) {
+  for (long long sl = (a.out_first >> 5) + (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5); sl < nslices;
+       sl += nwarps) {
     const long long r = sl * 32 + lane;
-    if (r >= e.dim) continue;
+    if (r >= r_end) continue;
     const long long base = e.slice_ptr[sl] + lane;
     const int len = e.slice_len[sl];
     TG acc[K];
@@ -238,7 +241,8 @@ int launch_ell_typed(const EllDevice& e, const MatvecArgs& a, cudaStream_t s) {
   DH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   DH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFastThreads, smem));
   DH_CHECK(per_sm >= 1, DH_ERR_UNSUPPORTED, "stored-element product: %d bytes of shared memory do not fit", smem);
-  long long need = ((e.dim + 31) / 32 * 32 + kFastThreads - 1) / kFastThreads;
+  const long long r_end = a.out_last > 0 ? a.out_last : e.dim;
+  long long need = ((r_end + 31) / 32 * 32 - (a.out_first & ~31ll) + kFastThreads - 1) / kFastThreads;
   long long grid = (long long)sms * per_sm;
   if (need < grid) grid = need;
   if (grid < 1) grid = 1;

@@ -110,7 +110,8 @@ __global__ void __launch_bounds__(kMatvecThreads) fqhe_matvec_kernel(FqheDevice 
   const TG* x = static_cast<const TG*>(a.x);
   const uint64_t full = (f.lz_max >= 63) ? ~0ull : ((1ull << (f.lz_max + 1)) - 1ull);
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+  const long long r_end = a.out_last > 0 ? a.out_last : f.dim;
+  for (long long r = a.out_first + (long long)blockIdx.x * blockDim.x + threadIdx.x; r < r_end; r += stride) {
     const uint64_t s = __ldg(f.words + r);
     TG acc[K];
 #pragma unroll
@@ -383,7 +384,8 @@ __global__ void __launch_bounds__(kMatvecThreads, kSplitMinBlocks)
   __syncthreads();
   const TG* x = static_cast<const TG*>(a.x);
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+  const long long r_end = a.out_last > 0 ? a.out_last : f.dim;
+  for (long long r = a.out_first + (long long)blockIdx.x * blockDim.x + threadIdx.x; r < r_end; r += stride) {
     TG acc[K];
 #pragma unroll
     for (int j = 0; j < K; ++j) acc[j] = TG(0);
@@ -490,7 +492,8 @@ int launch_one(const FqheDevice& f, const MatvecArgs& a, cudaStream_t s) {
     set_error("fqhe matvec: %d bytes of shared memory per block do not fit", lay.total);
     return DH_ERR_UNSUPPORTED;
   }
-  long long need = (f.dim + kMatvecThreads - 1) / kMatvecThreads;
+  const long long rows = (a.out_last > 0 ? a.out_last : f.dim) - a.out_first;
+  long long need = (rows + kMatvecThreads - 1) / kMatvecThreads;
   long long grid = (long long)sms * per_sm;
   if (need < grid) grid = need;
   if (grid < 1) grid = 1;

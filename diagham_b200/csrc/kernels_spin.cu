@@ -135,7 +135,8 @@ __global__ void __launch_bounds__(kSpinThreads) spin_j1j2_kernel(SpinDevice sp, 
   const TG hj1 = (TG)(0.5 * sp.j1), hj2 = (TG)(0.5 * sp.j2);
   const TG* x = static_cast<const TG*>(a.x);
   const int stride = gridDim.x * blockDim.x;
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < D; r += stride) {
+  const int r_end = a.out_last > 0 ? (int)a.out_last : D;
+  for (int r = (int)a.out_first + blockIdx.x * blockDim.x + threadIdx.x; r < r_end; r += stride) {
     const uint32_t w = __ldg(sp.words + r);
     const uint32_t rot1 = ((w >> 1) | (w << (L - 1))) & maskL;  // bit j = spin j+1 (mod L)
     const uint32_t rot2 = ((w >> 2) | (w << (L - 2))) & maskL;  // bit j = spin j+2 (mod L)
@@ -244,7 +245,8 @@ __global__ void __launch_bounds__(kSpinThreads) spin_j1j2_range_kernel(SpinDevic
   const long long D = sp.dim;
   const TG* x = static_cast<const TG*>(a.x);
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < D; r += stride) {
+  const long long r_end = a.out_last > 0 ? a.out_last : D;
+  for (long long r = a.out_first + (long long)blockIdx.x * blockDim.x + threadIdx.x; r < r_end; r += stride) {
     const uint32_t w = sp.words[r];
     for (int q = 0; q < a.nbr_vectors; ++q) {
       double acc = 0.0, diag = a.shift;
@@ -330,7 +332,7 @@ int launch_spin_typed(const SpinDevice& sp, MatvecArgs a, cudaStream_t s) {
   int dev = 0, sms = 0;
   DH_CUDA(cudaGetDevice(&dev));
   DH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  long long need = (sp.dim + kSpinThreads - 1) / kSpinThreads;
+  long long need = ((a.out_last > 0 ? a.out_last : sp.dim) - a.out_first + kSpinThreads - 1) / kSpinThreads;
   const bool range = (a.col_first > 0 || a.col_last < sp.dim);
   if (range) {
     long long grid = need < (long long)sms * 8 ? need : (long long)sms * 8;
