@@ -393,6 +393,76 @@ def spin_chain_product(dh, flush, steps=5, k=2, length=32, warmup=2):
 
 
 
+def boson_product(dh, flush, steps=5, k=4, warmup=2):
+    """BosonOnSphereShort N=12, 2S=22, 2Lz=0 (dimension 7,764,392, the size of the fermion sector
+    above), LLL Coulomb V_m with the odd m set to zero: FP32 block products of k vectors, their
+    algorithmic bytes (basis word, FP64 y, one FP32 x gather per off-diagonal element and per row)
+    and, on rank 0, the reference's own CPU product of the same sector on a row sample."""
+    import torch
+    n, s = 12, 22
+    v = dh.coulomb_pseudopotentials(s)
+    v[1::2] = 0.0
+    t0 = time.perf_counter()
+    sp = dh.BosonOnSphereShort(n, 0, s)
+    H = dh.ParticleOnSphereGenericHamiltonian(sp, n, s, v)
+    H.set_precision("fp32")
+    dim = sp.dim
+    setup = time.perf_counter() - t0
+    x = torch.empty(dim, k, dtype=torch.float64, device="cuda")
+    x.uniform_(-1.0, 1.0)
+    y = torch.empty_like(x)
+    for _ in range(warmup):
+        flush.zero_()
+        H.block_multiply(x, y)
+    ms = []
+    for _ in range(steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        H.block_multiply(x, y)
+        b.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    moves = H.count_elements()
+    off = moves - H.count_diagonal_elements()
+    alg = dim * 8 + k * dim * 8 + k * (off + dim) * 4
+    mean_s = statistics.mean(ms) / 1000.0
+    peak, kind = peaks()
+    del x, y, H, sp
+    torch.cuda.empty_cache()
+    return {"workload": "BosonOnSphereShort N=%d 2S=%d 2Lz=0 (dim %d), Coulomb V_m even m, FP32 block k=%d"
+                        % (n, s, dim, k),
+            "setup_seconds": setup, "mean_launch_ms": mean_s * 1000.0, "hv_per_s": k / mean_s,
+            "elements_per_product": moves, "off_diagonal_elements": off, "algorithmic_bytes_per_launch": alg,
+            "roofline": {"bound": "hbm", "achieved": alg / mean_s / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / mean_s / 1e9 / peak, "peak_kind": kind}}
+
+
+def reference_cpu_bosons(rows_target_s=6.0):
+    """The reference's own SMP product on the boson sector of boson_product (oracle/_ref/ref_tool
+    bench_bqhe: BosonOnSphereShort + ParticleOnSphereGenericHamiltonian, all host threads; its
+    hermitian mode is not implemented for bosons) over a row sample."""
+    import tempfile
+    import diagham_b200 as dh
+    if not os.path.exists(REF_TOOL):
+        return None
+    threads = os.cpu_count() or 1
+    v = dh.coulomb_pseudopotentials(22)
+    v[1::2] = 0.0
+    with tempfile.TemporaryDirectory() as tmp:
+        vf = os.path.join(tmp, "v.bin")
+        v.tofile(vf)
+        # about 170 us of one thread per row (measured on x86 hosts)
+        rows = int(min(7764392, max(2000, rows_target_s * threads / 170e-6)))
+        cmd = [REF_TOOL, "bench_bqhe", 12, 22, 0, vf, threads, 1, 0, rows]
+        out = subprocess.run([str(c) for c in cmd], check=True, capture_output=True, text=True)
+        r = json.loads([l for l in out.stdout.splitlines() if l.startswith("{")][-1])
+    per_matvec = r["mean_s"] * r["dim"] / r["rows"]
+    return {"value": 1.0 / per_matvec, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": "first %d of %d rows per product, SMP %d threads" % (r["rows"], r["dim"], threads),
+            "seconds_per_sample": r["mean_s"]}
+
+
 def stored_elements(dh, H, flush, dim):
     """The stored-element (fast multiplication) form of the sector's product: build time and size,
     device time per product next to the on-the-fly form, and the autotuner's choice between them."""
@@ -574,7 +644,7 @@ def run_b200(args, world, rank, local):
     e2e_s = reduce_max(time.perf_counter() - t0, world)
     e2e_value = world * BLOCK * e2e_steps / e2e_s
 
-    tte = tte_c = spin = grads = stored = None
+    tte = tte_c = spin = grads = stored = bosons = None
     if not args.no_solve:
         stored = stored_elements(dh, H, flush, dim)
         H.autotune(block_size=BLOCK, repeats=3)
@@ -584,6 +654,7 @@ def run_b200(args, world, rank, local):
         del xb, yb, hx, hy
         torch.cuda.empty_cache()
         spin = spin_chain_product(dh, flush)
+        bosons = boson_product(dh, flush)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -606,9 +677,15 @@ def run_b200(args, world, rank, local):
             "time_to_e0_all_sectors": tte_c,
             "gradients": grads,
             "stored_elements": stored,
-            "spin_chain_l32": spin}
+            "spin_chain_l32": spin,
+            "bosons": bosons}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
+        if bosons is not None:
+            try:
+                bosons["cpu_baseline"] = reference_cpu_bosons()
+            except (subprocess.CalledProcessError, OSError, ValueError, IndexError) as e:
+                bosons["cpu_baseline"] = {"unavailable": str(e)}
     if rank == 0:
         print(json.dumps(line))
 

@@ -72,6 +72,7 @@ SIGNATURES = {
     "dh_hamiltonian_get_interaction_factors": ([_vp, _vp, _c_int, _ip], _c_int),
     "dh_hamiltonian_pseudopotential_adjoint_static": ([_vp, _vp, _vp, _vp], _c_int),
     "dh_hamiltonian_count_elements": ([_vp, _i64p], _c_int),
+    "dh_hamiltonian_count_diagonal_elements": ([_vp, _i64p], _c_int),
     "dh_lanczos_create": ([_vp, _c_int, _c_int, _c_int, _c_int, _vp], _c_int),
     "dh_lanczos_destroy": ([_vp], _c_int),
     "dh_lanczos_set_eigenvalue_precision": ([_vp, _c_dbl], _c_int),
@@ -336,6 +337,12 @@ class _Hamiltonian:
         """Elements one product generates (moves incl. diagonal ones; spin flips)."""
         t = ctypes.c_int64(0)
         _check(_lib.dh_hamiltonian_count_elements(self._handle, ctypes.byref(t)))
+        return t.value
+
+    def count_diagonal_elements(self):
+        """Of count_elements(), those that return to their own row."""
+        t = ctypes.c_int64(0)
+        _check(_lib.dh_hamiltonian_count_diagonal_elements(self._handle, ctypes.byref(t)))
         return t.value
 
     def MatrixElement(self, v1, v2):

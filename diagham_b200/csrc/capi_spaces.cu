@@ -1101,16 +1101,43 @@ int dh_hamiltonian_count_elements(dh_hamiltonian_t h, int64_t* total) {
     *total = (int64_t)llround(2.0 * (double)L * frac * (double)sp->dim);
     return DH_OK;
   }
-  DH_CHECK(h->kind == SPACE_FERMION, DH_ERR_UNSUPPORTED, "element counts are implemented for fermions and spins");
   DevBuf t;
   int rc;
-  if ((rc = t.alloc(sizeof(unsigned long long))) != DH_OK) return rc;
-  if ((rc = launch_fqhe_count(fqhe_device(sp, h, DH_PRECISION_FP64), t.as<unsigned long long>(), h->stream)) != DH_OK)
-    return rc;
+  if ((rc = t.alloc(2 * sizeof(unsigned long long))) != DH_OK) return rc;
+  if (h->kind == SPACE_BOSON)
+    rc = launch_boson_count(fqhe_device(sp, h, DH_PRECISION_FP64), t.as<unsigned long long>(), h->stream);
+  else
+    rc = launch_fqhe_count(fqhe_device(sp, h, DH_PRECISION_FP64), t.as<unsigned long long>(), h->stream);
+  if (rc != DH_OK) return rc;
   unsigned long long v = 0;
   DH_CUDA(cudaMemcpyAsync(&v, t.ptr, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
   DH_CUDA(cudaStreamSynchronize(h->stream));
   *total = (int64_t)v;
+  return DH_OK;
+}
+
+int dh_hamiltonian_count_diagonal_elements(dh_hamiltonian_t h, int64_t* total) {
+  DH_CHECK(h && total, DH_ERR_ARGUMENT, "null argument");
+  dh_space_s* sp = h->space;
+  if (h->kind == SPACE_SPIN12) {
+    *total = 0;  // the chain's elements are its flips; the Sz Sz part is computed per row
+    return DH_OK;
+  }
+  if (h->kind == SPACE_FERMION) {
+    // every occupied pair m1 > m2 has one move back to its row (m3 = m1, m4 = m2)
+    const long long n = sp->nbr_fermions;
+    *total = (int64_t)(n * (n - 1) / 2) * sp->dim;
+    return DH_OK;
+  }
+  DevBuf t;
+  int rc;
+  if ((rc = t.alloc(2 * sizeof(unsigned long long))) != DH_OK) return rc;
+  if ((rc = launch_boson_count(fqhe_device(sp, h, DH_PRECISION_FP64), t.as<unsigned long long>(), h->stream)) != DH_OK)
+    return rc;
+  unsigned long long v[2] = {0, 0};
+  DH_CUDA(cudaMemcpyAsync(v, t.ptr, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+  DH_CUDA(cudaStreamSynchronize(h->stream));
+  *total = (int64_t)v[1];
   return DH_OK;
 }
 

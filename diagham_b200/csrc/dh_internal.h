@@ -173,6 +173,8 @@ int launch_fqhe_unrank(int nbr_fermions, int lz_max, int total_sum, long long di
 int launch_fqhe_matvec(const FqheDevice& f, const MatvecArgs& a, int precision, cudaStream_t s);
 // BosonOnSphereShort product (kernels_boson.cu), any vector layout, K = 1, 2, 4 (else in passes)
 int launch_boson_matvec(const FqheDevice& f, const MatvecArgs& a, int precision, cudaStream_t s);
+// total[0] = generated elements, total[1] = those that return to their row (one per annihilated pair)
+int launch_boson_count(const FqheDevice& f, unsigned long long* total, cudaStream_t s);
 int launch_fqhe_row_elements(const FqheDevice& f, long long row, int* targets, int* signs, int* factor_index,
                              int cap, int* count, cudaStream_t s);
 int launch_fqhe_bins(const FqheDevice& f, const double* u, const double* v, double* partial_bins, int nblocks,

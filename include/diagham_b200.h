@@ -107,7 +107,7 @@ int dh_space_set_index_mode(dh_space_t space, int mode);
  * (FQHESphereFermionsTwoBodyGeneric.cc:395-396).  On a BosonOnSphereShort space the factors are the
  * reference's bosonic ones (:620-806: pairs m1 >= m2, even relative angular momenta, weights 4, 2 and
  * 1) and the product applies AA / AdAd with their occupation square roots (BosonOnSphereShort.cc:
- * 353, 431); bosonic Hamiltonians have no L^2 term, stored elements, element counts or adjoint. */
+ * 353, 431); bosonic Hamiltonians have no L^2 term, stored elements or adjoint. */
 int dh_particle_on_sphere_generic_hamiltonian_create(dh_space_t space, int nbr_particles, int lz_max,
                                                      const double* pseudopotentials, double l2_factor,
                                                      dh_hamiltonian_t* out);
@@ -216,6 +216,12 @@ int dh_hamiltonian_pseudopotential_adjoint(dh_hamiltonian_t h, const double* u, 
 /* Number of elements (a+a+aa moves, diagonal ones included; spin flips for the chain) that one
  * product generates over all rows, counted on the GPU. */
 int dh_hamiltonian_count_elements(dh_hamiltonian_t h, int64_t* total);
+
+/* Of those, the elements whose target is their own row (one per annihilated pair for FQHE spaces:
+ * C(N, 2) per row for fermions, the number of pairs a_m1 a_m2 can empty for bosons; 0 for the chain,
+ * whose elements are its flips).  count_elements - this = the off-diagonal elements, the gathers
+ * of distinct targets in the algorithmic byte count.  No reference counterpart. */
+int dh_hamiltonian_count_diagonal_elements(dh_hamiltonian_t h, int64_t* total);
 
 /* Same result as dh_hamiltonian_pseudopotential_adjoint, for callers that cannot allocate device
  * memory: code running inside a CUDA stream capture, or applications whose framework owns all

@@ -449,6 +449,7 @@ static void Usage()
 	  "  spin_matvec L 2Sz J1 J2 xfile out\n"
 	  "  spin_lanczos L 2Sz J1 J2 algo nev block maxiter precision out x0 [x1 ...]\n"
 	  "  bench_fqhe N 2S 2Lz vfile threads reps hermitian [rows]\n"
+	  "  bench_bqhe N 2S 2Lz vfile threads reps hermitian [rows]\n"
 	  "  bench_spin L 2Sz J1 J2 threads reps 0\n");
   exit(1);
 }
@@ -772,8 +773,9 @@ int main(int argc, char** argv)
       RunLanczosLoop(&H, Arch, Algo, Nev, Block, MaxIter, Precision, Init, NbrInitial, argv[11], 0);
       return 0;
     }
-  if (strcmp(Cmd, "bench_fqhe") == 0 && (argc == 9 || argc == 10))
+  if ((strcmp(Cmd, "bench_fqhe") == 0 || strcmp(Cmd, "bench_bqhe") == 0) && (argc == 9 || argc == 10))
     {
+      // bench_bqhe: the same with BosonOnSphereShort
       // times the reference SMP matvec: VectorHamiltonianMultiplyOperation on SMPArchitecture
       // (VectorHamiltonianMultiplyOperation.cc:241-320), on-the-fly (memory 0) as with -m 0.
       // An optional row count bounds the sample: the architecture's typical range (the rows the
@@ -785,14 +787,19 @@ int main(int argc, char** argv)
       int Reps = atoi(argv[7]);
       bool Hermitian = atoi(argv[8]) != 0;
       double ts = Now();
-      FermionOnSphere Space(N, TotalLz, LzMax, 9ul << 20);
+      ParticleOnSphere* SpacePtr;
+      if (strcmp(Cmd, "bench_bqhe") == 0)
+	SpacePtr = new BosonOnSphereShort(N, TotalLz, LzMax);
+      else
+	SpacePtr = new FermionOnSphere(N, TotalLz, LzMax, 9ul << 20);
+      ParticleOnSphere& Space = *SpacePtr;
       SMPArchitecture Arch(Threads);
       long Dim = Space.GetHilbertSpaceDimension();
       long Rows = (argc == 10) ? atol(argv[9]) : Dim;
       if (Rows <= 0 || Rows > Dim)
 	Rows = Dim;
       Arch.SetDimension(Rows);
-      ParticleOnSphereGenericHamiltonian H(&Space, N, LzMax, V, 0.0, &Arch, 0, false, 0, Hermitian);
+      ParticleOnSphereGenericHamiltonian H(SpacePtr, N, LzMax, V, 0.0, &Arch, 0, false, 0, Hermitian);
       double tsetup = Now() - ts;
       RealVector X(Dim, true), Y(Dim, true);
       for (long i = 0; i < Dim; ++i)

@@ -130,3 +130,26 @@ def test_boson_errors(gpu, orc):
     x = orc.random_vector(1, sp.dim)
     ref = orc.BosonFQHE(6, 10, 0, v2).pull(x)
     assert np.max(np.abs(H.LowLevelMultiply(x) - ref)) <= 1e-13 * np.max(np.abs(ref))
+
+
+def test_boson_element_counts(gpu):
+    # moves per row: every pair m1 >= m2 that a_m1 a_m2 can empty, times its creations m3 >= m4, one of
+    # which (m3 = m1) returns to the row
+    z, sp, H = _setup(gpu, "boson_n7_2s12_lz2_coulomb.npz")
+    L = 12
+    moves = diag = 0
+    for row in z["occupations"]:
+        for m1 in range(L + 1):
+            if row[m1] == 0:
+                continue
+            for m2 in range(m1 + 1):
+                if row[m2] == 0 or (m2 == m1 and row[m1] < 2):
+                    continue
+                M = m1 + m2
+                moves += min(M, L) - (M + 1) // 2 + 1
+                diag += 1
+    assert H.count_elements() == moves
+    assert H.count_diagonal_elements() == diag
+    f = gpu.FermionOnSphere(7, 2, 18)
+    Hf = gpu.ParticleOnSphereGenericHamiltonian(f, 7, 18, gpu.coulomb_pseudopotentials(18))
+    assert Hf.count_diagonal_elements() == 21 * f.dim
