@@ -50,6 +50,9 @@ SIGNATURES = {
     "dh_space_get_states": ([_vp, _vp, _vp, _c_i64, _c_i64], _c_int),
     "dh_space_find_state_index": ([_vp, _vp, _c_i64, _vp], _c_int),
     "dh_space_set_index_mode": ([_vp, _c_int], _c_int),
+    "dh_fermion_on_sphere_partial_entanglement_matrix": ([_vp, _vp, _c_int, _c_int, _c_int, _vp, _c_i64, _i64p, _i64p],
+                                                         _c_int),
+    "dh_fermion_on_sphere_partial_density_matrix": ([_vp, _vp, _c_int, _c_int, _c_int, _vp, _c_i64, _i64p], _c_int),
     "dh_particle_on_sphere_generic_hamiltonian_create": ([_vp, _c_int, _c_int, _vp, _c_dbl, _vp], _c_int),
     "dh_particle_on_sphere_l2_hamiltonian_create": ([_vp, _c_int, _c_int, _c_int, _c_dbl, _vp], _c_int),
     "dh_spin_chain_j1j2_hamiltonian_create": ([_vp, _c_dbl, _c_dbl, _vp], _c_int),
@@ -218,6 +221,28 @@ class FermionOnSphere(_Space):
         _check(_lib.dh_fermion_on_sphere_create(nbr_fermions, total_lz, lz_max, memory, ctypes.byref(h)))
         self._handle = h
         self.nbr_fermions, self.total_lz, self.lz_max = nbr_fermions, total_lz, lz_max
+
+    def EvaluatePartialEntanglementMatrix(self, subsystem_size, nbr_fermion_sector, lz_sector, state):
+        """M[a][b] of the orbital cut at subsystem_size (FermionOnSphere.cc:2474), (rows, cols)."""
+        return _cut_matrix(self, _lib.dh_fermion_on_sphere_partial_entanglement_matrix, state,
+                           (subsystem_size, nbr_fermion_sector, lz_sector), False)
+
+    def EvaluatePartialDensityMatrix(self, subsystem_size, nbr_fermion_sector, lz_sector, state):
+        """rho_A = M M^T of the orbital cut (FermionOnSphere.cc:2070)."""
+        return _cut_matrix(self, _lib.dh_fermion_on_sphere_partial_density_matrix, state,
+                           (subsystem_size, nbr_fermion_sector, lz_sector), True)
+
+
+def _cut_matrix(space, fn, state, args, square):
+    b = _Buf(state)
+    r, c = ctypes.c_int64(0), ctypes.c_int64(0)
+    sizes = (ctypes.byref(r),) if square else (ctypes.byref(r), ctypes.byref(c))
+    _check(fn(space._handle, b.ptr, *args, None, 0, *sizes))
+    rows, cols = r.value, (r.value if square else c.value)
+    out = np.zeros((rows, cols), np.float64)
+    if out.size:
+        _check(fn(space._handle, b.ptr, *args, out.ctypes.data, out.size, *sizes))
+    return out
 
 
 class BosonOnSphereShort(_Space):

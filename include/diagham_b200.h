@@ -96,6 +96,27 @@ int dh_space_find_state_index(dh_space_t space, const uint64_t* words, int64_t n
 /* Selects DH_INDEX_RANK or DH_INDEX_LOOKUP for every kernel that uses this space. */
 int dh_space_set_index_mode(dh_space_t space, int mode);
 
+/* FermionOnSphere::EvaluatePartialEntanglementMatrix(subsytemSize, nbrFermionSector, lzSector, state)
+ * (FermionOnSphere.cc:2474): the orbital cut A = orbitals 0..subsystem_size-1 of state (host or device,
+ * the space's dimension), M[a][b] = component of the basis state a (x) b in the sector of N_A =
+ * nbr_fermion_sector fermions and 2 Lz_A = lz_sector in A, rows in the order of FermionOnSphere(N_A,
+ * lz_sector, subsystem_size - 1), columns in that of the complement's FermionOnSphere(N - N_A, .,
+ * 2S - subsystem_size).  *rows x *cols (0 x 0 for an empty sector); the matrix is written row-major
+ * into matrix (host or device) when it is not NULL and capacity >= rows * cols, so a first call with
+ * matrix = NULL gives the size.  subsystem_size <= 0 and > 2S follow the reference (1 x 1 [1]; the state
+ * as one column). */
+int dh_fermion_on_sphere_partial_entanglement_matrix(dh_space_t space, const double* state, int subsystem_size,
+                                                     int nbr_fermion_sector, int lz_sector, double* matrix,
+                                                     int64_t capacity, int64_t* rows, int64_t* cols);
+
+/* FermionOnSphere::EvaluatePartialDensityMatrix (FermionOnSphere.cc:2070): rho_A = M M^T of the same
+ * cut, *dim x *dim row-major (empty when no basis state lies in the sector).  As in the reference,
+ * N_A <= 1 gives the 1 x 1 weight of the states whose A part is empty (N_A = 0) or the single orbital
+ * (lz_sector + subsystem_size - 1) / 2 (N_A = 1). */
+int dh_fermion_on_sphere_partial_density_matrix(dh_space_t space, const double* state, int subsystem_size,
+                                                int nbr_fermion_sector, int lz_sector, double* matrix, int64_t capacity,
+                                                int64_t* dim);
+
 /* ================================================================ Hamiltonians */
 
 /* ParticleOnSphereGenericHamiltonian(particles, nbrParticles, lzmax, pseudoPotential, l2Factor, ...):

@@ -448,3 +448,32 @@ def read_lanczos_state(b, fmt):
     assert upper.size == nbr_row - 1
     return dict(index=index, ground_flag=flag, prev_last=float(prev), precision=float(prec), nbr_eigenvalue=nev,
                 nbr_row=nbr_row, diag=diag, upper=upper)
+
+
+def entanglement_matrix(n, two_s, total_lz, x, l, na, lza):
+    """The orbital-cut entanglement matrix of FermionOnSphere::EvaluatePartialEntanglementMatrix
+    (FermionOnSphere.cc:2474) restated with the oracle's bases: A = orbitals 0..l-1 in the sector
+    (na, lza), rows in FermionOnSphere(na, lza, l - 1) order, columns in the complement's order, M[a][b]
+    = x of the state a | (b << l).  Regular cuts only (0 < l <= 2S)."""
+    words, _ = fermion_basis(n, two_s, total_lz)
+    nb = n - na
+    sum_a = (lza + na * (l - 1)) // 2  # floored, as the reference does (FermionOnSphere.cc:2095)
+    lza = 2 * sum_a - na * (l - 1)
+    sum_b = (total_lz + n * two_s) // 2 - sum_a
+    if na > l or nb > two_s + 1 - l or not (na * (na - 1) // 2 <= sum_a <= na * (l - 1) - na * (na - 1) // 2):
+        return np.zeros((0, 0))
+    if not (l * nb + nb * (nb - 1) // 2 <= sum_b <= nb * two_s - nb * (nb - 1) // 2):
+        return np.zeros((0, 0))
+    a_words = fermion_basis(na, l - 1, lza)[0] if na > 0 else np.zeros(1, np.uint64)
+    lz_b = 2 * (sum_b - nb * l) - nb * (two_s - l)
+    b_words = fermion_basis(nb, two_s - l, lz_b)[0] if nb > 0 else np.zeros(1, np.uint64)
+    ra = {int(w): i for i, w in enumerate(a_words)}
+    rb = {int(w): i for i, w in enumerate(b_words)}
+    m = np.zeros((len(a_words), len(b_words)))
+    mask = (1 << l) - 1
+    for i, w in enumerate(words):
+        w = int(w)
+        a, b = w & mask, w >> l
+        if a in ra and b in rb:
+            m[ra[a], rb[b]] = x[i]
+    return m

@@ -42,6 +42,8 @@
 #include "LanczosAlgorithm/BasicLanczosAlgorithmWithDiskStorage.h"
 #include "LanczosAlgorithm/BasicLanczosAlgorithmWithGroundStateDiskStorage.h"
 #include "Matrix/RealTriDiagonalSymmetricMatrix.h"
+#include "Matrix/RealMatrix.h"
+#include "Matrix/RealSymmetricMatrix.h"
 #include "Tools/FQHESpectrum/PseudoPotentials.h"
 #include "Vector/RealVector.h"
 #include "MathTools/Complex.h"
@@ -440,6 +442,8 @@ static void Usage()
 	  "  fqhe_lanczos N 2S 2Lz vfile algo nev block maxiter precision out gsout x0 [x1 ...]\n"
 	  "  fqhe_lanczos_disk N 2S 2Lz vfile algo nbriter precision dir x0|resume gsiter out gsout\n"
 	  "  fqhe_expect N 2S 2Lz vfile psifile out\n"
+	  "  fqhe_entanglement N 2S 2Lz xfile l NA 2LzA out\n"
+	  "  fqhe_density N 2S 2Lz xfile l NA 2LzA out\n"
 	  "  bqhe_basis N 2S 2Lz out\n"
 	  "  bqhe_matvec N 2S 2Lz vfile xfile shift out\n"
 	  "  bqhe_lanczos N 2S 2Lz vfile algo nev block maxiter precision out gsout x0 [x1 ...]\n"
@@ -601,6 +605,47 @@ int main(int argc, char** argv)
 	Init[i].ReadVector(argv[13 + i]);
       RunLanczosLoop(&H, Arch, Algo, Nev, Block, MaxIter, Precision, Init, NbrInitial, argv[11],
 		     strcmp(argv[12], "-") == 0 ? 0 : argv[12]);
+      return 0;
+    }
+  // orbital-cut entanglement of a vector (FermionOnSphere.cc:2070, :2474); layout: int64 rows, int64
+  // columns, then the matrix row by row (a density matrix is written in full, rows = columns)
+  if ((strcmp(Cmd, "fqhe_entanglement") == 0 || strcmp(Cmd, "fqhe_density") == 0) && argc == 10)
+    {
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      int Cut = atoi(argv[6]), NA = atoi(argv[7]), LzA = atoi(argv[8]);
+      FermionOnSphere Space(N, TotalLz, LzMax, 9ul << 20);
+      RealVector X;
+      X.ReadVector(argv[5]);
+      FILE* f = OpenOut(argv[9]);
+      if (strcmp(Cmd, "fqhe_entanglement") == 0)
+	{
+	  RealMatrix M = Space.EvaluatePartialEntanglementMatrix(Cut, NA, LzA, X);
+	  long Rows = M.GetNbrRow(), Columns = M.GetNbrColumn();
+	  fwrite(&Rows, sizeof(long), 1, f);
+	  fwrite(&Columns, sizeof(long), 1, f);
+	  for (long i = 0; i < Rows; ++i)
+	    for (long j = 0; j < Columns; ++j)
+	      {
+		double Tmp;
+		M.GetMatrixElement(i, j, Tmp);
+		fwrite(&Tmp, sizeof(double), 1, f);
+	      }
+	}
+      else
+	{
+	  RealSymmetricMatrix Rho = Space.EvaluatePartialDensityMatrix(Cut, NA, LzA, X);
+	  long Rows = Rho.GetNbrRow();
+	  fwrite(&Rows, sizeof(long), 1, f);
+	  fwrite(&Rows, sizeof(long), 1, f);
+	  for (long i = 0; i < Rows; ++i)
+	    for (long j = 0; j < Rows; ++j)
+	      {
+		double Tmp;
+		Rho.GetMatrixElement(i, j, Tmp);
+		fwrite(&Tmp, sizeof(double), 1, f);
+	      }
+	}
+      fclose(f);
       return 0;
     }
   // bosons: BosonOnSphereShort with the same Hamiltonian class (its bosonic factors and AA / AdAd)

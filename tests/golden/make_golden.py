@@ -335,6 +335,37 @@ def boson_fixtures(tmp):
              occupations=occ, max_iter=300, **ys, **read_lanczos(lf))
 
 
+ENTANGLEMENT_CASES = [(11, 4, 0), (11, 4, 2), (11, 3, -3), (5, 2, 0), (1, 1, 0), (1, 0, 0), (0, 0, 0), (11, 0, 0),
+                      (21, 8, 0), (15, 8, 56), (20, 7, -5), (22, 8, 0)]
+
+
+def entanglement_fixtures(tmp):
+    # FermionOnSphere::EvaluatePartialEntanglementMatrix / EvaluatePartialDensityMatrix (orbital cut l,
+    # nbrFermionSector NA, lzSector 2LzA) of x = the splitmix64 vector of seed 0 on N=8 2S=21 2Lz=0;
+    # rho is stored for the cases with at most 600 rows (M M^T is checked against it)
+    def rd(path):
+        b = open(path, "rb").read()
+        r, c = np.frombuffer(b[:16], np.int64)
+        return np.frombuffer(b[16:], np.float64).reshape(r, c).copy()
+    n, s, lz = 8, 21, 0
+    bf = os.path.join(tmp, "b.bin")
+    run("fqhe_basis", n, s, lz, bf)
+    dim, _, _ = read_basis(bf)
+    xf = os.path.join(tmp, "xe.vec")
+    write_vector(xf, splitmix_vector(0, dim))
+    out, cmds = {}, []
+    for (l, na, lza) in ENTANGLEMENT_CASES:
+        tag = "l%d_na%d_lz%d" % (l, na, lza)
+        ef, df = os.path.join(tmp, "e.bin"), os.path.join(tmp, "d.bin")
+        cmds.append(run("fqhe_entanglement", n, s, lz, xf, l, na, lza, ef))
+        out["m_" + tag] = rd(ef)
+        if l <= s and out["m_" + tag].shape[0] <= 600:
+            run("fqhe_density", n, s, lz, xf, l, na, lza, df)
+            out["rho_" + tag] = rd(df)
+    save("entanglement_n%d_2s%d_lz%d.npz" % (n, s, lz), cmds[0] + " (and fqhe_density, per case)", seed=0,
+         cases=np.array(ENTANGLEMENT_CASES, np.int32), **out)
+
+
 def dir_files(d):
     names = sorted(os.listdir(d))
     return np.array(names), {"f%d" % i: np.frombuffer(open(os.path.join(d, f), "rb").read(), np.uint8)
@@ -419,6 +450,8 @@ def main():
             disk_fixtures(tmp)
         if args.only in (None, "boson"):
             boson_fixtures(tmp)
+        if args.only in (None, "entanglement"):
+            entanglement_fixtures(tmp)
         if args.slow:
             slow_fixtures(tmp)
 

@@ -256,3 +256,21 @@ def test_boson_oracle_matches_reference(orc, name):
     else:
         # the Laughlin state of the delta interaction at 2S = 2 (N - 1): E0 = 0
         assert abs(e_ref) < 1e-12
+
+
+def test_entanglement_oracle_matches_reference(orc):
+    # FermionOnSphere::EvaluatePartialEntanglementMatrix / EvaluatePartialDensityMatrix of a vector on
+    # N=8 2S=21 2Lz=0: the oracle's M equals the reference's for every regular cut, and the reference's
+    # rho is M M^T
+    z = golden("entanglement_n8_2s21_lz0.npz")
+    x = orc.random_vector(int(z["seed"]), 8512)
+    for l, na, lza in z["cases"]:
+        tag = "l%d_na%d_lz%d" % (l, na, lza)
+        ref = z["m_" + tag]
+        if 0 < l <= 21:
+            m = orc.entanglement_matrix(8, 21, 0, x, int(l), int(na), int(lza))
+            assert m.shape == ref.shape, tag
+            # the start vector's normalisation may differ in the last bit between generators
+            assert m.size == 0 or np.max(np.abs(m - ref)) <= 1e-15, tag
+        if "rho_" + tag in z.files and ref.size and na > 1:
+            assert np.max(np.abs(ref @ ref.T - z["rho_" + tag])) < 1e-15, tag
