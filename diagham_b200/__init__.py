@@ -8,6 +8,8 @@ diagham_b200/_build.py).  Class and method names follow the reference classes th
     Spin1_2Chain                        Spin/src/HilbertSpace/Spin1_2Chain.h
     ParticleOnSphereGenericHamiltonian  FQHE/src/Hamiltonian/ParticleOnSphereGenericHamiltonian.h
     SpinChainJ1J2Hamiltonian            (J1-J2 pattern of SpinChainJ1J2RealHamiltonianWithTranslations on a plain chain)
+    Spin1_2ChainWithTranslations, SpinChainJ1J2RealHamiltonianWithTranslations
+                                        Spin/src/HilbertSpace, Spin/src/Hamiltonian (momentum sectors)
     BasicLanczosAlgorithm, FullReorthogonalizedLanczosAlgorithm, BasicLanczosAlgorithmWithGroundState,
     BasicLanczosAlgorithmWithDiskStorage, BasicLanczosAlgorithmWithGroundStateDiskStorage
                                         src/LanczosAlgorithm/*.h
@@ -45,6 +47,7 @@ SIGNATURES = {
     "dh_fermion_on_sphere_create": ([_c_int, _c_int, _c_int, ctypes.c_ulong, _vp], _c_int),
     "dh_boson_on_sphere_create": ([_c_int, _c_int, _c_int, ctypes.c_ulong, _vp], _c_int),
     "dh_spin12_chain_create": ([_c_int, _c_int, _c_int, _vp], _c_int),
+    "dh_spin12_chain_translations_create": ([_c_int, _c_int, _c_int, _c_int, _vp], _c_int),
     "dh_space_destroy": ([_vp], _c_int),
     "dh_space_get_dimension": ([_vp, _i64p], _c_int),
     "dh_space_get_states": ([_vp, _vp, _vp, _c_i64, _c_i64], _c_int),
@@ -458,6 +461,19 @@ class ParticleOnSphereL2Hamiltonian(_Hamiltonian):
         return 0.5 * (np.sqrt(1.0 + 4.0 * max(l2, 0.0)) - 1.0)
 
 
+class Spin1_2ChainWithTranslations(_Space):
+    """Spin1_2ChainWithTranslations(chainLength, momentum, 1, sz, memory, memorySlice): the momentum
+    sector of the periodic chain (Spin1_2ChainWithTranslations.cc:167); states() gives the
+    representatives (smallest word of each orbit), ascending."""
+
+    def __init__(self, chain_length, momentum, sz, memory=1 << 20):
+        load()
+        h = ctypes.c_void_p()
+        _check(_lib.dh_spin12_chain_translations_create(chain_length, momentum, sz, memory, ctypes.byref(h)))
+        self._handle = h
+        self.chain_length, self.momentum, self.sz = chain_length, momentum, sz
+
+
 class SpinChainJ1J2Hamiltonian(_Hamiltonian):
     """Periodic J1-J2 chain on a plain Spin1_2Chain (element pattern of
     SpinChainJ1J2RealHamiltonianWithTranslations.cc:94-192, API of SpinChainHamiltonian.cc:257)."""
@@ -685,3 +701,14 @@ def eigenstate_file_name(statistics, interaction_name, nbr_particles, lz_max, to
     """<statistics>_<interaction>_n_<N>_2s_<2S>_lz_<2Lz>.<index>.vec, the eigenstate naming of
     FQHE/docs/DataFormat/FermionOnSphere.xml:9-16 (statistics "fermions" or "bosons", total_lz = 2 Lz)."""
     return "%s_%s_n_%d_2s_%d_lz_%d.%d.vec" % (statistics, interaction_name, nbr_particles, lz_max, total_lz, index)
+
+
+class SpinChainJ1J2RealHamiltonianWithTranslations(SpinChainJ1J2Hamiltonian):
+    """SpinChainJ1J2RealHamiltonianWithTranslations(chain, nbrSpin, j1, j2)
+    (SpinChainJ1J2RealHamiltonianWithTranslations.cc:58) on a Spin1_2ChainWithTranslations space,
+    momentum 0 or L / 2."""
+
+    def __init__(self, chain, nbr_spin, j1, j2):
+        if nbr_spin != chain.chain_length:
+            raise ValueError("nbr_spin must be the chain length")
+        super().__init__(chain, j1, j2)

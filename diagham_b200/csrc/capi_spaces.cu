@@ -7,6 +7,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <memory>
 #include <new>
 #include <vector>
 
@@ -181,6 +182,29 @@ FqheDevice fqhe_device(const dh_space_s* sp, const dh_hamiltonian_s* h, int prec
   return f;
 }
 
+TransDevice trans_device(const dh_space_s* sp, const dh_hamiltonian_s* h) {
+  TransDevice d = {};
+  d.reps = sp->words.as<uint32_t>();
+  d.rep_rank = sp->rep_rank.as<int32_t>();
+  d.orbits = sp->rep_orbit.as<uint8_t>();
+  d.map = sp->trans_map.as<unsigned long long>();
+  d.table = sp->trans_table.as<int>();
+  d.table_entries = sp->table_entries;
+  d.table_shift = sp->table_shift;
+  d.dim = sp->dim;
+  d.chain_dim = sp->chain_dim;
+  d.length = sp->length;
+  d.momentum = sp->momentum;
+  // ExponentialTable of the real Hamiltonian: cos(2 pi K m / L) (SpinChainRealHamiltonianWithTranslations.cc:204)
+  const double coef = 2.0 * M_PI / (double)sp->length * (double)sp->momentum;
+  for (int m = 0; m < 32; ++m) d.phase[m] = (m < sp->length) ? cos(coef * (double)m) : 0.0;
+  if (h) {
+    d.j1 = h->j1;
+    d.j2 = h->j2;
+  }
+  return d;
+}
+
 SpinDevice spin_device(const dh_space_s* sp, const dh_hamiltonian_s* h) {
   SpinDevice s = {};
   s.words = sp->words.as<uint32_t>();
@@ -274,6 +298,7 @@ int hamiltonian_apply_rows(dh_hamiltonian_s* h, const double* x, double* y, int 
     a.xdiag = nullptr;
   }
   if (sp->kind == SPACE_BOSON) return launch_boson_matvec(fqhe_device(sp, h, h->precision), a, h->precision, stream);
+  if (sp->kind == SPACE_SPIN12_TRANSLATIONS) return launch_trans_matvec(trans_device(sp, h), a, h->precision, stream);
   if (sp->kind == SPACE_FERMION) {
     if (h->fast && h->fast_use && first == 0 && nbr == dim) return launch_ell_product(ell_device(h, h->precision), a, h->precision, stream);
     if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
@@ -315,6 +340,7 @@ int hamiltonian_apply_block_rows(dh_hamiltonian_s* h, const double* x64, const f
   }
   int rc;
   if (sp->kind == SPACE_BOSON) return launch_boson_matvec(fqhe_device(sp, h, precision), a, precision, stream);
+  if (sp->kind == SPACE_SPIN12_TRANSLATIONS) return launch_trans_matvec(trans_device(sp, h), a, precision, stream);
   if (sp->kind == SPACE_FERMION) {
     if (h->fast && h->fast_use) return launch_ell_product(ell_device(h, precision), a, precision, stream);
     if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
@@ -416,6 +442,72 @@ int dh_boson_on_sphere_create(int nbr_bosons, int total_lz, int lz_max, unsigned
   return DH_OK;
 }
 
+int dh_spin12_chain_translations_create(int chain_length, int momentum, int sz, int memory, dh_space_t* out) {
+  DH_CHECK(out, DH_ERR_ARGUMENT, "null output handle");
+  *out = nullptr;
+  (void)memory;
+  DH_CHECK(chain_length >= 3 && chain_length <= 32, DH_ERR_UNSUPPORTED,
+           "Spin1_2ChainWithTranslations: chain length %d not in 3..32", chain_length);
+  DH_CHECK(((chain_length + sz) & 1) == 0 && sz >= -chain_length && sz <= chain_length, DH_ERR_ARGUMENT,
+           "Spin1_2ChainWithTranslations: sz = %d is not reachable with %d spins", sz, chain_length);
+  DH_CHECK(momentum >= 0 && momentum < chain_length, DH_ERR_ARGUMENT, "momentum %d not in 0..%d", momentum,
+           chain_length - 1);
+  dh_space_s* sp = new (std::nothrow) dh_space_s();
+  DH_CHECK(sp, DH_ERR_MEMORY, "out of host memory");
+  std::unique_ptr<dh_space_s> guard(sp);
+  sp->kind = SPACE_SPIN12_TRANSLATIONS;
+  sp->length = chain_length;
+  sp->sz = sz;
+  sp->nbr_up = (chain_length + sz) / 2;
+  sp->momentum = momentum;
+  sp->index_mode = DH_INDEX_RANK;
+  long long total = 1;
+  for (int q = 1; q <= sp->nbr_up; ++q) total = total * (chain_length - sp->nbr_up + q) / q;
+  sp->chain_dim = total;
+  // representatives in ascending order: per chunk of 1024 words a count, a scan of the counts, then
+  // each chunk writes its representatives at its offset (Spin1_2ChainWithTranslations.cc:167-235)
+  const long long chunks = (total + 1023) / 1024;
+  DevBuf counts, offsets;
+  int rc;
+  if ((rc = counts.alloc(chunks * sizeof(unsigned int))) != DH_OK) return rc;
+  if ((rc = launch_trans_count(total, chain_length, sp->nbr_up, momentum, counts.as<unsigned int>(), 0)) != DH_OK)
+    return rc;
+  std::vector<unsigned int> hc(chunks);
+  DH_CUDA(cudaMemcpy(hc.data(), counts.ptr, chunks * sizeof(unsigned int), cudaMemcpyDeviceToHost));
+  std::vector<long long> ho(chunks);
+  long long dim = 0;
+  for (long long c = 0; c < chunks; ++c) {
+    ho[c] = dim;
+    dim += hc[c];
+  }
+  sp->dim = dim;
+  if (dim > 0) {
+    if ((rc = offsets.alloc(chunks * sizeof(long long))) != DH_OK ||
+        (rc = sp->words.alloc(dim * sizeof(uint32_t))) != DH_OK || (rc = sp->rep_orbit.alloc(dim)) != DH_OK ||
+        (rc = sp->rep_rank.alloc(dim * sizeof(int32_t))) != DH_OK ||
+        (rc = sp->trans_map.alloc(total * sizeof(unsigned long long))) != DH_OK)
+      return rc;
+    DH_CUDA(cudaMemcpy(offsets.ptr, ho.data(), chunks * sizeof(long long), cudaMemcpyHostToDevice));
+    if ((rc = launch_trans_write(total, chain_length, sp->nbr_up, momentum, offsets.as<long long>(),
+                                 sp->words.as<uint32_t>(), sp->rep_orbit.as<uint8_t>(), 0)) != DH_OK)
+      return rc;
+    // lookup over the representatives: at most 2^24 + 2 entries of the top bits
+    uint32_t last = 0;
+    DH_CUDA(cudaMemcpy(&last, sp->words.as<uint32_t>() + (dim - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    const int bits = last ? 32 - __builtin_clz(last) : 1;
+    sp->table_shift = bits > 24 ? bits - 24 : 0;
+    sp->table_entries = (long long)(last >> sp->table_shift) + 2;
+    if ((rc = sp->trans_table.alloc(sp->table_entries * sizeof(int))) != DH_OK) return rc;
+    if ((rc = launch_trans_table(sp->words.as<uint32_t>(), dim, sp->table_shift, sp->table_entries,
+                                 sp->trans_table.as<int>(), 0)) != DH_OK)
+      return rc;
+    if ((rc = launch_trans_map(trans_device(sp, nullptr), total, sp->nbr_up, 0)) != DH_OK) return rc;
+    DH_CUDA(cudaDeviceSynchronize());
+  }
+  *out = guard.release();
+  return DH_OK;
+}
+
 int dh_spin12_chain_create(int chain_length, int sz, int memory, dh_space_t* out) {
   DH_CHECK(out, DH_ERR_ARGUMENT, "null output handle");
   *out = nullptr;
@@ -464,6 +556,12 @@ int dh_space_get_states(dh_space_t sp, uint64_t* words, int* lz_max, int64_t fir
     DH_CUDA(cudaMemcpy(words, sp->words.as<uint64_t>() + first, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
     if (lz_max)
       for (int64_t i = 0; i < n; ++i) lz_max[i] = words[i] ? 63 - __builtin_clzll(words[i]) : 0;
+  } else if (sp->kind == SPACE_SPIN12_TRANSLATIONS) {
+    std::vector<uint32_t> w(n);
+    DH_CUDA(cudaMemcpy(w.data(), sp->words.as<uint32_t>() + first, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < n; ++i) words[i] = w[i];
+    if (lz_max)
+      for (int64_t i = 0; i < n; ++i) lz_max[i] = 0;
   } else {
     std::vector<uint32_t> w(n);
     DH_CUDA(cudaMemcpy(w.data(), sp->words.as<uint32_t>() + first, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
@@ -509,6 +607,8 @@ int dh_space_find_state_index(dh_space_t sp, const uint64_t* words, int64_t n, i
   if (sp->kind == SPACE_FERMION || sp->kind == SPACE_BOSON) {
     if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
     rc = launch_fqhe_find(fqhe_device(sp, nullptr, 0), w, n, reinterpret_cast<long long*>(out), 0);
+  } else if (sp->kind == SPACE_SPIN12_TRANSLATIONS) {
+    rc = launch_trans_find(trans_device(sp, nullptr), w, n, reinterpret_cast<long long*>(out), 0);
   } else {
     rc = launch_spin_find(spin_device(sp, nullptr), w, n, reinterpret_cast<long long*>(out), 0);
   }
@@ -593,12 +693,18 @@ int dh_particle_on_sphere_l2_hamiltonian_create(dh_space_t sp, int nbr_particles
 int dh_spin_chain_j1j2_hamiltonian_create(dh_space_t sp, double j1, double j2, dh_hamiltonian_t* out) {
   DH_CHECK(out, DH_ERR_ARGUMENT, "null output handle");
   *out = nullptr;
-  DH_CHECK(sp && sp->kind == SPACE_SPIN12, DH_ERR_ARGUMENT, "the J1-J2 chain needs a Spin1_2Chain space");
+  DH_CHECK(sp && (sp->kind == SPACE_SPIN12 || sp->kind == SPACE_SPIN12_TRANSLATIONS), DH_ERR_ARGUMENT,
+           "the J1-J2 chain needs a Spin1_2Chain or Spin1_2ChainWithTranslations space");
   DH_CHECK(sp->length >= 3, DH_ERR_UNSUPPORTED, "the periodic J1-J2 chain needs at least 3 sites");
+  // the real Hamiltonian of a momentum sector (SpinChainJ1J2RealHamiltonianWithTranslations) is the
+  // Hamiltonian only where the phases are real: K = 0 and K = L / 2
+  DH_CHECK(sp->kind != SPACE_SPIN12_TRANSLATIONS || sp->momentum == 0 || 2 * sp->momentum == sp->length,
+           DH_ERR_UNSUPPORTED, "momentum %d of %d sites needs complex arithmetic (K = 0 or L / 2 only)", sp->momentum,
+           sp->length);
   dh_hamiltonian_s* h = new (std::nothrow) dh_hamiltonian_s();
   DH_CHECK(h, DH_ERR_MEMORY, "out of host memory");
   h->space = sp;
-  h->kind = SPACE_SPIN12;
+  h->kind = sp->kind;
   h->j1 = j1;
   h->j2 = j2;
   int rc = reducer_init(h->red, h->red_storage, 16);
@@ -1093,6 +1199,20 @@ int dh_hamiltonian_pseudopotential_adjoint(dh_hamiltonian_t h, const double* u, 
 int dh_hamiltonian_count_elements(dh_hamiltonian_t h, int64_t* total) {
   DH_CHECK(h && total, DH_ERR_ARGUMENT, "null argument");
   dh_space_s* sp = h->space;
+  if (h->kind == SPACE_SPIN12_TRANSLATIONS) {
+    // the flips whose word lies in the momentum sector (the others are dropped, as the reference's
+    // SymmetrizeResult returns no index for them)
+    DevBuf t;
+    int rc;
+    if ((rc = t.alloc(2 * sizeof(unsigned long long))) != DH_OK) return rc;
+    if ((rc = launch_trans_count_elements(trans_device(sp, h), t.as<unsigned long long>(), h->stream)) != DH_OK)
+      return rc;
+    unsigned long long v[2] = {0, 0};
+    DH_CUDA(cudaMemcpyAsync(v, t.ptr, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+    DH_CUDA(cudaStreamSynchronize(h->stream));
+    *total = (int64_t)v[1];
+    return DH_OK;
+  }
   if (h->kind == SPACE_SPIN12) {
     // every antiparallel bond is one flip: sum over the basis of #antiparallel bonds equals
     // (#bonds) * (fraction of states in which a given bond is antiparallel) * dim
@@ -1119,7 +1239,7 @@ int dh_hamiltonian_count_elements(dh_hamiltonian_t h, int64_t* total) {
 int dh_hamiltonian_count_diagonal_elements(dh_hamiltonian_t h, int64_t* total) {
   DH_CHECK(h && total, DH_ERR_ARGUMENT, "null argument");
   dh_space_s* sp = h->space;
-  if (h->kind == SPACE_SPIN12) {
+  if (h->kind == SPACE_SPIN12 || h->kind == SPACE_SPIN12_TRANSLATIONS) {
     *total = 0;  // the chain's elements are its flips; the Sz Sz part is computed per row
     return DH_OK;
   }

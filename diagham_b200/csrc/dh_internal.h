@@ -80,7 +80,7 @@ int tridiagonal_eigen(int n, const double* diag, const double* off, double* eig,
 int symmetric_eigen(int n, double* a, double* eig, double* z);
 
 // ------------------------------------------------------------- spaces
-enum SpaceKind { SPACE_FERMION = 1, SPACE_SPIN12 = 2, SPACE_BOSON = 3 };
+enum SpaceKind { SPACE_FERMION = 1, SPACE_SPIN12 = 2, SPACE_BOSON = 3, SPACE_SPIN12_TRANSLATIONS = 4 };
 
 struct FermionRankTables {
   int low_bits = 0;                 // LB: rank = high_offset[w >> LB] + low_rank[w & (2^LB - 1)]
@@ -206,6 +206,31 @@ struct SpinDevice {
   int nbr_up;
   double j1, j2;
 };
+// Spin1_2ChainWithTranslations with the real J1-J2 Hamiltonian (kernels_spin_translations.cu)
+struct TransDevice {
+  const uint32_t* reps;      // representatives, ascending
+  int32_t* rep_rank;         // their plain Spin1_2Chain index
+  const uint8_t* orbits;     // their orbit sizes
+  unsigned long long* map;   // per plain chain index: representative | rotations << 32 | orbit << 40
+  const int* table;          // lookup over the representatives (first index per word >> table_shift)
+  long long table_entries;
+  int table_shift;
+  long long dim;             // representatives
+  long long chain_dim;       // C(L, n_up)
+  int length, momentum;
+  double j1, j2;
+  double phase[32];          // cos(2 pi K m / L)
+};
+int launch_trans_count(long long total, int L, int n_up, int momentum, unsigned int* chunk_count, cudaStream_t s);
+int launch_trans_write(long long total, int L, int n_up, int momentum, const long long* chunk_offset, uint32_t* reps,
+                       uint8_t* orbits, cudaStream_t s);
+int launch_trans_table(const uint32_t* reps, long long dim, int shift, long long entries, int* table, cudaStream_t s);
+int launch_trans_map(const TransDevice& d, long long total, int n_up, cudaStream_t s);
+int launch_trans_matvec(const TransDevice& d, const MatvecArgs& a, int precision, cudaStream_t s);
+int launch_trans_find(const TransDevice& d, const uint64_t* words, long long n, long long* out, cudaStream_t s);
+// elements of one product: antiparallel bonds of every representative (total[0]) and those whose
+// flipped word lies in the momentum sector (total[1])
+int launch_trans_count_elements(const TransDevice& d, unsigned long long* total, cudaStream_t s);
 int launch_spin_unrank(int length, int nbr_up, long long dim, uint32_t* words, cudaStream_t s);
 int launch_spin_matvec(const SpinDevice& sp, const MatvecArgs& a, int precision, cudaStream_t s);
 int launch_spin_find(const SpinDevice& sp, const uint64_t* words, long long n, long long* out, cudaStream_t s);

@@ -31,6 +31,13 @@ struct dh_space_s {
   int lookup_bits = 0;
   // Spin1_2Chain
   int length = 0, sz = 0, nbr_up = 0;
+  // Spin1_2ChainWithTranslations: representatives in words (uint32, ascending), their orbit sizes
+  // and plain chain indices, the table over the whole Sz sector and the lookup over representatives
+  int momentum = 0;
+  long long chain_dim = 0;
+  dh::DevBuf rep_orbit, rep_rank, trans_map, trans_table;
+  int table_shift = 0;
+  long long table_entries = 0;
 };
 
 struct dh_hamiltonian_s {
@@ -84,6 +91,7 @@ int hamiltonian_apply_rows(dh_hamiltonian_s* h, const double* x, double* y, int 
 int hamiltonian_apply_block_rows(dh_hamiltonian_s* h, const double* x64, const float* x32, double* y, int k,
                                  int precision, cudaStream_t stream, int64_t out_first, int64_t out_last);
 SpinDevice spin_device(const dh_space_s* sp, const dh_hamiltonian_s* h);
+TransDevice trans_device(const dh_space_s* sp, const dh_hamiltonian_s* h);
 int upload_factors(dh_hamiltonian_s* h);
 // (re)build the split-word rank tables of a FermionOnSphere space for a split of low_bits (0: the
 // default, or the space's requested split) and upload them

@@ -1,0 +1,465 @@
+// The periodic J1-J2 chain in a momentum sector: Spin1_2ChainWithTranslations (fixed Sz, elementary
+// translation of one site) with SpinChainJ1J2RealHamiltonianWithTranslations (sm_100a).
+//
+// Basis (Spin1_2ChainWithTranslations.cc:167-235): the words of the Sz sector that are their own
+// canonical form (the smallest of their L rotations) and whose orbit size o (rotations back to the
+// word) satisfies K o = 0 mod L, in ascending order; NbrStateInOrbit = o.
+//
+// Product (SpinChainJ1J2RealHamiltonianWithTranslations.cc:94-192 with SymmetrizeResult,
+// Spin1_2ChainWithTranslations.h:419): a flip of an antiparallel bond of representative s gives a
+// word w; its canonical form c = rotation n of w (the first smallest), the target is c's index t,
+// and the element is J/2 sqrt(o_s / o_t) cos(2 pi K ((L - n) mod L) / L).  The matrix is real
+// symmetric for K = 0 and K = L/2, so the pull form y[s] = sum over flips of s of that element times
+// x[t] equals the reference's push form.
+//
+// B200 layout: instead of canonicalising every flipped word (L rotations and a search per element),
+// a table over the whole Sz sector, indexed by the word's plain Spin1_2Chain index (which the chain
+// kernels already compute from the row's own index with step tables), holds for every word the
+// index of its representative, the n above and its orbit size (8 bytes a word, 4.8 GB at L = 32).
+// Each element of the product is then one step-table rank, one table load and one gather.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dh_internal.h"
+#include "dh_spin_tables.cuh"
+
+namespace dh {
+namespace {
+
+constexpr int kTransThreads = 256;
+
+__device__ __forceinline__ uint32_t rotr1(uint32_t w, int L, uint32_t mask) {
+  return ((w >> 1) | (w << (L - 1))) & mask;
+}
+
+__device__ __forceinline__ long long binom64(int n, int k) {
+  if (k < 0 || k > n) return 0;
+  long long c = 1;
+  for (int q = 1; q <= k; ++q) c = c * (n - k + q) / q;
+  return c;
+}
+
+// the word of ascending rank q among the L-bit words with n ones (colex order)
+__device__ uint32_t unrank_ascending(long long q, int L, int n) {
+  uint32_t w = 0;
+  int k = n;
+  for (int pos = L - 1; pos >= 0 && k > 0; --pos) {
+    const long long c = binom64(pos, k);
+    if (q >= c) {
+      w |= 1u << pos;
+      q -= c;
+      --k;
+    }
+  }
+  return w;
+}
+
+// canonical form (first smallest rotation), rotations to it and orbit size
+__device__ __forceinline__ void canonical(uint32_t w, int L, uint32_t mask, uint32_t& c, int& n, int& orbit) {
+  c = w;
+  n = 0;
+  orbit = L;
+  uint32_t t = w;
+  for (int k = 1; k < L; ++k) {
+    t = rotr1(t, L, mask);
+    if (t == w && orbit == L) orbit = k;
+    if (t < c) {
+      c = t;
+      n = k;
+    }
+  }
+}
+
+// pass 1: per chunk of 1024 ascending ranks, the number of representatives
+__global__ void rep_count_kernel(long long total, int L, int n_up, int momentum, unsigned int* chunk_count) {
+  const uint32_t mask = (L == 32) ? 0xffffffffu : ((1u << L) - 1u);
+  const long long base = (long long)blockIdx.x * 1024;
+  unsigned int cnt = 0;
+  for (int j = threadIdx.x; j < 1024; j += blockDim.x) {
+    const long long q = base + j;
+    if (q >= total) break;
+    const uint32_t w = unrank_ascending(q, L, n_up);
+    uint32_t c;
+    int nn, o;
+    canonical(w, L, mask, c, nn, o);
+    if (c == w && ((long long)o * momentum) % L == 0) ++cnt;
+  }
+  for (int s = 16; s > 0; s >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, s);
+  __shared__ unsigned int part[kTransThreads / 32];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int t = 0;
+    for (int i = 0; i < kTransThreads / 32; ++i) t += part[i];
+    chunk_count[blockIdx.x] = t;
+  }
+}
+
+// pass 2: the representatives in ascending order (chunk offsets from pass 1), with their orbit sizes;
+// 256 threads take 4 consecutive ranks each and place them with a block scan
+__global__ void rep_write_kernel(long long total, int L, int n_up, int momentum, const long long* chunk_offset,
+                                 uint32_t* reps, uint8_t* orbits) {
+  const uint32_t mask = (L == 32) ? 0xffffffffu : ((1u << L) - 1u);
+  __shared__ unsigned int scan[kTransThreads];
+  const long long q0 = (long long)blockIdx.x * 1024 + threadIdx.x * 4;
+  uint32_t words[4];
+  int orb[4];
+  unsigned int keep = 0;
+  for (int j = 0; j < 4; ++j) {
+    const long long q = q0 + j;
+    words[j] = 0;
+    orb[j] = 0;
+    if (q >= total) continue;
+    const uint32_t w = unrank_ascending(q, L, n_up);
+    uint32_t c;
+    int nn, o;
+    canonical(w, L, mask, c, nn, o);
+    if (c == w && ((long long)o * momentum) % L == 0) {
+      words[j] = w;
+      orb[j] = o;
+      keep |= 1u << j;
+    }
+  }
+  scan[threadIdx.x] = __popc(keep);
+  __syncthreads();
+  for (int s = 1; s < kTransThreads; s <<= 1) {
+    const unsigned int v = (threadIdx.x >= (unsigned)s) ? scan[threadIdx.x - s] : 0u;
+    __syncthreads();
+    scan[threadIdx.x] += v;
+    __syncthreads();
+  }
+  long long pos = chunk_offset[blockIdx.x] + scan[threadIdx.x] - __popc(keep);
+  for (int j = 0; j < 4; ++j)
+    if ((keep >> j) & 1u) {
+      reps[pos] = words[j];
+      orbits[pos] = (uint8_t)orb[j];
+      ++pos;
+    }
+}
+
+// lookup table over the representatives: table[v] = first index whose word >> shift is >= v
+__global__ void rep_table_kernel(const uint32_t* reps, long long dim, int shift, long long entries, int* table) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < entries; v += stride) {
+    const unsigned long long key = (unsigned long long)v << shift;
+    long long lo = 0, hi = dim;  // first index with reps[i] >= key
+    while (lo < hi) {
+      const long long mid = (lo + hi) >> 1;
+      if ((unsigned long long)reps[mid] >= key)
+        hi = mid;
+      else
+        lo = mid + 1;
+    }
+    table[v] = (int)lo;
+  }
+}
+
+// index of representative c, or -1
+__device__ __forceinline__ long long rep_find(const TransDevice& d, uint32_t c) {
+  const long long v = (long long)(c >> d.table_shift);
+  if (v + 1 >= d.table_entries) return -1;
+  long long lo = d.table[v], hi = d.table[v + 1];
+  while (lo < hi) {
+    const long long mid = (lo + hi) >> 1;
+    if (d.reps[mid] >= c)
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  return (lo < d.dim && d.reps[lo] == c) ? lo : -1;
+}
+
+// every word of the Sz sector (ascending rank q): its plain chain index, the index of its
+// representative (or none), the rotations to it and its orbit size; and each representative's own
+// plain chain index
+__global__ void __launch_bounds__(kTransThreads) trans_map_kernel(TransDevice d, long long total, int n_up) {
+  __shared__ SpinTables tb;
+  build_spin_tables(tb, d.length);
+  const int L = d.length;
+  const uint32_t mask = (L == 32) ? 0xffffffffu : ((1u << L) - 1u);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += stride) {
+    const uint32_t w = unrank_ascending(q, L, n_up);
+    uint32_t c;
+    int n, o;
+    canonical(w, L, mask, c, n, o);
+    const long long t = rep_find(d, c);
+    const int r = spin_rank_index(tb, w, L, (int)d.chain_dim);
+    unsigned long long e = 0xffffffffull;
+    if (t >= 0) e = (unsigned long long)t | ((unsigned long long)n << 32) | ((unsigned long long)o << 40);
+    d.map[r] = e;
+    if (t >= 0 && c == w) d.rep_rank[t] = r;
+  }
+}
+
+template <typename TG, int K, bool IL>
+__device__ __forceinline__ void trans_gather(const TG* x, const MatvecArgs& a, long long idx, TG (&v)[K]) {
+  if constexpr (IL && sizeof(TG) == 4 && K == 4) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(x + idx * 4));
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+  } else if constexpr (IL && sizeof(TG) == 4 && K == 2) {
+    const float2 q = __ldg(reinterpret_cast<const float2*>(x + idx * 2));
+    v[0] = q.x; v[1] = q.y;
+  } else if constexpr (IL && sizeof(TG) == 8 && (K == 2 || K == 4)) {
+#pragma unroll
+    for (int j = 0; j < K; j += 2) {
+      const double2 q = __ldg(reinterpret_cast<const double2*>(x + idx * K) + j / 2);
+      v[j] = q.x;
+      v[j + 1] = q.y;
+    }
+  } else {
+    const TG* p = x + idx * a.ld;
+#pragma unroll
+    for (int q = 0; q < K; ++q) v[q] = __ldg(p + q * a.vstride);
+  }
+}
+
+struct TransShared {
+  SpinTables tb;
+  double ratio[33 * 33];  // sqrt(o_s / o_t)
+  double phase[32];       // cos(2 pi K m / L)
+};
+
+// one element: the flipped word's plain chain index ci -> representative, coefficient, gather
+template <typename TG, int K, bool IL, bool RANGE>
+__device__ __forceinline__ void trans_element(TG (&acc)[K], const TransDevice& d, const TransShared& sh, const TG* x,
+                                              const MatvecArgs& a, int ci, int os, TG hj) {
+  const unsigned long long e = __ldg(d.map + ci);
+  const unsigned int t = (unsigned int)(e & 0xffffffffull);
+  if (t == 0xffffffffu) return;  // the flipped word's orbit is not in this momentum sector
+  if (RANGE && ((long long)t < a.col_first || (long long)t >= a.col_last)) return;
+  const int n = (int)((e >> 32) & 0xffull), ot = (int)((e >> 40) & 0xffull);
+  const int m = (d.length - n) % d.length;
+  const TG c = hj * (TG)(sh.ratio[os * 33 + ot] * sh.phase[m]);
+  TG v[K];
+  trans_gather<TG, K, IL>(x, a, t, v);
+#pragma unroll
+  for (int q = 0; q < K; ++q) acc[q] += c * v[q];
+}
+
+template <typename TG, int K, bool IL, bool RANGE>
+__global__ void __launch_bounds__(kTransThreads) trans_matvec_kernel(TransDevice d, MatvecArgs a) {
+  __shared__ TransShared sh;
+  build_spin_tables(sh.tb, d.length);
+  for (int i = threadIdx.x; i < 33 * 33; i += blockDim.x) {
+    const int os = i / 33, ot = i % 33;
+    sh.ratio[i] = (os > 0 && ot > 0) ? sqrt((double)os / (double)ot) : 0.0;
+  }
+  for (int i = threadIdx.x; i < 32; i += blockDim.x) sh.phase[i] = d.phase[i];
+  __syncthreads();
+  const int L = d.length;
+  const int D = (int)d.chain_dim;
+  const uint32_t maskL = (L == 32) ? 0xffffffffu : ((1u << L) - 1u);
+  const TG hj1 = (TG)(0.5 * d.j1), hj2 = (TG)(0.5 * d.j2);
+  const TG* x = static_cast<const TG*>(a.x);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long r_end = a.out_last > 0 ? a.out_last : d.dim;
+  for (long long s = a.out_first + (long long)blockIdx.x * blockDim.x + threadIdx.x; s < r_end; s += stride) {
+    const uint32_t w = __ldg(d.reps + s);
+    const int r = __ldg(d.rep_rank + s);
+    const int os = d.orbits[s];
+    const uint32_t rot1 = ((w >> 1) | (w << (L - 1))) & maskL;
+    const uint32_t rot2 = ((w >> 2) | (w << (L - 2))) & maskL;
+    const uint32_t d1 = w ^ rot1, d2 = w ^ rot2;
+    TG acc[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) acc[j] = TG(0);
+    // J1 bonds (j, j+1), j = 0 .. L-2, by the plain chain's index steps
+    uint32_t f = d1 & (maskL >> 1);
+    while (f) {
+      const int ja = __ffs(f) - 1;
+      f &= f - 1u;
+      const int da = sh.tb.j1[(ja << 5) | __popc(__funnelshift_rc(w, 0u, ja + 2))];
+      trans_element<TG, K, IL, RANGE>(acc, d, sh, x, a, ((w >> ja) & 1u) ? r + da : r - da, os, hj1);
+    }
+    // J2 bonds (j, j+2), j = 0 .. L-3
+    f = d2 & (maskL >> 2);
+    while (f) {
+      const int ja = __ffs(f) - 1;
+      f &= f - 1u;
+      const int da =
+          sh.tb.j2[(((w >> (ja + 1)) & 1u) << 10) | (ja << 5) | __popc(__funnelshift_rc(w, 0u, ja + 3))];
+      trans_element<TG, K, IL, RANGE>(acc, d, sh, x, a, ((w >> ja) & 1u) ? r + da : r - da, os, hj2);
+    }
+    // bonds that wrap around the chain
+    if ((d1 >> (L - 1)) & 1u)
+      trans_element<TG, K, IL, RANGE>(acc, d, sh, x, a, spin_rank_index(sh.tb, w ^ (1u | (1u << (L - 1))), L, D), os,
+                                      hj1);
+    if ((d2 >> (L - 2)) & 1u)
+      trans_element<TG, K, IL, RANGE>(acc, d, sh, x, a, spin_rank_index(sh.tb, w ^ (1u | (1u << (L - 2))), L, D), os,
+                                      hj2);
+    if ((d2 >> (L - 1)) & 1u)
+      trans_element<TG, K, IL, RANGE>(acc, d, sh, x, a, spin_rank_index(sh.tb, w ^ (2u | (1u << (L - 1))), L, D), os,
+                                      hj2);
+    // diagonal: J/4 (L - 2 #antiparallel bonds) per bond type (SzSzContributions), plus the shift
+    const double diag = 0.25 * d.j1 * (double)(L - 2 * __popc(d1)) + 0.25 * d.j2 * (double)(L - 2 * __popc(d2)) +
+                        a.shift;
+    const bool on_diag = (s >= a.row_first && s < a.row_last);
+    double* y = static_cast<double*>(a.y);
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+      double v = (double)acc[q];
+      if (on_diag) {
+        const long long xo = IL ? s * K + q : s * a.ld + q * a.vstride;
+        const double xd = a.xdiag ? a.xdiag[xo] : (double)x[xo];
+        v += diag * xd;
+      }
+      double* yp = y + (IL ? s * K + q : s * a.ld_y + q * a.vstride_y);
+      *yp = a.accumulate ? (*yp + v) : v;
+    }
+  }
+}
+
+// elements of one product (antiparallel bonds of the representatives, and those in the sector)
+__global__ void __launch_bounds__(kTransThreads) trans_count_kernel(TransDevice d, unsigned long long* total) {
+  __shared__ SpinTables tb;
+  build_spin_tables(tb, d.length);
+  const int L = d.length;
+  const int D = (int)d.chain_dim;
+  const uint32_t maskL = (L == 32) ? 0xffffffffu : ((1u << L) - 1u);
+  unsigned long long bonds = 0, kept = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < d.dim; s += stride) {
+    const uint32_t w = d.reps[s];
+    const int r = d.rep_rank[s];
+    const uint32_t d1 = w ^ (((w >> 1) | (w << (L - 1))) & maskL);
+    const uint32_t d2 = w ^ (((w >> 2) | (w << (L - 2))) & maskL);
+    bonds += __popc(d1) + __popc(d2);
+    uint32_t f = d1 & (maskL >> 1);
+    while (f) {
+      const int ja = __ffs(f) - 1;
+      f &= f - 1u;
+      const int da = tb.j1[(ja << 5) | __popc(__funnelshift_rc(w, 0u, ja + 2))];
+      kept += (d.map[((w >> ja) & 1u) ? r + da : r - da] & 0xffffffffull) != 0xffffffffull;
+    }
+    f = d2 & (maskL >> 2);
+    while (f) {
+      const int ja = __ffs(f) - 1;
+      f &= f - 1u;
+      const int da = tb.j2[(((w >> (ja + 1)) & 1u) << 10) | (ja << 5) | __popc(__funnelshift_rc(w, 0u, ja + 3))];
+      kept += (d.map[((w >> ja) & 1u) ? r + da : r - da] & 0xffffffffull) != 0xffffffffull;
+    }
+    if ((d1 >> (L - 1)) & 1u)
+      kept += (d.map[spin_rank_index(tb, w ^ (1u | (1u << (L - 1))), L, D)] & 0xffffffffull) != 0xffffffffull;
+    if ((d2 >> (L - 2)) & 1u)
+      kept += (d.map[spin_rank_index(tb, w ^ (1u | (1u << (L - 2))), L, D)] & 0xffffffffull) != 0xffffffffull;
+    if ((d2 >> (L - 1)) & 1u)
+      kept += (d.map[spin_rank_index(tb, w ^ (2u | (1u << (L - 1))), L, D)] & 0xffffffffull) != 0xffffffffull;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    bonds += __shfl_down_sync(0xffffffffu, bonds, o);
+    kept += __shfl_down_sync(0xffffffffu, kept, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(total, bonds);
+    atomicAdd(total + 1, kept);
+  }
+}
+
+__global__ void trans_find_kernel(TransDevice d, const uint64_t* words, long long n, long long* out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t w = words[i];
+  out[i] = (w >> 32) ? -1 : rep_find(d, (uint32_t)w);
+}
+
+template <typename TG, int K>
+int launch_trans_typed(const TransDevice& d, const MatvecArgs& a, cudaStream_t s) {
+  const bool range = a.col_first > 0 || a.col_last < d.dim;
+  const bool il = (K > 1) && a.ld == K && a.vstride == 1 && a.ld_y == K && a.vstride_y == 1;
+  auto kern = range ? (il ? trans_matvec_kernel<TG, K, true, true> : trans_matvec_kernel<TG, K, false, true>)
+                    : (il ? trans_matvec_kernel<TG, K, true, false> : trans_matvec_kernel<TG, K, false, false>);
+  int dev = 0, sms = 148, per_sm = 1;
+  DH_CUDA(cudaGetDevice(&dev));
+  DH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  DH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTransThreads, 0));
+  const long long rows = (a.out_last > 0 ? a.out_last : d.dim) - a.out_first;
+  long long grid = (long long)sms * (per_sm > 0 ? per_sm : 1);
+  const long long need = (rows + kTransThreads - 1) / kTransThreads;
+  if (need < grid) grid = need;
+  if (grid < 1) grid = 1;
+  kern<<<(unsigned)grid, kTransThreads, 0, s>>>(d, a);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+template <typename TG>
+int launch_trans_k(const TransDevice& d, const MatvecArgs& a, cudaStream_t s) {
+  MatvecArgs b = a;
+  int done = 0;
+  while (done < a.nbr_vectors) {
+    const int left = a.nbr_vectors - done;
+    const int k = left >= 4 ? 4 : (left >= 2 ? 2 : 1);
+    b.x = static_cast<const TG*>(a.x) + (long long)done * a.vstride;
+    b.xdiag = a.xdiag ? a.xdiag + (long long)done * a.vstride : nullptr;
+    b.y = static_cast<double*>(a.y) + (long long)done * a.vstride_y;
+    b.nbr_vectors = k;
+    int rc = (k == 4) ? launch_trans_typed<TG, 4>(d, b, s)
+                      : (k == 2) ? launch_trans_typed<TG, 2>(d, b, s) : launch_trans_typed<TG, 1>(d, b, s);
+    if (rc != DH_OK) return rc;
+    done += k;
+  }
+  return DH_OK;
+}
+
+}  // namespace
+
+int launch_trans_count(long long total, int L, int n_up, int momentum, unsigned int* chunk_count, cudaStream_t s) {
+  const long long chunks = (total + 1023) / 1024;
+  if (chunks <= 0) return DH_OK;
+  rep_count_kernel<<<(unsigned)chunks, kTransThreads, 0, s>>>(total, L, n_up, momentum, chunk_count);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_trans_write(long long total, int L, int n_up, int momentum, const long long* chunk_offset, uint32_t* reps,
+                       uint8_t* orbits, cudaStream_t s) {
+  const long long chunks = (total + 1023) / 1024;
+  if (chunks <= 0) return DH_OK;
+  rep_write_kernel<<<(unsigned)chunks, kTransThreads, 0, s>>>(total, L, n_up, momentum, chunk_offset, reps, orbits);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_trans_table(const uint32_t* reps, long long dim, int shift, long long entries, int* table, cudaStream_t s) {
+  long long g = (entries + 255) / 256;
+  if (g > 148 * 32) g = 148 * 32;
+  if (g < 1) g = 1;
+  rep_table_kernel<<<(unsigned)g, 256, 0, s>>>(reps, dim, shift, entries, table);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_trans_map(const TransDevice& d, long long total, int n_up, cudaStream_t s) {
+  long long g = (total + kTransThreads - 1) / kTransThreads;
+  if (g > 148 * 16) g = 148 * 16;
+  if (g < 1) g = 1;
+  trans_map_kernel<<<(unsigned)g, kTransThreads, 0, s>>>(d, total, n_up);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_trans_matvec(const TransDevice& d, const MatvecArgs& a, int precision, cudaStream_t s) {
+  if (d.dim <= 0) return DH_OK;
+  return precision == DH_PRECISION_FP32 ? launch_trans_k<float>(d, a, s) : launch_trans_k<double>(d, a, s);
+}
+
+int launch_trans_find(const TransDevice& d, const uint64_t* words, long long n, long long* out, cudaStream_t s) {
+  if (n <= 0) return DH_OK;
+  trans_find_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(d, words, n, out);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_trans_count_elements(const TransDevice& d, unsigned long long* total, cudaStream_t s) {
+  DH_CUDA(cudaMemsetAsync(total, 0, 2 * sizeof(unsigned long long), s));
+  if (d.dim <= 0) return DH_OK;
+  long long g = (d.dim + kTransThreads - 1) / kTransThreads;
+  if (g > 148 * 16) g = 148 * 16;
+  if (g < 1) g = 1;
+  trans_count_kernel<<<(unsigned)g, kTransThreads, 0, s>>>(d, total);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+}  // namespace dh

@@ -79,6 +79,16 @@ int dh_boson_on_sphere_create(int nbr_bosons, int total_lz, int lz_max, unsigned
  * sz is twice the total Sz.  chain_length <= 32. */
 int dh_spin12_chain_create(int chain_length, int sz, int memory, dh_space_t* out);
 
+/* Spin1_2ChainWithTranslations(chainLength, momentum, translationStep = 1, sz, memory, memorySlice)
+ * (Spin/src/HilbertSpace/Spin1_2ChainWithTranslations.cc:167-235): the momentum-K sector of the
+ * periodic chain at fixed 2Sz = sz.  A state is an orbit of the L translations, represented by its
+ * smallest word; orbits of size o with K o != 0 mod L are not in the sector; states in ascending order
+ * of their representative (dh_space_get_states gives the representatives, dh_space_find_state_index
+ * takes them).  Set-up builds, for every word of the Sz sector, its representative's index, the
+ * translations to it and its orbit size: C(L, N_up) x 8 bytes of device memory (4.8 GB at L = 32).
+ * 3 <= L <= 32; memory is accepted for the signature and unused. */
+int dh_spin12_chain_translations_create(int chain_length, int momentum, int sz, int memory, dh_space_t* out);
+
 int dh_space_destroy(dh_space_t space);
 
 /* AbstractHilbertSpace::GetHilbertSpaceDimension (src/HilbertSpace/AbstractHilbertSpace.h). */
@@ -144,7 +154,11 @@ int dh_particle_on_sphere_l2_hamiltonian_create(dh_space_t space, int nbr_partic
 
 /* Periodic J1-J2 spin-1/2 chain on a plain Spin1_2Chain: the element pattern of
  * Spin/src/Hamiltonian/SpinChainJ1J2RealHamiltonianWithTranslations.cc:94-192 (flips J/2) and
- * :335-352 (diagonal J Sz_i Sz_j) behind the SpinChainHamiltonian API (SpinChainHamiltonian.cc:257). */
+ * :335-352 (diagonal J Sz_i Sz_j) behind the SpinChainHamiltonian API (SpinChainHamiltonian.cc:257).
+ * On a Spin1_2ChainWithTranslations space: SpinChainJ1J2RealHamiltonianWithTranslations(chain,
+ * nbrSpin, j1, j2) itself, each flip's word taken to its representative with the factor
+ * sqrt(o_from / o_to) cos(2 pi K n / L) (SymmetrizeResult, Spin1_2ChainWithTranslations.h:419); only
+ * the real sectors K = 0 and K = L / 2 (DH_ERR_UNSUPPORTED otherwise). */
 int dh_spin_chain_j1j2_hamiltonian_create(dh_space_t space, double j1, double j2, dh_hamiltonian_t* out);
 
 int dh_hamiltonian_destroy(dh_hamiltonian_t h);

@@ -29,6 +29,8 @@
 #include "HilbertSpace/FermionOnSphere.h"
 #include "HilbertSpace/BosonOnSphereShort.h"
 #include "HilbertSpace/Spin1_2Chain.h"
+#include "HilbertSpace/Spin1_2ChainWithTranslations.h"
+#include "Hamiltonian/SpinChainJ1J2RealHamiltonianWithTranslations.h"
 #include "Hamiltonian/ParticleOnSphereGenericHamiltonian.h"
 #include "Hamiltonian/ParticleOnSphereL2Hamiltonian.h"
 #include "Hamiltonian/AbstractHamiltonian.h"
@@ -452,6 +454,9 @@ static void Usage()
 	  "  spin_basis L 2Sz out\n"
 	  "  spin_matvec L 2Sz J1 J2 xfile out\n"
 	  "  spin_lanczos L 2Sz J1 J2 algo nev block maxiter precision out x0 [x1 ...]\n"
+	  "  spint_basis L 2Sz K out\n"
+	  "  spint_matvec L 2Sz K J1 J2 xfile out\n"
+	  "  spint_lanczos L 2Sz K J1 J2 maxiter precision out x0\n"
 	  "  bench_fqhe N 2S 2Lz vfile threads reps hermitian [rows]\n"
 	  "  bench_bqhe N 2S 2Lz vfile threads reps hermitian [rows]\n"
 	  "  bench_spin L 2Sz J1 J2 threads reps 0\n");
@@ -799,6 +804,51 @@ int main(int argc, char** argv)
       RealVector Y(Chain.GetHilbertSpaceDimension(), true);
       H.LowLevelMultiply(X, Y);
       Y.WriteVector(argv[7]);
+      return 0;
+    }
+  // translations: Spin1_2ChainWithTranslations(L, K, 1, 2Sz) with SpinChainJ1J2RealHamiltonianWithTranslations
+  // (real: K = 0 or L / 2)
+  if (strcmp(Cmd, "spint_basis") == 0 && argc == 6)
+    {
+      // layout: int64 dimension, then the states (PrintState's hexadecimal word) as uint64
+      int L = atoi(argv[2]), Sz = atoi(argv[3]), K = atoi(argv[4]);
+      Spin1_2ChainWithTranslations Chain(L, K, 1, Sz, 1 << 20, 1 << 20);
+      long Dim = Chain.GetHilbertSpaceDimension();
+      FILE* f = OpenOut(argv[5]);
+      fwrite(&Dim, sizeof(long), 1, f);
+      for (long i = 0; i < Dim; ++i)
+	{
+	  std::ostringstream Str;
+	  Chain.PrintState(Str, (int) i);
+	  std::string Text = Str.str();
+	  unsigned long Word = strtoul(Text.substr(Text.rfind(' ') + 1).c_str(), 0, 16);
+	  fwrite(&Word, sizeof(unsigned long), 1, f);
+	}
+      fclose(f);
+      return 0;
+    }
+  if (strcmp(Cmd, "spint_matvec") == 0 && argc == 9)
+    {
+      int L = atoi(argv[2]), Sz = atoi(argv[3]), K = atoi(argv[4]);
+      Spin1_2ChainWithTranslations Chain(L, K, 1, Sz, 1 << 20, 1 << 20);
+      SpinChainJ1J2RealHamiltonianWithTranslations H(&Chain, L, atof(argv[5]), atof(argv[6]));
+      RealVector X;
+      X.ReadVector(argv[7]);
+      RealVector Y(Chain.GetHilbertSpaceDimension(), true);
+      H.LowLevelMultiply(X, Y);
+      Y.WriteVector(argv[8]);
+      return 0;
+    }
+  if (strcmp(Cmd, "spint_lanczos") == 0 && argc == 11)
+    {
+      int L = atoi(argv[2]), Sz = atoi(argv[3]), K = atoi(argv[4]);
+      Spin1_2ChainWithTranslations Chain(L, K, 1, Sz, 1 << 20, 1 << 20);
+      SpinChainJ1J2RealHamiltonianWithTranslations H(&Chain, L, atof(argv[5]), atof(argv[6]));
+      AbstractArchitecture* Arch = MakeArchitecture();
+      Arch->SetDimension(Chain.GetHilbertSpaceDimension());
+      RealVector* Init = new RealVector[1];
+      Init[0].ReadVector(argv[10]);
+      RunLanczosLoop(&H, Arch, "basic", 1, 1, atoi(argv[7]), atof(argv[8]), Init, 1, argv[9], 0);
       return 0;
     }
   if (strcmp(Cmd, "spin_lanczos") == 0 && argc >= 13)
