@@ -477,3 +477,78 @@ def entanglement_matrix(n, two_s, total_lz, x, l, na, lza):
         if a in ra and b in rb:
             m[ra[a], rb[b]] = x[i]
     return m
+
+
+def _translation_canonical(w, L):
+    """Spin1_2ChainWithTranslations::FindCanonicalForm (.h:478) and FindNumberTranslation (:530): the
+    first smallest of the L rotations of w (one site each), the rotations to it, and the orbit size."""
+    c, n, orbit, t = w, 0, L, w
+    for k in range(1, L):
+        t = (t >> 1) | ((t & 1) << (L - 1))
+        if t == w and orbit == L:
+            orbit = k
+        if t < c:
+            c, n = t, k
+    return c, n, orbit
+
+
+def translation_basis(L, sz, k):
+    """Spin1_2ChainWithTranslations(L, k, 1, sz) (Spin1_2ChainWithTranslations.cc:167-235): the words
+    with (L + sz) / 2 up spins that are their own canonical form and whose orbit size o satisfies
+    k o = 0 mod L, ascending; returns (words, orbit sizes)."""
+    from itertools import combinations
+    n_up = (L + sz) // 2
+    words = sorted(sum(1 << p for p in c) for c in combinations(range(L), n_up))
+    reps, orbits = [], []
+    for w in words:
+        c, _, o = _translation_canonical(w, L)
+        if c == w and (o * k) % L == 0:
+            reps.append(w)
+            orbits.append(o)
+    return np.array(reps, np.uint64), np.array(orbits, np.int32)
+
+
+def translation_j1j2_push(L, sz, k, j1, j2, x):
+    """SpinChainJ1J2RealHamiltonianWithTranslations::LowLevelAddMultiply (.cc:94-192) restated: for every
+    representative s and every bond (J1: i, i+1; J2: i, i+2, periodic) with antiparallel spins, the flipped
+    word's representative t receives J/2 sqrt(o_s / o_t) cos(2 pi k ((L - n) mod L) / L) x[s] (SymmetrizeResult,
+    Spin1_2ChainWithTranslations.h:419); plus the SzSz diagonal (:335-352)."""
+    reps, orbits = translation_basis(L, sz, k)
+    index = {int(w): i for i, w in enumerate(reps)}
+    y = np.zeros(len(reps))
+    phase = [np.cos(2.0 * np.pi / L * k * m) for m in range(L)]
+    for i, w in enumerate(reps):
+        w = int(w)
+        diag = 0.0
+        for dist, j in ((1, j1), (2, j2)):
+            for a in range(L):
+                b = (a + dist) % L
+                if ((w >> a) & 1) == ((w >> b) & 1):
+                    diag += 0.25 * j
+                    continue
+                diag -= 0.25 * j
+                f = w ^ ((1 << a) | (1 << b))
+                c, n, o = _translation_canonical(f, L)
+                t = index.get(c)
+                if t is None:
+                    continue
+                y[t] += 0.5 * j * np.sqrt(orbits[i] / orbits[t]) * phase[(L - n) % L] * x[i]
+        y[i] += diag * x[i]
+    return y
+
+
+def translation_flip_count(L, sz, k):
+    """Number of spin flips of the J1-J2 chain (both bond types) from a representative whose word lies in
+    the momentum sector: the off-diagonal elements SymmetrizeResult keeps
+    (SpinChainJ1J2RealHamiltonianWithTranslations.cc:94-192)."""
+    reps, _ = translation_basis(L, sz, k)
+    index = set(int(w) for w in reps)
+    kept = 0
+    for w in reps:
+        w = int(w)
+        for dist in (1, 2):
+            for a in range(L):
+                b = (a + dist) % L
+                if ((w >> a) & 1) != ((w >> b) & 1):
+                    kept += _translation_canonical(w ^ ((1 << a) | (1 << b)), L)[0] in index
+    return kept

@@ -366,6 +366,35 @@ def entanglement_fixtures(tmp):
          cases=np.array(ENTANGLEMENT_CASES, np.int32), **out)
 
 
+TRANSLATION_CASES = [(8, 0, 0, 1.0, 0.5), (8, 0, 4, 1.0, 0.5), (12, 0, 0, 1.0, 0.5), (12, 0, 6, 1.0, 0.3),
+                     (12, 2, 6, 1.0, 0.5), (13, 1, 0, 1.0, 0.3), (16, 0, 0, 1.0, 0.5), (16, 0, 8, 1.0, 0.2),
+                     (18, 2, 0, 1.0, 0.5), (20, 0, 10, 1.0, 0.4)]
+
+
+def translation_fixtures(tmp):
+    # Spin1_2ChainWithTranslations(L, K, 1, 2Sz) with SpinChainJ1J2RealHamiltonianWithTranslations(J1, J2):
+    # the representatives (ascending), y = H x for x = the splitmix64 vector of seed 0, and the basic
+    # Lanczos run from it (precision MACHINE_PRECISION, 300 iterations at most) where the sector has
+    # 300 states or more (below that the reference's run outlives the Krylov space)
+    for (L, sz, k, j1, j2) in TRANSLATION_CASES:
+        bf = os.path.join(tmp, "tb.bin")
+        cmd = run("spint_basis", L, sz, k, bf)
+        b = open(bf, "rb").read()
+        dim = int(np.frombuffer(b[:8], np.int64)[0])
+        words = np.frombuffer(b[8:], np.uint64).copy()
+        xf = os.path.join(tmp, "xt.vec")
+        write_vector(xf, splitmix_vector(0, dim))
+        yf = os.path.join(tmp, "yt.vec")
+        cmd2 = run("spint_matvec", L, sz, k, j1, j2, xf, yf)
+        extra = {}
+        if dim >= 300:
+            lf = os.path.join(tmp, "lt.out")
+            run("spint_lanczos", L, sz, k, j1, j2, 300, 0, lf, xf)
+            extra = read_lanczos(lf)
+        save("translations_L%d_sz%d_k%d_j2_%g.npz" % (L, sz, k, j2), cmd + "; " + cmd2, seed=0, j1=j1, j2=j2,
+             words=words, y=read_vector(yf), **extra)
+
+
 def dir_files(d):
     names = sorted(os.listdir(d))
     return np.array(names), {"f%d" % i: np.frombuffer(open(os.path.join(d, f), "rb").read(), np.uint8)
@@ -452,6 +481,8 @@ def main():
             boson_fixtures(tmp)
         if args.only in (None, "entanglement"):
             entanglement_fixtures(tmp)
+        if args.only in (None, "translations"):
+            translation_fixtures(tmp)
         if args.slow:
             slow_fixtures(tmp)
 
