@@ -393,6 +393,80 @@ def spin_chain_product(dh, flush, steps=5, k=2, length=32, warmup=2):
 
 
 
+def momentum_sector(dh, flush, steps=5, k=2, length=32, warmup=2):
+    """Spin1_2ChainWithTranslations L = 32, Sz = 0, K = 0 with the J1-J2 Hamiltonian at J2 = J1/2
+    (dimension 18,784,170): set-up time, FP32 block products of k vectors and FP64 single products
+    with their algorithmic bytes (per row: word, chain index, orbit size, FP64 y and diagonal x; per
+    element: one 8-byte map entry and one x gather), and the FP64 Lanczos time to E0 (-3L/8 at this
+    point)."""
+    import torch
+    t0 = time.perf_counter()
+    sp = dh.Spin1_2ChainWithTranslations(length, 0, 0)
+    H = dh.SpinChainJ1J2RealHamiltonianWithTranslations(sp, length, 1.0, 0.5)
+    torch.cuda.synchronize()
+    setup = time.perf_counter() - t0
+    dim = sp.dim
+    flips = H.count_elements()
+    peak, kind = peaks()
+    out = {"workload": "Spin1_2ChainWithTranslations L=%d Sz=0 K=0, J1=1 J2=0.5 (dim %d)" % (length, dim),
+           "setup_seconds": setup, "off_diagonal_elements": flips}
+    for prec, kk in (("fp32", k), ("fp64", 1)):
+        H.set_precision(prec)
+        x = torch.empty(dim, kk, dtype=torch.float64, device="cuda")
+        x.uniform_(-1.0, 1.0)
+        y = torch.empty_like(x)
+        for _ in range(warmup):
+            flush.zero_()
+            H.block_multiply(x, y)
+        ms = []
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            H.block_multiply(x, y)
+            b.record()
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        xb = 4 if prec == "fp32" else 8
+        alg = dim * (9 + 16 * kk) + flips * (8 + xb * kk)
+        mean_s = statistics.mean(ms) / 1000.0
+        out["%s_block_k%d" % (prec, kk)] = {
+            "mean_launch_ms": mean_s * 1000.0, "hv_per_s": kk / mean_s, "algorithmic_bytes_per_launch": alg,
+            "roofline": {"bound": "hbm", "achieved": alg / mean_s / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / mean_s / 1e9 / peak, "peak_kind": kind}}
+        del x, y
+    H.set_precision("fp64")
+    t0 = time.perf_counter()
+    lz = dh.BasicLanczosAlgorithm(H, 1, 600)
+    lz.SetEigenvaluePrecision(1e-10)
+    lz.InitializeLanczosAlgorithm(seed=0)
+    r = lz.solve(600, graph_batch=16)
+    out["time_to_e0"] = {"seconds": time.perf_counter() - t0, "e0": float(r["eigenvalues"][0]),
+                         "iterations": r["iterations"], "abs_e0_plus_3L_over_8": abs(r["eigenvalues"][0] + 0.375 * length),
+                         "precision": 1e-10}
+    del lz, H, sp
+    torch.cuda.empty_cache()
+    return out
+
+
+def reference_cpu_momentum_sector(length=32, rows_target_s=6.0):
+    """The reference's own SMP product on the momentum sector of momentum_sector (oracle/_ref/ref_tool
+    bench_spint: Spin1_2ChainWithTranslations + SpinChainJ1J2RealHamiltonianWithTranslations, all host
+    threads) over a row sample; its basis set-up is reported beside it."""
+    if not os.path.exists(REF_TOOL):
+        return None
+    threads = os.cpu_count() or 1
+    # about 6 us of one thread per row (measured on x86 hosts)
+    rows = int(max(2000, rows_target_s * threads / 6e-6))
+    cmd = [REF_TOOL, "bench_spint", length, 0, 0, 1.0, 0.5, threads, 1, rows]
+    out = subprocess.run([str(c) for c in cmd], check=True, capture_output=True, text=True)
+    r = json.loads([l for l in out.stdout.splitlines() if l.startswith("{")][-1])
+    per_matvec = r["mean_s"] * r["dim"] / r["rows"]
+    return {"value": 1.0 / per_matvec, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": "first %d of %d rows per product, SMP %d threads" % (r["rows"], r["dim"], threads),
+            "seconds_per_sample": r["mean_s"], "reference_setup_seconds": r["setup_s"]}
+
+
 def boson_product(dh, flush, steps=5, k=4, warmup=2):
     """BosonOnSphereShort N=12, 2S=22, 2Lz=0 (dimension 7,764,392, the size of the fermion sector
     above), LLL Coulomb V_m with the odd m set to zero: FP32 block products of k vectors, their
@@ -644,7 +718,7 @@ def run_b200(args, world, rank, local):
     e2e_s = reduce_max(time.perf_counter() - t0, world)
     e2e_value = world * BLOCK * e2e_steps / e2e_s
 
-    tte = tte_c = spin = grads = stored = bosons = None
+    tte = tte_c = spin = grads = stored = bosons = momentum = None
     if not args.no_solve:
         stored = stored_elements(dh, H, flush, dim)
         H.autotune(block_size=BLOCK, repeats=3)
@@ -655,6 +729,7 @@ def run_b200(args, world, rank, local):
         torch.cuda.empty_cache()
         spin = spin_chain_product(dh, flush)
         bosons = boson_product(dh, flush)
+        momentum = momentum_sector(dh, flush)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -678,7 +753,8 @@ def run_b200(args, world, rank, local):
             "gradients": grads,
             "stored_elements": stored,
             "spin_chain_l32": spin,
-            "bosons": bosons}
+            "bosons": bosons,
+            "momentum_sector_l32": momentum}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
         if bosons is not None:
@@ -686,6 +762,11 @@ def run_b200(args, world, rank, local):
                 bosons["cpu_baseline"] = reference_cpu_bosons()
             except (subprocess.CalledProcessError, OSError, ValueError, IndexError) as e:
                 bosons["cpu_baseline"] = {"unavailable": str(e)}
+        if momentum is not None:
+            try:
+                momentum["cpu_baseline"] = reference_cpu_momentum_sector()
+            except (subprocess.CalledProcessError, OSError, ValueError, IndexError) as e:
+                momentum["cpu_baseline"] = {"unavailable": str(e)}
     if rank == 0:
         print(json.dumps(line))
 

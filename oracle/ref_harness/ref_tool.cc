@@ -459,6 +459,7 @@ static void Usage()
 	  "  spint_lanczos L 2Sz K J1 J2 maxiter precision out x0\n"
 	  "  bench_fqhe N 2S 2Lz vfile threads reps hermitian [rows]\n"
 	  "  bench_bqhe N 2S 2Lz vfile threads reps hermitian [rows]\n"
+	  "  bench_spint L 2Sz K J1 J2 threads reps [rows]\n"
 	  "  bench_spin L 2Sz J1 J2 threads reps 0\n");
   exit(1);
 }
@@ -914,6 +915,42 @@ int main(int argc, char** argv)
       printf("{\"dim\": %ld, \"rows\": %ld, \"threads\": %d, \"reps\": %d, \"best_s\": %.6e, \"mean_s\": %.6e, "
 	     "\"setup_s\": %.3f, \"hermitian\": %d, \"xHx\": %.15e}\n", Dim, Rows, Threads, Reps, Best, Total / Reps,
 	     tsetup, Hermitian ? 1 : 0, Check);
+      return 0;
+    }
+  if (strcmp(Cmd, "bench_spint") == 0 && (argc == 9 || argc == 10))
+    {
+      // the reference SMP product of SpinChainJ1J2RealHamiltonianWithTranslations on a momentum sector,
+      // over the first `rows` rows when given (as bench_bqhe)
+      int L = atoi(argv[2]), Sz = atoi(argv[3]), K = atoi(argv[4]);
+      int Threads = atoi(argv[7]);
+      int Reps = atoi(argv[8]);
+      double ts = Now();
+      Spin1_2ChainWithTranslations Chain(L, K, 1, Sz, 1 << 20, 1 << 20);
+      SMPArchitecture Arch(Threads);
+      long Dim = Chain.GetHilbertSpaceDimension();
+      long Rows = (argc == 10) ? atol(argv[9]) : Dim;
+      if (Rows <= 0 || Rows > Dim)
+	Rows = Dim;
+      Arch.SetDimension(Rows);
+      SpinChainJ1J2RealHamiltonianWithTranslations H(&Chain, L, atof(argv[5]), atof(argv[6]));
+      double tsetup = Now() - ts;
+      RealVector X(Dim, true), Y(Dim, true);
+      for (long i = 0; i < Dim; ++i)
+	X[i] = 1.0 / sqrt((double) Dim);
+      double Best = 1e30, Total = 0.0, Check = 0.0;
+      for (int r = 0; r < Reps; ++r)
+	{
+	  VectorHamiltonianMultiplyOperation Op(&H, &X, &Y);
+	  double t0 = Now();
+	  Op.ApplyOperation(&Arch);
+	  double t = Now() - t0;
+	  Total += t;
+	  if (t < Best)
+	    Best = t;
+	  Check = X * Y;
+	}
+      printf("{\"dim\": %ld, \"rows\": %ld, \"threads\": %d, \"reps\": %d, \"best_s\": %.6e, \"mean_s\": %.6e, "
+	     "\"setup_s\": %.3f, \"xHx\": %.15e}\n", Dim, Rows, Threads, Reps, Best, Total / Reps, tsetup, Check);
       return 0;
     }
   if (strcmp(Cmd, "bench_spin") == 0 && argc == 9)
