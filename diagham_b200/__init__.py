@@ -4,6 +4,7 @@ Python view of the C ABI in include/diagham_b200.h (libdiagham_b200.so, built in
 diagham_b200/_build.py).  Class and method names follow the reference classes they replace:
 
     FermionOnSphere                     FQHE/src/HilbertSpace/FermionOnSphere.h
+    FermionOnSphereLong                 FQHE/src/HilbertSpace/FermionOnSphereLong.h
     BosonOnSphereShort                  FQHE/src/HilbertSpace/BosonOnSphereShort.h
     Spin1_2Chain                        Spin/src/HilbertSpace/Spin1_2Chain.h
     ParticleOnSphereGenericHamiltonian  FQHE/src/Hamiltonian/ParticleOnSphereGenericHamiltonian.h
@@ -52,6 +53,9 @@ SIGNATURES = {
     "dh_space_get_dimension": ([_vp, _i64p], _c_int),
     "dh_space_get_states": ([_vp, _vp, _vp, _c_i64, _c_i64], _c_int),
     "dh_space_find_state_index": ([_vp, _vp, _c_i64, _vp], _c_int),
+    "dh_fermion_on_sphere_long_create": ([_c_int, _c_int, _c_int, ctypes.c_ulong, _vp], _c_int),
+    "dh_space_get_states_long": ([_vp, _vp, _vp, _c_i64, _c_i64], _c_int),
+    "dh_space_find_state_index_long": ([_vp, _vp, _c_i64, _vp], _c_int),
     "dh_space_set_index_mode": ([_vp, _c_int], _c_int),
     "dh_fermion_on_sphere_partial_entanglement_matrix": ([_vp, _vp, _c_int, _c_int, _c_int, _vp, _c_i64, _i64p, _i64p],
                                                          _c_int),
@@ -234,6 +238,46 @@ class FermionOnSphere(_Space):
         """rho_A = M M^T of the orbital cut (FermionOnSphere.cc:2070)."""
         return _cut_matrix(self, _lib.dh_fermion_on_sphere_partial_density_matrix, state,
                            (subsystem_size, nbr_fermion_sector, lz_sector), True)
+
+
+class FermionOnSphereLong(_Space):
+    """FermionOnSphereLong(nbrFermions, totalLz, lzMax, memory): FermionOnSphereLong.cc:67, lzMax up to
+    126.  states() gives the 128-bit words as an (n, 2) uint64 array of (low, high) halves;
+    FindStateIndex takes such pairs or Python integers (-1 outside the sector)."""
+
+    def __init__(self, nbr_fermions, total_lz, lz_max, memory=9 << 20):
+        load()
+        h = ctypes.c_void_p()
+        _check(_lib.dh_fermion_on_sphere_long_create(nbr_fermions, total_lz, lz_max, memory, ctypes.byref(h)))
+        self._handle = h
+        self.nbr_fermions, self.total_lz, self.lz_max = nbr_fermions, total_lz, lz_max
+
+    def states(self, first=0, n=None):
+        d = self.dim
+        n = d - first if n is None else n
+        words = np.zeros((n, 2), np.uint64)
+        lz = np.zeros(n, np.int32)
+        _check(_lib.dh_space_get_states_long(self._handle, words.ctypes.data, lz.ctypes.data, first, n))
+        return words, lz
+
+    @staticmethod
+    def word_values(pairs):
+        """Python integers of (low, high) pairs."""
+        return [int(a) | (int(b) << 64) for a, b in np.asarray(pairs, np.uint64).reshape(-1, 2)]
+
+    @staticmethod
+    def word_pairs(values):
+        """(n, 2) uint64 (low, high) pairs of Python integers."""
+        m = (1 << 64) - 1
+        return np.array([[v & m, v >> 64] for v in values], np.uint64).reshape(-1, 2)
+
+    def FindStateIndex(self, words):
+        if not (isinstance(words, np.ndarray) and words.dtype == np.uint64 and words.ndim == 2):
+            words = self.word_pairs([int(w) for w in words])
+        words = np.ascontiguousarray(words, np.uint64)
+        out = np.zeros(words.shape[0], np.int64)
+        _check(_lib.dh_space_find_state_index_long(self._handle, words.ctypes.data, words.shape[0], out.ctypes.data))
+        return out
 
 
 def _cut_matrix(space, fn, state, args, square):

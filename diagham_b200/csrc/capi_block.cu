@@ -1079,6 +1079,8 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
     rc = dh_fermion_on_sphere_create(nbr_fermions, total_lz[s], lz_max, 9ul << 20, &sp);
     if (rc != DH_OK) return rc;
     hb.spaces.push_back(sp);
+    DH_CHECK(sp->kind == SPACE_FERMION, DH_ERR_UNSUPPORTED,
+             "batched sectors use the split-word rank tables (lz_max <= 40), not lz_max = %d", lz_max);
     DH_CHECK(sp->rank.low_bits == hb.spaces[0]->rank.low_bits, DH_ERR_STATE, "sectors disagree on the table split");
     if (sp->dim <= full_diag_limit || sp->dim <= 2 * block_size)
       dense_sectors.push_back(s);

@@ -84,6 +84,50 @@ int build_rank_tables(dh_space_s* sp, int low_bits) {
   return DH_OK;
 }
 
+// counts[n][o][s]: n fermions in orbitals 0..o-1 with orbital-index sum s (o = 0 .. lz_max + 1), and
+// the sector's dimension
+static int fermion_counts(dh_space_s* sp) {
+  const int N = sp->nbr_fermions, L = sp->lz_max, K = sp->total_sum;
+  const int O = L + 2;
+  DH_CHECK((double)(N + 1) * O * (K + 1) <= 64.0 * 1024 * 1024, DH_ERR_UNSUPPORTED,
+           "FermionOnSphere(%d, %d, %d): the count table would exceed 64M entries", N, sp->total_lz, L);
+  sp->counts.assign((size_t)(N + 1) * O * (K + 1), 0);
+  auto C = [&](int n, int o, int s) -> int64_t& { return sp->counts[((size_t)n * O + o) * (K + 1) + s]; };
+  for (int o = 0; o < O; ++o) C(0, o, 0) = 1;
+  for (int n = 1; n <= N; ++n)
+    for (int o = 1; o < O; ++o)
+      for (int s = 0; s <= K; ++s) {
+        int64_t v = C(n, o - 1, s);
+        if (s - (o - 1) >= 0) v += C(n - 1, o - 1, s - (o - 1));
+        // saturate: only counts of states of the sector (at most its dimension) are ever used
+        C(n, o, s) = std::min<int64_t>(v, (int64_t)1 << 62);
+      }
+  const int64_t dim = C(N, L + 1, K);
+  DH_CHECK(dim > 0, DH_ERR_ARGUMENT, "FermionOnSphere(%d, %d, %d): empty sector", N, sp->total_lz, L);
+  DH_CHECK(dim < (1ll << 31), DH_ERR_UNSUPPORTED, "FermionOnSphere: dimension %lld >= 2^31", (long long)dim);
+  sp->dim = dim;
+  return DH_OK;
+}
+
+// FermionOnSphereLong (and FermionOnSphere beyond lz_max = 40): the int32 count table and the words,
+// unranked on the device in the reference's order
+static int build_long_fermion_space(dh_space_s* sp) {
+  int rc = fermion_counts(sp);
+  if (rc != DH_OK) return rc;
+  const int N = sp->nbr_fermions, L = sp->lz_max, K = sp->total_sum;
+  const size_t per_n = (size_t)(L + 2) * (K + 1);
+  std::vector<int32_t> table((size_t)N * per_n);
+  for (int n = 1; n <= N; ++n)
+    for (size_t i = 0; i < per_n; ++i)
+      table[(size_t)(n - 1) * per_n + i] = (int32_t)std::min<int64_t>(sp->counts[(size_t)n * per_n + i], INT32_MAX);
+  if ((rc = sp->long_table.alloc(table.size() * sizeof(int32_t))) != DH_OK) return rc;
+  DH_CUDA(cudaMemcpy(sp->long_table.ptr, table.data(), table.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if ((rc = sp->words.alloc((size_t)sp->dim * 2 * sizeof(uint64_t))) != DH_OK) return rc;
+  if ((rc = launch_long_unrank(fqhe_long_device(sp, nullptr, 0), sp->words.as<uint64_t>(), 0)) != DH_OK) return rc;
+  DH_CUDA(cudaDeviceSynchronize());
+  return DH_OK;
+}
+
 static int build_fermion_space(dh_space_s* sp) {
   const int N = sp->nbr_fermions, L = sp->lz_max, K = sp->total_sum;
   const int O = L + 2;  // orbital counts 0 .. L+1
@@ -178,6 +222,23 @@ FqheDevice fqhe_device(const dh_space_s* sp, const dh_hamiltonian_s* h, int prec
     f.factors = (precision == DH_PRECISION_FP32) ? h->factors32.ptr : h->factors64.ptr;
     f.nbr_pairs = h->tabs.nbr_pairs;
     f.nbr_factors = h->tabs.nbr_factors;
+  }
+  return f;
+}
+
+FqheLongDevice fqhe_long_device(const dh_space_s* sp, const dh_hamiltonian_s* h, int precision) {
+  FqheLongDevice f = {};
+  f.words = sp->words.as<uint64_t>();
+  f.table = sp->long_table.as<int32_t>();
+  f.dim = sp->dim;
+  f.nbr_fermions = sp->nbr_fermions;
+  f.lz_max = sp->lz_max;
+  f.total_sum = sp->total_sum;
+  f.stride_o = sp->total_sum + 1;
+  f.stride_n = (long long)(sp->lz_max + 2) * (sp->total_sum + 1);
+  if (h) {
+    f.pair_offset = h->pair_offset.as<int32_t>();
+    f.factors = (precision == DH_PRECISION_FP32) ? h->factors32.ptr : h->factors64.ptr;
   }
   return f;
 }
@@ -299,6 +360,7 @@ int hamiltonian_apply_rows(dh_hamiltonian_s* h, const double* x, double* y, int 
   }
   if (sp->kind == SPACE_BOSON) return launch_boson_matvec(fqhe_device(sp, h, h->precision), a, h->precision, stream);
   if (sp->kind == SPACE_SPIN12_TRANSLATIONS) return launch_trans_matvec(trans_device(sp, h), a, h->precision, stream);
+  if (sp->kind == SPACE_FERMION_LONG) return launch_long_matvec(fqhe_long_device(sp, h, h->precision), a, h->precision, stream);
   if (sp->kind == SPACE_FERMION) {
     if (h->fast && h->fast_use && first == 0 && nbr == dim) return launch_ell_product(ell_device(h, h->precision), a, h->precision, stream);
     if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
@@ -341,6 +403,7 @@ int hamiltonian_apply_block_rows(dh_hamiltonian_s* h, const double* x64, const f
   int rc;
   if (sp->kind == SPACE_BOSON) return launch_boson_matvec(fqhe_device(sp, h, precision), a, precision, stream);
   if (sp->kind == SPACE_SPIN12_TRANSLATIONS) return launch_trans_matvec(trans_device(sp, h), a, precision, stream);
+  if (sp->kind == SPACE_FERMION_LONG) return launch_long_matvec(fqhe_long_device(sp, h, precision), a, precision, stream);
   if (sp->kind == SPACE_FERMION) {
     if (h->fast && h->fast_use) return launch_ell_product(ell_device(h, precision), a, precision, stream);
     if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
@@ -376,7 +439,8 @@ int dh_fermion_on_sphere_create(int nbr_fermions, int total_lz, int lz_max, unsi
   DH_CHECK(nbr_fermions >= 1, DH_ERR_ARGUMENT, "FermionOnSphere: nbr_fermions must be >= 1");
   DH_CHECK(lz_max >= nbr_fermions - 1, DH_ERR_ARGUMENT, "FermionOnSphere: %d fermions do not fit in %d orbitals",
            nbr_fermions, lz_max + 1);
-  DH_CHECK(lz_max <= 40, DH_ERR_UNSUPPORTED, "FermionOnSphere: lz_max = %d > 40 is not supported", lz_max);
+  DH_CHECK(lz_max <= 62, DH_ERR_UNSUPPORTED,
+           "FermionOnSphere: lz_max = %d > 62 does not fit 64-bit words (FermionOnSphereLong takes up to 126)", lz_max);
   const int twice = total_lz + nbr_fermions * lz_max;
   DH_CHECK(twice >= 0 && (twice & 1) == 0, DH_ERR_ARGUMENT,
            "FermionOnSphere: total_lz = %d is not reachable by %d fermions with lz_max = %d", total_lz, nbr_fermions,
@@ -390,6 +454,18 @@ int dh_fermion_on_sphere_create(int nbr_fermions, int total_lz, int lz_max, unsi
   sp->total_sum = twice / 2;
   sp->memory = memory;
   sp->index_mode = DH_INDEX_RANK;
+  if (lz_max > 40) {
+    // beyond the split-word tables: the per-fermion ranks of the 128-bit engine, 64-bit words outside
+    sp->kind = SPACE_FERMION_LONG;
+    sp->api_halves = 1;
+    int rc = build_long_fermion_space(sp);
+    if (rc != DH_OK) {
+      delete sp;
+      return rc;
+    }
+    *out = sp;
+    return DH_OK;
+  }
   // product kernel of the rank mode: split-word (default) or the generic one (DH_FQHE_KERNEL=generic)
   // DH_FQHE_LOW_BITS sets the split of the rank tables; "smem" stages the low-rank table in shared
   // memory (the split is then lowered until the table fits in 64 KiB)
@@ -405,6 +481,35 @@ int dh_fermion_on_sphere_create(int nbr_fermions, int total_lz, int lz_max, unsi
     return rc;
   }
   *out = sp;
+  return DH_OK;
+}
+
+int dh_fermion_on_sphere_long_create(int nbr_fermions, int total_lz, int lz_max, unsigned long memory,
+                                     dh_space_t* out) {
+  DH_CHECK(out, DH_ERR_ARGUMENT, "null output handle");
+  *out = nullptr;
+  DH_CHECK(nbr_fermions >= 1, DH_ERR_ARGUMENT, "FermionOnSphereLong: nbr_fermions must be >= 1");
+  DH_CHECK(lz_max >= nbr_fermions - 1, DH_ERR_ARGUMENT, "FermionOnSphereLong: %d fermions do not fit in %d orbitals",
+           nbr_fermions, lz_max + 1);
+  DH_CHECK(lz_max >= 1 && lz_max <= 126, DH_ERR_UNSUPPORTED, "FermionOnSphereLong: lz_max = %d not in 1..126", lz_max);
+  const int twice = total_lz + nbr_fermions * lz_max;
+  DH_CHECK(twice >= 0 && (twice & 1) == 0, DH_ERR_ARGUMENT,
+           "FermionOnSphereLong: total_lz = %d is not reachable by %d fermions with lz_max = %d", total_lz,
+           nbr_fermions, lz_max);
+  dh_space_s* sp = new (std::nothrow) dh_space_s();
+  DH_CHECK(sp, DH_ERR_MEMORY, "out of host memory");
+  std::unique_ptr<dh_space_s> guard(sp);
+  sp->kind = SPACE_FERMION_LONG;
+  sp->api_halves = 2;
+  sp->nbr_fermions = nbr_fermions;
+  sp->lz_max = lz_max;
+  sp->total_lz = total_lz;
+  sp->total_sum = twice / 2;
+  sp->memory = memory;
+  sp->index_mode = DH_INDEX_RANK;
+  int rc = build_long_fermion_space(sp);
+  if (rc != DH_OK) return rc;
+  *out = guard.release();
   return DH_OK;
 }
 
@@ -556,6 +661,14 @@ int dh_space_get_states(dh_space_t sp, uint64_t* words, int* lz_max, int64_t fir
     DH_CUDA(cudaMemcpy(words, sp->words.as<uint64_t>() + first, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
     if (lz_max)
       for (int64_t i = 0; i < n; ++i) lz_max[i] = words[i] ? 63 - __builtin_clzll(words[i]) : 0;
+  } else if (sp->kind == SPACE_FERMION_LONG) {
+    DH_CHECK(sp->lz_max <= 63, DH_ERR_UNSUPPORTED,
+             "lz_max = %d: the states are 128-bit words (dh_space_get_states_long)", sp->lz_max);
+    // the low halves of the (low, high) pairs
+    DH_CUDA(cudaMemcpy2D(words, sizeof(uint64_t), sp->words.as<uint64_t>() + 2 * first, 2 * sizeof(uint64_t),
+                         sizeof(uint64_t), n, cudaMemcpyDeviceToHost));
+    if (lz_max)
+      for (int64_t i = 0; i < n; ++i) lz_max[i] = words[i] ? 63 - __builtin_clzll(words[i]) : 0;
   } else if (sp->kind == SPACE_SPIN12_TRANSLATIONS) {
     std::vector<uint32_t> w(n);
     DH_CUDA(cudaMemcpy(w.data(), sp->words.as<uint32_t>() + first, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
@@ -571,6 +684,66 @@ int dh_space_get_states(dh_space_t sp, uint64_t* words, int* lz_max, int64_t fir
     if (lz_max)
       for (int64_t i = 0; i < n; ++i) lz_max[i] = 0;
   }
+  return DH_OK;
+}
+
+int dh_space_get_states_long(dh_space_t sp, uint64_t* words, int* lz_max, int64_t first, int64_t n) {
+  DH_CHECK(sp && words, DH_ERR_ARGUMENT, "null argument");
+  DH_CHECK(sp->kind == SPACE_FERMION || sp->kind == SPACE_FERMION_LONG, DH_ERR_UNSUPPORTED,
+           "128-bit words exist for fermion spaces");
+  DH_CHECK(first >= 0 && n >= 0 && first + n <= sp->dim, DH_ERR_ARGUMENT, "state range out of bounds");
+  if (n == 0) return DH_OK;
+  if (sp->kind == SPACE_FERMION) {
+    DH_CUDA(cudaMemcpy2D(words, 2 * sizeof(uint64_t), sp->words.as<uint64_t>() + first, sizeof(uint64_t),
+                         sizeof(uint64_t), n, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < n; ++i) words[2 * i + 1] = 0;
+  } else {
+    DH_CUDA(cudaMemcpy(words, sp->words.as<uint64_t>() + 2 * first, n * 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  }
+  if (lz_max)
+    for (int64_t i = 0; i < n; ++i) {
+      const uint64_t lo = words[2 * i], hi = words[2 * i + 1];
+      lz_max[i] = hi ? 127 - __builtin_clzll(hi) : (lo ? 63 - __builtin_clzll(lo) : 0);
+    }
+  return DH_OK;
+}
+
+int dh_space_find_state_index_long(dh_space_t sp, const uint64_t* words, int64_t n, int64_t* indices) {
+  DH_CHECK(sp && words && indices, DH_ERR_ARGUMENT, "null argument");
+  DH_CHECK(sp->kind == SPACE_FERMION || sp->kind == SPACE_FERMION_LONG, DH_ERR_UNSUPPORTED,
+           "128-bit words exist for fermion spaces");
+  if (n <= 0) return DH_OK;
+  std::vector<uint64_t> host;
+  const uint64_t* src = words;
+  if (is_device_pointer(words)) {
+    host.resize(2 * n);
+    DH_CUDA(cudaMemcpy(host.data(), words, 2 * n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    src = host.data();
+  }
+  if (sp->kind == SPACE_FERMION) {
+    // words with high bits are not states of a 64-bit space
+    std::vector<uint64_t> low(n);
+    std::vector<int64_t> idx(n);
+    for (int64_t i = 0; i < n; ++i) low[i] = src[2 * i];
+    int rc = dh_space_find_state_index(sp, low.data(), n, idx.data());
+    if (rc != DH_OK) return rc;
+    for (int64_t i = 0; i < n; ++i)
+      if (src[2 * i + 1]) idx[i] = -1;
+    if (is_device_pointer(indices))
+      DH_CUDA(cudaMemcpy(indices, idx.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
+    else
+      memcpy(indices, idx.data(), n * sizeof(int64_t));
+    return DH_OK;
+  }
+  DevBuf dw, di;
+  int rc;
+  if ((rc = dw.alloc(2 * n * sizeof(uint64_t))) != DH_OK || (rc = di.alloc(n * sizeof(int64_t))) != DH_OK) return rc;
+  DH_CUDA(cudaMemcpy(dw.ptr, src, 2 * n * sizeof(uint64_t), cudaMemcpyHostToDevice));
+  if ((rc = launch_long_find(fqhe_long_device(sp, nullptr, 0), dw.as<uint64_t>(), n, di.as<long long>(), 0)) != DH_OK)
+    return rc;
+  DH_CUDA(cudaDeviceSynchronize());
+  DH_CUDA(cudaMemcpy(indices, di.ptr, n * sizeof(int64_t),
+                     is_device_pointer(indices) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost));
   return DH_OK;
 }
 
@@ -607,6 +780,15 @@ int dh_space_find_state_index(dh_space_t sp, const uint64_t* words, int64_t n, i
   if (sp->kind == SPACE_FERMION || sp->kind == SPACE_BOSON) {
     if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
     rc = launch_fqhe_find(fqhe_device(sp, nullptr, 0), w, n, reinterpret_cast<long long*>(out), 0);
+  } else if (sp->kind == SPACE_FERMION_LONG) {
+    // 64-bit words as (word, 0) pairs
+    DevBuf pairs;
+    if ((rc = pairs.alloc(2 * n * sizeof(uint64_t))) != DH_OK) return rc;
+    DH_CUDA(cudaMemset(pairs.ptr, 0, 2 * n * sizeof(uint64_t)));
+    DH_CUDA(cudaMemcpy2D(pairs.ptr, 2 * sizeof(uint64_t), w, sizeof(uint64_t), sizeof(uint64_t), n,
+                         cudaMemcpyDeviceToDevice));
+    rc = launch_long_find(fqhe_long_device(sp, nullptr, 0), pairs.as<uint64_t>(), n, reinterpret_cast<long long*>(out), 0);
+    if (rc == DH_OK) DH_CUDA(cudaDeviceSynchronize());
   } else if (sp->kind == SPACE_SPIN12_TRANSLATIONS) {
     rc = launch_trans_find(trans_device(sp, nullptr), w, n, reinterpret_cast<long long*>(out), 0);
   } else {
@@ -626,8 +808,8 @@ int dh_particle_on_sphere_generic_hamiltonian_create(dh_space_t sp, int nbr_part
   DH_CHECK(out, DH_ERR_ARGUMENT, "null output handle");
   *out = nullptr;
   DH_CHECK(sp && pseudopotentials, DH_ERR_ARGUMENT, "null argument");
-  DH_CHECK(sp->kind == SPACE_FERMION || sp->kind == SPACE_BOSON, DH_ERR_ARGUMENT,
-           "ParticleOnSphereGenericHamiltonian needs a FermionOnSphere or BosonOnSphereShort space");
+  DH_CHECK(sp->kind == SPACE_FERMION || sp->kind == SPACE_FERMION_LONG || sp->kind == SPACE_BOSON, DH_ERR_ARGUMENT,
+           "ParticleOnSphereGenericHamiltonian needs a FermionOnSphere(Long) or BosonOnSphereShort space");
   const bool bosons = sp->kind == SPACE_BOSON;
   const int space_lz_max = bosons ? sp->boson_lz_max : sp->lz_max;
   DH_CHECK(nbr_particles == sp->nbr_fermions && lz_max == space_lz_max, DH_ERR_ARGUMENT,
@@ -680,7 +862,8 @@ int dh_particle_on_sphere_l2_hamiltonian_create(dh_space_t sp, int nbr_particles
                                                 double l2_factor, dh_hamiltonian_t* out) {
   DH_CHECK(out, DH_ERR_ARGUMENT, "null output handle");
   *out = nullptr;
-  DH_CHECK(sp && sp->kind == SPACE_FERMION, DH_ERR_ARGUMENT, "ParticleOnSphereL2Hamiltonian needs a FermionOnSphere space");
+  DH_CHECK(sp && (sp->kind == SPACE_FERMION || sp->kind == SPACE_FERMION_LONG), DH_ERR_ARGUMENT,
+           "ParticleOnSphereL2Hamiltonian needs a FermionOnSphere(Long) space");
   DH_CHECK(total_lz == sp->total_lz, DH_ERR_ARGUMENT, "total_lz %d does not match the space's %d", total_lz, sp->total_lz);
   DH_CHECK(l2_factor != 0.0, DH_ERR_ARGUMENT, "l2_factor must not be 0");
   std::vector<double> zero(lz_max + 1, 0.0);
@@ -743,8 +926,8 @@ int dh_hamiltonian_set_precision(dh_hamiltonian_t h, int precision) {
 
 int dh_hamiltonian_set_pseudopotentials(dh_hamiltonian_t h, const double* v) {
   DH_CHECK(h && v, DH_ERR_ARGUMENT, "null argument");
-  DH_CHECK((h->kind == SPACE_FERMION || h->kind == SPACE_BOSON) && !h->l2_only, DH_ERR_ARGUMENT,
-           "pseudopotentials only apply to FQHE interaction Hamiltonians");
+  DH_CHECK((h->kind == SPACE_FERMION || h->kind == SPACE_FERMION_LONG || h->kind == SPACE_BOSON) && !h->l2_only,
+           DH_ERR_ARGUMENT, "pseudopotentials only apply to FQHE interaction Hamiltonians");
   h->v.assign(v, v + h->tabs.lz_max + 1);
   h->tabs.set_pseudopotentials(h->v.data());
   int rc = upload_factors(h);
@@ -1146,7 +1329,7 @@ int dh_hamiltonian_row_elements(dh_hamiltonian_t h, int64_t row, int* targets, i
 
 int dh_hamiltonian_get_interaction_factors(dh_hamiltonian_t h, double* factors, int cap, int* count) {
   DH_CHECK(h && count, DH_ERR_ARGUMENT, "null argument");
-  DH_CHECK(h->kind == SPACE_FERMION || h->kind == SPACE_BOSON, DH_ERR_UNSUPPORTED,
+  DH_CHECK(h->kind == SPACE_FERMION || h->kind == SPACE_FERMION_LONG || h->kind == SPACE_BOSON, DH_ERR_UNSUPPORTED,
            "interaction factors only exist for FQHE Hamiltonians");
   *count = h->tabs.nbr_factors;
   const int n = std::min(cap, h->tabs.nbr_factors);
@@ -1199,6 +1382,19 @@ int dh_hamiltonian_pseudopotential_adjoint(dh_hamiltonian_t h, const double* u, 
 int dh_hamiltonian_count_elements(dh_hamiltonian_t h, int64_t* total) {
   DH_CHECK(h && total, DH_ERR_ARGUMENT, "null argument");
   dh_space_s* sp = h->space;
+  if (h->kind == SPACE_FERMION_LONG) {
+    DevBuf t;
+    int rc;
+    if ((rc = t.alloc(sizeof(unsigned long long))) != DH_OK) return rc;
+    if ((rc = launch_long_count(fqhe_long_device(sp, h, DH_PRECISION_FP64), t.as<unsigned long long>(), h->stream)) !=
+        DH_OK)
+      return rc;
+    unsigned long long v = 0;
+    DH_CUDA(cudaMemcpyAsync(&v, t.ptr, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+    DH_CUDA(cudaStreamSynchronize(h->stream));
+    *total = (int64_t)v;
+    return DH_OK;
+  }
   if (h->kind == SPACE_SPIN12_TRANSLATIONS) {
     // the flips whose word lies in the momentum sector (the others are dropped, as the reference's
     // SymmetrizeResult returns no index for them)
@@ -1243,7 +1439,7 @@ int dh_hamiltonian_count_diagonal_elements(dh_hamiltonian_t h, int64_t* total) {
     *total = 0;  // the chain's elements are its flips; the Sz Sz part is computed per row
     return DH_OK;
   }
-  if (h->kind == SPACE_FERMION) {
+  if (h->kind == SPACE_FERMION || h->kind == SPACE_FERMION_LONG) {
     // every occupied pair m1 > m2 has one move back to its row (m3 = m1, m4 = m2)
     const long long n = sp->nbr_fermions;
     *total = (int64_t)(n * (n - 1) / 2) * sp->dim;
@@ -1262,14 +1458,14 @@ int dh_hamiltonian_count_diagonal_elements(dh_hamiltonian_t h, int64_t* total) {
 }
 
 int dh_coulomb_pseudopotentials(int nbr_flux, double* v) {
-  DH_CHECK(v && nbr_flux >= 1 && nbr_flux <= 60, DH_ERR_ARGUMENT, "nbr_flux must be in 1..60");
+  DH_CHECK(v && nbr_flux >= 1 && nbr_flux <= 126, DH_ERR_ARGUMENT, "nbr_flux must be in 1..126");
   coulomb_pseudopotentials(nbr_flux, v);
   return DH_OK;
 }
 
 int dh_clebsch_gordan(int j1, int m1, int j2, int m2, int j, double* out) {
   DH_CHECK(out, DH_ERR_ARGUMENT, "null output");
-  DH_CHECK(j1 >= 0 && j2 >= 0 && j >= 0 && j1 + j2 + j < 300, DH_ERR_ARGUMENT, "angular momenta out of range");
+  DH_CHECK(j1 >= 0 && j2 >= 0 && j >= 0 && j1 + j2 + j <= 1196, DH_ERR_ARGUMENT, "angular momenta out of range");
   *out = clebsch_gordan(j1, m1, j2, m2, j);
   return DH_OK;
 }

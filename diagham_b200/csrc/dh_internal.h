@@ -80,7 +80,14 @@ int tridiagonal_eigen(int n, const double* diag, const double* off, double* eig,
 int symmetric_eigen(int n, double* a, double* eig, double* z);
 
 // ------------------------------------------------------------- spaces
-enum SpaceKind { SPACE_FERMION = 1, SPACE_SPIN12 = 2, SPACE_BOSON = 3, SPACE_SPIN12_TRANSLATIONS = 4 };
+enum SpaceKind {
+  SPACE_FERMION = 1,
+  SPACE_SPIN12 = 2,
+  SPACE_BOSON = 3,
+  SPACE_SPIN12_TRANSLATIONS = 4,
+  // FermionOnSphere with 41 <= lz_max <= 62 and FermionOnSphereLong: 128-bit words, per-fermion ranks
+  SPACE_FERMION_LONG = 5
+};
 
 struct FermionRankTables {
   int low_bits = 0;                 // LB: rank = high_offset[w >> LB] + low_rank[w & (2^LB - 1)]
@@ -108,6 +115,18 @@ struct FqheDevice {
   int kernel_variant;          // 0: split-word rank kernel, 1: generic kernel (rank mode)
   int boson_lz_max;            // BosonOnSphereShort: orbitals 0..boson_lz_max (words of lz_max + 1 bits)
   int nbr_bosons;
+};
+
+// Fermions with 128-bit words (FermionOnSphereLong, and FermionOnSphere beyond the split-word tables)
+struct FqheLongDevice {
+  const uint64_t* words;        // [dim][2]: low and high 64 bits of each state, descending
+  const int32_t* table;         // C(n, o, s) at (n - 1) * stride_n + o * stride_o + s (saturated at 2^31 - 1)
+  const int32_t* pair_offset;   // [nbr_pairs]
+  const void* factors;          // FP64 or FP32 [nbr_factors]
+  long long dim;
+  long long stride_n;           // (lz_max + 2) * (total_sum + 1)
+  int stride_o;                 // total_sum + 1
+  int nbr_fermions, lz_max, total_sum;
 };
 
 struct MatvecArgs {
@@ -173,6 +192,10 @@ int launch_fqhe_unrank(int nbr_fermions, int lz_max, int total_sum, long long di
 int launch_fqhe_matvec(const FqheDevice& f, const MatvecArgs& a, int precision, cudaStream_t s);
 // BosonOnSphereShort product (kernels_boson.cu), any vector layout, K = 1, 2, 4 (else in passes)
 int launch_boson_matvec(const FqheDevice& f, const MatvecArgs& a, int precision, cudaStream_t s);
+int launch_long_unrank(const FqheLongDevice& f, uint64_t* words, cudaStream_t s);
+int launch_long_find(const FqheLongDevice& f, const uint64_t* words, long long n, long long* out, cudaStream_t s);
+int launch_long_count(const FqheLongDevice& f, unsigned long long* total, cudaStream_t s);
+int launch_long_matvec(const FqheLongDevice& f, const MatvecArgs& a, int precision, cudaStream_t s);
 // total[0] = generated elements, total[1] = those that return to their row (one per annihilated pair)
 int launch_boson_count(const FqheDevice& f, unsigned long long* total, cudaStream_t s);
 int launch_fqhe_row_elements(const FqheDevice& f, long long row, int* targets, int* signs, int* factor_index,

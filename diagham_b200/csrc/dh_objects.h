@@ -25,6 +25,10 @@ struct dh_space_s {
   // N fermions in boson_lz_max + N orbitals (nbr_fermions = N, lz_max = boson_lz_max + N - 1)
   int boson_lz_max = -1;
   unsigned long memory = 0;
+  // SPACE_FERMION_LONG: words are (low, high) pairs; the int32 count table; api_halves = 1 when the
+  // space was created as FermionOnSphere (its words are 64-bit for dh_space_get_states)
+  dh::DevBuf long_table;
+  int api_halves = 2;
   dh::FermionRankTables rank;
   dh::DevBuf low_rank, high_offset;
   dh::DevBuf lookup, lookup_shift;
@@ -92,6 +96,7 @@ int hamiltonian_apply_block_rows(dh_hamiltonian_s* h, const double* x64, const f
                                  int precision, cudaStream_t stream, int64_t out_first, int64_t out_last);
 SpinDevice spin_device(const dh_space_s* sp, const dh_hamiltonian_s* h);
 TransDevice trans_device(const dh_space_s* sp, const dh_hamiltonian_s* h);
+FqheLongDevice fqhe_long_device(const dh_space_s* sp, const dh_hamiltonian_s* h, int precision);
 int upload_factors(dh_hamiltonian_s* h);
 // (re)build the split-word rank tables of a FermionOnSphere space for a split of low_bits (0: the
 // default, or the space's requested split) and upload them

@@ -97,14 +97,49 @@ inline DD dd_sqrt(DD a) {
   return quick_two_sum(x, r.hi / (2.0 * x));
 }
 
-constexpr int kMaxFactorial = 170;
-const std::vector<DD>& factorials() {
-  static std::vector<DD> f;
+// A double-double mantissa with a binary exponent (value = m * 2^e, |m.hi| in [0.5, 1)): factorials
+// up to kMaxFactorial and Racah's products of six of them stay representable, and because scaling by
+// powers of two is exact the digits are those of plain double-double arithmetic.
+struct XD {
+  DD m;
+  int e;
+};
+inline XD xnorm(DD m, int e) {
+  if (m.hi == 0.0) return {dd(0.0), 0};
+  int k;
+  frexp(m.hi, &k);
+  return {{ldexp(m.hi, -k), ldexp(m.lo, -k)}, e + k};
+}
+inline XD xd(double a) { return xnorm(dd(a), 0); }
+inline XD operator*(XD a, XD b) { return xnorm(a.m * b.m, a.e + b.e); }
+inline XD operator/(XD a, XD b) { return xnorm(a.m / b.m, a.e - b.e); }
+inline XD operator-(XD a) { return {-a.m, a.e}; }
+inline XD operator+(XD a, XD b) {
+  if (a.m.hi == 0.0) return b;
+  if (b.m.hi == 0.0) return a;
+  if (a.e < b.e) std::swap(a, b);
+  const int d = a.e - b.e;
+  if (d > 240) return a;
+  return xnorm(a.m + DD{ldexp(b.m.hi, -d), ldexp(b.m.lo, -d)}, a.e);
+}
+inline XD xsqrt(XD a) {
+  if (a.m.hi <= 0.0) return {dd(0.0), 0};
+  if (a.e & 1) {
+    a.m = a.m * dd(2.0);
+    a.e -= 1;
+  }
+  return xnorm(dd_sqrt(a.m), a.e / 2);
+}
+inline double xvalue(XD a) { return ldexp(a.m.hi, a.e) + ldexp(a.m.lo, a.e); }
+
+constexpr int kMaxFactorial = 600;
+const std::vector<XD>& factorials() {
+  static std::vector<XD> f;
   static std::once_flag once;
   std::call_once(once, [] {
     f.resize(kMaxFactorial + 1);
-    f[0] = dd(1.0);
-    for (int n = 1; n <= kMaxFactorial; ++n) f[n] = f[n - 1] * dd((double)n);
+    f[0] = xd(1.0);
+    for (int n = 1; n <= kMaxFactorial; ++n) f[n] = f[n - 1] * xd((double)n);
   });
   return f;
 }
@@ -112,7 +147,7 @@ const std::vector<DD>& factorials() {
 
 // Racah's formula for <j1 m1; j2 m2 | j m1+m2>, Condon-Shortley phase; doubled arguments.
 double clebsch_gordan(int j1, int m1, int j2, int m2, int j) {
-  const std::vector<DD>& F = factorials();
+  const std::vector<XD>& F = factorials();
   int m = m1 + m2;
   if (abs(m1) > j1 || abs(m2) > j2 || abs(m) > j) return 0.0;
   if (((j1 + m1) | (j2 + m2) | (j + m) | (j1 + j2 + j)) & 1) return 0.0;
@@ -122,17 +157,29 @@ double clebsch_gordan(int j1, int m1, int j2, int m2, int j) {
   const int jm1 = (j1 - m1) / 2, jp1 = (j1 + m1) / 2, jm2 = (j2 - m2) / 2, jp2 = (j2 + m2) / 2;
   const int Jm = (j - m) / 2, Jp = (j + m) / 2;
   const int e1 = (j - j2 + m1) / 2, e2 = (j - j1 - m2) / 2;
-  DD norm2 = dd((double)(j + 1)) * F[a] * F[b] * F[c] / F[d];
+  XD norm2 = xd((double)(j + 1)) * F[a] * F[b] * F[c] / F[d];
   norm2 = norm2 * (F[Jp] * F[Jm] * F[jm1] * F[jp1] * F[jm2] * F[jp2]);
   int kmin = std::max(0, std::max(-e1, -e2));
   int kmax = std::min(a, std::min(jm1, jp2));
-  DD sum = dd(0.0);
-  for (int k = kmin; k <= kmax; ++k) {
-    DD t = dd(1.0) / (F[k] * F[a - k] * F[jm1 - k] * F[jp2 - k] * F[e1 + k] * F[e2 + k]);
-    sum = (k & 1) ? sum + (-t) : sum + t;
+  // sum over k of (-1)^k / (k! (a-k)! (jm1-k)! (jp2-k)! (e1+k)! (e2+k)!): the first term with its
+  // exponent, then the terms relative to it by their ratio, a ratio of integers below 2^53
+  // -(a-k)(jm1-k)(jp2-k) / ((k+1)(e1+k+1)(e2+k+1)), in double-double
+  XD first = xd((kmin & 1) ? -1.0 : 1.0) /
+             (F[kmin] * F[a - kmin] * F[jm1 - kmin] * F[jp2 - kmin] * F[e1 + kmin] * F[e2 + kmin]);
+  DD term = dd(1.0), sum = dd(1.0);
+  int scale = 0;  // sum and term are held times 2^-scale
+  for (int k = kmin; k < kmax; ++k) {
+    const double num = (double)(a - k) * (double)(jm1 - k) * (double)(jp2 - k);
+    const double den = (double)(k + 1) * (double)(e1 + k + 1) * (double)(e2 + k + 1);
+    term = term * dd(-num) / dd(den);
+    sum = sum + term;
+    if (fabs(term.hi) > 0x1p400) {
+      term = {ldexp(term.hi, -400), ldexp(term.lo, -400)};
+      sum = {ldexp(sum.hi, -400), ldexp(sum.lo, -400)};
+      scale += 400;
+    }
   }
-  DD r = dd_sqrt(norm2) * sum;
-  return r.hi + r.lo;
+  return xvalue(xsqrt(norm2) * first * xnorm(sum, scale));
 }
 
 // Lowest-Landau-level Coulomb pseudopotentials on the sphere: the multipole expansion of
@@ -191,10 +238,11 @@ void InteractionTables::build(int lzmax) {
   pair_offset[nbr_pairs] = nf;
   nbr_factors = nf;
   dfactor.assign((size_t)nf * nlz, 0.0);
-  // CG table over the pair's doubled projections: cg[(i1 * nlz + i2) * nlz + J/2]
+  // CG table over the pair's doubled projections: cg[(i1 * nlz + i2) * nlz + J/2], for the ordered
+  // pairs i1 > i2 that the factors use (m1 > m2 and m3 > m4)
   std::vector<double> cg((size_t)nlz * nlz * nlz, 0.0);
   for (int i1 = 0; i1 < nlz; ++i1)
-    for (int i2 = 0; i2 < nlz; ++i2)
+    for (int i2 = 0; i2 < i1; ++i2)
       for (int J = 0; J <= 2 * lzmax; J += 2)
         cg[((size_t)i1 * nlz + i2) * nlz + J / 2] = clebsch_gordan(lzmax, 2 * i1 - lzmax, lzmax, 2 * i2 - lzmax, J);
   for (int m1 = 0; m1 < nlz; ++m1)

@@ -1,0 +1,350 @@
+// Spin-polarised fermions on the sphere beyond the split-word rank tables: FermionOnSphere with
+// 41 <= lz_max <= 62 and FermionOnSphereLong (FQHE/src/HilbertSpace/FermionOnSphereLong.cc, lz_max up
+// to 126, one 128-bit word per state) on sm_100a.
+//
+// Words are two 64-bit halves (orbital m = bit m of low | high << 64).  States are in the reference's
+// order: descending words (FermionOnSphereLong::GenerateStates, .cc:911-943, places the highest
+// fermion as high as it can first).
+//
+// Rank.  With C(n, o, s) the number of ways to put n fermions in orbitals 0..o-1 with orbital sum s
+// (the sector's count table), the states below w in that order are, fermion by fermion, those that
+// keep every fermion above it and move it (and the ones below) lower with the same sum:
+//     index(w) = dim - 1 - sum over fermions i of C(n_i, p_i, s_i),
+// p_i the fermion's orbital, n_i the number of fermions at or below p_i and s_i the sum of their
+// orbitals.  One table load per fermion.  A move of two fermions m1, m2 -> m3, m4 (same sum) leaves
+// n_i and s_i of every fermion below min(m2, m4) and above max(m1, m3) unchanged, so the target's
+// index is the row's own index corrected over that orbital range only.  The counts used are numbers
+// of states of the sector, so they fit the int32 table (entries that no state uses saturate).
+//
+// Product.  Pull form, one thread per row, the factor tables of the generic Hamiltonian (pair m1 > m2,
+// then the creations m3 > m4 = m1 + m2 - m3) read through the read-only cache (at lz_max = 126 they
+// are 1.4 MB), the AA * AdAd sign from popcounts as in the 64-bit kernels (FermionOnSphere::AA
+// FermionOnSphere.cc:790, ::AdAd :949; FermionOnSphereLong.cc keeps the same conventions).  H is
+// real symmetric, so the pull form equals the reference's push form
+// (AbstractQHEOnSphereHamiltonian.cc:456-488).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dh_internal.h"
+
+namespace dh {
+
+namespace {
+
+constexpr int kLongThreads = 256;
+
+struct U128 {
+  uint64_t lo, hi;
+};
+
+__device__ __forceinline__ U128 u_and(U128 a, U128 b) { return {a.lo & b.lo, a.hi & b.hi}; }
+__device__ __forceinline__ U128 u_or(U128 a, U128 b) { return {a.lo | b.lo, a.hi | b.hi}; }
+__device__ __forceinline__ U128 u_not(U128 a) { return {~a.lo, ~a.hi}; }
+__device__ __forceinline__ bool u_any(U128 a) { return (a.lo | a.hi) != 0ull; }
+__device__ __forceinline__ int u_popc(U128 a) { return __popcll(a.lo) + __popcll(a.hi); }
+__device__ __forceinline__ U128 u_bit(int q) {
+  return q < 64 ? U128{1ull << q, 0ull} : U128{0ull, 1ull << (q - 64)};
+}
+// bits 0 .. q-1 (0 <= q <= 128)
+__device__ __forceinline__ U128 u_below(int q) {
+  if (q <= 0) return {0ull, 0ull};
+  if (q < 64) return {(1ull << q) - 1ull, 0ull};
+  if (q == 64) return {~0ull, 0ull};
+  if (q < 128) return {~0ull, (1ull << (q - 64)) - 1ull};
+  return {~0ull, ~0ull};
+}
+// bits strictly between lo and hi (lo < hi)
+__device__ __forceinline__ U128 u_between(int lo, int hi) { return u_and(u_below(hi), u_not(u_below(lo + 1))); }
+__device__ __forceinline__ int u_lowest(U128 a) { return a.lo ? __ffsll(a.lo) - 1 : 64 + __ffsll(a.hi) - 1; }
+__device__ __forceinline__ U128 u_clear_lowest(U128 a) {
+  if (a.lo) return {a.lo & (a.lo - 1ull), a.hi};
+  return {0ull, a.hi & (a.hi - 1ull)};
+}
+__device__ __forceinline__ int u_highest(U128 a) { return a.hi ? 127 - __clzll(a.hi) : 63 - __clzll(a.lo); }
+__device__ __forceinline__ U128 u_shr(U128 a, int n) {  // 0 <= n < 256
+  if (n == 0) return a;
+  if (n >= 128) return {0ull, 0ull};
+  if (n >= 64) return {a.hi >> (n - 64), 0ull};
+  return {(a.lo >> n) | (a.hi << (64 - n)), a.hi >> n};
+}
+__device__ __forceinline__ U128 u_shl(U128 a, int n) {  // 0 <= n < 256
+  if (n == 0) return a;
+  if (n >= 128) return {0ull, 0ull};
+  if (n >= 64) return {0ull, a.lo << (n - 64)};
+  return {a.lo << n, (a.hi << n) | (a.lo >> (64 - n))};
+}
+// bit p of the result = bit (M - p) of e (0 when M - p is outside 0..127)
+__device__ __forceinline__ U128 u_mirror(U128 e, int M) {
+  const U128 r = {__brevll(e.hi), __brevll(e.lo)};  // bit p = bit 127 - p of e
+  return (M <= 127) ? u_shr(r, 127 - M) : u_shl(r, M - 127);
+}
+// sum of the positions of the set bits
+__device__ __forceinline__ int u_position_sum(U128 a) {
+  const uint64_t m0 = 0xaaaaaaaaaaaaaaaaull, m1 = 0xccccccccccccccccull, m2 = 0xf0f0f0f0f0f0f0f0ull,
+                 m3 = 0xff00ff00ff00ff00ull, m4 = 0xffff0000ffff0000ull, m5 = 0xffffffff00000000ull;
+  return (__popcll(a.lo & m0) + __popcll(a.hi & m0)) + 2 * (__popcll(a.lo & m1) + __popcll(a.hi & m1)) +
+         4 * (__popcll(a.lo & m2) + __popcll(a.hi & m2)) + 8 * (__popcll(a.lo & m3) + __popcll(a.hi & m3)) +
+         16 * (__popcll(a.lo & m4) + __popcll(a.hi & m4)) + 32 * (__popcll(a.lo & m5) + __popcll(a.hi & m5)) +
+         64 * __popcll(a.hi);
+}
+
+__device__ __forceinline__ U128 load_word(const uint64_t* words, long long i) {
+  const ulonglong2 q = __ldg(reinterpret_cast<const ulonglong2*>(words) + i);
+  return {q.x, q.y};
+}
+
+// C(n, o, s), 1 <= n <= N, 0 <= o <= lz_max + 1, 0 <= s <= total_sum
+__device__ __forceinline__ long long count_at(const FqheLongDevice& f, int n, int o, int s) {
+  return (long long)__ldg(f.table + (size_t)(n - 1) * f.stride_n + (size_t)o * f.stride_o + s);
+}
+
+// sum over the fermions of w in orbitals [lo, hi] of C(n_i, p_i, s_i), given the number and the
+// orbital sum of the fermions below lo
+__device__ __forceinline__ long long range_terms(const FqheLongDevice& f, U128 w, int lo, int hi, int n, int s) {
+  U128 bits = u_and(w, u_and(u_below(hi + 1), u_not(u_below(lo))));
+  long long acc = 0;
+  while (u_any(bits)) {
+    const int q = u_lowest(bits);
+    bits = u_clear_lowest(bits);
+    ++n;
+    s += q;
+    acc += count_at(f, n, q, s);
+  }
+  return acc;
+}
+
+template <typename TG, int K, bool IL>
+__device__ __forceinline__ void gather_row(const TG* x, const MatvecArgs& a, long long idx, TG (&v)[K]) {
+  if constexpr (IL) {
+    const TG* p = x + idx * K;
+    if constexpr (sizeof(TG) == 4 && K == 4) {
+      const float4 q = __ldg(reinterpret_cast<const float4*>(p));
+      v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+    } else if constexpr (sizeof(TG) == 4 && K == 2) {
+      const float2 q = __ldg(reinterpret_cast<const float2*>(p));
+      v[0] = q.x; v[1] = q.y;
+    } else if constexpr (sizeof(TG) == 8 && (K == 2 || K == 4)) {
+#pragma unroll
+      for (int j = 0; j < K; j += 2) {
+        const double2 q = __ldg(reinterpret_cast<const double2*>(p) + j / 2);
+        v[j] = q.x;
+        v[j + 1] = q.y;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < K; ++j) v[j] = __ldg(p + j);
+    }
+  } else {
+    const TG* p = x + idx * a.ld;
+#pragma unroll
+    for (int j = 0; j < K; ++j) v[j] = __ldg(p + j * a.vstride);
+  }
+}
+
+template <typename TG, int K, bool RANGE, bool IL>
+__global__ void __launch_bounds__(kLongThreads) long_matvec_kernel(FqheLongDevice f, MatvecArgs a) {
+  const int L = f.lz_max;
+  const U128 full = u_below(L + 1);
+  const TG* fac = static_cast<const TG*>(f.factors);
+  const TG* x = static_cast<const TG*>(a.x);
+  double* y = static_cast<double*>(a.y);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long r_end = a.out_last > 0 ? a.out_last : f.dim;
+  for (long long r = a.out_first + (long long)blockIdx.x * blockDim.x + threadIdx.x; r < r_end; r += stride) {
+    const U128 s = load_word(f.words, r);
+    TG acc[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) acc[j] = TG(0);
+    U128 rem1 = s;
+    while (u_any(rem1)) {
+      const int m1 = u_highest(rem1);
+      rem1 = u_and(rem1, u_not(u_bit(m1)));
+      U128 rem2 = rem1;
+      while (u_any(rem2)) {
+        const int m2 = u_highest(rem2);
+        rem2 = u_and(rem2, u_not(u_bit(m2)));
+        const int M = m1 + m2;
+        const U128 an = u_and(s, u_not(u_or(u_bit(m1), u_bit(m2))));
+        const U128 e = u_and(u_not(an), full);
+        U128 valid = u_and(u_and(e, u_mirror(e, M)), u_not(u_below(M / 2 + 1)));
+        if (!u_any(valid)) continue;
+        const int paa = 1 + u_popc(u_and(s, u_between(m2, m1)));
+        const long long fbase = (long long)__ldg(f.pair_offset + m1 * (m1 - 1) / 2 + m2) - (M / 2 + 1);
+        while (u_any(valid)) {
+          const int m3 = u_lowest(valid);
+          valid = u_clear_lowest(valid);
+          const int m4 = M - m3;
+          const U128 t = u_or(an, u_or(u_bit(m3), u_bit(m4)));
+          const int par = paa + u_popc(u_and(an, u_between(m4, m3)));
+          // the target's index: the row's, corrected over the orbitals [lo, hi] the move touches
+          const int lo = min(m2, m4), hi = max(m1, m3);
+          const U128 low_part = u_and(s, u_below(lo));
+          const int n0 = u_popc(low_part), s0 = u_position_sum(low_part);
+          const long long idx = r + range_terms(f, s, lo, hi, n0, s0) - range_terms(f, t, lo, hi, n0, s0);
+          if (RANGE && (idx < a.col_first || idx >= a.col_last)) continue;
+          TG fct = __ldg(fac + fbase + m3);
+          if (par & 1) fct = -fct;
+          TG v[K];
+          gather_row<TG, K, IL>(x, a, idx, v);
+#pragma unroll
+          for (int j = 0; j < K; ++j) acc[j] += fct * v[j];
+        }
+      }
+    }
+    const bool diag = (r >= a.row_first && r < a.row_last);
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      double v = (double)acc[j];
+      if (diag && a.shift != 0.0) {
+        const long long xo = IL ? r * K + j : r * a.ld + j * a.vstride;
+        const double xd = a.xdiag ? a.xdiag[xo] : (double)x[xo];
+        v += a.shift * xd;
+      }
+      double* yp = y + (IL ? r * K + j : r * a.ld_y + j * a.vstride_y);
+      *yp = a.accumulate ? (*yp + v) : v;
+    }
+  }
+}
+
+// state index -> word: fermion by fermion from the top, the orbital q of the next fermion is the
+// lowest one whose block of states (those with that fermion at q or lower) still holds the index
+__global__ void long_unrank_kernel(FqheLongDevice f, uint64_t* words) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= f.dim) return;
+  long long r = i;
+  int n = f.nbr_fermions, s = f.total_sum, upper = f.lz_max + 1;
+  U128 w = {0ull, 0ull};
+  while (n > 0) {
+    const long long total = count_at(f, n, upper, s);
+    const long long need = total - r;  // 1 .. total
+    // smallest o in [1, upper] with C(n, o, s) >= need; the fermion sits at o - 1
+    int lo = 1, hi = upper;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (count_at(f, n, mid, s) >= need)
+        hi = mid;
+      else
+        lo = mid + 1;
+    }
+    const int q = lo - 1;
+    r -= total - count_at(f, n, lo, s);
+    w = u_or(w, u_bit(q));
+    s -= q;
+    --n;
+    upper = q;
+  }
+  reinterpret_cast<ulonglong2*>(words)[i] = make_ulonglong2(w.lo, w.hi);
+}
+
+// FindStateIndex for (low, high) words: the index, or -1 for a word outside the sector
+__global__ void long_find_kernel(FqheLongDevice f, const uint64_t* words, long long n, long long* out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const U128 w = {words[2 * i], words[2 * i + 1]};
+  const U128 outside = u_and(w, u_not(u_below(f.lz_max + 1)));
+  if (u_any(outside) || u_popc(w) != f.nbr_fermions || u_position_sum(w) != f.total_sum) {
+    out[i] = -1;
+    return;
+  }
+  out[i] = f.dim - 1 - range_terms(f, w, 0, f.lz_max, 0, 0);
+}
+
+// elements (moves, the diagonal ones included) that one product generates
+__global__ void __launch_bounds__(kLongThreads) long_count_kernel(FqheLongDevice f, unsigned long long* total) {
+  const int L = f.lz_max;
+  const U128 full = u_below(L + 1);
+  unsigned long long c = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+    const U128 s = load_word(f.words, r);
+    U128 rem1 = s;
+    while (u_any(rem1)) {
+      const int m1 = u_highest(rem1);
+      rem1 = u_and(rem1, u_not(u_bit(m1)));
+      U128 rem2 = rem1;
+      while (u_any(rem2)) {
+        const int m2 = u_highest(rem2);
+        rem2 = u_and(rem2, u_not(u_bit(m2)));
+        const int M = m1 + m2;
+        const U128 an = u_and(s, u_not(u_or(u_bit(m1), u_bit(m2))));
+        const U128 e = u_and(u_not(an), full);
+        c += u_popc(u_and(u_and(e, u_mirror(e, M)), u_not(u_below(M / 2 + 1))));
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(total, c);
+}
+
+int grid_for(long long rows) {
+  int sms = 148, dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  long long blocks = (rows + kLongThreads - 1) / kLongThreads;
+  const long long cap = (long long)sms * 16;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  return (int)blocks;
+}
+
+template <typename TG, int K>
+int launch_typed(const FqheLongDevice& f, const MatvecArgs& a, cudaStream_t s) {
+  const bool range = a.col_first > 0 || a.col_last < f.dim;
+  const bool il = (K > 1) && a.ld == K && a.vstride == 1;
+  auto kernel = range ? (il ? long_matvec_kernel<TG, K, true, true> : long_matvec_kernel<TG, K, true, false>)
+                      : (il ? long_matvec_kernel<TG, K, false, true> : long_matvec_kernel<TG, K, false, false>);
+  const long long rows = (a.out_last > 0 ? a.out_last : f.dim) - a.out_first;
+  kernel<<<grid_for(rows), kLongThreads, 0, s>>>(f, a);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+template <typename TG>
+int launch_k(const FqheLongDevice& f, const MatvecArgs& a, cudaStream_t s) {
+  // blocks of K vectors per pass; any vector count in passes of 4, 2 and 1
+  MatvecArgs b = a;
+  int done = 0;
+  while (done < a.nbr_vectors) {
+    const int left = a.nbr_vectors - done;
+    const int k = left >= 4 ? 4 : (left >= 2 ? 2 : 1);
+    b.x = static_cast<const TG*>(a.x) + (long long)done * a.vstride;
+    b.xdiag = a.xdiag ? a.xdiag + (long long)done * a.vstride : nullptr;
+    b.y = static_cast<double*>(a.y) + (long long)done * a.vstride_y;
+    b.nbr_vectors = k;
+    int rc = (k == 4) ? launch_typed<TG, 4>(f, b, s) : (k == 2) ? launch_typed<TG, 2>(f, b, s) : launch_typed<TG, 1>(f, b, s);
+    if (rc != DH_OK) return rc;
+    done += k;
+  }
+  return DH_OK;
+}
+
+}  // namespace
+
+int launch_long_unrank(const FqheLongDevice& f, uint64_t* words, cudaStream_t s) {
+  if (f.dim == 0) return DH_OK;
+  long_unrank_kernel<<<(unsigned)((f.dim + 255) / 256), 256, 0, s>>>(f, words);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_long_find(const FqheLongDevice& f, const uint64_t* words, long long n, long long* out, cudaStream_t s) {
+  if (n == 0) return DH_OK;
+  long_find_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(f, words, n, out);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_long_count(const FqheLongDevice& f, unsigned long long* total, cudaStream_t s) {
+  DH_CUDA(cudaMemsetAsync(total, 0, sizeof(unsigned long long), s));
+  if (f.dim == 0) return DH_OK;
+  long_count_kernel<<<grid_for(f.dim), kLongThreads, 0, s>>>(f, total);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_long_matvec(const FqheLongDevice& f, const MatvecArgs& a, int precision, cudaStream_t s) {
+  DH_CHECK(f.lz_max >= 1 && f.lz_max <= 126, DH_ERR_ARGUMENT, "bad FermionOnSphereLong space");
+  if (f.dim == 0) return DH_OK;
+  return precision == DH_PRECISION_FP32 ? launch_k<float>(f, a, s) : launch_k<double>(f, a, s);
+}
+
+}  // namespace dh

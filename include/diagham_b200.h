@@ -64,8 +64,23 @@ int dh_device_count(int* count);
  * FQHE/src/HilbertSpace/FermionOnSphere.cc:75-130.  total_lz is twice the total Lz, lz_max is 2S.
  * memory sizes DiagHam's lookup table (FermionOnSphere.cc:1659); it only matters for the
  * DH_INDEX_LOOKUP search mode, which stages a table of at most DH_LOOKUP_SMEM_BYTES in shared
- * memory.  Rejects lz_max > 40 and sectors of odd (total_lz + nbr_fermions * lz_max). */
+ * memory.  lz_max <= 40 uses the split-word rank tables (every index mode, stored elements, the
+ * adjoint, batched sectors, orbital cuts); 41 <= lz_max <= 62 (the reference's FermionOnSphere range,
+ * ParticleOnSphereManager.cc:282) uses the engine of dh_fermion_on_sphere_long_create, with 64-bit
+ * words at this interface and the products, counts, L^2 and Lanczos only.  Rejects lz_max > 62 and
+ * sectors of odd (total_lz + nbr_fermions * lz_max). */
 int dh_fermion_on_sphere_create(int nbr_fermions, int total_lz, int lz_max, unsigned long memory, dh_space_t* out);
+
+/* FermionOnSphereLong(nbrFermions, totalLz, lzMax, memory):
+ * FQHE/src/HilbertSpace/FermionOnSphereLong.cc:67-107, the space the reference selects for
+ * 63 <= lz_max <= 126 (ParticleOnSphereManager.cc:307-313): one 128-bit word per state, states in
+ * descending order (GenerateStates, .cc:911-943).  Words cross this interface as (low, high) pairs
+ * of uint64 (dh_space_get_states_long, dh_space_find_state_index_long).  The index of a word is
+ * computed from the sector's count table, one lookup per fermion; no search.  Generic Hamiltonian,
+ * L^2, products, counts and Lanczos; memory is accepted for the signature and unused.  Rejects
+ * lz_max > 126 and sectors whose count table ((N + 1)(lz_max + 2)(sum + 1) entries) exceeds 64M. */
+int dh_fermion_on_sphere_long_create(int nbr_fermions, int total_lz, int lz_max, unsigned long memory,
+                                     dh_space_t* out);
 
 /* BosonOnSphereShort(nbrBosons, totalLz, lzMax): FQHE/src/HilbertSpace/BosonOnSphereShort.cc:81-110.
  * The states are stored, ordered and found as the FermionOnSphere(N, totalLz, lzMax + N - 1) words
@@ -102,6 +117,15 @@ int dh_space_get_states(dh_space_t space, uint64_t* words, int* lz_max, int64_t 
 /* FindStateIndex for n words (FermionOnSphere.cc:1431, Spin1_2Chain.cc:1002), computed on the GPU
  * with the space's current index mode; host or device arrays. */
 int dh_space_find_state_index(dh_space_t space, const uint64_t* words, int64_t n, int64_t* indices);
+
+/* StateDescription of FermionOnSphereLong (FermionOnSphereLong.h:111, ULONGLONG words) as (low, high)
+ * uint64 pairs, words[2 i] and words[2 i + 1] for state first + i, with the highest occupied orbital
+ * (StateLzMax, .h:113) when lz_max is not NULL; a FermionOnSphere space gives (word, 0). */
+int dh_space_get_states_long(dh_space_t space, uint64_t* words, int* lz_max, int64_t first, int64_t n);
+
+/* FermionOnSphereLong::FindStateIndex (FermionOnSphereLong.cc:790, lookup table + bisection in the
+ * reference) for n (low, high) word pairs; -1 for a word outside the sector.  Host or device arrays. */
+int dh_space_find_state_index_long(dh_space_t space, const uint64_t* words, int64_t n, int64_t* indices);
 
 /* Selects DH_INDEX_RANK or DH_INDEX_LOOKUP for every kernel that uses this space. */
 int dh_space_set_index_mode(dh_space_t space, int mode);

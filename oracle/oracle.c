@@ -270,17 +270,84 @@ static inline dd dd_sqrt(dd a)
   return two_sum(x, corr);
 }
 
-#define ORC_MAX_FACT 180
-static dd fact_table[ORC_MAX_FACT + 1];
+/* a double-double mantissa with a binary exponent (value = m 2^e, |m.hi| in [0.5, 1)), so that
+ * factorials up to ORC_MAX_FACT and products of six of them stay representable; scaling by powers
+ * of two is exact, so the digits are those of plain double-double arithmetic */
+typedef struct
+{
+  dd m;
+  int e;
+} xd;
+
+static inline xd xd_norm(dd m, int e)
+{
+  xd r;
+  if (m.hi == 0.0)
+    {
+      r.m = dd_from(0.0);
+      r.e = 0;
+      return r;
+    }
+  int k;
+  frexp(m.hi, &k);
+  r.m.hi = ldexp(m.hi, -k);
+  r.m.lo = ldexp(m.lo, -k);
+  r.e = e + k;
+  return r;
+}
+static inline xd xd_from(double a)
+{
+  return xd_norm(dd_from(a), 0);
+}
+static inline xd xd_mul(xd a, xd b)
+{
+  return xd_norm(dd_mul(a.m, b.m), a.e + b.e);
+}
+static inline xd xd_div(xd a, xd b)
+{
+  return xd_norm(dd_div(a.m, b.m), a.e - b.e);
+}
+static inline xd xd_add(xd a, xd b)
+{
+  if (a.m.hi == 0.0)
+    return b;
+  if (b.m.hi == 0.0)
+    return a;
+  if (a.e < b.e)
+    {
+      xd t = a;
+      a = b;
+      b = t;
+    }
+  int d = a.e - b.e;
+  if (d > 240)
+    return a;
+  dd bs = {ldexp(b.m.hi, -d), ldexp(b.m.lo, -d)};
+  return xd_norm(dd_add(a.m, bs), a.e);
+}
+static inline xd xd_sqrt(xd a)
+{
+  if (a.m.hi <= 0.0)
+    return xd_from(0.0);
+  if (a.e & 1)
+    {
+      a.m = dd_mul(a.m, dd_from(2.0));
+      a.e -= 1;
+    }
+  return xd_norm(dd_sqrt(a.m), a.e / 2);
+}
+
+#define ORC_MAX_FACT 600
+static xd fact_table[ORC_MAX_FACT + 1];
 static int fact_ready = 0;
 
 static void init_factorials(void)
 {
   if (fact_ready)
     return;
-  fact_table[0] = dd_from(1.0);
+  fact_table[0] = xd_from(1.0);
   for (int n = 1; n <= ORC_MAX_FACT; ++n)
-    fact_table[n] = dd_mul(fact_table[n - 1], dd_from((double) n));
+    fact_table[n] = xd_mul(fact_table[n - 1], xd_from((double) n));
   fact_ready = 1;
 }
 
@@ -298,11 +365,13 @@ double orc_clebsch_gordan(int j1, int m1, int j2, int m2, int j)
   int a = (j1 + j2 - j) / 2, b = (j1 - j2 + j) / 2, c = (-j1 + j2 + j) / 2, d = (j1 + j2 + j) / 2 + 1;
   int jm1 = (j1 - m1) / 2, jp1 = (j1 + m1) / 2, jm2 = (j2 - m2) / 2, jp2 = (j2 + m2) / 2;
   int Jm = (j - m) / 2, Jp = (j + m) / 2;
-  dd pre = dd_mul(dd_from((double) (j + 1)), dd_mul(fact_table[a], dd_mul(fact_table[b], fact_table[c])));
-  pre = dd_div(pre, fact_table[d]);
-  dd pre2 = dd_mul(dd_mul(fact_table[Jp], fact_table[Jm]),
-                   dd_mul(dd_mul(fact_table[jm1], fact_table[jp1]), dd_mul(fact_table[jm2], fact_table[jp2])));
-  dd sum = dd_from(0.0);
+  if (d > ORC_MAX_FACT)
+    return NAN;
+  xd pre = xd_mul(xd_from((double) (j + 1)), xd_mul(fact_table[a], xd_mul(fact_table[b], fact_table[c])));
+  pre = xd_div(pre, fact_table[d]);
+  xd pre2 = xd_mul(xd_mul(fact_table[Jp], fact_table[Jm]),
+                   xd_mul(xd_mul(fact_table[jm1], fact_table[jp1]), xd_mul(fact_table[jm2], fact_table[jp2])));
+  xd sum = xd_from(0.0);
   /* k runs over all values keeping every factorial argument non-negative */
   int e1 = (j - j2 + m1) / 2; /* J - j2 + m1 */
   int e2 = (j - j1 - m2) / 2; /* J - j1 - m2 */
@@ -316,16 +385,32 @@ double orc_clebsch_gordan(int j1, int m1, int j2, int m2, int j)
     kmax = jm1;
   if (jp2 < kmax)
     kmax = jp2;
-  for (int k = kmin; k <= kmax; ++k)
+  /* the first term with its exponent, then every term relative to it through the ratio of
+   * consecutive terms, -(a-k)(jm1-k)(jp2-k) / ((k+1)(e1+k+1)(e2+k+1)), integers below 2^53 */
+  xd den0 = xd_mul(xd_mul(fact_table[kmin], fact_table[a - kmin]),
+                   xd_mul(xd_mul(fact_table[jm1 - kmin], fact_table[jp2 - kmin]),
+                          xd_mul(fact_table[e1 + kmin], fact_table[e2 + kmin])));
+  xd first = xd_div(xd_from((kmin & 1) ? -1.0 : 1.0), den0);
+  dd term = dd_from(1.0), rel = dd_from(1.0);
+  int scale = 0; /* rel and term are held times 2^-scale */
+  for (int k = kmin; k < kmax; ++k)
     {
-      dd den = dd_mul(dd_mul(fact_table[k], fact_table[a - k]),
-                      dd_mul(dd_mul(fact_table[jm1 - k], fact_table[jp2 - k]),
-                             dd_mul(fact_table[e1 + k], fact_table[e2 + k])));
-      dd term = dd_div(dd_from(1.0), den);
-      sum = (k & 1) ? dd_add(sum, dd_neg(term)) : dd_add(sum, term);
+      double num = (double) (a - k) * (double) (jm1 - k) * (double) (jp2 - k);
+      double dnm = (double) (k + 1) * (double) (e1 + k + 1) * (double) (e2 + k + 1);
+      term = dd_div(dd_mul(term, dd_from(-num)), dd_from(dnm));
+      rel = dd_add(rel, term);
+      if (fabs(term.hi) > 0x1p400)
+        {
+          term.hi = ldexp(term.hi, -400);
+          term.lo = ldexp(term.lo, -400);
+          rel.hi = ldexp(rel.hi, -400);
+          rel.lo = ldexp(rel.lo, -400);
+          scale += 400;
+        }
     }
-  dd r = dd_mul(dd_sqrt(dd_mul(pre, pre2)), sum);
-  return r.hi + r.lo;
+  sum = xd_mul(first, xd_norm(rel, scale));
+  xd r = xd_mul(xd_sqrt(xd_mul(pre, pre2)), sum);
+  return ldexp(r.m.hi, r.e) + ldexp(r.m.lo, r.e);
 }
 
 /* ===================================================================== */
@@ -345,6 +430,17 @@ static int interaction_core(int lz_max, const double* v, int* m1v, int* m2v, int
   int nlz = lz_max + 1;
   int sign = (lz_max & 1) ? 0 : 1; /* keeps odd relative angular momentum only (fermions) */
   int pair = 0, nf = 0;
+  /* <S m_a; S m_b | J/2 (m_a + m_b)/2> of the pairs, evaluated once each: cache[(a nlz + b) nlz + J/2]
+   * with NaN for "not yet" */
+  size_t ncache = (size_t) nlz * nlz * nlz;
+  double* cache = (double*) malloc(sizeof(double) * ncache);
+  for (size_t i = 0; i < ncache; ++i)
+    cache[i] = NAN;
+#define PAIR_CG(ia, ib, J)                                                                             \
+  (isnan(cache[((size_t) (ia) * nlz + (ib)) * nlz + (J) / 2])                                          \
+       ? (cache[((size_t) (ia) * nlz + (ib)) * nlz + (J) / 2] =                                        \
+              orc_clebsch_gordan(lz_max, 2 * (ia) - lz_max, lz_max, 2 * (ib) - lz_max, (J)))          \
+       : cache[((size_t) (ia) * nlz + (ib)) * nlz + (J) / 2])
   for (int m1 = 0; m1 < nlz; ++m1)
     for (int m2 = 0; m2 < m1; ++m2)
       {
@@ -363,7 +459,6 @@ static int interaction_core(int lz_max, const double* v, int* m1v, int* m2v, int
             if (2 * m3 <= m1 + m2)
               continue;
             int m4 = m1 + m2 - m3;
-            int d3 = 2 * m3 - lz_max, d4 = 2 * m4 - lz_max;
             if (m3v)
               m3v[nf] = m3;
             int jmin = abs(d1 + d2);
@@ -372,8 +467,8 @@ static int interaction_core(int lz_max, const double* v, int* m1v, int* m2v, int
               {
                 if (((J >> 1) & 1) != sign)
                   continue;
-                double c12 = orc_clebsch_gordan(lz_max, d1, lz_max, d2, J);
-                double c34 = orc_clebsch_gordan(lz_max, d3, lz_max, d4, J);
+                double c12 = PAIR_CG(m1, m2, J);
+                double c34 = PAIR_CG(m3, m4, J);
                 int mrel = lz_max - (J >> 1);
                 if (v)
                   acc += v[mrel] * c12 * c34;
@@ -389,6 +484,8 @@ static int interaction_core(int lz_max, const double* v, int* m1v, int* m2v, int
           nbr_m3[pair] = cnt;
         ++pair;
       }
+#undef PAIR_CG
+  free(cache);
   return nf;
 }
 

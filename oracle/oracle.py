@@ -552,3 +552,95 @@ def translation_flip_count(L, sz, k):
                 if ((w >> a) & 1) != ((w >> b) & 1):
                     kept += _translation_canonical(w ^ ((1 << a) | (1 << b)), L)[0] in index
     return kept
+
+
+# ------------------------------------------------------------------ FermionOnSphereLong (128-bit words)
+# Python integers stand for ULONGLONG words; small sectors only.
+
+def fermion_basis_long(n, two_s, total_lz):
+    """FermionOnSphereLong::GenerateStates (FermionOnSphereLong.cc:911-943) restated: every word of n
+    fermions in orbitals 0..two_s with orbital sum (total_lz + n two_s) / 2, highest fermion placed as
+    high as possible first (descending words)."""
+    total = total_lz + n * two_s
+    if total < 0 or total & 1:
+        raise ValueError("sector not reachable")
+    out = []
+
+    def rec(k, top, s, prefix):
+        if k == 0:
+            if s == 0:
+                out.append(prefix)
+            return
+        for q in range(top, k - 2, -1):
+            rest = s - q
+            if rest < (k - 1) * (k - 2) // 2:
+                continue
+            if rest > (k - 1) * (q - 1) - (k - 1) * (k - 2) // 2:
+                break
+            rec(k - 1, q - 1, rest, prefix | (1 << q))
+
+    rec(n, two_s, total // 2, 0)
+    return out
+
+
+def _parity(x):
+    return -1.0 if bin(x).count("1") & 1 else 1.0
+
+
+def fermion_aa_long(state, n1, n2):
+    """FermionOnSphereLong::AA (FermionOnSphereLong.cc:553): annihilate n2 then n1, each sign the parity
+    of the occupied orbitals at and above the annihilated one; (coefficient, word)."""
+    if n1 == n2 or not (state >> n1) & 1 or not (state >> n2) & 1:
+        return 0.0, 0
+    c = _parity(state >> n2)
+    state &= ~(1 << n2)
+    c *= _parity(state >> n1)
+    return c, state & ~(1 << n1)
+
+
+def fermion_adad_long(state, m1, m2):
+    """FermionOnSphereLong::AdAd (FermionOnSphereLong.cc:647): create m2 then m1, each sign the parity
+    of the occupied orbitals above the created one; (coefficient, word)."""
+    if (state >> m2) & 1:
+        return 0.0, 0
+    c = _parity(state >> m2)
+    state |= 1 << m2
+    if (state >> m1) & 1:
+        return 0.0, 0
+    c *= _parity(state >> m1)
+    return c, state | (1 << m1)
+
+
+class FQHELong:
+    """ParticleOnSphereGenericHamiltonian on FermionOnSphereLong, push form of
+    AbstractQHEOnSphereHamiltonian::LowLevelAddMultiply (AbstractQHEOnSphereHamiltonian.cc:456-488), with
+    the interaction tables of interaction_tables(); FindStateIndex by a dictionary."""
+
+    def __init__(self, n, two_s, total_lz, v, shift=0.0):
+        self.words = fermion_basis_long(n, two_s, total_lz)
+        self.index = {w: i for i, w in enumerate(self.words)}
+        self.dim = len(self.words)
+        self.shift = shift
+        t = interaction_tables(two_s, v)
+        self.moves = []
+        for p in range(len(t["m1"])):
+            m1, m2 = int(t["m1"][p]), int(t["m2"][p])
+            o, k = int(t["m3_offset"][p]), int(t["nbr_m3"][p])
+            self.moves.append((m1, m2, [(int(t["m3"][o + q]), float(t["factors"][o + q])) for q in range(k)]))
+
+    def push(self, x, first=0, nbr=None):
+        nbr = self.dim - first if nbr is None else nbr
+        y = np.zeros(self.dim)
+        for i in range(first, first + nbr):
+            s = self.words[i]
+            for m1, m2, creations in self.moves:
+                c, a = fermion_aa_long(s, m1, m2)
+                if c == 0.0:
+                    continue
+                c *= x[i]
+                for m3, f in creations:
+                    c2, t = fermion_adad_long(a, m3, m1 + m2 - m3)
+                    if c2 != 0.0:
+                        y[self.index[t]] += c * f * c2
+            y[i] += self.shift * x[i]
+        return y

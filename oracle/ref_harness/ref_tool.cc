@@ -27,6 +27,7 @@
 
 #include "config.h"
 #include "HilbertSpace/FermionOnSphere.h"
+#include "HilbertSpace/FermionOnSphereLong.h"
 #include "HilbertSpace/BosonOnSphereShort.h"
 #include "HilbertSpace/Spin1_2Chain.h"
 #include "HilbertSpace/Spin1_2ChainWithTranslations.h"
@@ -127,6 +128,18 @@ class ExposedFermionOnSphere : public FermionOnSphere
   int Find(unsigned long w, int lzmax) { return this->FindStateIndex(w, lzmax); }
 };
 
+class ExposedFermionOnSphereLong : public FermionOnSphereLong
+{
+ public:
+  ExposedFermionOnSphereLong(int nbrFermions, int totalLz, int lzMax, unsigned long memory)
+    : FermionOnSphereLong(nbrFermions, totalLz, lzMax, memory)
+  {
+  }
+  // the 128-bit word as its low and high 64-bit halves
+  unsigned long WordLow(long i) { return (unsigned long) this->StateDescription[i]; }
+  unsigned long WordHigh(long i) { return (unsigned long) (this->StateDescription[i] >> 64); }
+};
+
 class ExposedSpin1_2Chain : public Spin1_2Chain
 {
  public:
@@ -153,6 +166,7 @@ class ExposedGenericHamiltonian : public ParticleOnSphereGenericHamiltonian
   int M3(int i, int j) { return this->M3Values[i][j]; }
   int NbrFactors() { return this->NbrInteractionFactors; }
   double Factor(int i) { return this->InteractionFactors[i]; }
+  void SetFactor(int i, double x) { this->InteractionFactors[i] = x; }
 };
 
 // J1-J2 periodic chain on a plain Spin1_2Chain (see file header)
@@ -446,6 +460,11 @@ static void Usage()
 	  "  fqhe_expect N 2S 2Lz vfile psifile out\n"
 	  "  fqhe_entanglement N 2S 2Lz xfile l NA 2LzA out\n"
 	  "  fqhe_density N 2S 2Lz xfile l NA 2LzA out\n"
+	  "  lfqhe_basis N 2S 2Lz out\n"
+	  "  lfqhe_factors N 2S vfile out\n"
+	  "  lfqhe_matvec_f N 2S 2Lz vfile ffile xfile shift out\n"
+	  "  lfqhe_matvec N 2S 2Lz vfile xfile shift out\n"
+	  "  lfqhe_lanczos N 2S 2Lz vfile algo nev block maxiter precision out gsout x0 [x1 ...]\n"
 	  "  bqhe_basis N 2S 2Lz out\n"
 	  "  bqhe_matvec N 2S 2Lz vfile xfile shift out\n"
 	  "  bqhe_lanczos N 2S 2Lz vfile algo nev block maxiter precision out gsout x0 [x1 ...]\n"
@@ -496,13 +515,18 @@ int main(int argc, char** argv)
       fclose(f);
       return 0;
     }
-  if (strcmp(Cmd, "fqhe_factors") == 0 && argc == 6)
+  // lfqhe_factors: the same tables built on a FermionOnSphereLong space (lzMax up to 126)
+  if ((strcmp(Cmd, "fqhe_factors") == 0 || strcmp(Cmd, "lfqhe_factors") == 0) && argc == 6)
     {
       int N = atoi(argv[2]), LzMax = atoi(argv[3]);
       double* V = ReadDoubles(argv[4], LzMax + 1);
-      FermionOnSphere Space(N, (N & 1) ? 1 : 0, LzMax, 1ul << 20);
+      ParticleOnSphere* SpacePtr;
+      if (Cmd[0] == 'l')
+	SpacePtr = new FermionOnSphereLong(N, (N & 1) ? 1 : 0, LzMax, 1ul << 20);
+      else
+	SpacePtr = new FermionOnSphere(N, (N & 1) ? 1 : 0, LzMax, 1ul << 20);
       MonoProcessorArchitecture Arch;
-      ExposedGenericHamiltonian H(&Space, N, LzMax, V, &Arch, false);
+      ExposedGenericHamiltonian H(SpacePtr, N, LzMax, V, &Arch, false);
       FILE* f = OpenOut(argv[5]);
       // layout: int32 nbrM12, then per pair int32 (m1, m2, nbrM3, m3[nbrM3]); int32 nbrFactors; doubles
       int P = H.GetNbrM12();
@@ -577,6 +601,76 @@ int main(int argc, char** argv)
 	    fwrite(&Out[0], sizeof(int), Out.size(), f);
 	}
       fclose(f);
+      return 0;
+    }
+  // FermionOnSphereLong (lzMax up to 126): basis as int64 dimension then (low, high) uint64 per state
+  if (strcmp(Cmd, "lfqhe_basis") == 0 && argc == 6)
+    {
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      ExposedFermionOnSphereLong Space(N, TotalLz, LzMax, 1ul << 20);
+      long Dim = Space.GetHilbertSpaceDimension();
+      FILE* f = OpenOut(argv[5]);
+      fwrite(&Dim, sizeof(long), 1, f);
+      for (long i = 0; i < Dim; ++i)
+	{
+	  unsigned long w[2] = {Space.WordLow(i), Space.WordHigh(i)};
+	  fwrite(w, sizeof(unsigned long), 2, f);
+	}
+      fclose(f);
+      return 0;
+    }
+  if (strcmp(Cmd, "lfqhe_matvec") == 0 && argc == 9)
+    {
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      double* V = ReadDoubles(argv[5], LzMax + 1);
+      FermionOnSphereLong Space(N, TotalLz, LzMax, 1ul << 20);
+      MonoProcessorArchitecture Arch;
+      ParticleOnSphereGenericHamiltonian H(&Space, N, LzMax, V, 0.0, &Arch, 0, false, 0, false);
+      H.ShiftHamiltonian(atof(argv[7]));
+      RealVector X;
+      X.ReadVector(argv[6]);
+      RealVector Y(Space.GetHilbertSpaceDimension(), true);
+      H.LowLevelMultiply(X, Y);
+      Y.WriteVector(argv[8]);
+      return 0;
+    }
+  // the reference's FermionOnSphereLong product with its interaction factors replaced by the ones in
+  // ffile (NbrFactors doubles, in the order lfqhe_factors writes them)
+  if (strcmp(Cmd, "lfqhe_matvec_f") == 0 && argc == 10)
+    {
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      double* V = ReadDoubles(argv[5], LzMax + 1);
+      FermionOnSphereLong Space(N, TotalLz, LzMax, 1ul << 20);
+      MonoProcessorArchitecture Arch;
+      ExposedGenericHamiltonian H(&Space, N, LzMax, V, &Arch, false);
+      double* F = ReadDoubles(argv[6], H.NbrFactors());
+      for (int i = 0; i < H.NbrFactors(); ++i)
+	H.SetFactor(i, F[i]);
+      H.ShiftHamiltonian(atof(argv[8]));
+      RealVector X;
+      X.ReadVector(argv[7]);
+      RealVector Y(Space.GetHilbertSpaceDimension(), true);
+      H.LowLevelMultiply(X, Y);
+      Y.WriteVector(argv[9]);
+      return 0;
+    }
+  if (strcmp(Cmd, "lfqhe_lanczos") == 0 && argc >= 14)
+    {
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      double* V = ReadDoubles(argv[5], LzMax + 1);
+      const char* Algo = argv[6];
+      int Nev = atoi(argv[7]), Block = atoi(argv[8]), MaxIter = atoi(argv[9]);
+      double Precision = atof(argv[10]);
+      FermionOnSphereLong Space(N, TotalLz, LzMax, 9ul << 20);
+      AbstractArchitecture* Arch = MakeArchitecture();
+      Arch->SetDimension(Space.GetHilbertSpaceDimension());
+      ParticleOnSphereGenericHamiltonian H(&Space, N, LzMax, V, 0.0, Arch, 0, false, 0, false);
+      int NbrInitial = argc - 13;
+      RealVector* Init = new RealVector[NbrInitial];
+      for (int i = 0; i < NbrInitial; ++i)
+	Init[i].ReadVector(argv[13 + i]);
+      RunLanczosLoop(&H, Arch, Algo, Nev, Block, MaxIter, Precision, Init, NbrInitial, argv[11],
+		     strcmp(argv[12], "-") == 0 ? 0 : argv[12]);
       return 0;
     }
   if (strcmp(Cmd, "fqhe_matvec") == 0 && argc == 9)

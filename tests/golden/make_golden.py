@@ -395,6 +395,115 @@ def translation_fixtures(tmp):
              words=words, y=read_vector(yf), **extra)
 
 
+LONG_CASES = [  # (space, N, 2S, 2Lz): FermionOnSphere beyond 2S = 40 and FermionOnSphereLong
+    ("fermion", 3, 62, 0), ("fermion", 4, 50, 0), ("fermion", 5, 41, 1),
+    ("long", 2, 126, -2), ("long", 3, 63, 1), ("long", 3, 126, 0), ("long", 4, 70, 0), ("long", 4, 100, 2),
+    ("long", 5, 64, 0)]
+
+
+def coulomb_closed_form(two_s):
+    """LLL Coulomb pseudopotentials on the sphere from the closed form (Fano, Ortolani and Colombo):
+    V_m = 2 / sqrt(S) C(4S - 2L, 2S - L) C(4S + 2L + 2, 2S + L + 1) / C(4S + 2, 2S + 1)^2, L = 2S - m,
+    evaluated in exact integer arithmetic and rounded once."""
+    from fractions import Fraction
+    from math import comb, sqrt
+    out = np.zeros(two_s + 1)
+    for m in range(two_s + 1):
+        L = two_s - m
+        f = Fraction(2 * comb(2 * two_s - 2 * L, two_s - L) * comb(2 * two_s + 2 * L + 2, two_s + L + 1),
+                     comb(2 * two_s + 2, two_s + 1) ** 2)
+        out[m] = float(f) / sqrt(two_s / 2)
+    return out
+
+
+def exact_factors_in_reference_order(tmp, n, s, v):
+    """The oracle's interaction factors (Clebsch-Gordan coefficients exact to the last bit) laid out in
+    the reference's own (pair, m3) order, read from its lfqhe_factors table."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    vf = os.path.join(tmp, "vf.bin")
+    v.tofile(vf)
+    ff = os.path.join(tmp, "ff.bin")
+    run("lfqhe_factors", n, s, vf, ff)
+    r = read_factors(ff)
+    t = oracle.interaction_tables(s, v)
+    ours = {}
+    for p in range(len(t["m1"])):
+        o = int(t["m3_offset"][p])
+        for q in range(int(t["nbr_m3"][p])):
+            ours[(int(t["m1"][p]), int(t["m2"][p]), int(t["m3"][o + q]))] = float(t["factors"][o + q])
+    out, off = [], 0
+    for p in range(len(r["m1"])):
+        for q in range(int(r["nbr_m3"][p])):
+            out.append(ours[(int(r["m1"][p]), int(r["m2"][p]), int(r["m3"][off + q]))])
+        off += int(r["nbr_m3"][p])
+    return np.array(out), r["factors"]
+
+
+def long_fixtures(tmp):
+    # the words ((low, high) uint64 pairs), y = H x at shifts 0 and 0.37 for x = the splitmix64 vector of
+    # seed 0, and the basic Lanczos run from it (sectors up to 13,000 states), with V = the closed-form
+    # Coulomb pseudopotentials (odd m; both sides take the same file, so the products do not depend on
+    # either code's pseudopotential routine).  The reference's own interaction factors drift from the
+    # exact ones as 2S grows (3.6e-13 at 2S = 62, 1.4e-12 at 70, 33% at 100, 87% at 126: its
+    # Clebsch-Gordan evaluation), so for FermionOnSphereLong y is the reference's product with the exact
+    # factors put in its tables (lfqhe_matvec_f), and its product with its own factors is kept beside it
+    # (y_own_factors_*) with the factors' largest deviation; its Lanczos is recorded only up to 2S = 84.
+    # Also the reference's own EvaluatePseudopotentials at large 2S next to the closed form.
+    for (space, n, s, lz) in LONG_CASES:
+        prefix = "fqhe" if space == "fermion" else "lfqhe"
+        v = coulomb_closed_form(s)
+        v[0::2] = 0.0
+        vf = os.path.join(tmp, "vl.bin")
+        v.tofile(vf)
+        bf = os.path.join(tmp, "bl.bin")
+        cmd = run(prefix + "_basis", n, s, lz, bf)
+        if space == "fermion":
+            dim, w, _ = read_basis(bf)
+            words = np.stack([w, np.zeros_like(w)], axis=1)
+        else:
+            b = open(bf, "rb").read()
+            dim = int(np.frombuffer(b[:8], np.int64)[0])
+            words = np.frombuffer(b[8:8 + 16 * dim], np.uint64).reshape(dim, 2).copy()
+        xf = os.path.join(tmp, "xl.vec")
+        write_vector(xf, splitmix_vector(0, dim))
+        ys = {}
+        if space == "long":
+            exact, own = exact_factors_in_reference_order(tmp, n, s, v)
+            ff = os.path.join(tmp, "fe.bin")
+            exact.tofile(ff)
+            ys["own_factor_deviation"] = np.max(np.abs(exact - own)) / np.max(np.abs(exact))
+        for shift in (0.0, 0.37):
+            yf = os.path.join(tmp, "yl.vec")
+            cmd2 = run(prefix + "_matvec", n, s, lz, vf, xf, shift, yf)
+            if space == "long":
+                ys["y_own_factors_shift%g" % shift] = read_vector(yf)
+                cmd2 = run("lfqhe_matvec_f", n, s, lz, vf, ff, xf, shift, yf)
+            ys["y_shift%g" % shift] = read_vector(yf)
+        extra = {}
+        if dim <= 13000 and s <= 84:
+            lf = os.path.join(tmp, "ll.out")
+            run(prefix + "_lanczos", n, s, lz, vf, "basic", 1, 1, 300, 0, lf, "-", xf)
+            extra = read_lanczos(lf)
+        if dim > 13000:
+            # large sectors: the words as a SHA-256 of their (low, high) bytes, y at shift 0 only
+            import hashlib
+            ys = {"y_shift0": ys["y_shift0"], "own_factor_deviation": ys.get("own_factor_deviation", 0.0)}
+            save("long_%s_n%d_2s%d_lz%d.npz" % (space, n, s, lz), cmd + "; " + cmd2, v=v, seed=0, dim=dim,
+                 words_sha256=hashlib.sha256(words.tobytes()).hexdigest(), **ys, **extra)
+            continue
+        save("long_%s_n%d_2s%d_lz%d.npz" % (space, n, s, lz), cmd + "; " + cmd2, v=v, seed=0, words=words,
+             **ys, **extra)
+    sizes = np.array([84, 100, 126])
+    ref = {}
+    for s in sizes:
+        pf = os.path.join(tmp, "pl.bin")
+        run("pseudopotentials", s, pf)
+        ref["reference_%d" % s] = np.fromfile(pf, np.float64)[-(s + 1):]
+        ref["closed_form_%d" % s] = coulomb_closed_form(int(s))
+    save("pseudopotentials_large_2s.npz", "ref_tool pseudopotentials 2S", sizes=sizes, **ref)
+
+
 def dir_files(d):
     names = sorted(os.listdir(d))
     return np.array(names), {"f%d" % i: np.frombuffer(open(os.path.join(d, f), "rb").read(), np.uint8)
@@ -483,6 +592,8 @@ def main():
             entanglement_fixtures(tmp)
         if args.only in (None, "translations"):
             translation_fixtures(tmp)
+        if args.only in (None, "long"):
+            long_fixtures(tmp)
         if args.slow:
             slow_fixtures(tmp)
 

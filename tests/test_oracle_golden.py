@@ -294,3 +294,88 @@ def test_translation_oracle_matches_reference(orc, name):
     x = orc.random_vector(int(z["seed"]), len(reps))
     y = orc.translation_j1j2_push(L, sz, k, float(z["j1"]), float(z["j2"]), x)
     assert np.max(np.abs(y - z["y"])) <= 1e-13 * np.max(np.abs(z["y"]))
+
+
+LONG_FIXTURES = sorted(os.path.basename(f) for f in glob.glob(os.path.join(GOLDEN, "long_*.npz")))
+
+
+def long_sector(name):
+    import re
+    space, n, s, lz = re.match(r"long_(\w+?)_n(\d+)_2s(\d+)_lz(-?\d+)", name).groups()
+    return space, int(n), int(s), int(lz)
+
+
+@pytest.mark.parametrize("name", [n for n in LONG_FIXTURES if "words" in golden(n).files])
+def test_long_oracle_matches_reference(orc, name):
+    # FermionOnSphere beyond 2S = 40 and FermionOnSphereLong up to 2S = 126: the words bit for bit, the
+    # product at shift 0.37 within 1e-13 of max|y| (FermionOnSphereLong: the reference's product with
+    # exact factors in its tables) or within 1e-12 (FermionOnSphere with the reference's own factors,
+    # which deviate from the exact ones by up to 3.6e-13 at 2S = 62)
+    z = golden(name)
+    space, n, s, lz = long_sector(name)
+    words = orc.fermion_basis_long(n, s, lz)
+    assert words == [int(a) | (int(b) << 64) for a, b in z["words"]]
+    H = orc.FQHELong(n, s, lz, z["v"], shift=0.37)
+    y = H.push(orc.random_vector(int(z["seed"]), H.dim))
+    ref = z["y_shift0.37"]
+    tol = 1e-13 if space == "long" else 1e-12
+    assert np.max(np.abs(y - ref)) <= tol * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("name", [n for n in LONG_FIXTURES if "words_sha256" in golden(n).files])
+def test_long_oracle_basis_matches_reference_digest(orc, name):
+    import hashlib
+    z = golden(name)
+    _, n, s, lz = long_sector(name)
+    m = (1 << 64) - 1
+    words = np.array([[w & m, w >> 64] for w in orc.fermion_basis_long(n, s, lz)], np.uint64)
+    assert words.shape[0] == int(z["dim"])
+    assert hashlib.sha256(words.tobytes()).hexdigest() == str(z["words_sha256"])
+
+
+def _cg_exact(j1, m1, j2, m2, j):
+    """Racah's formula in exact rational arithmetic (doubled arguments), rounded once."""
+    from fractions import Fraction
+    from math import factorial as F
+    m = m1 + m2
+    a, b, c, d = (j1 + j2 - j) // 2, (j1 - j2 + j) // 2, (j2 - j1 + j) // 2, (j1 + j2 + j) // 2 + 1
+    jm1, jp1, jm2, jp2 = (j1 - m1) // 2, (j1 + m1) // 2, (j2 - m2) // 2, (j2 + m2) // 2
+    Jm, Jp = (j - m) // 2, (j + m) // 2
+    e1, e2 = (j - j2 + m1) // 2, (j - j1 - m2) // 2
+    pre = Fraction((j + 1) * F(a) * F(b) * F(c) * F(Jp) * F(Jm) * F(jm1) * F(jp1) * F(jm2) * F(jp2), F(d))
+    S = sum(Fraction((-1) ** k, F(k) * F(a - k) * F(jm1 - k) * F(jp2 - k) * F(e1 + k) * F(e2 + k))
+            for k in range(max(0, -e1, -e2), min(a, jm1, jp2) + 1))
+    v = pre * S * S
+    # sqrt of the rational to double precision through an integer square root
+    from math import isqrt
+    scale = 1 << 200
+    r = isqrt(v.numerator * scale * scale // v.denominator)
+    return (1 if S >= 0 else -1) * r / scale
+
+
+@pytest.mark.parametrize("two_s", [62, 100, 126])
+def test_clebsch_gordan_exact_at_large_2s(orc, dh, two_s):
+    # the pair coefficients <S m1; S m2 | J M> of the interaction factors, oracle and library, against
+    # exact rationals (the reference's own evaluation drifts here; see the fixtures above)
+    rng = np.random.default_rng(two_s)
+    for _ in range(40):
+        i1, i2 = (int(v) for v in rng.integers(0, two_s + 1, 2))
+        m1, m2 = 2 * i1 - two_s, 2 * i2 - two_s
+        J = int(rng.integers(abs(m1 + m2) // 2, two_s + 1)) * 2
+        e = _cg_exact(two_s, m1, two_s, m2, J)
+        if abs(e) < 1e-200:
+            continue
+        assert abs(orc.clebsch_gordan(two_s, m1, two_s, m2, J) - e) <= 4.5e-16 * abs(e)
+        assert abs(dh.clebsch_gordan(two_s, m1, two_s, m2, J) - e) <= 4.5e-16 * abs(e)
+
+
+def test_pseudopotentials_at_large_2s(orc, dh):
+    # closed form in exact arithmetic (fixture); the reference's EvaluatePseudopotentials is kept in the
+    # fixture beside it and agrees to 3e-14 up to 2S = 100 (5% off at 126)
+    z = golden("pseudopotentials_large_2s.npz")
+    for s in z["sizes"]:
+        ref = z["closed_form_%d" % s]
+        assert np.max(np.abs(orc.coulomb_pseudopotentials(int(s)) - ref)) <= 1e-14 * np.max(ref)
+        assert np.max(np.abs(dh.coulomb_pseudopotentials(int(s)) - ref)) <= 1e-14 * np.max(ref)
+        if s <= 100:
+            assert np.max(np.abs(z["reference_%d" % s] - ref)) <= 3e-14 * np.max(ref)
