@@ -9,7 +9,8 @@ diagham_b200/_build.py).  Class and method names follow the reference classes th
     Spin1_2Chain                        Spin/src/HilbertSpace/Spin1_2Chain.h
     ParticleOnSphereGenericHamiltonian  FQHE/src/Hamiltonian/ParticleOnSphereGenericHamiltonian.h
     SpinChainJ1J2Hamiltonian            (J1-J2 pattern of SpinChainJ1J2RealHamiltonianWithTranslations on a plain chain)
-    Spin1_2ChainWithTranslations, SpinChainJ1J2RealHamiltonianWithTranslations
+    Spin1_2ChainWithTranslations, SpinChainJ1J2RealHamiltonianWithTranslations,
+    SpinChainJ1J2HamiltonianWithTranslations
                                         Spin/src/HilbertSpace, Spin/src/Hamiltonian (momentum sectors)
     BasicLanczosAlgorithm, FullReorthogonalizedLanczosAlgorithm, BasicLanczosAlgorithmWithGroundState,
     BasicLanczosAlgorithmWithDiskStorage, BasicLanczosAlgorithmWithGroundStateDiskStorage
@@ -63,6 +64,7 @@ SIGNATURES = {
     "dh_particle_on_sphere_generic_hamiltonian_create": ([_vp, _c_int, _c_int, _vp, _c_dbl, _vp], _c_int),
     "dh_particle_on_sphere_l2_hamiltonian_create": ([_vp, _c_int, _c_int, _c_int, _c_dbl, _vp], _c_int),
     "dh_spin_chain_j1j2_hamiltonian_create": ([_vp, _c_dbl, _c_dbl, _vp], _c_int),
+    "dh_spin_chain_j1j2_complex_hamiltonian_create": ([_vp, _c_dbl, _c_dbl, _vp], _c_int),
     "dh_hamiltonian_destroy": ([_vp], _c_int),
     "dh_hamiltonian_get_dimension": ([_vp, _i64p], _c_int),
     "dh_hamiltonian_shift": ([_vp, _c_dbl], _c_int),
@@ -532,6 +534,7 @@ class SpinChainJ1J2Hamiltonian(_Hamiltonian):
 
 class _Lanczos:
     ALGORITHM = DH_LANCZOS_BASIC
+    _handle = None
 
     def __init__(self, hamiltonian, nbr_eigenvalue=1, max_iter=500, block_size=1):
         load()
@@ -745,6 +748,56 @@ def eigenstate_file_name(statistics, interaction_name, nbr_particles, lz_max, to
     """<statistics>_<interaction>_n_<N>_2s_<2S>_lz_<2Lz>.<index>.vec, the eigenstate naming of
     FQHE/docs/DataFormat/FermionOnSphere.xml:9-16 (statistics "fermions" or "bosons", total_lz = 2 Lz)."""
     return "%s_%s_n_%d_2s_%d_lz_%d.%d.vec" % (statistics, interaction_name, nbr_particles, lz_max, total_lz, index)
+
+
+class SpinChainJ1J2HamiltonianWithTranslations(_Hamiltonian):
+    """SpinChainJ1J2HamiltonianWithTranslations(chain, nbrSpin, j1, j2)
+    (SpinChainJ1J2HamiltonianWithTranslations.cc:62): the complex Hamiltonian of a momentum sector, any
+    K.  Products take and return complex vectors (numpy complex128; float64 arrays or torch CUDA
+    tensors of 2 D (Re, Im) pairs are taken as they are), with first / nbr counting complex
+    components.  dim is 2 D: the Lanczos classes run on the (Re, Im) form and give ground states in it
+    (as_complex turns them into complex arrays)."""
+
+    def __init__(self, chain, nbr_spin, j1, j2):
+        load()
+        if nbr_spin != chain.chain_length:
+            raise ValueError("nbr_spin must be the chain length")
+        self.space = chain
+        h = ctypes.c_void_p()
+        _check(_lib.dh_spin_chain_j1j2_complex_hamiltonian_create(chain._handle, float(j1), float(j2),
+                                                                  ctypes.byref(h)))
+        self._handle = h
+
+    @staticmethod
+    def as_complex(v):
+        v = v.detach().cpu().numpy() if hasattr(v, "detach") else np.asarray(v)
+        return np.ascontiguousarray(v, np.float64).view(np.complex128)
+
+    @staticmethod
+    def _real(v):
+        if isinstance(v, np.ndarray) and np.iscomplexobj(v):
+            return np.ascontiguousarray(v, np.complex128).view(np.float64)
+        return v
+
+    def LowLevelAddMultiply(self, src, dst, first=0, nbr=-1):
+        out = self._real(dst)
+        super().LowLevelAddMultiply(self._real(src), out, 2 * first, 2 * nbr if nbr >= 0 else -1)
+        return dst
+
+    def LowLevelMultiply(self, src, dst=None, first=0, nbr=-1):
+        if dst is None:
+            dst = np.zeros(self.dim // 2, np.complex128)
+        super().LowLevelMultiply(self._real(src), self._real(dst), 2 * first, 2 * nbr if nbr >= 0 else -1)
+        return dst
+
+    def LowLevelMultipleAddMultiply(self, srcs, dsts, first=0, nbr=-1):
+        s, d = self._real(srcs), self._real(dsts)
+        super().LowLevelMultipleAddMultiply(s, d, 2 * first, 2 * nbr if nbr >= 0 else -1)
+        return dsts
+
+    def MatrixElement(self, v1, v2):
+        """Re <v1|H|v2>."""
+        return super().MatrixElement(self._real(v1), self._real(v2))
 
 
 class SpinChainJ1J2RealHamiltonianWithTranslations(SpinChainJ1J2Hamiltonian):

@@ -785,6 +785,7 @@ int bl_ritz_block(BlockLanczos* b) {
 int block_lanczos_create(dh_hamiltonian_s* h, int nev, int k, int max_iter, BlockLanczos** out) {
   *out = nullptr;
   DH_CHECK(k == 1 || k == 2 || k == 4, DH_ERR_UNSUPPORTED, "block size %d not in {1, 2, 4}", k);
+  DH_CHECK(k == 1 || !h->complex_phases, DH_ERR_UNSUPPORTED, "complex vectors are multiplied one at a time");
   BlockLanczos* b = new (std::nothrow) BlockLanczos();
   DH_CHECK(b, DH_ERR_MEMORY, "out of host memory");
   b->h = h;
@@ -801,7 +802,7 @@ int block_lanczos_create(dh_hamiltonian_s* h, int nev, int k, int max_iter, Bloc
     e.stream = 0;
     rc = cuda_fail(cudaGetLastError(), "cudaStreamCreate", __FILE__, __LINE__);
   }
-  if (rc == DH_OK) rc = engine_setup(e, std::vector<long long>{(long long)h->space->dim});
+  if (rc == DH_OK) rc = engine_setup(e, std::vector<long long>{(long long)hamiltonian_dim(h)});
   if (rc == DH_OK) rc = bl_allocate_store(b);
   if (rc != DH_OK) {
     delete b;

@@ -432,7 +432,7 @@ int dh_lanczos_create(dh_hamiltonian_t h, int algorithm, int nbr_eigenvalue, int
     l->nev = nbr_eigenvalue;
     l->block = block_size;
     l->max_iter = max_iter;
-    l->dim = h->space->dim;
+    l->dim = hamiltonian_dim(h);
     int rc = block_lanczos_create(h, nbr_eigenvalue, block_size, max_iter, &l->blk);
     if (rc != DH_OK) {
       delete l;
@@ -445,7 +445,7 @@ int dh_lanczos_create(dh_hamiltonian_t h, int algorithm, int nbr_eigenvalue, int
   l->algorithm = algorithm;
   l->nev = nbr_eigenvalue;
   l->max_iter = max_iter;
-  l->dim = h->space->dim;
+  l->dim = hamiltonian_dim(h);
   l->cap = max_iter + 2;
   l->prev_wanted.assign(nbr_eigenvalue, 0.0);
   int rc;

@@ -259,9 +259,12 @@ TransDevice trans_device(const dh_space_s* sp, const dh_hamiltonian_s* h) {
   // ExponentialTable of the real Hamiltonian: cos(2 pi K m / L) (SpinChainRealHamiltonianWithTranslations.cc:204)
   const double coef = 2.0 * M_PI / (double)sp->length * (double)sp->momentum;
   for (int m = 0; m < 32; ++m) d.phase[m] = (m < sp->length) ? cos(coef * (double)m) : 0.0;
+  // ExponentialTable of the complex Hamiltonian: exp(2 pi i K m / L) (SpinChainJ1J2HamiltonianWithTranslations.cc:390-397)
+  for (int m = 0; m < 32; ++m) d.sine[m] = (m < sp->length) ? sin(coef * (double)m) : 0.0;
   if (h) {
     d.j1 = h->j1;
     d.j2 = h->j2;
+    d.complex_phases = h->complex_phases ? 1 : 0;
   }
   return d;
 }
@@ -328,7 +331,7 @@ int hamiltonian_apply_rows(dh_hamiltonian_s* h, const double* x, double* y, int 
                            int accumulate, const float* x32_ready, cudaStream_t stream, int64_t out_first,
                            int64_t out_last) {
   dh_space_s* sp = h->space;
-  const int64_t dim = sp->dim;
+  const int64_t dim = hamiltonian_dim(h);
   MatvecArgs a = {};
   a.out_first = out_first;
   a.out_last = out_last;
@@ -388,9 +391,9 @@ int hamiltonian_apply_block_rows(dh_hamiltonian_s* h, const double* x64, const f
   a.nbr_vectors = k;
   a.shift = h->shift;
   a.col_first = 0;
-  a.col_last = sp->dim;
+  a.col_last = hamiltonian_dim(h);
   a.row_first = 0;
-  a.row_last = sp->dim;
+  a.row_last = hamiltonian_dim(h);
   a.accumulate = 0;
   if (precision == DH_PRECISION_FP32) {
     DH_CHECK(x32, DH_ERR_STATE, "FP32 product without an FP32 copy of the block");
@@ -873,15 +876,17 @@ int dh_particle_on_sphere_l2_hamiltonian_create(dh_space_t sp, int nbr_particles
   return DH_OK;
 }
 
-int dh_spin_chain_j1j2_hamiltonian_create(dh_space_t sp, double j1, double j2, dh_hamiltonian_t* out) {
+static int j1j2_create(dh_space_t sp, double j1, double j2, bool complex_phases, dh_hamiltonian_t* out) {
   DH_CHECK(out, DH_ERR_ARGUMENT, "null output handle");
   *out = nullptr;
   DH_CHECK(sp && (sp->kind == SPACE_SPIN12 || sp->kind == SPACE_SPIN12_TRANSLATIONS), DH_ERR_ARGUMENT,
            "the J1-J2 chain needs a Spin1_2Chain or Spin1_2ChainWithTranslations space");
+  DH_CHECK(!complex_phases || sp->kind == SPACE_SPIN12_TRANSLATIONS, DH_ERR_ARGUMENT,
+           "the complex J1-J2 Hamiltonian needs a Spin1_2ChainWithTranslations space");
   DH_CHECK(sp->length >= 3, DH_ERR_UNSUPPORTED, "the periodic J1-J2 chain needs at least 3 sites");
   // the real Hamiltonian of a momentum sector (SpinChainJ1J2RealHamiltonianWithTranslations) is the
   // Hamiltonian only where the phases are real: K = 0 and K = L / 2
-  DH_CHECK(sp->kind != SPACE_SPIN12_TRANSLATIONS || sp->momentum == 0 || 2 * sp->momentum == sp->length,
+  DH_CHECK(complex_phases || sp->kind != SPACE_SPIN12_TRANSLATIONS || sp->momentum == 0 || 2 * sp->momentum == sp->length,
            DH_ERR_UNSUPPORTED, "momentum %d of %d sites needs complex arithmetic (K = 0 or L / 2 only)", sp->momentum,
            sp->length);
   dh_hamiltonian_s* h = new (std::nothrow) dh_hamiltonian_s();
@@ -890,6 +895,7 @@ int dh_spin_chain_j1j2_hamiltonian_create(dh_space_t sp, double j1, double j2, d
   h->kind = sp->kind;
   h->j1 = j1;
   h->j2 = j2;
+  h->complex_phases = complex_phases;
   int rc = reducer_init(h->red, h->red_storage, 16);
   if (rc != DH_OK) {
     delete h;
@@ -899,6 +905,14 @@ int dh_spin_chain_j1j2_hamiltonian_create(dh_space_t sp, double j1, double j2, d
   return DH_OK;
 }
 
+int dh_spin_chain_j1j2_hamiltonian_create(dh_space_t sp, double j1, double j2, dh_hamiltonian_t* out) {
+  return j1j2_create(sp, j1, j2, false, out);
+}
+
+int dh_spin_chain_j1j2_complex_hamiltonian_create(dh_space_t sp, double j1, double j2, dh_hamiltonian_t* out) {
+  return j1j2_create(sp, j1, j2, true, out);
+}
+
 int dh_hamiltonian_destroy(dh_hamiltonian_t h) {
   delete h;
   return DH_OK;
@@ -906,7 +920,7 @@ int dh_hamiltonian_destroy(dh_hamiltonian_t h) {
 
 int dh_hamiltonian_get_dimension(dh_hamiltonian_t h, int64_t* dim) {
   DH_CHECK(h && dim, DH_ERR_ARGUMENT, "null argument");
-  *dim = h->space->dim;
+  *dim = hamiltonian_dim(h);
   return DH_OK;
 }
 
@@ -1066,8 +1080,10 @@ static int product_to_host(dh_hamiltonian_s* h, int64_t dim, Run run, Copy copy)
 static int multiply_common(dh_hamiltonian_t h, const double* src, double* dst, int nvec, int64_t first, int64_t nbr,
                            int accumulate) {
   DH_CHECK(h && src && dst, DH_ERR_ARGUMENT, "null argument");
-  const int64_t dim = h->space->dim;
+  const int64_t dim = hamiltonian_dim(h);
   if (nbr < 0) nbr = dim - first;
+  DH_CHECK(!h->complex_phases || ((first | nbr) & 1) == 0, DH_ERR_ARGUMENT,
+           "complex components come in (Re, Im) pairs: first and nbr must be even");
   DH_CHECK(first >= 0 && first + nbr <= dim, DH_ERR_ARGUMENT, "component range [%lld, %lld) outside [0, %lld)",
            (long long)first, (long long)(first + nbr), (long long)dim);
   DH_CHECK(nvec >= 1, DH_ERR_ARGUMENT, "nbr_vectors must be >= 1");
@@ -1116,7 +1132,8 @@ static int multiply_common(dh_hamiltonian_t h, const double* src, double* dst, i
 int dh_hamiltonian_block_multiply(dh_hamiltonian_t h, const double* x, double* y, int k) {
   DH_CHECK(h && x && y, DH_ERR_ARGUMENT, "null argument");
   DH_CHECK(k >= 1, DH_ERR_ARGUMENT, "k must be >= 1");
-  const int64_t dim = h->space->dim;
+  DH_CHECK(k == 1 || !h->complex_phases, DH_ERR_UNSUPPORTED, "complex vectors are multiplied one at a time");
+  const int64_t dim = hamiltonian_dim(h);
   const size_t bytes = (size_t)dim * k * sizeof(double);
   const bool src_dev = is_device_pointer(x), dst_dev = is_device_pointer(y);
   const double* xd = x;
@@ -1160,6 +1177,7 @@ int dh_hamiltonian_autotune(dh_hamiltonian_t h, int block_size, int repeats, dou
   DH_CHECK(block_size == 1 || block_size == 2 || block_size == 4, DH_ERR_ARGUMENT, "block size %d not in {1, 2, 4}",
            block_size);
   if (repeats < 1) repeats = 3;
+  DH_CHECK(!h->complex_phases, DH_ERR_UNSUPPORTED, "the complex chain has a single product form");
   dh_space_s* sp = h->space;
   const int64_t dim = sp->dim;
   const int kmax = 4;
@@ -1272,7 +1290,7 @@ int dh_hamiltonian_low_level_multiple_add_multiply(dh_hamiltonian_t h, const dou
 
 int dh_hamiltonian_matrix_element(dh_hamiltonian_t h, const double* v1, const double* v2, double* out) {
   DH_CHECK(h && v1 && v2 && out, DH_ERR_ARGUMENT, "null argument");
-  const int64_t dim = h->space->dim;
+  const int64_t dim = hamiltonian_dim(h);
   const size_t bytes = (size_t)dim * sizeof(double);
   int rc;
   if ((rc = ensure_buffer(h->stage_y, bytes)) != DH_OK) return rc;

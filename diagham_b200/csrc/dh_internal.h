@@ -243,6 +243,8 @@ struct TransDevice {
   int length, momentum;
   double j1, j2;
   double phase[32];          // cos(2 pi K m / L)
+  double sine[32];           // sin(2 pi K m / L)
+  int complex_phases;        // SpinChainJ1J2HamiltonianWithTranslations: (Re, Im) interleaved vectors
 };
 int launch_trans_count(long long total, int L, int n_up, int momentum, unsigned int* chunk_count, cudaStream_t s);
 int launch_trans_write(long long total, int L, int n_up, int momentum, const long long* chunk_offset, uint32_t* reps,

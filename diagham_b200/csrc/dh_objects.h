@@ -56,8 +56,10 @@ struct dh_hamiltonian_s {
   dh::InteractionTables tabs;
   std::vector<double> v;
   dh::DevBuf pair_offset, factors64, factors32;
-  // J1-J2 chain
+  // J1-J2 chain; complex_phases: SpinChainJ1J2HamiltonianWithTranslations at any momentum, acting on
+  // complex vectors stored as (Re, Im) pairs, i.e. a real symmetric operator of dimension 2 D
   double j1 = 0.0, j2 = 0.0;
+  bool complex_phases = false;
   // stored elements (fast multiplication): built by dh_hamiltonian_enable_fast_multiplication
   bool fast = false;
   bool fast_use = true;  // products read the stored elements (the autotuner may prefer the on-the-fly form)
@@ -84,6 +86,11 @@ struct dh_hamiltonian_s {
 };
 
 namespace dh {
+// the length of the (real) vectors the Hamiltonian acts on: the space's dimension, twice that for
+// complex vectors stored as (Re, Im) pairs
+inline int64_t hamiltonian_dim(const dh_hamiltonian_s* h) {
+  return h->complex_phases ? 2 * h->space->dim : h->space->dim;
+}
 bool is_device_pointer(const void* p);
 int ensure_buffer(DevBuf& b, size_t bytes);
 int build_lookup(dh_space_s* sp);

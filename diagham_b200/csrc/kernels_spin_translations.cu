@@ -311,6 +311,113 @@ __global__ void __launch_bounds__(kTransThreads) trans_matvec_kernel(TransDevice
 }
 
 // elements of one product (antiparallel bonds of the representatives, and those in the sector)
+// every antiparallel bond of representative w (plain chain index r): f(plain index of the flipped
+// word, J / 2 of the bond)
+template <typename T, typename F>
+__device__ __forceinline__ void for_each_flip(const SpinTables& tb, const TransDevice& d, uint32_t w, int r, T hj1,
+                                              T hj2, F&& f) {
+  const int L = d.length;
+  const int D = (int)d.chain_dim;
+  const uint32_t maskL = (L == 32) ? 0xffffffffu : ((1u << L) - 1u);
+  const uint32_t d1 = w ^ (((w >> 1) | (w << (L - 1))) & maskL);
+  const uint32_t d2 = w ^ (((w >> 2) | (w << (L - 2))) & maskL);
+  uint32_t b = d1 & (maskL >> 1);
+  while (b) {
+    const int ja = __ffs(b) - 1;
+    b &= b - 1u;
+    const int da = tb.j1[(ja << 5) | __popc(__funnelshift_rc(w, 0u, ja + 2))];
+    f(((w >> ja) & 1u) ? r + da : r - da, hj1);
+  }
+  b = d2 & (maskL >> 2);
+  while (b) {
+    const int ja = __ffs(b) - 1;
+    b &= b - 1u;
+    const int da = tb.j2[(((w >> (ja + 1)) & 1u) << 10) | (ja << 5) | __popc(__funnelshift_rc(w, 0u, ja + 3))];
+    f(((w >> ja) & 1u) ? r + da : r - da, hj2);
+  }
+  if ((d1 >> (L - 1)) & 1u) f(spin_rank_index(tb, w ^ (1u | (1u << (L - 1))), L, D), hj1);
+  if ((d2 >> (L - 2)) & 1u) f(spin_rank_index(tb, w ^ (1u | (1u << (L - 2))), L, D), hj2);
+  if ((d2 >> (L - 1)) & 1u) f(spin_rank_index(tb, w ^ (2u | (1u << (L - 1))), L, D), hj2);
+}
+
+struct TransSharedComplex {
+  SpinTables tb;
+  double ratio[33 * 33];  // sqrt(o_s / o_t)
+  double phase[32];       // cos(2 pi K m / L)
+  double sine[32];        // sin(2 pi K m / L)
+};
+
+// SpinChainJ1J2HamiltonianWithTranslations (any K) on complex vectors stored as (Re, Im) pairs; the
+// row, column and output ranges of the arguments count doubles (twice the complex index).  The
+// reference pushes h(s -> t) = J/2 sqrt(o_s / o_t) exp(2 pi i K m / L) x[s] into y[t]
+// (SpinChainJ1J2HamiltonianWithTranslations.cc:149-247); H is Hermitian, so the pull form takes the
+// conjugate: y[s] += conj(h(s -> t)) x[t].
+template <typename TG, bool RANGE>
+__global__ void __launch_bounds__(kTransThreads) trans_matvec_complex_kernel(TransDevice d, MatvecArgs a) {
+  __shared__ TransSharedComplex sh;
+  build_spin_tables(sh.tb, d.length);
+  for (int i = threadIdx.x; i < 33 * 33; i += blockDim.x) {
+    const int os = i / 33, ot = i % 33;
+    sh.ratio[i] = (os > 0 && ot > 0) ? sqrt((double)os / (double)ot) : 0.0;
+  }
+  for (int i = threadIdx.x; i < 32; i += blockDim.x) {
+    sh.phase[i] = d.phase[i];
+    sh.sine[i] = d.sine[i];
+  }
+  __syncthreads();
+  const int L = d.length;
+  const uint32_t maskL = (L == 32) ? 0xffffffffu : ((1u << L) - 1u);
+  const TG* x = static_cast<const TG*>(a.x);
+  double* y = static_cast<double*>(a.y);
+  const long long c_first = a.col_first / 2, c_last = a.col_last / 2;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long r_end = (a.out_last > 0 ? a.out_last : 2 * d.dim) / 2;
+  for (long long s = a.out_first / 2 + (long long)blockIdx.x * blockDim.x + threadIdx.x; s < r_end; s += stride) {
+    const uint32_t w = __ldg(d.reps + s);
+    const int r = __ldg(d.rep_rank + s);
+    const int os = d.orbits[s];
+    TG re = TG(0), im = TG(0);
+    for_each_flip(sh.tb, d, w, r, (TG)(0.5 * d.j1), (TG)(0.5 * d.j2), [&](int ci, TG hj) {
+      const unsigned long long e = __ldg(d.map + ci);
+      const unsigned int t = (unsigned int)(e & 0xffffffffull);
+      if (t == 0xffffffffu) return;
+      if (RANGE && ((long long)t < c_first || (long long)t >= c_last)) return;
+      const int n = (int)((e >> 32) & 0xffull), ot = (int)((e >> 40) & 0xffull);
+      const int m = (L - n) % L;
+      const double mag = sh.ratio[os * 33 + ot];
+      const TG cr = hj * (TG)(mag * sh.phase[m]), cim = -hj * (TG)(mag * sh.sine[m]);
+      TG xr, xi;
+      if constexpr (sizeof(TG) == 8) {
+        const double2 q = __ldg(reinterpret_cast<const double2*>(x) + t);
+        xr = q.x;
+        xi = q.y;
+      } else {
+        const float2 q = __ldg(reinterpret_cast<const float2*>(x) + t);
+        xr = q.x;
+        xi = q.y;
+      }
+      re += cr * xr - cim * xi;
+      im += cr * xi + cim * xr;
+    });
+    const uint32_t d1 = w ^ (((w >> 1) | (w << (L - 1))) & maskL);
+    const uint32_t d2 = w ^ (((w >> 2) | (w << (L - 2))) & maskL);
+    double vr = (double)re, vi = (double)im;
+    if (2 * s >= a.row_first && 2 * s < a.row_last) {
+      const double diag = 0.25 * d.j1 * (double)(L - 2 * __popc(d1)) + 0.25 * d.j2 * (double)(L - 2 * __popc(d2)) +
+                          a.shift;
+      const double xr = a.xdiag ? a.xdiag[2 * s] : (double)x[2 * s];
+      const double xi = a.xdiag ? a.xdiag[2 * s + 1] : (double)x[2 * s + 1];
+      vr += diag * xr;
+      vi += diag * xi;
+    }
+    if (a.accumulate) {
+      vr += y[2 * s];
+      vi += y[2 * s + 1];
+    }
+    reinterpret_cast<double2*>(y)[s] = make_double2(vr, vi);
+  }
+}
+
 __global__ void __launch_bounds__(kTransThreads) trans_count_kernel(TransDevice d, unsigned long long* total) {
   __shared__ SpinTables tb;
   build_spin_tables(tb, d.length);
@@ -439,8 +546,36 @@ int launch_trans_map(const TransDevice& d, long long total, int n_up, cudaStream
   return DH_OK;
 }
 
+template <typename TG>
+int launch_trans_complex(const TransDevice& d, const MatvecArgs& a, cudaStream_t s) {
+  // vectors one after the other, each 2 dim doubles (or floats) of (Re, Im) pairs
+  DH_CHECK(a.nbr_vectors == 1 || a.ld == 1, DH_ERR_UNSUPPORTED, "complex vectors are multiplied one at a time");
+  DH_CHECK(((a.out_first | a.out_last | a.col_first | a.col_last | a.row_first | a.row_last) & 1) == 0,
+           DH_ERR_ARGUMENT, "complex ranges must cover whole (Re, Im) pairs");
+  const bool range = a.col_first > 0 || a.col_last < 2 * d.dim;
+  const long long rows = ((a.out_last > 0 ? a.out_last : 2 * d.dim) - a.out_first) / 2;
+  long long g = (rows + kTransThreads - 1) / kTransThreads;
+  if (g > 148 * 16) g = 148 * 16;
+  if (g < 1) g = 1;
+  for (int v = 0; v < a.nbr_vectors; ++v) {
+    MatvecArgs b = a;
+    b.x = static_cast<const TG*>(a.x) + (long long)v * a.vstride;
+    b.xdiag = a.xdiag ? a.xdiag + (long long)v * a.vstride : nullptr;
+    b.y = static_cast<double*>(a.y) + (long long)v * a.vstride_y;
+    b.nbr_vectors = 1;
+    if (range)
+      trans_matvec_complex_kernel<TG, true><<<(unsigned)g, kTransThreads, 0, s>>>(d, b);
+    else
+      trans_matvec_complex_kernel<TG, false><<<(unsigned)g, kTransThreads, 0, s>>>(d, b);
+    DH_CUDA(cudaGetLastError());
+  }
+  return DH_OK;
+}
+
 int launch_trans_matvec(const TransDevice& d, const MatvecArgs& a, int precision, cudaStream_t s) {
   if (d.dim <= 0) return DH_OK;
+  if (d.complex_phases)
+    return precision == DH_PRECISION_FP32 ? launch_trans_complex<float>(d, a, s) : launch_trans_complex<double>(d, a, s);
   return precision == DH_PRECISION_FP32 ? launch_trans_k<float>(d, a, s) : launch_trans_k<double>(d, a, s);
 }
 

@@ -185,6 +185,19 @@ int dh_particle_on_sphere_l2_hamiltonian_create(dh_space_t space, int nbr_partic
  * the real sectors K = 0 and K = L / 2 (DH_ERR_UNSUPPORTED otherwise). */
 int dh_spin_chain_j1j2_hamiltonian_create(dh_space_t space, double j1, double j2, dh_hamiltonian_t* out);
 
+/* SpinChainJ1J2HamiltonianWithTranslations(chain, nbrSpin, j1, j2)
+ * (Spin/src/Hamiltonian/SpinChainJ1J2HamiltonianWithTranslations.cc:62, product :149-247): the complex
+ * J1-J2 Hamiltonian of a momentum sector, any K, with the flip element J/2 sqrt(o_from / o_to)
+ * exp(2 pi i K m / L) (ExponentialTable, .cc:390).  Its vectors are the reference's ComplexVector
+ * storage, (Re, Im) pairs of doubles: every product, matrix-element and Lanczos entry point given this
+ * Hamiltonian takes 2 D doubles per vector (dh_hamiltonian_get_dimension returns 2 D), and component
+ * ranges count doubles and must be even.  On (Re, Im) pairs the Hermitian H is a real symmetric
+ * operator of dimension 2 D whose eigenvalues are H's, each twice, so the Lanczos entry points find
+ * H's spectrum and return complex ground states in this layout; the matrix element is Re <v1|H|v2>.
+ * One vector per product (row-interleaved blocks, block Lanczos and the autotuner answer
+ * DH_ERR_UNSUPPORTED).  Requires a Spin1_2ChainWithTranslations space. */
+int dh_spin_chain_j1j2_complex_hamiltonian_create(dh_space_t space, double j1, double j2, dh_hamiltonian_t* out);
+
 int dh_hamiltonian_destroy(dh_hamiltonian_t h);
 
 /* AbstractHamiltonian::GetHilbertSpaceDimension (src/Hamiltonian/AbstractHamiltonian.h:96). */

@@ -644,3 +644,33 @@ class FQHELong:
                         y[self.index[t]] += c * f * c2
             y[i] += self.shift * x[i]
         return y
+
+
+def translation_j1j2_push_complex(L, sz, k, j1, j2, x):
+    """SpinChainJ1J2HamiltonianWithTranslations::LowLevelAddMultiply (.cc:149-247) restated for any
+    momentum k: for every representative s and antiparallel bond, the flipped word's representative t
+    receives J/2 sqrt(o_s / o_t) exp(2 pi i k m / L) x[s], m = (L - n) mod L the translation count that
+    SymmetrizeResult returns (Spin1_2ChainWithTranslations.h:421-432); plus the SzSz diagonal.  x and the
+    result are complex."""
+    reps, orbits = translation_basis(L, sz, k)
+    index = {int(w): i for i, w in enumerate(reps)}
+    x = np.asarray(x, np.complex128)
+    y = np.zeros(len(reps), np.complex128)
+    phase = [np.exp(2j * np.pi / L * k * m) for m in range(L)]
+    for i, w in enumerate(reps):
+        w = int(w)
+        diag = 0.0
+        for dist, j in ((1, j1), (2, j2)):
+            for a in range(L):
+                b = (a + dist) % L
+                if ((w >> a) & 1) == ((w >> b) & 1):
+                    diag += 0.25 * j
+                    continue
+                diag -= 0.25 * j
+                c, n, o = _translation_canonical(w ^ ((1 << a) | (1 << b)), L)
+                t = index.get(c)
+                if t is None:
+                    continue
+                y[t] += 0.5 * j * np.sqrt(orbits[i] / orbits[t]) * phase[(L - n) % L] * x[i]
+        y[i] += diag * x[i]
+    return y

@@ -32,6 +32,8 @@
 #include "HilbertSpace/Spin1_2Chain.h"
 #include "HilbertSpace/Spin1_2ChainWithTranslations.h"
 #include "Hamiltonian/SpinChainJ1J2RealHamiltonianWithTranslations.h"
+#include "Hamiltonian/SpinChainJ1J2HamiltonianWithTranslations.h"
+#include "Vector/ComplexVector.h"
 #include "Hamiltonian/ParticleOnSphereGenericHamiltonian.h"
 #include "Hamiltonian/ParticleOnSphereL2Hamiltonian.h"
 #include "Hamiltonian/AbstractHamiltonian.h"
@@ -476,8 +478,11 @@ static void Usage()
 	  "  spint_basis L 2Sz K out\n"
 	  "  spint_matvec L 2Sz K J1 J2 xfile out\n"
 	  "  spint_lanczos L 2Sz K J1 J2 maxiter precision out x0\n"
+	  "  spintc_matvec L 2Sz K J1 J2 xfile out\n"
+	  "  spintc_dense L 2Sz K J1 J2 out\n"
 	  "  bench_fqhe N 2S 2Lz vfile threads reps hermitian [rows]\n"
 	  "  bench_bqhe N 2S 2Lz vfile threads reps hermitian [rows]\n"
+	  "  bench_lfqhe N 2S 2Lz vfile threads reps hermitian [rows]\n"
 	  "  bench_spint L 2Sz K J1 J2 threads reps [rows]\n"
 	  "  bench_spin L 2Sz J1 J2 threads reps 0\n");
   exit(1);
@@ -934,6 +939,45 @@ int main(int argc, char** argv)
       Y.WriteVector(argv[8]);
       return 0;
     }
+  // complex momentum sectors: SpinChainJ1J2HamiltonianWithTranslations on ComplexVector (any K)
+  if (strcmp(Cmd, "spintc_matvec") == 0 && argc == 9)
+    {
+      int L = atoi(argv[2]), Sz = atoi(argv[3]), K = atoi(argv[4]);
+      Spin1_2ChainWithTranslations Chain(L, K, 1, Sz, 1 << 20, 1 << 20);
+      SpinChainJ1J2HamiltonianWithTranslations H(&Chain, L, atof(argv[5]), atof(argv[6]));
+      ComplexVector X;
+      X.ReadVector(argv[7]);
+      ComplexVector Y(Chain.GetHilbertSpaceDimension(), true);
+      H.LowLevelMultiply(X, Y);
+      Y.WriteVector(argv[8]);
+      return 0;
+    }
+  // the dense matrix of that product, column by column (int64 dim, then dim x dim complex, row-major)
+  if (strcmp(Cmd, "spintc_dense") == 0 && argc == 8)
+    {
+      int L = atoi(argv[2]), Sz = atoi(argv[3]), K = atoi(argv[4]);
+      Spin1_2ChainWithTranslations Chain(L, K, 1, Sz, 1 << 20, 1 << 20);
+      SpinChainJ1J2HamiltonianWithTranslations H(&Chain, L, atof(argv[5]), atof(argv[6]));
+      long Dim = Chain.GetHilbertSpaceDimension();
+      std::vector<double> M(2 * Dim * Dim, 0.0);
+      ComplexVector X(Dim, true), Y(Dim, true);
+      for (long c = 0; c < Dim; ++c)
+	{
+	  X.ClearVector();
+	  X[c] = Complex(1.0, 0.0);
+	  H.LowLevelMultiply(X, Y);
+	  for (long r = 0; r < Dim; ++r)
+	    {
+	      M[2 * (r * Dim + c)] = Y[r].Re;
+	      M[2 * (r * Dim + c) + 1] = Y[r].Im;
+	    }
+	}
+      FILE* f = OpenOut(argv[7]);
+      fwrite(&Dim, sizeof(long), 1, f);
+      fwrite(M.data(), sizeof(double), M.size(), f);
+      fclose(f);
+      return 0;
+    }
   if (strcmp(Cmd, "spint_lanczos") == 0 && argc == 11)
     {
       int L = atoi(argv[2]), Sz = atoi(argv[3]), K = atoi(argv[4]);
@@ -963,9 +1007,10 @@ int main(int argc, char** argv)
       RunLanczosLoop(&H, Arch, Algo, Nev, Block, MaxIter, Precision, Init, NbrInitial, argv[11], 0);
       return 0;
     }
-  if ((strcmp(Cmd, "bench_fqhe") == 0 || strcmp(Cmd, "bench_bqhe") == 0) && (argc == 9 || argc == 10))
+  if ((strcmp(Cmd, "bench_fqhe") == 0 || strcmp(Cmd, "bench_bqhe") == 0 || strcmp(Cmd, "bench_lfqhe") == 0) &&
+      (argc == 9 || argc == 10))
     {
-      // bench_bqhe: the same with BosonOnSphereShort
+      // bench_bqhe: the same with BosonOnSphereShort; bench_lfqhe: with FermionOnSphereLong
       // times the reference SMP matvec: VectorHamiltonianMultiplyOperation on SMPArchitecture
       // (VectorHamiltonianMultiplyOperation.cc:241-320), on-the-fly (memory 0) as with -m 0.
       // An optional row count bounds the sample: the architecture's typical range (the rows the
@@ -980,6 +1025,8 @@ int main(int argc, char** argv)
       ParticleOnSphere* SpacePtr;
       if (strcmp(Cmd, "bench_bqhe") == 0)
 	SpacePtr = new BosonOnSphereShort(N, TotalLz, LzMax);
+      else if (strcmp(Cmd, "bench_lfqhe") == 0)
+	SpacePtr = new FermionOnSphereLong(N, TotalLz, LzMax, 9ul << 20);
       else
 	SpacePtr = new FermionOnSphere(N, TotalLz, LzMax, 9ul << 20);
       ParticleOnSphere& Space = *SpacePtr;

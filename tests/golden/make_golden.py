@@ -504,6 +504,52 @@ def long_fixtures(tmp):
     save("pseudopotentials_large_2s.npz", "ref_tool pseudopotentials 2S", sizes=sizes, **ref)
 
 
+TRANSLATION_COMPLEX_CASES = [(8, 0, 1, 1.0, 0.5), (8, 0, 3, 1.0, 0.3), (12, 0, 2, 1.0, 0.5), (12, 2, 5, 1.0, 0.4),
+                             (13, 1, 3, 1.0, 0.3), (16, 0, 3, 1.0, 0.2), (18, 0, 4, 1.0, 0.5), (20, 2, 7, 1.0, 0.3)]
+
+
+def write_complex_vector(path, z):
+    # ComplexVector::WriteVector: int32 dimension, then (Re, Im) pairs as doubles
+    with open(path, "wb") as f:
+        f.write(np.int32(len(z)).tobytes())
+        f.write(np.ascontiguousarray(np.stack([z.real, z.imag], axis=1)).tobytes())
+
+
+def read_complex_vector(path):
+    b = open(path, "rb").read()
+    d = int(np.frombuffer(b[:4], np.int32)[0])
+    a = np.frombuffer(b[4:4 + 16 * d], np.float64).reshape(d, 2)
+    return a[:, 0] + 1j * a[:, 1]
+
+
+def translation_complex_fixtures(tmp):
+    # SpinChainJ1J2HamiltonianWithTranslations (complex, any K) on Spin1_2ChainWithTranslations(L, K, 1,
+    # 2Sz): y = H x for x = (splitmix64 seed 0) + i (splitmix64 seed 1), and, for sectors up to 900
+    # states, the reference's dense matrix (assembled column by column through its own product)
+    # diagonalised by LAPACK: its four lowest eigenvalues and how far it is from Hermitian
+    for (L, sz, k, j1, j2) in TRANSLATION_COMPLEX_CASES:
+        bf = os.path.join(tmp, "tcb.bin")
+        run("spint_basis", L, sz, k, bf)
+        b = open(bf, "rb").read()
+        dim = int(np.frombuffer(b[:8], np.int64)[0])
+        words = np.frombuffer(b[8:], np.uint64).copy()
+        x = splitmix_vector(0, dim) + 1j * splitmix_vector(1, dim)
+        xf = os.path.join(tmp, "tcx.vec")
+        write_complex_vector(xf, x)
+        yf = os.path.join(tmp, "tcy.vec")
+        cmd = run("spintc_matvec", L, sz, k, j1, j2, xf, yf)
+        extra = {}
+        if dim <= 900:
+            df = os.path.join(tmp, "tcd.bin")
+            run("spintc_dense", L, sz, k, j1, j2, df)
+            m = np.fromfile(df, np.float64, offset=8).reshape(dim, dim, 2)
+            m = m[:, :, 0] + 1j * m[:, :, 1]
+            extra = dict(hermitian_error=np.max(np.abs(m - m.conj().T)),
+                         eigenvalues=np.linalg.eigvalsh(0.5 * (m + m.conj().T))[:4])
+        save("translations_complex_L%d_sz%d_k%d_j2_%g.npz" % (L, sz, k, j2), cmd, seed_re=0, seed_im=1, j1=j1,
+             j2=j2, words=words, y=read_complex_vector(yf), **extra)
+
+
 def dir_files(d):
     names = sorted(os.listdir(d))
     return np.array(names), {"f%d" % i: np.frombuffer(open(os.path.join(d, f), "rb").read(), np.uint8)
@@ -594,6 +640,8 @@ def main():
             translation_fixtures(tmp)
         if args.only in (None, "long"):
             long_fixtures(tmp)
+        if args.only in (None, "translations_complex"):
+            translation_complex_fixtures(tmp)
         if args.slow:
             slow_fixtures(tmp)
 

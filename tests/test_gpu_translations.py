@@ -22,7 +22,7 @@ from conftest import GOLDEN, golden
 
 pytestmark = pytest.mark.gpu
 
-NAMES = sorted(os.path.basename(f) for f in glob.glob(os.path.join(GOLDEN, "translations_*.npz")))
+NAMES = sorted(os.path.basename(f) for f in glob.glob(os.path.join(GOLDEN, "translations_L*.npz")))
 
 
 def _sector(name):

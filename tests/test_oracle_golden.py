@@ -276,7 +276,7 @@ def test_entanglement_oracle_matches_reference(orc):
             assert np.max(np.abs(ref @ ref.T - z["rho_" + tag])) < 1e-15, tag
 
 
-TRANSLATION_FIXTURES = sorted(os.path.basename(f) for f in glob.glob(os.path.join(GOLDEN, "translations_*.npz")))
+TRANSLATION_FIXTURES = sorted(os.path.basename(f) for f in glob.glob(os.path.join(GOLDEN, "translations_L*.npz")))
 
 
 @pytest.mark.parametrize("name", TRANSLATION_FIXTURES)
@@ -379,3 +379,25 @@ def test_pseudopotentials_at_large_2s(orc, dh):
         assert np.max(np.abs(dh.coulomb_pseudopotentials(int(s)) - ref)) <= 1e-14 * np.max(ref)
         if s <= 100:
             assert np.max(np.abs(z["reference_%d" % s] - ref)) <= 3e-14 * np.max(ref)
+
+
+COMPLEX_TRANSLATION_FIXTURES = sorted(os.path.basename(f) for f in
+                                      glob.glob(os.path.join(GOLDEN, "translations_complex_*.npz")))
+
+
+@pytest.mark.parametrize("name", COMPLEX_TRANSLATION_FIXTURES)
+def test_complex_translation_oracle_matches_reference(orc, name):
+    # SpinChainJ1J2HamiltonianWithTranslations at any K: the complex product within 1e-13 of max|y|, and
+    # the reference's own dense matrix Hermitian (sectors up to 2,700 states on the CPU)
+    import re
+    z = golden(name)
+    L, sz, k = (int(v) for v in re.search(r"L(\d+)_sz(-?\d+)_k(\d+)", name).groups())
+    if "hermitian_error" in z.files:
+        assert float(z["hermitian_error"]) < 1e-13
+    if len(z["words"]) > 3000:
+        pytest.skip("large sector: GPU test only")
+    reps, _ = orc.translation_basis(L, sz, k)
+    assert np.array_equal(reps, z["words"])
+    x = orc.random_vector(int(z["seed_re"]), len(reps)) + 1j * orc.random_vector(int(z["seed_im"]), len(reps))
+    y = orc.translation_j1j2_push_complex(L, sz, k, float(z["j1"]), float(z["j2"]), x)
+    assert np.max(np.abs(y - z["y"])) <= 1e-13 * np.max(np.abs(z["y"]))
