@@ -393,6 +393,79 @@ def spin_chain_product(dh, flush, steps=5, k=2, length=32, warmup=2):
 
 
 
+def long_product(dh, flush, steps=5, warmup=2):
+    """FermionOnSphereLong N=6, 2S=63, 2Lz=0 (dimension 671,430: the first 2S above 64-bit words), LLL
+    Coulomb V_m with the even m set to zero: FP64 single products and FP32 blocks of 4, with the
+    algorithmic bytes (16-byte word and FP64 y per row, one x gather per element)."""
+    import torch
+    n, s = 6, 63
+    v = dh.coulomb_pseudopotentials(s)
+    v[0::2] = 0.0
+    t0 = time.perf_counter()
+    sp = dh.FermionOnSphereLong(n, 0, s)
+    H = dh.ParticleOnSphereGenericHamiltonian(sp, n, s, v)
+    torch.cuda.synchronize()
+    setup = time.perf_counter() - t0
+    dim = sp.dim
+    moves = H.count_elements()
+    peak, kind = peaks()
+    out = {"workload": "FermionOnSphereLong N=%d 2S=%d 2Lz=0 (dim %d), Coulomb V_m odd m" % (n, s, dim),
+           "setup_seconds": setup, "elements_per_product": moves}
+    for prec, k in (("fp64", 1), ("fp32", 4)):
+        H.set_precision(prec)
+        x = torch.empty(dim, k, dtype=torch.float64, device="cuda")
+        x.uniform_(-1.0, 1.0)
+        y = torch.empty_like(x)
+        for _ in range(warmup):
+            flush.zero_()
+            H.block_multiply(x, y)
+        ms = []
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            H.block_multiply(x, y)
+            b.record()
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        xb = 4 if prec == "fp32" else 8
+        alg = dim * (16 + 8 * k) + moves * xb * k
+        mean_s = statistics.mean(ms) / 1000.0
+        out["%s_block_k%d" % (prec, k)] = {
+            "mean_launch_ms": mean_s * 1000.0, "hv_per_s": k / mean_s, "elements_per_s": moves * k / mean_s,
+            "algorithmic_bytes_per_launch": alg,
+            "roofline": {"bound": "hbm", "achieved": alg / mean_s / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / mean_s / 1e9 / peak, "peak_kind": kind}}
+        del x, y
+    del H, sp
+    torch.cuda.empty_cache()
+    return out
+
+
+def reference_cpu_long(rows_target_s=6.0):
+    """The reference's own SMP product on the sector of long_product (oracle/_ref/ref_tool bench_lfqhe:
+    FermionOnSphereLong + ParticleOnSphereGenericHamiltonian, all host threads) over a row sample."""
+    import tempfile
+    import diagham_b200 as dh
+    if not os.path.exists(REF_TOOL):
+        return None
+    threads = os.cpu_count() or 1
+    v = dh.coulomb_pseudopotentials(63)
+    v[0::2] = 0.0
+    with tempfile.TemporaryDirectory() as tmp:
+        vf = os.path.join(tmp, "v.bin")
+        v.tofile(vf)
+        # about 50 us of one thread per row (measured on x86 hosts)
+        rows = int(min(671430, max(2000, rows_target_s * threads / 50e-6)))
+        cmd = [REF_TOOL, "bench_lfqhe", 6, 63, 0, vf, threads, 1, 0, rows]
+        out = subprocess.run([str(c) for c in cmd], check=True, capture_output=True, text=True)
+        r = json.loads([l for l in out.stdout.splitlines() if l.startswith("{")][-1])
+    per_matvec = r["mean_s"] * r["dim"] / r["rows"]
+    return {"value": 1.0 / per_matvec, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": "first %d of %d rows per product, SMP %d threads" % (r["rows"], r["dim"], threads),
+            "seconds_per_sample": r["mean_s"]}
+
+
 def momentum_sector(dh, flush, steps=5, k=2, length=32, warmup=2):
     """Spin1_2ChainWithTranslations L = 32, Sz = 0, K = 0 with the J1-J2 Hamiltonian at J2 = J1/2
     (dimension 18,784,170): set-up time, FP32 block products of k vectors and FP64 single products
@@ -718,7 +791,7 @@ def run_b200(args, world, rank, local):
     e2e_s = reduce_max(time.perf_counter() - t0, world)
     e2e_value = world * BLOCK * e2e_steps / e2e_s
 
-    tte = tte_c = spin = grads = stored = bosons = momentum = None
+    tte = tte_c = spin = grads = stored = bosons = momentum = longs = None
     if not args.no_solve:
         stored = stored_elements(dh, H, flush, dim)
         H.autotune(block_size=BLOCK, repeats=3)
@@ -730,6 +803,7 @@ def run_b200(args, world, rank, local):
         spin = spin_chain_product(dh, flush)
         bosons = boson_product(dh, flush)
         momentum = momentum_sector(dh, flush)
+        longs = long_product(dh, flush)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -754,7 +828,8 @@ def run_b200(args, world, rank, local):
             "stored_elements": stored,
             "spin_chain_l32": spin,
             "bosons": bosons,
-            "momentum_sector_l32": momentum}
+            "momentum_sector_l32": momentum,
+            "fermions_long_2s63": longs}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
         if bosons is not None:
@@ -767,6 +842,11 @@ def run_b200(args, world, rank, local):
                 momentum["cpu_baseline"] = reference_cpu_momentum_sector()
             except (subprocess.CalledProcessError, OSError, ValueError, IndexError) as e:
                 momentum["cpu_baseline"] = {"unavailable": str(e)}
+        if longs is not None:
+            try:
+                longs["cpu_baseline"] = reference_cpu_long()
+            except (subprocess.CalledProcessError, OSError, ValueError, IndexError) as e:
+                longs["cpu_baseline"] = {"unavailable": str(e)}
     if rank == 0:
         print(json.dumps(line))
 
