@@ -466,7 +466,7 @@ def reference_cpu_long(rows_target_s=6.0):
             "seconds_per_sample": r["mean_s"]}
 
 
-def momentum_sector(dh, flush, steps=5, k=2, length=32, warmup=2):
+def momentum_sector(dh, flush, steps=5, k=2, length=32, warmup=2, solve=True):
     """Spin1_2ChainWithTranslations L = 32, Sz = 0, K = 0 with the J1-J2 Hamiltonian at J2 = J1/2
     (dimension 18,784,170): set-up time, FP32 block products of k vectors and FP64 single products
     with their algorithmic bytes (per row: word, chain index, orbit size, FP64 y and diagonal x; per
@@ -509,6 +509,10 @@ def momentum_sector(dh, flush, steps=5, k=2, length=32, warmup=2):
                          "frac": alg / mean_s / 1e9 / peak, "peak_kind": kind}}
         del x, y
     H.set_precision("fp64")
+    if not solve:
+        del H, sp
+        torch.cuda.empty_cache()
+        return out
     t0 = time.perf_counter()
     lz = dh.BasicLanczosAlgorithm(H, 1, 600)
     lz.SetEigenvaluePrecision(1e-10)
@@ -698,6 +702,18 @@ def run_b200(args, world, rank, local):
     _build.build()
     torch.cuda.set_device(local)
     stream = torch.cuda.current_stream()
+    if args.leg:
+        flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+        if args.leg == "long":
+            r = long_product(dh, flush, steps=args.steps, warmup=args.warmup)
+        elif args.leg == "momentum":
+            r = momentum_sector(dh, flush, steps=args.steps, length=args.chain_length or 32, warmup=args.warmup,
+                                solve=not args.no_solve)
+        else:
+            r = boson_product(dh, flush, steps=args.steps, warmup=args.warmup)
+        if rank == 0:
+            print(json.dumps(dict(leg=args.leg, **r)))
+        return
     if args.kernel_only and args.chain_length:
         flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
         r = spin_chain_product(dh, flush, steps=args.steps, length=args.chain_length, warmup=args.warmup)
@@ -863,6 +879,9 @@ def main():
                     help="only the timed FP32 products (the short command used for ncu captures)")
     ap.add_argument("--chain-length", type=int, default=0,
                     help="with --kernel-only: time the J1-J2 chain block product (k = 2) at this length instead")
+    ap.add_argument("--leg", default=None, choices=["long", "momentum", "bosons"],
+                    help="run one secondary measurement alone and print its JSON (FermionOnSphereLong N=6 2S=63; "
+                         "the momentum sector at --chain-length, 32 by default; BosonOnSphereShort N=12 2S=22)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
