@@ -220,22 +220,70 @@ struct TransShared {
   double phase[32];       // cos(2 pi K m / L)
 };
 
-// one element: the flipped word's plain chain index ci -> representative, coefficient, gather
-template <typename TG, int K, bool IL, bool RANGE>
-__device__ __forceinline__ void trans_element(TG (&acc)[K], const TransDevice& d, const TransShared& sh, const TG* x,
-                                              const MatvecArgs& a, int ci, int os, TG hj) {
-  const unsigned long long e = __ldg(d.map + ci);
-  const unsigned int t = (unsigned int)(e & 0xffffffffull);
-  if (t == 0xffffffffu) return;  // the flipped word's orbit is not in this momentum sector
-  if (RANGE && ((long long)t < a.col_first || (long long)t >= a.col_last)) return;
-  const int n = (int)((e >> 32) & 0xffull), ot = (int)((e >> 40) & 0xffull);
-  const int m = (d.length - n) % d.length;
-  const TG c = hj * (TG)(sh.ratio[os * 33 + ot] * sh.phase[m]);
-  TG v[K];
-  trans_gather<TG, K, IL>(x, a, t, v);
-#pragma unroll
-  for (int q = 0; q < K; ++q) acc[q] += c * v[q];
+// the antiparallel bonds of a representative, one flip at a time: the flipped word's plain chain
+// index (from the row's own index and the step tables) and J / 2 of the bond
+struct FlipCursor {
+  uint32_t w, f1, f2;
+  int r, wraps;  // wraps: bit 0 J1 (L-1, 0), bit 1 J2 (L-2, 0), bit 2 J2 (L-1, 1)
+};
+
+__device__ __forceinline__ FlipCursor flip_cursor(uint32_t w, int r, int L) {
+  const uint32_t maskL = (L == 32) ? 0xffffffffu : ((1u << L) - 1u);
+  const uint32_t d1 = w ^ (((w >> 1) | (w << (L - 1))) & maskL);
+  const uint32_t d2 = w ^ (((w >> 2) | (w << (L - 2))) & maskL);
+  FlipCursor c;
+  c.w = w;
+  c.r = r;
+  c.f1 = d1 & (maskL >> 1);
+  c.f2 = d2 & (maskL >> 2);
+  c.wraps = (int)((d1 >> (L - 1)) & 1u) | ((int)((d2 >> (L - 2)) & 1u) << 1) | ((int)((d2 >> (L - 1)) & 1u) << 2);
+  return c;
 }
+
+template <typename TG>
+__device__ __forceinline__ bool next_flip(FlipCursor& c, const SpinTables& tb, int L, int D, TG hj1, TG hj2, int& ci,
+                                          TG& hj) {
+  const uint32_t w = c.w;
+  if (c.f1) {
+    const int ja = __ffs(c.f1) - 1;
+    c.f1 &= c.f1 - 1u;
+    const int da = tb.j1[(ja << 5) | __popc(__funnelshift_rc(w, 0u, ja + 2))];
+    ci = ((w >> ja) & 1u) ? c.r + da : c.r - da;
+    hj = hj1;
+    return true;
+  }
+  if (c.f2) {
+    const int ja = __ffs(c.f2) - 1;
+    c.f2 &= c.f2 - 1u;
+    const int da = tb.j2[(((w >> (ja + 1)) & 1u) << 10) | (ja << 5) | __popc(__funnelshift_rc(w, 0u, ja + 3))];
+    ci = ((w >> ja) & 1u) ? c.r + da : c.r - da;
+    hj = hj2;
+    return true;
+  }
+  if (c.wraps & 1) {
+    c.wraps &= ~1;
+    ci = spin_rank_index(tb, w ^ (1u | (1u << (L - 1))), L, D);
+    hj = hj1;
+    return true;
+  }
+  if (c.wraps & 2) {
+    c.wraps &= ~2;
+    ci = spin_rank_index(tb, w ^ (1u | (1u << (L - 2))), L, D);
+    hj = hj2;
+    return true;
+  }
+  if (c.wraps & 4) {
+    c.wraps = 0;
+    ci = spin_rank_index(tb, w ^ (2u | (1u << (L - 1))), L, D);
+    hj = hj2;
+    return true;
+  }
+  return false;
+}
+
+// flips are taken kTransBatch at a time: their map loads are all issued before the first is used,
+// then their gathers, so several independent load chains are in flight per thread
+constexpr int kTransBatch = 4;
 
 template <typename TG, int K, bool IL, bool RANGE>
 __global__ void __launch_bounds__(kTransThreads) trans_matvec_kernel(TransDevice d, MatvecArgs a) {
@@ -258,39 +306,44 @@ __global__ void __launch_bounds__(kTransThreads) trans_matvec_kernel(TransDevice
     const uint32_t w = __ldg(d.reps + s);
     const int r = __ldg(d.rep_rank + s);
     const int os = d.orbits[s];
-    const uint32_t rot1 = ((w >> 1) | (w << (L - 1))) & maskL;
-    const uint32_t rot2 = ((w >> 2) | (w << (L - 2))) & maskL;
-    const uint32_t d1 = w ^ rot1, d2 = w ^ rot2;
+    const uint32_t d1 = w ^ (((w >> 1) | (w << (L - 1))) & maskL);
+    const uint32_t d2 = w ^ (((w >> 2) | (w << (L - 2))) & maskL);
     TG acc[K];
 #pragma unroll
     for (int j = 0; j < K; ++j) acc[j] = TG(0);
-    // J1 bonds (j, j+1), j = 0 .. L-2, by the plain chain's index steps
-    uint32_t f = d1 & (maskL >> 1);
-    while (f) {
-      const int ja = __ffs(f) - 1;
-      f &= f - 1u;
-      const int da = sh.tb.j1[(ja << 5) | __popc(__funnelshift_rc(w, 0u, ja + 2))];
-      trans_element<TG, K, IL, RANGE>(acc, d, sh, x, a, ((w >> ja) & 1u) ? r + da : r - da, os, hj1);
+    FlipCursor cur = flip_cursor(w, r, L);
+    bool more = true;
+    while (more) {
+      int ci[kTransBatch];
+      TG hj[kTransBatch];
+      bool have[kTransBatch];
+#pragma unroll
+      for (int q = 0; q < kTransBatch; ++q) {
+        have[q] = more && next_flip<TG>(cur, sh.tb, L, D, hj1, hj2, ci[q], hj[q]);
+        more = have[q];
+      }
+      unsigned long long e[kTransBatch];
+#pragma unroll
+      for (int q = 0; q < kTransBatch; ++q) e[q] = have[q] ? __ldg(d.map + ci[q]) : 0xffffffffull;
+      TG c[kTransBatch];
+      unsigned int t[kTransBatch];
+#pragma unroll
+      for (int q = 0; q < kTransBatch; ++q) {
+        t[q] = (unsigned int)(e[q] & 0xffffffffull);
+        bool ok = t[q] != 0xffffffffu;  // the flipped word's orbit is not in this momentum sector
+        if (RANGE) ok = ok && (long long)t[q] >= a.col_first && (long long)t[q] < a.col_last;
+        const int n = (int)((e[q] >> 32) & 0xffull), ot = (int)((e[q] >> 40) & 0xffull);
+        c[q] = ok ? hj[q] * (TG)(sh.ratio[os * 33 + ot] * sh.phase[(L - n) % L]) : TG(0);
+        if (!ok) t[q] = (unsigned int)s;  // a harmless in-range gather with a zero coefficient
+      }
+      TG v[kTransBatch][K];
+#pragma unroll
+      for (int q = 0; q < kTransBatch; ++q) trans_gather<TG, K, IL>(x, a, t[q], v[q]);
+#pragma unroll
+      for (int q = 0; q < kTransBatch; ++q)
+#pragma unroll
+        for (int j = 0; j < K; ++j) acc[j] += c[q] * v[q][j];
     }
-    // J2 bonds (j, j+2), j = 0 .. L-3
-    f = d2 & (maskL >> 2);
-    while (f) {
-      const int ja = __ffs(f) - 1;
-      f &= f - 1u;
-      const int da =
-          sh.tb.j2[(((w >> (ja + 1)) & 1u) << 10) | (ja << 5) | __popc(__funnelshift_rc(w, 0u, ja + 3))];
-      trans_element<TG, K, IL, RANGE>(acc, d, sh, x, a, ((w >> ja) & 1u) ? r + da : r - da, os, hj2);
-    }
-    // bonds that wrap around the chain
-    if ((d1 >> (L - 1)) & 1u)
-      trans_element<TG, K, IL, RANGE>(acc, d, sh, x, a, spin_rank_index(sh.tb, w ^ (1u | (1u << (L - 1))), L, D), os,
-                                      hj1);
-    if ((d2 >> (L - 2)) & 1u)
-      trans_element<TG, K, IL, RANGE>(acc, d, sh, x, a, spin_rank_index(sh.tb, w ^ (1u | (1u << (L - 2))), L, D), os,
-                                      hj2);
-    if ((d2 >> (L - 1)) & 1u)
-      trans_element<TG, K, IL, RANGE>(acc, d, sh, x, a, spin_rank_index(sh.tb, w ^ (2u | (1u << (L - 1))), L, D), os,
-                                      hj2);
     // diagonal: J/4 (L - 2 #antiparallel bonds) per bond type (SzSzContributions), plus the shift
     const double diag = 0.25 * d.j1 * (double)(L - 2 * __popc(d1)) + 0.25 * d.j2 * (double)(L - 2 * __popc(d2)) +
                         a.shift;
@@ -310,7 +363,6 @@ __global__ void __launch_bounds__(kTransThreads) trans_matvec_kernel(TransDevice
   }
 }
 
-// elements of one product (antiparallel bonds of the representatives, and those in the sector)
 // every antiparallel bond of representative w (plain chain index r): f(plain index of the flipped
 // word, J / 2 of the bond)
 template <typename T, typename F>
@@ -418,6 +470,7 @@ __global__ void __launch_bounds__(kTransThreads) trans_matvec_complex_kernel(Tra
   }
 }
 
+// elements of one product (antiparallel bonds of the representatives, and those in the sector)
 __global__ void __launch_bounds__(kTransThreads) trans_count_kernel(TransDevice d, unsigned long long* total) {
   __shared__ SpinTables tb;
   build_spin_tables(tb, d.length);
