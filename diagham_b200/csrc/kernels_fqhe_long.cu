@@ -88,10 +88,47 @@ __device__ __forceinline__ int u_position_sum(U128 a) {
          64 * __popcll(a.hi);
 }
 
-__device__ __forceinline__ U128 load_word(const uint64_t* words, long long i) {
-  const ulonglong2 q = __ldg(reinterpret_cast<const ulonglong2*>(words) + i);
-  return {q.x, q.y};
+// the same operations on one 64-bit word (sectors with lz_max <= 63)
+__device__ __forceinline__ uint64_t u_and(uint64_t a, uint64_t b) { return a & b; }
+__device__ __forceinline__ uint64_t u_or(uint64_t a, uint64_t b) { return a | b; }
+__device__ __forceinline__ uint64_t u_not(uint64_t a) { return ~a; }
+__device__ __forceinline__ bool u_any(uint64_t a) { return a != 0ull; }
+__device__ __forceinline__ int u_popc(uint64_t a) { return __popcll(a); }
+__device__ __forceinline__ int u_lowest(uint64_t a) { return __ffsll(a) - 1; }
+__device__ __forceinline__ uint64_t u_clear_lowest(uint64_t a) { return a & (a - 1ull); }
+__device__ __forceinline__ int u_highest(uint64_t a) { return 63 - __clzll(a); }
+__device__ __forceinline__ int u_position_sum(uint64_t a) {
+  return __popcll(a & 0xaaaaaaaaaaaaaaaaull) + 2 * __popcll(a & 0xccccccccccccccccull) +
+         4 * __popcll(a & 0xf0f0f0f0f0f0f0f0ull) + 8 * __popcll(a & 0xff00ff00ff00ff00ull) +
+         16 * __popcll(a & 0xffff0000ffff0000ull) + 32 * __popcll(a & 0xffffffff00000000ull);
 }
+
+template <typename W>
+struct Word;
+template <>
+struct Word<U128> {
+  __device__ static __forceinline__ U128 bit(int q) { return u_bit(q); }
+  __device__ static __forceinline__ U128 below(int q) { return u_below(q); }
+  __device__ static __forceinline__ U128 between(int lo, int hi) { return u_between(lo, hi); }
+  __device__ static __forceinline__ U128 mirror(U128 e, int M) { return u_mirror(e, M); }
+  __device__ static __forceinline__ U128 load(const uint64_t* words, long long i) {
+    const ulonglong2 q = __ldg(reinterpret_cast<const ulonglong2*>(words) + i);
+    return {q.x, q.y};
+  }
+};
+template <>
+struct Word<uint64_t> {
+  __device__ static __forceinline__ uint64_t bit(int q) { return 1ull << q; }
+  __device__ static __forceinline__ uint64_t below(int q) { return q >= 64 ? ~0ull : ((1ull << q) - 1ull); }
+  __device__ static __forceinline__ uint64_t between(int lo, int hi) { return below(hi) & ~below(lo + 1); }
+  // bit p of the result = bit (M - p) of e, M <= 125
+  __device__ static __forceinline__ uint64_t mirror(uint64_t e, int M) {
+    const uint64_t r = __brevll(e);
+    return (M <= 63) ? (r >> (63 - M)) : (r << (M - 63));
+  }
+  // the low half of the stored (low, high) pair: lz_max <= 63 leaves the high half zero
+  __device__ static __forceinline__ uint64_t load(const uint64_t* words, long long i) { return __ldg(words + 2 * i); }
+};
 
 // C(n, o, s), 1 <= n <= N, 0 <= o <= lz_max + 1, 0 <= s <= total_sum
 __device__ __forceinline__ long long count_at(const FqheLongDevice& f, int n, int o, int s) {
@@ -100,8 +137,9 @@ __device__ __forceinline__ long long count_at(const FqheLongDevice& f, int n, in
 
 // sum over the fermions of w in orbitals [lo, hi] of C(n_i, p_i, s_i), given the number and the
 // orbital sum of the fermions below lo
-__device__ __forceinline__ long long range_terms(const FqheLongDevice& f, U128 w, int lo, int hi, int n, int s) {
-  U128 bits = u_and(w, u_and(u_below(hi + 1), u_not(u_below(lo))));
+template <typename W>
+__device__ __forceinline__ long long range_terms(const FqheLongDevice& f, W w, int lo, int hi, int n, int s) {
+  W bits = u_and(w, u_and(Word<W>::below(hi + 1), u_not(Word<W>::below(lo))));
   long long acc = 0;
   while (u_any(bits)) {
     const int q = u_lowest(bits);
@@ -141,46 +179,80 @@ __device__ __forceinline__ void gather_row(const TG* x, const MatvecArgs& a, lon
   }
 }
 
-template <typename TG, int K, bool RANGE, bool IL>
+// Rows of at most kPrefixFermions fermions keep, in shared memory, the prefix sums of their own rank
+// terms and orbitals over their fermions in ascending order (term[j] = sum of the j lowest fermions'
+// C(n_i, p_i, s_i), osum[j] = sum of their orbitals): the row's share of any orbital range is then two
+// popcounts and three shared loads, and only the target's fermions in the range are walked.
+constexpr int kPrefixFermions = 20;
+
+template <typename W, typename TG, int K, bool RANGE, bool IL, bool PREFIX>
 __global__ void __launch_bounds__(kLongThreads) long_matvec_kernel(FqheLongDevice f, MatvecArgs a) {
+  using O = Word<W>;
+  extern __shared__ int prefix_smem[];
+  // thread-strided: entry j of this thread at [j * blockDim.x + threadIdx.x], N + 1 entries each
+  int* term = prefix_smem;
+  int* osum = prefix_smem + (f.nbr_fermions + 1) * kLongThreads;
   const int L = f.lz_max;
-  const U128 full = u_below(L + 1);
+  const W full = O::below(L + 1);
   const TG* fac = static_cast<const TG*>(f.factors);
   const TG* x = static_cast<const TG*>(a.x);
   double* y = static_cast<double*>(a.y);
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long r_end = a.out_last > 0 ? a.out_last : f.dim;
   for (long long r = a.out_first + (long long)blockIdx.x * blockDim.x + threadIdx.x; r < r_end; r += stride) {
-    const U128 s = load_word(f.words, r);
+    const W s = O::load(f.words, r);
     TG acc[K];
 #pragma unroll
     for (int j = 0; j < K; ++j) acc[j] = TG(0);
-    U128 rem1 = s;
+    if (PREFIX) {
+      W bits = s;
+      int j = 0, sum = 0, run = 0;
+      term[threadIdx.x] = 0;
+      osum[threadIdx.x] = 0;
+      while (u_any(bits)) {
+        const int q = u_lowest(bits);
+        bits = u_clear_lowest(bits);
+        ++j;
+        sum += q;
+        run += (int)count_at(f, j, q, sum);
+        term[j * kLongThreads + threadIdx.x] = run;
+        osum[j * kLongThreads + threadIdx.x] = sum;
+      }
+    }
+    W rem1 = s;
     while (u_any(rem1)) {
       const int m1 = u_highest(rem1);
-      rem1 = u_and(rem1, u_not(u_bit(m1)));
-      U128 rem2 = rem1;
+      rem1 = u_and(rem1, u_not(O::bit(m1)));
+      W rem2 = rem1;
       while (u_any(rem2)) {
         const int m2 = u_highest(rem2);
-        rem2 = u_and(rem2, u_not(u_bit(m2)));
+        rem2 = u_and(rem2, u_not(O::bit(m2)));
         const int M = m1 + m2;
-        const U128 an = u_and(s, u_not(u_or(u_bit(m1), u_bit(m2))));
-        const U128 e = u_and(u_not(an), full);
-        U128 valid = u_and(u_and(e, u_mirror(e, M)), u_not(u_below(M / 2 + 1)));
+        const W an = u_and(s, u_not(u_or(O::bit(m1), O::bit(m2))));
+        const W e = u_and(u_not(an), full);
+        W valid = u_and(u_and(e, O::mirror(e, M)), u_not(O::below(M / 2 + 1)));
         if (!u_any(valid)) continue;
-        const int paa = 1 + u_popc(u_and(s, u_between(m2, m1)));
+        const int paa = 1 + u_popc(u_and(s, O::between(m2, m1)));
         const long long fbase = (long long)__ldg(f.pair_offset + m1 * (m1 - 1) / 2 + m2) - (M / 2 + 1);
         while (u_any(valid)) {
           const int m3 = u_lowest(valid);
           valid = u_clear_lowest(valid);
           const int m4 = M - m3;
-          const U128 t = u_or(an, u_or(u_bit(m3), u_bit(m4)));
-          const int par = paa + u_popc(u_and(an, u_between(m4, m3)));
+          const W t = u_or(an, u_or(O::bit(m3), O::bit(m4)));
+          const int par = paa + u_popc(u_and(an, O::between(m4, m3)));
           // the target's index: the row's, corrected over the orbitals [lo, hi] the move touches
           const int lo = min(m2, m4), hi = max(m1, m3);
-          const U128 low_part = u_and(s, u_below(lo));
-          const int n0 = u_popc(low_part), s0 = u_position_sum(low_part);
-          const long long idx = r + range_terms(f, s, lo, hi, n0, s0) - range_terms(f, t, lo, hi, n0, s0);
+          long long idx;
+          if (PREFIX) {
+            const int n0 = u_popc(u_and(s, O::below(lo))), n1 = u_popc(u_and(s, O::below(hi + 1)));
+            const int s0 = osum[n0 * kLongThreads + threadIdx.x];
+            idx = r + (term[n1 * kLongThreads + threadIdx.x] - term[n0 * kLongThreads + threadIdx.x]) -
+                  range_terms<W>(f, t, lo, hi, n0, s0);
+          } else {
+            const W low_part = u_and(s, O::below(lo));
+            const int n0 = u_popc(low_part), s0 = u_position_sum(low_part);
+            idx = r + range_terms<W>(f, s, lo, hi, n0, s0) - range_terms<W>(f, t, lo, hi, n0, s0);
+          }
           if (RANGE && (idx < a.col_first || idx >= a.col_last)) continue;
           TG fct = __ldg(fac + fbase + m3);
           if (par & 1) fct = -fct;
@@ -246,29 +318,31 @@ __global__ void long_find_kernel(FqheLongDevice f, const uint64_t* words, long l
     out[i] = -1;
     return;
   }
-  out[i] = f.dim - 1 - range_terms(f, w, 0, f.lz_max, 0, 0);
+  out[i] = f.dim - 1 - range_terms<U128>(f, w, 0, f.lz_max, 0, 0);
 }
 
 // elements (moves, the diagonal ones included) that one product generates
+template <typename W>
 __global__ void __launch_bounds__(kLongThreads) long_count_kernel(FqheLongDevice f, unsigned long long* total) {
+  using O = Word<W>;
   const int L = f.lz_max;
-  const U128 full = u_below(L + 1);
+  const W full = O::below(L + 1);
   unsigned long long c = 0;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
-    const U128 s = load_word(f.words, r);
-    U128 rem1 = s;
+    const W s = O::load(f.words, r);
+    W rem1 = s;
     while (u_any(rem1)) {
       const int m1 = u_highest(rem1);
-      rem1 = u_and(rem1, u_not(u_bit(m1)));
-      U128 rem2 = rem1;
+      rem1 = u_and(rem1, u_not(O::bit(m1)));
+      W rem2 = rem1;
       while (u_any(rem2)) {
         const int m2 = u_highest(rem2);
-        rem2 = u_and(rem2, u_not(u_bit(m2)));
+        rem2 = u_and(rem2, u_not(O::bit(m2)));
         const int M = m1 + m2;
-        const U128 an = u_and(s, u_not(u_or(u_bit(m1), u_bit(m2))));
-        const U128 e = u_and(u_not(an), full);
-        c += u_popc(u_and(u_and(e, u_mirror(e, M)), u_not(u_below(M / 2 + 1))));
+        const W an = u_and(s, u_not(u_or(O::bit(m1), O::bit(m2))));
+        const W e = u_and(u_not(an), full);
+        c += u_popc(u_and(u_and(e, O::mirror(e, M)), u_not(O::below(M / 2 + 1))));
       }
     }
   }
@@ -286,16 +360,32 @@ int grid_for(long long rows) {
   return (int)blocks;
 }
 
-template <typename TG, int K>
-int launch_typed(const FqheLongDevice& f, const MatvecArgs& a, cudaStream_t s) {
+template <typename W, typename TG, int K, bool PREFIX>
+int launch_prefix(const FqheLongDevice& f, const MatvecArgs& a, cudaStream_t s) {
   const bool range = a.col_first > 0 || a.col_last < f.dim;
   const bool il = (K > 1) && a.ld == K && a.vstride == 1;
-  auto kernel = range ? (il ? long_matvec_kernel<TG, K, true, true> : long_matvec_kernel<TG, K, true, false>)
-                      : (il ? long_matvec_kernel<TG, K, false, true> : long_matvec_kernel<TG, K, false, false>);
+  auto kernel = range ? (il ? long_matvec_kernel<W, TG, K, true, true, PREFIX>
+                            : long_matvec_kernel<W, TG, K, true, false, PREFIX>)
+                      : (il ? long_matvec_kernel<W, TG, K, false, true, PREFIX>
+                            : long_matvec_kernel<W, TG, K, false, false, PREFIX>);
+  // sized by the sector's fermion count, so that the rest of the SM's shared storage stays L1
+  const size_t smem = PREFIX ? 2 * (size_t)(f.nbr_fermions + 1) * kLongThreads * sizeof(int) : 0;
   const long long rows = (a.out_last > 0 ? a.out_last : f.dim) - a.out_first;
-  kernel<<<grid_for(rows), kLongThreads, 0, s>>>(f, a);
+  kernel<<<grid_for(rows), kLongThreads, smem, s>>>(f, a);
   DH_CUDA(cudaGetLastError());
   return DH_OK;
+}
+
+template <typename W, typename TG, int K>
+int launch_word(const FqheLongDevice& f, const MatvecArgs& a, cudaStream_t s) {
+  return f.nbr_fermions <= kPrefixFermions ? launch_prefix<W, TG, K, true>(f, a, s)
+                                           : launch_prefix<W, TG, K, false>(f, a, s);
+}
+
+// one 64-bit word per state when every orbital fits (lz_max <= 63), the 128-bit form above
+template <typename TG, int K>
+int launch_typed(const FqheLongDevice& f, const MatvecArgs& a, cudaStream_t s) {
+  return f.lz_max <= 63 ? launch_word<uint64_t, TG, K>(f, a, s) : launch_word<U128, TG, K>(f, a, s);
 }
 
 template <typename TG>
@@ -336,7 +426,10 @@ int launch_long_find(const FqheLongDevice& f, const uint64_t* words, long long n
 int launch_long_count(const FqheLongDevice& f, unsigned long long* total, cudaStream_t s) {
   DH_CUDA(cudaMemsetAsync(total, 0, sizeof(unsigned long long), s));
   if (f.dim == 0) return DH_OK;
-  long_count_kernel<<<grid_for(f.dim), kLongThreads, 0, s>>>(f, total);
+  if (f.lz_max <= 63)
+    long_count_kernel<uint64_t><<<grid_for(f.dim), kLongThreads, 0, s>>>(f, total);
+  else
+    long_count_kernel<U128><<<grid_for(f.dim), kLongThreads, 0, s>>>(f, total);
   DH_CUDA(cudaGetLastError());
   return DH_OK;
 }
