@@ -523,6 +523,48 @@ def momentum_sector(dh, flush, steps=5, k=2, length=32, warmup=2, solve=True):
                          "precision": 1e-10}
     del lz, H, sp
     torch.cuda.empty_cache()
+    out["complex_k1"] = complex_momentum_sector(dh, flush, length, 1, steps, warmup)
+    return out
+
+
+def complex_momentum_sector(dh, flush, length, momentum, steps, warmup):
+    """The complex Hamiltonian (SpinChainJ1J2HamiltonianWithTranslations) of one momentum sector at
+    J2 = J1/2, FP64 products on (Re, Im) vectors, and the FP64 Lanczos time to its E0."""
+    import torch
+    t0 = time.perf_counter()
+    sp = dh.Spin1_2ChainWithTranslations(length, momentum, 0)
+    H = dh.SpinChainJ1J2HamiltonianWithTranslations(sp, length, 1.0, 0.5)
+    torch.cuda.synchronize()
+    setup = time.perf_counter() - t0
+    flips = H.count_elements()
+    x = torch.empty(2 * sp.dim, dtype=torch.float64, device="cuda")
+    x.uniform_(-1.0, 1.0)
+    y = torch.empty_like(x)
+    for _ in range(warmup):
+        flush.zero_()
+        H.LowLevelMultiply(x, y)
+    ms = []
+    for _ in range(steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        H.LowLevelMultiply(x, y)
+        b.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    del x, y
+    mean_s = statistics.mean(ms) / 1000.0
+    t0 = time.perf_counter()
+    lz = dh.BasicLanczosAlgorithm(H, 1, 600)
+    lz.SetEigenvaluePrecision(1e-10)
+    lz.InitializeLanczosAlgorithm(seed=0)
+    r = lz.solve(600, graph_batch=16)
+    out = {"workload": "K=%d (dim %d), complex vectors" % (momentum, sp.dim), "setup_seconds": setup,
+           "off_diagonal_elements": flips, "fp64_mean_launch_ms": mean_s * 1000.0, "hv_per_s": 1.0 / mean_s,
+           "time_to_e0": {"seconds": time.perf_counter() - t0, "e0": float(r["eigenvalues"][0]),
+                          "iterations": r["iterations"], "precision": 1e-10}}
+    del lz, H, sp
+    torch.cuda.empty_cache()
     return out
 
 

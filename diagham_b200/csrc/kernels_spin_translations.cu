@@ -363,35 +363,6 @@ __global__ void __launch_bounds__(kTransThreads) trans_matvec_kernel(TransDevice
   }
 }
 
-// every antiparallel bond of representative w (plain chain index r): f(plain index of the flipped
-// word, J / 2 of the bond)
-template <typename T, typename F>
-__device__ __forceinline__ void for_each_flip(const SpinTables& tb, const TransDevice& d, uint32_t w, int r, T hj1,
-                                              T hj2, F&& f) {
-  const int L = d.length;
-  const int D = (int)d.chain_dim;
-  const uint32_t maskL = (L == 32) ? 0xffffffffu : ((1u << L) - 1u);
-  const uint32_t d1 = w ^ (((w >> 1) | (w << (L - 1))) & maskL);
-  const uint32_t d2 = w ^ (((w >> 2) | (w << (L - 2))) & maskL);
-  uint32_t b = d1 & (maskL >> 1);
-  while (b) {
-    const int ja = __ffs(b) - 1;
-    b &= b - 1u;
-    const int da = tb.j1[(ja << 5) | __popc(__funnelshift_rc(w, 0u, ja + 2))];
-    f(((w >> ja) & 1u) ? r + da : r - da, hj1);
-  }
-  b = d2 & (maskL >> 2);
-  while (b) {
-    const int ja = __ffs(b) - 1;
-    b &= b - 1u;
-    const int da = tb.j2[(((w >> (ja + 1)) & 1u) << 10) | (ja << 5) | __popc(__funnelshift_rc(w, 0u, ja + 3))];
-    f(((w >> ja) & 1u) ? r + da : r - da, hj2);
-  }
-  if ((d1 >> (L - 1)) & 1u) f(spin_rank_index(tb, w ^ (1u | (1u << (L - 1))), L, D), hj1);
-  if ((d2 >> (L - 2)) & 1u) f(spin_rank_index(tb, w ^ (1u | (1u << (L - 2))), L, D), hj2);
-  if ((d2 >> (L - 1)) & 1u) f(spin_rank_index(tb, w ^ (2u | (1u << (L - 1))), L, D), hj2);
-}
-
 struct TransSharedComplex {
   SpinTables tb;
   double ratio[33 * 33];  // sqrt(o_s / o_t)
@@ -429,28 +400,55 @@ __global__ void __launch_bounds__(kTransThreads) trans_matvec_complex_kernel(Tra
     const int r = __ldg(d.rep_rank + s);
     const int os = d.orbits[s];
     TG re = TG(0), im = TG(0);
-    for_each_flip(sh.tb, d, w, r, (TG)(0.5 * d.j1), (TG)(0.5 * d.j2), [&](int ci, TG hj) {
-      const unsigned long long e = __ldg(d.map + ci);
-      const unsigned int t = (unsigned int)(e & 0xffffffffull);
-      if (t == 0xffffffffu) return;
-      if (RANGE && ((long long)t < c_first || (long long)t >= c_last)) return;
-      const int n = (int)((e >> 32) & 0xffull), ot = (int)((e >> 40) & 0xffull);
-      const int m = (L - n) % L;
-      const double mag = sh.ratio[os * 33 + ot];
-      const TG cr = hj * (TG)(mag * sh.phase[m]), cim = -hj * (TG)(mag * sh.sine[m]);
-      TG xr, xi;
-      if constexpr (sizeof(TG) == 8) {
-        const double2 q = __ldg(reinterpret_cast<const double2*>(x) + t);
-        xr = q.x;
-        xi = q.y;
-      } else {
-        const float2 q = __ldg(reinterpret_cast<const float2*>(x) + t);
-        xr = q.x;
-        xi = q.y;
+    // flips kTransBatch at a time, their map loads and then their gathers in flight together
+    const TG hj1 = (TG)(0.5 * d.j1), hj2 = (TG)(0.5 * d.j2);
+    FlipCursor cur = flip_cursor(w, r, L);
+    bool more = true;
+    while (more) {
+      int ci[kTransBatch];
+      TG hj[kTransBatch];
+      bool have[kTransBatch];
+#pragma unroll
+      for (int q = 0; q < kTransBatch; ++q) {
+        have[q] = more && next_flip<TG>(cur, sh.tb, L, (int)d.chain_dim, hj1, hj2, ci[q], hj[q]);
+        more = have[q];
       }
-      re += cr * xr - cim * xi;
-      im += cr * xi + cim * xr;
-    });
+      unsigned long long e[kTransBatch];
+#pragma unroll
+      for (int q = 0; q < kTransBatch; ++q) e[q] = have[q] ? __ldg(d.map + ci[q]) : 0xffffffffull;
+      TG cr[kTransBatch], cim[kTransBatch];
+      unsigned int t[kTransBatch];
+#pragma unroll
+      for (int q = 0; q < kTransBatch; ++q) {
+        t[q] = (unsigned int)(e[q] & 0xffffffffull);
+        bool ok = t[q] != 0xffffffffu;  // the flipped word's orbit is not in this momentum sector
+        if (RANGE) ok = ok && (long long)t[q] >= c_first && (long long)t[q] < c_last;
+        const int n = (int)((e[q] >> 32) & 0xffull), ot = (int)((e[q] >> 40) & 0xffull);
+        const int m = (L - n) % L;
+        const double mag = ok ? sh.ratio[os * 33 + ot] : 0.0;
+        cr[q] = hj[q] * (TG)(mag * sh.phase[m]);
+        cim[q] = -hj[q] * (TG)(mag * sh.sine[m]);
+        if (!ok) t[q] = (unsigned int)s;  // a harmless in-range gather with a zero coefficient
+      }
+      TG xr[kTransBatch], xi[kTransBatch];
+#pragma unroll
+      for (int q = 0; q < kTransBatch; ++q) {
+        if constexpr (sizeof(TG) == 8) {
+          const double2 v = __ldg(reinterpret_cast<const double2*>(x) + t[q]);
+          xr[q] = v.x;
+          xi[q] = v.y;
+        } else {
+          const float2 v = __ldg(reinterpret_cast<const float2*>(x) + t[q]);
+          xr[q] = v.x;
+          xi[q] = v.y;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kTransBatch; ++q) {
+        re += cr[q] * xr[q] - cim[q] * xi[q];
+        im += cr[q] * xi[q] + cim[q] * xr[q];
+      }
+    }
     const uint32_t d1 = w ^ (((w >> 1) | (w << (L - 1))) & maskL);
     const uint32_t d2 = w ^ (((w >> 2) | (w << (L - 2))) & maskL);
     double vr = (double)re, vi = (double)im;

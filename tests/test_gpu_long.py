@@ -235,3 +235,30 @@ def test_long_refusals(gpu):
     assert w.dtype == np.uint64 and np.all(lzm <= 50)
     with pytest.raises(gpu.DiagHamError, match="error -4"):
         f.EvaluatePartialDensityMatrix(20, 1, 0, np.ones(f.dim))
+
+
+@pytest.mark.parametrize("n,s,lz", [(1, 100, 10), (64, 63, 0), (3, 100, 294), (2, 126, -250)])
+def test_long_one_state_sectors(gpu, orc, n, s, lz):
+    # one fermion, the filled shell (every pair returns to itself), the highest and the lowest Lz
+    v = orc.coulomb_pseudopotentials(s)
+    v[0::2] = 0.0
+    sp = gpu.FermionOnSphereLong(n, lz, s)
+    assert sp.dim == 1
+    assert sp.word_values(sp.states()[0]) == orc.fermion_basis_long(n, s, lz)
+    H = gpu.ParticleOnSphereGenericHamiltonian(sp, n, s, v)
+    H.ShiftHamiltonian(0.25)
+    y = H.LowLevelMultiply(np.array([1.0]))
+    ref = orc.FQHELong(n, s, lz, v, shift=0.25).push(np.array([1.0]))
+    assert abs(y[0] - ref[0]) <= 1e-13 * max(1.0, abs(ref[0]))
+    assert H.count_elements() == n * (n - 1) // 2
+
+
+def test_long_empty_and_oversized_sectors(gpu):
+    with pytest.raises(gpu.DiagHamError, match="empty sector"):
+        gpu.FermionOnSphereLong(4, -312, 80)
+    with pytest.raises(gpu.DiagHamError, match="2\\^31"):
+        gpu.FermionOnSphereLong(40, 0, 126)
+    with pytest.raises(gpu.DiagHamError, match="not reachable"):
+        gpu.FermionOnSphereLong(3, 1, 100)
+    f = gpu.FermionOnSphere(63, 0, 62)  # the filled 64-bit shell through FermionOnSphere
+    assert f.dim == 1 and int(f.states()[0][0]) == (1 << 63) - 1
