@@ -128,6 +128,22 @@ static int build_long_fermion_space(dh_space_s* sp) {
   return DH_OK;
 }
 
+// a space of 64-bit words beyond the split-word tables (BosonOnSphereShort up to lz_max + N - 1 = 62):
+// the count table and the words of the 128-bit engine, kept as plain uint64 words
+static int build_count_rank_space(dh_space_s* sp) {
+  int rc = build_long_fermion_space(sp);
+  if (rc != DH_OK) return rc;
+  DevBuf pairs;
+  std::swap(pairs.ptr, sp->words.ptr);
+  std::swap(pairs.bytes, sp->words.bytes);
+  if ((rc = sp->words.alloc((size_t)sp->dim * sizeof(uint64_t))) != DH_OK) return rc;
+  DH_CUDA(cudaMemcpy2D(sp->words.ptr, sizeof(uint64_t), pairs.ptr, 2 * sizeof(uint64_t), sizeof(uint64_t), sp->dim,
+                       cudaMemcpyDeviceToDevice));
+  DH_CUDA(cudaDeviceSynchronize());
+  sp->count_rank = true;
+  return DH_OK;
+}
+
 static int build_fermion_space(dh_space_s* sp) {
   const int N = sp->nbr_fermions, L = sp->lz_max, K = sp->total_sum;
   const int O = L + 2;  // orbital counts 0 .. L+1
@@ -217,6 +233,12 @@ FqheDevice fqhe_device(const dh_space_s* sp, const dh_hamiltonian_s* h, int prec
   f.kernel_variant = sp->kernel_variant;
   f.boson_lz_max = sp->boson_lz_max;
   f.nbr_bosons = (sp->kind == SPACE_BOSON) ? sp->nbr_fermions : 0;
+  f.nbr_particles = sp->nbr_fermions;
+  if (sp->count_rank) {
+    f.count_table = sp->long_table.as<int32_t>();
+    f.count_stride_o = sp->total_sum + 1;
+    f.count_stride_n = (long long)(sp->lz_max + 2) * (sp->total_sum + 1);
+  }
   if (h) {
     f.pair_offset = h->pair_offset.as<int32_t>();
     f.factors = (precision == DH_PRECISION_FP32) ? h->factors32.ptr : h->factors64.ptr;
@@ -521,8 +543,10 @@ int dh_boson_on_sphere_create(int nbr_bosons, int total_lz, int lz_max, unsigned
   *out = nullptr;
   DH_CHECK(nbr_bosons >= 1, DH_ERR_ARGUMENT, "BosonOnSphereShort: nbr_bosons must be >= 1");
   DH_CHECK(lz_max >= 0, DH_ERR_ARGUMENT, "BosonOnSphereShort: lz_max must be >= 0");
-  DH_CHECK(lz_max + nbr_bosons - 1 <= 40, DH_ERR_UNSUPPORTED,
-           "BosonOnSphereShort: lz_max + N - 1 = %d > 40 is not supported", lz_max + nbr_bosons - 1);
+  // the reference's BosonOnSphereShort range (BosonOnSphere from lz_max + N - 1 = 63 on,
+  // ParticleOnSphereManager.cc:487)
+  DH_CHECK(lz_max + nbr_bosons - 1 <= 62, DH_ERR_UNSUPPORTED,
+           "BosonOnSphereShort: lz_max + N - 1 = %d > 62 needs the reference's BosonOnSphere", lz_max + nbr_bosons - 1);
   const int twice = total_lz + nbr_bosons * lz_max;
   DH_CHECK(twice >= 0 && (twice & 1) == 0 && twice <= 2 * nbr_bosons * lz_max, DH_ERR_ARGUMENT,
            "BosonOnSphereShort: total_lz = %d is not reachable by %d bosons with lz_max = %d", total_lz, nbr_bosons,
@@ -541,7 +565,8 @@ int dh_boson_on_sphere_create(int nbr_bosons, int total_lz, int lz_max, unsigned
   sp->kernel_variant = 1;
   const char* lb = getenv("DH_FQHE_LOW_BITS");
   sp->requested_low_bits = lb ? atoi(lb) : 0;
-  int rc = build_fermion_space(sp);
+  // up to 40 bits the split-word rank tables; beyond, ranks from the sector's count table
+  int rc = (sp->lz_max <= 40) ? build_fermion_space(sp) : build_count_rank_space(sp);
   if (rc != DH_OK) {
     delete sp;
     return rc;
@@ -780,10 +805,10 @@ int dh_space_find_state_index(dh_space_t sp, const uint64_t* words, int64_t n, i
     if ((rc = di.alloc(n * sizeof(int64_t))) != DH_OK) return rc;
     out = di.as<int64_t>();
   }
-  if (sp->kind == SPACE_FERMION || sp->kind == SPACE_BOSON) {
+  if ((sp->kind == SPACE_FERMION || sp->kind == SPACE_BOSON) && !sp->count_rank) {
     if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
     rc = launch_fqhe_find(fqhe_device(sp, nullptr, 0), w, n, reinterpret_cast<long long*>(out), 0);
-  } else if (sp->kind == SPACE_FERMION_LONG) {
+  } else if (sp->kind == SPACE_FERMION_LONG || sp->count_rank) {
     // 64-bit words as (word, 0) pairs
     DevBuf pairs;
     if ((rc = pairs.alloc(2 * n * sizeof(uint64_t))) != DH_OK) return rc;

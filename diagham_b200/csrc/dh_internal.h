@@ -115,6 +115,12 @@ struct FqheDevice {
   int kernel_variant;          // 0: split-word rank kernel, 1: generic kernel (rank mode)
   int boson_lz_max;            // BosonOnSphereShort: orbitals 0..boson_lz_max (words of lz_max + 1 bits)
   int nbr_bosons;
+  // words beyond the split-word tables (BosonOnSphereShort with lz_max + N - 1 > 40): ranks from the
+  // fermionic sector's count table C(n, o, s) at (n - 1) * count_stride_n + o * count_stride_o + s
+  const int32_t* count_table;
+  long long count_stride_n;
+  int count_stride_o;
+  int nbr_particles;           // N (fermions of the word)
 };
 
 // Fermions with 128-bit words (FermionOnSphereLong, and FermionOnSphere beyond the split-word tables)

@@ -29,6 +29,8 @@ struct dh_space_s {
   // space was created as FermionOnSphere (its words are 64-bit for dh_space_get_states)
   dh::DevBuf long_table;
   int api_halves = 2;
+  // BosonOnSphereShort beyond the split-word tables: uint64 words, ranks from long_table
+  bool count_rank = false;
   dh::FermionRankTables rank;
   dh::DevBuf low_rank, high_offset;
   dh::DevBuf lookup, lookup_shift;

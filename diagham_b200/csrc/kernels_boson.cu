@@ -82,13 +82,51 @@ __device__ __forceinline__ void gather_row(const TG* x, const MatvecArgs& a, lon
   }
 }
 
-template <typename TG, int K, bool RANGE, bool IL>
+// Ranks beyond the split-word tables (words of more than 41 bits).  With C(n, o, s) the fermionic
+// sector's count table, index(w) = dim - 1 - sum over the ones of w of C(n_i, p_i, s_i) (n_i ones at or
+// below bit p_i, s_i the sum of their positions).  A move changes the word only between the lowest
+// and the highest bit where row and target differ; outside that range every term is the row's, so the
+// target's index is the row's corrected by the terms of the ones inside the range.
+constexpr int kBosonPrefixParticles = 20;
+
+__device__ __forceinline__ long long count_at(const FqheDevice& f, int n, int o, int s) {
+  return (long long)__ldg(f.count_table + (size_t)(n - 1) * f.count_stride_n + (size_t)o * f.count_stride_o + s);
+}
+
+// the terms of the ones of w at bits lo..hi, given the count n and position sum s of its ones below lo
+__device__ __forceinline__ long long count_terms(const FqheDevice& f, uint64_t w, int lo, int hi, int n, int s) {
+  uint64_t bits = w & (((hi >= 63) ? ~0ull : ((2ull << hi) - 1ull)) & ~((1ull << lo) - 1ull));
+  long long acc = 0;
+  while (bits) {
+    const int q = __ffsll(bits) - 1;
+    bits &= bits - 1ull;
+    ++n;
+    s += q;
+    acc += count_at(f, n, q, s);
+  }
+  return acc;
+}
+
+__device__ __forceinline__ int position_sum(uint64_t a) {
+  return __popcll(a & 0xaaaaaaaaaaaaaaaaull) + 2 * __popcll(a & 0xccccccccccccccccull) +
+         4 * __popcll(a & 0xf0f0f0f0f0f0f0f0ull) + 8 * __popcll(a & 0xff00ff00ff00ff00ull) +
+         16 * __popcll(a & 0xffff0000ffff0000ull) + 32 * __popcll(a & 0xffffffff00000000ull);
+}
+
+// RM = 0: split-word rank tables, factors staged in shared memory; RM = 1: count-table ranks with the
+// row's prefix sums (its terms and position sums over its ones, thread-strided in shared memory),
+// factors read through the cache; RM = 2: count-table ranks walking row and target, factors cached
+template <typename TG, int K, bool RANGE, bool IL, int RM>
 __global__ void __launch_bounds__(kBosonThreads) boson_matvec_kernel(FqheDevice f, MatvecArgs a, int factor_smem) {
   extern __shared__ __align__(16) unsigned char smem[];
   TG* sfac = reinterpret_cast<TG*>(smem);
   int* spair = reinterpret_cast<int*>(smem + factor_smem);
+  int* term = spair + ((f.nbr_pairs + 3) & ~3);
+  int* osum = term + (f.nbr_particles + 1) * kBosonThreads;
   const TG* gfac = static_cast<const TG*>(f.factors);
-  for (int i = threadIdx.x; i < f.nbr_factors; i += blockDim.x) sfac[i] = gfac[i];
+  if (RM == 0)
+    for (int i = threadIdx.x; i < f.nbr_factors; i += blockDim.x) sfac[i] = gfac[i];
+  const TG* fac = (RM == 0) ? sfac : gfac;
   for (int i = threadIdx.x; i < f.nbr_pairs; i += blockDim.x) spair[i] = f.pair_offset[i];
   __syncthreads();
 
@@ -110,14 +148,31 @@ __global__ void __launch_bounds__(kBosonThreads) boson_matvec_kernel(FqheDevice 
   TG acc[K];
   TG dsum = TG(0), saa = TG(0);
   int m1 = -1, m2 = 0, m3 = 1, m3hi = 0, m4 = 0, q3 = 0, c3 = 0, q4 = 0, c4 = 0;
-  const TG* fp = sfac;
+  const TG* fp = fac;
   // row r's word, the halves of its rank, occupations, group starts and pair masks
   auto open_row = [&]() {
     s = __ldg(f.words + r);
-    sh = s >> LB;
-    sl = s & lmask;
-    ho_row = __ldg(f.high_offset + sh);
-    lr_row = (int)(r - ho_row);
+    if (RM == 0) {
+      sh = s >> LB;
+      sl = s & lmask;
+      ho_row = __ldg(f.high_offset + sh);
+      lr_row = (int)(r - ho_row);
+    } else if (RM == 1) {
+      uint64_t bits = s;
+      int j = 0, sum = 0;
+      long long run = 0;
+      term[threadIdx.x] = 0;
+      osum[threadIdx.x] = 0;
+      while (bits) {
+        const int q = __ffsll(bits) - 1;
+        bits &= bits - 1ull;
+        ++j;
+        sum += q;
+        run += count_at(f, j, q, sum);
+        term[j * kBosonThreads + threadIdx.x] = (int)run;
+        osum[j * kBosonThreads + threadIdx.x] = sum;
+      }
+    }
     occ = 0;
     dbl = 0;
     int pos = 0;
@@ -180,7 +235,7 @@ __global__ void __launch_bounds__(kBosonThreads) boson_matvec_kernel(FqheDevice 
       const int M = m1 + m2;
       const int m3lo = (M + 1) >> 1;
       m3hi = (M < L) ? M : L;
-      fp = sfac + (spair[m1 * (m1 + 1) / 2 + m2] - m3lo);
+      fp = fac + (spair[m1 * (m1 + 1) / 2 + m2] - m3lo);
       // diagonal move: a+_m1 a+_m2 a_m1 a_m2 gives back the row with coefficient n_m2 (n_m1 - [m1 = m2])
       dsum += fp[m1] * (TG)caa;
       // group start q and occupation c of orbitals m3 (walking up) and m4 = M - m3 (walking down) in
@@ -195,11 +250,28 @@ __global__ void __launch_bounds__(kBosonThreads) boson_matvec_kernel(FqheDevice 
     if (m3 != m1) {
       const int cad = (m3 == m4) ? (c4 + 1) * (c4 + 2) : (c4 + 1) * (c3 + 1);
       const uint64_t t = insert_one(insert_one(an, q3), q4);
-      const uint64_t th = t >> LB, tl = t & lmask;
-      int hoi = ho_row, lri = lr_row;
-      if (th != sh) hoi = __ldg(f.high_offset + th);
-      if (tl != sl) lri = (int)__ldg(f.low_rank + tl);
-      const long long idx = (long long)hoi + (long long)lri;
+      long long idx;
+      if (RM == 0) {
+        const uint64_t th = t >> LB, tl = t & lmask;
+        int hoi = ho_row, lri = lr_row;
+        if (th != sh) hoi = __ldg(f.high_offset + th);
+        if (tl != sl) lri = (int)__ldg(f.low_rank + tl);
+        idx = (long long)hoi + (long long)lri;
+      } else {
+        const uint64_t diff = s ^ t;  // never 0: m3 != m1 changes the occupations
+        const int lo = __ffsll(diff) - 1, hi = 63 - __clzll(diff);
+        const uint64_t low_part = s & ((1ull << lo) - 1ull);
+        const int n0 = __popcll(low_part);
+        if (RM == 1) {
+          const int n1 = __popcll(s & ((hi >= 63) ? ~0ull : ((2ull << hi) - 1ull)));
+          const int s0 = osum[n0 * kBosonThreads + threadIdx.x];
+          idx = r + (long long)(term[n1 * kBosonThreads + threadIdx.x] - term[n0 * kBosonThreads + threadIdx.x]) -
+                count_terms(f, t, lo, hi, n0, s0);
+        } else {
+          const int s0 = position_sum(low_part);
+          idx = r + count_terms(f, s, lo, hi, n0, s0) - count_terms(f, t, lo, hi, n0, s0);
+        }
+      }
       if (!RANGE || (idx >= a.col_first && idx < a.col_last)) {
         const TG c = fp[m3] * saa * coef_sqrt<TG>(cad);
         TG xv[K];
@@ -224,14 +296,15 @@ __global__ void __launch_bounds__(kBosonThreads) boson_matvec_kernel(FqheDevice 
   }
 }
 
-template <typename TG, int K>
-int launch_typed(const FqheDevice& f, const MatvecArgs& a, cudaStream_t s) {
-  const int factor_smem = (int)((f.nbr_factors * sizeof(TG) + 15) & ~(size_t)15);
-  const size_t smem = (size_t)factor_smem + (size_t)f.nbr_pairs * sizeof(int);
+template <typename TG, int K, int RM>
+int launch_rank(const FqheDevice& f, const MatvecArgs& a, cudaStream_t s) {
+  const int factor_smem = (RM == 0) ? (int)((f.nbr_factors * sizeof(TG) + 15) & ~(size_t)15) : 0;
+  size_t smem = (size_t)factor_smem + (size_t)((f.nbr_pairs + 3) & ~3) * sizeof(int);
+  if (RM == 1) smem += 2 * (size_t)(f.nbr_particles + 1) * kBosonThreads * sizeof(int);
   const bool range = a.col_first > 0 || a.col_last < f.dim;
   const bool il = (K > 1) && a.ld == K && a.vstride == 1;
-  auto kernel = range ? (il ? boson_matvec_kernel<TG, K, true, true> : boson_matvec_kernel<TG, K, true, false>)
-                      : (il ? boson_matvec_kernel<TG, K, false, true> : boson_matvec_kernel<TG, K, false, false>);
+  auto kernel = range ? (il ? boson_matvec_kernel<TG, K, true, true, RM> : boson_matvec_kernel<TG, K, true, false, RM>)
+                      : (il ? boson_matvec_kernel<TG, K, false, true, RM> : boson_matvec_kernel<TG, K, false, false, RM>);
   if (smem > 48 * 1024) DH_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int sms = 148;
   int dev = 0;
@@ -244,6 +317,12 @@ int launch_typed(const FqheDevice& f, const MatvecArgs& a, cudaStream_t s) {
   kernel<<<(unsigned)blocks, kBosonThreads, smem, s>>>(f, a, factor_smem);
   DH_CUDA(cudaGetLastError());
   return DH_OK;
+}
+
+template <typename TG, int K>
+int launch_typed(const FqheDevice& f, const MatvecArgs& a, cudaStream_t s) {
+  if (!f.count_table) return launch_rank<TG, K, 0>(f, a, s);
+  return f.nbr_particles <= kBosonPrefixParticles ? launch_rank<TG, K, 1>(f, a, s) : launch_rank<TG, K, 2>(f, a, s);
 }
 
 template <typename TG>

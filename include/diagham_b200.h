@@ -85,9 +85,11 @@ int dh_fermion_on_sphere_long_create(int nbr_fermions, int total_lz, int lz_max,
 /* BosonOnSphereShort(nbrBosons, totalLz, lzMax): FQHE/src/HilbertSpace/BosonOnSphereShort.cc:81-110.
  * The states are stored, ordered and found as the FermionOnSphere(N, totalLz, lzMax + N - 1) words
  * of their occupations (n_0 ones, a zero, n_1 ones, ...; BosonOnSphereShort.h:1231), so
- * dh_space_get_states and dh_space_find_state_index take those words.  Rank index mode only;
- * rejects lz_max + N - 1 > 40 (the reference switches to BosonOnSphere from lz_max + N - 1 = 63,
- * ParticleOnSphereManager.cc:487).  memory is accepted for the signature and unused. */
+ * dh_space_get_states and dh_space_find_state_index take those words.  Rank index mode only:
+ * split-word rank tables up to lz_max + N - 1 = 40, beyond that (to 62, the class's own range: the
+ * reference switches to BosonOnSphere from lz_max + N - 1 = 63, ParticleOnSphereManager.cc:487) ranks
+ * from the fermionic sector's count table.  Rejects lz_max + N - 1 > 62.  memory is accepted for the
+ * signature and unused. */
 int dh_boson_on_sphere_create(int nbr_bosons, int total_lz, int lz_max, unsigned long memory, dh_space_t* out);
 
 /* Spin1_2Chain(chainLength, sz, memorySize): Spin/src/HilbertSpace/Spin1_2Chain.cc:113-142.

@@ -465,6 +465,8 @@ static void Usage()
 	  "  lfqhe_basis N 2S 2Lz out\n"
 	  "  lfqhe_factors N 2S vfile out\n"
 	  "  lfqhe_matvec_f N 2S 2Lz vfile ffile xfile shift out\n"
+	  "  bqhe_factors N 2S vfile out\n"
+	  "  bqhe_matvec_f N 2S 2Lz vfile ffile xfile shift out\n"
 	  "  lfqhe_matvec N 2S 2Lz vfile xfile shift out\n"
 	  "  lfqhe_lanczos N 2S 2Lz vfile algo nev block maxiter precision out gsout x0 [x1 ...]\n"
 	  "  bqhe_basis N 2S 2Lz out\n"
@@ -521,13 +523,17 @@ int main(int argc, char** argv)
       return 0;
     }
   // lfqhe_factors: the same tables built on a FermionOnSphereLong space (lzMax up to 126)
-  if ((strcmp(Cmd, "fqhe_factors") == 0 || strcmp(Cmd, "lfqhe_factors") == 0) && argc == 6)
+  // bqhe_factors: the bosonic tables (BosonOnSphereShort space)
+  if ((strcmp(Cmd, "fqhe_factors") == 0 || strcmp(Cmd, "lfqhe_factors") == 0 || strcmp(Cmd, "bqhe_factors") == 0) &&
+      argc == 6)
     {
       int N = atoi(argv[2]), LzMax = atoi(argv[3]);
       double* V = ReadDoubles(argv[4], LzMax + 1);
       ParticleOnSphere* SpacePtr;
       if (Cmd[0] == 'l')
 	SpacePtr = new FermionOnSphereLong(N, (N & 1) ? 1 : 0, LzMax, 1ul << 20);
+      else if (Cmd[0] == 'b')
+	SpacePtr = new BosonOnSphereShort(N, ((N * LzMax) & 1) ? 1 : 0, LzMax);
       else
 	SpacePtr = new FermionOnSphere(N, (N & 1) ? 1 : 0, LzMax, 1ul << 20);
       MonoProcessorArchitecture Arch;
@@ -641,13 +647,19 @@ int main(int argc, char** argv)
     }
   // the reference's FermionOnSphereLong product with its interaction factors replaced by the ones in
   // ffile (NbrFactors doubles, in the order lfqhe_factors writes them)
-  if (strcmp(Cmd, "lfqhe_matvec_f") == 0 && argc == 10)
+  // bqhe_matvec_f: the same for BosonOnSphereShort
+  if ((strcmp(Cmd, "lfqhe_matvec_f") == 0 || strcmp(Cmd, "bqhe_matvec_f") == 0) && argc == 10)
     {
       int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
       double* V = ReadDoubles(argv[5], LzMax + 1);
-      FermionOnSphereLong Space(N, TotalLz, LzMax, 1ul << 20);
+      ParticleOnSphere* SpacePtr;
+      if (Cmd[0] == 'b')
+	SpacePtr = new BosonOnSphereShort(N, TotalLz, LzMax);
+      else
+	SpacePtr = new FermionOnSphereLong(N, TotalLz, LzMax, 1ul << 20);
+      ParticleOnSphere& Space = *SpacePtr;
       MonoProcessorArchitecture Arch;
-      ExposedGenericHamiltonian H(&Space, N, LzMax, V, &Arch, false);
+      ExposedGenericHamiltonian H(SpacePtr, N, LzMax, V, &Arch, false);
       double* F = ReadDoubles(argv[6], H.NbrFactors());
       for (int i = 0; i < H.NbrFactors(); ++i)
 	H.SetFactor(i, F[i]);

@@ -335,6 +335,60 @@ def boson_fixtures(tmp):
              occupations=occ, max_iter=300, **ys, **read_lanczos(lf))
 
 
+BOSON_LARGE_CASES = [(2, 61, 0), (3, 40, 0), (3, 60, 0), (4, 45, 2), (5, 50, 0)]
+
+
+def boson_large_fixtures(tmp):
+    # BosonOnSphereShort beyond 41-bit words (lz_max + N - 1 = 42 to 62, the reference's own range for
+    # this class): the states as their fermionic words (n_0 ones, a zero, n_1 ones, ...), or the SHA-256 of
+    # those words above 13,000 states, y = H x (x = splitmix64 seed 0) at shifts 0 and 0.37 (shift 0 only
+    # above 13,000 states) from the reference's product with the exact interaction factors written into
+    # its table (bqhe_matvec_f; its own factors drift at this 2S, so its own product is kept beside it
+    # with the factors' deviation), and the basic Lanczos run (its own factors) where the sector has at
+    # most 13,000 states; V = the reference's own LLL Coulomb pseudopotentials with the odd m set to zero
+    import hashlib
+    for (n, s, lz) in BOSON_LARGE_CASES:
+        p = os.path.join(tmp, "pp.bin")
+        run("pseudopotentials", s, p)
+        v = np.fromfile(p, np.float64)
+        v[1::2] = 0.0
+        vf = os.path.join(tmp, "vb.bin")
+        v.tofile(vf)
+        bf = os.path.join(tmp, "bb.bin")
+        cmd = run("bqhe_basis", n, s, lz, bf)
+        b = open(bf, "rb").read()
+        dim = int(np.frombuffer(b[:8], np.int64)[0])
+        occ = np.frombuffer(b[8:], np.int32).reshape(dim, s + 1)
+        words = np.zeros(dim, np.uint64)
+        for i in range(dim):
+            w, pos = 0, 0
+            for m in range(s + 1):
+                w |= ((1 << int(occ[i, m])) - 1) << pos
+                pos += int(occ[i, m]) + 1
+            words[i] = w
+        xf = os.path.join(tmp, "xb.vec")
+        write_vector(xf, splitmix_vector(0, dim))
+        exact, own = exact_factors_in_reference_order(tmp, n, s, v, bosons=True)
+        ff = os.path.join(tmp, "fb.bin")
+        exact.tofile(ff)
+        ys = {"own_factor_deviation": np.max(np.abs(exact - own)) / np.max(np.abs(exact))}
+        for shift in ((0.0, 0.37) if dim <= 13000 else (0.0,)):
+            yf = os.path.join(tmp, "yb.vec")
+            run("bqhe_matvec", n, s, lz, vf, xf, shift, yf)
+            ys["y_own_factors_shift%g" % shift] = read_vector(yf)
+            cmd2 = run("bqhe_matvec_f", n, s, lz, vf, ff, xf, shift, yf)
+            ys["y_shift%g" % shift] = read_vector(yf)
+        extra = {}
+        if dim <= 13000:
+            lf = os.path.join(tmp, "lb.out")
+            run("bqhe_lanczos", n, s, lz, vf, "basic", 1, 1, 300, 0, lf, "-", xf)
+            extra = read_lanczos(lf)
+            extra["words"] = words
+        else:
+            extra["words_sha256"] = hashlib.sha256(words.tobytes()).hexdigest()
+        save("boson_large_n%d_2s%d_lz%d.npz" % (n, s, lz), cmd + "; " + cmd2, v=v, seed=0, dim=dim, **ys, **extra)
+
+
 ENTANGLEMENT_CASES = [(11, 4, 0), (11, 4, 2), (11, 3, -3), (5, 2, 0), (1, 1, 0), (1, 0, 0), (0, 0, 0), (11, 0, 0),
                       (21, 8, 0), (15, 8, 56), (20, 7, -5), (22, 8, 0)]
 
@@ -416,17 +470,17 @@ def coulomb_closed_form(two_s):
     return out
 
 
-def exact_factors_in_reference_order(tmp, n, s, v):
+def exact_factors_in_reference_order(tmp, n, s, v, bosons=False):
     """The oracle's interaction factors (Clebsch-Gordan coefficients exact to the last bit) laid out in
-    the reference's own (pair, m3) order, read from its lfqhe_factors table."""
+    the reference's own (pair, m3) order, read from its lfqhe_factors (bqhe_factors) table."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     vf = os.path.join(tmp, "vf.bin")
     v.tofile(vf)
     ff = os.path.join(tmp, "ff.bin")
-    run("lfqhe_factors", n, s, vf, ff)
+    run("bqhe_factors" if bosons else "lfqhe_factors", n, s, vf, ff)
     r = read_factors(ff)
-    t = oracle.interaction_tables(s, v)
+    t = oracle.boson_interaction_tables(s, v) if bosons else oracle.interaction_tables(s, v)
     ours = {}
     for p in range(len(t["m1"])):
         o = int(t["m3_offset"][p])
@@ -640,6 +694,8 @@ def main():
             translation_fixtures(tmp)
         if args.only in (None, "long"):
             long_fixtures(tmp)
+        if args.only in (None, "boson_large"):
+            boson_large_fixtures(tmp)
         if args.only in (None, "translations_complex"):
             translation_complex_fixtures(tmp)
         if args.slow:

@@ -19,7 +19,7 @@ from conftest import GOLDEN, golden, parse_sector
 
 pytestmark = pytest.mark.gpu
 
-NAMES = sorted(os.path.basename(f) for f in glob.glob(os.path.join(GOLDEN, "boson_*.npz")))
+NAMES = sorted(os.path.basename(f) for f in glob.glob(os.path.join(GOLDEN, "boson_n*.npz")))
 
 
 def _setup(gpu, name):

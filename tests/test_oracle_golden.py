@@ -228,7 +228,7 @@ def test_disk_state_files_of_the_reference(orc, fmt):
     assert float(z["resumed_eigenvalue"]) == float(z["full_eigenvalue"])
 
 
-BOSON_FIXTURES = sorted(os.path.basename(f) for f in glob.glob(os.path.join(GOLDEN, "boson_*.npz")))
+BOSON_FIXTURES = sorted(os.path.basename(f) for f in glob.glob(os.path.join(GOLDEN, "boson_n*.npz")))
 
 
 @pytest.mark.parametrize("name", BOSON_FIXTURES)
@@ -401,3 +401,26 @@ def test_complex_translation_oracle_matches_reference(orc, name):
     x = orc.random_vector(int(z["seed_re"]), len(reps)) + 1j * orc.random_vector(int(z["seed_im"]), len(reps))
     y = orc.translation_j1j2_push_complex(L, sz, k, float(z["j1"]), float(z["j2"]), x)
     assert np.max(np.abs(y - z["y"])) <= 1e-13 * np.max(np.abs(z["y"]))
+
+
+BOSON_LARGE_FIXTURES = sorted(os.path.basename(f) for f in glob.glob(os.path.join(GOLDEN, "boson_large_*.npz")))
+
+
+@pytest.mark.parametrize("name", BOSON_LARGE_FIXTURES)
+def test_boson_large_oracle_matches_reference(orc, name):
+    # BosonOnSphereShort with lz_max + N - 1 = 42 to 62: the words bit for bit (or their SHA-256), the
+    # product within 1e-13 of max|y| of the reference's product with exact factors in its tables (its
+    # own factors deviate from the exact ones by up to 4.8e-12 at 2S = 60)
+    import hashlib
+    import re
+    z = golden(name)
+    n, s, lz = (int(v) for v in re.search(r"n(\d+)_2s(\d+)_lz(-?\d+)", name).groups())
+    B = orc.BosonFQHE(n, s, lz, z["v"])
+    if "words" in z.files:
+        assert np.array_equal(B.words, z["words"])
+    else:
+        assert hashlib.sha256(np.ascontiguousarray(B.words, np.uint64).tobytes()).hexdigest() == str(z["words_sha256"])
+    if B.dim > 13000:
+        pytest.skip("large sector: GPU product test only")
+    y = B.push(orc.random_vector(int(z["seed"]), B.dim))
+    assert np.max(np.abs(y - z["y_shift0"])) <= 1e-13 * np.max(np.abs(z["y_shift0"]))
