@@ -211,7 +211,8 @@ def run_reference_arm(args, world, rank):
     if not os.path.exists(REF_TOOL):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_tool was not built (make -C oracle ref)"}))
         return
-    budget = 150.0
+    # seconds of reference CPU work spread over the steps (DH_BENCH_REFERENCE_SECONDS, 150 by default)
+    budget = float(os.environ.get("DH_BENCH_REFERENCE_SECONDS", "150"))
     per = max(0.05, budget / float(args.steps + args.warmup))
     cb = reference_cpu_matvec(rows_target_s=per, reps=args.steps)
     line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
