@@ -56,6 +56,9 @@ SIGNATURES = {
     "dh_space_find_state_index": ([_vp, _vp, _c_i64, _vp], _c_int),
     "dh_fermion_on_sphere_long_create": ([_c_int, _c_int, _c_int, ctypes.c_ulong, _vp], _c_int),
     "dh_space_get_states_long": ([_vp, _vp, _vp, _c_i64, _c_i64], _c_int),
+    "dh_complex_vector_write": ([ctypes.c_char_p, _vp, _c_i64], _c_int),
+    "dh_complex_vector_file_dimension": ([ctypes.c_char_p, _vp], _c_int),
+    "dh_complex_vector_read": ([ctypes.c_char_p, _vp, _c_i64], _c_int),
     "dh_space_find_state_index_long": ([_vp, _vp, _c_i64, _vp], _c_int),
     "dh_space_set_index_mode": ([_vp, _c_int], _c_int),
     "dh_fermion_on_sphere_partial_entanglement_matrix": ([_vp, _vp, _c_int, _c_int, _c_int, _vp, _c_i64, _i64p, _i64p],
@@ -719,9 +722,14 @@ def fqhe_sectors_block_lanczos(nbr_fermions, lz_max, total_lz, pseudopotentials,
 
 
 def WriteVector(vec, file_name):
-    """RealVector::WriteVector: vec (numpy or torch CUDA, FP64) into file_name."""
-    b = _Buf(vec)
+    """RealVector::WriteVector: vec (numpy or torch CUDA, FP64) into file_name; a complex numpy vector is
+    written as ComplexVector::WriteVector writes it."""
     load()
+    if isinstance(vec, np.ndarray) and np.iscomplexobj(vec):
+        pairs = np.ascontiguousarray(vec, np.complex128).view(np.float64)
+        _check(_lib.dh_complex_vector_write(os.fsencode(file_name), pairs.ctypes.data, vec.size))
+        return
+    b = _Buf(vec)
     _check(_lib.dh_vector_write(os.fsencode(file_name), b.ptr, b.n))
 
 
@@ -730,6 +738,16 @@ def vector_file_dimension(file_name):
     d = ctypes.c_int64(0)
     _check(_lib.dh_vector_file_dimension(os.fsencode(file_name), ctypes.byref(d)))
     return d.value
+
+
+def ReadComplexVector(file_name):
+    """ComplexVector::ReadVector: the complex vector stored in file_name (numpy complex128)."""
+    load()
+    d = ctypes.c_int64(0)
+    _check(_lib.dh_complex_vector_file_dimension(os.fsencode(file_name), ctypes.byref(d)))
+    out = np.zeros(d.value, np.complex128)
+    _check(_lib.dh_complex_vector_read(os.fsencode(file_name), out.view(np.float64).ctypes.data, d.value))
+    return out
 
 
 def ReadVector(file_name, out=None):

@@ -724,6 +724,10 @@ int dh_lanczos_set_disk_storage(dh_lanczos_t l, const char* directory, int inter
   DH_CHECK(l, DH_ERR_ARGUMENT, "null lanczos");
   DH_CHECK(!l->blk && (l->algorithm == DH_LANCZOS_BASIC || l->algorithm == DH_LANCZOS_WITH_GROUND_STATE),
            DH_ERR_UNSUPPORTED, "disk storage is implemented for the basic and with-ground-state algorithms");
+  // the files are the real classes' formats; the complex classes (ComplexBasicLanczosAlgorithmWith-
+  // DiskStorage) keep complex vectors, which these files would not be
+  DH_CHECK(!l->h->complex_phases, DH_ERR_UNSUPPORTED,
+           "disk storage of the complex Lanczos classes is not implemented (real formats only)");
   int rc = l->writer.wait();
   if (rc != DH_OK) return rc;
   if (!directory) {

@@ -12,9 +12,9 @@ namespace dh {
 std::string join_path(const std::string& directory, const char* name);
 
 // RealVector::WriteVector / ReadVector (src/Vector/RealVector.cc:3669, :3798), host arrays
-int vector_file_write(const std::string& path, const double* v, int64_t dim);
-int vector_file_read(const std::string& path, double* v, int64_t dim);
-int vector_file_dimension(const std::string& path, int64_t* dim);
+int vector_file_write(const std::string& path, const double* v, int64_t dim, int per = 1);
+int vector_file_read(const std::string& path, double* v, int64_t dim, int per = 1);
+int vector_file_dimension(const std::string& path, int64_t* dim, int per = 1);
 
 // The fields of lanczos.dat.  algorithm DH_LANCZOS_BASIC: BasicLanczosAlgorithmWithDiskStorage
 // (Index, PreviousLastWantedEigenvalue, EigenvaluePrecision, NbrRow, the three vector file names,

@@ -77,7 +77,7 @@ std::string join_path(const std::string& directory, const char* name) {
   return directory + "/" + name;
 }
 
-int vector_file_write(const std::string& path, const double* v, int64_t dim) {
+int vector_file_write(const std::string& path, const double* v, int64_t dim, int per) {
   DH_CHECK(dim >= 0, DH_ERR_ARGUMENT, "negative vector dimension");
   const std::string tmp = path + ".tmp";
   File out;
@@ -92,7 +92,7 @@ int vector_file_write(const std::string& path, const double* v, int64_t dim) {
     const int32_t flag = -1;
     ok = put(out.f, &flag, 4) && put(out.f, &dim, 8);
   }
-  ok = ok && put(out.f, v, (size_t)dim * sizeof(double));
+  ok = ok && put(out.f, v, (size_t)dim * per * sizeof(double));
   if (!ok) {
     fclose(out.f);
     out.f = nullptr;
@@ -103,7 +103,7 @@ int vector_file_write(const std::string& path, const double* v, int64_t dim) {
 }
 
 // header of a vector file: dimension and offset of the first component; checks the file length
-static int vector_file_header(FILE* f, const std::string& path, int64_t* dim, long long* offset) {
+static int vector_file_header(FILE* f, const std::string& path, int64_t* dim, long long* offset, int per) {
   const long long size = file_size(f);
   if (size < 4) return io_fail(path, "not a vector file (too short):");
   int32_t d32 = 0;
@@ -122,34 +122,35 @@ static int vector_file_header(FILE* f, const std::string& path, int64_t* dim, lo
     off = 12;
     DH_CHECK(d >= 0, DH_ERR_IO, "%s: negative vector dimension %lld", path.c_str(), (long long)d);
   }
-  DH_CHECK(size == off + d * (long long)sizeof(double), DH_ERR_IO,
-           "%s: %lld bytes do not hold a vector of dimension %lld", path.c_str(), size, (long long)d);
+  DH_CHECK(size == off + d * per * (long long)sizeof(double), DH_ERR_IO,
+           "%s: %lld bytes do not hold a %s vector of dimension %lld", path.c_str(), size,
+           per == 2 ? "complex" : "real", (long long)d);
   *dim = d;
   *offset = off;
   return DH_OK;
 }
 
-int vector_file_dimension(const std::string& path, int64_t* dim) {
+int vector_file_dimension(const std::string& path, int64_t* dim, int per) {
   File in;
   errno = 0;
   in.f = fopen(path.c_str(), "rb");
   if (!in.f) return io_fail(path, "cannot open");
   long long off = 0;
-  return vector_file_header(in.f, path, dim, &off);
+  return vector_file_header(in.f, path, dim, &off, per);
 }
 
-int vector_file_read(const std::string& path, double* v, int64_t dim) {
+int vector_file_read(const std::string& path, double* v, int64_t dim, int per) {
   File in;
   errno = 0;
   in.f = fopen(path.c_str(), "rb");
   if (!in.f) return io_fail(path, "cannot open");
   int64_t d = 0;
   long long off = 0;
-  int rc = vector_file_header(in.f, path, &d, &off);
+  int rc = vector_file_header(in.f, path, &d, &off, per);
   if (rc != DH_OK) return rc;
   DH_CHECK(d == dim, DH_ERR_IO, "%s holds a vector of dimension %lld, expected %lld", path.c_str(), (long long)d,
            (long long)dim);
-  if (fseeko(in.f, off, SEEK_SET) != 0 || !get(in.f, v, (size_t)dim * sizeof(double)))
+  if (fseeko(in.f, off, SEEK_SET) != 0 || !get(in.f, v, (size_t)dim * per * sizeof(double)))
     return io_fail(path, "cannot read");
   return DH_OK;
 }
@@ -238,31 +239,53 @@ int lanczos_state_read(const std::string& path, int algorithm, LanczosDiskState*
 
 extern "C" {
 
-int dh_vector_write(const char* file_name, const double* vec, int64_t dim) {
+// RealVector (per = 1) and ComplexVector (per = 2: (Re, Im) pairs) files share the header
+static int write_common(const char* file_name, const double* vec, int64_t dim, int per) {
   DH_CHECK(file_name && (vec || dim == 0), DH_ERR_ARGUMENT, "null argument");
   if (dim > 0 && dh::is_device_pointer(vec)) {
-    std::vector<double> host((size_t)dim);
-    DH_CUDA(cudaMemcpy(host.data(), vec, (size_t)dim * sizeof(double), cudaMemcpyDeviceToHost));
-    return dh::vector_file_write(file_name, host.data(), dim);
+    std::vector<double> host((size_t)dim * per);
+    DH_CUDA(cudaMemcpy(host.data(), vec, (size_t)dim * per * sizeof(double), cudaMemcpyDeviceToHost));
+    return dh::vector_file_write(file_name, host.data(), dim, per);
   }
-  return dh::vector_file_write(file_name, vec, dim);
+  return dh::vector_file_write(file_name, vec, dim, per);
+}
+
+static int read_common(const char* file_name, double* vec, int64_t dim, int per) {
+  DH_CHECK(file_name && (vec || dim == 0) && dim >= 0, DH_ERR_ARGUMENT, "bad argument");
+  if (dim > 0 && dh::is_device_pointer(vec)) {
+    std::vector<double> host((size_t)dim * per);
+    int rc = dh::vector_file_read(file_name, host.data(), dim, per);
+    if (rc != DH_OK) return rc;
+    DH_CUDA(cudaMemcpy(vec, host.data(), (size_t)dim * per * sizeof(double), cudaMemcpyHostToDevice));
+    return DH_OK;
+  }
+  return dh::vector_file_read(file_name, vec, dim, per);
+}
+
+int dh_vector_write(const char* file_name, const double* vec, int64_t dim) {
+  return write_common(file_name, vec, dim, 1);
 }
 
 int dh_vector_file_dimension(const char* file_name, int64_t* dim) {
   DH_CHECK(file_name && dim, DH_ERR_ARGUMENT, "null argument");
-  return dh::vector_file_dimension(file_name, dim);
+  return dh::vector_file_dimension(file_name, dim, 1);
 }
 
 int dh_vector_read(const char* file_name, double* vec, int64_t dim) {
-  DH_CHECK(file_name && (vec || dim == 0) && dim >= 0, DH_ERR_ARGUMENT, "bad argument");
-  if (dim > 0 && dh::is_device_pointer(vec)) {
-    std::vector<double> host((size_t)dim);
-    int rc = dh::vector_file_read(file_name, host.data(), dim);
-    if (rc != DH_OK) return rc;
-    DH_CUDA(cudaMemcpy(vec, host.data(), (size_t)dim * sizeof(double), cudaMemcpyHostToDevice));
-    return DH_OK;
-  }
-  return dh::vector_file_read(file_name, vec, dim);
+  return read_common(file_name, vec, dim, 1);
+}
+
+int dh_complex_vector_write(const char* file_name, const double* pairs, int64_t dim) {
+  return write_common(file_name, pairs, dim, 2);
+}
+
+int dh_complex_vector_file_dimension(const char* file_name, int64_t* dim) {
+  DH_CHECK(file_name && dim, DH_ERR_ARGUMENT, "null argument");
+  return dh::vector_file_dimension(file_name, dim, 2);
+}
+
+int dh_complex_vector_read(const char* file_name, double* pairs, int64_t dim) {
+  return read_common(file_name, pairs, dim, 2);
 }
 
 }  // extern "C"

@@ -443,6 +443,18 @@ int dh_vector_file_dimension(const char* file_name, int64_t* dim);
  * the stored dimension must be dim and the file length must match it exactly (DH_ERR_IO otherwise). */
 int dh_vector_read(const char* file_name, double* vec, int64_t dim);
 
+/* ComplexVector::WriteVector (src/Vector/ComplexVector.cc:2606): the same header with the number of
+ * complex components dim, then dim (Re, Im) pairs of little-endian doubles; pairs holds 2 dim doubles
+ * (host or device), the storage of a complex vector of the complex momentum-sector Hamiltonian. */
+int dh_complex_vector_write(const char* file_name, const double* pairs, int64_t dim);
+
+/* The number of complex components of the vector stored in file_name. */
+int dh_complex_vector_file_dimension(const char* file_name, int64_t* dim);
+
+/* ComplexVector::ReadVector (src/Vector/ComplexVector.cc:2722) into pairs (host or device, 2 dim doubles);
+ * the stored dimension and the file length must match dim (DH_ERR_IO otherwise). */
+int dh_complex_vector_read(const char* file_name, double* pairs, int64_t dim);
+
 /* ================================================================ batched sectors */
 
 /* All requested Lz sectors of N fermions in 2S+1 orbitals with one two-body interaction, solved by

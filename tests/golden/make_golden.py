@@ -602,6 +602,10 @@ def translation_complex_fixtures(tmp):
                          eigenvalues=np.linalg.eigvalsh(0.5 * (m + m.conj().T))[:4])
         save("translations_complex_L%d_sz%d_k%d_j2_%g.npz" % (L, sz, k, j2), cmd, seed_re=0, seed_im=1, j1=j1,
              j2=j2, words=words, y=read_complex_vector(yf), **extra)
+        if (L, sz, k) == (8, 0, 1):
+            # a file written by ComplexVector::WriteVector itself, for the vector-file tests
+            import shutil
+            shutil.copyfile(yf, os.path.join(HERE, "complexvector_translations_L8_sz0_k1.vec"))
 
 
 def dir_files(d):

@@ -7,7 +7,7 @@ import re
 import numpy as np
 import pytest
 
-from conftest import ROOT, golden
+from conftest import GOLDEN, ROOT, golden
 
 HEADER = os.path.join(ROOT, "include", "diagham_b200.h")
 
@@ -108,3 +108,22 @@ def test_vector_file_forms_and_errors(dh, tmp_path):
 def test_eigenstate_file_name(dh):
     # FQHE/docs/DataFormat/FermionOnSphere.xml:9-16; QHEOnSphereMainTask.cc:891
     assert dh.eigenstate_file_name("fermions", "coulomb", 8, 21, 0, 0) == "fermions_coulomb_n_8_2s_21_lz_0.0.vec"
+
+
+def test_complex_vector_files_match_the_reference(dh, tmp_path):
+    # a file written by the reference's ComplexVector::WriteVector (its product in the L = 8, K = 1
+    # momentum sector): read back exactly, and written again byte for byte
+    ref_file = os.path.join(GOLDEN, "complexvector_translations_L8_sz0_k1.vec")
+    y = golden("translations_complex_L8_sz0_k1_j2_0.5.npz")["y"]
+    z = dh.ReadComplexVector(ref_file)
+    assert z.dtype == np.complex128 and np.array_equal(z, y)
+    out = str(tmp_path / "again.vec")
+    dh.WriteVector(z, out)
+    assert open(out, "rb").read() == open(ref_file, "rb").read()
+    # a complex file is not a real vector of the same length, nor the other way round
+    with pytest.raises(dh.DiagHamError, match="error -7"):
+        dh.ReadVector(ref_file)
+    real = str(tmp_path / "real.vec")
+    dh.WriteVector(np.arange(5.0), real)
+    with pytest.raises(dh.DiagHamError, match="error -7"):
+        dh.ReadComplexVector(real)

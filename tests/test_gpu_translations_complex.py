@@ -121,9 +121,11 @@ def test_all_momenta_hold_the_chain_spectrum_bottom(gpu, L, j2):
     assert abs(min(e) - e_chain) <= 1e-10 * abs(e_chain)
 
 
-def test_complex_refusals(gpu):
+def test_complex_refusals(gpu, tmp_path):
     sp = gpu.Spin1_2ChainWithTranslations(12, 1, 0)
     H = gpu.SpinChainJ1J2HamiltonianWithTranslations(sp, 12, 1.0, 0.5)
+    with pytest.raises(gpu.DiagHamError, match="error -4"):
+        gpu.BasicLanczosAlgorithmWithDiskStorage(H, 1, 100, directory=str(tmp_path))
     with pytest.raises(gpu.DiagHamError, match="error -4"):
         H.block_multiply(np.ones((H.dim, 2)))
     with pytest.raises(gpu.DiagHamError, match="error -4"):
