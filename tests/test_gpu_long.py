@@ -262,3 +262,26 @@ def test_long_empty_and_oversized_sectors(gpu):
         gpu.FermionOnSphereLong(3, 1, 100)
     f = gpu.FermionOnSphere(63, 0, 62)  # the filled 64-bit shell through FermionOnSphere
     assert f.dim == 1 and int(f.states()[0][0]) == (1 << 63) - 1
+
+
+def test_many_fermion_sectors_walk_both_sides(gpu, orc):
+    # more than 20 fermions: no per-row prefix sums, the rank correction walks row and target;
+    # near-full shells (3 and 2 holes) keep the sectors small
+    v = orc.coulomb_pseudopotentials(62)
+    v[0::2] = 0.0
+    f = gpu.FermionOnSphere(59, 0, 62)
+    O = orc.FQHE(59, 62, 0, v, shift=0.2)
+    assert np.array_equal(f.states()[0], O.words)
+    H = gpu.ParticleOnSphereGenericHamiltonian(f, 59, 62, v)
+    H.ShiftHamiltonian(0.2)
+    x = orc.random_vector(3, f.dim)
+    ref = O.push(x)
+    assert np.max(np.abs(H.LowLevelMultiply(x) - ref)) <= 1e-13 * np.max(np.abs(ref))
+    v41 = orc.coulomb_pseudopotentials(41)
+    v41[0::2] = 0.0
+    sp = gpu.FermionOnSphereLong(40, 2, 41)
+    assert sp.word_values(sp.states()[0]) == orc.fermion_basis_long(40, 41, 2)
+    Hl = gpu.ParticleOnSphereGenericHamiltonian(sp, 40, 41, v41)
+    xl = orc.random_vector(4, sp.dim)
+    ref = orc.FQHELong(40, 41, 2, v41).push(xl)
+    assert np.max(np.abs(Hl.LowLevelMultiply(xl) - ref)) <= 1e-13 * np.max(np.abs(ref))
