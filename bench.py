@@ -341,6 +341,7 @@ def time_to_e0_all_sectors(dh, k=2, runs=3, precisions=(1e-10, 1e-13)):
                                                                     full_diag_limit=200), nr)
             res["batched_%s" % ("fp32_refined" if fp32 else "fp64")] = {
                 "seconds": t, "energies": r["energies"], "block_products": r["block_products"],
+                "setup_seconds": r["setup_seconds"], "solve_seconds": r["solve_seconds"],
                 "product_seconds": r["product_seconds"], "fp32_seconds": r["fp32_seconds"],
                 "refine_seconds": r["refine_seconds"], "refined_sectors": r["refined_sectors"],
                 "speedup_vs_plain_fp64": tp / t}

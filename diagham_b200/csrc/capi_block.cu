@@ -89,6 +89,7 @@ struct BlockEngine {
   DevBuf start_block;    // the orthonormal start block, for replays and the projection
   DevBuf store;          // every block when keep_blocks (store_cap blocks of total * k)
   int store_cap = 0;
+  int store_max = 0;     // the store grows (doubling) up to this many blocks while memory allows
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   ~BlockEngine() {
     if (ev0) cudaEventDestroy(ev0);
@@ -274,6 +275,34 @@ int engine_product(BlockEngine& e, const double* x, double* y, int step = -1) {
 }
 
 // orthonormalise the start block (slot 0) and prepare its FP32 copy
+
+// the block store doubles (up to store_max blocks) when the next block would not fit; when the new
+// size does not fit in half of the free memory, storing stops there and the Ritz vectors are rebuilt
+// by replaying the recurrence instead
+constexpr int kStoreBlocks = 32;  // blocks stored before the first growth
+
+void store_grow(BlockEngine& e) {
+  const int cap = std::min(e.store_max, std::max(2 * e.store_cap, e.store_cap + 1));
+  const size_t block = (size_t)e.total * e.k * sizeof(double);
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  DevBuf bigger;
+  if ((size_t)cap * block >= free_b / 2 || bigger.alloc((size_t)cap * block) != DH_OK) {
+    cudaGetLastError();
+    e.store_max = e.store_cap;
+    return;
+  }
+  if (cudaMemcpyAsync(bigger.ptr, e.store.ptr, (size_t)e.store_cap * block, cudaMemcpyDeviceToDevice, e.stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(e.stream) != cudaSuccess) {
+    cudaGetLastError();
+    e.store_max = e.store_cap;
+    return;
+  }
+  std::swap(e.store.ptr, bigger.ptr);
+  std::swap(e.store.bytes, bigger.bytes);
+  e.store_cap = cap;
+}
 int engine_start(BlockEngine& e) {
   std::vector<double> B;
   e.slot_cur = 0;
@@ -401,6 +430,7 @@ int engine_step(BlockEngine& e) {
   if ((rc = engine_qr(e, W, B, e.x32.as<float>(), &scale, &rec.inv1, &rec.inv2)) != DH_OK) return rc;
   e.history.push_back(std::move(rec));
   const int nb = (int)e.history.size();  // W now holds block nb
+  if (nb >= e.store_cap && e.store_cap > 0 && e.store_cap < e.store_max) store_grow(e);
   if (nb < e.store_cap)
     DH_CUDA(cudaMemcpyAsync(e.store.as<double>() + (size_t)nb * e.total * e.k, W, (size_t)e.total * e.k * sizeof(double),
                             cudaMemcpyDeviceToDevice, e.stream));
@@ -747,13 +777,18 @@ int bl_allocate_store(BlockLanczos* b) {
   e.store.release();
   e.store_cap = 0;
   if (!b->keep) return DH_OK;
-  const int cap = b->max_iter / b->k + 3;
+  const int cap_max = b->max_iter / b->k + 3;
+  const int cap = std::min(cap_max, kStoreBlocks);
   const size_t bytes = (size_t)cap * e.total * e.k * sizeof(double);
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
   if (bytes < free_b / 2) {
-    if (e.store.alloc(bytes) == DH_OK) e.store_cap = cap;
-    else cudaGetLastError();
+    if (e.store.alloc(bytes) == DH_OK) {
+      e.store_cap = cap;
+      e.store_max = cap_max;
+    } else {
+      cudaGetLastError();
+    }
   }
   return DH_OK;
 }
@@ -1042,14 +1077,21 @@ int bind_sector_product(SectorBatchHost& hb, const std::vector<int>& sectors, Bl
 }
 
 // keep every block on the device when the store fits in half of the free memory
+// the first kStoreBlocks blocks (or all of max_iter / k + 3, when fewer) in half of the free memory;
+// the store then grows with the run
 void engine_store_if_fits(BlockEngine& e) {
-  const int cap = e.max_iter / e.k + 3;
+  const int cap_max = e.max_iter / e.k + 3;
+  const int cap = std::min(cap_max, kStoreBlocks);
   const size_t bytes = (size_t)cap * e.total * e.k * sizeof(double);
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
   if (bytes < free_b / 2) {
-    if (e.store.alloc(bytes) == DH_OK) e.store_cap = cap;
-    else cudaGetLastError();
+    if (e.store.alloc(bytes) == DH_OK) {
+      e.store_cap = cap;
+      e.store_max = cap_max;
+    } else {
+      cudaGetLastError();
+    }
   }
 }
 
