@@ -472,7 +472,10 @@ int dh_complex_vector_read(const char* file_name, double* pairs, int64_t dim);
  * energies[s] = lowest eigenvalue of sector s, iterations[s] = the driver's counter (both phases;
  * 0 for dense sectors); stats (optional, DH_SECTOR_STATS values): set-up seconds, solve seconds,
  * device time of the block products, number of block products, FP32-phase seconds, refinement
- * seconds, number of sectors restarted in FP64, largest |E_refined - E_FP32| over the sectors. */
+ * seconds, number of sectors restarted in FP64, largest |E_refined - E_FP32| over the sectors.
+ * The sectors share the split-word rank tables: lz_max <= 40 (DH_ERR_UNSUPPORTED above).  The
+ * Krylov blocks the refinement needs are kept in device memory as far as half of the free memory
+ * allows (growing with the run), else rebuilt by replaying the recurrence. */
 #define DH_SECTOR_STATS 8
 int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const int* total_lz, int nbr_sectors,
                                   const double* pseudopotentials, int block_size, int max_iter,
