@@ -241,3 +241,37 @@ def test_disk_storage_errors(gpu, orc, tmp_path):
         bad.InitializeLanczosAlgorithm(orc.random_vector(2, H.dim))
         bad.RunLanczosAlgorithm(3)
         bad.WriteState()
+
+
+@pytest.mark.parametrize("space", ["fermions_2s70", "bosons_2s45"])
+def test_disk_storage_on_the_wider_spaces(gpu, orc, tmp_path, space):
+    # checkpoint/resume is the same on the 128-bit fermion engine (FermionOnSphereLong N=4 2S=70) and on
+    # bosons beyond 41-bit words (BosonOnSphereShort N=4 2S=45): an interrupted ground-state run resumed
+    # from its files ends where the uninterrupted run does
+    if space == "fermions_2s70":
+        v = orc.coulomb_pseudopotentials(70)
+        v[0::2] = 0.0
+        sp = gpu.FermionOnSphereLong(4, 0, 70)
+        H = gpu.ParticleOnSphereGenericHamiltonian(sp, 4, 70, v)
+    else:
+        v = orc.coulomb_pseudopotentials(45)
+        v[1::2] = 0.0
+        sp = gpu.BosonOnSphereShort(4, 2, 45)
+        H = gpu.ParticleOnSphereGenericHamiltonian(sp, 4, 45, v)
+    x0 = orc.random_vector(7, H.dim)
+    a = gpu.BasicLanczosAlgorithmWithGroundState(H, 1, 600)
+    a.InitializeLanczosAlgorithm(x0)
+    ra = a.solve(max_iter=600)
+    psi_a = a.GetGroundState()
+    b = _lanczos(gpu, "ground", H, tmp_path, interval=4, max_iter=600)
+    b.InitializeLanczosAlgorithm(x0)
+    rb = b.solve(max_iter=21)
+    assert not rb["converged"]
+    del b
+    c = _lanczos(gpu, "ground", H, tmp_path, max_iter=600)
+    c.ResumeLanczosAlgorithm()
+    rc = c.solve(max_iter=600)
+    assert rc["converged"] and rb["iterations"] + rc["iterations"] == ra["iterations"]
+    e = ra["eigenvalues"][0]
+    assert abs(rc["eigenvalues"][0] - e) <= 1e-13 * abs(e)
+    assert _overlap_error(c.GetGroundState(), psi_a) < 1e-10
