@@ -184,7 +184,9 @@ __device__ __forceinline__ void load_row(const TG* x, const MatvecArgs& a, int i
   if constexpr (IL) {
     const TG* p = x + (long long)idx * K;
     if constexpr (sizeof(TG) == 4 && K == 4) {
-      const float4 q = __ldg(reinterpret_cast<const float4*>(p));
+      // the FP32 block of 4 (124 MB at N=12, 2S=33) lives in L2: its gathers skip L1, which keeps L1
+      // for the rank tables (9.60-9.65 ms per step against 9.68-9.75 ms with cached gathers)
+      const float4 q = __ldcg(reinterpret_cast<const float4*>(p));
       v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
     } else if constexpr (sizeof(TG) == 4 && K == 2) {
       const float2 q = __ldg(reinterpret_cast<const float2*>(p));
