@@ -25,12 +25,14 @@ namespace {
 
 constexpr int kCutThreads = 256;
 
-__global__ void cut_split_kernel(const uint64_t* words, long long dim, const double* psi, int l, int na, int sum_a,
-                                 uint64_t* aw, uint64_t* bw, double* val, unsigned long long* count) {
+// words of state i at words[i * wstride]: wstride 2 for the (low, high) pairs of the 128-bit engine,
+// whose high halves are zero up to lz_max = 62
+__global__ void cut_split_kernel(const uint64_t* words, int wstride, long long dim, const double* psi, int l, int na,
+                                 int sum_a, uint64_t* aw, uint64_t* bw, double* val, unsigned long long* count) {
   const uint64_t amask = (l >= 64) ? ~0ull : ((1ull << l) - 1ull);
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < dim; i += stride) {
-    const uint64_t w = words[i];
+    const uint64_t w = words[i * wstride];
     const uint64_t a = w & amask;
     if (__popcll(a) != na) continue;
     int s = 0;
@@ -44,13 +46,13 @@ __global__ void cut_split_kernel(const uint64_t* words, long long dim, const dou
 }
 
 // sum of psi^2 over the states whose A part (low l bits) is key
-__global__ void cut_weight_kernel(const uint64_t* words, long long dim, const double* psi, int l, uint64_t key,
-                                  double* total) {
+__global__ void cut_weight_kernel(const uint64_t* words, int wstride, long long dim, const double* psi, int l,
+                                  uint64_t key, double* total) {
   const uint64_t amask = (l >= 64) ? ~0ull : ((1ull << l) - 1ull);
   double acc = 0.0;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < dim; i += stride)
-    if ((words[i] & amask) == key) acc += psi[i] * psi[i];
+    if ((words[i * wstride] & amask) == key) acc += psi[i] * psi[i];
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
   if ((threadIdx.x & 31) == 0 && acc != 0.0) atomicAdd(total, acc);
 }
@@ -151,7 +153,8 @@ int cut_matrix(dh_space_s* sp, const double* state_dev, int l, int na, int lza, 
       (rc = val.alloc(dim * sizeof(double))) != DH_OK || (rc = cnt.alloc(sizeof(unsigned long long))) != DH_OK)
     return rc;
   DH_CUDA(cudaMemset(cnt.ptr, 0, sizeof(unsigned long long)));
-  cut_split_kernel<<<grid_of(dim), kCutThreads>>>(sp->words.as<uint64_t>(), dim, state_dev, l, na, sum_a,
+  cut_split_kernel<<<grid_of(dim), kCutThreads>>>(sp->words.as<uint64_t>(), sp->kind == SPACE_FERMION_LONG ? 2 : 1,
+                                                 dim, state_dev, l, na, sum_a,
                                                  aw.as<uint64_t>(), bw.as<uint64_t>(), val.as<double>(),
                                                  cnt.as<unsigned long long>());
   DH_CUDA(cudaGetLastError());
@@ -161,14 +164,13 @@ int cut_matrix(dh_space_s* sp, const double* state_dev, int l, int na, int lza, 
   *nonzero = true;
   if (na > 0) {
     if ((rc = ia.alloc(n * sizeof(long long))) != DH_OK) return rc;
-    if ((rc = launch_fqhe_find(fqhe_device(a_space.s, nullptr, 0), aw.as<uint64_t>(), (long long)n, ia.as<long long>(),
-                               0)) != DH_OK)
+    // the subsystem spaces may be of either engine: the C entry point picks the right search
+    if ((rc = dh_space_find_state_index(a_space.s, aw.as<uint64_t>(), (int64_t)n, ia.as<int64_t>())) != DH_OK)
       return rc;
   }
   if (nb > 0) {
     if ((rc = ib.alloc(n * sizeof(long long))) != DH_OK) return rc;
-    if ((rc = launch_fqhe_find(fqhe_device(b_space.s, nullptr, 0), bw.as<uint64_t>(), (long long)n, ib.as<long long>(),
-                               0)) != DH_OK)
+    if ((rc = dh_space_find_state_index(b_space.s, bw.as<uint64_t>(), (int64_t)n, ib.as<int64_t>())) != DH_OK)
       return rc;
   }
   cut_scatter_kernel<<<grid_of((long long)n), kCutThreads>>>(na > 0 ? ia.as<long long>() : nullptr,
@@ -189,7 +191,8 @@ int copy_out(double* out, const double* dev, int64_t n) {
 int entanglement_common(dh_space_t sp, const double* state, int l, int na, int lza, bool density, double* out,
                         int64_t capacity, int64_t* rows, int64_t* cols) {
   DH_CHECK(sp && state && rows && cols, DH_ERR_ARGUMENT, "null argument");
-  DH_CHECK(sp->kind == SPACE_FERMION, DH_ERR_UNSUPPORTED, "orbital cuts are implemented for FermionOnSphere");
+  DH_CHECK(sp->kind == SPACE_FERMION || (sp->kind == SPACE_FERMION_LONG && sp->lz_max <= 62), DH_ERR_UNSUPPORTED,
+           "orbital cuts are implemented for FermionOnSphere (lz_max <= 62)");
   *rows = *cols = 0;
   const int64_t dim = sp->dim;
   int rc;
@@ -241,7 +244,8 @@ int entanglement_common(dh_space_t sp, const double* state, int l, int na, int l
     if ((rc = t.alloc(sizeof(double))) != DH_OK) return rc;
     DH_CUDA(cudaMemset(t.ptr, 0, sizeof(double)));
     if (key != ~0ull) {
-      cut_weight_kernel<<<grid_of(dim), kCutThreads>>>(sp->words.as<uint64_t>(), dim, psi, l, key, t.as<double>());
+      cut_weight_kernel<<<grid_of(dim), kCutThreads>>>(sp->words.as<uint64_t>(), sp->kind == SPACE_FERMION_LONG ? 2 : 1,
+                                                      dim, psi, l, key, t.as<double>());
       DH_CUDA(cudaGetLastError());
     }
     *rows = *cols = 1;

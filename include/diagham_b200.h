@@ -140,7 +140,8 @@ int dh_space_set_index_mode(dh_space_t space, int mode);
  * 2S - subsystem_size).  *rows x *cols (0 x 0 for an empty sector); the matrix is written row-major
  * into matrix (host or device) when it is not NULL and capacity >= rows * cols, so a first call with
  * matrix = NULL gives the size.  subsystem_size <= 0 and > 2S follow the reference (1 x 1 [1]; the state
- * as one column). */
+ * as one column).  Any FermionOnSphere space (2S <= 62, either word engine); FermionOnSphereLong spaces
+ * answer DH_ERR_UNSUPPORTED. */
 int dh_fermion_on_sphere_partial_entanglement_matrix(dh_space_t space, const double* state, int subsystem_size,
                                                      int nbr_fermion_sector, int lz_sector, double* matrix,
                                                      int64_t capacity, int64_t* rows, int64_t* cols);

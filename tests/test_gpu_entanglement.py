@@ -64,3 +64,27 @@ def test_larger_sector_and_normalisation(gpu, orc):
     npart = np.array([bin(int(w)).count("1") for w in a])
     low = float(np.sum(x[npart < 2] ** 2))
     assert abs(total + low - float(x @ x)) <= 1e-12
+
+
+@pytest.mark.parametrize("n,s,lz,cuts", [(4, 50, 0, [(25, 2, 2), (45, 3, 1), (5, 1, 0), (12, 1, 3)]),
+                                          (5, 41, 1, [(20, 2, 1), (35, 4, 2), (6, 2, -1)])])
+def test_cuts_beyond_the_split_tables(gpu, orc, n, s, lz, cuts):
+    # FermionOnSphere above 2S = 40 (the 128-bit engine's words), and subsystems of more than 41
+    # orbitals on either side of the cut, against the oracle
+    sp = gpu.FermionOnSphere(n, lz, s)
+    x = orc.random_vector(3, sp.dim)
+    for l, na, lza in cuts:
+        ref = orc.entanglement_matrix(n, s, lz, x, l, na, lza)
+        m = sp.EvaluatePartialEntanglementMatrix(l, na, lza, x)
+        assert m.shape == ref.shape and (m.size == 0 or np.max(np.abs(m - ref)) <= 1e-15), (l, na, lza)
+        rho = sp.EvaluatePartialDensityMatrix(l, na, lza, x)
+        if na > 1 and ref.size:
+            assert np.max(np.abs(rho - ref @ ref.T)) <= 1e-14, (l, na, lza)
+    # sum over the sectors of a cut of tr(rho_A) = |x|^2
+    l = 25
+    total = 0.0
+    for na in range(0, n + 1):
+        for lza in range(-na * (l - 1), na * (l - 1) + 1, 2):
+            rho = sp.EvaluatePartialDensityMatrix(l, na, lza, x)
+            total += float(np.trace(rho)) if rho.size else 0.0
+    assert abs(total - float(x @ x)) <= 1e-12

@@ -233,8 +233,11 @@ def test_long_refusals(gpu):
     f = gpu.FermionOnSphere(3, 0, 50)
     w, lzm = f.states()
     assert w.dtype == np.uint64 and np.all(lzm <= 50)
+    # orbital cuts work on these words too (against the oracle in test_gpu_entanglement.py)
+    assert f.EvaluatePartialDensityMatrix(20, 1, 0, np.ones(f.dim)).shape == (1, 1)
+    lng = gpu.FermionOnSphereLong(3, 0, 70)  # 128-bit words: no orbital cuts
     with pytest.raises(gpu.DiagHamError, match="error -4"):
-        f.EvaluatePartialDensityMatrix(20, 1, 0, np.ones(f.dim))
+        gpu._cut_matrix(lng, gpu.load().dh_fermion_on_sphere_partial_density_matrix, np.ones(lng.dim), (20, 1, 0), True)
 
 
 @pytest.mark.parametrize("n,s,lz", [(1, 100, 10), (64, 63, 0), (3, 100, 294), (2, 126, -250)])
