@@ -768,6 +768,58 @@ def eigenstate_file_name(statistics, interaction_name, nbr_particles, lz_max, to
     return "%s_%s_n_%d_2s_%d_lz_%d.%d.vec" % (statistics, interaction_name, nbr_particles, lz_max, total_lz, index)
 
 
+def spectrum_file_name(statistics, interaction_name, nbr_particles, lz_max, extra_terms=""):
+    """<statistics>_<interaction><extra>_n_<N>_2s_<2S>_lz.dat, the spectrum file of the sphere programs
+    (FQHESphereFermionsTwoBodyGeneric.cc:243)."""
+    return "%s_%s%s_n_%d_2s_%d_lz.dat" % (statistics, interaction_name, extra_terms, nbr_particles, lz_max)
+
+
+def back_up_file(file_name, extension=".bak"):
+    """BackUpFile (src/GeneralTools/FilenameTools.cc:381): an existing file_name is renamed to
+    file_name.bak, or file_name.bak1, .bak2, ... (the first free name); returns the counter, -1 when
+    there was nothing to back up."""
+    if not os.path.exists(file_name):
+        return -1
+    counter, target = 0, file_name + extension
+    while os.path.exists(target):
+        counter += 1
+        target = "%s%s%d" % (file_name, extension, counter)
+    os.rename(file_name, target)
+    return counter
+
+
+def _stream_double(x):
+    # a double through a C++ stream in its default format at precision 14
+    return "%.14g" % x
+
+
+class QHEOnSphereSpectrumFile:
+    """The spectrum file QHEOnSphereMainTask::ExecuteMainTask writes (QHEOnSphereMainTask.cc:361-456): the
+    first sector backs up an existing file and writes the header "# Lz E" (with " <H>" when the energies are
+    also evaluated on the eigenvectors, " <L^2> <L>" with the total angular momentum), then every
+    eigenvalue of a sector is a line "LValue/2 E" (LValue = 2 Lz, integer division as in C++; E minus
+    the energy shift; doubles at 14 significant digits), followed by <H> and <L^2> L when given."""
+
+    def __init__(self, file_name, energy_column=False, l_value_columns=False):
+        self.file_name = file_name
+        back_up_file(file_name)
+        header = "# Lz E" + (" <H>" if energy_column else "") + (" <L^2> <L>" if l_value_columns else "")
+        with open(file_name, "w") as f:
+            f.write(header + "\n")
+
+    def add(self, two_lz, energies, energy_shift=0.0, expectations=None, l2_values=None):
+        lz = int(two_lz / 2)  # truncation toward zero, as LValue / 2 on ints
+        with open(self.file_name, "a") as f:
+            for j, e in enumerate(energies):
+                line = "%d %s" % (lz, _stream_double(e - energy_shift))
+                if expectations is not None:
+                    line += " " + _stream_double(expectations[j] - energy_shift)
+                if l2_values is not None:
+                    l2 = float(l2_values[j])
+                    line += " %s %s" % (_stream_double(l2), _stream_double(0.5 * (np.sqrt(4.0 * l2 + 1.0) - 1.0)))
+                f.write(line + "\n")
+
+
 class SpinChainJ1J2HamiltonianWithTranslations(_Hamiltonian):
     """SpinChainJ1J2HamiltonianWithTranslations(chain, nbrSpin, j1, j2)
     (SpinChainJ1J2HamiltonianWithTranslations.cc:62): the complex Hamiltonian of a momentum sector, any

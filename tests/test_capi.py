@@ -127,3 +127,21 @@ def test_complex_vector_files_match_the_reference(dh, tmp_path):
     dh.WriteVector(np.arange(5.0), real)
     with pytest.raises(dh.DiagHamError, match="error -7"):
         dh.ReadComplexVector(real)
+
+
+def test_spectrum_file_in_the_reference_layout(dh, tmp_path):
+    # QHEOnSphereMainTask's spectrum file: header, "LValue/2 E" lines at 14 significant digits, LValue/2
+    # truncated toward zero, the energy shift removed, optional <H> and <L^2> <L> columns; an existing
+    # file is backed up as .bak, then .bak1
+    name = str(tmp_path / dh.spectrum_file_name("fermions", "coulomb", 8, 21))
+    assert name.endswith("fermions_coulomb_n_8_2s_21_lz.dat")
+    f = dh.QHEOnSphereSpectrumFile(name)
+    f.add(0, [13.914890702090714, -0.5])
+    f.add(-3, [1.25e-20], energy_shift=-1.0)
+    assert open(name).read() == "# Lz E\n0 13.914890702091\n0 -0.5\n-1 1\n"
+    g = dh.QHEOnSphereSpectrumFile(name, energy_column=True, l_value_columns=True)
+    g.add(4, [2.0], expectations=[2.0 + 1e-15], l2_values=[6.0])
+    assert open(name).read() == "# Lz E <H> <L^2> <L>\n2 2 2 6 2\n"
+    assert open(name + ".bak").read().startswith("# Lz E\n0 13.914890702091")
+    dh.QHEOnSphereSpectrumFile(name)
+    assert open(name + ".bak1").read().startswith("# Lz E <H>")
