@@ -145,3 +145,35 @@ def test_spectrum_file_in_the_reference_layout(dh, tmp_path):
     assert open(name + ".bak").read().startswith("# Lz E\n0 13.914890702091")
     dh.QHEOnSphereSpectrumFile(name)
     assert open(name + ".bak1").read().startswith("# Lz E <H>")
+
+
+@pytest.mark.parametrize("make, pattern", [
+    (lambda dh: dh.FermionOnSphere(0, 0, 8), "nbr_fermions must be >= 1"),
+    (lambda dh: dh.FermionOnSphere(10, 0, 8), "do not fit in 9 orbitals"),
+    (lambda dh: dh.FermionOnSphere(4, 0, 63), "FermionOnSphereLong takes up to 126"),
+    (lambda dh: dh.FermionOnSphereLong(4, 0, 127), r"not in 1\.\.126"),
+    (lambda dh: dh.FermionOnSphereLong(3, 1, 64), "not reachable"),
+    (lambda dh: dh.BosonOnSphereShort(0, 0, 4), "nbr_bosons must be >= 1"),
+    (lambda dh: dh.BosonOnSphereShort(10, 0, 54), "needs the reference's BosonOnSphere"),
+    (lambda dh: dh.BosonOnSphereShort(3, 1, 4), "not reachable"),
+    (lambda dh: dh.BosonOnSphereShort(2, 10, 4), "not reachable"),
+    (lambda dh: dh.Spin1_2Chain(8, 1), "not reachable with 8 spins"),
+    (lambda dh: dh.Spin1_2ChainWithTranslations(2, 0, 0), r"not in 3\.\.32"),
+    (lambda dh: dh.Spin1_2ChainWithTranslations(33, 0, 1), r"not in 3\.\.32"),
+    (lambda dh: dh.Spin1_2ChainWithTranslations(8, 8, 0), r"momentum 8 not in 0\.\.7"),
+    (lambda dh: dh.Spin1_2ChainWithTranslations(8, 0, 3), "not reachable with 8 spins"),
+])
+def test_constructor_limits_are_codes(dh, make, pattern):
+    """Every space constructor checks its sector before touching the device: the error is a status
+    code with a message, on a machine without a GPU as on one with it."""
+    with pytest.raises(dh.DiagHamError, match=pattern):
+        make(dh)
+
+
+def test_null_handles_are_codes(dh):
+    lib = dh.load()
+    d = ctypes.c_int64(-1)
+    assert lib.dh_space_get_dimension(None, ctypes.byref(d)) != 0
+    assert "null" in lib.dh_last_error().decode()
+    assert lib.dh_fermion_on_sphere_create(4, 0, 8, 0, None) != 0
+    assert "null output handle" in lib.dh_last_error().decode()
