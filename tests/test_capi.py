@@ -177,3 +177,18 @@ def test_null_handles_are_codes(dh):
     assert "null" in lib.dh_last_error().decode()
     assert lib.dh_fermion_on_sphere_create(4, 0, 8, 0, None) != 0
     assert "null output handle" in lib.dh_last_error().decode()
+
+
+def test_missing_library_fails_loudly():
+    """Without the built CUDA library the package raises on first use: there is no host fallback."""
+    import subprocess
+    import sys
+    code = ("import diagham_b200 as dh\n"
+            "dh._LIB_PATH = '/nonexistent/libdiagham_b200.so'\n"
+            "try:\n"
+            "    dh.FermionOnSphere(4, 0, 8)\n"
+            "except dh.DiagHamError as e:\n"
+            "    print('raised:', e)\n")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    assert "raised: libdiagham_b200.so is not built" in out.stdout
