@@ -108,7 +108,7 @@ int dh_spin12_chain_translations_create(int chain_length, int momentum, int sz, 
 
 int dh_space_destroy(dh_space_t space);
 
-/* AbstractHilbertSpace::GetHilbertSpaceDimension (src/HilbertSpace/AbstractHilbertSpace.h). */
+/* AbstractHilbertSpace::GetHilbertSpaceDimension (src/HilbertSpace/AbstractHilbertSpace.h:81). */
 int dh_space_get_dimension(dh_space_t space, int64_t* dim);
 
 /* StateDescription[first .. first+n) and, for fermions, StateLzMax (FermionOnSphere.h:166-168,
@@ -129,7 +129,8 @@ int dh_space_get_states_long(dh_space_t space, uint64_t* words, int* lz_max, int
  * reference) for n (low, high) word pairs; -1 for a word outside the sector.  Host or device arrays. */
 int dh_space_find_state_index_long(dh_space_t space, const uint64_t* words, int64_t n, int64_t* indices);
 
-/* Selects DH_INDEX_RANK or DH_INDEX_LOOKUP for every kernel that uses this space. */
+/* Selects DH_INDEX_RANK or DH_INDEX_LOOKUP for every kernel that uses this space.  No reference
+ * counterpart: the lookup mode is FindStateIndex's own search (FermionOnSphere.cc:1431). */
 int dh_space_set_index_mode(dh_space_t space, int mode);
 
 /* FermionOnSphere::EvaluatePartialEntanglementMatrix(subsytemSize, nbrFermionSector, lzSector, state)
@@ -210,13 +211,16 @@ int dh_hamiltonian_get_dimension(dh_hamiltonian_t h, int64_t* dim);
  * H + shift * 1 in every product. */
 int dh_hamiltonian_shift(dh_hamiltonian_t h, double shift);
 
-/* DH_PRECISION_FP64 (default) or DH_PRECISION_FP32 for every following product. */
+/* DH_PRECISION_FP64 (default) or DH_PRECISION_FP32 for every following product.  No reference
+ * counterpart: the reference's products are FP64. */
 int dh_hamiltonian_set_precision(dh_hamiltonian_t h, int precision);
 
-/* Replaces V_0..V_lzmax (rebuilds the interaction factors; FQHE Hamiltonians only). */
+/* Replaces V_0..V_lzmax and rebuilds the interaction factors as EvaluateInteractionFactors does
+ * (ParticleOnSphereGenericHamiltonian.cc:493); FQHE Hamiltonians only. */
 int dh_hamiltonian_set_pseudopotentials(dh_hamiltonian_t h, const double* pseudopotentials);
 
-/* CUDA stream (a cudaStream_t passed as void*) the handle's work is ordered on. */
+/* CUDA stream (a cudaStream_t passed as void*) the handle's work is ordered on.  No reference
+ * counterpart. */
 int dh_hamiltonian_set_stream(dh_hamiltonian_t h, void* stream);
 
 /* AbstractHamiltonian::LowLevelAddMultiply(vSource, vDestination, firstComponent, nbrComponent)
@@ -254,7 +258,8 @@ int dh_hamiltonian_block_multiply(dh_hamiltonian_t h, const double* x, double* y
  * ones only recomputes the diagonal.  FQHE Hamiltonians only; partial column ranges stay on the fly. */
 int dh_hamiltonian_enable_fast_multiplication(dh_hamiltonian_t h, int64_t allowed_memory, int* enabled,
                                               int64_t* bytes);
-/* Frees the stored elements: products go back to the on-the-fly kernels. */
+/* Frees the stored elements: products go back to the on-the-fly kernels.  No reference counterpart
+ * (the reference frees them with the Hamiltonian, AbstractQHEOnSphereHamiltonian.cc:3625 allocates). */
 int dh_hamiltonian_disable_fast_multiplication(dh_hamiltonian_t h);
 
 /* Autotuner of the product (no reference counterpart): times this Hamiltonian's product on random
@@ -289,7 +294,8 @@ int dh_hamiltonian_row_elements(dh_hamiltonian_t h, int64_t row, int* targets, i
 int dh_hamiltonian_pseudopotential_adjoint(dh_hamiltonian_t h, const double* u, const double* v, double* out);
 
 /* Number of elements (a+a+aa moves, diagonal ones included; spin flips for the chain) that one
- * product generates over all rows, counted on the GPU. */
+ * product generates over all rows, counted on the GPU: the total of the per-row counting pass of
+ * FastMultiplicationMemory (AbstractQHEOnSphereHamiltonian.cc:3625). */
 int dh_hamiltonian_count_elements(dh_hamiltonian_t h, int64_t* total);
 
 /* Of those, the elements whose target is their own row (one per annihilated pair for FQHE spaces:
@@ -339,14 +345,15 @@ int dh_lanczos_destroy(dh_lanczos_t l);
  * dh_lanczos_initialize. */
 int dh_lanczos_set_vector_storage(dh_lanczos_t l, int keep);
 
-/* SetEigenvaluePrecision (AbstractLanczosAlgorithm.h); default 1e-14 = MACHINE_PRECISION. */
+/* SetEigenvaluePrecision (AbstractLanczosAlgorithm.h:147); default 1e-14 = MACHINE_PRECISION. */
 int dh_lanczos_set_eigenvalue_precision(dh_lanczos_t l, double precision);
 
-/* InitializeLanczosAlgorithm(vector) / (vectors, nbrVectors): nbr_vectors vectors one after the
- * other (host or device).  Block algorithms orthonormalise the block; others use vectors[0]. */
+/* InitializeLanczosAlgorithm(vector) / (vectors, nbrVectors) (AbstractLanczosAlgorithm.h:83, :89): nbr_vectors
+ * vectors one after the other (host or device).  Block algorithms orthonormalise the block; others use
+ * vectors[0]. */
 int dh_lanczos_initialize(dh_lanczos_t l, const double* vectors, int nbr_vectors);
 
-/* InitializeLanczosAlgorithm() with a reproducible start: component i of vector b is the
+/* InitializeLanczosAlgorithm() (AbstractLanczosAlgorithm.h:78) with a reproducible start: component i of vector b is the
  * (i+1)-th splitmix64 output of seed + b mapped to [-1, 1), then normalised. */
 int dh_lanczos_initialize_random(dh_lanczos_t l, uint64_t seed);
 
@@ -356,7 +363,8 @@ int dh_lanczos_run(dh_lanczos_t l, int nbr_iter);
 /* TestConvergence (BasicLanczosAlgorithm.cc:220, BasicBlockLanczosAlgorithm.cc:731). */
 int dh_lanczos_test_convergence(dh_lanczos_t l, int* converged);
 
-/* Lowest n Ritz values, ascending (GetDiagonalizedMatrix + SortMatrixUpOrder). */
+/* Lowest n Ritz values, ascending: GetEigenvalues (AbstractLanczosAlgorithm.h:121), i.e. GetDiagonalizedMatrix
+ * (:137) + SortMatrixUpOrder. */
 int dh_lanczos_get_eigenvalues(dh_lanczos_t l, double* eigenvalues, int n);
 
 /* GetGroundStateEnergy (AbstractLanczosAlgorithm.cc:136-150). */
@@ -372,7 +380,8 @@ int dh_lanczos_get_ground_state(dh_lanczos_t l, double* vec);
  * need the stored Krylov vectors for n > 1. */
 int dh_lanczos_get_eigenstates(dh_lanczos_t l, int n, double* vecs);
 
-/* Number of matrix-vector products and tridiagonal rows so far. */
+/* Number of matrix-vector products and tridiagonal rows so far.  No reference counterpart (the
+ * driver loop counts its own iterations, QHEOnSphereMainTask.cc:732-753). */
 int dh_lanczos_get_counters(dh_lanczos_t l, int64_t* matvecs, int* rows);
 
 /* Whole driver loop of QHEOnSphereMainTask.cc:732-753: RunLanczosAlgorithm(nbrEigenvalue + 2), then
@@ -412,7 +421,8 @@ int dh_lanczos_solve_refined(dh_lanczos_t l, int max_iter, double precision, dou
  * run without CUDA-graph batches; dh_lanczos_solve_refined rejects it. */
 int dh_lanczos_set_disk_storage(dh_lanczos_t l, const char* directory, int interval);
 
-/* WriteState: a checkpoint of the current state now; returns once every file is written. */
+/* WriteState (BasicLanczosAlgorithmWithDiskStorage.cc:286, BasicLanczosAlgorithmWithGroundStateDiskStorage.cc:399):
+ * a checkpoint of the current state now; returns once every file is written. */
 int dh_lanczos_write_state(dh_lanczos_t l);
 
 /* ResumeLanczosAlgorithm (BasicLanczosAlgorithmWithDiskStorage.cc:161,
@@ -437,7 +447,7 @@ int dh_lanczos_resume(dh_lanczos_t l);
  * (FQHE/docs/DataFormat/FermionOnSphere.xml:9-16, QHEOnSphereMainTask.cc:891). */
 int dh_vector_write(const char* file_name, const double* vec, int64_t dim);
 
-/* The dimension of the vector stored in file_name (RealVector::ReadVector's header). */
+/* The dimension of the vector stored in file_name: RealVector::ReadVectorDimension (RealVector.cc:3914). */
 int dh_vector_file_dimension(const char* file_name, int64_t* dim);
 
 /* RealVector::ReadVector (src/Vector/RealVector.cc:3798) into vec (host or device) of dim doubles:
@@ -449,7 +459,8 @@ int dh_vector_read(const char* file_name, double* vec, int64_t dim);
  * (host or device), the storage of a complex vector of the complex momentum-sector Hamiltonian. */
 int dh_complex_vector_write(const char* file_name, const double* pairs, int64_t dim);
 
-/* The number of complex components of the vector stored in file_name. */
+/* The number of complex components of the vector stored in file_name: ComplexVector::ReadVectorDimension
+ * (ComplexVector.cc:2854). */
 int dh_complex_vector_file_dimension(const char* file_name, int64_t* dim);
 
 /* ComplexVector::ReadVector (src/Vector/ComplexVector.cc:2722) into pairs (host or device, 2 dim doubles);
