@@ -290,7 +290,9 @@ int dh_hamiltonian_row_elements(dh_hamiltonian_t h, int64_t row, int* targets, i
 
 /* Adjoint of the pseudopotentials (Hellmann-Feynman / bilinear VJP): out[m] = <u| dH/dV_m |v> for
  * m = 0..lz_max.  With u = v = normalised ground state this is dE0/dV_m; with u = upstream gradient
- * and v = x it is the V part of the vector-Jacobian product of H(V) x.  FQHE Hamiltonians only. */
+ * and v = x it is the V part of the vector-Jacobian product of H(V) x.  FQHE Hamiltonians only.  No
+ * reference counterpart; its oracle is MatrixElement (AbstractQHEOnSphereHamiltonian.cc:380) of the
+ * Hamiltonian with V = e_m. */
 int dh_hamiltonian_pseudopotential_adjoint(dh_hamiltonian_t h, const double* u, const double* v, double* out);
 
 /* Number of elements (a+a+aa moves, diagonal ones included; spin flips for the chain) that one
@@ -399,7 +401,8 @@ int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eige
  * FP64 Lanczos restarted from it polishes the energy.  out[0] = refined E0, out[1] = FP32-phase E0,
  * out[2] = residual norm, out[3] = FP32 matvecs, out[4] = FP64 matvecs.  With DH_LANCZOS_BLOCK the
  * whole block of Ritz vectors is refined and the FP64 restart is a block Lanczos from it; the
- * algorithm must be freshly initialised. */
+ * algorithm must be freshly initialised.  No reference counterpart: the reference's Lanczos runs its
+ * products in FP64 throughout (BasicLanczosAlgorithm.cc:148-216). */
 int dh_lanczos_solve_refined(dh_lanczos_t l, int max_iter, double precision, double* out);
 
 /* Disk storage of the Lanczos state, in the files of the reference's disk-storage classes, so that an

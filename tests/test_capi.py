@@ -192,3 +192,20 @@ def test_missing_library_fails_loudly():
     out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=120)
     assert out.returncode == 0, out.stderr
     assert "raised: libdiagham_b200.so is not built" in out.stdout
+
+
+def test_every_entry_cites_its_reference_interface():
+    """Each declared entry's comment gives the reference interface it replaces as file:line, or says
+    that it has no reference counterpart; only the library's own utilities are exempt."""
+    text = open(HEADER).read()
+    utilities = {"dh_last_error", "dh_version", "dh_device_count", "dh_space_destroy", "dh_hamiltonian_destroy",
+                 "dh_lanczos_destroy"}
+    uncited = []
+    for m in re.finditer(r"\b(dh_[a-z0-9_]+)\s*\(", text):
+        before = text[:m.start()]
+        if before.count("/*") > before.count("*/") or m.group(1) in utilities:
+            continue
+        comment = before[before.rfind("/*"):before.rfind("*/")]
+        if not re.search(r"\.(cc|h):\d+|[Nn]o[\s*]+(reference[\s*]+)?counterpart", comment):
+            uncited.append(m.group(1))
+    assert not uncited, uncited
