@@ -3,13 +3,15 @@
 
 Workload (the precision configuration): N = 12 spin-polarised fermions on the sphere, 2S = 33,
 total Lz = 0 (dimension 7,764,392), lowest-Landau-level Coulomb pseudopotentials V_m (odd m),
-synthetic inputs.  One step = one block product H X of 4 vectors (4 H.v) through the C ABI with the
-input already in HBM, the batched form of the block Lanczos: FP32 matrix elements and FP32 per-row
-accumulation, FP64 in and out.  L2 is flushed (a 256 MiB write) before every step.  The line also
-carries the single-vector FP64 / FP32 rates, the time to E0 of the sector (plain FP64 against FP32
-products + FP64 refinement), of all 91 sectors of N = 10, 2S = 27 (batched against sector by
-sector), the adjoint gradients of N = 10, 2S = 27 against the reference's and finite differences,
-and the L = 32 J1-J2 chain product with its roofline.
+synthetic inputs.  One step = one FP64 block product H X of 4 vectors (4 H.v, the product of
+block Lanczos: LowLevelMultipleMultiply) through the C ABI with X already in HBM; X (248 MB) is
+larger than L2 and a 256 MiB write also precedes every step.  The reference arm times the same
+product with the reference's own SMP code (MultipleVectorHamiltonianMultiplyOperation ->
+HermitianLowLevelMultipleMultiply, FP64, all host threads).  The line also carries the FP32 rates,
+the time to E0 of the sector (plain FP64 against FP32 products + FP64 refinement), of all 91
+sectors of N = 10, 2S = 27 (batched against sector by sector), of the L = 32 J1-J2 chain (block
+k = 2, FP32 + FP64 refinement), the adjoint gradients of N = 10, 2S = 27 against the reference's
+and finite differences, and secondary product legs; a compact time-to-E0 summary ends the line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -37,11 +39,21 @@ UNIT = "H·v/s"
 REF_TOOL = os.path.join(ROOT, "oracle", "_ref", "ref_tool")
 FLUSH_BYTES = 256 << 20
 BLOCK = 4  # vectors per product in the measured step (the batched form)
+KERNEL_FP64_BLOCK4 = "fqhe_split_kernel<double, 4, RANGE=0, LR_SMEM=0, IL=1>"
+# the unit that bounds the headline kernel (from its committed ncu summary)
+BINDING_UNIT_FP64_BLOCK4 = "not profiled"
 
 
-def workload_name():
-    return ("FermionOnSphere N=12 2S=33 2Lz=0 (dim 7764392), LLL Coulomb V_m odd m, on-the-fly H.v on "
-            "row-interleaved blocks of 4 vectors, FP32 elements + FP32 row accumulation, FP64 vectors")
+DIM = 7764392
+REFERENCE_WINDOWS = 2  # the reference arm alternates two half-basis row windows (two steps = one product)
+
+
+def workload_config():
+    """The config both arms print, identical: the sector, the block and the arithmetic."""
+    return {"workload": "FermionOnSphere N=12 2S=33 2Lz=0 (dim 7764392), LLL Coulomb V_m odd m, on-the-fly "
+                        "FP64 product H X of blocks of 4 vectors (block Lanczos LowLevelMultipleMultiply)",
+            "dim": DIM, "block": BLOCK, "hv_per_step": BLOCK, "arithmetic": "fp64",
+            "l2": "X is 248 MB (> 126 MB L2); the GPU arm also writes 256 MiB before every step"}
 
 
 def pseudopotentials(dh):
@@ -61,7 +73,7 @@ def peaks():
 
 def profile_traffic():
     """DRAM bytes per launch of the measured block product from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "fqhe_block4_fp32_n12_2s33.md")
+    p = os.path.join(ROOT, "profiles", "fqhe_block4_fp64_n12_2s33.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -157,28 +169,29 @@ def barrier(world):
 
 # ------------------------------------------------------------------ CPU baselines
 
-def reference_cpu_matvec(rows_target_s, reps, hermitian=1):
-    """The reference's own SMP product (oracle/_ref/ref_tool bench_fqhe) on all host threads, over
-    a bounded sample of rows sized to take about rows_target_s seconds per repetition."""
-    import tempfile
-    import diagham_b200 as dh
+def reference_cpu_block(windows, reps, skip=0):
+    """The reference's own SMP block product (oracle/_ref/ref_tool bench_fqhe_block:
+    MultipleVectorHamiltonianMultiplyOperation on SMPArchitecture -> HermitianLowLevelMultipleMultiply,
+    FP64, on the fly, all host threads, pseudopotentials from the reference's EvaluatePseudopotentials)
+    on blocks of 4 vectors.  The basis is cut into `windows` equal row windows and repetition r
+    multiplies window r mod windows; the first `skip` repetitions are not counted.  Every call pays the
+    reference's per-call SMP cost (per-thread destination copies of the whole block and their sum),
+    so a windowed product costs slightly more than a whole one."""
     threads = os.cpu_count() or 1
-    with tempfile.TemporaryDirectory() as tmp:
-        vf = os.path.join(tmp, "v.bin")
-        pseudopotentials(dh).tofile(vf)
-        dim = 7764392
-        # calibrate: about 45 us of one thread per row (hermitian product), measured on x86 hosts
-        rows = int(min(dim, max(2000, rows_target_s * threads / 45e-6)))
-        cmd = [REF_TOOL, "bench_fqhe", N_FERMIONS, TWO_S, TWO_LZ, vf, threads, reps, hermitian, rows]
-        out = subprocess.run([str(c) for c in cmd], check=True, capture_output=True, text=True)
-        line = [l for l in out.stdout.splitlines() if l.startswith("{")][-1]
-        r = json.loads(line)
-    per_matvec = r["mean_s"] * r["dim"] / r["rows"]
-    return {"value": 1.0 / per_matvec, "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": "first %d of %d rows per product, %d repetition(s), SMP %d threads, hermitian %s "
-                      "(VectorHamiltonianMultiplyOperation on SMPArchitecture, -m 0)"
-                      % (r["rows"], r["dim"], reps, threads, "on" if hermitian else "off"),
-            "seconds_per_sample": r["mean_s"]}
+    cmd = [REF_TOOL, "bench_fqhe_block", N_FERMIONS, TWO_S, TWO_LZ, "coulomb", threads, reps + skip, 1, BLOCK,
+           windows]
+    out = subprocess.run([str(c) for c in cmd], check=True, capture_output=True, text=True)
+    r = json.loads([l for l in out.stdout.splitlines() if l.startswith("{")][-1])
+    counted = r["reps"][skip:]
+    seconds = sum(c["s"] for c in counted)
+    products = sum(c["rows"] for c in counted) / float(r["dim"])
+    return {"value": BLOCK * products / seconds, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": "%d call(s), each one of %d equal row windows of the %d-row basis in turn (%.2f whole block "
+                      "products), SMP %d threads, hermitian (MultipleVectorHamiltonianMultiplyOperation on "
+                      "SMPArchitecture, -m 0), FP64 blocks of %d vectors"
+                      % (len(counted), windows, r["dim"], products, threads, BLOCK),
+            "seconds_per_sample": seconds / len(counted), "seconds_per_block_product": seconds / products,
+            "reference_setup_seconds": r["setup_s"]}
 
 
 def port_cpu_matvec(rows):
@@ -199,28 +212,27 @@ def port_cpu_matvec(rows):
 def cpu_baseline():
     if os.path.exists(REF_TOOL):
         try:
-            return reference_cpu_matvec(rows_target_s=12.0, reps=1)
-        except (subprocess.CalledProcessError, OSError, ValueError, IndexError) as e:
+            # one whole block product, as two half-basis calls
+            return reference_cpu_block(REFERENCE_WINDOWS, REFERENCE_WINDOWS)
+        except (subprocess.CalledProcessError, OSError, ValueError, IndexError, KeyError) as e:
             sys.stderr.write("reference CPU baseline failed (%s); timing the oracle port\n" % e)
     return port_cpu_matvec(20000)
 
 
 def run_reference_arm(args, world, rank):
+    """The reference's own CPU block product on this arm's workload and metric: each step is one
+    half-basis window (two steps = one whole product), the warm-up steps are run and not counted.
+    Nothing from the diagham_b200 package is loaded."""
     if rank != 0:
         return
     if not os.path.exists(REF_TOOL):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_tool was not built (make -C oracle ref)"}))
         return
-    # seconds of reference CPU work spread over the steps (DH_BENCH_REFERENCE_SECONDS, 150 by default)
-    budget = float(os.environ.get("DH_BENCH_REFERENCE_SECONDS", "150"))
-    per = max(0.05, budget / float(args.steps + args.warmup))
-    cb = reference_cpu_matvec(rows_target_s=per, reps=args.steps)
+    cb = reference_cpu_block(REFERENCE_WINDOWS, args.steps, skip=args.warmup)
     line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * cb["seconds_per_sample"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload_name().replace("FP32 elements + FP32 row accumulation, FP64 vectors",
-                                                           "FP64 (reference CPU path)")},
-            "impl": "reference", "cpu_baseline": cb,
+            "config": workload_config(), "impl": "reference", "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -348,10 +360,20 @@ def time_to_e0_all_sectors(dh, k=2, runs=3, precisions=(1e-10, 1e-13)):
         out["precision_%g" % precision] = res
         if precision == min(precisions):
             e_strict = e_plain
+    # the reference's lowest energy of every sector (its block Lanczos, k = 4, or full diagonalisation
+    # below 300 states; tests/golden/sectors_n10_2s27_block4.npz), when the fixture is present
+    ref_path = os.path.join(ROOT, "tests", "golden", "sectors_n10_2s27_block4.npz")
+    e_ref = None
+    if os.path.exists(ref_path):
+        z = np.load(ref_path)
+        ref_of = dict(zip((int(t) for t in z["two_lz"]), (float(e) for e in z["e0"])))
+        e_ref = np.array([ref_of[lz] for lz in sectors])
     for key in [k_ for k_ in out if k_.startswith("precision_")]:
         for v_ in out[key].values():
             e = np.asarray(v_.pop("energies"))
             v_["max_rel_e_minus_plain_fp64_strict"] = float(np.max(np.abs(e - e_strict) / np.abs(e_strict)))
+            if e_ref is not None:
+                v_["max_rel_e_minus_reference"] = float(np.max(np.abs(e - e_ref) / np.abs(e_ref)))
     out["ground_state"] = {"two_lz": int(sectors[int(np.argmin(e_strict))]), "e0": float(np.min(e_strict))}
     return out
 
@@ -393,6 +415,70 @@ def spin_chain_product(dh, flush, steps=5, k=2, length=32, warmup=2):
             "roofline": {"bound": "hbm", "achieved": alg / mean_s / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": alg / mean_s / 1e9 / peak, "peak_kind": kind}}
 
+
+
+def spin_chain_solve(dh, length=32, k=2, precision=1e-10, max_iter=400):
+    """The large-spin-chain configuration end to end: periodic J1-J2 chain, L = 32, J2 = J1/2, Sz = 0
+    (dimension 601,080,390), block Lanczos with k = 2, FP32 products with FP64 vectors and FP64
+    refinement, stopping at the stated precision; the exact E0 = -3L/8 is the check."""
+    import torch
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    chain = dh.Spin1_2Chain(length, 0)
+    H = dh.SpinChainJ1J2Hamiltonian(chain, 1.0, 0.5)
+    H.set_precision("fp32")
+    torch.cuda.synchronize()
+    setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    lz = dh.BasicBlockLanczosAlgorithm(H, 1, max_iter, block_size=k)
+    lz.InitializeLanczosAlgorithm(seed=0)
+    r = lz.solve_refined(max_iter, precision=precision)
+    torch.cuda.synchronize()
+    solve = time.perf_counter() - t0
+    exact = -0.375 * length
+    out = {"workload": "Spin1_2Chain L=%d Sz=0 periodic J1=1 J2=0.5 (dim %d), block k=%d, FP32 products + FP64 "
+                       "refinement" % (length, chain.dim, k),
+           "setup_seconds": setup, "seconds": solve, "e0": r["energy"], "e0_fp32_phase": r["energy_fp32"],
+           "rel_e0_minus_exact": abs(r["energy"] - exact) / abs(exact), "residual": r["residual"],
+           "fp32_block_products": r["fp32_matvecs"], "fp64_products": r["fp64_matvecs"], "precision": precision}
+    del lz, H, chain
+    torch.cuda.empty_cache()
+    return out
+
+
+def time_to_e0_summary(line):
+    """A compact digest of the time-to-E0 legs (seconds, speed-ups, errors) for the end of the line."""
+    out = {}
+    tte = line.get("time_to_e0")
+    if tte:
+        p = tte.get("precision_1e-10", {})
+        if p:
+            best = p["best_fp32_refined"]["form"]
+            out["n12_2s33"] = {"plain_fp64_s": round(p["plain_fp64"]["seconds"], 4),
+                               "fp32_refined_s": round(p[best]["seconds"], 4), "form": best,
+                               "speedup": round(p["plain_fp64"]["seconds"] / p[best]["seconds"], 3),
+                               "rel_err_plain": p["plain_fp64"].get("rel_e_minus_reference"),
+                               "rel_err_refined": p[best].get("rel_e_minus_reference")}
+    tc = line.get("time_to_e0_all_sectors")
+    if tc:
+        p = tc.get("precision_1e-10", {})
+        if p:
+            pl = p["plain_fp64_per_sector"]
+            out["n10_2s27_91_sectors"] = {
+                "plain_fp64_s": round(pl["seconds"], 4),
+                "batched_fp32_refined_s": round(p["batched_fp32_refined"]["seconds"], 4),
+                "batched_fp64_s": round(p["batched_fp64"]["seconds"], 4),
+                "speedup": round(p["batched_fp32_refined"]["speedup_vs_plain_fp64"], 3),
+                "max_rel_err_refined": p["batched_fp32_refined"].get("max_rel_e_minus_plain_fp64_strict"),
+                "max_rel_err_vs_reference": p["batched_fp32_refined"].get("max_rel_e_minus_reference")}
+    cs = line.get("spin_chain_l32_solve")
+    if cs:
+        out["chain_l32"] = {"s": round(cs["seconds"], 3), "e0": cs["e0"], "rel_err": cs["rel_e0_minus_exact"]}
+    cb = line.get("cpu_baseline")
+    if cb:
+        out["headline_fp64_block4"] = {"b200_hv_s": round(line["value"], 2), "reference_cpu_hv_s": round(cb["value"], 4),
+                                       "e2e_hv_s": round(line["e2e"]["value"], 2)}
+    return out
 
 
 def long_product(dh, flush, steps=5, warmup=2):
@@ -516,13 +602,16 @@ def momentum_sector(dh, flush, steps=5, k=2, length=32, warmup=2, solve=True):
         torch.cuda.empty_cache()
         return out
     t0 = time.perf_counter()
+    # the stopping test bounds the change of the Ritz value, not its error: 1e-12 leaves a margin
+    # under the 1e-10 relative target
     lz = dh.BasicLanczosAlgorithm(H, 1, 600)
-    lz.SetEigenvaluePrecision(1e-10)
+    lz.SetEigenvaluePrecision(1e-12)
     lz.InitializeLanczosAlgorithm(seed=0)
     r = lz.solve(600, graph_batch=16)
     out["time_to_e0"] = {"seconds": time.perf_counter() - t0, "e0": float(r["eigenvalues"][0]),
                          "iterations": r["iterations"], "abs_e0_plus_3L_over_8": abs(r["eigenvalues"][0] + 0.375 * length),
-                         "precision": 1e-10}
+                         "rel_e0_minus_exact": abs(r["eigenvalues"][0] + 0.375 * length) / (0.375 * length),
+                         "stopping_precision": 1e-12}
     del lz, H, sp
     torch.cuda.empty_cache()
     out["complex_k1"] = complex_momentum_sector(dh, flush, length, 1, steps, warmup)
@@ -766,12 +855,14 @@ def run_b200(args, world, rank, local):
         return
     space = dh.FermionOnSphere(N_FERMIONS, TWO_LZ, TWO_S)
     dim = space.dim
+    assert dim == DIM
     H = dh.ParticleOnSphereGenericHamiltonian(space, N_FERMIONS, TWO_S, pseudopotentials(dh))
     H.set_stream(stream.cuda_stream)
     moves = H.count_elements()
     # the project autotuner picks the kernel form and rank-table split for this sector and block
-    H.set_precision("fp32")
-    tuning = H.autotune(block_size=BLOCK, repeats=3)
+    # (--no-autotune: the defaults, or DH_FQHE_KERNEL / DH_FQHE_LOW_BITS, as for a short ncu capture)
+    H.set_precision("fp64")
+    tuning = None if args.no_autotune else H.autotune(block_size=BLOCK, repeats=3)
     g = torch.Generator(device="cuda")
     g.manual_seed(0)
     xb = torch.rand(dim, BLOCK, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
@@ -803,42 +894,42 @@ def run_b200(args, world, rank, local):
         return e0.elapsed_time(e1), [s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)]
 
     if args.kernel_only:
-        total_ms, launch_ms = timed("fp32", BLOCK, args.steps, args.warmup)
+        prec = args.precision
+        if prec != "fp64" and not args.no_autotune:
+            H.set_precision(prec)
+            H.autotune(block_size=BLOCK, repeats=3)
+        total_ms, launch_ms = timed(prec, BLOCK, args.steps, args.warmup)
         if rank == 0:
-            print(json.dumps({"kernel_only": True, "dim": dim, "block": BLOCK, "elements_per_product": moves,
-                              "steps": args.steps, "mean_launch_ms": statistics.mean(launch_ms),
-                              "ms_per_step": total_ms / args.steps}))
+            print(json.dumps({"kernel_only": True, "dim": dim, "block": BLOCK, "precision": prec,
+                              "elements_per_product": moves, "steps": args.steps,
+                              "mean_launch_ms": statistics.mean(launch_ms), "ms_per_step": total_ms / args.steps}))
         return
-    # single-vector rates for the record (the plain FP64 form and the FP32 single-vector form)
-    singles = {}
-    for prec in ("fp64", "fp32"):
-        t_ms, l_ms = timed(prec, 1, max(5, args.steps // 10), 3)
-        singles[prec] = {"hv_per_s": len(l_ms) / (t_ms / 1000.0), "mean_launch_ms": statistics.mean(l_ms)}
-    t_ms, l_ms = timed("fp64", BLOCK, max(5, args.steps // 10), 3)
-    singles["fp64_block%d" % BLOCK] = {"hv_per_s": BLOCK * len(l_ms) / (t_ms / 1000.0),
-                                       "mean_launch_ms": statistics.mean(l_ms)}
+    # the headline: FP64 blocks of 4 (the block Lanczos product in the reference's arithmetic)
     with ClockSampler(local) as clocks:
-        total_ms, launch_ms = timed("fp32", BLOCK, args.steps, args.warmup)
+        total_ms, launch_ms = timed("fp64", BLOCK, args.steps, args.warmup)
     total_ms = reduce_max(total_ms, world)
     value = world * BLOCK * args.steps / (total_ms / 1000.0)
 
     # roofline of the block product: algorithmic bytes per launch (basis word and k FP64 outputs per
-    # row, k FP32 inputs per off-diagonal element and for the row itself) over the mean device time
-    # of one C-ABI call (the FP64 -> FP32 conversion of x included)
+    # row, k FP64 inputs per off-diagonal element and for the row itself) over the mean device time
+    # of one C-ABI call
     c_n2 = N_FERMIONS * (N_FERMIONS - 1) // 2
     nnz_off = moves - c_n2 * dim
-    alg_bytes = dim * 8 + BLOCK * dim * 8 + BLOCK * (nnz_off + dim) * 4
+
+    def alg_bytes(xbytes, k):
+        return dim * 8 + k * dim * 8 + k * (nnz_off + dim) * xbytes
+
     launch_mean = statistics.mean(launch_ms) / 1000.0
     peak, peak_kind = peaks()
-    achieved = alg_bytes / launch_mean / 1e9
+    achieved = alg_bytes(8, BLOCK) / launch_mean / 1e9
     traffic = profile_traffic()
 
-    # end to end through the public API with pinned host buffers (H2D of x, D2H of y every step)
+    # end to end through the public API with pinned host buffers (H2D of X, D2H of Y every step)
     hx = torch.empty(dim, BLOCK, dtype=torch.float64, pin_memory=True)
     hy = torch.empty(dim, BLOCK, dtype=torch.float64, pin_memory=True)
     hx.copy_(xb.cpu())
     hxn, hyn = hx.numpy(), hy.numpy()
-    H.set_precision("fp32")
+    H.set_precision("fp64")
     e2e_steps = max(3, min(args.steps, 40))
     for _ in range(2):
         H.block_multiply(hxn, hyn)
@@ -851,39 +942,55 @@ def run_b200(args, world, rank, local):
     e2e_s = reduce_max(time.perf_counter() - t0, world)
     e2e_value = world * BLOCK * e2e_steps / e2e_s
 
-    tte = tte_c = spin = grads = stored = bosons = momentum = longs = None
+    # the other arithmetic / widths of the same product, for the record
+    other = {}
+    for prec, k in (("fp64", 1), ("fp32", 1), ("fp32", BLOCK)):
+        if prec == "fp32" and "fp32_tuning" not in other:
+            H.set_precision("fp32")
+            t = H.autotune(block_size=BLOCK, repeats=3)
+            other["fp32_tuning"] = {k_: t[k_] for k_ in ("kernel_variant", "low_bits")}
+        t_ms, l_ms = timed(prec, k, max(5, args.steps // 4), 3)
+        lm = statistics.mean(l_ms) / 1000.0
+        ab = alg_bytes(8 if prec == "fp64" else 4, k)
+        other["%s_block%d" % (prec, k)] = {"hv_per_s": k * len(l_ms) / (t_ms / 1000.0), "mean_launch_ms": lm * 1000.0,
+                                          "algorithmic_bytes_per_launch": ab,
+                                          "roofline_frac": ab / lm / 1e9 / peak}
+
+    tte = tte_c = spin = grads = stored = bosons = momentum = longs = chain_solve = None
     if not args.no_solve:
+        H.set_precision("fp32")
         stored = stored_elements(dh, H, flush, dim)
         H.autotune(block_size=BLOCK, repeats=3)
         tte = time_to_e0_single_sector(dh, H)
         tte_c = time_to_e0_all_sectors(dh)
         grads = gradients_two_sectors(dh)
-        del xb, yb, hx, hy
+        del xb, yb, hx, hy, x1, y1
+        del H, space
         torch.cuda.empty_cache()
         spin = spin_chain_product(dh, flush)
+        chain_solve = spin_chain_solve(dh)
         bosons = boson_product(dh, flush)
         momentum = momentum_sector(dh, flush)
         longs = long_product(dh, flush)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload_name(), "dim": dim, "block": BLOCK, "elements_per_product": moves,
-                       "hv_per_step": BLOCK, "l2": "flushed: 256 MiB write before every step",
-                       "autotuned": {k: tuning[k] for k in ("kernel_variant", "low_bits", "candidates")},
-                       "parallelism": "replicas" if world > 1 else "single GPU"},
-            "gpu_launches": 2 * args.steps,
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(),
+            "gpu_launches": args.steps,
+            "autotuned": {k: tuning[k] for k in ("kernel_variant", "low_bits", "candidates")} if tuning else None,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": dim * BLOCK * 8,
                     "d2h_bytes_per_step": dim * BLOCK * 8, "steps": e2e_steps, "buffers": "pinned host"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": alg_bytes,
-                         "kernel": "fqhe_split_kernel<float, 4, RANGE=0, LR_SMEM=0, IL=1> (+ x FP64->FP32 conversion)",
+                         "algorithmic_bytes_per_launch": alg_bytes(8, BLOCK),
+                         "kernel": KERNEL_FP64_BLOCK4, "binding_unit": BINDING_UNIT_FP64_BLOCK4,
                          "mean_launch_ms": launch_mean * 1000.0},
-            "single_vector": singles,
+            "other_forms": other,
             "clocks": clocks.summary(),
             "time_to_e0": tte,
             "time_to_e0_all_sectors": tte_c,
+            "spin_chain_l32_solve": chain_solve,
             "gradients": grads,
             "stored_elements": stored,
             "spin_chain_l32": spin,
@@ -907,6 +1014,8 @@ def run_b200(args, world, rank, local):
                 longs["cpu_baseline"] = reference_cpu_long()
             except (subprocess.CalledProcessError, OSError, ValueError, IndexError) as e:
                 longs["cpu_baseline"] = {"unavailable": str(e)}
+    # last: the compact time-to-E0 summary (the end of the line is what short log tails keep)
+    line["time_to_e0_summary"] = time_to_e0_summary(line)
     if rank == 0:
         print(json.dumps(line))
 
@@ -921,6 +1030,10 @@ def main():
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only the timed FP32 products (the short command used for ncu captures)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="with --kernel-only: skip the autotuner (kernel form from DH_FQHE_KERNEL / DH_FQHE_LOW_BITS)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
+                    help="with --kernel-only: the arithmetic of the timed block products")
     ap.add_argument("--chain-length", type=int, default=0,
                     help="with --kernel-only: time the J1-J2 chain block product (k = 2) at this length instead")
     ap.add_argument("--leg", default=None, choices=["long", "momentum", "bosons"],

@@ -2,13 +2,17 @@
 //
 // dh_hamiltonian_pseudopotential_adjoint needs a [blocks][factors] FP64 scratch array for the
 // per-block bins of its kernel and allocates it (and staging buffers for host vectors) on first
-// use.  Some callers cannot allocate device memory at all: code running inside a CUDA stream
-// capture, or an application whose framework owns every byte of device memory through its own
-// allocator or a fixed arena.  This entry point runs the same kernels with their scratch in a
-// file-scope static device array instead, and stages nothing: u and v must already be on the
-// device.  The array is sized for lz_max <= 33 (2S <= 33, at most DH_STATIC_ADJOINT_MAX_FACTORS
-// interaction factors) and DH_STATIC_ADJOINT_BLOCKS blocks; it costs about 7.6 MB on every GPU that
-// loads the library, held until the process exits.
+// use.  Some callers cannot allocate device memory at all: an application whose framework owns
+// every byte of device memory through its own allocator or a fixed arena, where a library's
+// cudaMalloc would fail or break that framework's accounting.  This entry point runs the same
+// kernels with their scratch in a file-scope static device array instead, and stages nothing: u
+// and v must already be on the device.  The array is sized for lz_max <= 33 (2S <= 33, at most
+// DH_STATIC_ADJOINT_MAX_FACTORS interaction factors) and DH_STATIC_ADJOINT_BLOCKS blocks; it costs
+// about 7.6 MB on every GPU that loads the library, held until the process exits.
+//
+// The call is synchronous: it waits on the handle's stream for the summed bins, copies them into a
+// static host array and contracts them with dfactor/dV_m on the host.  A process-wide mutex
+// serialises the calls (on every GPU), so two calls never use the array at the same time.
 #include <cuda_runtime.h>
 #include <mutex>
 
@@ -60,6 +64,11 @@ extern "C" int dh_hamiltonian_pseudopotential_adjoint_static(dh_hamiltonian_t h,
   DH_CHECK(nf <= DH_STATIC_ADJOINT_MAX_FACTORS, DH_ERR_UNSUPPORTED,
            "%d interaction factors exceed the static scratch of %d (lz_max <= 33)", nf, DH_STATIC_ADJOINT_MAX_FACTORS);
   dh_space_s* sp = h->space;
+  int current = -1;
+  DH_CUDA(cudaGetDevice(&current));
+  DH_CHECK(current == sp->device, DH_ERR_STATE,
+           "device %d is current but the Hamiltonian's space lives on device %d: make that device current", current,
+           sp->device);
   // the lookup mode's table is built when the mode is selected, so nothing is allocated here
   DH_CHECK(sp->index_mode != DH_INDEX_LOOKUP || sp->lookup.ptr, DH_ERR_STATE, "lookup table missing");
   std::lock_guard<std::mutex> lock(g_scratch_mutex);

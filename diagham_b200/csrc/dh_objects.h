@@ -11,8 +11,15 @@
 // Largest DiagHam lookup table staged in shared memory by the DH_INDEX_LOOKUP kernels.
 #define DH_LOOKUP_SMEM_BYTES (96 * 1024)
 
+// The device current when a handle is created; its device memory lives there (-1 without a device).
+inline int dh_current_device() {
+  int d = -1;
+  return cudaGetDevice(&d) == cudaSuccess ? d : -1;
+}
+
 struct dh_space_s {
   int kind = 0;
+  int device = dh_current_device();
   int64_t dim = 0;
   int index_mode = DH_INDEX_RANK;
   int kernel_variant = 0;  // product kernel of the rank mode (0 split-word, 1 generic, 2 split + smem table)

@@ -307,16 +307,21 @@ int dh_hamiltonian_count_elements(dh_hamiltonian_t h, int64_t* total);
 int dh_hamiltonian_count_diagonal_elements(dh_hamiltonian_t h, int64_t* total);
 
 /* Same result as dh_hamiltonian_pseudopotential_adjoint, for callers that cannot allocate device
- * memory: code running inside a CUDA stream capture, or applications whose framework owns all
- * device memory through its own allocator or a fixed arena.  No counterpart in the reference.
+ * memory: applications whose framework owns all device memory through its own allocator or a
+ * fixed arena, where a cudaMalloc made by a library fails or breaks the framework's accounting.
+ * No counterpart in the reference.
  * It allocates nothing (no cudaMalloc / cudaFree, no staging): u and v must be device pointers;
  * out (lz_max + 1 values) may be host or device memory.  Its per-block scratch is a static device
  * array sized for DH_STATIC_ADJOINT_BLOCKS x DH_STATIC_ADJOINT_MAX_FACTORS doubles (about 7.6 MB,
  * held by every GPU that loads the library until the process exits); Hamiltonians with more
  * interaction factors (lz_max > 33) are rejected with DH_ERR_UNSUPPORTED.  The first call on a
- * device looks up the array's device address; make that first call before any stream capture.
- * All calls share the one array, so calls that overlap on the GPU (other threads or streams) race;
- * each call overwrites what it uses, so the contents left by a previous call do not matter. */
+ * device looks up the array's device address (cudaGetSymbolAddress with that device current).
+ * The device that was current when the Hamiltonian's space was created must be current for the
+ * call (DH_ERR_STATE otherwise).  The call is synchronous: it waits on the handle's stream and
+ * returns with the result written to out.  All calls share the one array; a process-wide mutex
+ * serialises them (on every GPU), so calls never overlap on it; calls that overlapped on the GPU
+ * would race.  Each call overwrites what it uses, so the contents left by a previous call do not
+ * matter. */
 #define DH_STATIC_ADJOINT_BLOCKS 148
 #define DH_STATIC_ADJOINT_MAX_FACTORS 6400
 int dh_hamiltonian_pseudopotential_adjoint_static(dh_hamiltonian_t h, const double* u, const double* v, double* out);

@@ -40,6 +40,7 @@
 #include "Architecture/MonoProcessorArchitecture.h"
 #include "Architecture/SMPArchitecture.h"
 #include "Architecture/ArchitectureOperation/VectorHamiltonianMultiplyOperation.h"
+#include "Architecture/ArchitectureOperation/MultipleVectorHamiltonianMultiplyOperation.h"
 #include "LanczosAlgorithm/BasicLanczosAlgorithm.h"
 #include "LanczosAlgorithm/FullReorthogonalizedLanczosAlgorithm.h"
 #include "LanczosAlgorithm/BasicBlockLanczosAlgorithm.h"
@@ -169,7 +170,45 @@ class ExposedGenericHamiltonian : public ParticleOnSphereGenericHamiltonian
   int NbrFactors() { return this->NbrInteractionFactors; }
   double Factor(int i) { return this->InteractionFactors[i]; }
   void SetFactor(int i, double x) { this->InteractionFactors[i] = x; }
+  // GetLoadBalancing (AbstractQHEOnSphereHamiltonian.cc:3547) caches its segments for a thread count;
+  // dropping the cache makes the next product split the architecture's current typical range
+  void ResetLoadBalancing()
+  {
+    delete[] this->LoadBalancingArray;
+    this->LoadBalancingArray = 0;
+  }
 };
+
+// SMPArchitecture whose typical range (AbstractArchitecture.cc:65, [0, dim - 1] in the reference) is a
+// window [First, Last] of the space: the rows the reference SMP product splits between its threads
+class WindowSMPArchitecture : public SMPArchitecture
+{
+ public:
+  long First, Last;
+  WindowSMPArchitecture(int nbrThreads) : SMPArchitecture(nbrThreads), First(0), Last(-1) {}
+  void GetTypicalRange(long& minIndex, long& maxIndex)
+  {
+    if (this->Last >= this->First)
+      {
+	minIndex = this->First;
+	maxIndex = this->Last;
+      }
+    else
+      SMPArchitecture::GetTypicalRange(minIndex, maxIndex);
+  }
+};
+
+// pseudopotentials: "coulomb" = the reference's LLL Coulomb V_m (EvaluatePseudopotentials,
+// PseudoPotentials.cc:35) with the even m set to zero (spin-polarised fermions), else a raw file
+static double* PseudopotentialsFromSpec(const char* spec, int lzMax)
+{
+  if (strcmp(spec, "coulomb") != 0)
+    return ReadDoubles(spec, lzMax + 1);
+  double* V = EvaluatePseudopotentials(lzMax, 0, 0.0, true);
+  for (int m = 0; m <= lzMax; m += 2)
+    V[m] = 0.0;
+  return V;
+}
 
 // J1-J2 periodic chain on a plain Spin1_2Chain (see file header)
 class J1J2ChainHarness : public AbstractHamiltonian
@@ -457,6 +496,7 @@ static void Usage()
 	  "  fqhe_factors N 2S vfile out\n"
 	  "  fqhe_rows N 2S 2Lz vfile rowsfile out\n"
 	  "  fqhe_matvec N 2S 2Lz vfile xfile shift out\n"
+	  "  fqhe_sectors N 2S vfile block maxiter precision fulldiag out\n"
 	  "  fqhe_lanczos N 2S 2Lz vfile algo nev block maxiter precision out gsout x0 [x1 ...]\n"
 	  "  fqhe_lanczos_disk N 2S 2Lz vfile algo nbriter precision dir x0|resume gsiter out gsout\n"
 	  "  fqhe_expect N 2S 2Lz vfile psifile out\n"
@@ -483,6 +523,7 @@ static void Usage()
 	  "  spintc_matvec L 2Sz K J1 J2 xfile out\n"
 	  "  spintc_dense L 2Sz K J1 J2 out\n"
 	  "  bench_fqhe N 2S 2Lz vfile threads reps hermitian [rows]\n"
+	  "  bench_fqhe_block N 2S 2Lz vspec threads reps hermitian k windows\n"
 	  "  bench_bqhe N 2S 2Lz vfile threads reps hermitian [rows]\n"
 	  "  bench_lfqhe N 2S 2Lz vfile threads reps hermitian [rows]\n"
 	  "  bench_spint L 2Sz K J1 J2 threads reps [rows]\n"
@@ -694,15 +735,92 @@ int main(int argc, char** argv)
     {
       int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
       double* V = ReadDoubles(argv[5], LzMax + 1);
-      FermionOnSphere Space(N, TotalLz, LzMax, 1ul << 20);
-      MonoProcessorArchitecture Arch;
-      ParticleOnSphereGenericHamiltonian H(&Space, N, LzMax, V, 0.0, &Arch, 0, false, 0, false);
+      FermionOnSphere Space(N, TotalLz, LzMax, 9ul << 20);
+      // REF_THREADS > 1: the SMP product (VectorHamiltonianMultiplyOperation on SMPArchitecture)
+      AbstractArchitecture* Arch = MakeArchitecture();
+      Arch->SetDimension(Space.GetHilbertSpaceDimension());
+      ParticleOnSphereGenericHamiltonian H(&Space, N, LzMax, V, 0.0, Arch, 0, false, 0, false);
       H.ShiftHamiltonian(atof(argv[7]));
       RealVector X;
       X.ReadVector(argv[6]);
       RealVector Y(Space.GetHilbertSpaceDimension(), true);
-      H.LowLevelMultiply(X, Y);
+      VectorHamiltonianMultiplyOperation Op(&H, &X, &Y);
+      Op.ApplyOperation(Arch);
       Y.WriteVector(argv[8]);
+      return 0;
+    }
+  if (strcmp(Cmd, "fqhe_sectors") == 0 && argc == 10)
+    {
+      // every Lz sector 2Lz = Lzmax .. 0 of N fermions (the positive half: 2Lz >= 0), as
+      // QHEOnSphereMainTask does per sector: full diagonalisation below `fulldiag` states
+      // (GetHamiltonian + Householder + Diagonalize, QHEOnSphereMainTask.cc:397-471), else
+      // BasicBlockLanczosAlgorithm with `block` vectors from its own random start
+      // (BasicBlockLanczosAlgorithm.cc:233) under the driver loop (QHEOnSphereMainTask.cc:732-753).
+      // Output text: per sector "2Lz dim E0 iterations converged method".
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]);
+      double* V = ReadDoubles(argv[4], LzMax + 1);
+      int Block = atoi(argv[5]), MaxIter = atoi(argv[6]);
+      double Precision = atof(argv[7]);
+      int FullDiag = atoi(argv[8]);
+      FILE* f = fopen(argv[9], "w");
+      if (f == 0)
+	{
+	  fprintf(stderr, "cannot open %s\n", argv[9]);
+	  exit(2);
+	}
+      int MaxTwoLz = N * (LzMax - N + 1);
+      for (int TwoLz = MaxTwoLz; TwoLz >= 0; TwoLz -= 2)
+	{
+	  FermionOnSphere Space(N, TwoLz, LzMax, 9ul << 20);
+	  long Dim = Space.GetHilbertSpaceDimension();
+	  AbstractArchitecture* Arch = MakeArchitecture();
+	  Arch->SetDimension(Dim);
+	  ParticleOnSphereGenericHamiltonian H(&Space, N, LzMax, V, 0.0, Arch, 0, false, 0, false);
+	  double E0;
+	  int Iter = 0, Conv = 1;
+	  const char* Method;
+	  if (Dim < FullDiag)
+	    {
+	      RealSymmetricMatrix HRep(Dim);
+	      H.GetHamiltonian(HRep);
+	      if (Dim > 1)
+		{
+		  RealTriDiagonalSymmetricMatrix TmpTriDiag(Dim);
+		  HRep.Householder(TmpTriDiag, 1e-7);
+		  TmpTriDiag.Diagonalize();
+		  TmpTriDiag.SortMatrixUpOrder();
+		  E0 = TmpTriDiag.DiagonalElement(0);
+		}
+	      else
+		HRep.GetMatrixElement(0, 0, E0);
+	      Method = "full";
+	    }
+	  else
+	    {
+	      BasicBlockLanczosAlgorithm Lanczos(Arch, 1, Block, MaxIter);
+	      if (Precision != 0.0)
+		Lanczos.SetEigenvaluePrecision(Precision);
+	      Lanczos.SetHamiltonian(&H);
+	      Lanczos.InitializeLanczosAlgorithm();
+	      Lanczos.RunLanczosAlgorithm(3);
+	      Iter = 4 * Block;
+	      while ((Lanczos.TestConvergence() == false) && (Iter < MaxIter))
+		{
+		  Iter += Block;
+		  Lanczos.RunLanczosAlgorithm(1);
+		}
+	      Conv = Lanczos.TestConvergence() ? 1 : 0;
+	      RealTriDiagonalSymmetricMatrix TmpMatrix;
+	      TmpMatrix.Copy(Lanczos.GetDiagonalizedMatrix());
+	      TmpMatrix.SortMatrixUpOrder();
+	      E0 = TmpMatrix.DiagonalElement(0);
+	      Method = "block";
+	    }
+	  fprintf(f, "%d %ld %.17g %d %d %s\n", TwoLz, Dim, E0, Iter, Conv, Method);
+	  fflush(f);
+	  delete Arch;
+	}
+      fclose(f);
       return 0;
     }
   if (strcmp(Cmd, "fqhe_lanczos") == 0 && argc >= 14)
@@ -1068,6 +1186,61 @@ int main(int argc, char** argv)
       printf("{\"dim\": %ld, \"rows\": %ld, \"threads\": %d, \"reps\": %d, \"best_s\": %.6e, \"mean_s\": %.6e, "
 	     "\"setup_s\": %.3f, \"hermitian\": %d, \"xHx\": %.15e}\n", Dim, Rows, Threads, Reps, Best, Total / Reps,
 	     tsetup, Hermitian ? 1 : 0, Check);
+      return 0;
+    }
+  if (strcmp(Cmd, "bench_fqhe_block") == 0 && argc == 11)
+    {
+      // times the reference SMP block product of block Lanczos: MultipleVectorHamiltonianMultiplyOperation
+      // (MultipleVectorHamiltonianMultiplyOperation.cc:56, SMP split :555-640) on k vectors, on the fly
+      // (memory 0, as with -m 0), hermitian as the Hamiltonian says (:73-79) ->
+      // HermitianLowLevelMultipleMultiply (AbstractQHEOnSphereHamiltonian.cc:3019).  The space is cut
+      // into `windows` equal row windows; repetition r multiplies window r mod windows (all windows
+      // together are one whole product).  vspec: "coulomb" or a raw file of 2S + 1 doubles.
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      double* V = PseudopotentialsFromSpec(argv[5], LzMax);
+      int Threads = atoi(argv[6]);
+      int Reps = atoi(argv[7]);
+      bool Hermitian = atoi(argv[8]) != 0;
+      int K = atoi(argv[9]);
+      long Windows = atol(argv[10]);
+      double ts = Now();
+      FermionOnSphere Space(N, TotalLz, LzMax, 9ul << 20);
+      WindowSMPArchitecture Arch(Threads);
+      long Dim = Space.GetHilbertSpaceDimension();
+      if (Windows < 1 || Windows > Dim)
+	Windows = 1;
+      Arch.SetDimension(Dim);
+      ExposedGenericHamiltonian H(&Space, N, LzMax, V, &Arch, Hermitian);
+      double tsetup = Now() - ts;
+      RealVector* X = new RealVector[K];
+      RealVector* Y = new RealVector[K];
+      for (int j = 0; j < K; ++j)
+	{
+	  X[j] = RealVector(Dim, true);
+	  Y[j] = RealVector(Dim, true);
+	  for (long i = 0; i < Dim; ++i)
+	    X[j][i] = (1.0 + 0.25 * j * ((i % 7) - 3.0)) / sqrt((double) Dim);
+	}
+      printf("{\"dim\": %ld, \"threads\": %d, \"k\": %d, \"windows\": %ld, \"hermitian\": %d, \"setup_s\": %.3f, "
+	     "\"reps\": [", Dim, Threads, K, Windows, Hermitian ? 1 : 0, tsetup);
+      for (int r = 0; r < Reps; ++r)
+	{
+	  long w = r % Windows;
+	  Arch.First = (Dim * w) / Windows;
+	  Arch.Last = (Dim * (w + 1)) / Windows - 1;
+	  H.ResetLoadBalancing();
+	  MultipleVectorHamiltonianMultiplyOperation Op(&H, X, Y, K);
+	  double t0 = Now();
+	  Op.ApplyOperation(&Arch);
+	  double t = Now() - t0;
+	  double Check = 0.0;
+	  for (int j = 0; j < K; ++j)
+	    Check += X[j] * Y[j];
+	  printf("%s{\"first\": %ld, \"rows\": %ld, \"s\": %.6e, \"xHx\": %.15e}", r ? ", " : "", Arch.First,
+		 Arch.Last - Arch.First + 1, t, Check);
+	  fflush(stdout);
+	}
+      printf("]}\n");
       return 0;
     }
   if (strcmp(Cmd, "bench_spint") == 0 && (argc == 9 || argc == 10))

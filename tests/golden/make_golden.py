@@ -6,7 +6,8 @@ calls).  This script needs the reference checkout (default /root/reference, or $
 run by hand; the tests only read the .npz files it writes.
 
     python tests/golden/make_golden.py            # all small fixtures (about a minute)
-    python tests/golden/make_golden.py --slow     # adds the long N=12, 2S=33 reference Lanczos run
+    python tests/golden/make_golden.py --slow     # adds the long runs: the N=12, 2S=33 reference Lanczos
+                                                  # and full product, the 91 sectors of N=10, 2S=27
 
 Binary layouts written by ref_tool are documented next to each reader below.  Start vectors are
 the repository's splitmix64 vectors (component i = (i+1)-th splitmix64 output of the seed mapped to
@@ -259,6 +260,55 @@ def slow_fixtures(tmp):
     cmd = run("fqhe_lanczos", 12, 33, 0, vf, "basic", 1, 1, 400, 1e-13, lf, "-", xf, env={"REF_THREADS": str(threads)})
     save("lanczos_n12_2s33_lz0_coulomb_basic.npz", cmd + " (REF_THREADS=%d)" % threads, v=v, seed=0, precision=1e-13,
          **read_lanczos(lf))
+
+
+def read_sectors(path):
+    # text, one line per sector: 2Lz dim E0 iterations converged method
+    rows = [l.split() for l in open(path) if l.strip()]
+    rows.sort(key=lambda r: int(r[0]))
+    return dict(two_lz=np.array([int(r[0]) for r in rows], np.int32), dims=np.array([int(r[1]) for r in rows], np.int64),
+                e0=np.array([float(r[2]) for r in rows]), iterations=np.array([int(r[3]) for r in rows], np.int32),
+                converged=np.array([int(r[4]) for r in rows], np.int32),
+                method=np.array([r[5] for r in rows]))
+
+
+def sectors_fixture(tmp, out=None):
+    # the batching workload: N = 10, 2S = 27, every sector 2Lz = 0..180, V_1 = 1 and V_3, V_5, V_7
+    # uniform in [0, 0.5) from splitmix64 seed 1; the reference's block Lanczos (k = 4, its own random
+    # start, stopping at 1e-13) per sector, full diagonalisation below 300 states (about 15 minutes
+    # on 8 threads)
+    v = np.zeros(28)
+    v[1] = 1.0
+    v[[3, 5, 7]] = uniform(1, 3, 0.0, 0.5)
+    vf = os.path.join(tmp, "v27.bin")
+    v.tofile(vf)
+    out = out or os.path.join(tmp, "sectors.txt")
+    threads = os.cpu_count() or 1
+    cmd = run("fqhe_sectors", 10, 27, vf, 4, 2000, 1e-13, 300, out, env={"REF_THREADS": str(threads)})
+    save("sectors_n10_2s27_block4.npz", cmd + " (REF_THREADS=%d)" % threads, v=v, block=4, precision=1e-13,
+         full_diag=300, **read_sectors(out))
+
+
+def product_fixture_n12_2s33(tmp):
+    # the precision workload's full product: y = H x for the splitmix64 seed-5 vector, computed by the
+    # reference's SMP product (non-hermitian LowLevelMultiply split over threads); 62 MB, so only a
+    # strided sample of y (every 997th entry), its norm and its dot products with two more seeded
+    # vectors are kept (about a minute on 8 threads)
+    v = coulomb_odd(33, tmp)
+    vf = os.path.join(tmp, "vv.bin")
+    v.tofile(vf)
+    dim = 7764392
+    xf = os.path.join(tmp, "x5.vec")
+    write_vector(xf, splitmix_vector(5, dim))
+    yf = os.path.join(tmp, "y5.vec")
+    threads = os.cpu_count() or 1
+    cmd = run("fqhe_matvec", 12, 33, 0, vf, xf, 0.0, yf, env={"REF_THREADS": str(threads)})
+    y = read_vector(yf)
+    stride = 997
+    save("product_n12_2s33_lz0_coulomb_seed5.npz", cmd + " (REF_THREADS=%d)" % threads, v=v, seed=5, stride=stride,
+         sample=y[::stride].copy(), norm=np.linalg.norm(y), max_abs=np.max(np.abs(y)),
+         dot_seed6=float(np.dot(y, splitmix_vector(6, dim))), dot_seed7=float(np.dot(y, splitmix_vector(7, dim))),
+         x_dot_y=float(np.dot(y, splitmix_vector(5, dim))))
 
 
 def gradient_fixtures(tmp):
@@ -704,6 +754,10 @@ def main():
             translation_complex_fixtures(tmp)
         if args.slow:
             slow_fixtures(tmp)
+        if args.slow or args.only == "product_n12":
+            product_fixture_n12_2s33(tmp)
+        if args.slow or args.only == "sectors_n10":
+            sectors_fixture(tmp)
 
 
 if __name__ == "__main__":

@@ -1,9 +1,10 @@
 """The allocation-free pseudopotential adjoint, called through the C ABI.
 
-Some callers cannot allocate device memory (code inside a CUDA stream capture, applications
-whose framework owns all device memory); dh_hamiltonian_pseudopotential_adjoint_static serves them
+Some callers cannot allocate device memory (applications whose framework owns all device memory
+through its own allocator or arena); dh_hamiltonian_pseudopotential_adjoint_static serves them
 with a static device scratch array.  It must give the allocating entry point's result (same
-1e-12 tolerance as the other adjoint tests) on consecutive calls, which reuse the array.
+1e-12 tolerance as the other adjoint tests) on consecutive calls, which reuse the array, in both
+index modes, and must leave the device's free memory unchanged once its module is loaded.
 This file is collected last so that a failure here comes after every other test has run.
 """
 import ctypes
@@ -25,11 +26,13 @@ def _entry(gpu):
     return lib, fn
 
 
-def test_static_adjoint_matches_allocating_entry_point(gpu, orc):
+@pytest.mark.parametrize("mode", ["rank", "lookup"])
+def test_static_adjoint_matches_allocating_entry_point(gpu, orc, mode):
     import torch
     lib, fn = _entry(gpu)
     v = golden("matvec_n8_2s21_lz0_coulomb_shift0.npz")["v"]
     sp = gpu.FermionOnSphere(8, 0, 21)
+    sp.set_index_mode(mode)
     H = gpu.ParticleOnSphereGenericHamiltonian(sp, 8, 21, v)
     for call in range(2):
         u = torch.tensor(orc.random_vector(40 + call, sp.dim), device="cuda")
@@ -45,6 +48,25 @@ def test_static_adjoint_matches_allocating_entry_point(gpu, orc):
     rc = fn(H._handle, ctypes.c_void_p(u.data_ptr()), ctypes.c_void_p(w.data_ptr()), ctypes.c_void_p(out_dev.data_ptr()))
     assert rc == 0, lib.dh_last_error()
     assert np.max(np.abs(out_dev.cpu().numpy() - ref)) < 1e-12
+
+
+def test_static_adjoint_leaves_free_memory_unchanged(gpu, orc):
+    import torch
+    lib, fn = _entry(gpu)
+    v = golden("matvec_n8_2s21_lz0_coulomb_shift0.npz")["v"]
+    sp = gpu.FermionOnSphere(8, 0, 21)
+    H = gpu.ParticleOnSphereGenericHamiltonian(sp, 8, 21, v)
+    u = torch.tensor(orc.random_vector(60, sp.dim), device="cuda")
+    w = torch.tensor(orc.random_vector(61, sp.dim), device="cuda")
+    out = np.zeros(22, np.float64)
+    args = (H._handle, ctypes.c_void_p(u.data_ptr()), ctypes.c_void_p(w.data_ptr()), ctypes.c_void_p(out.ctypes.data))
+    assert fn(*args) == 0, lib.dh_last_error()  # loads the kernels' module and looks up the array
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        assert fn(*args) == 0, lib.dh_last_error()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
 
 
 def test_static_adjoint_rejects_what_it_cannot_hold(gpu, orc):
