@@ -759,7 +759,8 @@ def stored_elements(dh, H, flush, dim):
     res.update(built=on, bytes=nbytes, build_seconds=time.perf_counter() - t0)
     if not on:
         return res
-    for prec, k in (("fp64", 1), ("fp32", 1), ("fp32", BLOCK)):
+    stream_bytes = nbytes
+    for prec, k in (("fp64", 1), ("fp32", 1), ("fp32", BLOCK), ("fp64", BLOCK)):
         H.set_precision(prec)
         x = torch.rand(dim, k, dtype=torch.float64, device="cuda") - 0.5
         y = torch.empty_like(x)
@@ -774,6 +775,9 @@ def stored_elements(dh, H, flush, dim):
             torch.cuda.synchronize()
             ms.append(a.elapsed_time(b))
         res["%s_k%d_ms" % (prec, k)] = statistics.median(ms)
+        # the stored structure streamed once per product (element targets and indices, the per-row
+        # slice data and diagonal), against the measured HBM bandwidth
+        res["%s_k%d_stream_gbs" % (prec, k)] = stream_bytes / (statistics.median(ms) / 1000.0) / 1e9
     H.set_precision("fp32")
     t = H.autotune(block_size=BLOCK, repeats=3)
     res["autotuned_k%d" % BLOCK] = {"stored_ms": t["stored_ms"], "best_ms": t["best_ms"],
@@ -839,6 +843,12 @@ def run_b200(args, world, rank, local):
         flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
         if args.leg == "long":
             r = long_product(dh, flush, steps=args.steps, warmup=args.warmup)
+        elif args.leg == "stored":
+            sp_ = dh.FermionOnSphere(N_FERMIONS, TWO_LZ, TWO_S)
+            H_ = dh.ParticleOnSphereGenericHamiltonian(sp_, N_FERMIONS, TWO_S, pseudopotentials(dh))
+            H_.set_stream(stream.cuda_stream)
+            H_.set_precision("fp32")
+            r = stored_elements(dh, H_, flush, sp_.dim)
         elif args.leg == "momentum":
             r = momentum_sector(dh, flush, steps=args.steps, length=args.chain_length or 32, warmup=args.warmup,
                                 solve=not args.no_solve)
@@ -1036,9 +1046,10 @@ def main():
                     help="with --kernel-only: the arithmetic of the timed block products")
     ap.add_argument("--chain-length", type=int, default=0,
                     help="with --kernel-only: time the J1-J2 chain block product (k = 2) at this length instead")
-    ap.add_argument("--leg", default=None, choices=["long", "momentum", "bosons"],
+    ap.add_argument("--leg", default=None, choices=["long", "momentum", "bosons", "stored"],
                     help="run one secondary measurement alone and print its JSON (FermionOnSphereLong N=6 2S=63; "
-                         "the momentum sector at --chain-length, 32 by default; BosonOnSphereShort N=12 2S=22)")
+                         "the momentum sector at --chain-length, 32 by default; BosonOnSphereShort N=12 2S=22; "
+                         "the stored-element product of the N=12 2S=33 sector)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -29,6 +29,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libdiagham_b200.so")
 
 DH_OK = 0
+# launch forms of the split-word FQHE kernel (dh_hamiltonian_autotune's last result)
+SPLIT_FORMS = ["256x4", "256x3", "256x3 pipelined", "256x2 pipelined", "128x8", "256x2", "192x4", "128x6"]
 DH_INDEX_RANK = 0
 DH_INDEX_LOOKUP = 1
 DH_PRECISION_FP64 = 0
@@ -61,6 +63,7 @@ SIGNATURES = {
     "dh_complex_vector_read": ([ctypes.c_char_p, _vp, _c_i64], _c_int),
     "dh_space_find_state_index_long": ([_vp, _vp, _c_i64, _vp], _c_int),
     "dh_space_set_index_mode": ([_vp, _c_int], _c_int),
+    "dh_space_set_split_form": ([_vp, _c_int], _c_int),
     "dh_fermion_on_sphere_partial_entanglement_matrix": ([_vp, _vp, _c_int, _c_int, _c_int, _vp, _c_i64, _i64p, _i64p],
                                                          _c_int),
     "dh_fermion_on_sphere_partial_density_matrix": ([_vp, _vp, _c_int, _c_int, _c_int, _vp, _c_i64, _i64p], _c_int),
@@ -217,6 +220,11 @@ class _Space:
     def set_index_mode(self, mode):
         m = {"rank": DH_INDEX_RANK, "lookup": DH_INDEX_LOOKUP}.get(mode, mode)
         _check(_lib.dh_space_set_index_mode(self._handle, m))
+
+    def set_split_form(self, form):
+        """Launch form of the split-word product kernel (an index into SPLIT_FORMS or its name)."""
+        f = SPLIT_FORMS.index(form) if isinstance(form, str) else int(form)
+        _check(_lib.dh_space_set_split_form(self._handle, f))
 
     def __del__(self):
         if self._handle and _lib is not None:
@@ -404,11 +412,11 @@ class _Hamiltonian:
 
     def autotune(self, block_size=1, repeats=3):
         """Time the product's kernel forms on this Hamiltonian and keep the fastest one."""
-        out = np.zeros(9, np.float64)
+        out = np.zeros(10, np.float64)
         _check(_lib.dh_hamiltonian_autotune(self._handle, block_size, repeats, out.ctypes.data))
         return dict(best_ms=out[0], kernel_variant={0: "split", 1: "generic", 2: "split+smem"}[int(out[1])],
                     low_bits=int(out[2]), ms_k1=out[3], ms_k2=out[4], ms_k4=out[5], candidates=int(out[6]),
-                    stored_ms=out[7], stored_in_use=bool(out[8]))
+                    stored_ms=out[7], stored_in_use=bool(out[8]), launch_form=SPLIT_FORMS[int(out[9])])
 
     def count_elements(self):
         """Elements one product generates (moves incl. diagonal ones; spin flips)."""

@@ -231,6 +231,7 @@ FqheDevice fqhe_device(const dh_space_s* sp, const dh_hamiltonian_s* h, int prec
   f.lookup_bits = sp->lookup_bits;
   f.index_mode = sp->index_mode;
   f.kernel_variant = sp->kernel_variant;
+  f.split_form = sp->split_form;
   f.boson_lz_max = sp->boson_lz_max;
   f.nbr_bosons = (sp->kind == SPACE_BOSON) ? sp->nbr_fermions : 0;
   f.nbr_particles = sp->nbr_fermions;
@@ -788,6 +789,14 @@ int dh_space_set_index_mode(dh_space_t sp, int mode) {
   return DH_OK;
 }
 
+int dh_space_set_split_form(dh_space_t sp, int form) {
+  DH_CHECK(sp, DH_ERR_ARGUMENT, "null space");
+  DH_CHECK(form >= 0 && form < kNbrSplitForms && kNbrSplitForms == DH_SPLIT_FORMS, DH_ERR_ARGUMENT,
+           "launch form %d not in 0..%d", form, kNbrSplitForms - 1);
+  sp->split_form = form;
+  return DH_OK;
+}
+
 int dh_space_find_state_index(dh_space_t sp, const uint64_t* words, int64_t n, int64_t* indices) {
   DH_CHECK(sp && words && indices, DH_ERR_ARGUMENT, "null argument");
   if (n <= 0) return DH_OK;
@@ -1007,6 +1016,7 @@ int dh_hamiltonian_enable_fast_multiplication(dh_hamiltonian_t h, int64_t allowe
   for (long long sl = 0; sl < nslices; ++sl) {
     int mx = 0;
     for (long long r = sl * 32; r < std::min(dim, sl * 32 + 32); ++r) mx = std::max(mx, counts[r]);
+    mx = (mx + kEllChunk - 1) / kEllChunk * kEllChunk;  // the product reads whole chunks
     slice_ptr[sl] = total;
     slice_len[sl] = mx;
     total += 32ll * mx;
@@ -1246,6 +1256,7 @@ int dh_hamiltonian_autotune(dh_hamiltonian_t h, int block_size, int repeats, dou
   double best = 1e300;
   int best_variant = sp->kernel_variant, best_lb = sp->rank.low_bits, tried = 0;
   h->fast_use = false;  // the on-the-fly forms first
+  sp->split_form = 0;
   if (sp->kind == SPACE_FERMION && sp->index_mode == DH_INDEX_RANK) {
     const int L = sp->lz_max;
     const int lb0 = (L + 2) / 2;
@@ -1268,6 +1279,22 @@ int dh_hamiltonian_autotune(dh_hamiltonian_t h, int block_size, int repeats, dou
     }
     sp->kernel_variant = best_variant;
     if ((rc = build_rank_tables(sp, best_lb)) != DH_OK) return rc;
+    // launch forms of the split-word kernel (threads per block, register budget, gather pipeline)
+    // at the chosen split
+    if (best_variant == 0) {
+      int best_form = 0;
+      for (int form = 1; form < kNbrSplitForms; ++form) {
+        sp->split_form = form;
+        double ms = 0.0;
+        if ((rc = time_one(block_size, &ms)) != DH_OK) return rc;
+        ++tried;
+        if (ms < best) {
+          best = ms;
+          best_form = form;
+        }
+      }
+      sp->split_form = best_form;
+    }
   } else {
     if ((rc = time_one(block_size, &best)) != DH_OK) return rc;
     tried = 1;
@@ -1295,6 +1322,7 @@ int dh_hamiltonian_autotune(dh_hamiltonian_t h, int block_size, int repeats, dou
     out[4] = per_k[1];
     out[5] = per_k[2];
     out[6] = tried;
+    out[9] = sp->kind == SPACE_FERMION ? sp->split_form : 0;
   }
   return DH_OK;
 }

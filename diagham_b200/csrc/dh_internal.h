@@ -97,6 +97,10 @@ struct FermionRankTables {
 };
 
 // ------------------------------------------------------ kernel launchers
+// Launch forms of the split-word FQHE product kernel (threads per block, register budget, gather
+// pipeline depth), chosen per space by dh_hamiltonian_autotune.
+constexpr int kNbrSplitForms = 8;
+
 struct FqheDevice {
   const uint64_t* words;
   const uint16_t* low_rank;
@@ -113,6 +117,7 @@ struct FqheDevice {
   int nbr_factors;
   int index_mode;              // DH_INDEX_RANK or DH_INDEX_LOOKUP
   int kernel_variant;          // 0: split-word rank kernel, 1: generic kernel (rank mode)
+  int split_form;              // launch form of the split-word kernel (0 .. kNbrSplitForms - 1)
   int boson_lz_max;            // BosonOnSphereShort: orbitals 0..boson_lz_max (words of lz_max + 1 bits)
   int nbr_bosons;
   // words beyond the split-word tables (BosonOnSphereShort with lz_max + N - 1 > 40): ranks from the
@@ -134,6 +139,16 @@ struct FqheLongDevice {
   int stride_o;                 // total_sum + 1
   int nbr_fermions, lz_max, total_sum;
 };
+
+#ifdef __CUDACC__
+// One 32-byte row (four doubles) in a single 256-bit load (sm_100 vector width), through the
+// read-only path without allocating in L1.  p must be 32-byte aligned.
+__device__ __forceinline__ void ldg_row32_no_l1(const double* p, double (&v)[4]) {
+  asm("ld.global.nc.L1::no_allocate.v4.f64 {%0, %1, %2, %3}, [%4];"
+      : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+      : "l"(p));
+}
+#endif
 
 struct MatvecArgs {
   const void* x;       // gather source: element (i, j) at x[i * ld + j * vstride]
@@ -212,9 +227,13 @@ int launch_fqhe_count(const FqheDevice& f, unsigned long long* total, cudaStream
 int launch_fqhe_find(const FqheDevice& f, const uint64_t* words, long long n, long long* out, cudaStream_t s);
 
 // Stored elements of an FQHE Hamiltonian (sliced ELL, 32-row slices; see kernels_fast.cu)
+// Stored elements: per-row lengths of a slice are padded to a multiple of kEllChunk; within a slice a
+// row's elements come in groups of kEllGroup (one 16-byte load of targets per lane).
+constexpr int kEllChunk = 8;
+constexpr int kEllGroup = 4;
 struct EllDevice {
-  const long long* slice_ptr;  // [nslices] first element of each slice
-  const int* slice_len;        // [nslices] elements per row of the slice (padded)
+  const long long* slice_ptr;  // [nslices] first element of each slice (a multiple of 32 * kEllChunk)
+  const int* slice_len;        // [nslices] elements per row of the slice (padded to a multiple of kEllChunk)
   const int* cols;             // target index of each element
   const uint16_t* coef;        // factor index | sign << 15; padding holds nbr_factors (a zero factor)
   const void* diag;            // [dim] diagonal, FP64 or FP32 like the factors

@@ -23,6 +23,7 @@ struct dh_space_s {
   int64_t dim = 0;
   int index_mode = DH_INDEX_RANK;
   int kernel_variant = 0;  // product kernel of the rank mode (0 split-word, 1 generic, 2 split + smem table)
+  int split_form = 0;      // launch form of the split-word kernel (the autotuner's choice)
   int requested_low_bits = 0;
   std::vector<int64_t> counts;  // [n][o][s]: n fermions in orbitals 0..o-1 with orbital-index sum s
   dh::DevBuf words;  // uint64 FermionOnSphere words, uint32 spin words (chain bits only)

@@ -5,11 +5,13 @@
 // (AbstractQHEOnSphereHamiltonian::EnableFastMultiplication / FastMultiplicationMemory,
 // AbstractQHEOnSphereHamiltonian.cc:3625,3814; QHEParticlePrecalculationOperation.cc:95).  Here the
 // lists are kept in device memory as sliced ELL: rows are grouped in slices of 32 consecutive rows
-// (one warp), every row of a slice is padded to the slice's longest row, and element j of the
-// slice's 32 rows is stored contiguously, so that a warp reads one coalesced run per element.
-// Each element is an int32 target and a uint16 factor index with the fermionic sign in bit 15; the
-// structure does not depend on the pseudopotentials.  Diagonal moves are summed per row into a
-// separate diagonal array, recomputed when the pseudopotentials change.
+// (one warp), every row of a slice is padded to the slice's longest row rounded up to a multiple of
+// kEllChunk, and the slice is stored in groups of kEllGroup elements per row: element j of lane l
+// sits at slice_ptr + (j / G) * 32 G + l G + j % G, so one 16-byte load gives a lane G targets and
+// a warp reads 512 contiguous bytes per load.  Each element is an int32 target and a uint16 factor
+// index with the fermionic sign in bit 15; the structure does not depend on the pseudopotentials.
+// Diagonal moves are summed per row into a separate diagonal array, recomputed when the
+// pseudopotentials change.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -19,6 +21,10 @@ namespace dh {
 namespace {
 
 constexpr int kFastThreads = 256;
+
+__device__ __forceinline__ long long ell_pos(long long slice_base, int lane, int j) {
+  return slice_base + (long long)(j / kEllGroup) * (32 * kEllGroup) + lane * kEllGroup + (j % kEllGroup);
+}
 
 __device__ __forceinline__ uint64_t bits_between(int lo, int hi) {
   // bits strictly between lo and hi (lo < hi <= 63)
@@ -94,17 +100,20 @@ __global__ void ell_fill_kernel(FqheDevice f, const long long* slice_ptr, const 
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
     const long long sl = r >> 5;
-    const long long base = slice_ptr[sl] + (r & 31);
+    const long long base = slice_ptr[sl];
     const int len = slice_len[sl];
+    const int lane = (int)(r & 31);
     int j = 0;
     visit_row(f, __ldg(f.words + r), [&](int idx, int fidx, bool neg) {
-      cols[base + (long long)j * 32] = idx;
-      coef[base + (long long)j * 32] = (uint16_t)(fidx | (neg ? 0x8000 : 0));
+      const long long p = ell_pos(base, lane, j);
+      cols[p] = idx;
+      coef[p] = (uint16_t)(fidx | (neg ? 0x8000 : 0));
       ++j;
     });
     for (; j < len; ++j) {  // padding: the row itself times a zero factor
-      cols[base + (long long)j * 32] = (int)r;
-      coef[base + (long long)j * 32] = (uint16_t)f.nbr_factors;
+      const long long p = ell_pos(base, lane, j);
+      cols[p] = (int)r;
+      coef[p] = (uint16_t)f.nbr_factors;
     }
   }
 }
@@ -132,9 +141,11 @@ __global__ void diag_kernel(FqheDevice f, const double* factors, double* diag64,
   }
 }
 
-template <typename TG, int K, bool IL>
+template <typename TG, int K, bool IL, bool W256 = false>
 __device__ __forceinline__ void gather(const TG* x, const MatvecArgs& a, long long idx, TG (&v)[K]) {
-  if constexpr (IL && sizeof(TG) == 4 && K == 4) {
+  if constexpr (W256 && IL && sizeof(TG) == 8 && K == 4) {
+    ldg_row32_no_l1(reinterpret_cast<const double*>(x + idx * 4), *reinterpret_cast<double(*)[4]>(&v));
+  } else if constexpr (IL && sizeof(TG) == 4 && K == 4) {
     const float4 q = __ldg(reinterpret_cast<const float4*>(x + idx * 4));
     v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
   } else if constexpr (IL && sizeof(TG) == 4 && K == 2) {
@@ -154,10 +165,13 @@ __device__ __forceinline__ void gather(const TG* x, const MatvecArgs& a, long lo
   }
 }
 
-// y = H x from the stored elements: lanes own the 32 rows of a slice; the element stream, the
-// diagonal and y go through L2 with streaming (evict-first) accesses so that the gathered x keeps
-// the cache
-template <typename TG, int K, bool IL>
+// y = H x from the stored elements: lanes own the 32 rows of a slice.  The element stream is read
+// kEllChunk elements ahead of the gathers (two 16-byte target loads and two 8-byte index loads per
+// lane per chunk, issued before the chunk in hand is gathered), so every warp keeps a chunk of the
+// stream and a chunk of gathers in flight.  The stream, the diagonal and y go through L2 with
+// streaming (evict-first) accesses so that the gathered x keeps the cache.
+// W256: FP64 rows of 4 that are 32-byte aligned, gathered with one 256-bit load each
+template <typename TG, int K, bool IL, bool W256 = false>
 __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, MatvecArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   TG* sfac = reinterpret_cast<TG*>(smem);
@@ -168,6 +182,7 @@ __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, 
   const TG* x = static_cast<const TG*>(a.x);
   const TG* diag = static_cast<const TG*>(e.diag);
   const int lane = threadIdx.x & 31;
+  constexpr int NG = kEllChunk / kEllGroup;  // 16-byte target groups per chunk
   // a row range starts on a slice boundary (callers split at multiples of 32 rows)
   const long long r_end = a.out_last > 0 ? a.out_last : e.dim;
   const long long nslices = (r_end + 31) >> 5;
@@ -175,39 +190,59 @@ __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, 
   for (long long sl = (a.out_first >> 5) + (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5); sl < nslices;
        sl += nwarps) {
     const long long r = sl * 32 + lane;
-    if (r >= r_end) continue;
-    const long long base = e.slice_ptr[sl] + lane;
+    if (r >= r_end) continue;  // the last slice's lanes beyond the space hold no elements
     const int len = e.slice_len[sl];
+    const int4* cg = reinterpret_cast<const int4*>(e.cols + e.slice_ptr[sl]) + lane;
+    const uint2* kg = reinterpret_cast<const uint2*>(e.coef + e.slice_ptr[sl]) + lane;
     TG acc[K];
 #pragma unroll
     for (int q = 0; q < K; ++q) acc[q] = TG(0);
-    int j = 0;
-    for (; j + 1 < len; j += 2) {
-      const long long pa = base + (long long)j * 32, pb = pa + 32;
-      const int ca = __ldcs(e.cols + pa), cb = __ldcs(e.cols + pb);
-      const unsigned short ka = __ldcs(e.coef + pa), kb = __ldcs(e.coef + pb);
-      TG fa = sfac[ka & 0x7fff], fb = sfac[kb & 0x7fff];
-      if (ka & 0x8000) fa = -fa;
-      if (kb & 0x8000) fb = -fb;
-      TG xa[K], xb[K];
-      gather<TG, K, IL>(x, a, ca, xa);
-      gather<TG, K, IL>(x, a, cb, xb);
+    int4 c[NG];
+    uint2 k[NG];
+    if (len > 0) {
 #pragma unroll
-      for (int q = 0; q < K; ++q) acc[q] += fa * xa[q] + fb * xb[q];
+      for (int g = 0; g < NG; ++g) {
+        c[g] = __ldcs(cg + g * 32);
+        k[g] = __ldcs(kg + g * 32);
+      }
     }
-    if (j < len) {
-      const long long pa = base + (long long)j * 32;
-      const int ca = __ldcs(e.cols + pa);
-      const unsigned short ka = __ldcs(e.coef + pa);
-      TG fa = sfac[ka & 0x7fff];
-      if (ka & 0x8000) fa = -fa;
-      TG xa[K];
-      gather<TG, K, IL>(x, a, ca, xa);
+    for (int j = 0; j < len; j += kEllChunk) {
+      int4 cn[NG];
+      uint2 kn[NG];
+      const bool more = j + kEllChunk < len;
+      if (more) {
+        const int gn = (j + kEllChunk) / kEllGroup;
 #pragma unroll
-      for (int q = 0; q < K; ++q) acc[q] += fa * xa[q];
+        for (int g = 0; g < NG; ++g) {
+          cn[g] = __ldcs(cg + (gn + g) * 32);
+          kn[g] = __ldcs(kg + (gn + g) * 32);
+        }
+      }
+#pragma unroll
+      for (int g = 0; g < NG; ++g) {
+        const int cols[4] = {c[g].x, c[g].y, c[g].z, c[g].w};
+        const unsigned ks[4] = {k[g].x & 0xffffu, k[g].x >> 16, k[g].y & 0xffffu, k[g].y >> 16};
+        TG xv[4][K];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) gather<TG, K, IL, W256>(x, a, cols[u], xv[u]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          TG fu = sfac[ks[u] & 0x7fffu];
+          if (ks[u] & 0x8000u) fu = -fu;
+#pragma unroll
+          for (int q = 0; q < K; ++q) acc[q] += fu * xv[u][q];
+        }
+      }
+      if (more) {
+#pragma unroll
+        for (int g = 0; g < NG; ++g) {
+          c[g] = cn[g];
+          k[g] = kn[g];
+        }
+      }
     }
     TG xr[K];
-    gather<TG, K, IL>(x, a, r, xr);
+    gather<TG, K, IL, W256>(x, a, r, xr);
     const TG d = __ldcs(diag + r);
 #pragma unroll
     for (int q = 0; q < K; ++q) acc[q] += d * xr[q];
@@ -234,6 +269,8 @@ unsigned grid_for(long long n) {
 template <typename TG, int K, bool IL>
 int launch_ell_typed(const EllDevice& e, const MatvecArgs& a, cudaStream_t s) {
   auto kern = ell_product_kernel<TG, K, IL>;
+  if constexpr (IL && sizeof(TG) == 8 && K == 4)
+    if ((reinterpret_cast<uintptr_t>(a.x) & 31) == 0) kern = ell_product_kernel<TG, K, IL, true>;
   const int smem = (e.nbr_factors + 1) * (int)sizeof(TG);
   if (smem > 48 * 1024) DH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int dev = 0, sms = 0, per_sm = 0;

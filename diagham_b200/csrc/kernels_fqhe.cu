@@ -178,12 +178,16 @@ __device__ __forceinline__ uint32_t between32(int lo, int hi) {
   return upto & ~((2u << lo) - 1u);
 }
 
-// K gathered values of target row idx: interleaved blocks ([row][K], IL) load them as one vector
-template <typename TG, int K, bool IL>
+// K gathered values of target row idx: interleaved blocks ([row][K], IL) load them as one vector.
+// W256: the FP64 block of 4 with 32-byte aligned rows, one 256-bit load per row that bypasses L1
+// (the 248 MB block at N=12, 2S=33 does not fit L1 or L2; L1 is left to the rank tables)
+template <typename TG, int K, bool IL, bool W256 = false>
 __device__ __forceinline__ void load_row(const TG* x, const MatvecArgs& a, int idx, TG (&v)[K]) {
   if constexpr (IL) {
     const TG* p = x + (long long)idx * K;
-    if constexpr (sizeof(TG) == 4 && K == 4) {
+    if constexpr (W256 && sizeof(TG) == 8 && K == 4) {
+      ldg_row32_no_l1(reinterpret_cast<const double*>(p), *reinterpret_cast<double(*)[4]>(&v));
+    } else if constexpr (sizeof(TG) == 4 && K == 4) {
       // the FP32 block of 4 (124 MB at N=12, 2S=33) lives in L2: its gathers skip L1, which keeps L1
       // for the rank tables (9.60-9.65 ms per step against 9.68-9.75 ms with cached gathers)
       const float4 q = __ldcg(reinterpret_cast<const float4*>(p));
@@ -213,19 +217,47 @@ __device__ __forceinline__ void load_row(const TG* x, const MatvecArgs& a, int i
   }
 }
 
-template <typename TG, int K, bool RANGE, bool IL>
-__device__ __forceinline__ void accumulate2(TG (&acc)[K], const TG* x, const MatvecArgs& a, int ia, TG fa, int ib,
-                                            TG fb) {
-  if (RANGE) {
-    if (ia < a.col_first || ia >= a.col_last) fa = TG(0);
-    if (ib < a.col_first || ib >= a.col_last) fb = TG(0);
-  }
-  TG xa[K], xb[K];
-  load_row<TG, K, IL>(x, a, ia, xa);
-  load_row<TG, K, IL>(x, a, ib, xb);
+// The gathers of a row's elements, two targets per call.  PIPE: the two loads of a call are issued
+// before the previous call's values are used, so four target rows are in flight per thread; the
+// pairs are added in the same order either way (identical results).
+template <typename TG, int K, bool RANGE, bool IL, bool W256, bool PIPE>
+struct Gatherer {
+  TG pa[K], pb[K];
+  TG pfa, pfb;
+  __device__ __forceinline__ Gatherer() : pfa(TG(0)), pfb(TG(0)) {
 #pragma unroll
-  for (int j = 0; j < K; ++j) acc[j] += fa * xa[j] + fb * xb[j];
-}
+    for (int j = 0; j < K; ++j) pa[j] = pb[j] = TG(0);
+  }
+  __device__ __forceinline__ void add2(TG (&acc)[K], const TG* x, const MatvecArgs& a, int ia, TG fa, int ib, TG fb) {
+    if (RANGE) {
+      if (ia < a.col_first || ia >= a.col_last) fa = TG(0);
+      if (ib < a.col_first || ib >= a.col_last) fb = TG(0);
+    }
+    TG xa[K], xb[K];
+    load_row<TG, K, IL, W256>(x, a, ia, xa);
+    load_row<TG, K, IL, W256>(x, a, ib, xb);
+    if constexpr (PIPE) {
+#pragma unroll
+      for (int j = 0; j < K; ++j) acc[j] += pfa * pa[j] + pfb * pb[j];
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
+        pa[j] = xa[j];
+        pb[j] = xb[j];
+      }
+      pfa = fa;
+      pfb = fb;
+    } else {
+#pragma unroll
+      for (int j = 0; j < K; ++j) acc[j] += fa * xa[j] + fb * xb[j];
+    }
+  }
+  __device__ __forceinline__ void finish(TG (&acc)[K]) {
+    if constexpr (PIPE) {
+#pragma unroll
+      for (int j = 0; j < K; ++j) acc[j] += pfa * pa[j] + pfb * pb[j];
+    }
+  }
+};
 
 // the rank tables and words of one sector
 struct SplitTables {
@@ -238,9 +270,10 @@ struct SplitTables {
 
 // Off-diagonal elements of row r accumulated into acc (K vectors) and the sum of its diagonal
 // factors into dsum; the caller adds dsum * x[r] and the shift.
-template <typename TG, int K, bool RANGE, bool IL>
+template <typename TG, int K, bool RANGE, bool IL, bool W256 = false, bool PIPE = false>
 __device__ __forceinline__ void split_row(const SplitTables& t, const TG* sfac, const int* spair, long long r,
                                           const TG* x, const MatvecArgs& a, TG (&acc)[K], TG& dsum) {
+  Gatherer<TG, K, RANGE, IL, W256, PIPE> g;
   const int LB = t.LB;
   const uint32_t lmask = (1u << LB) - 1u;
   const int32_t* __restrict__ HO = t.HO;
@@ -309,7 +342,7 @@ __device__ __forceinline__ void split_row(const SplitTables& t, const TG* sfac, 
           TG fa = fp[m3a], fb = two ? fp[m3b] : TG(0);
           if ((paa + __popc(anl & between32(m4a, m3a))) & 1) fa = -fa;
           if ((paa + __popc(anl & between32(m4b, m3b))) & 1) fb = -fb;
-          accumulate2<TG, K, RANGE, IL>(acc, x, a, ia, fa, ib, fb);
+          g.add2(acc, x, a, ia, fa, ib, fb);
         }
       }
       if (vh) {
@@ -328,7 +361,7 @@ __device__ __forceinline__ void split_row(const SplitTables& t, const TG* sfac, 
           TG fa = fph[ha3], fb = two ? fph[hb3] : TG(0);
           if ((paa + __popc(anh & between32(ha4, ha3))) & 1) fa = -fa;
           if ((paa + __popc(anh & between32(hb4, hb3))) & 1) fb = -fb;
-          accumulate2<TG, K, RANGE, IL>(acc, x, a, ia, fa, ib, fb);
+          g.add2(acc, x, a, ia, fa, ib, fb);
         }
       }
       if (vm) {
@@ -349,20 +382,32 @@ __device__ __forceinline__ void split_row(const SplitTables& t, const TG* sfac, 
           const int pb = __popc(anl & between32(m4b, LB)) + __popc(anh & ((1u << hb3) - 1u));
           if ((paa + pa) & 1) fa = -fa;
           if ((paa + pb) & 1) fb = -fb;
-          accumulate2<TG, K, RANGE, IL>(acc, x, a, ia, fa, ib, fb);
+          g.add2(acc, x, a, ia, fa, ib, fb);
         }
       }
     }
   }
+  g.finish(acc);
 }
 
-// four resident blocks per SM: at most 64 registers per thread (a tighter bound of 48 registers for
-// the FP32 single-vector form measured slower)
+// four resident blocks of 256 threads per SM: at most 64 registers per thread (a tighter bound of 48
+// registers for the FP32 single-vector form measured slower)
 constexpr int kSplitMinBlocks = 4;
 
-// IL: the K vectors are row-interleaved ([row][K], ld = K, vstride = 1 for x and y)
-template <typename TG, int K, bool RANGE, bool LR_SMEM, bool IL>
-__global__ void __launch_bounds__(kMatvecThreads, kSplitMinBlocks)
+// Launch forms of the split kernel the autotuner chooses between (threads per block, resident
+// blocks per SM, i.e. the register budget, and the gather pipeline depth).
+struct SplitForm {
+  int threads, min_blocks;
+  bool pipe;
+};
+constexpr SplitForm kSplitForms[kNbrSplitForms] = {
+    {256, 4, false}, {256, 3, false}, {256, 3, true}, {256, 2, true},
+    {128, 8, false}, {256, 2, false}, {192, 4, false}, {128, 6, false}};
+
+// IL: the K vectors are row-interleaved ([row][K], ld = K, vstride = 1 for x and y); W256: and the
+// FP64 rows of 4 are 32-byte aligned (one 256-bit gather per target row); FORM: kSplitForms entry
+template <typename TG, int K, bool RANGE, bool LR_SMEM, bool IL, bool W256 = false, int FORM = 0>
+__global__ void __launch_bounds__(kSplitForms[FORM].threads, kSplitForms[FORM].min_blocks)
     fqhe_split_kernel(FqheDevice f, MatvecArgs a, SmemLayout lay) {
   extern __shared__ __align__(16) unsigned char smem[];
   TG* sfac = reinterpret_cast<TG*>(smem);
@@ -392,10 +437,10 @@ __global__ void __launch_bounds__(kMatvecThreads, kSplitMinBlocks)
 #pragma unroll
     for (int j = 0; j < K; ++j) acc[j] = TG(0);
     TG dsum = TG(0);
-    split_row<TG, K, RANGE, IL>(t, sfac, spair, r, x, a, acc, dsum);
+    split_row<TG, K, RANGE, IL, W256, kSplitForms[FORM].pipe>(t, sfac, spair, r, x, a, acc, dsum);
     if (!RANGE || (r >= a.col_first && r < a.col_last)) {
       TG xr[K];
-      load_row<TG, K, IL>(x, a, (int)r, xr);
+      load_row<TG, K, IL, W256>(x, a, (int)r, xr);
 #pragma unroll
       for (int j = 0; j < K; ++j) acc[j] += dsum * xr[j];
     }
@@ -470,36 +515,64 @@ __global__ void __launch_bounds__(kMatvecThreads) fqhe_sectors_kernel(SectorBatc
   }
 }
 
+using MatvecKernel = void (*)(FqheDevice, MatvecArgs, SmemLayout);
+
+// the split-word kernel of one launch form (full column range, tables read through L1)
+template <typename TG, int K, bool IL, bool W256>
+MatvecKernel split_form_kernel(int form) {
+  switch (form) {
+    case 1: return fqhe_split_kernel<TG, K, false, false, IL, W256, 1>;
+    case 2: return fqhe_split_kernel<TG, K, false, false, IL, W256, 2>;
+    case 3: return fqhe_split_kernel<TG, K, false, false, IL, W256, 3>;
+    case 4: return fqhe_split_kernel<TG, K, false, false, IL, W256, 4>;
+    case 5: return fqhe_split_kernel<TG, K, false, false, IL, W256, 5>;
+    case 6: return fqhe_split_kernel<TG, K, false, false, IL, W256, 6>;
+    case 7: return fqhe_split_kernel<TG, K, false, false, IL, W256, 7>;
+    default: return fqhe_split_kernel<TG, K, false, false, IL, W256, 0>;
+  }
+}
+
 template <typename TG, int K, int MODE, bool RANGE>
 int launch_one(const FqheDevice& f, const MatvecArgs& a, cudaStream_t s) {
   SmemLayout lay = smem_layout(f, sizeof(TG));
-  auto kern = fqhe_matvec_kernel<TG, K, MODE, RANGE>;
+  MatvecKernel kern = fqhe_matvec_kernel<TG, K, MODE, RANGE>;
+  int threads = kMatvecThreads;
   // the split-word form needs both halves of a word in 32 bits; variant 2 stages the low-rank table
   // in shared memory
   if (MODE == DH_INDEX_RANK && f.kernel_variant != 1 && f.low_bits <= 31 && f.lz_max + 1 - f.low_bits <= 31) {
     kern = (f.kernel_variant == 2) ? fqhe_split_kernel<TG, K, RANGE, true, false>
                                    : fqhe_split_kernel<TG, K, RANGE, false, false>;
-    if constexpr (!RANGE && K > 1) {
-      // row-interleaved blocks (block Lanczos): vector loads of the K values of a target row
-      if (f.kernel_variant != 2 && a.ld == K && a.vstride == 1 && a.ld_y == K && a.vstride_y == 1)
-        kern = fqhe_split_kernel<TG, K, false, false, true>;
+    if constexpr (!RANGE) {
+      if (f.kernel_variant != 2) {
+        const int form = (f.split_form >= 0 && f.split_form < kNbrSplitForms) ? f.split_form : 0;
+        kern = split_form_kernel<TG, K, false, false>(form);
+        if constexpr (K > 1) {
+          // row-interleaved blocks (block Lanczos): vector loads of the K values of a target row
+          if (a.ld == K && a.vstride == 1 && a.ld_y == K && a.vstride_y == 1) {
+            kern = split_form_kernel<TG, K, true, false>(form);
+            if constexpr (sizeof(TG) == 8 && K == 4)
+              if ((reinterpret_cast<uintptr_t>(a.x) & 31) == 0) kern = split_form_kernel<TG, K, true, true>(form);
+          }
+        }
+        threads = kSplitForms[form].threads;
+      }
     }
   }
   if (lay.total > 48 * 1024) DH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total));
   int dev = 0, sms = 0, per_sm = 0;
   DH_CUDA(cudaGetDevice(&dev));
   DH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  DH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kMatvecThreads, lay.total));
+  DH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, lay.total));
   if (per_sm < 1) {
     set_error("fqhe matvec: %d bytes of shared memory per block do not fit", lay.total);
     return DH_ERR_UNSUPPORTED;
   }
   const long long rows = (a.out_last > 0 ? a.out_last : f.dim) - a.out_first;
-  long long need = (rows + kMatvecThreads - 1) / kMatvecThreads;
+  long long need = (rows + threads - 1) / threads;
   long long grid = (long long)sms * per_sm;
   if (need < grid) grid = need;
   if (grid < 1) grid = 1;
-  kern<<<(unsigned)grid, kMatvecThreads, lay.total, s>>>(f, a, lay);
+  kern<<<(unsigned)grid, threads, lay.total, s>>>(f, a, lay);
   DH_CUDA(cudaGetLastError());
   return DH_OK;
 }

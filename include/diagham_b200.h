@@ -133,6 +133,12 @@ int dh_space_find_state_index_long(dh_space_t space, const uint64_t* words, int6
  * counterpart: the lookup mode is FindStateIndex's own search (FermionOnSphere.cc:1431). */
 int dh_space_set_index_mode(dh_space_t space, int mode);
 
+/* Launch form (0 .. DH_SPLIT_FORMS - 1) of the split-word product kernel for this space, the choice
+ * dh_hamiltonian_autotune makes by timing (see there); every form gives bit-identical products.
+ * No reference counterpart. */
+#define DH_SPLIT_FORMS 8
+int dh_space_set_split_form(dh_space_t space, int form);
+
 /* FermionOnSphere::EvaluatePartialEntanglementMatrix(subsytemSize, nbrFermionSector, lzSector, state)
  * (FermionOnSphere.cc:2474): the orbital cut A = orbitals 0..subsystem_size-1 of state (host or device,
  * the space's dimension), M[a][b] = component of the basis state a (x) b in the sector of N_A =
@@ -270,11 +276,15 @@ int dh_hamiltonian_disable_fast_multiplication(dh_hamiltonian_t h);
  * same product (the rank function does not depend on the split).  Spin chains have one form.
  * When stored elements exist (dh_hamiltonian_enable_fast_multiplication) their product is timed too
  * and stays in use only if it is the fastest.
+ * For the split-word kernel it then times its launch forms at the chosen split (threads per block
+ * 256, 192 or 128, resident blocks per SM, i.e. the register budget per thread, and a gather pipeline
+ * that keeps four target rows in flight per thread instead of two) and keeps the fastest.
  * out (optional, DH_TUNE_RESULTS doubles): best ms per product, kernel variant (0 split-word,
  * 1 generic, 2 staged table), LB, ms per product of blocks of 1, 2 and 4 vectors with the chosen
  * form, number of candidates timed, ms of the stored-element product (0: none), 1 if the stored
- * elements are in use. */
-#define DH_TUNE_RESULTS 9
+ * elements are in use, launch form of the split-word kernel (0 .. 7: 256 threads x 4 resident
+ * blocks, 256 x 3, 256 x 3 pipelined, 256 x 2 pipelined, 128 x 8, 256 x 2, 192 x 4, 128 x 6). */
+#define DH_TUNE_RESULTS 10
 int dh_hamiltonian_autotune(dh_hamiltonian_t h, int block_size, int repeats, double* out);
 
 /* AbstractHamiltonian::MatrixElement(V1, V2) (AbstractQHEOnSphereHamiltonian.cc:380): <v1|H|v2>. */

@@ -206,3 +206,29 @@ def test_autotune_keeps_parity(gpu, orc, prec):
     assert 0 < r["ms_k1"] and 0 < r["ms_k4"]
     y = H.LowLevelMultiply(x)
     assert np.max(np.abs(y - ref)) <= tol * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("k", [1, 2, 4])
+def test_launch_forms_bit_identical(gpu, orc, precision, k):
+    # every launch form of the split-word kernel (threads per block, register budget, gather
+    # pipeline) computes the same sums in the same order: bit-identical blocks, and the form-0
+    # FP64 product matches the oracle
+    import torch
+    v = golden("matvec_n8_2s21_lz0_coulomb_shift0.npz")["v"]
+    sp = gpu.FermionOnSphere(8, 0, 21)
+    H = gpu.ParticleOnSphereGenericHamiltonian(sp, 8, 21, v)
+    H.set_precision(precision)
+    x = torch.tensor(np.stack([orc.random_vector(70 + j, sp.dim) for j in range(k)], axis=1), device="cuda")
+    ys = []
+    for form in range(len(gpu.SPLIT_FORMS)):
+        sp.set_split_form(form)
+        ys.append(H.block_multiply(x).cpu().numpy())
+    for form in range(1, len(ys)):
+        assert np.array_equal(ys[form], ys[0]), form
+    if precision == "fp64":
+        ref = orc.FQHE(8, 21, 0, v)
+        for j in range(k):
+            assert np.max(np.abs(ys[0][:, j] - ref.pull(x[:, j].cpu().numpy()))) < 1e-12
+    with pytest.raises(Exception):
+        sp.set_split_form(len(gpu.SPLIT_FORMS))
