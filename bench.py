@@ -330,7 +330,7 @@ def splitmix_uniform(seed, n, lo, hi):
     return lo + (hi - lo) * (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
 
 
-def time_to_e0_all_sectors(dh, k=2, runs=3, precisions=(1e-10, 1e-13)):
+def time_to_e0_all_sectors(dh, k=None, runs=3, precisions=(1e-10, 1e-13)):
     """Every Lz sector of N=10, 2S=27 (2Lz = 0..180, 91 sectors) with V1 = 1 and V3, V5, V7 uniform
     in [0, 0.5) from splitmix64 seed 1: the batched block form (FP32 products + FP64 refinement,
     and FP64) against plain FP64 single-vector Lanczos run sector after sector (sectors of
@@ -344,7 +344,16 @@ def time_to_e0_all_sectors(dh, k=2, runs=3, precisions=(1e-10, 1e-13)):
     sectors = list(range(0, 181, 2))
     dims = [dh.FermionOnSphere(n, lz, s).dim for lz in sectors]
     dense = [lz for lz, d in zip(sectors, dims) if d <= 200]
-    out = {"sectors": len(sectors), "total_rows": int(sum(dims)), "largest": int(max(dims)), "block": k}
+    tuned = None
+    if k is None:
+        # the block size from the tuner: time to the refined ground energy of the largest sector
+        sp0 = dh.FermionOnSphere(n, 0, s)
+        H0 = dh.ParticleOnSphereGenericHamiltonian(sp0, n, s, v)
+        k, tk = H0.tune_block_size(max_iter=800, precision=1e-10, refined=True)
+        tuned = {"k": k, "seconds_2lz0_by_k": tk}
+        del H0, sp0
+    out = {"sectors": len(sectors), "total_rows": int(sum(dims)), "largest": int(max(dims)), "block": k,
+           "block_tuned": tuned}
     dh.fqhe_sectors_block_lanczos(n, s, sectors[-12:], v, block_size=k, max_iter=400)  # warm-up
 
     def plain_all(precision):
@@ -487,6 +496,7 @@ def time_to_e0_summary(line):
         if p:
             pl = p["plain_fp64_per_sector"]
             out["n10_2s27_91_sectors"] = {
+                "block_k": tc.get("block"),
                 "plain_fp64_s": round(pl["seconds"], 4),
                 "batched_fp32_refined_s": round(p["batched_fp32_refined"]["seconds"], 4),
                 "batched_fp64_s": round(p["batched_fp64"]["seconds"], 4),
@@ -865,6 +875,8 @@ def run_b200(args, world, rank, local):
         flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
         if args.leg == "long":
             r = long_product(dh, flush, steps=args.steps, warmup=args.warmup)
+        elif args.leg == "sectors":
+            r = time_to_e0_all_sectors(dh, runs=args.steps, precisions=(1e-10,))
         elif args.leg == "stored":
             sp_ = dh.FermionOnSphere(N_FERMIONS, TWO_LZ, TWO_S)
             H_ = dh.ParticleOnSphereGenericHamiltonian(sp_, N_FERMIONS, TWO_S, pseudopotentials(dh))
@@ -1068,10 +1080,11 @@ def main():
                     help="with --kernel-only: the arithmetic of the timed block products")
     ap.add_argument("--chain-length", type=int, default=0,
                     help="with --kernel-only: time the J1-J2 chain block product (k = 2) at this length instead")
-    ap.add_argument("--leg", default=None, choices=["long", "momentum", "bosons", "stored"],
+    ap.add_argument("--leg", default=None, choices=["long", "momentum", "bosons", "stored", "sectors"],
                     help="run one secondary measurement alone and print its JSON (FermionOnSphereLong N=6 2S=63; "
                          "the momentum sector at --chain-length, 32 by default; BosonOnSphereShort N=12 2S=22; "
-                         "the stored-element product of the N=12 2S=33 sector)")
+                         "the stored-element product of the N=12 2S=33 sector; the 91-sector time to E0 at 1e-10, "
+                         "median of --steps runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -106,6 +106,7 @@ SIGNATURES = {
     "dh_lanczos_get_counters": ([_vp, _i64p, _ip], _c_int),
     "dh_lanczos_solve": ([_vp, _c_int, _c_int, _vp, _ip, _ip], _c_int),
     "dh_lanczos_solve_refined": ([_vp, _c_int, _c_dbl, _vp], _c_int),
+    "dh_hamiltonian_tune_block_size": ([_vp, _c_int, _c_dbl, _c_int, _vp, _vp], _c_int),
     "dh_lanczos_set_disk_storage": ([_vp, ctypes.c_char_p, _c_int], _c_int),
     "dh_lanczos_write_state": ([_vp], _c_int),
     "dh_lanczos_resume": ([_vp], _c_int),
@@ -417,6 +418,14 @@ class _Hamiltonian:
         return dict(best_ms=out[0], kernel_variant={0: "split", 1: "generic", 2: "split+smem"}[int(out[1])],
                     low_bits=int(out[2]), ms_k1=out[3], ms_k2=out[4], ms_k4=out[5], candidates=int(out[6]),
                     stored_ms=out[7], stored_in_use=bool(out[8]), launch_form=SPLIT_FORMS[int(out[9])])
+
+    def tune_block_size(self, max_iter=600, precision=1e-10, refined=True):
+        """Block size (1, 2 or 4) with the shortest time to the converged ground energy, and the times."""
+        k = ctypes.c_int(0)
+        t = np.zeros(3, np.float64)
+        _check(_lib.dh_hamiltonian_tune_block_size(self._handle, int(max_iter), float(precision), int(bool(refined)),
+                                                   ctypes.byref(k), t.ctypes.data))
+        return k.value, dict(zip((1, 2, 4), t.tolist()))
 
     def count_elements(self):
         """Elements one product generates (moves incl. diagonal ones; spin flips)."""

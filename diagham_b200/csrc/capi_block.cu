@@ -33,6 +33,7 @@ using namespace dh;
 namespace dh {
 
 constexpr long long kTileRows = 4096;
+constexpr int EngineRing = 8;  // BlockEngine::kRing
 // largest exhausted space diagonalised densely on the host when its band matrix is not exact
 constexpr long long kDenseFallbackLimit = 2048;
 
@@ -76,7 +77,6 @@ struct BlockEngine {
   double* slot[3] = {nullptr, nullptr, nullptr};
   bool have_prev = false;
   std::vector<BlockSector> sec;
-  std::vector<double> bt_host;  // B_i^T of every sector for the next update
   std::function<int(const double*, const float*, double*)> product;
   double product_ms = 0.0;
   long long products = 0;
@@ -91,9 +91,33 @@ struct BlockEngine {
   int store_cap = 0;
   int store_max = 0;     // the store grows (doubling) up to this many blocks while memory allows
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // Device-resident steps (engine_step_async): the per-sector k x k matrices of a step live on the
+  // device; each step's coefficients and flags go back to a pinned record slot asynchronously, and
+  // the host's bookkeeping (engine_process_step) follows the device by a few steps.
+  static const int kRing = 8;                    // record slots (steps in flight at most kRing)
+  DevBuf stepbuf;                                // G, A, Bt[2], R1, R2, inv1, inv2, B, lock, scale, flags, active
+  double *dG = nullptr, *dA = nullptr, *dBt[2] = {nullptr, nullptr}, *dR1 = nullptr, *dR2 = nullptr;
+  double *dInv1 = nullptr, *dInv2 = nullptr, *dB = nullptr, *dLock = nullptr, *dScale = nullptr;
+  int *dFlags = nullptr, *dActive = nullptr;
+  double* rec_host = nullptr;                    // pinned [kRing][6][nsec][k][k]
+  int* rec_flags = nullptr;                      // pinned [kRing][nsec]
+  int* mask_host = nullptr;                      // pinned [kRing][nsec] active masks being uploaded
+  bool rec_locked[kRing] = {}, rec_have_prev[kRing] = {};
+  cudaEvent_t ev_rec[kRing] = {}, ev_p0[kRing] = {}, ev_p1[kRing] = {};
+  long long issued = 0;                          // steps issued; history.size() = steps processed
+  std::vector<int> mask_sent;                    // the active mask the device has (or will have)
   ~BlockEngine() {
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    for (int i = 0; i < kRing; ++i) {
+      if (ev_rec[i]) cudaEventDestroy(ev_rec[i]);
+      if (ev_p0[i]) cudaEventDestroy(ev_p0[i]);
+      if (ev_p1[i]) cudaEventDestroy(ev_p1[i]);
+    }
+    if (stream) cudaStreamSynchronize(stream);
+    if (rec_host) cudaFreeHost(rec_host);
+    if (rec_flags) cudaFreeHost(rec_flags);
+    if (mask_host) cudaFreeHost(mask_host);
   }
 };
 
@@ -148,11 +172,46 @@ int engine_setup(BlockEngine& e, const std::vector<long long>& dims) {
   if ((rc = e.small.alloc((size_t)e.nsec * e.k * e.k * 4 * sizeof(double) + 64)) != DH_OK) return rc;
   DH_CUDA(cudaMemset(e.vec.ptr, 0, 3 * vb));
   for (int q = 0; q < 3; ++q) e.slot[q] = e.vec.as<double>() + (size_t)q * e.total * e.k;
-  e.bt_host.assign((size_t)e.nsec * e.k * e.k, 0.0);
   if (!e.ev0) {
     DH_CUDA(cudaEventCreate(&e.ev0));
     DH_CUDA(cudaEventCreate(&e.ev1));
   }
+  // device-resident step state and the pinned record ring
+  const size_t nk = (size_t)e.nsec * e.k * e.k;
+  if ((rc = e.stepbuf.alloc((10 * nk + e.nsec) * sizeof(double) + 2 * (size_t)e.nsec * sizeof(int))) != DH_OK) return rc;
+  double* d = e.stepbuf.as<double>();
+  e.dG = d;
+  e.dA = d + nk;
+  e.dBt[0] = d + 2 * nk;
+  e.dBt[1] = d + 3 * nk;
+  e.dR1 = d + 4 * nk;
+  e.dR2 = d + 5 * nk;
+  e.dInv1 = d + 6 * nk;
+  e.dInv2 = d + 7 * nk;
+  e.dB = d + 8 * nk;
+  e.dLock = d + 9 * nk;
+  e.dScale = d + 10 * nk;
+  e.dFlags = reinterpret_cast<int*>(e.dScale + e.nsec);
+  e.dActive = e.dFlags + e.nsec;
+  DH_CUDA(cudaMemset(e.stepbuf.ptr, 0, e.stepbuf.bytes));
+  if (e.rec_host) {
+    cudaFreeHost(e.rec_host);
+    cudaFreeHost(e.rec_flags);
+    cudaFreeHost(e.mask_host);
+    e.rec_host = nullptr;
+    e.rec_flags = e.mask_host = nullptr;
+  }
+  DH_CUDA(cudaMallocHost(&e.rec_host, (size_t)EngineRing * 6 * nk * sizeof(double)));
+  DH_CUDA(cudaMallocHost(&e.rec_flags, (size_t)EngineRing * e.nsec * sizeof(int)));
+  DH_CUDA(cudaMallocHost(&e.mask_host, (size_t)EngineRing * e.nsec * sizeof(int)));
+  if (!e.ev_rec[0]) {
+    for (int i = 0; i < EngineRing; ++i) {
+      DH_CUDA(cudaEventCreateWithFlags(&e.ev_rec[i], cudaEventDisableTiming));
+      DH_CUDA(cudaEventCreate(&e.ev_p0[i]));
+      DH_CUDA(cudaEventCreate(&e.ev_p1[i]));
+    }
+  }
+  e.mask_sent.assign(e.nsec, -1);
   return DH_OK;
 }
 
@@ -307,6 +366,8 @@ int engine_start(BlockEngine& e) {
   std::vector<double> B;
   e.slot_cur = 0;
   e.have_prev = false;
+  e.issued = 0;
+  if (e.dBt[0]) DH_CUDA(cudaMemsetAsync(e.dBt[0], 0, 2 * (size_t)e.nsec * e.k * e.k * sizeof(double), e.stream));
   int rc = engine_qr(e, e.slot[0], B, e.x32.as<float>(), nullptr);
   if (rc != DH_OK) return rc;
   const size_t vb = (size_t)e.total * e.k * sizeof(double);
@@ -382,63 +443,141 @@ inline double restart_residual_target(double precision) { return 0.1 * precision
 // passes without a restart
 inline double fp32_phase_residual_target(double precision) { return std::max(0.1 * precision, 1e-11); }
 
-// one block step for every sector (results recorded for the active ones)
-int engine_step(BlockEngine& e) {
-  const int k = e.k, kk = k * k;
+// The device's active mask follows the sectors' active flags (finished sectors' product rows are
+// zeroed instead of enumerated); uploaded from a pinned ring slot when it changes.
+int engine_sync_active(BlockEngine& e) {
+  if (!e.dActive) return DH_OK;
+  bool changed = false;
+  for (int s = 0; s < e.nsec; ++s) changed |= (e.mask_sent[s] != (e.sec[s].active ? 1 : 0));
+  if (!changed) return DH_OK;
+  int* m = e.mask_host + (size_t)(e.issued % EngineRing) * e.nsec;
+  for (int s = 0; s < e.nsec; ++s) m[s] = e.mask_sent[s] = e.sec[s].active ? 1 : 0;
+  DH_CUDA(cudaMemcpyAsync(e.dActive, m, (size_t)e.nsec * sizeof(int), cudaMemcpyHostToDevice, e.stream));
+  return DH_OK;
+}
+
+// One block step for every sector, issued on the stream with no host synchronisation:
+//   W = H V;  A = sym(V^T W);  W -= V A + V_prev B^T;  [W -= S (S^T W)];  CholQR2(W) -> B
+// The per-sector matrices stay on the device; the step's coefficients and flags are copied to the
+// record slot (step mod kRing) and an event marks them complete.  At most kRing - 1 steps may be in
+// flight ahead of engine_process_step.
+int engine_step_async(BlockEngine& e) {
+  const int k = e.k;
+  const long long step = e.issued;
+  DH_CHECK(step - (long long)e.history.size() < EngineRing - 1, DH_ERR_STATE, "too many block steps in flight");
+  const int slot = (int)(step % EngineRing);
   double* V = e.slot[e.slot_cur];
   double* W = e.slot[(e.slot_cur + 1) % 3];
   double* Vp = e.slot[(e.slot_cur + 2) % 3];
+  const double* Bt = e.dBt[step & 1];
+  double* Bt_next = e.dBt[(step + 1) & 1];
   int rc;
-  const int step = (int)e.history.size();
-  if ((rc = engine_product(e, V, W, step)) != DH_OK) return rc;
-  std::vector<double> A;
-  if ((rc = engine_gram(e, V, W, A)) != DH_OK) return rc;
-  for (int s = 0; s < e.nsec; ++s)
-    for (int i = 0; i < k; ++i)
-      for (int j = i + 1; j < k; ++j) {
-        const double m = 0.5 * (A[(size_t)s * kk + i * k + j] + A[(size_t)s * kk + j * k + i]);
-        A[(size_t)s * kk + i * k + j] = A[(size_t)s * kk + j * k + i] = m;
-      }
-  double* dA = e.small.as<double>() + 2 * (size_t)e.nsec * kk;
-  double* dBt = dA + (size_t)e.nsec * kk;
-  DH_CUDA(cudaMemcpyAsync(dA, A.data(), A.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
-  DH_CUDA(cudaMemcpyAsync(dBt, e.bt_host.data(), e.bt_host.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
-  if ((rc = launch_seg_update(W, V, dA, e.have_prev ? Vp : nullptr, e.have_prev ? dBt : nullptr, k, e.tiles, e.stream)) !=
+  if ((rc = engine_sync_active(e)) != DH_OK) return rc;
+  // the product (FP64 for the start block of a mixed restart), timed by events read at processing
+  const int saved = e.precision;
+  if (step == 0 && e.fp64_first_product) e.precision = DH_PRECISION_FP64;
+  const float* x32 = e.precision == DH_PRECISION_FP32 ? e.x32.as<float>() : nullptr;
+  if (e.precision == DH_PRECISION_FP64) ++e.fp64_products;
+  DH_CUDA(cudaEventRecord(e.ev_p0[slot], e.stream));
+  rc = e.product(V, x32, W);
+  e.precision = saved;
+  if (rc != DH_OK) return rc;
+  DH_CUDA(cudaEventRecord(e.ev_p1[slot], e.stream));
+  ++e.products;
+  // A = sym(V^T W) and the step's scale |A|^2 + |B|^2; W -= V A + V_prev B^T
+  if ((rc = launch_seg_gram(V, W, k, e.tiles, e.partial.as<double>(), e.dG, e.stream)) != DH_OK) return rc;
+  if ((rc = launch_step_sym(e.dG, Bt, k, e.nsec, e.dA, e.dScale, e.stream)) != DH_OK) return rc;
+  if ((rc = launch_seg_update(W, V, e.dA, e.have_prev ? Vp : nullptr, e.have_prev ? Bt : nullptr, k, e.tiles,
+                              e.stream)) != DH_OK)
+    return rc;
+  // W -= S (S^T W) with S the start block: the FP32 products of the later blocks leave components
+  // along S of the order of their rounding, which the recurrence alone would keep
+  const bool locked = e.lock_start && step >= 1;
+  if (locked) {
+    if ((rc = launch_seg_gram(e.start_block.as<double>(), W, k, e.tiles, e.partial.as<double>(), e.dLock, e.stream)) !=
+        DH_OK)
+      return rc;
+    if ((rc = launch_seg_update(W, e.start_block.as<double>(), e.dLock, nullptr, nullptr, k, e.tiles, e.stream)) != DH_OK)
+      return rc;
+  }
+  // CholQR2: X = V B.  With FP32 products an exhausted Krylov space leaves FP32 rounding noise, not
+  // zero: the vanishing and pivot thresholds are about (32 u)^2 of the product's precision.  A
+  // sector whose block is numerically zero against its step's scale (the Krylov space is complete)
+  // or whose Gram matrix breaks down gets a zero block and is flagged.
+  const bool f32 = e.precision == DH_PRECISION_FP32;
+  const double vanish_tol = f32 ? 4e-12 : 1e-24, pivot_tol = f32 ? 4e-12 : 1e-26;
+  if ((rc = launch_seg_gram(W, W, k, e.tiles, e.partial.as<double>(), e.dG, e.stream)) != DH_OK) return rc;
+  if ((rc = launch_step_chol(e.dG, k, e.nsec, 0, vanish_tol, pivot_tol, e.dScale, e.dR1, e.dInv1, e.dFlags, e.stream)) !=
       DH_OK)
     return rc;
-  std::vector<double> B, scale(e.nsec, 0.0);
-  std::vector<char> was_exhausted(e.nsec);
-  for (int s = 0; s < e.nsec; ++s) {
-    was_exhausted[s] = e.sec[s].exhausted;
-    for (int i = 0; i < kk; ++i)
-      scale[s] += A[(size_t)s * kk + i] * A[(size_t)s * kk + i] + e.bt_host[(size_t)s * kk + i] * e.bt_host[(size_t)s * kk + i];
-  }
-  StepRecord rec;
-  rec.A = A;
-  rec.Bt = e.bt_host;
-  rec.have_prev = e.have_prev;
-  if (e.lock_start && step >= 1) {
-    // W -= S (S^T W) with S the start block: the FP32 products of the later blocks leave components
-    // along S of the order of their rounding, which the recurrence alone would keep
-    if ((rc = engine_gram(e, e.start_block.as<double>(), W, rec.lock)) != DH_OK) return rc;
-    double* dL = e.small.as<double>() + 2 * (size_t)e.nsec * kk;  // dA is free again after the update
-    DH_CUDA(cudaMemcpyAsync(dL, rec.lock.data(), rec.lock.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
-    if ((rc = launch_seg_update(W, e.start_block.as<double>(), dL, nullptr, nullptr, k, e.tiles, e.stream)) != DH_OK)
-      return rc;
-    DH_CUDA(cudaStreamSynchronize(e.stream));
-  }
-  if ((rc = engine_qr(e, W, B, e.x32.as<float>(), &scale, &rec.inv1, &rec.inv2)) != DH_OK) return rc;
-  e.history.push_back(std::move(rec));
-  const int nb = (int)e.history.size();  // W now holds block nb
-  if (nb >= e.store_cap && e.store_cap > 0 && e.store_cap < e.store_max) store_grow(e);
-  if (nb < e.store_cap)
-    DH_CUDA(cudaMemcpyAsync(e.store.as<double>() + (size_t)nb * e.total * e.k, W, (size_t)e.total * e.k * sizeof(double),
+  if ((rc = launch_seg_rmul(W, e.dInv1, k, e.tiles, nullptr, e.stream)) != DH_OK) return rc;
+  if ((rc = launch_seg_gram(W, W, k, e.tiles, e.partial.as<double>(), e.dG, e.stream)) != DH_OK) return rc;
+  if ((rc = launch_step_chol(e.dG, k, e.nsec, 1, vanish_tol, pivot_tol, nullptr, e.dR2, e.dInv2, e.dFlags, e.stream)) !=
+      DH_OK)
+    return rc;
+  if ((rc = launch_seg_rmul(W, e.dInv2, k, e.tiles, e.x32.as<float>(), e.stream)) != DH_OK) return rc;
+  if ((rc = launch_step_b(e.dR1, e.dR2, e.dFlags, k, e.nsec, e.dB, Bt_next, e.stream)) != DH_OK) return rc;
+  // the step's record: A, the B^T it used, the two CholQR inverses, the lock coefficients, B, flags
+  const size_t nk = (size_t)e.nsec * k * k, nb_ = nk * sizeof(double);
+  double* rec = e.rec_host + (size_t)slot * 6 * nk;
+  DH_CUDA(cudaMemcpyAsync(rec, e.dA, nb_, cudaMemcpyDeviceToHost, e.stream));
+  DH_CUDA(cudaMemcpyAsync(rec + nk, Bt, nb_, cudaMemcpyDeviceToHost, e.stream));
+  DH_CUDA(cudaMemcpyAsync(rec + 2 * nk, e.dInv1, nb_, cudaMemcpyDeviceToHost, e.stream));
+  DH_CUDA(cudaMemcpyAsync(rec + 3 * nk, e.dInv2, nb_, cudaMemcpyDeviceToHost, e.stream));
+  if (locked) DH_CUDA(cudaMemcpyAsync(rec + 4 * nk, e.dLock, nb_, cudaMemcpyDeviceToHost, e.stream));
+  DH_CUDA(cudaMemcpyAsync(rec + 5 * nk, e.dB, nb_, cudaMemcpyDeviceToHost, e.stream));
+  DH_CUDA(cudaMemcpyAsync(e.rec_flags + (size_t)slot * e.nsec, e.dFlags, (size_t)e.nsec * sizeof(int),
+                          cudaMemcpyDeviceToHost, e.stream));
+  DH_CUDA(cudaEventRecord(e.ev_rec[slot], e.stream));
+  e.rec_locked[slot] = locked;
+  e.rec_have_prev[slot] = e.have_prev;
+  // the block store (W is block step + 1)
+  const long long nbk = step + 1;
+  if (nbk >= e.store_cap && e.store_cap > 0 && e.store_cap < e.store_max) store_grow(e);
+  if (nbk < e.store_cap)
+    DH_CUDA(cudaMemcpyAsync(e.store.as<double>() + (size_t)nbk * e.total * e.k, W, (size_t)e.total * e.k * sizeof(double),
                             cudaMemcpyDeviceToDevice, e.stream));
+  e.have_prev = true;
+  e.slot_cur = (e.slot_cur + 1) % 3;
+  ++e.issued;
+  return DH_OK;
+}
+
+// The host's bookkeeping of the oldest issued step not yet processed: waits for its record, keeps
+// its coefficients for replays, and appends A and B to every active sector (exhaustion from the
+// device's flags and the counting rule).
+int engine_process_step(BlockEngine& e) {
+  const int k = e.k, kk = k * k;
+  const long long step = (long long)e.history.size();
+  DH_CHECK(step < e.issued, DH_ERR_STATE, "no block step in flight");
+  const int slot = (int)(step % EngineRing);
+  DH_CUDA(cudaEventSynchronize(e.ev_rec[slot]));
+  float ms = 0.0f;
+  DH_CUDA(cudaEventElapsedTime(&ms, e.ev_p0[slot], e.ev_p1[slot]));
+  e.product_ms += ms;
+  const size_t nk = (size_t)e.nsec * kk;
+  const double* rec = e.rec_host + (size_t)slot * 6 * nk;
+  const int* flags = e.rec_flags + (size_t)slot * e.nsec;
+  StepRecord r;
+  r.A.assign(rec, rec + nk);
+  r.Bt.assign(rec + nk, rec + 2 * nk);
+  r.inv1.assign(rec + 2 * nk, rec + 3 * nk);
+  r.inv2.assign(rec + 3 * nk, rec + 4 * nk);
+  if (e.rec_locked[slot]) r.lock.assign(rec + 4 * nk, rec + 5 * nk);
+  r.have_prev = e.rec_have_prev[slot];
+  e.history.push_back(std::move(r));
+  const double* B = rec + 5 * nk;
+  const double* A = e.history.back().A.data();
   for (int s = 0; s < e.nsec; ++s) {
     BlockSector& b = e.sec[s];
     if (!b.active) continue;
-    b.A.insert(b.A.end(), A.begin() + (size_t)s * kk, A.begin() + (size_t)(s + 1) * kk);
-    b.B.insert(b.B.end(), B.begin() + (size_t)s * kk, B.begin() + (size_t)(s + 1) * kk);
+    const bool was_exhausted = b.exhausted;
+    if (flags[s] & 1) {
+      if (!b.exhausted) b.partial = !(flags[s] & 2);
+      b.exhausted = true;
+    }
+    b.A.insert(b.A.end(), A + (size_t)s * kk, A + (size_t)(s + 1) * kk);
+    b.B.insert(b.B.end(), B + (size_t)s * kk, B + (size_t)(s + 1) * kk);
     ++b.blocks;
     ++b.steps;
     // counting rule: once the blocks would outnumber the dimension the Krylov space is complete
@@ -447,14 +586,33 @@ int engine_step(BlockEngine& e) {
       b.exhausted = true;
       b.partial = (long long)b.blocks * k < b.dim;
     }
-    if (b.exhausted && !was_exhausted[s]) b.converged = true;  // the Krylov space is complete
+    if (b.exhausted && !was_exhausted) b.converged = true;  // the Krylov space is complete
   }
-  for (int s = 0; s < e.nsec; ++s)
-    for (int i = 0; i < k; ++i)
-      for (int j = 0; j < k; ++j) e.bt_host[(size_t)s * kk + i * k + j] = B[(size_t)s * kk + j * k + i];
-  e.have_prev = true;
-  e.slot_cur = (e.slot_cur + 1) % 3;
   return DH_OK;
+}
+
+// one block step for every sector, its bookkeeping done before returning
+int engine_step(BlockEngine& e) {
+  int rc = engine_step_async(e);
+  if (rc != DH_OK) return rc;
+  return engine_process_step(e);
+}
+
+// the band matrix of sector s (blocks A_0..A_{m-1} on the diagonal, B_1..B_{m-1} below), dense
+void sector_band_matrix(const BlockEngine& e, const BlockSector& b, std::vector<double>& t) {
+  const int k = e.k, kk = k * k, m = b.blocks, n = m * k;
+  t.assign((size_t)n * n, 0.0);
+  for (int j = 0; j < m; ++j) {
+    for (int p = 0; p < k; ++p)
+      for (int q = 0; q < k; ++q) t[(size_t)(j * k + p) * n + j * k + q] = b.A[(size_t)j * kk + p * k + q];
+    if (j + 1 < m)
+      for (int p = 0; p < k; ++p)
+        for (int q = 0; q < k; ++q) {
+          const double v = b.B[(size_t)(j + 1) * kk + p * k + q];
+          t[(size_t)((j + 1) * k + p) * n + j * k + q] = v;
+          t[(size_t)(j * k + q) * n + (j + 1) * k + p] = v;
+        }
+  }
 }
 
 // eigenvalues of the band matrix of sector s (blocks A_0..A_{m-1}, B_1..B_{m-1})
@@ -599,8 +757,10 @@ int sector_evaluate(const BlockEngine& e, BlockSector& b) {
     // the Ritz value has settled to 1e-7, which any residual small enough to pass implies anyway
     const double l0 = b.ritz[0];
     if (!(fabs(l0 - b.prev_last) < 1e-7 * fabs(l0))) return DH_OK;
-    std::vector<double> C, vals;
-    if ((rc = sector_ritz_coefficients(e, b, 1, C, vals)) != DH_OK) return rc;
+    // the lowest eigenvector of the band matrix by inverse iteration at the known l0
+    std::vector<double> t, C((size_t)b.blocks * e.k);
+    sector_band_matrix(e, b, t);
+    if ((rc = band_inverse_iteration(b.blocks * e.k, std::max(1, 2 * e.k - 1), t.data(), l0, C.data())) != DH_OK) return rc;
     const int k = e.k, m = b.blocks;
     const double* Bm = &b.B[(size_t)m * k * k];  // X_m = V_m B_m: the block after the last A
     double r2 = 0.0;
@@ -610,6 +770,8 @@ int sector_evaluate(const BlockEngine& e, BlockSector& b) {
       r2 += v * v;
     }
     if (r2 < e.residual_target * fabs(b.ritz[0])) b.converged = true;
+    // a Ritz value that no longer moves at all: the products' rounding floor is reached
+    if (fabs(l0 - b.prev_last) < 1e-13 * fabs(l0)) b.converged = true;
     return DH_OK;
   }
   if ((int)b.ritz.size() > e.nev) {
@@ -619,16 +781,24 @@ int sector_evaluate(const BlockEngine& e, BlockSector& b) {
   return DH_OK;
 }
 
-// run every active sector until converged, exhausted or at the iteration limit; the driver loop of
-// QHEOnSphereMainTask.cc:732-753 per sector (first call nev + 2 block steps, counter (nev + 3) k)
+// Run every active sector until converged, exhausted or at the iteration limit; the driver loop of
+// QHEOnSphereMainTask.cc:732-753 per sector (first call nev + 2 block steps, counter (nev + 3) k).
+// The device runs kStepLag steps ahead of the host: while step i's band matrices are diagonalised
+// on the host (convergence), step i + 1 runs on the GPU.  A sector found finished at step i stops
+// being enumerated from the next issued step on (its rows are zeroed); the steps issued past the
+// last sector's stop are processed for the replay record and otherwise unused.
+constexpr int kStepLag = 2;
+
 int engine_solve(BlockEngine& e) {
   const int first = e.nev + 2;
+  int rc;
   for (;;) {
     bool any = false;
     for (auto& b : e.sec) any |= b.active;
     if (!any) break;
-    int rc = engine_step(e);
-    if (rc != DH_OK) return rc;
+    while (e.issued - (long long)e.history.size() < kStepLag)
+      if ((rc = engine_step_async(e)) != DH_OK) return rc;
+    if ((rc = engine_process_step(e)) != DH_OK) return rc;
     std::vector<int> eval;
     for (int s = 0; s < e.nsec; ++s) {
       BlockSector& b = e.sec[s];
@@ -644,18 +814,24 @@ int engine_solve(BlockEngine& e) {
     // band eigenvalues of the sectors due, spread over host threads
     std::vector<int> status(eval.size(), DH_OK);
     const int nthreads = std::max(1, std::min((int)eval.size(), (int)std::thread::hardware_concurrency()));
-    std::vector<std::thread> pool;
-    for (int t = 0; t < nthreads; ++t)
-      pool.emplace_back([&, t] {
-        for (size_t i = t; i < eval.size(); i += nthreads) status[i] = sector_evaluate(e, e.sec[eval[i]]);
-      });
-    for (auto& th : pool) th.join();
+    if (nthreads == 1) {
+      for (size_t i = 0; i < eval.size(); ++i) status[i] = sector_evaluate(e, e.sec[eval[i]]);
+    } else {
+      std::vector<std::thread> pool;
+      for (int t = 0; t < nthreads; ++t)
+        pool.emplace_back([&, t] {
+          for (size_t i = t; i < eval.size(); i += nthreads) status[i] = sector_evaluate(e, e.sec[eval[i]]);
+        });
+      for (auto& th : pool) th.join();
+    }
     for (size_t i = 0; i < eval.size(); ++i) {
       if (status[i] != DH_OK) return status[i];
       BlockSector& b = e.sec[eval[i]];
       if (b.converged || b.exhausted || b.count >= e.max_iter) b.active = false;
     }
   }
+  while ((long long)e.history.size() < e.issued)
+    if ((rc = engine_process_step(e)) != DH_OK) return rc;
   return DH_OK;
 }
 
@@ -1071,6 +1247,7 @@ int bind_sector_product(SectorBatchHost& hb, const std::vector<int>& sectors, Bl
     c.x = f32 ? static_cast<const void*>(x32) : static_cast<const void*>(x64);
     c.xdiag = f32 ? x64 : nullptr;
     c.y = y;
+    c.active = ep->dActive;
     return launch_fqhe_sectors(c, ep->precision, ep->stream);
   };
   return DH_OK;
@@ -1167,6 +1344,10 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
   if (!lanczos_sectors.empty()) {
     const auto ta = clk::now();
     e.eig_precision = precision == DH_PRECISION_FP32 ? std::max(e.eig_precision, 1e-9) : e.eig_precision;
+    // the FP32 phase stops on each sector's Ritz residual (from its band matrix) rather than on the
+    // Ritz value's change, so that the FP64 check after it passes without a restart
+    if (precision == DH_PRECISION_FP32)
+      e.residual_target = fp32_phase_residual_target(precision_target > 0.0 ? precision_target : 1e-14);
     if ((rc = engine_setup(e, dims)) != DH_OK) return rc;
     if (precision == DH_PRECISION_FP32) engine_store_if_fits(e);
     SectorProduct prod;

@@ -11,6 +11,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <new>
 #include <string>
 #include <thread>
@@ -912,3 +913,55 @@ int dh_lanczos_solve_refined(dh_lanczos_t l, int max_iter, double precision, dou
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ block-size tuner
+
+extern "C" int dh_hamiltonian_tune_block_size(dh_hamiltonian_t h, int max_iter, double precision, int refined,
+                                              int* best_k, double* seconds) {
+  DH_CHECK(h && best_k, DH_ERR_ARGUMENT, "null argument");
+  DH_CHECK(precision > 0.0, DH_ERR_ARGUMENT, "precision must be > 0");
+  const int saved_precision = h->precision;
+  const int ks[3] = {1, 2, 4};
+  double best = 1e300;
+  *best_k = 1;
+  for (int i = 0; i < 3; ++i) {
+    const int k = ks[i];
+    if (seconds) seconds[i] = 0.0;
+    if (k > 1 && h->complex_phases) continue;  // complex vectors go one at a time
+    if ((long long)4 * k > hamiltonian_dim(h)) continue;
+    h->precision = refined ? DH_PRECISION_FP32 : DH_PRECISION_FP64;
+    dh_lanczos_t l = nullptr;
+    int rc = dh_lanczos_create(h, k == 1 ? DH_LANCZOS_BASIC : DH_LANCZOS_BLOCK, 1, k, max_iter, &l);
+    if (rc != DH_OK) {
+      h->precision = saved_precision;
+      return rc;
+    }
+    struct Guard {
+      dh_lanczos_t l;
+      ~Guard() { dh_lanczos_destroy(l); }
+    } guard{l};
+    DH_CUDA(cudaDeviceSynchronize());
+    const auto t0 = std::chrono::steady_clock::now();
+    if ((rc = dh_lanczos_set_eigenvalue_precision(l, precision)) == DH_OK &&
+        (rc = dh_lanczos_initialize_random(l, 0)) == DH_OK) {
+      if (refined) {
+        double out[5];
+        rc = dh_lanczos_solve_refined(l, max_iter, precision, out);
+      } else {
+        double e = 0.0;
+        int it = 0, conv = 0;
+        rc = dh_lanczos_solve(l, max_iter, 16, &e, &it, &conv);
+      }
+    }
+    h->precision = saved_precision;
+    if (rc != DH_OK) return rc;
+    DH_CUDA(cudaDeviceSynchronize());
+    const double t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (seconds) seconds[i] = t;
+    if (t < best) {
+      best = t;
+      *best_k = k;
+    }
+  }
+  return DH_OK;
+}

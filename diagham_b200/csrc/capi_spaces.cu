@@ -501,6 +501,9 @@ int dh_fermion_on_sphere_create(int nbr_fermions, int total_lz, int lz_max, unsi
   if (kv && strcmp(kv, "smem") == 0) sp->kernel_variant = 2;
   const char* lb = getenv("DH_FQHE_LOW_BITS");
   sp->requested_low_bits = lb ? atoi(lb) : 0;
+  // DH_FQHE_SPLIT_FORM: launch form of the split-word kernel (as dh_space_set_split_form)
+  const char* sf = getenv("DH_FQHE_SPLIT_FORM");
+  if (sf && atoi(sf) >= 0 && atoi(sf) < kNbrSplitForms) sp->split_form = atoi(sf);
   int rc = build_fermion_space(sp);
   if (rc != DH_OK) {
     delete sp;
@@ -616,10 +619,14 @@ int dh_spin12_chain_translations_create(int chain_length, int momentum, int sz, 
   }
   sp->dim = dim;
   if (dim > 0) {
+    // the whole-sector map (DH_TRANS_MAP=1) or, by default, flipped words canonicalised in the kernels
+    const char* tm = getenv("DH_TRANS_MAP");
+    const bool with_map = tm && atoi(tm) != 0;
     if ((rc = offsets.alloc(chunks * sizeof(long long))) != DH_OK ||
-        (rc = sp->words.alloc(dim * sizeof(uint32_t))) != DH_OK || (rc = sp->rep_orbit.alloc(dim)) != DH_OK ||
-        (rc = sp->rep_rank.alloc(dim * sizeof(int32_t))) != DH_OK ||
-        (rc = sp->trans_map.alloc(total * sizeof(unsigned long long))) != DH_OK)
+        (rc = sp->words.alloc(dim * sizeof(uint32_t))) != DH_OK || (rc = sp->rep_orbit.alloc(dim)) != DH_OK)
+      return rc;
+    if (with_map && ((rc = sp->rep_rank.alloc(dim * sizeof(int32_t))) != DH_OK ||
+                     (rc = sp->trans_map.alloc(total * sizeof(unsigned long long))) != DH_OK))
       return rc;
     DH_CUDA(cudaMemcpy(offsets.ptr, ho.data(), chunks * sizeof(long long), cudaMemcpyHostToDevice));
     if ((rc = launch_trans_write(total, chain_length, sp->nbr_up, momentum, offsets.as<long long>(),
@@ -635,7 +642,7 @@ int dh_spin12_chain_translations_create(int chain_length, int momentum, int sz, 
     if ((rc = launch_trans_table(sp->words.as<uint32_t>(), dim, sp->table_shift, sp->table_entries,
                                  sp->trans_table.as<int>(), 0)) != DH_OK)
       return rc;
-    if ((rc = launch_trans_map(trans_device(sp, nullptr), total, sp->nbr_up, 0)) != DH_OK) return rc;
+    if (with_map && (rc = launch_trans_map(trans_device(sp, nullptr), total, sp->nbr_up, 0)) != DH_OK) return rc;
     DH_CUDA(cudaDeviceSynchronize());
   }
   *out = guard.release();

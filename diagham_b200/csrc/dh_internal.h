@@ -174,6 +174,7 @@ struct SectorBatchDevice {
   const void* x;                      // [total_rows][block]
   const double* xdiag;                // optional FP64 copy of x for the shift term
   double* y;                          // [total_rows][block]
+  const int* active;                  // optional [nbr_sectors]: 0 = the sector's rows get y = 0
   long long total_rows;
   double shift;
   int nbr_sectors, block, lz_max, low_bits, nbr_pairs, nbr_factors;
@@ -201,12 +202,22 @@ int launch_seg_combine_blocks(const double* blocks, int nb, long long stride, co
 int launch_random_block(double* x, long long rows, int k, const long long* row_sector_base, const TileSetDevice& t,
                         uint64_t seed, cudaStream_t s, int first_col = 0);
 int launch_f32_copy(const double* x, float* y, long long n, cudaStream_t s);
+// per-sector k x k math of a block step on the device (one thread per sector): A = sym(G) with
+// scale = |A|^2 + |Bt|^2; a CholQR pass (R, R^-1, breakdown / vanishing flags); B = R2 R1, Bt = B^T
+int launch_step_sym(const double* G, const double* Bt, int k, int nsec, double* A, double* scale, cudaStream_t s);
+int launch_step_chol(const double* G, int k, int nsec, int pass, double vanish_tol, double pivot_tol, const double* scale,
+                     double* R, double* Rinv, int* flags, cudaStream_t s);
+int launch_step_b(const double* R1, const double* R2, const int* flags, int k, int nsec, double* B, double* Bt_next,
+                  cudaStream_t s);
 // x[i][col] = v[i] and v[i] = scale * x[i][col] for a [n][k] block x
 int launch_put_column(const double* v, long long n, int k, int col, double* x, cudaStream_t s);
 int launch_get_column(const double* x, long long n, int k, int col, double scale, double* v, cudaStream_t s);
 // eigenvalues (ascending) of a symmetric band matrix of half-bandwidth b stored densely (row-major,
 // destroyed): Givens reduction to tridiagonal form touching only the band, then implicit QL
 int band_eigenvalues(int n, int b, double* a, double* eig);
+// eigenvector of the symmetric band matrix a (dense storage, unchanged) for its eigenvalue lambda, by
+// inverse iteration with a banded LU (O(n b^2))
+int band_inverse_iteration(int n, int b, const double* a, double lambda, double* vec);
 
 int launch_fqhe_unrank(int nbr_fermions, int lz_max, int total_sum, long long dim, uint64_t* words,
                        const int64_t* counts_dev, int count_stride_o, int count_stride_s, cudaStream_t s);

@@ -156,6 +156,93 @@ __global__ void __launch_bounds__(kThreads) seg_combine_blocks_kernel(const doub
   }
 }
 
+// ------------------------------------------------------------ per-sector k x k step math
+// One thread per sector (k <= 4): the small matrices of a block step stay on the device, so a step
+// needs no host round trip.  Layout of every matrix: [sector][k][k] row-major.
+
+// A = (G + G^T) / 2 and scale[s] = |A|_F^2 + |Bt|_F^2 (the step's Gram V^T W and B_i^T)
+__global__ void step_sym_kernel(const double* G, const double* Bt, int k, int nsec, double* A, double* scale) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsec) return;
+  const int kk = k * k;
+  const double* g = G + (size_t)s * kk;
+  double* a = A + (size_t)s * kk;
+  double sc = 0.0;
+  for (int i = 0; i < k; ++i)
+    for (int j = 0; j < k; ++j) {
+      const double v = (i == j) ? g[i * k + i] : 0.5 * (g[i * k + j] + g[j * k + i]);
+      a[i * k + j] = v;
+      const double b = Bt ? Bt[(size_t)s * kk + i * k + j] : 0.0;
+      sc += v * v + b * b;
+    }
+  scale[s] = sc;
+}
+
+// One CholQR pass: G = R^T R (R upper) and Rinv = R^-1.  flags[s] bit 0: the block broke down (a
+// pivot below pivot_tol trace(G)), bit 1: it vanished (pass 0 only: trace(G) <= vanish_tol scale[s]).
+// A broken sector gets R = Rinv = 0, which zeroes its block.  Pass 0 resets the flags.
+__global__ void step_chol_kernel(const double* G, int k, int nsec, int pass, double vanish_tol, double pivot_tol,
+                                 const double* scale, double* R, double* Rinv, int* flags) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsec) return;
+  const int kk = k * k;
+  const double* g = G + (size_t)s * kk;
+  double* r = R + (size_t)s * kk;
+  double* ri = Rinv + (size_t)s * kk;
+  int f = pass == 0 ? 0 : flags[s];
+  double trace = 0.0;
+  for (int i = 0; i < k; ++i) trace += fabs(g[i * k + i]);
+  if (pass == 0 && scale && !(trace > vanish_tol * scale[s])) f |= 3;
+  for (int i = 0; i < kk; ++i) r[i] = ri[i] = 0.0;
+  bool ok = (f & 1) == 0;
+  for (int j = 0; j < k && ok; ++j) {
+    double d = g[j * k + j];
+    for (int p = 0; p < j; ++p) d -= r[p * k + j] * r[p * k + j];
+    if (!(d > pivot_tol * fmax(trace, 1e-300))) {
+      ok = false;
+      break;
+    }
+    const double rjj = sqrt(d);
+    r[j * k + j] = rjj;
+    for (int c = j + 1; c < k; ++c) {
+      double v = 0.5 * (g[j * k + c] + g[c * k + j]);
+      for (int p = 0; p < j; ++p) v -= r[p * k + j] * r[p * k + c];
+      r[j * k + c] = v / rjj;
+    }
+  }
+  if (ok) {
+    for (int c = 0; c < k; ++c)  // R Rinv = I, column by column (back substitution)
+      for (int i = c; i >= 0; --i) {
+        double v = (i == c) ? 1.0 : 0.0;
+        for (int p = i + 1; p <= c; ++p) v -= r[i * k + p] * ri[p * k + c];
+        ri[i * k + c] = v / r[i * k + i];
+      }
+  } else {
+    f |= 1;
+    for (int i = 0; i < kk; ++i) r[i] = ri[i] = 0.0;
+  }
+  flags[s] = f;
+}
+
+// B = R2 R1 (the new block's coefficient, upper; zero for a broken sector) and Bt_next = B^T
+__global__ void step_b_kernel(const double* R1, const double* R2, const int* flags, int k, int nsec, double* B,
+                              double* Bt_next) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsec) return;
+  const int kk = k * k;
+  const double* a = R2 + (size_t)s * kk;
+  const double* b = R1 + (size_t)s * kk;
+  const bool broke = flags[s] & 1;
+  for (int i = 0; i < k; ++i)
+    for (int j = 0; j < k; ++j) {
+      double v = 0.0;
+      if (!broke)
+        for (int p = 0; p < k; ++p) v += a[i * k + p] * b[p * k + j];
+      B[(size_t)s * kk + i * k + j] = v;
+      Bt_next[(size_t)s * kk + j * k + i] = v;
+    }
+}
+
 __global__ void random_block_kernel(double* x, long long rows, int k, int first_col, const long long* row_sector_base,
                                     TileSetDevice t, uint64_t seed) {
   const int tile = blockIdx.x;
@@ -253,6 +340,29 @@ int launch_seg_combine_blocks(const double* blocks, int nb, long long stride, co
     case 4: seg_combine_blocks_kernel<4><<<t.nbr_tiles, kThreads, 0, s>>>(blocks, nb, stride, C, cstride, t, out); break;
     default: set_error("block size %d not in {1, 2, 4}", k); return DH_ERR_UNSUPPORTED;
   }
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_step_sym(const double* G, const double* Bt, int k, int nsec, double* A, double* scale, cudaStream_t s) {
+  if (nsec <= 0) return DH_OK;
+  step_sym_kernel<<<(nsec + 127) / 128, 128, 0, s>>>(G, Bt, k, nsec, A, scale);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_step_chol(const double* G, int k, int nsec, int pass, double vanish_tol, double pivot_tol, const double* scale,
+                     double* R, double* Rinv, int* flags, cudaStream_t s) {
+  if (nsec <= 0) return DH_OK;
+  step_chol_kernel<<<(nsec + 127) / 128, 128, 0, s>>>(G, k, nsec, pass, vanish_tol, pivot_tol, scale, R, Rinv, flags);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_step_b(const double* R1, const double* R2, const int* flags, int k, int nsec, double* B, double* Bt_next,
+                  cudaStream_t s) {
+  if (nsec <= 0) return DH_OK;
+  step_b_kernel<<<(nsec + 127) / 128, 128, 0, s>>>(R1, R2, flags, k, nsec, B, Bt_next);
   DH_CUDA(cudaGetLastError());
   return DH_OK;
 }

@@ -490,6 +490,11 @@ __global__ void __launch_bounds__(kMatvecThreads) fqhe_sectors_kernel(SectorBatc
     }
     const long long off = soff[lo];
     const long long r = g - off;
+    if (b.active && !b.active[lo]) {  // a finished sector: zero rows, no enumeration
+#pragma unroll
+      for (int j = 0; j < K; ++j) b.y[g * K + j] = 0.0;
+      continue;
+    }
     SplitTables t;
     t.words = b.words[lo];
     t.HO = b.high_offset[lo];

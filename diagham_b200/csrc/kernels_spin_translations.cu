@@ -12,11 +12,14 @@
 // symmetric for K = 0 and K = L/2, so the pull form y[s] = sum over flips of s of that element times
 // x[t] equals the reference's push form.
 //
-// B200 layout: instead of canonicalising every flipped word (L rotations and a search per element),
-// a table over the whole Sz sector, indexed by the word's plain Spin1_2Chain index (which the chain
-// kernels already compute from the row's own index with step tables), holds for every word the
-// index of its representative, the n above and its orbit size (8 bytes a word, 4.8 GB at L = 32).
-// Each element of the product is then one step-table rank, one table load and one gather.
+// B200 layout, two forms.  Canonical (default): every flipped word is canonicalised in registers (its
+// L rotations by funnel shifts, the first smallest kept with its rotation count n) and found among
+// the representatives (75 MB at L = 32, mostly L2-resident) through a lookup table over their top
+// bits and a short bisection; the target's orbit size is the representative's.  Map (optional, the
+// DH_TRANS_MAP=1 environment at set-up): a table over the whole Sz sector, indexed by the word's plain
+// Spin1_2Chain index (computed from the row's own index with step tables), holds for every word the
+// index of its representative, n and its orbit size (8 bytes a word, 4.8 GB at L = 32): one step-
+// table rank and one random 8-byte load per element instead of the rotations and the search.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -169,6 +172,58 @@ __device__ __forceinline__ long long rep_find(const TransDevice& d, uint32_t c) 
   return (lo < d.dim && d.reps[lo] == c) ? lo : -1;
 }
 
+// the smallest of the L rotations of w (rotr1 steps) and the number n of steps to it, the first when
+// several rotations give it; L = 32 unrolled with funnel shifts (independent rotations)
+__device__ __forceinline__ uint32_t canonical_rotation(uint32_t w, int L, uint32_t mask, int& n) {
+  uint32_t c = w;
+  n = 0;
+  if (L == 32) {
+#pragma unroll
+    for (int j = 1; j < 32; ++j) {
+      const uint32_t r = __funnelshift_r(w, w, j);
+      if (r < c) {
+        c = r;
+        n = j;
+      }
+    }
+  } else {
+    uint32_t r = w;
+    for (int j = 1; j < L; ++j) {
+      r = rotr1(r, L, mask);
+      if (r < c) {
+        c = r;
+        n = j;
+      }
+    }
+  }
+  return c;
+}
+
+// index of representative c through the read-only path, or -1
+__device__ __forceinline__ long long rep_find_ro(const TransDevice& d, uint32_t c) {
+  const long long v = (long long)(c >> d.table_shift);
+  if (v + 1 >= d.table_entries) return -1;
+  long long lo = __ldg(d.table + v), hi = __ldg(d.table + v + 1);
+  while (lo < hi) {
+    const long long mid = (lo + hi) >> 1;
+    if (__ldg(d.reps + mid) >= c)
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  return (lo < d.dim && __ldg(d.reps + lo) == c) ? lo : -1;
+}
+
+// the map entry of a flipped word computed in registers: representative index | n << 32 |
+// orbit << 40, or 0xffffffff when the word's orbit is not in the sector
+__device__ __forceinline__ unsigned long long canonical_entry(const TransDevice& d, uint32_t wf, int L, uint32_t mask) {
+  int n = 0;
+  const uint32_t c = canonical_rotation(wf, L, mask, n);
+  const long long t = rep_find_ro(d, c);
+  if (t < 0) return 0xffffffffull;
+  return (unsigned long long)t | ((unsigned long long)n << 32) | ((unsigned long long)__ldg(d.orbits + t) << 40);
+}
+
 // every word of the Sz sector (ascending rank q): its plain chain index, the index of its
 // representative (or none), the rotations to it and its orbit size; and each representative's own
 // plain chain index
@@ -281,11 +336,50 @@ __device__ __forceinline__ bool next_flip(FlipCursor& c, const SpinTables& tb, i
   return false;
 }
 
+// the same bonds as next_flip, giving the flip's bit mask (the flipped word is w ^ mask)
+template <typename TG>
+__device__ __forceinline__ bool next_flip_mask(FlipCursor& c, int L, TG hj1, TG hj2, uint32_t& fm, TG& hj) {
+  if (c.f1) {
+    const int ja = __ffs(c.f1) - 1;
+    c.f1 &= c.f1 - 1u;
+    fm = 3u << ja;
+    hj = hj1;
+    return true;
+  }
+  if (c.f2) {
+    const int ja = __ffs(c.f2) - 1;
+    c.f2 &= c.f2 - 1u;
+    fm = 5u << ja;
+    hj = hj2;
+    return true;
+  }
+  if (c.wraps & 1) {
+    c.wraps &= ~1;
+    fm = 1u | (1u << (L - 1));
+    hj = hj1;
+    return true;
+  }
+  if (c.wraps & 2) {
+    c.wraps &= ~2;
+    fm = 1u | (1u << (L - 2));
+    hj = hj2;
+    return true;
+  }
+  if (c.wraps & 4) {
+    c.wraps = 0;
+    fm = 2u | (1u << (L - 1));
+    hj = hj2;
+    return true;
+  }
+  return false;
+}
+
 // flips are taken kTransBatch at a time: their map loads are all issued before the first is used,
 // then their gathers, so several independent load chains are in flight per thread
 constexpr int kTransBatch = 4;
 
-template <typename TG, int K, bool IL, bool RANGE>
+// CANON: targets from canonicalising the flipped words (no whole-sector map)
+template <typename TG, int K, bool IL, bool RANGE, bool CANON>
 __global__ void __launch_bounds__(kTransThreads) trans_matvec_kernel(TransDevice d, MatvecArgs a) {
   __shared__ TransShared sh;
   build_spin_tables(sh.tb, d.length);
@@ -304,7 +398,7 @@ __global__ void __launch_bounds__(kTransThreads) trans_matvec_kernel(TransDevice
   const long long r_end = a.out_last > 0 ? a.out_last : d.dim;
   for (long long s = a.out_first + (long long)blockIdx.x * blockDim.x + threadIdx.x; s < r_end; s += stride) {
     const uint32_t w = __ldg(d.reps + s);
-    const int r = __ldg(d.rep_rank + s);
+    const int r = CANON ? 0 : __ldg(d.rep_rank + s);
     const int os = d.orbits[s];
     const uint32_t d1 = w ^ (((w >> 1) | (w << (L - 1))) & maskL);
     const uint32_t d2 = w ^ (((w >> 2) | (w << (L - 2))) & maskL);
@@ -319,12 +413,23 @@ __global__ void __launch_bounds__(kTransThreads) trans_matvec_kernel(TransDevice
       bool have[kTransBatch];
 #pragma unroll
       for (int q = 0; q < kTransBatch; ++q) {
-        have[q] = more && next_flip<TG>(cur, sh.tb, L, D, hj1, hj2, ci[q], hj[q]);
+        if constexpr (CANON) {
+          uint32_t fm = 0;
+          have[q] = more && next_flip_mask<TG>(cur, L, hj1, hj2, fm, hj[q]);
+          ci[q] = (int)fm;
+        } else {
+          have[q] = more && next_flip<TG>(cur, sh.tb, L, D, hj1, hj2, ci[q], hj[q]);
+        }
         more = have[q];
       }
       unsigned long long e[kTransBatch];
 #pragma unroll
-      for (int q = 0; q < kTransBatch; ++q) e[q] = have[q] ? __ldg(d.map + ci[q]) : 0xffffffffull;
+      for (int q = 0; q < kTransBatch; ++q) {
+        if constexpr (CANON)
+          e[q] = have[q] ? canonical_entry(d, w ^ (uint32_t)ci[q], L, maskL) : 0xffffffffull;
+        else
+          e[q] = have[q] ? __ldg(d.map + ci[q]) : 0xffffffffull;
+      }
       TG c[kTransBatch];
       unsigned int t[kTransBatch];
 #pragma unroll
@@ -375,7 +480,7 @@ struct TransSharedComplex {
 // reference pushes h(s -> t) = J/2 sqrt(o_s / o_t) exp(2 pi i K m / L) x[s] into y[t]
 // (SpinChainJ1J2HamiltonianWithTranslations.cc:149-247); H is Hermitian, so the pull form takes the
 // conjugate: y[s] += conj(h(s -> t)) x[t].
-template <typename TG, bool RANGE>
+template <typename TG, bool RANGE, bool CANON>
 __global__ void __launch_bounds__(kTransThreads) trans_matvec_complex_kernel(TransDevice d, MatvecArgs a) {
   __shared__ TransSharedComplex sh;
   build_spin_tables(sh.tb, d.length);
@@ -397,7 +502,7 @@ __global__ void __launch_bounds__(kTransThreads) trans_matvec_complex_kernel(Tra
   const long long r_end = (a.out_last > 0 ? a.out_last : 2 * d.dim) / 2;
   for (long long s = a.out_first / 2 + (long long)blockIdx.x * blockDim.x + threadIdx.x; s < r_end; s += stride) {
     const uint32_t w = __ldg(d.reps + s);
-    const int r = __ldg(d.rep_rank + s);
+    const int r = CANON ? 0 : __ldg(d.rep_rank + s);
     const int os = d.orbits[s];
     TG re = TG(0), im = TG(0);
     // flips kTransBatch at a time, their map loads and then their gathers in flight together
@@ -410,12 +515,23 @@ __global__ void __launch_bounds__(kTransThreads) trans_matvec_complex_kernel(Tra
       bool have[kTransBatch];
 #pragma unroll
       for (int q = 0; q < kTransBatch; ++q) {
-        have[q] = more && next_flip<TG>(cur, sh.tb, L, (int)d.chain_dim, hj1, hj2, ci[q], hj[q]);
+        if constexpr (CANON) {
+          uint32_t fm = 0;
+          have[q] = more && next_flip_mask<TG>(cur, L, hj1, hj2, fm, hj[q]);
+          ci[q] = (int)fm;
+        } else {
+          have[q] = more && next_flip<TG>(cur, sh.tb, L, (int)d.chain_dim, hj1, hj2, ci[q], hj[q]);
+        }
         more = have[q];
       }
       unsigned long long e[kTransBatch];
 #pragma unroll
-      for (int q = 0; q < kTransBatch; ++q) e[q] = have[q] ? __ldg(d.map + ci[q]) : 0xffffffffull;
+      for (int q = 0; q < kTransBatch; ++q) {
+        if constexpr (CANON)
+          e[q] = have[q] ? canonical_entry(d, w ^ (uint32_t)ci[q], L, maskL) : 0xffffffffull;
+        else
+          e[q] = have[q] ? __ldg(d.map + ci[q]) : 0xffffffffull;
+      }
       TG cr[kTransBatch], cim[kTransBatch];
       unsigned int t[kTransBatch];
 #pragma unroll
@@ -469,6 +585,7 @@ __global__ void __launch_bounds__(kTransThreads) trans_matvec_complex_kernel(Tra
 }
 
 // elements of one product (antiparallel bonds of the representatives, and those in the sector)
+template <bool CANON>
 __global__ void __launch_bounds__(kTransThreads) trans_count_kernel(TransDevice d, unsigned long long* total) {
   __shared__ SpinTables tb;
   build_spin_tables(tb, d.length);
@@ -479,10 +596,18 @@ __global__ void __launch_bounds__(kTransThreads) trans_count_kernel(TransDevice 
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < d.dim; s += stride) {
     const uint32_t w = d.reps[s];
-    const int r = d.rep_rank[s];
     const uint32_t d1 = w ^ (((w >> 1) | (w << (L - 1))) & maskL);
     const uint32_t d2 = w ^ (((w >> 2) | (w << (L - 2))) & maskL);
     bonds += __popc(d1) + __popc(d2);
+    if constexpr (CANON) {
+      FlipCursor cur = flip_cursor(w, 0, L);
+      uint32_t fm = 0;
+      double hj = 0.0;
+      while (next_flip_mask<double>(cur, L, 0.0, 0.0, fm, hj))
+        kept += (canonical_entry(d, w ^ fm, L, maskL) & 0xffffffffull) != 0xffffffffull;
+      continue;
+    }
+    const int r = d.rep_rank[s];
     uint32_t f = d1 & (maskL >> 1);
     while (f) {
       const int ja = __ffs(f) - 1;
@@ -525,8 +650,11 @@ template <typename TG, int K>
 int launch_trans_typed(const TransDevice& d, const MatvecArgs& a, cudaStream_t s) {
   const bool range = a.col_first > 0 || a.col_last < d.dim;
   const bool il = (K > 1) && a.ld == K && a.vstride == 1 && a.ld_y == K && a.vstride_y == 1;
-  auto kern = range ? (il ? trans_matvec_kernel<TG, K, true, true> : trans_matvec_kernel<TG, K, false, true>)
-                    : (il ? trans_matvec_kernel<TG, K, true, false> : trans_matvec_kernel<TG, K, false, false>);
+  auto kern = range ? (il ? trans_matvec_kernel<TG, K, true, true, true> : trans_matvec_kernel<TG, K, false, true, true>)
+                    : (il ? trans_matvec_kernel<TG, K, true, false, true> : trans_matvec_kernel<TG, K, false, false, true>);
+  if (d.map)
+    kern = range ? (il ? trans_matvec_kernel<TG, K, true, true, false> : trans_matvec_kernel<TG, K, false, true, false>)
+                 : (il ? trans_matvec_kernel<TG, K, true, false, false> : trans_matvec_kernel<TG, K, false, false, false>);
   int dev = 0, sms = 148, per_sm = 1;
   DH_CUDA(cudaGetDevice(&dev));
   DH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -614,10 +742,17 @@ int launch_trans_complex(const TransDevice& d, const MatvecArgs& a, cudaStream_t
     b.xdiag = a.xdiag ? a.xdiag + (long long)v * a.vstride : nullptr;
     b.y = static_cast<double*>(a.y) + (long long)v * a.vstride_y;
     b.nbr_vectors = 1;
-    if (range)
-      trans_matvec_complex_kernel<TG, true><<<(unsigned)g, kTransThreads, 0, s>>>(d, b);
-    else
-      trans_matvec_complex_kernel<TG, false><<<(unsigned)g, kTransThreads, 0, s>>>(d, b);
+    if (d.map) {
+      if (range)
+        trans_matvec_complex_kernel<TG, true, false><<<(unsigned)g, kTransThreads, 0, s>>>(d, b);
+      else
+        trans_matvec_complex_kernel<TG, false, false><<<(unsigned)g, kTransThreads, 0, s>>>(d, b);
+    } else {
+      if (range)
+        trans_matvec_complex_kernel<TG, true, true><<<(unsigned)g, kTransThreads, 0, s>>>(d, b);
+      else
+        trans_matvec_complex_kernel<TG, false, true><<<(unsigned)g, kTransThreads, 0, s>>>(d, b);
+    }
     DH_CUDA(cudaGetLastError());
   }
   return DH_OK;
@@ -643,7 +778,10 @@ int launch_trans_count_elements(const TransDevice& d, unsigned long long* total,
   long long g = (d.dim + kTransThreads - 1) / kTransThreads;
   if (g > 148 * 16) g = 148 * 16;
   if (g < 1) g = 1;
-  trans_count_kernel<<<(unsigned)g, kTransThreads, 0, s>>>(d, total);
+  if (d.map)
+    trans_count_kernel<false><<<(unsigned)g, kTransThreads, 0, s>>>(d, total);
+  else
+    trans_count_kernel<true><<<(unsigned)g, kTransThreads, 0, s>>>(d, total);
   DH_CUDA(cudaGetLastError());
   return DH_OK;
 }

@@ -420,6 +420,16 @@ int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eige
  * products in FP64 throughout (BasicLanczosAlgorithm.cc:148-216). */
 int dh_lanczos_solve_refined(dh_lanczos_t l, int max_iter, double precision, double* out);
 
+/* Block-size tuner: solves H's ground energy to `precision` with k = 1 (DH_LANCZOS_BASIC), 2 and 4
+ * (DH_LANCZOS_BLOCK) from the same seeded start, FP32 products + FP64 refinement when refined != 0
+ * (dh_lanczos_solve_refined), else FP64 products (dh_lanczos_solve), and returns in *best_k the block
+ * size with the shortest wall time to the converged energy (the time per converged Ritz value: a
+ * larger block costs more per step and needs fewer steps).  seconds (optional, 3 doubles): the time
+ * of each k (0 where a k does not apply).  The Hamiltonian's precision is left as it was.  No
+ * reference counterpart: the reference's block size is the --block-size option. */
+int dh_hamiltonian_tune_block_size(dh_hamiltonian_t h, int max_iter, double precision, int refined, int* best_k,
+                                   double* seconds);
+
 /* Disk storage of the Lanczos state, in the files of the reference's disk-storage classes, so that an
  * interrupted run resumes (here or in the reference) where it stopped:
  *   DH_LANCZOS_BASIC             BasicLanczosAlgorithmWithDiskStorage (src/LanczosAlgorithm/

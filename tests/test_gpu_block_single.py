@@ -167,3 +167,23 @@ def test_spin_block_multiply_matches_oracle(gpu, orc, prec, tol, k):
     for j in range(k):
         ref = orc.spin_j1j2_multiply(L, sz, words, 1.0, 0.5, x[:, j])
         assert np.max(np.abs(y[:, j] - ref)) <= tol * np.max(np.abs(ref)), (j, prec)
+
+
+@pytest.mark.parametrize("refined", [True, False])
+def test_block_size_tuner(gpu, refined):
+    # the tuner solves the sector with k = 1, 2, 4 and keeps the fastest; whatever it picks, the
+    # block Lanczos with that k reaches the reference's energy
+    z = golden("lanczos_n8_2s21_lz0_coulomb_basic.npz")
+    sp, H = _fqhe(gpu, z["v"], n=8, s=21, lz=0)
+    H.set_precision("fp64")
+    k, times = H.tune_block_size(max_iter=600, precision=1e-10, refined=refined)
+    assert k in (1, 2, 4) and all(t > 0 for t in times.values())
+    assert times[k] == min(times.values())
+    if refined:
+        H.set_precision("fp32")
+    lz = gpu.BasicLanczosAlgorithm(H, 1, 600) if k == 1 else gpu.BasicBlockLanczosAlgorithm(H, 1, 600, block_size=k)
+    lz.InitializeLanczosAlgorithm(seed=0)
+    e = lz.solve_refined(600, precision=1e-10)["energy"] if refined else lz.solve(600)["eigenvalues"][0]
+    e_ref = float(z["eigenvalues"][0])
+    assert abs(e - e_ref) < 1e-10 * abs(e_ref)
+    H.set_precision("fp64")
