@@ -39,9 +39,7 @@ UNIT = "H·v/s"
 REF_TOOL = os.path.join(ROOT, "oracle", "_ref", "ref_tool")
 FLUSH_BYTES = 256 << 20
 BLOCK = 4  # vectors per product in the measured step (the batched form)
-KERNEL_FP64_BLOCK4 = "fqhe_split_kernel<double, 4, RANGE=0, LR_SMEM=0, IL=1>"
-# the unit that bounds the headline kernel (from its committed ncu summary)
-BINDING_UNIT_FP64_BLOCK4 = "not profiled"
+KERNEL_FP64_BLOCK4 = "fqhe_split_kernel<double, 4, RANGE=0, LR_SMEM=0, IL=1, W256=1, FORM=autotuned>"
 
 
 DIM = 7764392
@@ -71,15 +69,23 @@ def peaks():
     return 6650.0, "fallback"
 
 
+HEADLINE_PROFILE = os.path.join(ROOT, "profiles", "fqhe_block4_fp64_n12_2s33.md")
+
+
+def profile_field(key, number=True):
+    """A field of the committed ncu summary of the measured block product (None if absent)."""
+    if not os.path.exists(HEADLINE_PROFILE):
+        return None
+    for line in open(HEADLINE_PROFILE):
+        if line.startswith(key + ":"):
+            v = line.split(":", 1)[1].strip()
+            return float(v.split()[0]) if number else v
+    return None
+
+
 def profile_traffic():
     """DRAM bytes per launch of the measured block product from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "fqhe_block4_fp64_n12_2s33.md")
-    if not os.path.exists(p):
-        return None
-    for line in open(p):
-        if line.startswith("dram_bytes_per_launch:"):
-            return float(line.split(":")[1].split()[0])
-    return None
+    return profile_field("dram_bytes_per_launch")
 
 
 class ClockSampler:
@@ -589,9 +595,9 @@ def reference_cpu_long(rows_target_s=6.0):
 def momentum_sector(dh, flush, steps=5, k=2, length=32, warmup=2, solve=True):
     """Spin1_2ChainWithTranslations L = 32, Sz = 0, K = 0 with the J1-J2 Hamiltonian at J2 = J1/2
     (dimension 18,784,170): set-up time, FP32 block products of k vectors and FP64 single products
-    with their algorithmic bytes (per row: word, chain index, orbit size, FP64 y and diagonal x; per
-    element: one 8-byte map entry and one x gather), and the FP64 Lanczos time to E0 (-3L/8 at this
-    point)."""
+    with their algorithmic bytes (per row: word, orbit size, FP64 y and diagonal x; per element one x
+    gather: the flipped words are canonicalised in registers and found among the representatives,
+    search probes not counted), and the FP64 Lanczos time to E0 (-3L/8 at this point)."""
     import torch
     t0 = time.perf_counter()
     sp = dh.Spin1_2ChainWithTranslations(length, 0, 0)
@@ -621,12 +627,14 @@ def momentum_sector(dh, flush, steps=5, k=2, length=32, warmup=2, solve=True):
             torch.cuda.synchronize()
             ms.append(a.elapsed_time(b))
         xb = 4 if prec == "fp32" else 8
-        alg = dim * (9 + 16 * kk) + flips * (8 + xb * kk)
+        alg = dim * (5 + 16 * kk) + flips * xb * kk
         mean_s = statistics.mean(ms) / 1000.0
         out["%s_block_k%d" % (prec, kk)] = {
             "mean_launch_ms": mean_s * 1000.0, "hv_per_s": kk / mean_s, "algorithmic_bytes_per_launch": alg,
             "roofline": {"bound": "hbm", "achieved": alg / mean_s / 1e9, "peak": peak, "unit": "GB/s",
-                         "frac": alg / mean_s / 1e9 / peak, "peak_kind": kind}}
+                         "frac": alg / mean_s / 1e9 / peak, "peak_kind": kind,
+                         "limiter": "ALU: the canonical forms of the flipped words (ncu at L = 28: ALU 61 %, "
+                                    "issue 68 %, DRAM 1 %)"}}
         del x, y
     H.set_precision("fp64")
     if not solve:
@@ -813,7 +821,12 @@ def stored_elements(dh, H, flush, dim):
     H.set_precision("fp32")
     t = H.autotune(block_size=BLOCK, repeats=3)
     res["autotuned_k%d" % BLOCK] = {"stored_ms": t["stored_ms"], "best_ms": t["best_ms"],
-                                   "stored_in_use": t["stored_in_use"]}
+                                   "stored_in_use": t["stored_in_use"], "read_ahead": t["stored_read_ahead"]}
+    # both read-ahead depths of the FP32 single product, for the record
+    H.set_precision("fp32")
+    t1 = H.autotune(block_size=1, repeats=5)
+    res["autotuned_k1"] = {"stored_ms": t1["stored_ms"], "read_ahead": t1["stored_read_ahead"],
+                           "stream_gbs": stream_bytes / (t1["stored_ms"] / 1000.0) / 1e9}
     H.DisableFastMultiplication()
     return res
 
@@ -878,8 +891,11 @@ def run_b200(args, world, rank, local):
         elif args.leg == "sectors":
             r = time_to_e0_all_sectors(dh, runs=args.steps, precisions=(1e-10,))
         elif args.leg == "stored":
-            sp_ = dh.FermionOnSphere(N_FERMIONS, TWO_LZ, TWO_S)
-            H_ = dh.ParticleOnSphereGenericHamiltonian(sp_, N_FERMIONS, TWO_S, pseudopotentials(dh))
+            nf, ts = args.nbr_fermions, args.two_s
+            v_ = dh.coulomb_pseudopotentials(ts)
+            v_[0::2] = 0.0
+            sp_ = dh.FermionOnSphere(nf, 0 if (nf * ts) % 2 == 0 else 1, ts)
+            H_ = dh.ParticleOnSphereGenericHamiltonian(sp_, nf, ts, v_)
             H_.set_stream(stream.cuda_stream)
             H_.set_precision("fp32")
             r = stored_elements(dh, H_, flush, sp_.dim)
@@ -1028,7 +1044,7 @@ def run_b200(args, world, rank, local):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes(8, BLOCK),
-                         "kernel": KERNEL_FP64_BLOCK4, "binding_unit": BINDING_UNIT_FP64_BLOCK4,
+                         "kernel": KERNEL_FP64_BLOCK4, "limiter": profile_field("limiter", number=False),
                          "mean_launch_ms": launch_mean * 1000.0},
             "other_forms": other,
             "clocks": clocks.summary(),
@@ -1074,6 +1090,8 @@ def main():
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only the timed FP32 products (the short command used for ncu captures)")
+    ap.add_argument("--nbr-fermions", type=int, default=N_FERMIONS, help="with --leg stored: N")
+    ap.add_argument("--two-s", type=int, default=TWO_S, help="with --leg stored: 2S")
     ap.add_argument("--no-autotune", action="store_true",
                     help="with --kernel-only: skip the autotuner (kernel form from DH_FQHE_KERNEL / DH_FQHE_LOW_BITS)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],

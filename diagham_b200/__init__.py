@@ -413,11 +413,12 @@ class _Hamiltonian:
 
     def autotune(self, block_size=1, repeats=3):
         """Time the product's kernel forms on this Hamiltonian and keep the fastest one."""
-        out = np.zeros(10, np.float64)
+        out = np.zeros(11, np.float64)
         _check(_lib.dh_hamiltonian_autotune(self._handle, block_size, repeats, out.ctypes.data))
         return dict(best_ms=out[0], kernel_variant={0: "split", 1: "generic", 2: "split+smem"}[int(out[1])],
                     low_bits=int(out[2]), ms_k1=out[3], ms_k2=out[4], ms_k4=out[5], candidates=int(out[6]),
-                    stored_ms=out[7], stored_in_use=bool(out[8]), launch_form=SPLIT_FORMS[int(out[9])])
+                    stored_ms=out[7], stored_in_use=bool(out[8]), launch_form=SPLIT_FORMS[int(out[9])],
+                    stored_read_ahead=int(out[10]))
 
     def tune_block_size(self, max_iter=600, precision=1e-10, refined=True):
         """Block size (1, 2 or 4) with the shortest time to the converged ground energy, and the times."""

@@ -114,10 +114,12 @@ struct BlockEngine {
       if (ev_p0[i]) cudaEventDestroy(ev_p0[i]);
       if (ev_p1[i]) cudaEventDestroy(ev_p1[i]);
     }
-    if (stream) cudaStreamSynchronize(stream);
+    // the owner has waited for the stream (every record's event is waited on by the bookkeeping) and
+    // may already have destroyed it: nothing here touches the stream
     if (rec_host) cudaFreeHost(rec_host);
     if (rec_flags) cudaFreeHost(rec_flags);
     if (mask_host) cudaFreeHost(mask_host);
+    cudaGetLastError();  // leave no error of this clean-up for a later call to read
   }
 };
 
@@ -392,8 +394,12 @@ int engine_start(BlockEngine& e) {
 // FP64 check of a block X holding each sector's Ritz vectors: Y = H X with FP64 products,
 // E[s] = <x0|H x0> / <x0|x0> and r2[s] = |H x0 - E x0|^2 / |x0|^2 for the lowest vector x0 of every
 // sector.  Y is left holding the residual block.
+int engine_mask_all_active(BlockEngine& e);
+
 int engine_fp64_check(BlockEngine& e, const double* X, double* Y, std::vector<double>& E, std::vector<double>& r2) {
   const int k = e.k, kk = k * k;
+  int rc0 = engine_mask_all_active(e);
+  if (rc0 != DH_OK) return rc0;
   const int saved = e.precision;
   e.precision = DH_PRECISION_FP64;
   int rc = engine_product(e, X, Y);
@@ -453,6 +459,22 @@ int engine_sync_active(BlockEngine& e) {
   int* m = e.mask_host + (size_t)(e.issued % EngineRing) * e.nsec;
   for (int s = 0; s < e.nsec; ++s) m[s] = e.mask_sent[s] = e.sec[s].active ? 1 : 0;
   DH_CUDA(cudaMemcpyAsync(e.dActive, m, (size_t)e.nsec * sizeof(int), cudaMemcpyHostToDevice, e.stream));
+  return DH_OK;
+}
+
+// Products outside the recurrence (the FP64 check of Ritz blocks, the replay of recorded steps) cover
+// every sector: the device mask is set to all active (and re-sent from the sectors' flags at the next
+// issued step).
+int engine_mask_all_active(BlockEngine& e) {
+  if (!e.dActive) return DH_OK;
+  bool all = true;
+  for (int s = 0; s < e.nsec; ++s) all &= (e.mask_sent[s] == 1);
+  if (all) return DH_OK;
+  int* m = e.mask_host + (size_t)(e.issued % EngineRing) * e.nsec;
+  for (int s = 0; s < e.nsec; ++s) m[s] = e.mask_sent[s] = 1;
+  DH_CUDA(cudaMemcpyAsync(e.dActive, m, (size_t)e.nsec * sizeof(int), cudaMemcpyHostToDevice, e.stream));
+  // the slot may be reused by the next issued step's mask: wait for this copy to have read it
+  DH_CUDA(cudaStreamSynchronize(e.stream));
   return DH_OK;
 }
 
@@ -690,7 +712,9 @@ int engine_ritz(BlockEngine& e, double* out) {
     DH_CUDA(cudaStreamSynchronize(e.stream));
     return DH_OK;
   }
-  // replay: V_0 = start block; V_{j+1} = (H V_j - V_j A_j - V_{j-1} B_j^T) inv1_j inv2_j
+  // replay: V_0 = start block; V_{j+1} = (H V_j - V_j A_j - V_{j-1} B_j^T) inv1_j inv2_j, every sector
+  // enumerated (a sector's needed blocks came from steps where it was active)
+  if ((rc = engine_mask_all_active(e)) != DH_OK) return rc;
   DH_CUDA(cudaMemsetAsync(out, 0, (size_t)stride * sizeof(double), e.stream));
   double* V = e.slot[0];
   double* W = e.slot[1];

@@ -331,6 +331,7 @@ EllDevice ell_device(const dh_hamiltonian_s* h, int precision) {
   e.factors = precision == DH_PRECISION_FP32 ? h->factors32.ptr : h->factors64.ptr;
   e.dim = h->space->dim;
   e.nbr_factors = h->tabs.nbr_factors;
+  e.chunk = h->ell_chunk;
   return e;
 }
 
@@ -1023,7 +1024,7 @@ int dh_hamiltonian_enable_fast_multiplication(dh_hamiltonian_t h, int64_t allowe
   for (long long sl = 0; sl < nslices; ++sl) {
     int mx = 0;
     for (long long r = sl * 32; r < std::min(dim, sl * 32 + 32); ++r) mx = std::max(mx, counts[r]);
-    mx = (mx + kEllChunk - 1) / kEllChunk * kEllChunk;  // the product reads whole chunks
+    mx = (mx + kEllPad - 1) / kEllPad * kEllPad;  // the product reads whole chunks
     slice_ptr[sl] = total;
     slice_len[sl] = mx;
     total += 32ll * mx;
@@ -1306,12 +1307,24 @@ int dh_hamiltonian_autotune(dh_hamiltonian_t h, int block_size, int repeats, dou
     if ((rc = time_one(block_size, &best)) != DH_OK) return rc;
     tried = 1;
   }
-  // stored elements, when built: kept in use only if they beat the best on-the-fly form
+  // stored elements, when built, at both read-ahead depths: kept in use only if they beat the best
+  // on-the-fly form
   double stored_ms = 0.0;
   if (h->fast) {
     h->fast_use = true;
-    if ((rc = time_one(block_size, &stored_ms)) != DH_OK) return rc;
-    ++tried;
+    stored_ms = 1e300;
+    int best_chunk = 8;
+    for (int chunk : {8, 16}) {
+      h->ell_chunk = chunk;
+      double ms = 0.0;
+      if ((rc = time_one(block_size, &ms)) != DH_OK) return rc;
+      ++tried;
+      if (ms < stored_ms) {
+        stored_ms = ms;
+        best_chunk = chunk;
+      }
+    }
+    h->ell_chunk = best_chunk;
     if (stored_ms < best) best = stored_ms;
     else h->fast_use = false;
   }
@@ -1330,6 +1343,7 @@ int dh_hamiltonian_autotune(dh_hamiltonian_t h, int block_size, int repeats, dou
     out[5] = per_k[2];
     out[6] = tried;
     out[9] = sp->kind == SPACE_FERMION ? sp->split_form : 0;
+    out[10] = h->fast ? h->ell_chunk : 0;
   }
   return DH_OK;
 }

@@ -238,19 +238,21 @@ int launch_fqhe_count(const FqheDevice& f, unsigned long long* total, cudaStream
 int launch_fqhe_find(const FqheDevice& f, const uint64_t* words, long long n, long long* out, cudaStream_t s);
 
 // Stored elements of an FQHE Hamiltonian (sliced ELL, 32-row slices; see kernels_fast.cu)
-// Stored elements: per-row lengths of a slice are padded to a multiple of kEllChunk; within a slice a
-// row's elements come in groups of kEllGroup (one 16-byte load of targets per lane).
-constexpr int kEllChunk = 8;
+// Stored elements: per-row lengths of a slice are padded to a multiple of kEllPad; within a slice a
+// row's elements come in groups of kEllGroup (one 16-byte load of targets per lane); the product
+// reads chunks of 8 or 16 elements ahead of its gathers (EllDevice::chunk, chosen by the autotuner).
+constexpr int kEllPad = 16;
 constexpr int kEllGroup = 4;
 struct EllDevice {
-  const long long* slice_ptr;  // [nslices] first element of each slice (a multiple of 32 * kEllChunk)
-  const int* slice_len;        // [nslices] elements per row of the slice (padded to a multiple of kEllChunk)
+  const long long* slice_ptr;  // [nslices] first element of each slice (a multiple of 32 * kEllPad)
+  const int* slice_len;        // [nslices] elements per row of the slice (padded to a multiple of kEllPad)
   const int* cols;             // target index of each element
   const uint16_t* coef;        // factor index | sign << 15; padding holds nbr_factors (a zero factor)
   const void* diag;            // [dim] diagonal, FP64 or FP32 like the factors
   const void* factors;         // [nbr_factors] FP64 or FP32
   long long dim;
   int nbr_factors;
+  int chunk;                   // elements read ahead of the gathers: 8 or 16
 };
 int launch_fqhe_row_counts(const FqheDevice& f, int* counts, cudaStream_t s);
 int launch_fqhe_ell_fill(const FqheDevice& f, const long long* slice_ptr, const int* slice_len, int* cols,

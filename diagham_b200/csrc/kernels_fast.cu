@@ -6,7 +6,7 @@
 // AbstractQHEOnSphereHamiltonian.cc:3625,3814; QHEParticlePrecalculationOperation.cc:95).  Here the
 // lists are kept in device memory as sliced ELL: rows are grouped in slices of 32 consecutive rows
 // (one warp), every row of a slice is padded to the slice's longest row rounded up to a multiple of
-// kEllChunk, and the slice is stored in groups of kEllGroup elements per row: element j of lane l
+// kEllPad, and the slice is stored in groups of kEllGroup elements per row: element j of lane l
 // sits at slice_ptr + (j / G) * 32 G + l G + j % G, so one 16-byte load gives a lane G targets and
 // a warp reads 512 contiguous bytes per load.  Each element is an int32 target and a uint16 factor
 // index with the fermionic sign in bit 15; the structure does not depend on the pseudopotentials.
@@ -166,12 +166,12 @@ __device__ __forceinline__ void gather(const TG* x, const MatvecArgs& a, long lo
 }
 
 // y = H x from the stored elements: lanes own the 32 rows of a slice.  The element stream is read
-// kEllChunk elements ahead of the gathers (two 16-byte target loads and two 8-byte index loads per
+// CH elements ahead of the gathers (CH / 4 16-byte target loads and as many 8-byte index loads per
 // lane per chunk, issued before the chunk in hand is gathered), so every warp keeps a chunk of the
 // stream and a chunk of gathers in flight.  The stream, the diagonal and y go through L2 with
 // streaming (evict-first) accesses so that the gathered x keeps the cache.
 // W256: FP64 rows of 4 that are 32-byte aligned, gathered with one 256-bit load each
-template <typename TG, int K, bool IL, bool W256 = false>
+template <typename TG, int K, bool IL, bool W256, int CH>
 __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, MatvecArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   TG* sfac = reinterpret_cast<TG*>(smem);
@@ -182,7 +182,8 @@ __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, 
   const TG* x = static_cast<const TG*>(a.x);
   const TG* diag = static_cast<const TG*>(e.diag);
   const int lane = threadIdx.x & 31;
-  constexpr int NG = kEllChunk / kEllGroup;  // 16-byte target groups per chunk
+  static_assert(kEllPad % CH == 0 && CH % kEllGroup == 0, "chunks must tile the padded rows");
+  constexpr int NG = CH / kEllGroup;  // 16-byte target groups per chunk
   // a row range starts on a slice boundary (callers split at multiples of 32 rows)
   const long long r_end = a.out_last > 0 ? a.out_last : e.dim;
   const long long nslices = (r_end + 31) >> 5;
@@ -206,12 +207,12 @@ __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, 
         k[g] = __ldcs(kg + g * 32);
       }
     }
-    for (int j = 0; j < len; j += kEllChunk) {
+    for (int j = 0; j < len; j += CH) {
       int4 cn[NG];
       uint2 kn[NG];
-      const bool more = j + kEllChunk < len;
+      const bool more = j + CH < len;
       if (more) {
-        const int gn = (j + kEllChunk) / kEllGroup;
+        const int gn = (j + CH) / kEllGroup;
 #pragma unroll
         for (int g = 0; g < NG; ++g) {
           cn[g] = __ldcs(cg + (gn + g) * 32);
@@ -268,9 +269,11 @@ unsigned grid_for(long long n) {
 
 template <typename TG, int K, bool IL>
 int launch_ell_typed(const EllDevice& e, const MatvecArgs& a, cudaStream_t s) {
-  auto kern = ell_product_kernel<TG, K, IL>;
+  const bool deep = e.chunk == 16;
+  auto kern = deep ? ell_product_kernel<TG, K, IL, false, 16> : ell_product_kernel<TG, K, IL, false, 8>;
   if constexpr (IL && sizeof(TG) == 8 && K == 4)
-    if ((reinterpret_cast<uintptr_t>(a.x) & 31) == 0) kern = ell_product_kernel<TG, K, IL, true>;
+    if ((reinterpret_cast<uintptr_t>(a.x) & 31) == 0)
+      kern = deep ? ell_product_kernel<TG, K, IL, true, 16> : ell_product_kernel<TG, K, IL, true, 8>;
   const int smem = (e.nbr_factors + 1) * (int)sizeof(TG);
   if (smem > 48 * 1024) DH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int dev = 0, sms = 0, per_sm = 0;

@@ -217,9 +217,18 @@ __device__ __forceinline__ void load_row(const TG* x, const MatvecArgs& a, int i
   }
 }
 
+// acc + fa xa + fb xb with the roundings fixed: fb xb, then fused with fa xa, then added to acc
+// (left to the compiler, the contraction into FMAs may differ between launch forms)
+__device__ __forceinline__ double pair_term(double acc, double fa, double xa, double fb, double xb) {
+  return __dadd_rn(acc, __fma_rn(fa, xa, __dmul_rn(fb, xb)));
+}
+__device__ __forceinline__ float pair_term(float acc, float fa, float xa, float fb, float xb) {
+  return __fadd_rn(acc, __fmaf_rn(fa, xa, __fmul_rn(fb, xb)));
+}
+
 // The gathers of a row's elements, two targets per call.  PIPE: the two loads of a call are issued
 // before the previous call's values are used, so four target rows are in flight per thread; the
-// pairs are added in the same order either way (identical results).
+// pairs are added in the same order and with the same roundings either way (identical results).
 template <typename TG, int K, bool RANGE, bool IL, bool W256, bool PIPE>
 struct Gatherer {
   TG pa[K], pb[K];
@@ -238,7 +247,7 @@ struct Gatherer {
     load_row<TG, K, IL, W256>(x, a, ib, xb);
     if constexpr (PIPE) {
 #pragma unroll
-      for (int j = 0; j < K; ++j) acc[j] += pfa * pa[j] + pfb * pb[j];
+      for (int j = 0; j < K; ++j) acc[j] = pair_term(acc[j], pfa, pa[j], pfb, pb[j]);
 #pragma unroll
       for (int j = 0; j < K; ++j) {
         pa[j] = xa[j];
@@ -248,13 +257,13 @@ struct Gatherer {
       pfb = fb;
     } else {
 #pragma unroll
-      for (int j = 0; j < K; ++j) acc[j] += fa * xa[j] + fb * xb[j];
+      for (int j = 0; j < K; ++j) acc[j] = pair_term(acc[j], fa, xa[j], fb, xb[j]);
     }
   }
   __device__ __forceinline__ void finish(TG (&acc)[K]) {
     if constexpr (PIPE) {
 #pragma unroll
-      for (int j = 0; j < K; ++j) acc[j] += pfa * pa[j] + pfb * pb[j];
+      for (int j = 0; j < K; ++j) acc[j] = pair_term(acc[j], pfa, pa[j], pfb, pb[j]);
     }
   }
 };

@@ -172,28 +172,39 @@ __device__ __forceinline__ long long rep_find(const TransDevice& d, uint32_t c) 
   return (lo < d.dim && d.reps[lo] == c) ? lo : -1;
 }
 
-// the smallest of the L rotations of w (rotr1 steps) and the number n of steps to it, the first when
-// several rotations give it; L = 32 unrolled with funnel shifts (independent rotations)
+// rotation of an L-bit word by s sites towards the low bits (s rotr1 steps), 0 <= s < L
+__device__ __forceinline__ uint32_t rotr_by(uint32_t w, int s, int L, uint32_t mask) {
+  return s == 0 ? w : (((w >> s) | (w << (L - s))) & mask);
+}
+
+// The smallest of the L rotations of w (rotr1 steps) and the number n of steps to it, the first (the
+// smallest n) when several rotations give it.  The smallest rotation starts with the longest run of
+// zeros at its top, so only the rotations that put a longest zero run there are compared: with
+// A_t bit p = 1 iff bits p .. p + t - 1 (cyclically) of w are all zero, the longest run length T is
+// the last t with A_t != 0, and each run start p in A_T gives the candidate n = p + T (mod L).
 __device__ __forceinline__ uint32_t canonical_rotation(uint32_t w, int L, uint32_t mask, int& n) {
-  uint32_t c = w;
+  const uint32_t z = ~w & mask;
   n = 0;
-  if (L == 32) {
-#pragma unroll
-    for (int j = 1; j < 32; ++j) {
-      const uint32_t r = __funnelshift_r(w, w, j);
-      if (r < c) {
-        c = r;
-        n = j;
-      }
-    }
-  } else {
-    uint32_t r = w;
-    for (int j = 1; j < L; ++j) {
-      r = rotr1(r, L, mask);
-      if (r < c) {
-        c = r;
-        n = j;
-      }
+  if (z == 0) return w;  // all ones: every rotation is w
+  uint32_t a = z;
+  int t = 1;
+  while (t < L) {
+    const uint32_t next = a & rotr_by(z, t, L, mask);
+    if (next == 0) break;
+    a = next;
+    ++t;
+  }
+  // candidates in increasing n: n = (p + t) mod L for every set bit p of a
+  const uint32_t cand = rotr_by(a, L - t, L, mask);  // bit (p + t) mod L for each p
+  uint32_t c = 0xffffffffu;
+  uint32_t rem = cand;
+  while (rem) {
+    const int j = __ffs(rem) - 1;
+    rem &= rem - 1u;
+    const uint32_t r = rotr_by(w, j, L, mask);
+    if (r < c) {
+      c = r;
+      n = j;
     }
   }
   return c;
@@ -269,11 +280,17 @@ __device__ __forceinline__ void trans_gather(const TG* x, const MatvecArgs& a, l
   }
 }
 
-struct TransShared {
-  SpinTables tb;
+// per-block constants; the step tables only where flipped words are ranked (the map form)
+struct TransCoefficients {
   double ratio[33 * 33];  // sqrt(o_s / o_t)
   double phase[32];       // cos(2 pi K m / L)
 };
+template <bool CANON>
+struct TransShared : TransCoefficients {
+  SpinTables tb;
+};
+template <>
+struct TransShared<true> : TransCoefficients {};
 
 // the antiparallel bonds of a representative, one flip at a time: the flipped word's plain chain
 // index (from the row's own index and the step tables) and J / 2 of the bond
@@ -381,8 +398,8 @@ constexpr int kTransBatch = 4;
 // CANON: targets from canonicalising the flipped words (no whole-sector map)
 template <typename TG, int K, bool IL, bool RANGE, bool CANON>
 __global__ void __launch_bounds__(kTransThreads) trans_matvec_kernel(TransDevice d, MatvecArgs a) {
-  __shared__ TransShared sh;
-  build_spin_tables(sh.tb, d.length);
+  __shared__ TransShared<CANON> sh;
+  if constexpr (!CANON) build_spin_tables(sh.tb, d.length);
   for (int i = threadIdx.x; i < 33 * 33; i += blockDim.x) {
     const int os = i / 33, ot = i % 33;
     sh.ratio[i] = (os > 0 && ot > 0) ? sqrt((double)os / (double)ot) : 0.0;
@@ -418,7 +435,7 @@ __global__ void __launch_bounds__(kTransThreads) trans_matvec_kernel(TransDevice
           have[q] = more && next_flip_mask<TG>(cur, L, hj1, hj2, fm, hj[q]);
           ci[q] = (int)fm;
         } else {
-          have[q] = more && next_flip<TG>(cur, sh.tb, L, D, hj1, hj2, ci[q], hj[q]);
+          if constexpr (!CANON) have[q] = more && next_flip<TG>(cur, sh.tb, L, D, hj1, hj2, ci[q], hj[q]);
         }
         more = have[q];
       }
@@ -468,11 +485,18 @@ __global__ void __launch_bounds__(kTransThreads) trans_matvec_kernel(TransDevice
   }
 }
 
+template <bool CANON>
 struct TransSharedComplex {
-  SpinTables tb;
   double ratio[33 * 33];  // sqrt(o_s / o_t)
   double phase[32];       // cos(2 pi K m / L)
   double sine[32];        // sin(2 pi K m / L)
+  SpinTables tb;
+};
+template <>
+struct TransSharedComplex<true> {
+  double ratio[33 * 33];
+  double phase[32];
+  double sine[32];
 };
 
 // SpinChainJ1J2HamiltonianWithTranslations (any K) on complex vectors stored as (Re, Im) pairs; the
@@ -482,8 +506,8 @@ struct TransSharedComplex {
 // conjugate: y[s] += conj(h(s -> t)) x[t].
 template <typename TG, bool RANGE, bool CANON>
 __global__ void __launch_bounds__(kTransThreads) trans_matvec_complex_kernel(TransDevice d, MatvecArgs a) {
-  __shared__ TransSharedComplex sh;
-  build_spin_tables(sh.tb, d.length);
+  __shared__ TransSharedComplex<CANON> sh;
+  if constexpr (!CANON) build_spin_tables(sh.tb, d.length);
   for (int i = threadIdx.x; i < 33 * 33; i += blockDim.x) {
     const int os = i / 33, ot = i % 33;
     sh.ratio[i] = (os > 0 && ot > 0) ? sqrt((double)os / (double)ot) : 0.0;
@@ -520,7 +544,7 @@ __global__ void __launch_bounds__(kTransThreads) trans_matvec_complex_kernel(Tra
           have[q] = more && next_flip_mask<TG>(cur, L, hj1, hj2, fm, hj[q]);
           ci[q] = (int)fm;
         } else {
-          have[q] = more && next_flip<TG>(cur, sh.tb, L, (int)d.chain_dim, hj1, hj2, ci[q], hj[q]);
+          if constexpr (!CANON) have[q] = more && next_flip<TG>(cur, sh.tb, L, (int)d.chain_dim, hj1, hj2, ci[q], hj[q]);
         }
         more = have[q];
       }

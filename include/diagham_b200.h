@@ -283,8 +283,10 @@ int dh_hamiltonian_disable_fast_multiplication(dh_hamiltonian_t h);
  * 1 generic, 2 staged table), LB, ms per product of blocks of 1, 2 and 4 vectors with the chosen
  * form, number of candidates timed, ms of the stored-element product (0: none), 1 if the stored
  * elements are in use, launch form of the split-word kernel (0 .. 7: 256 threads x 4 resident
- * blocks, 256 x 3, 256 x 3 pipelined, 256 x 2 pipelined, 128 x 8, 256 x 2, 192 x 4, 128 x 6). */
-#define DH_TUNE_RESULTS 10
+ * blocks, 256 x 3, 256 x 3 pipelined, 256 x 2 pipelined, 128 x 8, 256 x 2, 192 x 4, 128 x 6), the
+ * stored-element product's read-ahead depth per lane (8 or 16 elements; 0 without stored elements),
+ * which is timed at both depths. */
+#define DH_TUNE_RESULTS 11
 int dh_hamiltonian_autotune(dh_hamiltonian_t h, int block_size, int repeats, double* out);
 
 /* AbstractHamiltonian::MatrixElement(V1, V2) (AbstractQHEOnSphereHamiltonian.cc:380): <v1|H|v2>. */
