@@ -392,6 +392,8 @@ def time_to_e0_all_sectors(dh, k=None, runs=3, precisions=(1e-10, 1e-13)):
                 "setup_seconds": r["setup_seconds"], "solve_seconds": r["solve_seconds"],
                 "product_seconds": r["product_seconds"], "fp32_seconds": r["fp32_seconds"],
                 "refine_seconds": r["refine_seconds"], "refined_sectors": r["refined_sectors"],
+                "dense_fallback_sectors": r["dense_fallback_sectors"],
+                "dense_fallback_seconds": r["dense_fallback_seconds"],
                 "speedup_vs_plain_fp64": tp / t}
         out["precision_%g" % precision] = res
         if precision == min(precisions):

@@ -729,14 +729,15 @@ def fqhe_sectors_block_lanczos(nbr_fermions, lz_max, total_lz, pseudopotentials,
     ns = tl.size
     e = np.zeros(ns, np.float64)
     it = np.zeros(ns, np.int32)
-    secs = np.zeros(8, np.float64)
+    secs = np.zeros(10, np.float64)
     _check(_lib.dh_fqhe_sectors_block_lanczos(nbr_fermions, lz_max, tl.ctypes.data, ns, v.ctypes.data, block_size,
                                               max_iter, float(precision),
                                               DH_PRECISION_FP32 if fp32 else DH_PRECISION_FP64, full_diag_limit, seed,
                                               e.ctypes.data, it.ctypes.data, secs.ctypes.data))
     return dict(energies=e, iterations=it, setup_seconds=secs[0], solve_seconds=secs[1], product_seconds=secs[2],
                 block_products=int(secs[3]), fp32_seconds=secs[4], refine_seconds=secs[5],
-                refined_sectors=int(secs[6]), max_refine_shift=secs[7])
+                refined_sectors=int(secs[6]), max_refine_shift=secs[7], dense_fallback_sectors=int(secs[8]),
+                dense_fallback_seconds=secs[9])
 
 
 def WriteVector(vec, file_name):

@@ -66,6 +66,8 @@ struct BlockEngine {
   // (|r| = |B_m s_last| from the band matrix), used by the mixed-precision restarts whose Ritz
   // values move at the FP32 rounding level long after the vector is accurate enough
   double residual_target = 0.0;
+  // with residual_target: also stop a sector whose lowest Ritz value no longer moves (1e-13)
+  bool stop_on_stagnation = false;
   int max_iter = 400;  // in vectors, as the reference's --iter-max
   long long total = 0;
   std::vector<long long> off;
@@ -784,7 +786,22 @@ int sector_evaluate(const BlockEngine& e, BlockSector& b) {
     // the lowest eigenvector of the band matrix by inverse iteration at the known l0
     std::vector<double> t, C((size_t)b.blocks * e.k);
     sector_band_matrix(e, b, t);
-    if ((rc = band_inverse_iteration(b.blocks * e.k, std::max(1, 2 * e.k - 1), t.data(), l0, C.data())) != DH_OK) return rc;
+    const int n = b.blocks * e.k;
+    rc = band_inverse_iteration(n, std::max(1, 2 * e.k - 1), t.data(), l0, C.data());
+    // a nearly degenerate lowest pair (or a failed solve) leaves a mixed vector: check T s = l0 s,
+    // else take the dense eigensolve's vector
+    double res = 0.0, nrm = 0.0;
+    if (rc == DH_OK)
+      for (int i = 0; i < n; ++i) {
+        double v = -l0 * C[i];
+        for (int j = std::max(0, i - 2 * e.k); j <= std::min(n - 1, i + 2 * e.k); ++j) v += t[(size_t)i * n + j] * C[j];
+        res += v * v;
+        nrm += C[i] * C[i];
+      }
+    if (rc != DH_OK || !(res <= 1e-20 * std::max(1.0, l0 * l0) * nrm)) {
+      std::vector<double> vals;
+      if ((rc = sector_ritz_coefficients(e, b, 1, C, vals)) != DH_OK) return rc;
+    }
     const int k = e.k, m = b.blocks;
     const double* Bm = &b.B[(size_t)m * k * k];  // X_m = V_m B_m: the block after the last A
     double r2 = 0.0;
@@ -794,8 +811,8 @@ int sector_evaluate(const BlockEngine& e, BlockSector& b) {
       r2 += v * v;
     }
     if (r2 < e.residual_target * fabs(b.ritz[0])) b.converged = true;
-    // a Ritz value that no longer moves at all: the products' rounding floor is reached
-    if (fabs(l0 - b.prev_last) < 1e-13 * fabs(l0)) b.converged = true;
+    // (FP32 phase) a Ritz value that no longer moves at all: the products' rounding floor is reached
+    if (e.stop_on_stagnation && fabs(l0 - b.prev_last) < 1e-13 * fabs(l0)) b.converged = true;
     return DH_OK;
   }
   if ((int)b.ritz.size() > e.nev) {
@@ -1361,8 +1378,8 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
     energies[s] = ev[0];
     iterations[s] = 0;
   }
-  double fp32_seconds = 0.0, refine_seconds = 0.0, max_shift = 0.0;
-  int refined = 0;
+  double fp32_seconds = 0.0, refine_seconds = 0.0, max_shift = 0.0, dense_seconds = 0.0;
+  int refined = 0, dense_fallback = 0;
   long long products = 0;
   double product_ms = 0.0;
   if (!lanczos_sectors.empty()) {
@@ -1370,8 +1387,10 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
     e.eig_precision = precision == DH_PRECISION_FP32 ? std::max(e.eig_precision, 1e-9) : e.eig_precision;
     // the FP32 phase stops on each sector's Ritz residual (from its band matrix) rather than on the
     // Ritz value's change, so that the FP64 check after it passes without a restart
-    if (precision == DH_PRECISION_FP32)
+    if (precision == DH_PRECISION_FP32) {
       e.residual_target = fp32_phase_residual_target(precision_target > 0.0 ? precision_target : 1e-14);
+      e.stop_on_stagnation = true;
+    }
     if ((rc = engine_setup(e, dims)) != DH_OK) return rc;
     if (precision == DH_PRECISION_FP32) engine_store_if_fits(e);
     SectorProduct prod;
@@ -1389,11 +1408,12 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
     }
     products += e.products;
     product_ms += e.product_ms;
-    // exhausted sectors whose band matrix is not exact (rank lost in the last block, or FP32
-    // products) are small: they are diagonalised densely in FP64 at the end
+    // exhausted sectors whose band matrix is not exact (rank lost in the last block) are small: with
+    // FP64 products they are diagonalised densely in FP64 at the end; with FP32 products the FP64
+    // check of the refinement decides, and only a sector it cannot certify goes dense
     std::vector<char> need_dense(ns, 0);
     for (int i = 0; i < ns; ++i)
-      need_dense[i] = e.sec[i].exhausted && (e.sec[i].partial || precision == DH_PRECISION_FP32) &&
+      need_dense[i] = precision == DH_PRECISION_FP64 && e.sec[i].exhausted && e.sec[i].partial &&
                       e.sec[i].dim <= kDenseFallbackLimit;
     const auto tb = clk::now();
     fp32_seconds = precision == DH_PRECISION_FP32 ? std::chrono::duration<double>(tb - ta).count() : 0.0;
@@ -1433,7 +1453,13 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
           product_ms = e.product_ms;
         }
         if (round == 0) refined = (int)redo.size();
-        if (redo.empty() || round == 3) break;
+        if (redo.empty()) break;
+        if (round == 3) {
+          // not certified after the last restart: small sectors are diagonalised densely
+          for (int i : redo)
+            if (e.sec[i].dim <= kDenseFallbackLimit) need_dense[i] = 1;
+          break;
+        }
         auto f = std::make_unique<BlockEngine>();
         f->k = k;
         f->nev = 1;
@@ -1460,7 +1486,6 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
         for (size_t jj = 0; jj < redo.size(); ++jj) {
           const BlockSector& bs = f->sec[jj];
           iterations[rsec[jj]] += bs.count;
-          if (bs.exhausted && bs.partial && bs.dim <= kDenseFallbackLimit) need_dense[redo[jj]] = 1;
           src_pos[redo[jj]] = (int)jj;
         }
         pending.clear();
@@ -1472,6 +1497,7 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
       }
       refine_seconds = std::chrono::duration<double>(clk::now() - tb).count();
     }
+    const auto td = clk::now();
     for (int i = 0; i < ns; ++i) {
       if (!need_dense[i]) continue;
       const int s = lanczos_sectors[i];
@@ -1479,7 +1505,9 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
       if ((rc = dense_lowest(hb.spaces[s], hb, 1, ev, e.stream)) != DH_OK) return rc;
       if (precision == DH_PRECISION_FP32) max_shift = std::max(max_shift, fabs(ev[0] - energies[s]));
       energies[s] = ev[0];
+      ++dense_fallback;
     }
+    dense_seconds = std::chrono::duration<double>(clk::now() - td).count();
   }
   const auto t2 = clk::now();
   if (stats) {
@@ -1491,6 +1519,8 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
     stats[5] = refine_seconds;
     stats[6] = (double)refined;
     stats[7] = max_shift;
+    stats[8] = (double)dense_fallback;
+    stats[9] = dense_seconds;
   }
   return DH_OK;
 }

@@ -73,7 +73,7 @@ struct dh_hamiltonian_s {
   // stored elements (fast multiplication): built by dh_hamiltonian_enable_fast_multiplication
   bool fast = false;
   bool fast_use = true;  // products read the stored elements (the autotuner may prefer the on-the-fly form)
-  int ell_chunk = 8;     // stored elements read ahead of the gathers per lane: 8 or 16
+  int ell_chunk = 16;    // stored elements read ahead of the gathers per lane: 8 or 16
   long long fast_elements = 0;  // stored elements, padding included
   size_t fast_bytes = 0;
   dh::DevBuf ell_slice_ptr, ell_slice_len, ell_cols, ell_coef, diag64, diag32;

@@ -507,18 +507,20 @@ int dh_complex_vector_read(const char* file_name, double* pairs, int64_t dim);
  * Sectors of dimension <= full_diag_limit (or <= 2 block_size) are diagonalised densely, as
  * QHEOnSphereMainTask does below --full-diag (:397); so are sectors whose block Krylov space runs
  * out with a band matrix that is not exact (a last block that only lost rank, or FP32 products).
- * precision == DH_PRECISION_FP32: FP32 products with the FP64 recurrence until the Ritz values
- * settle to max(precision_target, 1e-9); then every sector's lowest Ritz vector gets an FP64
+ * precision == DH_PRECISION_FP32: FP32 products with the FP64 recurrence until each sector's Ritz
+ * residual (from its band matrix) falls below max(0.1 precision_target, 1e-11) |E| or its lowest Ritz
+ * value stops moving; then every sector's lowest Ritz vector gets an FP64
  * Rayleigh quotient and residual, and the sectors whose |r|^2 > precision_target |E| are polished
  * by an FP64 block Lanczos restarted from their Ritz blocks, all of them in lockstep.
  * energies[s] = lowest eigenvalue of sector s, iterations[s] = the driver's counter (both phases;
  * 0 for dense sectors); stats (optional, DH_SECTOR_STATS values): set-up seconds, solve seconds,
  * device time of the block products, number of block products, FP32-phase seconds, refinement
- * seconds, number of sectors restarted in FP64, largest |E_refined - E_FP32| over the sectors.
+ * seconds, number of sectors restarted in FP64, largest |E_refined - E_FP32| over the sectors,
+ * number of sectors diagonalised densely after an exhausted Krylov space, seconds spent on them.
  * The sectors share the split-word rank tables: lz_max <= 40 (DH_ERR_UNSUPPORTED above).  The
  * Krylov blocks the refinement needs are kept in device memory as far as half of the free memory
  * allows (growing with the run), else rebuilt by replaying the recurrence. */
-#define DH_SECTOR_STATS 8
+#define DH_SECTOR_STATS 10
 int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const int* total_lz, int nbr_sectors,
                                   const double* pseudopotentials, int block_size, int max_iter,
                                   double precision_target, int precision, int full_diag_limit,
