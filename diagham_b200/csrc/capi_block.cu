@@ -432,12 +432,13 @@ int engine_fp64_check(BlockEngine& e, const double* X, double* Y, std::vector<do
 // following ones FP32, and every new block is projected against it.  The Krylov space is the one
 // an FP64 restart would build; the FP32 products only touch directions whose coefficients in the
 // refined ground state are of the order of the Ritz vector's residual.
-int engine_mixed_restart(BlockEngine& e, uint64_t seed) {
+// fp64: every product of the restart in FP64 (the last resort of the batched refinement)
+int engine_mixed_restart(BlockEngine& e, uint64_t seed, bool fp64 = false) {
   int rc;
   if ((rc = launch_random_block(e.slot[0], e.total, e.k, e.row_offset_dev, e.tiles, seed, e.stream, 1)) != DH_OK)
     return rc;
-  e.precision = DH_PRECISION_FP32;
-  e.fp64_first_product = true;
+  e.precision = fp64 ? DH_PRECISION_FP64 : DH_PRECISION_FP32;
+  e.fp64_first_product = !fp64;
   e.lock_start = true;
   for (auto& b : e.sec) b.exhausted = b.partial = false;
   return engine_start(e);
@@ -1454,16 +1455,19 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
         }
         if (round == 0) refined = (int)redo.size();
         if (redo.empty()) break;
-        if (round == 3) {
-          // not certified after the last restart: small sectors are diagonalised densely
+        if (round == 4) {
+          // not certified after the FP64 restart either: small sectors are diagonalised densely
           for (int i : redo)
             if (e.sec[i].dim <= kDenseFallbackLimit) need_dense[i] = 1;
           break;
         }
+        // rounds 0-2 restart with FP32 products after an FP64 first one; a sector still above the
+        // target after them restarts with FP64 products throughout
+        const bool fp64_round = round == 3;
         auto f = std::make_unique<BlockEngine>();
         f->k = k;
         f->nev = 1;
-        f->precision = DH_PRECISION_FP32;
+        f->precision = fp64_round ? DH_PRECISION_FP64 : DH_PRECISION_FP32;
         f->eig_precision = precision_target > 0.0 ? precision_target : 1e-14;
         f->residual_target = restart_residual_target(f->eig_precision);
         f->max_iter = std::min(max_iter, 100 * k);
@@ -1481,7 +1485,7 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
                                   (size_t)rdims[jj] * k * sizeof(double), cudaMemcpyDeviceToDevice, f->stream));
         auto fprod = std::make_unique<SectorProduct>();
         if ((rc = bind_sector_product(hb, rsec, *f, *fprod)) != DH_OK) return rc;
-        if ((rc = engine_mixed_restart(*f, seed + 1000 + round)) != DH_OK) return rc;
+        if ((rc = engine_mixed_restart(*f, seed + 1000 + round, fp64_round)) != DH_OK) return rc;
         if ((rc = engine_solve(*f)) != DH_OK) return rc;
         for (size_t jj = 0; jj < redo.size(); ++jj) {
           const BlockSector& bs = f->sec[jj];
