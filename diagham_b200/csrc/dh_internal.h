@@ -163,6 +163,15 @@ struct MatvecArgs {
   long long out_first, out_last; // rows computed: [out_first, out_last); out_last = 0: every row
 };
 
+// The row-interleaved kernels read a row's K values (and may write its K outputs) with one vector
+// access: the x, y and xdiag pointers must be aligned to that access (at most 16 bytes), else the
+// strided kernels are used.  elem = sizeof(TG) of the gathered x.
+inline bool il_rows_aligned(const MatvecArgs& a, int k, int elem) {
+  const uintptr_t ax = (uintptr_t)(k * elem < 16 ? k * elem : 16);
+  const uintptr_t ay = (uintptr_t)(k * 8 < 16 ? k * 8 : 16);
+  return ((uintptr_t)a.x % ax) == 0 && ((uintptr_t)a.y % ay) == 0 && ((uintptr_t)a.xdiag % ay) == 0;
+}
+
 // Every Lz sector of one system in one launch (rows concatenated, vectors K-interleaved).
 struct SectorBatchDevice {
   const uint64_t* const* words;       // [nbr_sectors] device pointers (array in device memory)

@@ -302,7 +302,7 @@ int launch_rank(const FqheDevice& f, const MatvecArgs& a, cudaStream_t s) {
   size_t smem = (size_t)factor_smem + (size_t)((f.nbr_pairs + 3) & ~3) * sizeof(int);
   if (RM == 1) smem += 2 * (size_t)(f.nbr_particles + 1) * kBosonThreads * sizeof(int);
   const bool range = a.col_first > 0 || a.col_last < f.dim;
-  const bool il = (K > 1) && a.ld == K && a.vstride == 1;
+  const bool il = (K > 1) && a.ld == K && a.vstride == 1 && il_rows_aligned(a, K, sizeof(TG));
   auto kernel = range ? (il ? boson_matvec_kernel<TG, K, true, true, RM> : boson_matvec_kernel<TG, K, true, false, RM>)
                       : (il ? boson_matvec_kernel<TG, K, false, true, RM> : boson_matvec_kernel<TG, K, false, false, RM>);
   if (smem > 48 * 1024) DH_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

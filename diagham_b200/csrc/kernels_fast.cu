@@ -294,7 +294,8 @@ int launch_ell_typed(const EllDevice& e, const MatvecArgs& a, cudaStream_t s) {
 template <typename TG>
 int launch_ell_k(const EllDevice& e, MatvecArgs a, cudaStream_t s) {
   const int nv = a.nbr_vectors;
-  if ((nv == 2 || nv == 4) && a.ld == nv && a.vstride == 1 && a.ld_y == nv && a.vstride_y == 1)
+  if ((nv == 2 || nv == 4) && a.ld == nv && a.vstride == 1 && a.ld_y == nv && a.vstride_y == 1 &&
+      il_rows_aligned(a, nv, sizeof(TG)))
     return nv == 4 ? launch_ell_typed<TG, 4, true>(e, a, s) : launch_ell_typed<TG, 2, true>(e, a, s);
   // separate or strided vectors: groups of 4, 2 and 1 sharing one pass over the elements
   int left = nv, done = 0;

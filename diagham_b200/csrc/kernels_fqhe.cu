@@ -562,7 +562,7 @@ int launch_one(const FqheDevice& f, const MatvecArgs& a, cudaStream_t s) {
         kern = split_form_kernel<TG, K, false, false>(form);
         if constexpr (K > 1) {
           // row-interleaved blocks (block Lanczos): vector loads of the K values of a target row
-          if (a.ld == K && a.vstride == 1 && a.ld_y == K && a.vstride_y == 1) {
+          if (a.ld == K && a.vstride == 1 && a.ld_y == K && a.vstride_y == 1 && il_rows_aligned(a, K, sizeof(TG))) {
             kern = split_form_kernel<TG, K, true, false>(form);
             if constexpr (sizeof(TG) == 8 && K == 4)
               if ((reinterpret_cast<uintptr_t>(a.x) & 31) == 0) kern = split_form_kernel<TG, K, true, true>(form);

@@ -283,7 +283,8 @@ int launch_spin_typed(const SpinDevice& sp, MatvecArgs a, cudaStream_t s) {
     return DH_OK;
   }
   const int nv = a.nbr_vectors;
-  if ((nv == 2 || nv == 4) && a.ld == nv && a.vstride == 1 && a.ld_y == nv && a.vstride_y == 1) {
+  if ((nv == 2 || nv == 4) && a.ld == nv && a.vstride == 1 && a.ld_y == nv && a.vstride_y == 1 &&
+      il_rows_aligned(a, nv, sizeof(TG))) {
     // row-interleaved block: one launch with vector gathers and stores
     auto kern = (nv == 4) ? spin_j1j2_kernel<TG, 4, true> : spin_j1j2_kernel<TG, 2, true>;
     int per_sm = 0;

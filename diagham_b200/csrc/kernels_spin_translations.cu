@@ -673,7 +673,8 @@ __global__ void trans_find_kernel(TransDevice d, const uint64_t* words, long lon
 template <typename TG, int K>
 int launch_trans_typed(const TransDevice& d, const MatvecArgs& a, cudaStream_t s) {
   const bool range = a.col_first > 0 || a.col_last < d.dim;
-  const bool il = (K > 1) && a.ld == K && a.vstride == 1 && a.ld_y == K && a.vstride_y == 1;
+  const bool il = (K > 1) && a.ld == K && a.vstride == 1 && a.ld_y == K && a.vstride_y == 1 &&
+                  il_rows_aligned(a, K, sizeof(TG));
   auto kern = range ? (il ? trans_matvec_kernel<TG, K, true, true, true> : trans_matvec_kernel<TG, K, false, true, true>)
                     : (il ? trans_matvec_kernel<TG, K, true, false, true> : trans_matvec_kernel<TG, K, false, false, true>);
   if (d.map)

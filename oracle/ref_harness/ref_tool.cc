@@ -522,7 +522,7 @@ static void Usage()
 	  "  spint_lanczos L 2Sz K J1 J2 maxiter precision out x0\n"
 	  "  spintc_matvec L 2Sz K J1 J2 xfile out\n"
 	  "  spintc_dense L 2Sz K J1 J2 out\n"
-	  "  bench_fqhe N 2S 2Lz vfile threads reps hermitian [rows]\n"
+	  "  bench_fqhe N 2S 2Lz vspec threads reps hermitian [rows]\n"
 	  "  bench_fqhe_block N 2S 2Lz vspec threads reps hermitian k windows\n"
 	  "  bench_bqhe N 2S 2Lz vfile threads reps hermitian [rows]\n"
 	  "  bench_lfqhe N 2S 2Lz vfile threads reps hermitian [rows]\n"
@@ -1147,7 +1147,7 @@ int main(int argc, char** argv)
       // SMP operation splits between its threads, AbstractArchitecture.cc:65) is set to the first
       // `rows` rows instead of the whole space.
       int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
-      double* V = ReadDoubles(argv[5], LzMax + 1);
+      double* V = PseudopotentialsFromSpec(argv[5], LzMax);
       int Threads = atoi(argv[6]);
       int Reps = atoi(argv[7]);
       bool Hermitian = atoi(argv[8]) != 0;
