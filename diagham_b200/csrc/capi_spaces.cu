@@ -327,6 +327,7 @@ EllDevice ell_device(const dh_hamiltonian_s* h, int precision) {
   e.slice_len = h->ell_slice_len.as<int>();
   e.cols = h->ell_cols.as<int>();
   e.coef = h->ell_coef.as<uint16_t>();
+  e.coef32 = h->ell_coef32.as<uint32_t>();
   e.diag = precision == DH_PRECISION_FP32 ? h->diag32.ptr : h->diag64.ptr;
   e.factors = precision == DH_PRECISION_FP32 ? h->factors32.ptr : h->factors64.ptr;
   e.dim = h->space->dim;
@@ -337,8 +338,10 @@ EllDevice ell_device(const dh_hamiltonian_s* h, int precision) {
 
 int refresh_fast_diagonal(dh_hamiltonian_s* h) {
   if (!h->fast) return DH_OK;
-  int rc = launch_fqhe_diag(fqhe_device(h->space, h, DH_PRECISION_FP64), h->factors64.as<double>(),
-                            h->diag64.as<double>(), h->diag32.as<float>(), h->stream);
+  const FqheDevice f = fqhe_device(h->space, h, DH_PRECISION_FP64);
+  int rc = (h->kind == SPACE_BOSON)
+               ? launch_boson_diag(f, h->factors64.as<double>(), h->diag64.as<double>(), h->diag32.as<float>(), h->stream)
+               : launch_fqhe_diag(f, h->factors64.as<double>(), h->diag64.as<double>(), h->diag32.as<float>(), h->stream);
   if (rc != DH_OK) return rc;
   DH_CUDA(cudaStreamSynchronize(h->stream));
   return DH_OK;
@@ -385,7 +388,10 @@ int hamiltonian_apply_rows(dh_hamiltonian_s* h, const double* x, double* y, int 
     a.x = x;
     a.xdiag = nullptr;
   }
-  if (sp->kind == SPACE_BOSON) return launch_boson_matvec(fqhe_device(sp, h, h->precision), a, h->precision, stream);
+  if (sp->kind == SPACE_BOSON) {
+    if (h->fast && h->fast_use && first == 0 && nbr == dim) return launch_ell_product(ell_device(h, h->precision), a, h->precision, stream);
+    return launch_boson_matvec(fqhe_device(sp, h, h->precision), a, h->precision, stream);
+  }
   if (sp->kind == SPACE_SPIN12_TRANSLATIONS) return launch_trans_matvec(trans_device(sp, h), a, h->precision, stream);
   if (sp->kind == SPACE_FERMION_LONG) return launch_long_matvec(fqhe_long_device(sp, h, h->precision), a, h->precision, stream);
   if (sp->kind == SPACE_FERMION) {
@@ -428,7 +434,10 @@ int hamiltonian_apply_block_rows(dh_hamiltonian_s* h, const double* x64, const f
     a.xdiag = nullptr;
   }
   int rc;
-  if (sp->kind == SPACE_BOSON) return launch_boson_matvec(fqhe_device(sp, h, precision), a, precision, stream);
+  if (sp->kind == SPACE_BOSON) {
+    if (h->fast && h->fast_use) return launch_ell_product(ell_device(h, precision), a, precision, stream);
+    return launch_boson_matvec(fqhe_device(sp, h, precision), a, precision, stream);
+  }
   if (sp->kind == SPACE_SPIN12_TRANSLATIONS) return launch_trans_matvec(trans_device(sp, h), a, precision, stream);
   if (sp->kind == SPACE_FERMION_LONG) return launch_long_matvec(fqhe_long_device(sp, h, precision), a, precision, stream);
   if (sp->kind == SPACE_FERMION) {
@@ -861,7 +870,6 @@ int dh_particle_on_sphere_generic_hamiltonian_create(dh_space_t sp, int nbr_part
            "Hamiltonian (N = %d, lz_max = %d) does not match its space (N = %d, lz_max = %d)", nbr_particles, lz_max,
            sp->nbr_fermions, space_lz_max);
   DH_CHECK(l2_factor == 0.0 || nbr_particles >= 2, DH_ERR_UNSUPPORTED, "an L^2 term needs at least two particles");
-  DH_CHECK(l2_factor == 0.0 || !bosons, DH_ERR_UNSUPPORTED, "the L^2 term is implemented for fermions");
   dh_hamiltonian_s* h = new (std::nothrow) dh_hamiltonian_s();
   DH_CHECK(h, DH_ERR_MEMORY, "out of host memory");
   h->space = sp;
@@ -907,8 +915,8 @@ int dh_particle_on_sphere_l2_hamiltonian_create(dh_space_t sp, int nbr_particles
                                                 double l2_factor, dh_hamiltonian_t* out) {
   DH_CHECK(out, DH_ERR_ARGUMENT, "null output handle");
   *out = nullptr;
-  DH_CHECK(sp && (sp->kind == SPACE_FERMION || sp->kind == SPACE_FERMION_LONG), DH_ERR_ARGUMENT,
-           "ParticleOnSphereL2Hamiltonian needs a FermionOnSphere(Long) space");
+  DH_CHECK(sp && (sp->kind == SPACE_FERMION || sp->kind == SPACE_FERMION_LONG || sp->kind == SPACE_BOSON),
+           DH_ERR_ARGUMENT, "ParticleOnSphereL2Hamiltonian needs a FermionOnSphere(Long) or BosonOnSphereShort space");
   DH_CHECK(total_lz == sp->total_lz, DH_ERR_ARGUMENT, "total_lz %d does not match the space's %d", total_lz, sp->total_lz);
   DH_CHECK(l2_factor != 0.0, DH_ERR_ARGUMENT, "l2_factor must not be 0");
   std::vector<double> zero(lz_max + 1, 0.0);
@@ -996,9 +1004,14 @@ int dh_hamiltonian_enable_fast_multiplication(dh_hamiltonian_t h, int64_t allowe
   DH_CHECK(h, DH_ERR_ARGUMENT, "null hamiltonian");
   if (enabled) *enabled = 0;
   if (bytes) *bytes = 0;
-  DH_CHECK(h->kind == SPACE_FERMION, DH_ERR_UNSUPPORTED, "stored elements are available for FQHE Hamiltonians");
-  DH_CHECK(h->tabs.nbr_factors < 0x8000, DH_ERR_UNSUPPORTED, "%d interaction factors do not fit 15-bit indices",
-           h->tabs.nbr_factors);
+  DH_CHECK(h->kind == SPACE_FERMION || h->kind == SPACE_BOSON, DH_ERR_UNSUPPORTED,
+           "stored elements are available for FermionOnSphere and BosonOnSphereShort Hamiltonians");
+  const bool bosons = h->kind == SPACE_BOSON;
+  DH_CHECK(h->tabs.nbr_factors < (bosons ? 0x10000 : 0x8000), DH_ERR_UNSUPPORTED,
+           "%d interaction factors do not fit %d-bit indices", h->tabs.nbr_factors, bosons ? 16 : 15);
+  // a bosonic element keeps n_m2 (n_m1 - [m1 = m2]) <= N (N - 1) and its creation product in 8 bits each
+  DH_CHECK(!bosons || h->space->nbr_fermions <= 16, DH_ERR_UNSUPPORTED,
+           "stored bosonic elements hold occupation products of at most 16 bosons (N = %d)", h->space->nbr_fermions);
   if (h->fast) {
     if (enabled) *enabled = 1;
     if (bytes) *bytes = (int64_t)h->fast_bytes;
@@ -1013,7 +1026,9 @@ int dh_hamiltonian_enable_fast_multiplication(dh_hamiltonian_t h, int64_t allowe
   {
     DevBuf dcounts;
     if ((rc = dcounts.alloc((size_t)dim * sizeof(int))) != DH_OK) return rc;
-    if ((rc = launch_fqhe_row_counts(f, dcounts.as<int>(), h->stream)) != DH_OK) return rc;
+    if ((rc = bosons ? launch_boson_row_counts(f, dcounts.as<int>(), h->stream)
+                     : launch_fqhe_row_counts(f, dcounts.as<int>(), h->stream)) != DH_OK)
+      return rc;
     DH_CUDA(cudaMemcpyAsync(counts.data(), dcounts.ptr, (size_t)dim * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     DH_CUDA(cudaStreamSynchronize(h->stream));
   }
@@ -1029,7 +1044,8 @@ int dh_hamiltonian_enable_fast_multiplication(dh_hamiltonian_t h, int64_t allowe
     slice_len[sl] = mx;
     total += 32ll * mx;
   }
-  const size_t need = (size_t)total * (sizeof(int) + sizeof(uint16_t)) + (size_t)nslices * (sizeof(long long) + sizeof(int)) +
+  const size_t payload = bosons ? sizeof(uint32_t) : sizeof(uint16_t);
+  const size_t need = (size_t)total * (sizeof(int) + payload) + (size_t)nslices * (sizeof(long long) + sizeof(int)) +
                       (size_t)dim * (sizeof(double) + sizeof(float));
   if (bytes) *bytes = (int64_t)need;
   if (allowed_memory >= 0 && need > (size_t)allowed_memory) return DH_OK;  // the caller's memory budget
@@ -1039,7 +1055,7 @@ int dh_hamiltonian_enable_fast_multiplication(dh_hamiltonian_t h, int64_t allowe
   if ((rc = h->ell_slice_ptr.alloc((size_t)nslices * sizeof(long long))) != DH_OK ||
       (rc = h->ell_slice_len.alloc((size_t)nslices * sizeof(int))) != DH_OK ||
       (rc = h->ell_cols.alloc((size_t)total * sizeof(int))) != DH_OK ||
-      (rc = h->ell_coef.alloc((size_t)total * sizeof(uint16_t))) != DH_OK ||
+      (rc = (bosons ? h->ell_coef32 : h->ell_coef).alloc((size_t)total * payload)) != DH_OK ||
       (rc = h->diag64.alloc((size_t)dim * sizeof(double))) != DH_OK ||
       (rc = h->diag32.alloc((size_t)dim * sizeof(float))) != DH_OK)
     return rc;
@@ -1047,8 +1063,10 @@ int dh_hamiltonian_enable_fast_multiplication(dh_hamiltonian_t h, int64_t allowe
                           cudaMemcpyHostToDevice, h->stream));
   DH_CUDA(cudaMemcpyAsync(h->ell_slice_len.ptr, slice_len.data(), slice_len.size() * sizeof(int), cudaMemcpyHostToDevice,
                           h->stream));
-  if ((rc = launch_fqhe_ell_fill(f, h->ell_slice_ptr.as<long long>(), h->ell_slice_len.as<int>(), h->ell_cols.as<int>(),
-                                 h->ell_coef.as<uint16_t>(), h->stream)) != DH_OK)
+  if ((rc = bosons ? launch_boson_ell_fill(f, h->ell_slice_ptr.as<long long>(), h->ell_slice_len.as<int>(),
+                                           h->ell_cols.as<int>(), h->ell_coef32.as<uint32_t>(), h->stream)
+                  : launch_fqhe_ell_fill(f, h->ell_slice_ptr.as<long long>(), h->ell_slice_len.as<int>(),
+                                         h->ell_cols.as<int>(), h->ell_coef.as<uint16_t>(), h->stream)) != DH_OK)
     return rc;
   h->fast = true;
   h->fast_use = true;
@@ -1069,6 +1087,7 @@ int dh_hamiltonian_disable_fast_multiplication(dh_hamiltonian_t h) {
   h->ell_slice_len.release();
   h->ell_cols.release();
   h->ell_coef.release();
+  h->ell_coef32.release();
   h->diag64.release();
   h->diag32.release();
   return DH_OK;
@@ -1431,8 +1450,8 @@ int dh_hamiltonian_get_interaction_factors(dh_hamiltonian_t h, double* factors, 
 
 int dh_hamiltonian_pseudopotential_adjoint(dh_hamiltonian_t h, const double* u, const double* v, double* out) {
   DH_CHECK(h && u && v && out, DH_ERR_ARGUMENT, "null argument");
-  DH_CHECK(h->kind == SPACE_FERMION && !h->l2_only, DH_ERR_UNSUPPORTED,
-           "the pseudopotential adjoint needs an FQHE interaction Hamiltonian");
+  DH_CHECK((h->kind == SPACE_FERMION || h->kind == SPACE_BOSON) && !h->l2_only, DH_ERR_UNSUPPORTED,
+           "the pseudopotential adjoint needs a FermionOnSphere or BosonOnSphereShort interaction Hamiltonian");
   dh_space_s* sp = h->space;
   const int64_t dim = sp->dim;
   const size_t bytes = (size_t)dim * sizeof(double);
@@ -1456,8 +1475,11 @@ int dh_hamiltonian_pseudopotential_adjoint(dh_hamiltonian_t h, const double* u, 
   const int nf = h->tabs.nbr_factors;
   if ((rc = ensure_buffer(h->bins_partial, (size_t)nblocks * nf * sizeof(double))) != DH_OK) return rc;
   if ((rc = ensure_buffer(h->bins, (size_t)nf * sizeof(double))) != DH_OK) return rc;
-  if ((rc = launch_fqhe_bins(fqhe_device(sp, h, DH_PRECISION_FP64), du, dv, h->bins_partial.as<double>(), nblocks,
-                             h->bins.as<double>(), h->stream)) != DH_OK)
+  const FqheDevice fd = fqhe_device(sp, h, DH_PRECISION_FP64);
+  if ((rc = (h->kind == SPACE_BOSON)
+                ? launch_boson_bins(fd, du, dv, h->bins_partial.as<double>(), nblocks, h->bins.as<double>(), h->stream)
+                : launch_fqhe_bins(fd, du, dv, h->bins_partial.as<double>(), nblocks, h->bins.as<double>(), h->stream)) !=
+      DH_OK)
     return rc;
   std::vector<double> bins(nf);
   DH_CUDA(cudaMemcpyAsync(bins.data(), h->bins.ptr, nf * sizeof(double), cudaMemcpyDeviceToHost, h->stream));

@@ -257,6 +257,9 @@ struct EllDevice {
   const int* slice_len;        // [nslices] elements per row of the slice (padded to a multiple of kEllPad)
   const int* cols;             // target index of each element
   const uint16_t* coef;        // factor index | sign << 15; padding holds nbr_factors (a zero factor)
+  // bosons (BosonOnSphereShort): factor index | caa << 16 | cad << 24, the element being
+  // factor * sqrt(caa) * sqrt(cad); coef is then null
+  const uint32_t* coef32;
   const void* diag;            // [dim] diagonal, FP64 or FP32 like the factors
   const void* factors;         // [nbr_factors] FP64 or FP32
   long long dim;
@@ -268,6 +271,12 @@ int launch_fqhe_ell_fill(const FqheDevice& f, const long long* slice_ptr, const 
                          uint16_t* coef, cudaStream_t s);
 int launch_fqhe_diag(const FqheDevice& f, const double* factors64, double* diag64, float* diag32, cudaStream_t s);
 int launch_ell_product(const EllDevice& e, const MatvecArgs& a, int precision, cudaStream_t s);
+int launch_boson_row_counts(const FqheDevice& f, int* counts, cudaStream_t s);
+int launch_boson_ell_fill(const FqheDevice& f, const long long* slice_ptr, const int* slice_len, int* cols,
+                          uint32_t* coef, cudaStream_t s);
+int launch_boson_diag(const FqheDevice& f, const double* factors64, double* diag64, float* diag32, cudaStream_t s);
+int launch_boson_bins(const FqheDevice& f, const double* u, const double* v, double* partial_bins, int nblocks,
+                      double* bins, cudaStream_t s);
 
 struct SpinDevice {
   const uint32_t* words;

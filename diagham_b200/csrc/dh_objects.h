@@ -76,7 +76,7 @@ struct dh_hamiltonian_s {
   int ell_chunk = 16;    // stored elements read ahead of the gathers per lane: 8 or 16
   long long fast_elements = 0;  // stored elements, padding included
   size_t fast_bytes = 0;
-  dh::DevBuf ell_slice_ptr, ell_slice_len, ell_cols, ell_coef, diag64, diag32;
+  dh::DevBuf ell_slice_ptr, ell_slice_len, ell_cols, ell_coef, ell_coef32, diag64, diag32;  // ell_coef32: bosons
   // staging / scratch
   dh::DevBuf stage_x, stage_y, stage_v, x32, bins_partial, bins;
   dh::Reducer red;

@@ -329,6 +329,26 @@ void InteractionTables::build_l2(int nbr_particles) {
   std::vector<double> lam(S2 + 1, 0.0);
   for (int m = 0; m <= S2; ++m) lam[m] = 0.5 * sqrt((double)(S2 * (S2 + 2) - (2 * m - S2) * (2 * m - S2 + 2)));
   l2_part.assign(nbr_factors, 0.0);
+  if (bosonic) {
+    // Bosons commute: a_{m'+1} a+_{m+1} = a+_{m+1} a_{m'+1} + [m = m'], so
+    //   L-L+ = sum_m lam_m^2 n_m + sum_{m, m'} lam_m lam_m' a+_m' a+_{m+1} a_{m'+1} a_m,
+    // and every two-body term is already the table's operator a+_m3 a+_m4 a_m1 a_m2 with m1 = max(m'+1, m),
+    // m2 = min(m'+1, m), m3 = max(m', m+1), no sign.  The one-body part goes into the diagonal factors:
+    // at fixed N, sum_m w_m n_m = sum_{a > b} (w_a + w_b) / (N - 1) n_a n_b + sum_a w_a / (N - 1) n_a (n_a - 1),
+    // and the diagonal move (a, b) -> (a, b) has the element n_a n_b (a > b) or n_a (n_a - 1) (a = b).
+    auto bslot = [&](int m1, int m2, int m3) -> double& {
+      const int M = m1 + m2;
+      return l2_part[pair_offset[m1 * (m1 + 1) / 2 + m2] + (m3 - (M + 1) / 2)];
+    };
+    for (int m = 0; m < S2; ++m)
+      for (int mp = 0; mp < S2; ++mp)
+        bslot(std::max(mp + 1, m), std::min(mp + 1, m), std::max(mp, m + 1)) += lam[m] * lam[mp];
+    for (int a = 0; a <= S2; ++a) {
+      for (int b = 0; b < a; ++b) bslot(a, b, a) += (lam[a] * lam[a] + lam[b] * lam[b]) / (nbr_particles - 1);
+      bslot(a, a, a) += lam[a] * lam[a] / (nbr_particles - 1);
+    }
+    return;
+  }
   auto slot = [&](int m1, int m2, int m3) -> double& {
     const int M = m1 + m2;
     return l2_part[pair_offset[m1 * (m1 - 1) / 2 + m2] + (m3 - (M / 2 + 1))];

@@ -386,7 +386,211 @@ __global__ void __launch_bounds__(kBosonThreads) boson_count_kernel(FqheDevice f
   }
 }
 
+// ------------------------------------------- moves one at a time: stored elements and the adjoint
+// The index of target word t of row r (word s): the split-word rank tables, or the count-table walk
+// between the lowest and highest changed bits.
+__device__ __forceinline__ long long boson_target(const FqheDevice& f, uint64_t s, long long r, uint64_t t) {
+  if (!f.count_table)
+    return (long long)__ldg(f.high_offset + (t >> f.low_bits)) +
+           (long long)__ldg(f.low_rank + (t & ((1ull << f.low_bits) - 1ull)));
+  const uint64_t diff = s ^ t;
+  const int lo = __ffsll(diff) - 1, hi = 63 - __clzll(diff);
+  const uint64_t low_part = s & ((1ull << lo) - 1ull);
+  const int n0 = __popcll(low_part), s0 = position_sum(low_part);
+  return r + count_terms(f, s, lo, hi, n0, s0) - count_terms(f, t, lo, hi, n0, s0);
+}
+
+// Visits every move of row r (word s) in the product kernel's order: m1 ascending over the occupied
+// orbitals, m2 ascending over the occupied orbitals below m1 then m2 = m1 when orbital m1 holds two
+// bosons or more, m3 = ceil(M / 2) .. min(M, L) ascending.  visit(target, factor index, caa, cad,
+// diagonal): the element is factor * sqrt(caa) * sqrt(cad) for a move to another word, and
+// factor * caa for the diagonal move m3 = m1 (target r, cad unused).
+template <typename Visit>
+__device__ __forceinline__ void boson_visit_row(const FqheDevice& f, long long r, uint64_t s, Visit&& visit) {
+  const int L = f.boson_lz_max;
+  uint8_t n[64], P[64];
+  uint64_t occ = 0, dbl = 0;
+  int pos = 0;
+  for (int m = 0; m <= L; ++m) {
+    const int c = __ffsll(~(s >> pos)) - 1;
+    P[m] = (uint8_t)pos;
+    n[m] = (uint8_t)c;
+    occ |= (uint64_t)(c > 0) << m;
+    dbl |= (uint64_t)(c > 1) << m;
+    pos += c + 1;
+  }
+  uint64_t rem1 = occ;
+  while (rem1) {
+    const int m1 = __ffsll(rem1) - 1;
+    rem1 &= rem1 - 1ull;
+    uint64_t rem2 = (occ & ((1ull << m1) - 1ull)) | (dbl & (1ull << m1));
+    while (rem2) {
+      const int m2 = __ffsll(rem2) - 1;
+      rem2 &= rem2 - 1ull;
+      const int caa = n[m2] * (n[m1] - (m1 == m2 ? 1 : 0));
+      const uint64_t an = delete_bit(delete_bit(s, P[m1]), P[m2]);
+      const int M = m1 + m2;
+      const int m3lo = (M + 1) >> 1, m3hi = (M < L) ? M : L;
+      const int fb = __ldg(f.pair_offset + (m1 * (m1 + 1) / 2 + m2)) - m3lo;
+      for (int m3 = m3lo; m3 <= m3hi; ++m3) {
+        if (m3 == m1) {
+          visit(r, fb + m3, caa, 0, true);
+          continue;
+        }
+        const int m4 = M - m3;
+        const int q3 = P[m3] - (m3 > m1) - (m3 > m2), c3 = n[m3] - (m3 == m1) - (m3 == m2);
+        const int q4 = P[m4] - (m4 > m1) - (m4 > m2), c4 = n[m4] - (m4 == m1) - (m4 == m2);
+        const int cad = (m3 == m4) ? (c4 + 1) * (c4 + 2) : (c4 + 1) * (c3 + 1);
+        visit(boson_target(f, s, r, insert_one(insert_one(an, q3), q4)), fb + m3, caa, cad, false);
+      }
+    }
+  }
+}
+
+// off-diagonal elements per row (the stored form keeps the diagonal moves as one value per row)
+__global__ void boson_row_counts_kernel(FqheDevice f, int* counts) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const int L = f.boson_lz_max;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+    const uint64_t s = __ldg(f.words + r);
+    uint8_t n[64];
+    int pos = 0;
+    for (int m = 0; m <= L; ++m) {
+      const int c = __ffsll(~(s >> pos)) - 1;
+      n[m] = (uint8_t)c;
+      pos += c + 1;
+    }
+    int cnt = 0;
+    for (int m1 = 0; m1 <= L; ++m1) {
+      if (n[m1] == 0) continue;
+      for (int m2 = 0; m2 <= m1; ++m2) {
+        if (n[m2] == 0 || (m2 == m1 && n[m1] < 2)) continue;
+        const int M = m1 + m2;
+        cnt += ((M < L) ? M : L) - ((M + 1) >> 1);  // the m3 range less its diagonal move
+      }
+    }
+    counts[r] = cnt;
+  }
+}
+
+// element payload: factor index | caa << 16 | cad << 24; padding: the row itself times the zero
+// factor nbr_factors
+__global__ void boson_ell_fill_kernel(FqheDevice f, const long long* slice_ptr, const int* slice_len, int* cols,
+                                      uint32_t* coef) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+    const long long base = slice_ptr[r >> 5];
+    const int len = slice_len[r >> 5];
+    const int lane = (int)(r & 31);
+    int j = 0;
+    auto at = [&](int jj) {
+      return base + (long long)(jj / kEllGroup) * (32 * kEllGroup) + lane * kEllGroup + (jj % kEllGroup);
+    };
+    boson_visit_row(f, r, __ldg(f.words + r), [&](long long idx, int fidx, int caa, int cad, bool diag) {
+      if (diag) return;
+      const long long p = at(j++);
+      cols[p] = (int)idx;
+      coef[p] = (uint32_t)fidx | ((uint32_t)caa << 16) | ((uint32_t)cad << 24);
+    });
+    for (; j < len; ++j) {
+      const long long p = at(j);
+      cols[p] = (int)r;
+      coef[p] = (uint32_t)f.nbr_factors;
+    }
+  }
+}
+
+// diagonal of every row: sum over the pairs of factor(m1, m2, m1) n_m2 (n_m1 - [m1 = m2])
+__global__ void boson_diag_kernel(FqheDevice f, const double* factors, double* diag64, float* diag32) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+    double d = 0.0;
+    boson_visit_row(f, r, __ldg(f.words + r), [&](long long, int fidx, int caa, int, bool diag) {
+      if (diag) d += factors[fidx] * (double)caa;
+    });
+    diag64[r] = d;
+    diag32[r] = (float)d;
+  }
+}
+
+// bins[f] = sum over rows r and moves (r -> t) of factor f of u[r] * coefficient * v[t]; per-block
+// partial rows of a [blocks][factors] array, summed in block order afterwards
+constexpr int kBosonBinThreads = 256;
+__global__ void __launch_bounds__(kBosonBinThreads) boson_bins_kernel(FqheDevice f, const double* u, const double* v,
+                                                                      double* partial) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double* sbins = reinterpret_cast<double*>(smem);
+  for (int i = threadIdx.x; i < f.nbr_factors; i += blockDim.x) sbins[i] = 0.0;
+  __syncthreads();
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+    const double ur = u[r];
+    if (ur == 0.0) continue;
+    boson_visit_row(f, r, __ldg(f.words + r), [&](long long idx, int fidx, int caa, int cad, bool diag) {
+      const double c = diag ? (double)caa : sqrt((double)caa) * sqrt((double)cad);
+      atomicAdd(sbins + fidx, c * ur * __ldg(v + idx));
+    });
+  }
+  __syncthreads();
+  double* out = partial + (size_t)blockIdx.x * f.nbr_factors;
+  for (int i = threadIdx.x; i < f.nbr_factors; i += blockDim.x) out[i] = sbins[i];
+}
+
+__global__ void boson_sum_partial_bins(const double* partial, int nblocks, int nbins, double* bins) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nbins) return;
+  double acc = 0.0;
+  for (int b = 0; b < nblocks; ++b) acc += partial[(size_t)b * nbins + i];
+  bins[i] = acc;
+}
+
+unsigned boson_grid(long long n) {
+  long long g = (n + 255) / 256;
+  if (g > 148 * 32) g = 148 * 32;
+  if (g < 1) g = 1;
+  return (unsigned)g;
+}
+
 }  // namespace
+
+int launch_boson_row_counts(const FqheDevice& f, int* counts, cudaStream_t s) {
+  if (f.dim <= 0) return DH_OK;
+  boson_row_counts_kernel<<<boson_grid(f.dim), 256, 0, s>>>(f, counts);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_boson_ell_fill(const FqheDevice& f, const long long* slice_ptr, const int* slice_len, int* cols,
+                          uint32_t* coef, cudaStream_t s) {
+  if (f.dim <= 0) return DH_OK;
+  boson_ell_fill_kernel<<<boson_grid(f.dim), 256, 0, s>>>(f, slice_ptr, slice_len, cols, coef);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_boson_diag(const FqheDevice& f, const double* factors64, double* diag64, float* diag32, cudaStream_t s) {
+  if (f.dim <= 0) return DH_OK;
+  boson_diag_kernel<<<boson_grid(f.dim), 256, 0, s>>>(f, factors64, diag64, diag32);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_boson_bins(const FqheDevice& f, const double* u, const double* v, double* partial_bins, int nblocks,
+                      double* bins, cudaStream_t s) {
+  const int smem = f.nbr_factors * (int)sizeof(double);
+  DH_CHECK(smem <= 227 * 1024, DH_ERR_UNSUPPORTED, "%d bosonic factors do not fit the adjoint's shared bins",
+           f.nbr_factors);
+  if (f.dim > 0) {
+    if (smem > 48 * 1024)
+      DH_CUDA(cudaFuncSetAttribute(boson_bins_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    boson_bins_kernel<<<nblocks, kBosonBinThreads, smem, s>>>(f, u, v, partial_bins);
+    DH_CUDA(cudaGetLastError());
+  }
+  boson_sum_partial_bins<<<(f.nbr_factors + 255) / 256, 256, 0, s>>>(partial_bins, f.dim > 0 ? nblocks : 0,
+                                                                     f.nbr_factors, bins);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
 
 int launch_boson_count(const FqheDevice& f, unsigned long long* total, cudaStream_t s) {
   DH_CUDA(cudaMemsetAsync(total, 0, 2 * sizeof(unsigned long long), s));

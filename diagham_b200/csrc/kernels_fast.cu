@@ -11,9 +11,13 @@
 // a warp reads 512 contiguous bytes per load.  Each element is an int32 target and a uint16 factor
 // index with the fermionic sign in bit 15; the structure does not depend on the pseudopotentials.
 // Diagonal moves are summed per row into a separate diagonal array, recomputed when the
-// pseudopotentials change.
+// pseudopotentials change.  Bosonic elements (BosonOnSphereShort) carry their occupation factors: a
+// uint32 of factor index | caa << 16 | cad << 24 for the element factor * sqrt(caa) * sqrt(cad), the
+// square roots read from a 256-entry table in shared memory.
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <type_traits>
 
 #include "dh_internal.h"
 
@@ -171,14 +175,30 @@ __device__ __forceinline__ void gather(const TG* x, const MatvecArgs& a, long lo
 // stream and a chunk of gathers in flight.  The stream, the diagonal and y go through L2 with
 // streaming (evict-first) accesses so that the gathered x keeps the cache.
 // W256: FP64 rows of 4 that are 32-byte aligned, gathered with one 256-bit load each
-template <typename TG, int K, bool IL, bool W256, int CH>
+// BOSON: uint32 payloads (16-byte groups of 4, like the targets) with the occupation square roots
+template <typename TG>
+__device__ __forceinline__ TG occupation_sqrt(int v);
+template <>
+__device__ __forceinline__ double occupation_sqrt<double>(int v) {
+  return sqrt((double)v);
+}
+template <>
+__device__ __forceinline__ float occupation_sqrt<float>(int v) {
+  return sqrtf((float)v);
+}
+
+template <typename TG, int K, bool IL, bool W256, int CH, bool BOSON>
 __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, MatvecArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   TG* sfac = reinterpret_cast<TG*>(smem);
+  TG* ssq = sfac + e.nbr_factors + 1;
   const TG* gfac = static_cast<const TG*>(e.factors);
   for (int i = threadIdx.x; i < e.nbr_factors; i += blockDim.x) sfac[i] = gfac[i];
   if (threadIdx.x == 0) sfac[e.nbr_factors] = TG(0);
+  if (BOSON)
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) ssq[i] = occupation_sqrt<TG>(i);
   __syncthreads();
+  using KT = std::conditional_t<BOSON, uint4, uint2>;
   const TG* x = static_cast<const TG*>(a.x);
   const TG* diag = static_cast<const TG*>(e.diag);
   const int lane = threadIdx.x & 31;
@@ -194,12 +214,14 @@ __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, 
     if (r >= r_end) continue;  // the last slice's lanes beyond the space hold no elements
     const int len = e.slice_len[sl];
     const int4* cg = reinterpret_cast<const int4*>(e.cols + e.slice_ptr[sl]) + lane;
-    const uint2* kg = reinterpret_cast<const uint2*>(e.coef + e.slice_ptr[sl]) + lane;
+    const KT* kg;
+    if constexpr (BOSON) kg = reinterpret_cast<const uint4*>(e.coef32 + e.slice_ptr[sl]) + lane;
+    else kg = reinterpret_cast<const uint2*>(e.coef + e.slice_ptr[sl]) + lane;
     TG acc[K];
 #pragma unroll
     for (int q = 0; q < K; ++q) acc[q] = TG(0);
     int4 c[NG];
-    uint2 k[NG];
+    KT k[NG];
     if (len > 0) {
 #pragma unroll
       for (int g = 0; g < NG; ++g) {
@@ -209,7 +231,7 @@ __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, 
     }
     for (int j = 0; j < len; j += CH) {
       int4 cn[NG];
-      uint2 kn[NG];
+      KT kn[NG];
       const bool more = j + CH < len;
       if (more) {
         const int gn = (j + CH) / kEllGroup;
@@ -222,14 +244,24 @@ __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, 
 #pragma unroll
       for (int g = 0; g < NG; ++g) {
         const int cols[4] = {c[g].x, c[g].y, c[g].z, c[g].w};
-        const unsigned ks[4] = {k[g].x & 0xffffu, k[g].x >> 16, k[g].y & 0xffffu, k[g].y >> 16};
+        unsigned ks[4];
+        if constexpr (BOSON) {
+          ks[0] = k[g].x; ks[1] = k[g].y; ks[2] = k[g].z; ks[3] = k[g].w;
+        } else {
+          ks[0] = k[g].x & 0xffffu; ks[1] = k[g].x >> 16; ks[2] = k[g].y & 0xffffu; ks[3] = k[g].y >> 16;
+        }
         TG xv[4][K];
 #pragma unroll
         for (int u = 0; u < 4; ++u) gather<TG, K, IL, W256>(x, a, cols[u], xv[u]);
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          TG fu = sfac[ks[u] & 0x7fffu];
-          if (ks[u] & 0x8000u) fu = -fu;
+          TG fu;
+          if constexpr (BOSON) {
+            fu = sfac[ks[u] & 0xffffu] * ssq[(ks[u] >> 16) & 0xffu] * ssq[ks[u] >> 24];
+          } else {
+            fu = sfac[ks[u] & 0x7fffu];
+            if (ks[u] & 0x8000u) fu = -fu;
+          }
 #pragma unroll
           for (int q = 0; q < K; ++q) acc[q] += fu * xv[u][q];
         }
@@ -267,14 +299,14 @@ unsigned grid_for(long long n) {
   return (unsigned)g;
 }
 
-template <typename TG, int K, bool IL>
-int launch_ell_typed(const EllDevice& e, const MatvecArgs& a, cudaStream_t s) {
+template <typename TG, int K, bool IL, bool BOSON>
+int launch_ell_payload(const EllDevice& e, const MatvecArgs& a, cudaStream_t s) {
   const bool deep = e.chunk == 16;
-  auto kern = deep ? ell_product_kernel<TG, K, IL, false, 16> : ell_product_kernel<TG, K, IL, false, 8>;
+  auto kern = deep ? ell_product_kernel<TG, K, IL, false, 16, BOSON> : ell_product_kernel<TG, K, IL, false, 8, BOSON>;
   if constexpr (IL && sizeof(TG) == 8 && K == 4)
     if ((reinterpret_cast<uintptr_t>(a.x) & 31) == 0)
-      kern = deep ? ell_product_kernel<TG, K, IL, true, 16> : ell_product_kernel<TG, K, IL, true, 8>;
-  const int smem = (e.nbr_factors + 1) * (int)sizeof(TG);
+      kern = deep ? ell_product_kernel<TG, K, IL, true, 16, BOSON> : ell_product_kernel<TG, K, IL, true, 8, BOSON>;
+  const int smem = (e.nbr_factors + 1 + (BOSON ? 256 : 0)) * (int)sizeof(TG);
   if (smem > 48 * 1024) DH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int dev = 0, sms = 0, per_sm = 0;
   DH_CUDA(cudaGetDevice(&dev));
@@ -289,6 +321,11 @@ int launch_ell_typed(const EllDevice& e, const MatvecArgs& a, cudaStream_t s) {
   kern<<<(unsigned)grid, kFastThreads, smem, s>>>(e, a);
   DH_CUDA(cudaGetLastError());
   return DH_OK;
+}
+
+template <typename TG, int K, bool IL>
+int launch_ell_typed(const EllDevice& e, const MatvecArgs& a, cudaStream_t s) {
+  return e.coef32 ? launch_ell_payload<TG, K, IL, true>(e, a, s) : launch_ell_payload<TG, K, IL, false>(e, a, s);
 }
 
 template <typename TG>

@@ -172,7 +172,9 @@ int dh_fermion_on_sphere_partial_density_matrix(dh_space_t space, const double* 
  * (FQHESphereFermionsTwoBodyGeneric.cc:395-396).  On a BosonOnSphereShort space the factors are the
  * reference's bosonic ones (:620-806: pairs m1 >= m2, even relative angular momenta, weights 4, 2 and
  * 1) and the product applies AA / AdAd with their occupation square roots (BosonOnSphereShort.cc:
- * 353, 431); bosonic Hamiltonians have no L^2 term, stored elements or adjoint. */
+ * 353, 431).  Bosonic Hamiltonians take the L^2 term (the operator's bosonic branch,
+ * ParticleOnSphereL2Hamiltonian.cc:256-368), stored elements (N <= 16) and the pseudopotential
+ * adjoint like fermionic ones. */
 int dh_particle_on_sphere_generic_hamiltonian_create(dh_space_t space, int nbr_particles, int lz_max,
                                                      const double* pseudopotentials, double l2_factor,
                                                      dh_hamiltonian_t* out);
@@ -261,7 +263,9 @@ int dh_hamiltonian_block_multiply(dh_hamiltonian_t h, const double* x, double* y
  * device memory; every later full product of this Hamiltonian then reads them instead of
  * enumerating the moves.  *bytes = the memory the structure needs (set even when it is not built),
  * *enabled = 1 if it was built.  The elements do not depend on the pseudopotentials: setting new
- * ones only recomputes the diagonal.  FQHE Hamiltonians only; partial column ranges stay on the fly. */
+ * ones only recomputes the diagonal.  FermionOnSphere and BosonOnSphereShort Hamiltonians; a bosonic
+ * element stores, beside its target, the factor index and the two occupation products under its square
+ * roots in 8 bits each (N <= 16, else DH_ERR_UNSUPPORTED).  Partial column ranges stay on the fly. */
 int dh_hamiltonian_enable_fast_multiplication(dh_hamiltonian_t h, int64_t allowed_memory, int* enabled,
                                               int64_t* bytes);
 /* Frees the stored elements: products go back to the on-the-fly kernels.  No reference counterpart
@@ -302,9 +306,9 @@ int dh_hamiltonian_row_elements(dh_hamiltonian_t h, int64_t row, int* targets, i
 
 /* Adjoint of the pseudopotentials (Hellmann-Feynman / bilinear VJP): out[m] = <u| dH/dV_m |v> for
  * m = 0..lz_max.  With u = v = normalised ground state this is dE0/dV_m; with u = upstream gradient
- * and v = x it is the V part of the vector-Jacobian product of H(V) x.  FQHE Hamiltonians only.  No
- * reference counterpart; its oracle is MatrixElement (AbstractQHEOnSphereHamiltonian.cc:380) of the
- * Hamiltonian with V = e_m. */
+ * and v = x it is the V part of the vector-Jacobian product of H(V) x.  FermionOnSphere and
+ * BosonOnSphereShort interaction Hamiltonians.  No reference counterpart; its oracle is MatrixElement
+ * (AbstractQHEOnSphereHamiltonian.cc:380) of the Hamiltonian with V = e_m. */
 int dh_hamiltonian_pseudopotential_adjoint(dh_hamiltonian_t h, const double* u, const double* v, double* out);
 
 /* Number of elements (a+a+aa moves, diagonal ones included; spin flips for the chain) that one

@@ -387,6 +387,41 @@ def l2_factors(n, two_s, total_lz):
     return f, lz * lz + lz
 
 
+def boson_l2_factors(n, two_s, total_lz):
+    """L^2 of N bosons as a two-body table in the layout of boson_interaction_tables (pairs m1 >= m2,
+    creation m3 >= M/2, element = F(m1, m2, m3) <t|a+_m3 a+_m4 a_m1 a_m2|s>), the reference's bosonic
+    branch of ParticleOnSphereL2Hamiltonian (ParticleOnSphereL2Hamiltonian.cc:240-368).  Bosons
+    commute, so L-L+ = sum_m lam_m^2 n_m + sum_{m,m'} lam_m lam_m' a+_m' a+_{m+1} a_{m'+1} a_m with no
+    sign; at fixed N the one-body part is sum_{a>b} (w_a + w_b) / (N - 1) n_a n_b +
+    sum_a w_a / (N - 1) n_a (n_a - 1).  Returns (factors, Lz^2 + Lz)."""
+    t = boson_interaction_tables(two_s, np.zeros(two_s + 1))
+    lam = [0.5 * np.sqrt(two_s * (two_s + 2) - (2 * m - two_s) * (2 * m - two_s + 2)) for m in range(two_s + 1)]
+    F = {}
+
+    def add(c, d, a, val):
+        F[(c, d, a)] = F.get((c, d, a), 0.0) + val
+
+    for m in range(two_s):
+        for mp in range(two_s):
+            add(max(mp + 1, m), min(mp + 1, m), max(mp, m + 1), lam[m] * lam[mp])
+    w = [lam[m] ** 2 for m in range(two_s + 1)]
+    for a_ in range(two_s + 1):
+        for b_ in range(a_):
+            add(a_, b_, a_, (w[a_] + w[b_]) / (n - 1))
+        add(a_, a_, a_, w[a_] / (n - 1))
+    f = np.zeros_like(t["factors"])
+    slots = set()
+    for p in range(len(t["m1"])):
+        m1, m2 = int(t["m1"][p]), int(t["m2"][p])
+        for q in range(int(t["nbr_m3"][p])):
+            key = (m1, m2, int(t["m3"][t["m3_offset"][p] + q]))
+            slots.add(key)
+            f[t["m3_offset"][p] + q] = F.get(key, 0.0)
+    assert all(k in slots for k in F), "an L^2 term outside the bosonic table"
+    lz = total_lz / 2.0
+    return f, lz * lz + lz
+
+
 def l2_raise(n, two_s, total_lz, x):
     """L+ x from the sector 2Lz to 2Lz + 2: a+_{m+1} a_m hops with coefficient lam_m and sign +1
     (no orbital lies between m and m + 1)."""

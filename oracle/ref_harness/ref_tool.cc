@@ -513,6 +513,7 @@ static void Usage()
 	  "  bqhe_matvec N 2S 2Lz vfile xfile shift out\n"
 	  "  bqhe_lanczos N 2S 2Lz vfile algo nev block maxiter precision out gsout x0 [x1 ...]\n"
 	  "  fqhe_l2 N 2S 2Lz xfile out\n"
+	  "  bqhe_l2 N 2S 2Lz xfile out\n"
 	  "  pseudopotentials 2S out\n"
 	  "  spin_basis L 2Sz out\n"
 	  "  spin_matvec L 2Sz J1 J2 xfile out\n"
@@ -986,6 +987,20 @@ int main(int argc, char** argv)
       // sector, on the fly, hermitian symmetry off)
       int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
       FermionOnSphere Space(N, TotalLz, LzMax, 1ul << 20);
+      MonoProcessorArchitecture Arch;
+      RealVector X;
+      X.ReadVector(argv[5]);
+      RealVector Y(Space.GetHilbertSpaceDimension(), true);
+      ParticleOnSphereL2Hamiltonian L2(&Space, N, LzMax, TotalLz, &Arch, 1.0, 0, true, false, 0, false);
+      L2.LowLevelMultiply(X, Y);
+      Y.WriteVector(argv[6]);
+      return 0;
+    }
+  if (strcmp(Cmd, "bqhe_l2") == 0 && argc == 7)
+    {
+      // the same L^2 product on a BosonOnSphereShort space (the operator's bosonic branch)
+      int N = atoi(argv[2]), LzMax = atoi(argv[3]), TotalLz = atoi(argv[4]);
+      BosonOnSphereShort Space(N, TotalLz, LzMax);
       MonoProcessorArchitecture Arch;
       RealVector X;
       X.ReadVector(argv[5]);

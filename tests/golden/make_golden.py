@@ -349,6 +349,15 @@ def l2_fixtures(tmp):
         write_vector(xf, splitmix_vector(7, dim))
         cmd = run("fqhe_l2", n, s, lz, xf, yf)
         save("l2_n%d_2s%d_lz%d.npz" % (n, s, lz), cmd, seed=7, y=read_vector(yf))
+    # the same product on BosonOnSphereShort sectors (the operator's bosonic branch)
+    for (n, s, lz) in [(6, 10, 0), (5, 9, 1), (7, 12, 2), (8, 14, 0), (8, 8, 4)]:
+        bf = os.path.join(tmp, "bb.bin")
+        run("bqhe_basis", n, s, lz, bf)
+        dim = int(np.frombuffer(open(bf, "rb").read(8), np.int64)[0])
+        xf, yf = os.path.join(tmp, "xl2.vec"), os.path.join(tmp, "yl2.vec")
+        write_vector(xf, splitmix_vector(7, dim))
+        cmd = run("bqhe_l2", n, s, lz, xf, yf)
+        save("boson_l2_n%d_2s%d_lz%d.npz" % (n, s, lz), cmd, seed=7, y=read_vector(yf))
 
 
 def boson_fixtures(tmp):

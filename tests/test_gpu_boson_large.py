@@ -106,3 +106,19 @@ def test_boson_large_lanczos_matches_reference(gpu, orc, name):
     r = lz.solve(600)
     e_ref = float(z["eigenvalues"][0])
     assert abs(r["eigenvalues"][0] - e_ref) <= 1e-10 * abs(e_ref)
+
+
+@pytest.mark.parametrize("n,s,lz", [(3, 40, 0), (4, 45, 2), (5, 50, 0)])
+def test_boson_large_stored_elements_match_oracle(gpu, orc, n, s, lz):
+    # stored elements whose targets come from the count-table ranks
+    v = orc.coulomb_pseudopotentials(s)
+    v[1::2] = 0.0
+    sp = gpu.BosonOnSphereShort(n, lz, s)
+    H = gpu.ParticleOnSphereGenericHamiltonian(sp, n, s, v)
+    x = orc.random_vector(6, sp.dim)
+    y_fly = H.LowLevelMultiply(x)
+    assert H.EnableFastMultiplication()[0]
+    ref = orc.BosonFQHE(n, s, lz, v).push(x)
+    y = H.LowLevelMultiply(x)
+    assert np.max(np.abs(y - ref)) <= 1e-13 * np.max(np.abs(ref))
+    assert np.max(np.abs(y - y_fly)) <= 1e-15 * np.max(np.abs(ref))

@@ -424,3 +424,17 @@ def test_boson_large_oracle_matches_reference(orc, name):
         pytest.skip("large sector: GPU product test only")
     y = B.push(orc.random_vector(int(z["seed"]), B.dim))
     assert np.max(np.abs(y - z["y_shift0"])) <= 1e-13 * np.max(np.abs(z["y_shift0"]))
+
+
+@pytest.mark.parametrize("tag", ["n6_2s10_lz0", "n5_2s9_lz1", "n7_2s12_lz2", "n8_2s14_lz0", "n8_2s8_lz4"])
+def test_boson_l2_table_matches_reference(orc, tag):
+    # the oracle's bosonic two-body form of L^2 (plus its constant) against the reference's
+    # ParticleOnSphereL2Hamiltonian product on BosonOnSphereShort
+    z = golden("boson_l2_%s.npz" % tag)
+    n, s, lz = parse_sector(tag)
+    O = orc.BosonFQHE(n, s, lz, np.zeros(s + 1))
+    f, c = orc.boson_l2_factors(n, s, lz)
+    O.tabs["factors"][:len(f)] = f
+    x = orc.random_vector(int(z["seed"]), O.dim)
+    y = O.pull(x) + c * x
+    assert np.max(np.abs(y - z["y"])) <= 1e-13 * np.max(np.abs(z["y"]))
