@@ -719,13 +719,13 @@ def reference_cpu_momentum_sector(length=32, rows_target_s=6.0):
             "seconds_per_sample": r["mean_s"], "reference_setup_seconds": r["setup_s"]}
 
 
-def boson_product(dh, flush, steps=5, k=4, warmup=2):
-    """BosonOnSphereShort N=12, 2S=22, 2Lz=0 (dimension 7,764,392, the size of the fermion sector
-    above), LLL Coulomb V_m with the odd m set to zero: FP32 block products of k vectors, their
-    algorithmic bytes (basis word, FP64 y, one FP32 x gather per off-diagonal element and per row)
-    and, on rank 0, the reference's own CPU product of the same sector on a row sample."""
+def boson_product(dh, flush, steps=5, k=4, warmup=2, n=12, s=22):
+    """BosonOnSphereShort N=12, 2S=22, 2Lz=0 by default (dimension 7,764,392, the size of the fermion
+    sector above), LLL Coulomb V_m with the odd m set to zero: FP32 block products of k vectors, their
+    algorithmic bytes (basis word, FP64 y, one FP32 x gather per off-diagonal element and per row),
+    the same products from stored elements, and, on rank 0 of the default run, the reference's own CPU
+    product of the same sector on a row sample."""
     import torch
-    n, s = 12, 22
     v = dh.coulomb_pseudopotentials(s)
     v[1::2] = 0.0
     t0 = time.perf_counter()
@@ -754,14 +754,46 @@ def boson_product(dh, flush, steps=5, k=4, warmup=2):
     alg = dim * 8 + k * dim * 8 + k * (off + dim) * 4
     mean_s = statistics.mean(ms) / 1000.0
     peak, kind = peaks()
+    res = {"workload": "BosonOnSphereShort N=%d 2S=%d 2Lz=0 (dim %d), Coulomb V_m even m, FP32 block k=%d"
+                       % (n, s, dim, k),
+           "setup_seconds": setup, "mean_launch_ms": mean_s * 1000.0, "hv_per_s": k / mean_s,
+           "elements_per_product": moves, "off_diagonal_elements": off, "algorithmic_bytes_per_launch": alg,
+           "roofline": {"bound": "hbm", "achieved": alg / mean_s / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": alg / mean_s / 1e9 / peak, "peak_kind": kind}}
+    # stored elements (8 bytes each: target, factor index, the two occupation products), streamed once
+    # per product; the autotuner then keeps whichever form is faster
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    on, nbytes = H.EnableFastMultiplication()
+    torch.cuda.synchronize()
+    stored = {"built": on, "bytes": nbytes, "build_seconds": time.perf_counter() - t0}
+    if on:
+        H.block_multiply(x, y)
+        sms = []
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            H.block_multiply(x, y)
+            b.record()
+            torch.cuda.synchronize()
+            sms.append(a.elapsed_time(b))
+        st = statistics.median(sms) / 1000.0
+        # bytes that must come from HBM: the structure, y and the FP32 block x once (124 MB, which
+        # stays in L2, so the per-element gathers are L2 traffic and set the pace at k = 4)
+        dram_st = nbytes + k * dim * 8 + k * dim * 4
+        stored.update(mean_launch_ms=st * 1000.0, hv_per_s=k / st, speedup_vs_on_the_fly=mean_s / st,
+                      stream_gbs=nbytes / st / 1e9, l2_gathers_per_s=(off + dim) / st,
+                      roofline={"bound": "hbm", "achieved": dram_st / st / 1e9, "peak": peak, "unit": "GB/s",
+                                "frac": dram_st / st / 1e9 / peak, "peak_kind": kind,
+                                "bytes": "structure + y + x once; gathers of x served by L2"})
+        t = H.autotune(block_size=k, repeats=3)
+        stored["autotuned"] = {"stored_in_use": t["stored_in_use"], "best_ms": t["best_ms"],
+                               "read_ahead": t["stored_read_ahead"]}
+    res["stored"] = stored
     del x, y, H, sp
     torch.cuda.empty_cache()
-    return {"workload": "BosonOnSphereShort N=%d 2S=%d 2Lz=0 (dim %d), Coulomb V_m even m, FP32 block k=%d"
-                        % (n, s, dim, k),
-            "setup_seconds": setup, "mean_launch_ms": mean_s * 1000.0, "hv_per_s": k / mean_s,
-            "elements_per_product": moves, "off_diagonal_elements": off, "algorithmic_bytes_per_launch": alg,
-            "roofline": {"bound": "hbm", "achieved": alg / mean_s / 1e9, "peak": peak, "unit": "GB/s",
-                         "frac": alg / mean_s / 1e9 / peak, "peak_kind": kind}}
+    return res
 
 
 def reference_cpu_bosons(rows_target_s=6.0):
@@ -905,7 +937,8 @@ def run_b200(args, world, rank, local):
             r = momentum_sector(dh, flush, steps=args.steps, length=args.chain_length or 32, warmup=args.warmup,
                                 solve=not args.no_solve)
         else:
-            r = boson_product(dh, flush, steps=args.steps, warmup=args.warmup)
+            r = boson_product(dh, flush, steps=args.steps, warmup=args.warmup, n=args.nbr_bosons,
+                              s=args.boson_two_s)
         if rank == 0:
             print(json.dumps(dict(leg=args.leg, **r)))
         return
@@ -1094,6 +1127,8 @@ def main():
                     help="only the timed FP32 products (the short command used for ncu captures)")
     ap.add_argument("--nbr-fermions", type=int, default=N_FERMIONS, help="with --leg stored: N")
     ap.add_argument("--two-s", type=int, default=TWO_S, help="with --leg stored: 2S")
+    ap.add_argument("--nbr-bosons", type=int, default=12, help="with --leg bosons: N")
+    ap.add_argument("--boson-two-s", type=int, default=22, help="with --leg bosons: 2S")
     ap.add_argument("--no-autotune", action="store_true",
                     help="with --kernel-only: skip the autotuner (kernel form from DH_FQHE_KERNEL / DH_FQHE_LOW_BITS)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
