@@ -451,7 +451,12 @@ def spin_chain_product(dh, flush, steps=5, k=2, length=32, warmup=2):
             "setup_seconds": setup, "mean_launch_ms": mean_s * 1000.0, "hv_per_s": k / mean_s,
             "off_diagonal_flips": flips, "algorithmic_bytes_per_launch": alg,
             "roofline": {"bound": "hbm", "achieved": alg / mean_s / 1e9, "peak": peak, "unit": "GB/s",
-                         "frac": alg / mean_s / 1e9 / peak, "peak_kind": kind}}
+                         "frac": alg / mean_s / 1e9 / peak, "peak_kind": kind,
+                         # ncu, one launch at L = 30 (x ten times L2): DRAM bytes against the model
+                         "measured_dram": {"profile": "profiles/spin_j1j2_fp32_block2_L30_dram.md",
+                                           "dram_over_algorithmic": 0.474, "dram_gbs": 2355.0,
+                                           "frac_of_hbm": 0.36,
+                                           "limiter": "gather and rank-table latency, not DRAM bandwidth"}}}
 
 
 
