@@ -529,7 +529,8 @@ def time_to_e0_summary(line):
 def long_product(dh, flush, steps=5, warmup=2):
     """FermionOnSphereLong N=6, 2S=63, 2Lz=0 (dimension 671,430: the first 2S above 64-bit words), LLL
     Coulomb V_m with the even m set to zero: FP64 single products and FP32 blocks of 4, with the
-    algorithmic bytes (16-byte word and FP64 y per row, one x gather per element)."""
+    algorithmic bytes (16-byte word and FP64 y per row, one x gather per element), and the same
+    products from stored elements."""
     import torch
     n, s = 6, 63
     v = dh.coulomb_pseudopotentials(s)
@@ -544,8 +545,7 @@ def long_product(dh, flush, steps=5, warmup=2):
     peak, kind = peaks()
     out = {"workload": "FermionOnSphereLong N=%d 2S=%d 2Lz=0 (dim %d), Coulomb V_m odd m" % (n, s, dim),
            "setup_seconds": setup, "elements_per_product": moves}
-    for prec, k in (("fp64", 1), ("fp32", 4)):
-        H.set_precision(prec)
+    def timed(k):
         x = torch.empty(dim, k, dtype=torch.float64, device="cuda")
         x.uniform_(-1.0, 1.0)
         y = torch.empty_like(x)
@@ -561,15 +561,34 @@ def long_product(dh, flush, steps=5, warmup=2):
             b.record()
             torch.cuda.synchronize()
             ms.append(a.elapsed_time(b))
+        return statistics.mean(ms) / 1000.0
+
+    for prec, k in (("fp64", 1), ("fp32", 4)):
+        H.set_precision(prec)
+        mean_s = timed(k)
         xb = 4 if prec == "fp32" else 8
         alg = dim * (16 + 8 * k) + moves * xb * k
-        mean_s = statistics.mean(ms) / 1000.0
         out["%s_block_k%d" % (prec, k)] = {
             "mean_launch_ms": mean_s * 1000.0, "hv_per_s": k / mean_s, "elements_per_s": moves * k / mean_s,
             "algorithmic_bytes_per_launch": alg,
             "roofline": {"bound": "hbm", "achieved": alg / mean_s / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": alg / mean_s / 1e9 / peak, "peak_kind": kind}}
-        del x, y
+    # stored elements (8 bytes each: target, factor index | sign), streamed once per product
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    on, nbytes = H.EnableFastMultiplication()
+    torch.cuda.synchronize()
+    stored = {"built": on, "bytes": nbytes, "build_seconds": time.perf_counter() - t0}
+    if on:
+        for prec, k in (("fp64", 1), ("fp32", 4)):
+            H.set_precision(prec)
+            t = H.autotune(block_size=k, repeats=3)  # read-ahead depth; keeps the faster form
+            st = timed(k)
+            stored["%s_block_k%d" % (prec, k)] = {
+                "mean_launch_ms": st * 1000.0, "hv_per_s": k / st, "stream_gbs": nbytes / st / 1e9,
+                "stored_in_use": t["stored_in_use"], "read_ahead": t["stored_read_ahead"],
+                "speedup_vs_on_the_fly": out["%s_block_k%d" % (prec, k)]["mean_launch_ms"] / (st * 1000.0)}
+    out["stored"] = stored
     del H, sp
     torch.cuda.empty_cache()
     return out

@@ -328,6 +328,7 @@ EllDevice ell_device(const dh_hamiltonian_s* h, int precision) {
   e.cols = h->ell_cols.as<int>();
   e.coef = h->ell_coef.as<uint16_t>();
   e.coef32 = h->ell_coef32.as<uint32_t>();
+  e.payload = (h->kind == SPACE_BOSON) ? 1 : (h->kind == SPACE_FERMION_LONG ? 2 : 0);
   e.diag = precision == DH_PRECISION_FP32 ? h->diag32.ptr : h->diag64.ptr;
   e.factors = precision == DH_PRECISION_FP32 ? h->factors32.ptr : h->factors64.ptr;
   e.dim = h->space->dim;
@@ -338,10 +339,16 @@ EllDevice ell_device(const dh_hamiltonian_s* h, int precision) {
 
 int refresh_fast_diagonal(dh_hamiltonian_s* h) {
   if (!h->fast) return DH_OK;
-  const FqheDevice f = fqhe_device(h->space, h, DH_PRECISION_FP64);
-  int rc = (h->kind == SPACE_BOSON)
-               ? launch_boson_diag(f, h->factors64.as<double>(), h->diag64.as<double>(), h->diag32.as<float>(), h->stream)
-               : launch_fqhe_diag(f, h->factors64.as<double>(), h->diag64.as<double>(), h->diag32.as<float>(), h->stream);
+  int rc;
+  if (h->kind == SPACE_FERMION_LONG) {
+    rc = launch_long_diag(fqhe_long_device(h->space, h, DH_PRECISION_FP64), h->factors64.as<double>(),
+                          h->diag64.as<double>(), h->diag32.as<float>(), h->stream);
+  } else {
+    const FqheDevice f = fqhe_device(h->space, h, DH_PRECISION_FP64);
+    rc = (h->kind == SPACE_BOSON)
+             ? launch_boson_diag(f, h->factors64.as<double>(), h->diag64.as<double>(), h->diag32.as<float>(), h->stream)
+             : launch_fqhe_diag(f, h->factors64.as<double>(), h->diag64.as<double>(), h->diag32.as<float>(), h->stream);
+  }
   if (rc != DH_OK) return rc;
   DH_CUDA(cudaStreamSynchronize(h->stream));
   return DH_OK;
@@ -393,7 +400,10 @@ int hamiltonian_apply_rows(dh_hamiltonian_s* h, const double* x, double* y, int 
     return launch_boson_matvec(fqhe_device(sp, h, h->precision), a, h->precision, stream);
   }
   if (sp->kind == SPACE_SPIN12_TRANSLATIONS) return launch_trans_matvec(trans_device(sp, h), a, h->precision, stream);
-  if (sp->kind == SPACE_FERMION_LONG) return launch_long_matvec(fqhe_long_device(sp, h, h->precision), a, h->precision, stream);
+  if (sp->kind == SPACE_FERMION_LONG) {
+    if (h->fast && h->fast_use && first == 0 && nbr == dim) return launch_ell_product(ell_device(h, h->precision), a, h->precision, stream);
+    return launch_long_matvec(fqhe_long_device(sp, h, h->precision), a, h->precision, stream);
+  }
   if (sp->kind == SPACE_FERMION) {
     if (h->fast && h->fast_use && first == 0 && nbr == dim) return launch_ell_product(ell_device(h, h->precision), a, h->precision, stream);
     if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
@@ -439,7 +449,10 @@ int hamiltonian_apply_block_rows(dh_hamiltonian_s* h, const double* x64, const f
     return launch_boson_matvec(fqhe_device(sp, h, precision), a, precision, stream);
   }
   if (sp->kind == SPACE_SPIN12_TRANSLATIONS) return launch_trans_matvec(trans_device(sp, h), a, precision, stream);
-  if (sp->kind == SPACE_FERMION_LONG) return launch_long_matvec(fqhe_long_device(sp, h, precision), a, precision, stream);
+  if (sp->kind == SPACE_FERMION_LONG) {
+    if (h->fast && h->fast_use) return launch_ell_product(ell_device(h, precision), a, precision, stream);
+    return launch_long_matvec(fqhe_long_device(sp, h, precision), a, precision, stream);
+  }
   if (sp->kind == SPACE_FERMION) {
     if (h->fast && h->fast_use) return launch_ell_product(ell_device(h, precision), a, precision, stream);
     if (sp->index_mode == DH_INDEX_LOOKUP && (rc = build_lookup(sp)) != DH_OK) return rc;
@@ -1004,11 +1017,13 @@ int dh_hamiltonian_enable_fast_multiplication(dh_hamiltonian_t h, int64_t allowe
   DH_CHECK(h, DH_ERR_ARGUMENT, "null hamiltonian");
   if (enabled) *enabled = 0;
   if (bytes) *bytes = 0;
-  DH_CHECK(h->kind == SPACE_FERMION || h->kind == SPACE_BOSON, DH_ERR_UNSUPPORTED,
-           "stored elements are available for FermionOnSphere and BosonOnSphereShort Hamiltonians");
+  DH_CHECK(h->kind == SPACE_FERMION || h->kind == SPACE_BOSON || h->kind == SPACE_FERMION_LONG, DH_ERR_UNSUPPORTED,
+           "stored elements are available for FermionOnSphere(Long) and BosonOnSphereShort Hamiltonians");
   const bool bosons = h->kind == SPACE_BOSON;
-  DH_CHECK(h->tabs.nbr_factors < (bosons ? 0x10000 : 0x8000), DH_ERR_UNSUPPORTED,
-           "%d interaction factors do not fit %d-bit indices", h->tabs.nbr_factors, bosons ? 16 : 15);
+  const bool wide = h->kind == SPACE_FERMION_LONG;  // uint32 index | sign payloads
+  DH_CHECK(h->tabs.nbr_factors < (wide ? 0x7fffffff : bosons ? 0x10000 : 0x8000), DH_ERR_UNSUPPORTED,
+           "%d interaction factors do not fit %d-bit indices", h->tabs.nbr_factors, wide ? 31 : bosons ? 16 : 15);
+  DH_CHECK(h->space->dim < (1ll << 31), DH_ERR_UNSUPPORTED, "stored elements hold int32 targets");
   // a bosonic element keeps n_m2 (n_m1 - [m1 = m2]) <= N (N - 1) and its creation product in 8 bits each
   DH_CHECK(!bosons || h->space->nbr_fermions <= 16, DH_ERR_UNSUPPORTED,
            "stored bosonic elements hold occupation products of at most 16 bosons (N = %d)", h->space->nbr_fermions);
@@ -1026,8 +1041,9 @@ int dh_hamiltonian_enable_fast_multiplication(dh_hamiltonian_t h, int64_t allowe
   {
     DevBuf dcounts;
     if ((rc = dcounts.alloc((size_t)dim * sizeof(int))) != DH_OK) return rc;
-    if ((rc = bosons ? launch_boson_row_counts(f, dcounts.as<int>(), h->stream)
-                     : launch_fqhe_row_counts(f, dcounts.as<int>(), h->stream)) != DH_OK)
+    if ((rc = wide     ? launch_long_row_counts(fqhe_long_device(sp, h, DH_PRECISION_FP64), dcounts.as<int>(), h->stream)
+              : bosons ? launch_boson_row_counts(f, dcounts.as<int>(), h->stream)
+                       : launch_fqhe_row_counts(f, dcounts.as<int>(), h->stream)) != DH_OK)
       return rc;
     DH_CUDA(cudaMemcpyAsync(counts.data(), dcounts.ptr, (size_t)dim * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     DH_CUDA(cudaStreamSynchronize(h->stream));
@@ -1044,7 +1060,7 @@ int dh_hamiltonian_enable_fast_multiplication(dh_hamiltonian_t h, int64_t allowe
     slice_len[sl] = mx;
     total += 32ll * mx;
   }
-  const size_t payload = bosons ? sizeof(uint32_t) : sizeof(uint16_t);
+  const size_t payload = (bosons || wide) ? sizeof(uint32_t) : sizeof(uint16_t);
   const size_t need = (size_t)total * (sizeof(int) + payload) + (size_t)nslices * (sizeof(long long) + sizeof(int)) +
                       (size_t)dim * (sizeof(double) + sizeof(float));
   if (bytes) *bytes = (int64_t)need;
@@ -1055,7 +1071,7 @@ int dh_hamiltonian_enable_fast_multiplication(dh_hamiltonian_t h, int64_t allowe
   if ((rc = h->ell_slice_ptr.alloc((size_t)nslices * sizeof(long long))) != DH_OK ||
       (rc = h->ell_slice_len.alloc((size_t)nslices * sizeof(int))) != DH_OK ||
       (rc = h->ell_cols.alloc((size_t)total * sizeof(int))) != DH_OK ||
-      (rc = (bosons ? h->ell_coef32 : h->ell_coef).alloc((size_t)total * payload)) != DH_OK ||
+      (rc = ((bosons || wide) ? h->ell_coef32 : h->ell_coef).alloc((size_t)total * payload)) != DH_OK ||
       (rc = h->diag64.alloc((size_t)dim * sizeof(double))) != DH_OK ||
       (rc = h->diag32.alloc((size_t)dim * sizeof(float))) != DH_OK)
     return rc;
@@ -1063,10 +1079,13 @@ int dh_hamiltonian_enable_fast_multiplication(dh_hamiltonian_t h, int64_t allowe
                           cudaMemcpyHostToDevice, h->stream));
   DH_CUDA(cudaMemcpyAsync(h->ell_slice_len.ptr, slice_len.data(), slice_len.size() * sizeof(int), cudaMemcpyHostToDevice,
                           h->stream));
-  if ((rc = bosons ? launch_boson_ell_fill(f, h->ell_slice_ptr.as<long long>(), h->ell_slice_len.as<int>(),
-                                           h->ell_cols.as<int>(), h->ell_coef32.as<uint32_t>(), h->stream)
-                  : launch_fqhe_ell_fill(f, h->ell_slice_ptr.as<long long>(), h->ell_slice_len.as<int>(),
-                                         h->ell_cols.as<int>(), h->ell_coef.as<uint16_t>(), h->stream)) != DH_OK)
+  if ((rc = wide ? launch_long_ell_fill(fqhe_long_device(sp, h, DH_PRECISION_FP64), h->tabs.nbr_factors,
+                                        h->ell_slice_ptr.as<long long>(), h->ell_slice_len.as<int>(),
+                                        h->ell_cols.as<int>(), h->ell_coef32.as<uint32_t>(), h->stream)
+              : bosons ? launch_boson_ell_fill(f, h->ell_slice_ptr.as<long long>(), h->ell_slice_len.as<int>(),
+                                               h->ell_cols.as<int>(), h->ell_coef32.as<uint32_t>(), h->stream)
+                       : launch_fqhe_ell_fill(f, h->ell_slice_ptr.as<long long>(), h->ell_slice_len.as<int>(),
+                                              h->ell_cols.as<int>(), h->ell_coef.as<uint16_t>(), h->stream)) != DH_OK)
     return rc;
   h->fast = true;
   h->fast_use = true;

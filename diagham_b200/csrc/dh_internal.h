@@ -257,9 +257,11 @@ struct EllDevice {
   const int* slice_len;        // [nslices] elements per row of the slice (padded to a multiple of kEllPad)
   const int* cols;             // target index of each element
   const uint16_t* coef;        // factor index | sign << 15; padding holds nbr_factors (a zero factor)
-  // bosons (BosonOnSphereShort): factor index | caa << 16 | cad << 24, the element being
-  // factor * sqrt(caa) * sqrt(cad); coef is then null
+  // payload 1, bosons (BosonOnSphereShort): factor index | caa << 16 | cad << 24, the element being
+  // factor * sqrt(caa) * sqrt(cad); payload 2, fermions of the count-table engine (FermionOnSphereLong,
+  // FermionOnSphere beyond 40 orbitals): factor index | sign << 31, factors read through the cache
   const uint32_t* coef32;
+  int payload;                 // 0: coef (uint16), 1 or 2: coef32 as above
   const void* diag;            // [dim] diagonal, FP64 or FP32 like the factors
   const void* factors;         // [nbr_factors] FP64 or FP32
   long long dim;
@@ -271,6 +273,10 @@ int launch_fqhe_ell_fill(const FqheDevice& f, const long long* slice_ptr, const 
                          uint16_t* coef, cudaStream_t s);
 int launch_fqhe_diag(const FqheDevice& f, const double* factors64, double* diag64, float* diag32, cudaStream_t s);
 int launch_ell_product(const EllDevice& e, const MatvecArgs& a, int precision, cudaStream_t s);
+int launch_long_row_counts(const FqheLongDevice& f, int* counts, cudaStream_t s);
+int launch_long_ell_fill(const FqheLongDevice& f, int nbr_factors, const long long* slice_ptr, const int* slice_len,
+                         int* cols, uint32_t* coef, cudaStream_t s);
+int launch_long_diag(const FqheLongDevice& f, const double* factors64, double* diag64, float* diag32, cudaStream_t s);
 int launch_boson_row_counts(const FqheDevice& f, int* counts, cudaStream_t s);
 int launch_boson_ell_fill(const FqheDevice& f, const long long* slice_ptr, const int* slice_len, int* cols,
                           uint32_t* coef, cudaStream_t s);

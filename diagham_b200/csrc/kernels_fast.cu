@@ -13,7 +13,10 @@
 // Diagonal moves are summed per row into a separate diagonal array, recomputed when the
 // pseudopotentials change.  Bosonic elements (BosonOnSphereShort) carry their occupation factors: a
 // uint32 of factor index | caa << 16 | cad << 24 for the element factor * sqrt(caa) * sqrt(cad), the
-// square roots read from a 256-entry table in shared memory.
+// square roots read from a 256-entry table in shared memory.  Fermions of the count-table engine
+// (FermionOnSphereLong, FermionOnSphere beyond 40 orbitals) have factor tables too large for 15-bit
+// indices and for shared memory: a uint32 of factor index | sign << 31, factors read through the
+// cache.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -175,7 +178,9 @@ __device__ __forceinline__ void gather(const TG* x, const MatvecArgs& a, long lo
 // stream and a chunk of gathers in flight.  The stream, the diagonal and y go through L2 with
 // streaming (evict-first) accesses so that the gathered x keeps the cache.
 // W256: FP64 rows of 4 that are 32-byte aligned, gathered with one 256-bit load each
-// BOSON: uint32 payloads (16-byte groups of 4, like the targets) with the occupation square roots
+// PK (payload kind): 0 uint16 index | sign << 15, factors in shared memory; 1 (bosons) uint32 payloads
+// (16-byte groups of 4, like the targets) with the occupation square roots; 2 uint32 index | sign << 31,
+// factors read through the cache
 template <typename TG>
 __device__ __forceinline__ TG occupation_sqrt(int v);
 template <>
@@ -187,18 +192,20 @@ __device__ __forceinline__ float occupation_sqrt<float>(int v) {
   return sqrtf((float)v);
 }
 
-template <typename TG, int K, bool IL, bool W256, int CH, bool BOSON>
+template <typename TG, int K, bool IL, bool W256, int CH, int PK>
 __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, MatvecArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   TG* sfac = reinterpret_cast<TG*>(smem);
   TG* ssq = sfac + e.nbr_factors + 1;
   const TG* gfac = static_cast<const TG*>(e.factors);
-  for (int i = threadIdx.x; i < e.nbr_factors; i += blockDim.x) sfac[i] = gfac[i];
-  if (threadIdx.x == 0) sfac[e.nbr_factors] = TG(0);
-  if (BOSON)
+  if (PK != 2) {
+    for (int i = threadIdx.x; i < e.nbr_factors; i += blockDim.x) sfac[i] = gfac[i];
+    if (threadIdx.x == 0) sfac[e.nbr_factors] = TG(0);
+  }
+  if (PK == 1)
     for (int i = threadIdx.x; i < 256; i += blockDim.x) ssq[i] = occupation_sqrt<TG>(i);
   __syncthreads();
-  using KT = std::conditional_t<BOSON, uint4, uint2>;
+  using KT = std::conditional_t<PK == 0, uint2, uint4>;
   const TG* x = static_cast<const TG*>(a.x);
   const TG* diag = static_cast<const TG*>(e.diag);
   const int lane = threadIdx.x & 31;
@@ -215,7 +222,7 @@ __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, 
     const int len = e.slice_len[sl];
     const int4* cg = reinterpret_cast<const int4*>(e.cols + e.slice_ptr[sl]) + lane;
     const KT* kg;
-    if constexpr (BOSON) kg = reinterpret_cast<const uint4*>(e.coef32 + e.slice_ptr[sl]) + lane;
+    if constexpr (PK != 0) kg = reinterpret_cast<const uint4*>(e.coef32 + e.slice_ptr[sl]) + lane;
     else kg = reinterpret_cast<const uint2*>(e.coef + e.slice_ptr[sl]) + lane;
     TG acc[K];
 #pragma unroll
@@ -245,7 +252,7 @@ __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, 
       for (int g = 0; g < NG; ++g) {
         const int cols[4] = {c[g].x, c[g].y, c[g].z, c[g].w};
         unsigned ks[4];
-        if constexpr (BOSON) {
+        if constexpr (PK != 0) {
           ks[0] = k[g].x; ks[1] = k[g].y; ks[2] = k[g].z; ks[3] = k[g].w;
         } else {
           ks[0] = k[g].x & 0xffffu; ks[1] = k[g].x >> 16; ks[2] = k[g].y & 0xffffu; ks[3] = k[g].y >> 16;
@@ -256,8 +263,12 @@ __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, 
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           TG fu;
-          if constexpr (BOSON) {
+          if constexpr (PK == 1) {
             fu = sfac[ks[u] & 0xffffu] * ssq[(ks[u] >> 16) & 0xffu] * ssq[ks[u] >> 24];
+          } else if constexpr (PK == 2) {
+            const unsigned fi = ks[u] & 0x7fffffffu;
+            fu = (fi < (unsigned)e.nbr_factors) ? __ldg(gfac + fi) : TG(0);
+            if (ks[u] & 0x80000000u) fu = -fu;
           } else {
             fu = sfac[ks[u] & 0x7fffu];
             if (ks[u] & 0x8000u) fu = -fu;
@@ -299,14 +310,14 @@ unsigned grid_for(long long n) {
   return (unsigned)g;
 }
 
-template <typename TG, int K, bool IL, bool BOSON>
+template <typename TG, int K, bool IL, int PK>
 int launch_ell_payload(const EllDevice& e, const MatvecArgs& a, cudaStream_t s) {
   const bool deep = e.chunk == 16;
-  auto kern = deep ? ell_product_kernel<TG, K, IL, false, 16, BOSON> : ell_product_kernel<TG, K, IL, false, 8, BOSON>;
+  auto kern = deep ? ell_product_kernel<TG, K, IL, false, 16, PK> : ell_product_kernel<TG, K, IL, false, 8, PK>;
   if constexpr (IL && sizeof(TG) == 8 && K == 4)
     if ((reinterpret_cast<uintptr_t>(a.x) & 31) == 0)
-      kern = deep ? ell_product_kernel<TG, K, IL, true, 16, BOSON> : ell_product_kernel<TG, K, IL, true, 8, BOSON>;
-  const int smem = (e.nbr_factors + 1 + (BOSON ? 256 : 0)) * (int)sizeof(TG);
+      kern = deep ? ell_product_kernel<TG, K, IL, true, 16, PK> : ell_product_kernel<TG, K, IL, true, 8, PK>;
+  const int smem = (PK == 2) ? 0 : (e.nbr_factors + 1 + (PK == 1 ? 256 : 0)) * (int)sizeof(TG);
   if (smem > 48 * 1024) DH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int dev = 0, sms = 0, per_sm = 0;
   DH_CUDA(cudaGetDevice(&dev));
@@ -325,7 +336,9 @@ int launch_ell_payload(const EllDevice& e, const MatvecArgs& a, cudaStream_t s) 
 
 template <typename TG, int K, bool IL>
 int launch_ell_typed(const EllDevice& e, const MatvecArgs& a, cudaStream_t s) {
-  return e.coef32 ? launch_ell_payload<TG, K, IL, true>(e, a, s) : launch_ell_payload<TG, K, IL, false>(e, a, s);
+  if (e.payload == 1) return launch_ell_payload<TG, K, IL, 1>(e, a, s);
+  if (e.payload == 2) return launch_ell_payload<TG, K, IL, 2>(e, a, s);
+  return launch_ell_payload<TG, K, IL, 0>(e, a, s);
 }
 
 template <typename TG>

@@ -350,6 +350,129 @@ __global__ void __launch_bounds__(kLongThreads) long_count_kernel(FqheLongDevice
   if ((threadIdx.x & 31) == 0) atomicAdd(total, c);
 }
 
+// ------------------------------------------- moves one at a time: stored elements
+// Visits the moves of row r (word s) in the product kernel's order (m1 > m2 descending, m3 ascending);
+// visit(target, factor index, negative, diagonal).  Targets from the count-table walk over the
+// orbitals the move touches, both sides.
+template <typename W, typename Visit>
+__device__ __forceinline__ void long_visit_row(const FqheLongDevice& f, long long r, W s, Visit&& visit) {
+  using O = Word<W>;
+  const W full = O::below(f.lz_max + 1);
+  W rem1 = s;
+  while (u_any(rem1)) {
+    const int m1 = u_highest(rem1);
+    rem1 = u_and(rem1, u_not(O::bit(m1)));
+    W rem2 = rem1;
+    while (u_any(rem2)) {
+      const int m2 = u_highest(rem2);
+      rem2 = u_and(rem2, u_not(O::bit(m2)));
+      const int M = m1 + m2;
+      const W an = u_and(s, u_not(u_or(O::bit(m1), O::bit(m2))));
+      const W e = u_and(u_not(an), full);
+      W valid = u_and(u_and(e, O::mirror(e, M)), u_not(O::below(M / 2 + 1)));
+      const int paa = 1 + u_popc(u_and(s, O::between(m2, m1)));
+      const int fbase = __ldg(f.pair_offset + m1 * (m1 - 1) / 2 + m2) - (M / 2 + 1);
+      while (u_any(valid)) {
+        const int m3 = u_lowest(valid);
+        valid = u_clear_lowest(valid);
+        const int m4 = M - m3;
+        const int par = paa + u_popc(u_and(an, O::between(m4, m3)));
+        if (m3 == m1) {
+          visit(r, fbase + m3, (par & 1) != 0, true);
+          continue;
+        }
+        const W t = u_or(an, u_or(O::bit(m3), O::bit(m4)));
+        const int lo = min(m2, m4), hi = max(m1, m3);
+        const W low_part = u_and(s, O::below(lo));
+        const int n0 = u_popc(low_part), s0 = u_position_sum(low_part);
+        const long long idx = r + range_terms<W>(f, s, lo, hi, n0, s0) - range_terms<W>(f, t, lo, hi, n0, s0);
+        visit(idx, fbase + m3, (par & 1) != 0, false);
+      }
+    }
+  }
+}
+
+// off-diagonal moves per row: every pair's valid creations less its diagonal one (always valid)
+template <typename W>
+__global__ void long_row_counts_kernel(FqheLongDevice f, int* counts) {
+  using O = Word<W>;
+  const W full = O::below(f.lz_max + 1);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+    const W s = O::load(f.words, r);
+    int c = 0;
+    W rem1 = s;
+    while (u_any(rem1)) {
+      const int m1 = u_highest(rem1);
+      rem1 = u_and(rem1, u_not(O::bit(m1)));
+      W rem2 = rem1;
+      while (u_any(rem2)) {
+        const int m2 = u_highest(rem2);
+        rem2 = u_and(rem2, u_not(O::bit(m2)));
+        const int M = m1 + m2;
+        const W an = u_and(s, u_not(u_or(O::bit(m1), O::bit(m2))));
+        const W e = u_and(u_not(an), full);
+        c += u_popc(u_and(u_and(e, O::mirror(e, M)), u_not(O::below(M / 2 + 1)))) - 1;
+      }
+    }
+    counts[r] = c;
+  }
+}
+
+// element payload: factor index | sign << 31; padding: the row itself times the zero factor
+// nbr_factors
+template <typename W>
+__global__ void long_ell_fill_kernel(FqheLongDevice f, int nbr_factors, const long long* slice_ptr,
+                                     const int* slice_len, int* cols, uint32_t* coef) {
+  using O = Word<W>;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+    const long long base = slice_ptr[r >> 5];
+    const int len = slice_len[r >> 5];
+    const int lane = (int)(r & 31);
+    auto at = [&](int jj) {
+      return base + (long long)(jj / kEllGroup) * (32 * kEllGroup) + lane * kEllGroup + (jj % kEllGroup);
+    };
+    int j = 0;
+    long_visit_row<W>(f, r, O::load(f.words, r), [&](long long idx, int fidx, bool neg, bool diag) {
+      if (diag) return;
+      const long long p = at(j++);
+      cols[p] = (int)idx;
+      coef[p] = (uint32_t)fidx | (neg ? 0x80000000u : 0u);
+    });
+    for (; j < len; ++j) {
+      const long long p = at(j);
+      cols[p] = (int)r;
+      coef[p] = (uint32_t)nbr_factors;
+    }
+  }
+}
+
+// diagonal of every row: the moves (m3, m4) = (m1, m2), each with sign -1
+template <typename W>
+__global__ void long_diag_kernel(FqheLongDevice f, const double* factors, double* diag64, float* diag32) {
+  using O = Word<W>;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+    const W s = O::load(f.words, r);
+    double d = 0.0;
+    W rem1 = s;
+    while (u_any(rem1)) {
+      const int m1 = u_highest(rem1);
+      rem1 = u_and(rem1, u_not(O::bit(m1)));
+      W rem2 = rem1;
+      while (u_any(rem2)) {
+        const int m2 = u_highest(rem2);
+        rem2 = u_and(rem2, u_not(O::bit(m2)));
+        const int M = m1 + m2;
+        d -= factors[__ldg(f.pair_offset + m1 * (m1 - 1) / 2 + m2) - (M / 2 + 1) + m1];
+      }
+    }
+    diag64[r] = d;
+    diag32[r] = (float)d;
+  }
+}
+
 int grid_for(long long rows) {
   int sms = 148, dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -430,6 +553,38 @@ int launch_long_count(const FqheLongDevice& f, unsigned long long* total, cudaSt
     long_count_kernel<uint64_t><<<grid_for(f.dim), kLongThreads, 0, s>>>(f, total);
   else
     long_count_kernel<U128><<<grid_for(f.dim), kLongThreads, 0, s>>>(f, total);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_long_row_counts(const FqheLongDevice& f, int* counts, cudaStream_t s) {
+  if (f.dim <= 0) return DH_OK;
+  if (f.lz_max <= 63)
+    long_row_counts_kernel<uint64_t><<<grid_for(f.dim), kLongThreads, 0, s>>>(f, counts);
+  else
+    long_row_counts_kernel<U128><<<grid_for(f.dim), kLongThreads, 0, s>>>(f, counts);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_long_ell_fill(const FqheLongDevice& f, int nbr_factors, const long long* slice_ptr, const int* slice_len,
+                         int* cols, uint32_t* coef, cudaStream_t s) {
+  if (f.dim <= 0) return DH_OK;
+  if (f.lz_max <= 63)
+    long_ell_fill_kernel<uint64_t><<<grid_for(f.dim), kLongThreads, 0, s>>>(f, nbr_factors, slice_ptr, slice_len, cols,
+                                                                              coef);
+  else
+    long_ell_fill_kernel<U128><<<grid_for(f.dim), kLongThreads, 0, s>>>(f, nbr_factors, slice_ptr, slice_len, cols, coef);
+  DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_long_diag(const FqheLongDevice& f, const double* factors64, double* diag64, float* diag32, cudaStream_t s) {
+  if (f.dim <= 0) return DH_OK;
+  if (f.lz_max <= 63)
+    long_diag_kernel<uint64_t><<<grid_for(f.dim), kLongThreads, 0, s>>>(f, factors64, diag64, diag32);
+  else
+    long_diag_kernel<U128><<<grid_for(f.dim), kLongThreads, 0, s>>>(f, factors64, diag64, diag32);
   DH_CUDA(cudaGetLastError());
   return DH_OK;
 }

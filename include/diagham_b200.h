@@ -263,9 +263,11 @@ int dh_hamiltonian_block_multiply(dh_hamiltonian_t h, const double* x, double* y
  * device memory; every later full product of this Hamiltonian then reads them instead of
  * enumerating the moves.  *bytes = the memory the structure needs (set even when it is not built),
  * *enabled = 1 if it was built.  The elements do not depend on the pseudopotentials: setting new
- * ones only recomputes the diagonal.  FermionOnSphere and BosonOnSphereShort Hamiltonians; a bosonic
- * element stores, beside its target, the factor index and the two occupation products under its square
- * roots in 8 bits each (N <= 16, else DH_ERR_UNSUPPORTED).  Partial column ranges stay on the fly. */
+ * ones only recomputes the diagonal.  FermionOnSphere, FermionOnSphereLong and BosonOnSphereShort
+ * Hamiltonians; a bosonic element stores, beside its target, the factor index and the two occupation
+ * products under its square roots in 8 bits each (N <= 16, else DH_ERR_UNSUPPORTED); an element of the
+ * 128-bit engine (FermionOnSphereLong, FermionOnSphere above 40 orbitals) a 31-bit factor index and its
+ * sign.  Partial column ranges stay on the fly. */
 int dh_hamiltonian_enable_fast_multiplication(dh_hamiltonian_t h, int64_t allowed_memory, int* enabled,
                                               int64_t* bytes);
 /* Frees the stored elements: products go back to the on-the-fly kernels.  No reference counterpart

@@ -11,6 +11,8 @@
 - Lanczos: the reference's E0 (1e-10) where its factors are accurate, the lowest eigenvalue of the
   dense matrix at 2S = 126, and E0 = 0 with <L^2> = 0 for the Laughlin 1/M state of its parent
   pseudopotentials at 2S = 66; block and FP32-refined solves reach the same energy;
+- stored elements (EnableFastMultiplication, uint32 factor index | sign payloads, factors read
+  through the cache): the same products and Lanczos runs;
 - counts, and what the 128-bit engine does not offer is refused with an error."""
 import glob
 import hashlib
@@ -216,8 +218,6 @@ def test_long_refusals(gpu):
     sp = gpu.FermionOnSphereLong(4, 0, 70)
     H = gpu.ParticleOnSphereGenericHamiltonian(sp, 4, 70, v)
     with pytest.raises(gpu.DiagHamError, match="error -4"):
-        H.EnableFastMultiplication()
-    with pytest.raises(gpu.DiagHamError, match="error -4"):
         H.pseudopotential_adjoint(np.ones(sp.dim), np.ones(sp.dim))
     with pytest.raises(gpu.DiagHamError, match="error -4"):
         sp.set_index_mode("lookup")
@@ -288,3 +288,58 @@ def test_many_fermion_sectors_walk_both_sides(gpu, orc):
     xl = orc.random_vector(4, sp.dim)
     ref = orc.FQHELong(40, 41, 2, v41).push(xl)
     assert np.max(np.abs(Hl.LowLevelMultiply(xl) - ref)) <= 1e-13 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("prec,tol64", [("fp64", None), ("fp32", 2e-6)])
+@pytest.mark.parametrize("name", NAMES)
+def test_long_stored_elements_match_reference(gpu, orc, name, prec, tol64):
+    # EnableFastMultiplication on the count-table engine (AbstractQHEOnSphereHamiltonian.cc:3625, 3814):
+    # the rows' (target, factor index, sign) in device memory, then products from them
+    z = golden(name)
+    space, n, s, lz = _sector(name)
+    sp = _space(gpu, name)
+    H = gpu.ParticleOnSphereGenericHamiltonian(sp, n, s, z["v"])
+    H.set_precision(prec)
+    tol = tol64 if tol64 is not None else (1e-13 if space == "long" else 1e-12)
+    x = orc.random_vector(int(z["seed"]), sp.dim)
+    y_fly = H.LowLevelMultiply(x)
+    enabled, nbytes = H.EnableFastMultiplication()
+    assert enabled and nbytes >= 8 * (H.count_elements() - H.count_diagonal_elements())
+    shifts = [0.0] + ([0.37] if "y_shift0.37" in z.files else [])
+    for shift in shifts:
+        H.ShiftHamiltonian(shift)
+        ref = z["y_shift%g" % shift]
+        assert np.max(np.abs(H.LowLevelMultiply(x) - ref)) <= tol * np.max(np.abs(ref)), shift
+    H.ShiftHamiltonian(0.0)
+    ref = z["y_shift0"]
+    scale = np.max(np.abs(ref))
+    # the same elements in the same order as the on-the-fly kernel, the diagonal summed apart
+    assert np.max(np.abs(H.LowLevelMultiply(x) - y_fly)) <= (1e-14 if prec == "fp64" else 1e-6) * scale
+    for k in (2, 4):
+        X = np.stack([x * c for c in (1.0, -0.5, 2.0, 0.25)[:k]], axis=1)
+        Y = H.block_multiply(X)
+        for j in range(k):
+            c = X[0, j] / x[0]
+            assert np.max(np.abs(Y[:, j] - c * ref)) <= tol * abs(c) * scale, (k, j)
+
+
+def test_long_stored_elements_new_pseudopotentials_and_lanczos(gpu, orc):
+    n, s, lz = 4, 70, 0
+    z = golden("long_long_n4_2s70_lz0.npz")
+    sp = gpu.FermionOnSphereLong(n, lz, s)
+    H = gpu.ParticleOnSphereGenericHamiltonian(sp, n, s, z["v"])
+    e_fly = gpu.BasicLanczosAlgorithm(H, 1, 600)
+    e_fly.InitializeLanczosAlgorithm(orc.random_vector(3, sp.dim))
+    r_fly = e_fly.solve(600)
+    assert H.EnableFastMultiplication()[0]
+    lz_ = gpu.BasicLanczosAlgorithm(H, 1, 600)
+    lz_.InitializeLanczosAlgorithm(orc.random_vector(3, sp.dim))
+    r = lz_.solve(600)
+    assert abs(r["eigenvalues"][0] - r_fly["eigenvalues"][0]) <= 1e-10 * abs(r_fly["eigenvalues"][0])
+    # new pseudopotentials: the stored elements hold factor indices, only the diagonal is recomputed
+    v2 = np.array(z["v"]) * 0.5
+    v2[1] += 0.25
+    H.set_pseudopotentials(v2)
+    x = orc.random_vector(4, sp.dim)
+    ref = orc.FQHELong(n, s, lz, v2).push(x)
+    assert np.max(np.abs(H.LowLevelMultiply(x) - ref)) <= 1e-13 * np.max(np.abs(ref))
