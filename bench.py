@@ -659,8 +659,8 @@ def momentum_sector(dh, flush, steps=5, k=2, length=32, warmup=2, solve=True):
             "mean_launch_ms": mean_s * 1000.0, "hv_per_s": kk / mean_s, "algorithmic_bytes_per_launch": alg,
             "roofline": {"bound": "hbm", "achieved": alg / mean_s / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": alg / mean_s / 1e9 / peak, "peak_kind": kind,
-                         "limiter": "ALU: the canonical forms of the flipped words (ncu at L = 28: ALU 61 %, "
-                                    "issue 68 %, DRAM 1 %)"}}
+                         "limiter": "issue: the integer work of the canonical forms of the flipped words (ncu "
+                                    "at L = 28: issue 69 %, ALU 56 %, DRAM 1.5 %)"}}
         del x, y
     H.set_precision("fp64")
     if not solve:

@@ -173,8 +173,17 @@ __device__ __forceinline__ long long rep_find(const TransDevice& d, uint32_t c) 
 }
 
 // rotation of an L-bit word by s sites towards the low bits (s rotr1 steps), 0 <= s < L
-__device__ __forceinline__ uint32_t rotr_by(uint32_t w, int s, int L, uint32_t mask) {
-  return s == 0 ? w : (((w >> s) | (w << (L - s))) & mask);
+// Rotations within L bits by one funnel shift: with W = w | w << L (2L bits), the low L bits of W >> s
+// are w rotated right by s (0 <= s < L).  lo, hi are the low and high 32 bits of W.
+struct RotWord {
+  uint32_t lo, hi;
+};
+__device__ __forceinline__ RotWord rot_prep(uint32_t w, int L) {
+  const uint64_t W = (uint64_t)w | ((uint64_t)w << L);
+  return {(uint32_t)W, (uint32_t)(W >> 32)};
+}
+__device__ __forceinline__ uint32_t rot_apply(RotWord r, int s, uint32_t mask) {
+  return __funnelshift_r(r.lo, r.hi, s) & mask;
 }
 
 // The smallest of the L rotations of w (rotr1 steps) and the number n of steps to it, the first (the
@@ -186,22 +195,23 @@ __device__ __forceinline__ uint32_t canonical_rotation(uint32_t w, int L, uint32
   const uint32_t z = ~w & mask;
   n = 0;
   if (z == 0) return w;  // all ones: every rotation is w
+  const RotWord zr = rot_prep(z, L);
   uint32_t a = z;
   int t = 1;
   while (t < L) {
-    const uint32_t next = a & rotr_by(z, t, L, mask);
+    const uint32_t next = a & rot_apply(zr, t, mask);
     if (next == 0) break;
     a = next;
     ++t;
   }
   // candidates in increasing n: n = (p + t) mod L for every set bit p of a
-  const uint32_t cand = rotr_by(a, L - t, L, mask);  // bit (p + t) mod L for each p
+  uint32_t rem = rot_apply(rot_prep(a, L), L - t, mask);  // bit (p + t) mod L for each p
+  const RotWord wr = rot_prep(w, L);
   uint32_t c = 0xffffffffu;
-  uint32_t rem = cand;
   while (rem) {
     const int j = __ffs(rem) - 1;
     rem &= rem - 1u;
-    const uint32_t r = rotr_by(w, j, L, mask);
+    const uint32_t r = rot_apply(wr, j, mask);
     if (r < c) {
       c = r;
       n = j;
@@ -210,19 +220,19 @@ __device__ __forceinline__ uint32_t canonical_rotation(uint32_t w, int L, uint32
   return c;
 }
 
-// index of representative c through the read-only path, or -1
-__device__ __forceinline__ long long rep_find_ro(const TransDevice& d, uint32_t c) {
+// index of representative c through the read-only path, or -1 (dimensions below 2^31)
+__device__ __forceinline__ int rep_find_ro(const TransDevice& d, uint32_t c) {
   const long long v = (long long)(c >> d.table_shift);
   if (v + 1 >= d.table_entries) return -1;
-  long long lo = __ldg(d.table + v), hi = __ldg(d.table + v + 1);
+  int lo = __ldg(d.table + v), hi = __ldg(d.table + v + 1);
   while (lo < hi) {
-    const long long mid = (lo + hi) >> 1;
+    const int mid = (int)(((unsigned)lo + (unsigned)hi) >> 1);
     if (__ldg(d.reps + mid) >= c)
       hi = mid;
     else
       lo = mid + 1;
   }
-  return (lo < d.dim && __ldg(d.reps + lo) == c) ? lo : -1;
+  return (lo < (int)d.dim && __ldg(d.reps + lo) == c) ? lo : -1;
 }
 
 // the map entry of a flipped word computed in registers: representative index | n << 32 |
@@ -230,7 +240,7 @@ __device__ __forceinline__ long long rep_find_ro(const TransDevice& d, uint32_t 
 __device__ __forceinline__ unsigned long long canonical_entry(const TransDevice& d, uint32_t wf, int L, uint32_t mask) {
   int n = 0;
   const uint32_t c = canonical_rotation(wf, L, mask, n);
-  const long long t = rep_find_ro(d, c);
+  const int t = rep_find_ro(d, c);
   if (t < 0) return 0xffffffffull;
   return (unsigned long long)t | ((unsigned long long)n << 32) | ((unsigned long long)__ldg(d.orbits + t) << 40);
 }
@@ -455,7 +465,7 @@ __global__ void __launch_bounds__(kTransThreads) trans_matvec_kernel(TransDevice
         bool ok = t[q] != 0xffffffffu;  // the flipped word's orbit is not in this momentum sector
         if (RANGE) ok = ok && (long long)t[q] >= a.col_first && (long long)t[q] < a.col_last;
         const int n = (int)((e[q] >> 32) & 0xffull), ot = (int)((e[q] >> 40) & 0xffull);
-        c[q] = ok ? hj[q] * (TG)(sh.ratio[os * 33 + ot] * sh.phase[(L - n) % L]) : TG(0);
+        c[q] = ok ? hj[q] * (TG)(sh.ratio[os * 33 + ot] * sh.phase[n ? L - n : 0]) : TG(0);
         if (!ok) t[q] = (unsigned int)s;  // a harmless in-range gather with a zero coefficient
       }
       TG v[kTransBatch][K];
@@ -564,7 +574,7 @@ __global__ void __launch_bounds__(kTransThreads) trans_matvec_complex_kernel(Tra
         bool ok = t[q] != 0xffffffffu;  // the flipped word's orbit is not in this momentum sector
         if (RANGE) ok = ok && (long long)t[q] >= c_first && (long long)t[q] < c_last;
         const int n = (int)((e[q] >> 32) & 0xffull), ot = (int)((e[q] >> 40) & 0xffull);
-        const int m = (L - n) % L;
+        const int m = n ? L - n : 0;
         const double mag = ok ? sh.ratio[os * 33 + ot] : 0.0;
         cr[q] = hj[q] * (TG)(mag * sh.phase[m]);
         cim[q] = -hj[q] * (TG)(mag * sh.sine[m]);
