@@ -1469,8 +1469,9 @@ int dh_hamiltonian_get_interaction_factors(dh_hamiltonian_t h, double* factors, 
 
 int dh_hamiltonian_pseudopotential_adjoint(dh_hamiltonian_t h, const double* u, const double* v, double* out) {
   DH_CHECK(h && u && v && out, DH_ERR_ARGUMENT, "null argument");
-  DH_CHECK((h->kind == SPACE_FERMION || h->kind == SPACE_BOSON) && !h->l2_only, DH_ERR_UNSUPPORTED,
-           "the pseudopotential adjoint needs a FermionOnSphere or BosonOnSphereShort interaction Hamiltonian");
+  DH_CHECK((h->kind == SPACE_FERMION || h->kind == SPACE_FERMION_LONG || h->kind == SPACE_BOSON) && !h->l2_only,
+           DH_ERR_UNSUPPORTED,
+           "the pseudopotential adjoint needs a FermionOnSphere(Long) or BosonOnSphereShort interaction Hamiltonian");
   dh_space_s* sp = h->space;
   const int64_t dim = sp->dim;
   const size_t bytes = (size_t)dim * sizeof(double);
@@ -1492,10 +1493,15 @@ int dh_hamiltonian_pseudopotential_adjoint(dh_hamiltonian_t h, const double* u, 
   DH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const int nblocks = sms * 2;
   const int nf = h->tabs.nbr_factors;
-  if ((rc = ensure_buffer(h->bins_partial, (size_t)nblocks * nf * sizeof(double))) != DH_OK) return rc;
+  // per-block partial bins, except for the 128-bit engine's large tables (atomics into the bins)
+  const bool partial = !(h->kind == SPACE_FERMION_LONG && (size_t)nf * sizeof(double) > 200 * 1024);
+  if (partial && (rc = ensure_buffer(h->bins_partial, (size_t)nblocks * nf * sizeof(double))) != DH_OK) return rc;
   if ((rc = ensure_buffer(h->bins, (size_t)nf * sizeof(double))) != DH_OK) return rc;
   const FqheDevice fd = fqhe_device(sp, h, DH_PRECISION_FP64);
-  if ((rc = (h->kind == SPACE_BOSON)
+  if ((rc = (h->kind == SPACE_FERMION_LONG)
+                ? launch_long_bins(fqhe_long_device(sp, h, DH_PRECISION_FP64), nf, du, dv, h->bins_partial.as<double>(),
+                                   nblocks, h->bins.as<double>(), h->stream)
+            : (h->kind == SPACE_BOSON)
                 ? launch_boson_bins(fd, du, dv, h->bins_partial.as<double>(), nblocks, h->bins.as<double>(), h->stream)
                 : launch_fqhe_bins(fd, du, dv, h->bins_partial.as<double>(), nblocks, h->bins.as<double>(), h->stream)) !=
       DH_OK)

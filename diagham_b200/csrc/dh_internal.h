@@ -277,6 +277,8 @@ int launch_long_row_counts(const FqheLongDevice& f, int* counts, cudaStream_t s)
 int launch_long_ell_fill(const FqheLongDevice& f, int nbr_factors, const long long* slice_ptr, const int* slice_len,
                          int* cols, uint32_t* coef, cudaStream_t s);
 int launch_long_diag(const FqheLongDevice& f, const double* factors64, double* diag64, float* diag32, cudaStream_t s);
+int launch_long_bins(const FqheLongDevice& f, int nbr_factors, const double* u, const double* v, double* partial_bins,
+                     int nblocks, double* bins, cudaStream_t s);
 int launch_boson_row_counts(const FqheDevice& f, int* counts, cudaStream_t s);
 int launch_boson_ell_fill(const FqheDevice& f, const long long* slice_ptr, const int* slice_len, int* cols,
                           uint32_t* coef, cudaStream_t s);

@@ -473,6 +473,44 @@ __global__ void long_diag_kernel(FqheLongDevice f, const double* factors, double
   }
 }
 
+// adjoint bins: bins[f] = sum over rows r and moves (r -> t) of factor f of u[r] * sign * v[t], every
+// move (the diagonal ones included).  SHARED: per-block partial rows of a [blocks][factors] array
+// accumulated in shared memory and summed in block order afterwards (tables up to 2S of about 54);
+// else atomics straight into the global bins (the tables of 2S up to 126 reach 2.6 MB)
+template <typename W, bool SHARED>
+__global__ void __launch_bounds__(kLongThreads) long_bins_kernel(FqheLongDevice f, int nbr_factors, const double* u,
+                                                                 const double* v, double* out) {
+  using O = Word<W>;
+  extern __shared__ __align__(16) unsigned char smem_bins[];
+  double* bins = SHARED ? reinterpret_cast<double*>(smem_bins) : out;
+  if (SHARED) {
+    for (int i = threadIdx.x; i < nbr_factors; i += blockDim.x) bins[i] = 0.0;
+    __syncthreads();
+  }
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
+    const double ur = u[r];
+    if (ur == 0.0) continue;
+    long_visit_row<W>(f, r, O::load(f.words, r), [&](long long idx, int fidx, bool neg, bool) {
+      const double c = ur * __ldg(v + idx);
+      atomicAdd(bins + fidx, neg ? -c : c);
+    });
+  }
+  if (SHARED) {
+    __syncthreads();
+    double* row = out + (size_t)blockIdx.x * nbr_factors;
+    for (int i = threadIdx.x; i < nbr_factors; i += blockDim.x) row[i] = bins[i];
+  }
+}
+
+__global__ void long_sum_partial_bins(const double* partial, int nblocks, int nbins, double* bins) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nbins) return;
+  double acc = 0.0;
+  for (int b = 0; b < nblocks; ++b) acc += partial[(size_t)b * nbins + i];
+  bins[i] = acc;
+}
+
 int grid_for(long long rows) {
   int sms = 148, dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -586,6 +624,30 @@ int launch_long_diag(const FqheLongDevice& f, const double* factors64, double* d
   else
     long_diag_kernel<U128><<<grid_for(f.dim), kLongThreads, 0, s>>>(f, factors64, diag64, diag32);
   DH_CUDA(cudaGetLastError());
+  return DH_OK;
+}
+
+int launch_long_bins(const FqheLongDevice& f, int nbr_factors, const double* u, const double* v, double* partial_bins,
+                     int nblocks, double* bins, cudaStream_t s) {
+  const int smem = nbr_factors * (int)sizeof(double);
+  const bool shared = smem <= 200 * 1024;
+  if (!shared) DH_CUDA(cudaMemsetAsync(bins, 0, (size_t)nbr_factors * sizeof(double), s));
+  if (f.dim > 0) {
+    if (shared) {
+      auto kern = (f.lz_max <= 63) ? long_bins_kernel<uint64_t, true> : long_bins_kernel<U128, true>;
+      if (smem > 48 * 1024) DH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      kern<<<nblocks, kLongThreads, smem, s>>>(f, nbr_factors, u, v, partial_bins);
+    } else {
+      auto kern = (f.lz_max <= 63) ? long_bins_kernel<uint64_t, false> : long_bins_kernel<U128, false>;
+      kern<<<nblocks, kLongThreads, 0, s>>>(f, nbr_factors, u, v, bins);
+    }
+    DH_CUDA(cudaGetLastError());
+  }
+  if (shared) {
+    long_sum_partial_bins<<<(nbr_factors + 255) / 256, 256, 0, s>>>(partial_bins, f.dim > 0 ? nblocks : 0, nbr_factors,
+                                                                    bins);
+    DH_CUDA(cudaGetLastError());
+  }
   return DH_OK;
 }
 

@@ -308,9 +308,10 @@ int dh_hamiltonian_row_elements(dh_hamiltonian_t h, int64_t row, int* targets, i
 
 /* Adjoint of the pseudopotentials (Hellmann-Feynman / bilinear VJP): out[m] = <u| dH/dV_m |v> for
  * m = 0..lz_max.  With u = v = normalised ground state this is dE0/dV_m; with u = upstream gradient
- * and v = x it is the V part of the vector-Jacobian product of H(V) x.  FermionOnSphere and
- * BosonOnSphereShort interaction Hamiltonians.  No reference counterpart; its oracle is MatrixElement
- * (AbstractQHEOnSphereHamiltonian.cc:380) of the Hamiltonian with V = e_m. */
+ * and v = x it is the V part of the vector-Jacobian product of H(V) x.  FermionOnSphere(Long) and
+ * BosonOnSphereShort interaction Hamiltonians (the 128-bit engine accumulates into the global bins with
+ * atomics once its factor table outgrows shared memory, 2S above about 54).  No reference counterpart;
+ * its oracle is MatrixElement (AbstractQHEOnSphereHamiltonian.cc:380) of the Hamiltonian with V = e_m. */
 int dh_hamiltonian_pseudopotential_adjoint(dh_hamiltonian_t h, const double* u, const double* v, double* out);
 
 /* Number of elements (a+a+aa moves, diagonal ones included; spin flips for the chain) that one

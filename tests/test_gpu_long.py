@@ -13,6 +13,8 @@
   pseudopotentials at 2S = 66; block and FP32-refined solves reach the same energy;
 - stored elements (EnableFastMultiplication, uint32 factor index | sign payloads, factors read
   through the cache): the same products and Lanczos runs;
+- the pseudopotential adjoint (shared-memory bins up to 2S of about 54, atomics beyond) against
+  products of the oracle;
 - counts, and what the 128-bit engine does not offer is refused with an error."""
 import glob
 import hashlib
@@ -218,8 +220,6 @@ def test_long_refusals(gpu):
     sp = gpu.FermionOnSphereLong(4, 0, 70)
     H = gpu.ParticleOnSphereGenericHamiltonian(sp, 4, 70, v)
     with pytest.raises(gpu.DiagHamError, match="error -4"):
-        H.pseudopotential_adjoint(np.ones(sp.dim), np.ones(sp.dim))
-    with pytest.raises(gpu.DiagHamError, match="error -4"):
         sp.set_index_mode("lookup")
     with pytest.raises(gpu.DiagHamError, match="error -4"):
         gpu._Space.states(sp)  # 128-bit words need the pair form
@@ -343,3 +343,24 @@ def test_long_stored_elements_new_pseudopotentials_and_lanczos(gpu, orc):
     x = orc.random_vector(4, sp.dim)
     ref = orc.FQHELong(n, s, lz, v2).push(x)
     assert np.max(np.abs(H.LowLevelMultiply(x) - ref)) <= 1e-13 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("space,n,s,lz", [("fermion", 4, 50, 0), ("long", 3, 63, 1), ("long", 3, 126, 0)])
+def test_long_pseudopotential_adjoint(gpu, orc, space, n, s, lz):
+    # <u|H(V)|v> is linear in V, so g . r = <u|H(r)|v> for any V = r: three random r against the oracle's
+    # 128-bit product (2S = 50: shared-memory bins; 63 and above: atomics into the global bins)
+    sp = gpu.FermionOnSphere(n, lz, s) if space == "fermion" else gpu.FermionOnSphereLong(n, lz, s)
+    v0 = orc.coulomb_pseudopotentials(s)
+    H = gpu.ParticleOnSphereGenericHamiltonian(sp, n, s, v0)
+    H.ShiftHamiltonian(0.7)  # the shift does not depend on V
+    u = orc.random_vector(21, sp.dim)
+    w = orc.random_vector(22, sp.dim)
+    g = H.pseudopotential_adjoint(u, w)
+    rng = np.random.default_rng(5)
+    for _ in range(3):
+        r = rng.uniform(-1.0, 1.0, s + 1)
+        ref = float(u @ orc.FQHELong(n, s, lz, r).push(w))
+        assert abs(float(g @ r) - ref) <= 1e-12 * max(1.0, float(np.abs(g) @ np.abs(r)))
+    # only odd relative angular momenta enter spin-polarised factors
+    assert np.all(g[0::2] == 0.0)
+    assert np.max(np.abs(H.pseudopotential_adjoint(w, u) - g)) <= 1e-12 * np.max(np.abs(g))
