@@ -957,6 +957,13 @@ def run_b200(args, world, rank, local):
             H_.set_stream(stream.cuda_stream)
             H_.set_precision("fp32")
             r = stored_elements(dh, H_, flush, sp_.dim)
+        elif args.leg == "single":
+            v_ = dh.coulomb_pseudopotentials(TWO_S)
+            v_[0::2] = 0.0
+            sp_ = dh.FermionOnSphere(N_FERMIONS, TWO_LZ, TWO_S)
+            H_ = dh.ParticleOnSphereGenericHamiltonian(sp_, N_FERMIONS, TWO_S, v_)
+            H_.set_stream(stream.cuda_stream)
+            r = time_to_e0_single_sector(dh, H_, runs=args.steps, precisions=(1e-10,))
         elif args.leg == "momentum":
             r = momentum_sector(dh, flush, steps=args.steps, length=args.chain_length or 32, warmup=args.warmup,
                                 solve=not args.no_solve)
@@ -1159,11 +1166,11 @@ def main():
                     help="with --kernel-only: the arithmetic of the timed block products")
     ap.add_argument("--chain-length", type=int, default=0,
                     help="with --kernel-only: time the J1-J2 chain block product (k = 2) at this length instead")
-    ap.add_argument("--leg", default=None, choices=["long", "momentum", "bosons", "stored", "sectors"],
+    ap.add_argument("--leg", default=None, choices=["long", "momentum", "bosons", "stored", "sectors", "single"],
                     help="run one secondary measurement alone and print its JSON (FermionOnSphereLong N=6 2S=63; "
                          "the momentum sector at --chain-length, 32 by default; BosonOnSphereShort N=12 2S=22; "
                          "the stored-element product of the N=12 2S=33 sector; the 91-sector time to E0 at 1e-10, "
-                         "median of --steps runs)")
+                         "median of --steps runs; the N=12 2S=33 time to E0 at 1e-10, median of --steps runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

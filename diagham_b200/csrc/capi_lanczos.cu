@@ -87,6 +87,7 @@ struct dh_lanczos_s {
   Reducer red;
   LanczosDev st = {};
   int krylov_cap = 0;
+  bool krylov_keep = false;  // the Krylov store grows with the run (up to cap vectors)
   bool initialized = false;
   bool ground_valid = false;
   int index = 0;   // reference "Index": the newest vector is v_{index + 1}
@@ -123,6 +124,49 @@ struct dh_lanczos_s {
 };
 
 namespace {
+
+// The Krylov store grows with the run instead of holding max_iter vectors from the start: the first
+// kKrylovFirst vectors, then doubling (one device-to-device copy per growth), each growth only while
+// it takes less than half of the free device memory.  When it cannot grow the store stops where it
+// is (the ground state is then replayed from the start vector), except under full
+// re-orthogonalisation, which needs every vector.  A growth drops the captured iterations (their
+// kernels hold the store's address).
+constexpr int kKrylovFirst = 64;
+
+int lz_reserve_krylov(dh_lanczos_s* l, int rows) {
+  rows = std::min(rows, l->cap);
+  if (!l->krylov_keep || rows <= l->krylov_cap) return DH_OK;
+  const size_t vb = (size_t)l->dim * sizeof(double);
+  const int want = std::min(l->cap, std::max(rows, std::max(kKrylovFirst, 2 * l->krylov_cap)));
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  DevBuf grown;
+  const bool fits = l->algorithm == DH_LANCZOS_FULL_REORTHOGONALIZED || (size_t)want * vb < free_b / 2;
+  if (!fits || grown.alloc((size_t)want * vb) != DH_OK) {
+    cudaGetLastError();
+    DH_CHECK(l->algorithm != DH_LANCZOS_FULL_REORTHOGONALIZED, DH_ERR_MEMORY,
+             "full re-orthogonalisation needs %zu bytes for its vectors", (size_t)want * vb);
+    l->krylov_keep = false;
+    return DH_OK;
+  }
+  if (l->krylov_cap > 0) {
+    DH_CUDA(cudaMemcpyAsync(grown.ptr, l->krylov.ptr, (size_t)l->krylov_cap * vb, cudaMemcpyDeviceToDevice, l->stream));
+    DH_CUDA(cudaStreamSynchronize(l->stream));
+  }
+  l->krylov.release();
+  l->krylov.ptr = grown.ptr;
+  l->krylov.bytes = grown.bytes;
+  grown.ptr = nullptr;
+  grown.bytes = 0;
+  l->krylov_cap = want;
+  l->st.krylov = l->krylov.as<double>();
+  l->st.krylov_cap = want;
+  if (l->graph3) {
+    cudaGraphExecDestroy(l->graph3);
+    l->graph3 = nullptr;
+  }
+  return DH_OK;
+}
 
 int lz_matvec(dh_lanczos_s* l, int src_slot, int dst_slot) {
   double* x = l->st.vec + (size_t)src_slot * l->dim;
@@ -296,6 +340,7 @@ int lz_run(dh_lanczos_s* l, int nbr_iter) {
   if (l->rows == 0) {
     target = std::max(nbr_iter, 2);
     DH_CHECK(target <= l->cap, DH_ERR_ARGUMENT, "more Lanczos rows (%d) than max_iter allows (%d)", target, l->cap);
+    if ((rc = lz_reserve_krylov(l, target)) != DH_OK) return rc;
     if ((rc = lz_first_steps(l)) != DH_OK) return rc;
     l->index = 0;
     l->rows = 2;
@@ -305,6 +350,7 @@ int lz_run(dh_lanczos_s* l, int nbr_iter) {
     DH_CHECK(target <= l->cap, DH_ERR_ARGUMENT, "more Lanczos rows (%d) than max_iter allows (%d)", target, l->cap);
   }
   l->pending = 0;
+  if ((rc = lz_reserve_krylov(l, target)) != DH_OK) return rc;
   while (l->rows < target) {
     if ((rc = lz_iteration(l, l->index + 1)) != DH_OK) return rc;
     ++l->index;
@@ -462,17 +508,18 @@ int dh_lanczos_create(dh_hamiltonian_t h, int algorithm, int nbr_eigenvalue, int
     delete l;
     return rc;
   }
-  // keep the Krylov basis on the device when it fits in half of the free memory (needed by the full
-  // re-orthogonalisation; spares the ground-state replay otherwise)
+  // keep the Krylov basis on the device (needed by the full re-orthogonalisation; spares the
+  // ground-state replay otherwise): its first vectors now, the rest as the run grows
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
   const size_t kb = (size_t)l->cap * vb;
-  if (algorithm == DH_LANCZOS_FULL_REORTHOGONALIZED || kb < free_b / 2) {
-    if (l->krylov.alloc(kb) == DH_OK) l->krylov_cap = l->cap;
-    else cudaGetLastError();
-  }
-  DH_CHECK(algorithm != DH_LANCZOS_FULL_REORTHOGONALIZED || l->krylov_cap > 0, DH_ERR_MEMORY,
+  DH_CHECK(algorithm != DH_LANCZOS_FULL_REORTHOGONALIZED || kb < free_b, DH_ERR_MEMORY,
            "full re-orthogonalisation needs %zu bytes for its vectors", kb);
+  l->krylov_keep = true;
+  if ((rc = lz_reserve_krylov(l, kKrylovFirst)) != DH_OK) {
+    delete l;
+    return rc;
+  }
   if (cudaStreamCreateWithFlags(&l->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete l;
     return cuda_fail(cudaGetLastError(), "cudaStreamCreate", __FILE__, __LINE__);
@@ -512,10 +559,11 @@ int dh_lanczos_set_vector_storage(dh_lanczos_t l, int keep) {
   if (!keep) {
     l->krylov.release();
     l->krylov_cap = 0;
+    l->krylov_keep = false;
   } else if (!l->krylov.ptr) {
-    int rc = l->krylov.alloc((size_t)l->cap * l->dim * sizeof(double));
+    l->krylov_keep = true;
+    int rc = lz_reserve_krylov(l, kKrylovFirst);
     if (rc != DH_OK) return rc;
-    l->krylov_cap = l->cap;
   }
   l->st.krylov = l->krylov.as<double>();
   l->st.krylov_cap = l->krylov_cap;
@@ -663,6 +711,7 @@ int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eige
     int todo = std::min(graph_batch, max_iter - count);
     todo = std::min(todo, l->cap - l->rows);
     if (todo <= 0) break;
+    if ((rc = lz_reserve_krylov(l, l->rows + todo)) != DH_OK) return rc;
     const int start_rows = l->rows;
     int issued = 0;
     while (issued < todo && ((l->index + 1) % 3) != 0) {
