@@ -227,3 +227,18 @@ def test_boson_element_counts(gpu):
     f = gpu.FermionOnSphere(7, 2, 18)
     Hf = gpu.ParticleOnSphereGenericHamiltonian(f, 7, 18, gpu.coulomb_pseudopotentials(18))
     assert Hf.count_diagonal_elements() == 21 * f.dim
+
+
+@pytest.mark.parametrize("n,s,lz", [(1, 6, 2), (16, 2, 0), (16, 3, 2), (2, 0, 0)])
+def test_boson_stored_elements_edge_sectors(gpu, orc, n, s, lz):
+    # one boson (no pairs: only the shift), sixteen bosons (the largest occupation products a stored
+    # element holds: 16 x 15 = 240), and a single orbital
+    v = np.linspace(1.0, 0.1, s + 1)
+    sp = gpu.BosonOnSphereShort(n, lz, s)
+    H = gpu.ParticleOnSphereGenericHamiltonian(sp, n, s, v)
+    H.ShiftHamiltonian(0.25)
+    x = orc.random_vector(9, sp.dim)
+    ref = orc.BosonFQHE(n, s, lz, v, shift=0.25).pull(x)
+    assert np.max(np.abs(H.LowLevelMultiply(x) - ref)) <= 1e-13 * max(1.0, np.max(np.abs(ref)))
+    assert H.EnableFastMultiplication()[0]
+    assert np.max(np.abs(H.LowLevelMultiply(x) - ref)) <= 1e-13 * max(1.0, np.max(np.abs(ref)))
