@@ -263,12 +263,19 @@ bool lz_converged(const dh_lanczos_s* l) {
   if (l->residual_target > 0.0) {
     const int n = l->rows - 1;
     if (n < 2 || (int)l->beta.size() < n || l->ritz.empty()) return false;
-    // the residual (an O(n^3) eigenvector solve on the host) only once the Ritz value has settled:
-    // near the residual target its changes are orders of magnitude below this
+    // the residual only once the Ritz value has settled: near the residual target its changes are
+    // orders of magnitude below this.  The lowest eigenvalue of the matrix one row short (implicit QL
+    // without vectors), then its eigenvector's last component by inverse iteration on that
+    // tridiagonal matrix (O(n) per step instead of accumulating all n eigenvectors)
     if (fabs(l->ritz[0] - l->prev_last) > 1e-7 * fabs(l->ritz[0])) return false;
-    std::vector<double> eig(n), z((size_t)n * n);
-    if (tridiagonal_eigen(n, l->alpha.data(), l->beta.data(), eig.data(), z.data()) != DH_OK) return false;
-    const double r = l->beta[n - 1] * z[n - 1];  // column 0, last component
+    std::vector<double> eig(n), t((size_t)n * n, 0.0), z(n);
+    if (tridiagonal_eigen(n, l->alpha.data(), l->beta.data(), eig.data(), nullptr) != DH_OK) return false;
+    for (int i = 0; i < n; ++i) {
+      t[(size_t)i * n + i] = l->alpha[i];
+      if (i + 1 < n) t[(size_t)i * n + i + 1] = t[(size_t)(i + 1) * n + i] = l->beta[i];
+    }
+    if (band_inverse_iteration(n, 1, t.data(), eig[0], z.data()) != DH_OK) return false;
+    const double r = l->beta[n - 1] * z[n - 1];  // the eigenvector's last component
     return r * r < l->residual_target * fabs(eig[0]);
   }
   if ((int)l->ritz.size() < l->nev) return false;
