@@ -123,11 +123,15 @@ __global__ void __launch_bounds__(kBosonThreads) boson_matvec_kernel(FqheDevice 
   int* spair = reinterpret_cast<int*>(smem + factor_smem);
   int* term = spair + ((f.nbr_pairs + 3) & ~3);
   int* osum = term + (f.nbr_particles + 1) * kBosonThreads;
+  // square roots of the occupation products 0 .. N (N - 1) (every n_m2 (n_m1 - [m1 = m2]) and
+  // (n'_m4 + 1)(n'_m3 + 1 + [m3 = m4]) lies in that range)
+  TG* ssq = reinterpret_cast<TG*>(RM == 1 ? osum + (f.nbr_particles + 1) * kBosonThreads : term);
   const TG* gfac = static_cast<const TG*>(f.factors);
   if (RM == 0)
     for (int i = threadIdx.x; i < f.nbr_factors; i += blockDim.x) sfac[i] = gfac[i];
   const TG* fac = (RM == 0) ? sfac : gfac;
   for (int i = threadIdx.x; i < f.nbr_pairs; i += blockDim.x) spair[i] = f.pair_offset[i];
+  for (int i = threadIdx.x; i <= f.nbr_particles * (f.nbr_particles - 1); i += blockDim.x) ssq[i] = coef_sqrt<TG>(i);
   __syncthreads();
 
   const int L = f.boson_lz_max;
@@ -230,7 +234,7 @@ __global__ void __launch_bounds__(kBosonThreads) boson_matvec_kernel(FqheDevice 
       rem2 &= rem2 - 1ull;
       const int n1 = n[m1], n2 = n[m2];
       const int caa = n2 * (n1 - (m1 == m2 ? 1 : 0));
-      saa = coef_sqrt<TG>(caa);
+      saa = ssq[caa];
       an = delete_bit(delete_bit(s, P[m1]), P[m2]);
       const int M = m1 + m2;
       const int m3lo = (M + 1) >> 1;
@@ -273,7 +277,7 @@ __global__ void __launch_bounds__(kBosonThreads) boson_matvec_kernel(FqheDevice 
         }
       }
       if (!RANGE || (idx >= a.col_first && idx < a.col_last)) {
-        const TG c = fp[m3] * saa * coef_sqrt<TG>(cad);
+        const TG c = fp[m3] * saa * ssq[cad];
         TG xv[K];
         gather_row<TG, K, IL>(x, a, idx, xv);
 #pragma unroll
@@ -301,6 +305,7 @@ int launch_rank(const FqheDevice& f, const MatvecArgs& a, cudaStream_t s) {
   const int factor_smem = (RM == 0) ? (int)((f.nbr_factors * sizeof(TG) + 15) & ~(size_t)15) : 0;
   size_t smem = (size_t)factor_smem + (size_t)((f.nbr_pairs + 3) & ~3) * sizeof(int);
   if (RM == 1) smem += 2 * (size_t)(f.nbr_particles + 1) * kBosonThreads * sizeof(int);
+  smem += ((size_t)f.nbr_particles * (f.nbr_particles - 1) + 2) * sizeof(TG);  // occupation square roots
   const bool range = a.col_first > 0 || a.col_last < f.dim;
   const bool il = (K > 1) && a.ld == K && a.vstride == 1 && il_rows_aligned(a, K, sizeof(TG));
   auto kernel = range ? (il ? boson_matvec_kernel<TG, K, true, true, RM> : boson_matvec_kernel<TG, K, true, false, RM>)
