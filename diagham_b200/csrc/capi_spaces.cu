@@ -1493,8 +1493,10 @@ int dh_hamiltonian_pseudopotential_adjoint(dh_hamiltonian_t h, const double* u, 
   DH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const int nblocks = sms * 2;
   const int nf = h->tabs.nbr_factors;
-  // per-block partial bins, except for the 128-bit engine's large tables (atomics into the bins)
-  const bool partial = !(h->kind == SPACE_FERMION_LONG && (size_t)nf * sizeof(double) > 200 * 1024);
+  // per-block partial bins, except for the large tables of the 128-bit engine and the widest bosonic
+  // sectors (atomics into the bins)
+  const bool partial =
+      !((h->kind == SPACE_FERMION_LONG || h->kind == SPACE_BOSON) && (size_t)nf * sizeof(double) > 200 * 1024);
   if (partial && (rc = ensure_buffer(h->bins_partial, (size_t)nblocks * nf * sizeof(double))) != DH_OK) return rc;
   if ((rc = ensure_buffer(h->bins, (size_t)nf * sizeof(double))) != DH_OK) return rc;
   const FqheDevice fd = fqhe_device(sp, h, DH_PRECISION_FP64);

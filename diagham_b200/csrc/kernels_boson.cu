@@ -518,27 +518,34 @@ __global__ void boson_diag_kernel(FqheDevice f, const double* factors, double* d
   }
 }
 
-// bins[f] = sum over rows r and moves (r -> t) of factor f of u[r] * coefficient * v[t]; per-block
-// partial rows of a [blocks][factors] array, summed in block order afterwards
+// bins[f] = sum over rows r and moves (r -> t) of factor f of u[r] * coefficient * v[t].  SHARED:
+// per-block partial rows of a [blocks][factors] array accumulated in shared memory, summed in block
+// order afterwards; else atomics straight into the global bins (the widest bosonic tables outgrow
+// shared memory)
 constexpr int kBosonBinThreads = 256;
+template <bool SHARED>
 __global__ void __launch_bounds__(kBosonBinThreads) boson_bins_kernel(FqheDevice f, const double* u, const double* v,
-                                                                      double* partial) {
+                                                                      double* out) {
   extern __shared__ __align__(16) unsigned char smem[];
-  double* sbins = reinterpret_cast<double*>(smem);
-  for (int i = threadIdx.x; i < f.nbr_factors; i += blockDim.x) sbins[i] = 0.0;
-  __syncthreads();
+  double* bins = SHARED ? reinterpret_cast<double*>(smem) : out;
+  if (SHARED) {
+    for (int i = threadIdx.x; i < f.nbr_factors; i += blockDim.x) bins[i] = 0.0;
+    __syncthreads();
+  }
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
     const double ur = u[r];
     if (ur == 0.0) continue;
     boson_visit_row(f, r, __ldg(f.words + r), [&](long long idx, int fidx, int caa, int cad, bool diag) {
       const double c = diag ? (double)caa : sqrt((double)caa) * sqrt((double)cad);
-      atomicAdd(sbins + fidx, c * ur * __ldg(v + idx));
+      atomicAdd(bins + fidx, c * ur * __ldg(v + idx));
     });
   }
-  __syncthreads();
-  double* out = partial + (size_t)blockIdx.x * f.nbr_factors;
-  for (int i = threadIdx.x; i < f.nbr_factors; i += blockDim.x) out[i] = sbins[i];
+  if (SHARED) {
+    __syncthreads();
+    double* row = out + (size_t)blockIdx.x * f.nbr_factors;
+    for (int i = threadIdx.x; i < f.nbr_factors; i += blockDim.x) row[i] = bins[i];
+  }
 }
 
 __global__ void boson_sum_partial_bins(const double* partial, int nblocks, int nbins, double* bins) {
@@ -583,17 +590,23 @@ int launch_boson_diag(const FqheDevice& f, const double* factors64, double* diag
 int launch_boson_bins(const FqheDevice& f, const double* u, const double* v, double* partial_bins, int nblocks,
                       double* bins, cudaStream_t s) {
   const int smem = f.nbr_factors * (int)sizeof(double);
-  DH_CHECK(smem <= 227 * 1024, DH_ERR_UNSUPPORTED, "%d bosonic factors do not fit the adjoint's shared bins",
-           f.nbr_factors);
+  const bool shared = smem <= 200 * 1024;
+  if (!shared) DH_CUDA(cudaMemsetAsync(bins, 0, (size_t)f.nbr_factors * sizeof(double), s));
   if (f.dim > 0) {
-    if (smem > 48 * 1024)
-      DH_CUDA(cudaFuncSetAttribute(boson_bins_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    boson_bins_kernel<<<nblocks, kBosonBinThreads, smem, s>>>(f, u, v, partial_bins);
+    if (shared) {
+      if (smem > 48 * 1024)
+        DH_CUDA(cudaFuncSetAttribute(boson_bins_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      boson_bins_kernel<true><<<nblocks, kBosonBinThreads, smem, s>>>(f, u, v, partial_bins);
+    } else {
+      boson_bins_kernel<false><<<nblocks, kBosonBinThreads, 0, s>>>(f, u, v, bins);
+    }
     DH_CUDA(cudaGetLastError());
   }
-  boson_sum_partial_bins<<<(f.nbr_factors + 255) / 256, 256, 0, s>>>(partial_bins, f.dim > 0 ? nblocks : 0,
-                                                                     f.nbr_factors, bins);
-  DH_CUDA(cudaGetLastError());
+  if (shared) {
+    boson_sum_partial_bins<<<(f.nbr_factors + 255) / 256, 256, 0, s>>>(partial_bins, f.dim > 0 ? nblocks : 0,
+                                                                       f.nbr_factors, bins);
+    DH_CUDA(cudaGetLastError());
+  }
   return DH_OK;
 }
 

@@ -122,3 +122,21 @@ def test_boson_large_stored_elements_match_oracle(gpu, orc, n, s, lz):
     y = H.LowLevelMultiply(x)
     assert np.max(np.abs(y - ref)) <= 1e-13 * np.max(np.abs(ref))
     assert np.max(np.abs(y - y_fly)) <= 1e-15 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("n,s,lz", [(2, 61, 0), (3, 40, 0)])
+def test_boson_large_pseudopotential_adjoint(gpu, orc, n, s, lz):
+    # g . r = <u|H(r)|v> for random V = r against the oracle; 2S = 61 has 41 K bosonic factors, beyond
+    # shared memory (atomics into the global bins), 2S = 40 keeps them in shared memory
+    v0 = orc.coulomb_pseudopotentials(s)
+    v0[1::2] = 0.0
+    sp = gpu.BosonOnSphereShort(n, lz, s)
+    H = gpu.ParticleOnSphereGenericHamiltonian(sp, n, s, v0)
+    u = orc.random_vector(31, sp.dim)
+    w = orc.random_vector(32, sp.dim)
+    g = H.pseudopotential_adjoint(u, w)
+    rng = np.random.default_rng(7)
+    for _ in range(3):
+        r = rng.uniform(-1.0, 1.0, s + 1)
+        ref = float(u @ orc.BosonFQHE(n, s, lz, r).pull(w))
+        assert abs(float(g @ r) - ref) <= 1e-12 * max(1.0, float(np.abs(g) @ np.abs(r)))
