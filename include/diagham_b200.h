@@ -302,7 +302,7 @@ int dh_hamiltonian_matrix_element(dh_hamiltonian_t h, const double* v1, const do
  * AbstractQHEOnSphereHamiltonian::EvaluateMNTwoBodyFastMultiplicationComponent (.h:531):
  * target index, sign (+1/-1) of AA*AdAd and interaction-factor index for every generated element
  * of `row`, in the reference enumeration order.  *count receives the total; at most cap entries
- * are written.  FQHE Hamiltonians only. */
+ * are written.  FermionOnSphere Hamiltonians (up to 40 orbitals) only. */
 int dh_hamiltonian_row_elements(dh_hamiltonian_t h, int64_t row, int* targets, int* signs, int* factor_index,
                                 int cap, int* count);
 
