@@ -383,18 +383,22 @@ def time_to_e0_all_sectors(dh, k=None, runs=3, precisions=(1e-10, 1e-13)):
         res = {}
         tp, e_plain = _median_run(lambda: plain_all(precision), nr)
         res["plain_fp64_per_sector"] = {"seconds": tp, "energies": e_plain}
-        for fp32 in (True, False):
-            t, r = _median_run(lambda: dh.fqhe_sectors_block_lanczos(n, s, sectors, v, block_size=k, max_iter=800,
-                                                                    precision=precision, fp32=fp32,
-                                                                    full_diag_limit=200), nr)
-            res["batched_%s" % ("fp32_refined" if fp32 else "fp64")] = {
-                "seconds": t, "energies": r["energies"], "block_products": r["block_products"],
-                "setup_seconds": r["setup_seconds"], "solve_seconds": r["solve_seconds"],
-                "product_seconds": r["product_seconds"], "fp32_seconds": r["fp32_seconds"],
-                "refine_seconds": r["refine_seconds"], "refined_sectors": r["refined_sectors"],
-                "dense_fallback_sectors": r["dense_fallback_sectors"],
-                "dense_fallback_seconds": r["dense_fallback_seconds"],
-                "speedup_vs_plain_fp64": tp / t}
+        # the batched forms on the fly and with the batch's stored elements (memory = -1: built inside
+        # the timed call, one ELL over the concatenated sectors)
+        for memory in (0, -1):
+            for fp32 in (True, False):
+                t, r = _median_run(lambda: dh.fqhe_sectors_block_lanczos(n, s, sectors, v, block_size=k, max_iter=800,
+                                                                        precision=precision, fp32=fp32,
+                                                                        full_diag_limit=200, memory=memory), nr)
+                res["batched_%s%s" % ("fp32_refined" if fp32 else "fp64", "_stored" if memory else "")] = {
+                    "seconds": t, "energies": r["energies"], "block_products": r["block_products"],
+                    "setup_seconds": r["setup_seconds"], "solve_seconds": r["solve_seconds"],
+                    "product_seconds": r["product_seconds"], "fp32_seconds": r["fp32_seconds"],
+                    "refine_seconds": r["refine_seconds"], "refined_sectors": r["refined_sectors"],
+                    "dense_fallback_sectors": r["dense_fallback_sectors"],
+                    "dense_fallback_seconds": r["dense_fallback_seconds"],
+                    "stored_bytes": r["stored_bytes"], "store_seconds": r["store_seconds"],
+                    "speedup_vs_plain_fp64": tp / t}
         out["precision_%g" % precision] = res
         if precision == min(precisions):
             e_strict = e_plain
@@ -508,14 +512,16 @@ def time_to_e0_summary(line):
         p = tc.get("precision_1e-10", {})
         if p:
             pl = p["plain_fp64_per_sector"]
+            refined = min((k_ for k_ in p if k_.startswith("batched_fp32_refined")), key=lambda k_: p[k_]["seconds"])
+            fp64 = min((k_ for k_ in p if k_.startswith("batched_fp64")), key=lambda k_: p[k_]["seconds"])
             out["n10_2s27_91_sectors"] = {
                 "block_k": tc.get("block"),
                 "plain_fp64_s": round(pl["seconds"], 4),
-                "batched_fp32_refined_s": round(p["batched_fp32_refined"]["seconds"], 4),
-                "batched_fp64_s": round(p["batched_fp64"]["seconds"], 4),
-                "speedup": round(p["batched_fp32_refined"]["speedup_vs_plain_fp64"], 3),
-                "max_rel_err_refined": p["batched_fp32_refined"].get("max_rel_e_minus_plain_fp64_strict"),
-                "max_rel_err_vs_reference": p["batched_fp32_refined"].get("max_rel_e_minus_reference")}
+                "batched_fp32_refined_s": round(p[refined]["seconds"], 4), "refined_form": refined,
+                "batched_fp64_s": round(p[fp64]["seconds"], 4), "fp64_form": fp64,
+                "speedup": round(p[refined]["speedup_vs_plain_fp64"], 3),
+                "max_rel_err_refined": p[refined].get("max_rel_e_minus_plain_fp64_strict"),
+                "max_rel_err_vs_reference": p[refined].get("max_rel_e_minus_reference")}
     cs = line.get("spin_chain_l32_solve")
     if cs:
         out["chain_l32"] = {"s": round(cs["seconds"], 3), "e0": cs["e0"], "rel_err": cs["rel_e0_minus_exact"]}

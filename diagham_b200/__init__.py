@@ -114,7 +114,7 @@ SIGNATURES = {
     "dh_vector_file_dimension": ([ctypes.c_char_p, _i64p], _c_int),
     "dh_vector_read": ([ctypes.c_char_p, _vp, _c_i64], _c_int),
     "dh_fqhe_sectors_block_lanczos": ([_c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _c_dbl, _c_int, _c_int,
-                                       _c_u64, _vp, _vp, _vp], _c_int),
+                                       _c_i64, _c_u64, _vp, _vp, _vp], _c_int),
     "dh_coulomb_pseudopotentials": ([_c_int, _vp], _c_int),
     "dh_clebsch_gordan": ([_c_int, _c_int, _c_int, _c_int, _c_int, _vp], _c_int),
 }
@@ -719,25 +719,27 @@ def clebsch_gordan(j1, m1, j2, m2, j):
 
 
 def fqhe_sectors_block_lanczos(nbr_fermions, lz_max, total_lz, pseudopotentials, block_size=4, max_iter=400,
-                               precision=1e-14, fp32=False, full_diag_limit=200, seed=100):
+                               precision=1e-14, fp32=False, full_diag_limit=200, seed=100, memory=0):
     """Lowest energy of every requested Lz sector: block Lanczos over all sectors in lockstep, one
     launch per block product (BasicBlockLanczosAlgorithm + QHEOnSphereMainTask's loop per sector).
-    fp32=True: FP32 products, then FP64 refinement of every sector to `precision`."""
+    fp32=True: FP32 products, then FP64 refinement of every sector to `precision`.  memory: bytes the
+    stored elements of the whole batch may take (the reference's --memory; 0: on the fly, < 0: as
+    much as fits)."""
     load()
     tl = np.ascontiguousarray(total_lz, np.int32)
     v = np.ascontiguousarray(pseudopotentials, np.float64)
     ns = tl.size
     e = np.zeros(ns, np.float64)
     it = np.zeros(ns, np.int32)
-    secs = np.zeros(10, np.float64)
+    secs = np.zeros(12, np.float64)
     _check(_lib.dh_fqhe_sectors_block_lanczos(nbr_fermions, lz_max, tl.ctypes.data, ns, v.ctypes.data, block_size,
                                               max_iter, float(precision),
-                                              DH_PRECISION_FP32 if fp32 else DH_PRECISION_FP64, full_diag_limit, seed,
-                                              e.ctypes.data, it.ctypes.data, secs.ctypes.data))
+                                              DH_PRECISION_FP32 if fp32 else DH_PRECISION_FP64, full_diag_limit,
+                                              int(memory), seed, e.ctypes.data, it.ctypes.data, secs.ctypes.data))
     return dict(energies=e, iterations=it, setup_seconds=secs[0], solve_seconds=secs[1], product_seconds=secs[2],
                 block_products=int(secs[3]), fp32_seconds=secs[4], refine_seconds=secs[5],
                 refined_sectors=int(secs[6]), max_refine_shift=secs[7], dense_fallback_sectors=int(secs[8]),
-                dense_fallback_seconds=secs[9])
+                dense_fallback_seconds=secs[9], stored_bytes=int(secs[10]), store_seconds=secs[11])
 
 
 def WriteVector(vec, file_name):

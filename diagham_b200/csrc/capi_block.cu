@@ -1295,6 +1295,127 @@ int bind_sector_product(SectorBatchHost& hb, const std::vector<int>& sectors, Bl
   return DH_OK;
 }
 
+// Stored elements over the concatenated rows of the batched sectors (the batch's
+// EnableFastMultiplication, AbstractQHEOnSphereHamiltonian.cc:3625,3814): one sliced ELL in the
+// engine's row order, every sector's targets shifted by its row offset, the factor indices of the
+// shared interaction and one diagonal per row.  Products then stream it instead of enumerating the
+// moves; the rows of converged sectors are skipped as in the on-the-fly kernel.
+struct SectorEll {
+  DevBuf slice_ptr, slice_len, cols, coef, diag64, diag32;
+  size_t bytes = 0;
+  int chunk = 16;
+};
+
+// built when it needs at most allowed_memory bytes (< 0: no budget) and fits in nine tenths of the
+// free device memory; *bytes_needed = its size either way
+int build_sector_ell(SectorBatchHost& hb, const std::vector<int>& sectors, const BlockEngine& e, int64_t allowed_memory,
+                     SectorEll& ell, bool* built, size_t* bytes_needed) {
+  *built = false;
+  *bytes_needed = 0;
+  const long long total = e.total;
+  const int ns = (int)sectors.size();
+  DH_CHECK(total < (1ll << 31), DH_ERR_UNSUPPORTED, "stored elements hold int32 targets");
+  DH_CHECK(hb.tabs.nbr_factors < 0x8000, DH_ERR_UNSUPPORTED, "%d interaction factors do not fit 15-bit indices",
+           hb.tabs.nbr_factors);
+  auto device_of = [&](int i) {
+    FqheDevice f = fqhe_device(hb.spaces[sectors[i]], nullptr, DH_PRECISION_FP64);
+    f.pair_offset = hb.pair_offset.as<int32_t>();
+    f.factors = hb.f64.ptr;
+    f.nbr_pairs = hb.tabs.nbr_pairs;
+    f.nbr_factors = hb.tabs.nbr_factors;
+    return f;
+  };
+  int rc;
+  std::vector<int> counts(total);
+  {
+    DevBuf dcounts;
+    if ((rc = dcounts.alloc((size_t)total * sizeof(int))) != DH_OK) return rc;
+    for (int i = 0; i < ns; ++i)
+      if ((rc = launch_fqhe_row_counts(device_of(i), dcounts.as<int>(), e.stream, e.off[i])) != DH_OK) return rc;
+    DH_CUDA(cudaMemcpyAsync(counts.data(), dcounts.ptr, (size_t)total * sizeof(int), cudaMemcpyDeviceToHost, e.stream));
+    DH_CUDA(cudaStreamSynchronize(e.stream));
+  }
+  const long long nslices = (total + 31) / 32;
+  std::vector<long long> slice_ptr(nslices);
+  std::vector<int> slice_len(nslices);
+  long long elems = 0;
+  for (long long sl = 0; sl < nslices; ++sl) {
+    int mx = 0;
+    for (long long r = sl * 32; r < std::min(total, sl * 32 + 32); ++r) mx = std::max(mx, counts[r]);
+    mx = (mx + kEllPad - 1) / kEllPad * kEllPad;
+    slice_ptr[sl] = elems;
+    slice_len[sl] = mx;
+    elems += 32ll * mx;
+  }
+  const size_t need = (size_t)elems * (sizeof(int) + sizeof(uint16_t)) + (size_t)nslices * (sizeof(long long) + sizeof(int)) +
+                      (size_t)total * (sizeof(double) + sizeof(float));
+  *bytes_needed = need;
+  if (allowed_memory >= 0 && need > (size_t)allowed_memory) return DH_OK;
+  size_t free_b = 0, total_b = 0;
+  DH_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  if (need > free_b / 10 * 9) return DH_OK;
+  if ((rc = ell.slice_ptr.alloc((size_t)nslices * sizeof(long long))) != DH_OK ||
+      (rc = ell.slice_len.alloc((size_t)nslices * sizeof(int))) != DH_OK ||
+      (rc = ell.cols.alloc((size_t)elems * sizeof(int))) != DH_OK ||
+      (rc = ell.coef.alloc((size_t)elems * sizeof(uint16_t))) != DH_OK ||
+      (rc = ell.diag64.alloc((size_t)total * sizeof(double))) != DH_OK ||
+      (rc = ell.diag32.alloc((size_t)total * sizeof(float))) != DH_OK)
+    return rc;
+  DH_CUDA(cudaMemcpyAsync(ell.slice_ptr.ptr, slice_ptr.data(), nslices * sizeof(long long), cudaMemcpyHostToDevice,
+                          e.stream));
+  DH_CUDA(cudaMemcpyAsync(ell.slice_len.ptr, slice_len.data(), nslices * sizeof(int), cudaMemcpyHostToDevice, e.stream));
+  for (int i = 0; i < ns; ++i) {
+    const FqheDevice f = device_of(i);
+    if ((rc = launch_fqhe_ell_fill(f, ell.slice_ptr.as<long long>(), ell.slice_len.as<int>(), ell.cols.as<int>(),
+                                   ell.coef.as<uint16_t>(), e.stream, e.off[i])) != DH_OK ||
+        (rc = launch_fqhe_diag(f, hb.f64.as<double>(), ell.diag64.as<double>(), ell.diag32.as<float>(), e.stream,
+                               e.off[i])) != DH_OK)
+      return rc;
+  }
+  DH_CUDA(cudaStreamSynchronize(e.stream));
+  ell.bytes = need;
+  *built = true;
+  return DH_OK;
+}
+
+// the engine's products from the stored elements
+void bind_sector_ell(SectorBatchHost& hb, SectorEll& ell, BlockEngine& e) {
+  SectorBatchHost* hbp = &hb;
+  SectorEll* lp = &ell;
+  BlockEngine* ep = &e;
+  e.product = [hbp, lp, ep](const double* x64, const float* x32, double* y) {
+    const bool f32 = ep->precision == DH_PRECISION_FP32;
+    EllDevice d = {};
+    d.slice_ptr = lp->slice_ptr.as<long long>();
+    d.slice_len = lp->slice_len.as<int>();
+    d.cols = lp->cols.as<int>();
+    d.coef = lp->coef.as<uint16_t>();
+    d.payload = 0;
+    d.diag = f32 ? lp->diag32.ptr : lp->diag64.ptr;
+    d.factors = f32 ? hbp->f32.ptr : hbp->f64.ptr;
+    d.dim = ep->total;
+    d.nbr_factors = hbp->tabs.nbr_factors;
+    d.chunk = lp->chunk;
+    d.active = ep->dActive;
+    d.sector_offset = ep->row_offset_dev;
+    d.nbr_sectors = ep->nsec;
+    MatvecArgs a = {};
+    a.x = f32 ? static_cast<const void*>(x32) : static_cast<const void*>(x64);
+    a.xdiag = f32 ? x64 : nullptr;
+    a.y = y;
+    a.ld = ep->k;
+    a.vstride = 1;
+    a.ld_y = ep->k;
+    a.vstride_y = 1;
+    a.nbr_vectors = ep->k;
+    a.col_first = 0;
+    a.col_last = ep->total;
+    a.row_first = 0;
+    a.row_last = ep->total;
+    return launch_ell_product(d, a, ep->precision, ep->stream);
+  };
+}
+
 // keep every block on the device when the store fits in half of the free memory
 // the first kStoreBlocks blocks (or all of max_iter / k + 3, when fewer) in half of the free memory;
 // the store then grows with the run
@@ -1319,7 +1440,8 @@ void engine_store_if_fits(BlockEngine& e) {
 extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const int* total_lz, int nbr_sectors,
                                              const double* pseudopotentials, int block_size, int max_iter,
                                              double precision_target, int precision, int full_diag_limit,
-                                             uint64_t seed, double* energies, int* iterations, double* stats) {
+                                             int64_t allowed_memory, uint64_t seed, double* energies,
+                                             int* iterations, double* stats) {
   using clk = std::chrono::steady_clock;
   const auto t0 = clk::now();
   DH_CHECK(total_lz && pseudopotentials && energies && iterations && nbr_sectors >= 1, DH_ERR_ARGUMENT, "bad argument");
@@ -1327,6 +1449,9 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
   DH_CHECK(precision == DH_PRECISION_FP64 || precision == DH_PRECISION_FP32, DH_ERR_ARGUMENT, "unknown precision");
   SectorBatchHost hb;
   BlockEngine e;
+  SectorEll ell;  // stored elements of the batch (allowed_memory != 0), destroyed before the engine
+  size_t ell_bytes = 0;
+  double ell_seconds = 0.0;
   e.k = block_size;
   e.nev = 1;
   e.precision = precision;
@@ -1396,6 +1521,17 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
     if (precision == DH_PRECISION_FP32) engine_store_if_fits(e);
     SectorProduct prod;
     if ((rc = bind_sector_product(hb, lanczos_sectors, e, prod)) != DH_OK) return rc;
+    if (allowed_memory != 0) {
+      const auto ts = clk::now();
+      bool built = false;
+      size_t need = 0;
+      if ((rc = build_sector_ell(hb, lanczos_sectors, e, allowed_memory, ell, &built, &need)) != DH_OK) return rc;
+      if (built) {
+        bind_sector_ell(hb, ell, e);
+        ell_bytes = ell.bytes;
+      }
+      ell_seconds = std::chrono::duration<double>(clk::now() - ts).count();
+    }
     const int ns = (int)lanczos_sectors.size();
     // start block: splitmix64 vectors per sector (seed + j for vector j)
     if ((rc = launch_random_block(e.slot[0], e.total, e.k, e.row_offset_dev, e.tiles, seed, e.stream)) != DH_OK)
@@ -1525,6 +1661,8 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
     stats[7] = max_shift;
     stats[8] = (double)dense_fallback;
     stats[9] = dense_seconds;
+    stats[10] = (double)ell_bytes;
+    stats[11] = ell_seconds;
   }
   return DH_OK;
 }

@@ -262,16 +262,24 @@ struct EllDevice {
   // FermionOnSphere beyond 40 orbitals): factor index | sign << 31, factors read through the cache
   const uint32_t* coef32;
   int payload;                 // 0: coef (uint16), 1 or 2: coef32 as above
+  // optional, the batched sectors: rows of sector i are sector_offset[i] .. sector_offset[i + 1] - 1,
+  // and the rows of a sector whose active[i] is 0 get y = 0 without their elements
+  const int* active;
+  const long long* sector_offset;
+  int nbr_sectors;
   const void* diag;            // [dim] diagonal, FP64 or FP32 like the factors
   const void* factors;         // [nbr_factors] FP64 or FP32
   long long dim;
   int nbr_factors;
   int chunk;                   // elements read ahead of the gathers: 8 or 16
 };
-int launch_fqhe_row_counts(const FqheDevice& f, int* counts, cudaStream_t s);
+// row_offset: the space's rows sit at row_offset .. row_offset + dim - 1 of a concatenated structure
+// (targets shifted alike)
+int launch_fqhe_row_counts(const FqheDevice& f, int* counts, cudaStream_t s, long long row_offset = 0);
 int launch_fqhe_ell_fill(const FqheDevice& f, const long long* slice_ptr, const int* slice_len, int* cols,
-                         uint16_t* coef, cudaStream_t s);
-int launch_fqhe_diag(const FqheDevice& f, const double* factors64, double* diag64, float* diag32, cudaStream_t s);
+                         uint16_t* coef, cudaStream_t s, long long row_offset = 0);
+int launch_fqhe_diag(const FqheDevice& f, const double* factors64, double* diag64, float* diag32, cudaStream_t s,
+                     long long row_offset = 0);
 int launch_ell_product(const EllDevice& e, const MatvecArgs& a, int precision, cudaStream_t s);
 int launch_long_row_counts(const FqheLongDevice& f, int* counts, cudaStream_t s);
 int launch_long_ell_fill(const FqheLongDevice& f, int nbr_factors, const long long* slice_ptr, const int* slice_len,

@@ -79,7 +79,9 @@ __device__ __forceinline__ void visit_row(const FqheDevice& f, uint64_t s, Visit
   }
 }
 
-__global__ void row_counts_kernel(FqheDevice f, int* counts) {
+// row_offset: the space's rows are rows row_offset .. row_offset + dim - 1 of a larger structure (the
+// concatenated sectors of the batched solver), their targets shifted by it
+__global__ void row_counts_kernel(FqheDevice f, int* counts, long long row_offset) {
   const long long stride = (long long)gridDim.x * blockDim.x;
   const uint64_t full = (f.lz_max >= 63) ? ~0ull : ((1ull << (f.lz_max + 1)) - 1ull);
   for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
@@ -98,35 +100,36 @@ __global__ void row_counts_kernel(FqheDevice f, int* counts) {
         n += __popcll(E & mirror_of(E, M) & (~0ull << (M / 2 + 1)));
       }
     }
-    counts[r] = n;
+    counts[row_offset + r] = n;
   }
 }
 
 __global__ void ell_fill_kernel(FqheDevice f, const long long* slice_ptr, const int* slice_len, int* cols,
-                                uint16_t* coef) {
+                                uint16_t* coef, long long row_offset) {
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
-    const long long sl = r >> 5;
+    const long long g = row_offset + r;
+    const long long sl = g >> 5;
     const long long base = slice_ptr[sl];
     const int len = slice_len[sl];
-    const int lane = (int)(r & 31);
+    const int lane = (int)(g & 31);
     int j = 0;
     visit_row(f, __ldg(f.words + r), [&](int idx, int fidx, bool neg) {
       const long long p = ell_pos(base, lane, j);
-      cols[p] = idx;
+      cols[p] = (int)(row_offset + idx);
       coef[p] = (uint16_t)(fidx | (neg ? 0x8000 : 0));
       ++j;
     });
     for (; j < len; ++j) {  // padding: the row itself times a zero factor
       const long long p = ell_pos(base, lane, j);
-      cols[p] = (int)r;
+      cols[p] = (int)g;
       coef[p] = (uint16_t)f.nbr_factors;
     }
   }
 }
 
 // diagonal of every row: the (m3, m4) = (m1, m2) moves have sign -1, so d = -sum factor(m1, m2, m1)
-__global__ void diag_kernel(FqheDevice f, const double* factors, double* diag64, float* diag32) {
+__global__ void diag_kernel(FqheDevice f, const double* factors, double* diag64, float* diag32, long long row_offset) {
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < f.dim; r += stride) {
     const uint64_t s = __ldg(f.words + r);
@@ -143,9 +146,20 @@ __global__ void diag_kernel(FqheDevice f, const double* factors, double* diag64,
         d -= factors[__ldg(f.pair_offset + (m1 * (m1 - 1) / 2 + m2)) - (M / 2 + 1) + m1];
       }
     }
-    diag64[r] = d;
-    diag32[r] = (float)d;
+    diag64[row_offset + r] = d;
+    diag32[row_offset + r] = (float)d;
   }
+}
+
+// sector of concatenated row r (row_offset ascending, nbr_sectors + 1 entries)
+__device__ __forceinline__ int ell_sector_of(const long long* row_offset, int nbr_sectors, long long r) {
+  int lo = 0, hi = nbr_sectors - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(row_offset + mid) <= r) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
 }
 
 template <typename TG, int K, bool IL, bool W256 = false>
@@ -219,7 +233,10 @@ __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, 
        sl += nwarps) {
     const long long r = sl * 32 + lane;
     if (r >= r_end) continue;  // the last slice's lanes beyond the space hold no elements
-    const int len = e.slice_len[sl];
+    int len = e.slice_len[sl];
+    // concatenated sectors: the rows of an inactive (converged) sector get y = 0 and no elements
+    const bool live = !e.active || __ldg(e.active + ell_sector_of(e.sector_offset, e.nbr_sectors, r)) != 0;
+    if (!__any_sync(__activemask(), live)) len = 0;
     const int4* cg = reinterpret_cast<const int4*>(e.cols + e.slice_ptr[sl]) + lane;
     const KT* kg;
     if constexpr (PK != 0) kg = reinterpret_cast<const uint4*>(e.coef32 + e.slice_ptr[sl]) + lane;
@@ -297,6 +314,7 @@ __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, 
       double v = (double)acc[q];
       const long long xo = IL ? r * K + q : r * a.ld + q * a.vstride;
       if (on_diag && a.shift != 0.0) v += a.shift * (a.xdiag ? a.xdiag[xo] : (double)x[xo]);
+      if (!live) v = 0.0;
       double* yp = y + (IL ? r * K + q : r * a.ld_y + q * a.vstride_y);
       __stcs(yp, a.accumulate ? (__ldcs(yp) + v) : v);
     }
@@ -367,24 +385,25 @@ int launch_ell_k(const EllDevice& e, MatvecArgs a, cudaStream_t s) {
 
 }  // namespace
 
-int launch_fqhe_row_counts(const FqheDevice& f, int* counts, cudaStream_t s) {
+int launch_fqhe_row_counts(const FqheDevice& f, int* counts, cudaStream_t s, long long row_offset) {
   if (f.dim <= 0) return DH_OK;
-  row_counts_kernel<<<grid_for(f.dim), 256, 0, s>>>(f, counts);
+  row_counts_kernel<<<grid_for(f.dim), 256, 0, s>>>(f, counts, row_offset);
   DH_CUDA(cudaGetLastError());
   return DH_OK;
 }
 
 int launch_fqhe_ell_fill(const FqheDevice& f, const long long* slice_ptr, const int* slice_len, int* cols,
-                         uint16_t* coef, cudaStream_t s) {
+                         uint16_t* coef, cudaStream_t s, long long row_offset) {
   if (f.dim <= 0) return DH_OK;
-  ell_fill_kernel<<<grid_for(f.dim), 256, 0, s>>>(f, slice_ptr, slice_len, cols, coef);
+  ell_fill_kernel<<<grid_for(f.dim), 256, 0, s>>>(f, slice_ptr, slice_len, cols, coef, row_offset);
   DH_CUDA(cudaGetLastError());
   return DH_OK;
 }
 
-int launch_fqhe_diag(const FqheDevice& f, const double* factors64, double* diag64, float* diag32, cudaStream_t s) {
+int launch_fqhe_diag(const FqheDevice& f, const double* factors64, double* diag64, float* diag32, cudaStream_t s,
+                     long long row_offset) {
   if (f.dim <= 0) return DH_OK;
-  diag_kernel<<<grid_for(f.dim), 256, 0, s>>>(f, factors64, diag64, diag32);
+  diag_kernel<<<grid_for(f.dim), 256, 0, s>>>(f, factors64, diag64, diag32, row_offset);
   DH_CUDA(cudaGetLastError());
   return DH_OK;
 }

@@ -523,15 +523,23 @@ int dh_complex_vector_read(const char* file_name, double* pairs, int64_t dim);
  * 0 for dense sectors); stats (optional, DH_SECTOR_STATS values): set-up seconds, solve seconds,
  * device time of the block products, number of block products, FP32-phase seconds, refinement
  * seconds, number of sectors restarted in FP64, largest |E_refined - E_FP32| over the sectors,
- * number of sectors diagonalised densely after an exhausted Krylov space, seconds spent on them.
- * The sectors share the split-word rank tables: lz_max <= 40 (DH_ERR_UNSUPPORTED above).  The
- * Krylov blocks the refinement needs are kept in device memory as far as half of the free memory
- * allows (growing with the run), else rebuilt by replaying the recurrence. */
-#define DH_SECTOR_STATS 10
+ * number of sectors diagonalised densely after an exhausted Krylov space, seconds spent on them,
+ * bytes of the stored elements (0: products on the fly), seconds spent building them.
+ * allowed_memory: the reference's --memory (FastMultiplicationMemory / EnableFastMultiplication,
+ * AbstractQHEOnSphereHamiltonian.cc:3625,3814) for the whole batch: 0 computes every product on the
+ * fly; otherwise the Lanczos sectors' elements are stored once as one sliced ELL over their
+ * concatenated rows when they take at most allowed_memory bytes (< 0: no budget) and fit in the free
+ * device memory, and the first phase's products (and the FP64 checks) stream them; the rows of
+ * converged sectors are skipped either way.  The sectors share the split-word rank tables:
+ * lz_max <= 40 (DH_ERR_UNSUPPORTED above).  The Krylov blocks the refinement needs are kept in
+ * device memory as far as half of the free memory allows (growing with the run), else rebuilt by
+ * replaying the recurrence. */
+#define DH_SECTOR_STATS 12
 int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const int* total_lz, int nbr_sectors,
                                   const double* pseudopotentials, int block_size, int max_iter,
                                   double precision_target, int precision, int full_diag_limit,
-                                  uint64_t seed, double* energies, int* iterations, double* stats);
+                                  int64_t allowed_memory, uint64_t seed, double* energies, int* iterations,
+                                  double* stats);
 
 /* ================================================================ setup helpers */
 

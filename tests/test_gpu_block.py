@@ -59,3 +59,25 @@ def test_every_sector_fp32_refined_against_dense(gpu, orc, k):
     for lz, e in zip(sectors, r["energies"]):
         ref = dense_e0(orc, 6, 15, lz, v)
         assert abs(e - ref) < 1e-10 * max(1.0, abs(ref)), (lz, e, ref)
+
+
+@pytest.mark.parametrize("k", [1, 2, 4])
+def test_all_sectors_stored_elements_against_dense(gpu, orc, k):
+    # the batch's stored elements (one ELL over the concatenated sectors, converged sectors skipped):
+    # FP64 and FP32 + refinement, against dense diagonalisation and the on-the-fly batch
+    v = golden("lanczos_n6_2s15_lz0_coulomb_block4.npz")["v"]
+    sectors = list(range(0, 61, 2))
+    r_fly = gpu.fqhe_sectors_block_lanczos(6, 15, sectors, v, block_size=k, max_iter=600, full_diag_limit=16)
+    r64 = gpu.fqhe_sectors_block_lanczos(6, 15, sectors, v, block_size=k, max_iter=600, full_diag_limit=16, memory=-1)
+    r32 = gpu.fqhe_sectors_block_lanczos(6, 15, sectors, v, block_size=k, max_iter=600, fp32=True, precision=1e-13,
+                                         full_diag_limit=16, memory=-1)
+    assert r64["stored_bytes"] > 0 and r32["stored_bytes"] > 0 and r_fly["stored_bytes"] == 0
+    for lz, e_fly, e64, e32 in zip(sectors, r_fly["energies"], r64["energies"], r32["energies"]):
+        ref = dense_e0(orc, 6, 15, lz, v)
+        assert abs(e64 - ref) < 1e-10 * max(1.0, abs(ref)), (lz, e64, ref)
+        assert abs(e32 - ref) < 1e-10 * max(1.0, abs(ref)), (lz, e32, ref)
+        assert abs(e64 - e_fly) < 1e-11 * max(1.0, abs(ref)), (lz, e64, e_fly)
+    # a budget below the structure's size keeps the products on the fly
+    r_small = gpu.fqhe_sectors_block_lanczos(6, 15, sectors, v, block_size=k, max_iter=600, full_diag_limit=16,
+                                             memory=1024)
+    assert r_small["stored_bytes"] == 0

@@ -66,13 +66,16 @@ def test_precision_config_ground_energy(gpu, sector_b):
     H.set_precision("fp64")
 
 
+@pytest.mark.parametrize("memory", [0, -1])
 @pytest.mark.parametrize("fp32", [True, False])
-def test_batching_config_every_sector_against_reference(gpu, fp32):
+def test_batching_config_every_sector_against_reference(gpu, fp32, memory):
+    # memory = -1: the batch's elements stored once (one sliced ELL over the concatenated sectors)
     z = golden("sectors_n10_2s27_block4.npz")
     sectors = [int(s) for s in z["two_lz"]]
     assert len(sectors) == 91 and int(z["dims"].sum()) == 6684779
     r = gpu.fqhe_sectors_block_lanczos(10, 27, sectors, z["v"], block_size=2, max_iter=800, precision=1e-10 if fp32 else 1e-13,
-                                       fp32=fp32, full_diag_limit=200)
+                                       fp32=fp32, full_diag_limit=200, memory=memory)
+    assert (r["stored_bytes"] > 0) == (memory != 0)
     e_ref = z["e0"]
     rel = np.abs(r["energies"] - e_ref) / np.abs(e_ref)
     assert np.max(rel) < 1e-10, (sectors[int(np.argmax(rel))], float(np.max(rel)))
