@@ -686,6 +686,55 @@ int sector_ritz_coefficients(const BlockEngine& e, const BlockSector& b, int nve
   return DH_OK;
 }
 
+// The nvec lowest eigenvectors of a sector's band matrix as coefficients over its blocks
+// (C[r * nvec + c]): the band's eigenvalues (Givens reduction and QL, O(n b^2)), then inverse iteration
+// at each, orthogonalised against the lower ones and checked against T v = lambda v.  A failed check
+// (a nearly degenerate cluster) falls back to the dense eigensolve.
+int sector_lowest_vectors(const BlockEngine& e, const BlockSector& b, int nvec, std::vector<double>& C) {
+  const int n = b.blocks * e.k;
+  const int bw = std::max(1, 2 * e.k - 1);
+  std::vector<double> t;
+  sector_band_matrix(e, b, t);
+  std::vector<double> work(t), eig(n), v(n);
+  bool ok = band_eigenvalues(n, bw, work.data(), eig.data()) == DH_OK;
+  C.assign((size_t)n * nvec, 0.0);
+  for (int c = 0; ok && c < std::min(nvec, n); ++c) {
+    if (band_inverse_iteration(n, bw, t.data(), eig[c], v.data()) != DH_OK) {
+      ok = false;
+      break;
+    }
+    for (int p = 0; p < c; ++p) {
+      double d = 0.0;
+      for (int i = 0; i < n; ++i) d += v[i] * C[(size_t)i * nvec + p];
+      for (int i = 0; i < n; ++i) v[i] -= d * C[(size_t)i * nvec + p];
+    }
+    double nrm = 0.0;
+    for (int i = 0; i < n; ++i) nrm += v[i] * v[i];
+    nrm = sqrt(nrm);
+    if (!(nrm > 1e-8)) {
+      ok = false;
+      break;
+    }
+    double res = 0.0;
+    for (int i = 0; i < n; ++i) {
+      v[i] /= nrm;
+    }
+    for (int i = 0; i < n; ++i) {
+      double r = -eig[c] * v[i];
+      for (int j = std::max(0, i - bw); j <= std::min(n - 1, i + bw); ++j) r += t[(size_t)i * n + j] * v[j];
+      res += r * r;
+    }
+    if (!(res <= 1e-20 * std::max(1.0, eig[c] * eig[c]))) {
+      ok = false;
+      break;
+    }
+    for (int i = 0; i < n; ++i) C[(size_t)i * nvec + c] = v[i];
+  }
+  if (ok) return DH_OK;
+  std::vector<double> vals;
+  return sector_ritz_coefficients(e, b, nvec, C, vals);
+}
+
 // out = the k lowest Ritz vectors of every sector (k-interleaved like the blocks): from the stored
 // blocks when they were kept, otherwise by replaying the recorded steps from the start block.
 // After a replay the engine's work vectors hold the replayed state.
@@ -699,8 +748,8 @@ int engine_ritz(BlockEngine& e, double* out) {
   for (int s = 0; s < e.nsec; ++s) {
     const BlockSector& b = e.sec[s];
     if (b.blocks == 0) continue;
-    std::vector<double> cs, vals;
-    int rc = sector_ritz_coefficients(e, b, k, cs, vals);
+    std::vector<double> cs;
+    int rc = sector_lowest_vectors(e, b, k, cs);
     if (rc != DH_OK) return rc;
     std::copy(cs.begin(), cs.end(), C.begin() + (size_t)s * nb * kk);
   }
