@@ -80,6 +80,9 @@ struct BlockEngine {
   bool have_prev = false;
   std::vector<BlockSector> sec;
   std::function<int(const double*, const float*, double*)> product;
+  // the per-step bookkeeping needs only the lowest nev + 1 Ritz values (the batched sectors): for
+  // k = 1 they come from bisection on the tridiagonal matrix instead of all of its eigenvalues
+  bool lowest_only = false;
   double product_ms = 0.0;
   long long products = 0;
   long long fp64_products = 0;
@@ -820,7 +823,16 @@ int engine_ritz(BlockEngine& e, double* out) {
 // (:731): first evaluation sets previous = 2 * lambda, later ones the previous lambda
 int sector_evaluate(const BlockEngine& e, BlockSector& b) {
   std::vector<double> eig;
-  int rc = sector_eigenvalues(e, b, eig);
+  int rc;
+  if (e.lowest_only && e.k == 1) {
+    const int m = b.blocks;
+    std::vector<double> off(std::max(m - 1, 0));
+    for (int j = 0; j + 1 < m; ++j) off[j] = b.B[j + 1];
+    eig.assign(std::min(m, e.nev + 1), 0.0);
+    rc = tridiagonal_lowest(m, b.A.data(), off.data(), (int)eig.size(), eig.data());
+  } else {
+    rc = sector_eigenvalues(e, b, eig);
+  }
   if (rc != DH_OK) return rc;
   const int nev = std::min(e.nev, (int)eig.size());
   if (b.prev_last != 0.0 && !b.ritz.empty())
@@ -1503,6 +1515,7 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
   double ell_seconds = 0.0;
   e.k = block_size;
   e.nev = 1;
+  e.lowest_only = true;
   e.precision = precision;
   e.eig_precision = precision_target > 0.0 ? precision_target : 1e-14;
   e.max_iter = max_iter;
@@ -1652,6 +1665,7 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
         auto f = std::make_unique<BlockEngine>();
         f->k = k;
         f->nev = 1;
+        f->lowest_only = true;
         f->precision = fp64_round ? DH_PRECISION_FP64 : DH_PRECISION_FP32;
         f->eig_precision = precision_target > 0.0 ? precision_target : 1e-14;
         f->residual_target = restart_residual_target(f->eig_precision);

@@ -75,6 +75,9 @@ double l2_constant(int total_lz);
 // Symmetric tridiagonal eigenvalues (ascending) by implicit QL; optional eigenvectors
 // (column-major n x n) when z != nullptr.
 int tridiagonal_eigen(int n, const double* diag, const double* off, double* eig, double* z);
+// the m lowest eigenvalues (ascending) of the same tridiagonal matrix by bisection on Sturm counts
+// (O(n) per count, about 60 counts per eigenvalue)
+int tridiagonal_lowest(int n, const double* diag, const double* off, int m, double* eig);
 // Dense symmetric eigen-decomposition (row-major a, destroyed), eigenvalues ascending, optional
 // eigenvectors (columns of z, row-major n x n).
 int symmetric_eigen(int n, double* a, double* eig, double* z);

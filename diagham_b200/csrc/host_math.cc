@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <limits>
 #include <cmath>
 #include <mutex>
 #include <numeric>
@@ -456,6 +457,49 @@ int tridiagonal_eigen(int n, const double* diag, const double* off, double* eig,
     std::vector<double> tmp((size_t)n * n);
     for (int i = 0; i < n; ++i) memcpy(&tmp[(size_t)i * n], z + (size_t)order[i] * n, sizeof(double) * n);
     memcpy(z, tmp.data(), sizeof(double) * n * n);
+  }
+  return DH_OK;
+}
+
+// Bisection on the Sturm sequence: the number of eigenvalues below x is the number of negative
+// pivots of the LDL^T factorisation of T - x (q_0 = d_0 - x, q_i = d_i - x - e_{i-1}^2 / q_{i-1}),
+// started from the Gershgorin interval and halved until it is a few ulps wide.
+int tridiagonal_lowest(int n, const double* diag, const double* off, int m, double* eig) {
+  if (n <= 0 || m <= 0) return DH_OK;
+  m = std::min(m, n);
+  double lo = diag[0], hi = diag[0], scale = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double r = (i > 0 ? fabs(off[i - 1]) : 0.0) + (i + 1 < n ? fabs(off[i]) : 0.0);
+    lo = std::min(lo, diag[i] - r);
+    hi = std::max(hi, diag[i] + r);
+    scale = std::max(scale, fabs(diag[i]) + r);
+  }
+  const double tiny = std::numeric_limits<double>::min() / std::numeric_limits<double>::epsilon();
+  auto below = [&](double x) {
+    int c = 0;
+    double q = diag[0] - x;
+    if (q < 0.0) ++c;
+    for (int i = 1; i < n; ++i) {
+      if (fabs(q) < tiny) q = (q < 0.0) ? -tiny : tiny;
+      q = diag[i] - x - off[i - 1] * off[i - 1] / q;
+      if (q < 0.0) ++c;
+    }
+    return c;
+  };
+  const double tol = 4.0 * std::numeric_limits<double>::epsilon() * std::max(scale, tiny);
+  double left = lo - tol;
+  for (int j = 0; j < m; ++j) {
+    double a = left, b = hi + tol;
+    // eigenvalue j: the smallest x with more than j eigenvalues below it
+    for (int it = 0; it < 200 && b - a > tol; ++it) {
+      const double mid = 0.5 * (a + b);
+      if (below(mid) > j)
+        b = mid;
+      else
+        a = mid;
+    }
+    eig[j] = 0.5 * (a + b);
+    left = a;  // the next eigenvalue is not below this one
   }
   return DH_OK;
 }
