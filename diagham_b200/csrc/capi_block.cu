@@ -1630,6 +1630,7 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
       for (int i = 0; i < ns; ++i) src_pos[i] = i;
       std::unique_ptr<BlockEngine> cur;
       std::unique_ptr<SectorProduct> cur_prod;
+      std::unique_ptr<SectorEll> cur_ell;  // the restarted sectors' stored elements (a stored batch)
       DevBuf R;
       for (int round = 0; !pending.empty(); ++round) {
         if ((rc = ensure_buffer(R, (size_t)src->total * k * sizeof(double))) != DH_OK) return rc;
@@ -1684,6 +1685,15 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
                                   (size_t)rdims[jj] * k * sizeof(double), cudaMemcpyDeviceToDevice, f->stream));
         auto fprod = std::make_unique<SectorProduct>();
         if ((rc = bind_sector_product(hb, rsec, *f, *fprod)) != DH_OK) return rc;
+        std::unique_ptr<SectorEll> fell;
+        if (ell_bytes > 0) {
+          // a stored batch stores the restarted sectors too (their rows at the restart's offsets)
+          fell = std::make_unique<SectorEll>();
+          bool built = false;
+          size_t need = 0;
+          if ((rc = build_sector_ell(hb, rsec, *f, allowed_memory, *fell, &built, &need)) != DH_OK) return rc;
+          if (built) bind_sector_ell(hb, *fell, *f);
+        }
         if ((rc = engine_mixed_restart(*f, seed + 1000 + round, fp64_round)) != DH_OK) return rc;
         if ((rc = engine_solve(*f)) != DH_OK) return rc;
         for (size_t jj = 0; jj < redo.size(); ++jj) {
@@ -1694,7 +1704,9 @@ extern "C" int dh_fqhe_sectors_block_lanczos(int nbr_fermions, int lz_max, const
         pending.clear();
         for (int i : redo)
           if (!need_dense[i]) pending.push_back(i);
+        cur = nullptr;  // the previous round's engine goes before the bindings it used
         cur_prod = std::move(fprod);  // the product binding must outlive the engine using it
+        cur_ell = std::move(fell);
         cur = std::move(f);
         src = cur.get();
       }

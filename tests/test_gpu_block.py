@@ -81,3 +81,14 @@ def test_all_sectors_stored_elements_against_dense(gpu, orc, k):
     r_small = gpu.fqhe_sectors_block_lanczos(6, 15, sectors, v, block_size=k, max_iter=600, full_diag_limit=16,
                                              memory=1024)
     assert r_small["stored_bytes"] == 0
+
+
+def test_fp32_refined_restarts_from_stored_elements(gpu, orc):
+    # a stored batch restarts the sectors it could not certify from stored elements of their own
+    v = golden("lanczos_n8_2s21_lz0_coulomb_basic.npz")["v"]
+    sectors = [0, 2, 4, 6]
+    r64 = gpu.fqhe_sectors_block_lanczos(8, 21, sectors, v, block_size=4, max_iter=800)
+    r32 = gpu.fqhe_sectors_block_lanczos(8, 21, sectors, v, block_size=4, max_iter=800, fp32=True, precision=1e-12,
+                                         memory=-1)
+    assert r32["stored_bytes"] > 0 and r32["refined_sectors"] >= 1
+    assert np.max(np.abs(r32["energies"] - r64["energies"]) / np.abs(r64["energies"])) < 1e-10, (r32, r64)
