@@ -5,6 +5,8 @@
 * Hellmann-Feynman gradients of E0 and of the neutral gap for N = 10, 2S = 27, Lz = 0 and 1
   (Coulomb + uniform noise from seed 2) against the reference's FP64 gradient
   <psi_ref|H_m|psi_ref> and against central finite differences of the GPU E0 (h = 1e-6).
+* The same VJP on BosonOnSphereShort and FermionOnSphereLong, and a bosonic Hellmann-Feynman
+  gradient against central differences.
 Tolerances: gradcheck at its FP64 defaults; energies 1e-10 relative; gradients against the reference
 1e-7 absolute (both sides carry Lanczos eigenvector errors, first order in a Hellmann-Feynman
 gradient); finite differences 2e-6 absolute (E0 converged to 1e-14 relative over 2h = 2e-6)."""
@@ -104,3 +106,46 @@ def test_gradients_against_central_differences(gpu, config_d):
             fd.append((ep - em) / (2 * h))
         err = np.abs(np.array(fd) - V.grad.numpy()[odd])
         assert np.max(err) < 2e-6, (err, fd)
+
+
+@pytest.mark.parametrize("space", ["boson", "long"])
+def test_product_gradcheck_bosons_and_128_bit_words(gpu, space):
+    # the same VJP on BosonOnSphereShort (its bosonic adjoint) and on the 128-bit fermion engine
+    from diagham_b200.autograd import hamiltonian_product
+    if space == "boson":
+        n, s, lz = 5, 9, 1
+        v0 = gpu.coulomb_pseudopotentials(s)
+        v0[1::2] = 0.0
+        sp = gpu.BosonOnSphereShort(n, lz, s)
+    else:
+        n, s, lz = 3, 63, 1
+        v0 = gpu.coulomb_pseudopotentials(s)
+        sp = gpu.FermionOnSphereLong(n, lz, s)
+    H = gpu.ParticleOnSphereGenericHamiltonian(sp, n, s, v0)
+    V = torch.tensor(v0, dtype=torch.float64, requires_grad=True)
+    g = torch.Generator(device="cuda").manual_seed(4)
+    x = torch.rand(sp.dim, 2, dtype=torch.float64, device="cuda", generator=g).requires_grad_(True)
+    assert torch.autograd.gradcheck(lambda V_, x_: hamiltonian_product(V_, x_, H), (V, x), eps=1e-6, atol=1e-8,
+                                    rtol=1e-6)
+
+
+def test_boson_ground_state_gradient_against_central_differences(gpu):
+    # Hellmann-Feynman dE0/dV_m of BosonOnSphereShort N = 8, 2S = 14 (even m enter the bosonic factors)
+    from diagham_b200.autograd import ground_state_energy
+    z = golden("boson_n8_2s14_lz0_coulomb.npz")
+    v = np.array(z["v"])
+    sp = gpu.BosonOnSphereShort(8, 0, 14)
+    H = gpu.ParticleOnSphereGenericHamiltonian(sp, 8, 14, v)
+    V = torch.tensor(v, dtype=torch.float64, requires_grad=True)
+    e0 = ground_state_energy(V, H)
+    assert abs(float(e0.detach()) - float(z["eigenvalues"][0])) <= 1e-10 * abs(float(z["eigenvalues"][0]))
+    e0.backward()
+    g = V.grad.numpy()
+    h = 1e-6
+    for m in (0, 2, 4):
+        vp, vm = v.copy(), v.copy()
+        vp[m] += h
+        vm[m] -= h
+        fd = (float(ground_state_energy(torch.tensor(vp), H)) - float(ground_state_energy(torch.tensor(vm), H))) / (2 * h)
+        assert abs(fd - g[m]) < 2e-6, (m, fd, g[m])
+    assert np.all(g[1::2] == 0.0)  # odd m never enter a bosonic factor
