@@ -825,11 +825,14 @@ int sector_evaluate(const BlockEngine& e, BlockSector& b) {
   std::vector<double> eig;
   int rc;
   if (e.lowest_only && e.k == 1) {
+    // the lowest Ritz value only: Newton from the previous one (an upper bound by interlacing), or
+    // bisection the first time
     const int m = b.blocks;
     std::vector<double> off(std::max(m - 1, 0));
     for (int j = 0; j + 1 < m; ++j) off[j] = b.B[j + 1];
-    eig.assign(std::min(m, e.nev + 1), 0.0);
-    rc = tridiagonal_lowest(m, b.A.data(), off.data(), (int)eig.size(), eig.data());
+    eig.assign(1, 0.0);
+    rc = b.ritz.empty() ? tridiagonal_lowest(m, b.A.data(), off.data(), 1, eig.data())
+                        : tridiagonal_lowest_below(m, b.A.data(), off.data(), b.ritz[0], eig.data());
   } else {
     rc = sector_eigenvalues(e, b, eig);
   }
@@ -877,7 +880,9 @@ int sector_evaluate(const BlockEngine& e, BlockSector& b) {
     if (e.stop_on_stagnation && fabs(l0 - b.prev_last) < 1e-13 * fabs(l0)) b.converged = true;
     return DH_OK;
   }
-  if ((int)b.ritz.size() > e.nev) {
+  // the test needs more Ritz values than wanted ones (rows beyond nev); the lowest-only form keeps
+  // just the wanted one and counts the rows instead
+  if ((e.lowest_only && e.k == 1) ? b.blocks > e.nev : (int)b.ritz.size() > e.nev) {
     const double l = b.ritz[e.nev - 1];
     if (fabs(l - b.prev_last) < e.eig_precision * fabs(l)) b.converged = true;
   }
@@ -914,9 +919,12 @@ int engine_solve(BlockEngine& e) {
         eval.push_back(s);
       }
     }
-    // band eigenvalues of the sectors due, spread over host threads
+    // band eigenvalues of the sectors due, spread over host threads (a few microseconds per sector
+    // with the lowest-only Newton steps of k = 1: then on this thread)
     std::vector<int> status(eval.size(), DH_OK);
-    const int nthreads = std::max(1, std::min((int)eval.size(), (int)std::thread::hardware_concurrency()));
+    const int nthreads = (e.lowest_only && e.k == 1)
+                             ? 1
+                             : std::max(1, std::min((int)eval.size(), (int)std::thread::hardware_concurrency()));
     if (nthreads == 1) {
       for (size_t i = 0; i < eval.size(); ++i) status[i] = sector_evaluate(e, e.sec[eval[i]]);
     } else {

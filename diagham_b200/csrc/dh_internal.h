@@ -78,6 +78,9 @@ int tridiagonal_eigen(int n, const double* diag, const double* off, double* eig,
 // the m lowest eigenvalues (ascending) of the same tridiagonal matrix by bisection on Sturm counts
 // (O(n) per count, about 60 counts per eigenvalue)
 int tridiagonal_lowest(int n, const double* diag, const double* off, int m, double* eig);
+// the lowest eigenvalue of the same matrix when an upper bound is known (the previous lowest Ritz
+// value of a growing Lanczos matrix): safeguarded Newton on the pivots, a few O(n) passes
+int tridiagonal_lowest_below(int n, const double* diag, const double* off, double above, double* eig0);
 // Dense symmetric eigen-decomposition (row-major a, destroyed), eigenvalues ascending, optional
 // eigenvectors (columns of z, row-major n x n).
 int symmetric_eigen(int n, double* a, double* eig, double* z);

@@ -504,6 +504,75 @@ int tridiagonal_lowest(int n, const double* diag, const double* off, int m, doub
   return DH_OK;
 }
 
+// The lowest eigenvalue of the tridiagonal matrix given an upper bound `above` (the lowest eigenvalue
+// of its leading (n - 1) x (n - 1) block: by interlacing the new one is not above it).  Newton steps on
+// det(T - x) from the pivots q_k of T - x (q_0 = d_0 - x, q_k = d_k - x - e_{k-1}^2 / q_{k-1}; the
+// logarithmic derivative is sum_k q_k' / q_k), kept inside a bracket that the Sturm counts (the
+// number of negative pivots = eigenvalues below x) shrink; a step that leaves the bracket bisects.
+int tridiagonal_lowest_below(int n, const double* diag, const double* off, double above, double* eig0) {
+  if (n <= 0) return DH_OK;
+  double lo = diag[0], scale = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double r = (i > 0 ? fabs(off[i - 1]) : 0.0) + (i + 1 < n ? fabs(off[i]) : 0.0);
+    lo = std::min(lo, diag[i] - r);
+    scale = std::max(scale, fabs(diag[i]) + r);
+  }
+  const double tiny = std::numeric_limits<double>::min() / std::numeric_limits<double>::epsilon();
+  const double tol = 4.0 * std::numeric_limits<double>::epsilon() * std::max(scale, tiny);
+  // pivots at x: the Sturm count and the Newton step -det / det'
+  auto eval = [&](double x, int& below, double& step) {
+    below = 0;
+    double q = diag[0] - x, dq = -1.0, sum = 0.0;
+    for (int i = 0;; ++i) {
+      if (fabs(q) < tiny) q = (q < 0.0) ? -tiny : tiny;
+      if (q < 0.0) ++below;
+      sum += dq / q;
+      if (i + 1 == n) break;
+      const double e2 = off[i] * off[i];
+      const double qn = diag[i + 1] - x - e2 / q;
+      dq = -1.0 + e2 * dq / (q * q);
+      q = qn;
+    }
+    step = (sum != 0.0) ? -1.0 / sum : 0.0;
+  };
+  double hi = std::max(above, lo) + tol;
+  int c = 0;
+  double step = 0.0;
+  eval(hi, c, step);
+  if (c == 0) {  // nothing below the bound: the eigenvalue is the bound (to rounding)
+    *eig0 = above;
+    return DH_OK;
+  }
+  lo -= tol;
+  double x = hi;
+  for (int it = 0; it < 200 && hi - lo > tol; ++it) {
+    double nx = x + step;
+    if (!(nx > lo && nx < hi)) nx = 0.5 * (lo + hi);
+    x = nx;
+    eval(x, c, step);
+    if (c >= 1)
+      hi = x;
+    else
+      lo = x;
+    if (fabs(step) <= tol) {
+      // a root: the lowest one only if nothing lies below it (Newton may have found the next one,
+      // which can sit at the top of the bracket), else the bracket drops below it and bisects on
+      const double root = x + step;
+      int below = 0;
+      double unused = 0.0;
+      eval(root - tol, below, unused);
+      if (below == 0) {
+        *eig0 = root;
+        return DH_OK;
+      }
+      hi = std::min(hi, root - tol);
+      step = hi - lo;  // outside the bracket: the next point is its midpoint
+    }
+  }
+  *eig0 = 0.5 * (lo + hi);
+  return DH_OK;
+}
+
 // Householder reduction of a dense symmetric matrix to tridiagonal form, then implicit QL.
 // a (row-major n x n) is overwritten; z (row-major, columns = eigenvectors) optional.
 int symmetric_eigen(int n, double* a, double* eig, double* z) {
