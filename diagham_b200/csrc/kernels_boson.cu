@@ -219,10 +219,11 @@ __global__ void __launch_bounds__(kBosonThreads) boson_matvec_kernel(FqheDevice 
         for (int j = 0; j < K; ++j) {
           double v = (double)acc[j];
           if (diag && a.shift != 0.0) {
-            const double xd = a.xdiag ? a.xdiag[r * a.ld + j * a.vstride] : (double)x[r * a.ld + j * a.vstride];
+            const long long xo = IL ? r * K + j : r * a.ld + j * a.vstride;
+            const double xd = a.xdiag ? a.xdiag[xo] : (double)x[xo];
             v += a.shift * xd;
           }
-          double* yp = y + r * a.ld_y + j * a.vstride_y;
+          double* yp = y + (IL ? r * K + j : r * a.ld_y + j * a.vstride_y);
           *yp = a.accumulate ? (*yp + v) : v;
         }
         r += stride;
@@ -307,7 +308,10 @@ int launch_rank(const FqheDevice& f, const MatvecArgs& a, cudaStream_t s) {
   if (RM == 1) smem += 2 * (size_t)(f.nbr_particles + 1) * kBosonThreads * sizeof(int);
   smem += ((size_t)f.nbr_particles * (f.nbr_particles - 1) + 2) * sizeof(TG);  // occupation square roots
   const bool range = a.col_first > 0 || a.col_last < f.dim;
-  const bool il = (K > 1) && a.ld == K && a.vstride == 1 && il_rows_aligned(a, K, sizeof(TG));
+  // row-interleaved blocks, or one contiguous vector: row strides known at compile time
+  const bool il = K == 1 ? (a.ld == 1 && a.ld_y == 1)
+                         : (a.ld == K && a.vstride == 1 && a.ld_y == K && a.vstride_y == 1 &&
+                            il_rows_aligned(a, K, sizeof(TG)));
   auto kernel = range ? (il ? boson_matvec_kernel<TG, K, true, true, RM> : boson_matvec_kernel<TG, K, true, false, RM>)
                       : (il ? boson_matvec_kernel<TG, K, false, true, RM> : boson_matvec_kernel<TG, K, false, false, RM>);
   if (smem > 48 * 1024) DH_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

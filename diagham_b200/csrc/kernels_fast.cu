@@ -180,9 +180,9 @@ __device__ __forceinline__ void gather(const TG* x, const MatvecArgs& a, long lo
       v[j + 1] = q.y;
     }
   } else {
-    const TG* p = x + idx * a.ld;
+    const TG* p = x + idx * (IL ? K : a.ld);
 #pragma unroll
-    for (int q = 0; q < K; ++q) v[q] = __ldg(p + q * a.vstride);
+    for (int q = 0; q < K; ++q) v[q] = __ldg(p + q * (IL ? 1 : a.vstride));
   }
 }
 
@@ -365,6 +365,10 @@ int launch_ell_k(const EllDevice& e, MatvecArgs a, cudaStream_t s) {
   if ((nv == 2 || nv == 4) && a.ld == nv && a.vstride == 1 && a.ld_y == nv && a.vstride_y == 1 &&
       il_rows_aligned(a, nv, sizeof(TG)))
     return nv == 4 ? launch_ell_typed<TG, 4, true>(e, a, s) : launch_ell_typed<TG, 2, true>(e, a, s);
+  // one contiguous vector of 128-bit-engine elements: row strides known at compile time (FP64 at
+  // N = 6, 2S = 63: 0.409 ms against 0.479 ms; the 16-bit payloads gain nothing from it, and FP32 at
+  // N = 11, 2S = 30 takes 0.448 ms against 0.443 ms, so they keep the strided form)
+  if (nv == 1 && a.ld == 1 && a.ld_y == 1 && e.payload == 2) return launch_ell_typed<TG, 1, true>(e, a, s);
   // separate or strided vectors: groups of 4, 2 and 1 sharing one pass over the elements
   int left = nv, done = 0;
   while (left > 0) {

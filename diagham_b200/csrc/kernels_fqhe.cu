@@ -567,6 +567,9 @@ int launch_one(const FqheDevice& f, const MatvecArgs& a, cudaStream_t s) {
             if constexpr (sizeof(TG) == 8 && K == 4)
               if ((reinterpret_cast<uintptr_t>(a.x) & 31) == 0) kern = split_form_kernel<TG, K, true, true>(form);
           }
+        } else if (a.ld == 1 && a.ld_y == 1) {
+          // one contiguous vector: the same form with the row stride known at compile time
+          kern = split_form_kernel<TG, K, true, false>(form);
         }
         threads = kSplitForms[form].threads;
       }

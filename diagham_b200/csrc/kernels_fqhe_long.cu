@@ -524,7 +524,10 @@ int grid_for(long long rows) {
 template <typename W, typename TG, int K, bool PREFIX>
 int launch_prefix(const FqheLongDevice& f, const MatvecArgs& a, cudaStream_t s) {
   const bool range = a.col_first > 0 || a.col_last < f.dim;
-  const bool il = (K > 1) && a.ld == K && a.vstride == 1 && il_rows_aligned(a, K, sizeof(TG));
+  // row-interleaved blocks, or one contiguous vector: row strides known at compile time
+  const bool il = K == 1 ? (a.ld == 1 && a.ld_y == 1)
+                         : (a.ld == K && a.vstride == 1 && a.ld_y == K && a.vstride_y == 1 &&
+                            il_rows_aligned(a, K, sizeof(TG)));
   auto kernel = range ? (il ? long_matvec_kernel<W, TG, K, true, true, PREFIX>
                             : long_matvec_kernel<W, TG, K, true, false, PREFIX>)
                       : (il ? long_matvec_kernel<W, TG, K, false, true, PREFIX>

@@ -49,9 +49,9 @@ __device__ __forceinline__ void spin_gather(const TG* x, const MatvecArgs& a, lo
       v[j + 1] = q.y;
     }
   } else {
-    const TG* p = x + idx * a.ld;
+    const TG* p = x + idx * (IL ? K : a.ld);
 #pragma unroll
-    for (int q = 0; q < K; ++q) v[q] = __ldg(p + q * a.vstride);
+    for (int q = 0; q < K; ++q) v[q] = __ldg(p + q * (IL ? 1 : a.vstride));
   }
 }
 
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(kSpinThreads) spin_j1j2_kernel(SpinDevice sp, 
     } else {
 #pragma unroll
       for (int q = 0; q < K; ++q) {
-        double* yp = y + r * a.ld_y + q * a.vstride_y;
+        double* yp = y + (IL ? (long long)r * K + q : r * a.ld_y + q * a.vstride_y);
         *yp = a.accumulate ? (*yp + out[q]) : out[q];
       }
     }
@@ -283,10 +283,13 @@ int launch_spin_typed(const SpinDevice& sp, MatvecArgs a, cudaStream_t s) {
     return DH_OK;
   }
   const int nv = a.nbr_vectors;
-  if ((nv == 2 || nv == 4) && a.ld == nv && a.vstride == 1 && a.ld_y == nv && a.vstride_y == 1 &&
-      il_rows_aligned(a, nv, sizeof(TG))) {
-    // row-interleaved block: one launch with vector gathers and stores
-    auto kern = (nv == 4) ? spin_j1j2_kernel<TG, 4, true> : spin_j1j2_kernel<TG, 2, true>;
+  const bool one = nv == 1 && a.ld == 1 && a.ld_y == 1;
+  if (one || ((nv == 2 || nv == 4) && a.ld == nv && a.vstride == 1 && a.ld_y == nv && a.vstride_y == 1 &&
+              il_rows_aligned(a, nv, sizeof(TG)))) {
+    // row-interleaved block (or one contiguous vector): one launch with the row strides known at
+    // compile time, vector gathers and stores
+    auto kern = one ? spin_j1j2_kernel<TG, 1, true>
+                    : ((nv == 4) ? spin_j1j2_kernel<TG, 4, true> : spin_j1j2_kernel<TG, 2, true>);
     int per_sm = 0;
     DH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSpinThreads, 0));
     long long grid = (long long)sms * (per_sm > 0 ? per_sm : 1);
