@@ -195,6 +195,35 @@ __device__ __forceinline__ void gather(const TG* x, const MatvecArgs& a, long lo
 // PK (payload kind): 0 uint16 index | sign << 15, factors in shared memory; 1 (bosons) uint32 payloads
 // (16-byte groups of 4, like the targets) with the occupation square roots; 2 uint32 index | sign << 31,
 // factors read through the cache
+// The element stream is read once: evict-first in L2 and not allocated in L1, which both keep the
+// gathered x.
+__device__ __forceinline__ uint64_t stream_policy() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ int4 ld_stream(const int4* a, uint64_t pol) {
+  int4 v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint4 ld_stream(const uint4* a, uint64_t pol) {
+  uint4 v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint2 ld_stream(const uint2* a, uint64_t pol) {
+  uint2 v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;"
+               : "=r"(v.x), "=r"(v.y)
+               : "l"(a), "l"(pol));
+  return v;
+}
+
 template <typename TG>
 __device__ __forceinline__ TG occupation_sqrt(int v);
 template <>
@@ -223,6 +252,7 @@ __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, 
   const TG* x = static_cast<const TG*>(a.x);
   const TG* diag = static_cast<const TG*>(e.diag);
   const int lane = threadIdx.x & 31;
+  const uint64_t pol = stream_policy();
   static_assert(kEllPad % CH == 0 && CH % kEllGroup == 0, "chunks must tile the padded rows");
   constexpr int NG = CH / kEllGroup;  // 16-byte target groups per chunk
   // a row range starts on a slice boundary (callers split at multiples of 32 rows)
@@ -249,8 +279,8 @@ __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, 
     if (len > 0) {
 #pragma unroll
       for (int g = 0; g < NG; ++g) {
-        c[g] = __ldcs(cg + g * 32);
-        k[g] = __ldcs(kg + g * 32);
+        c[g] = ld_stream(cg + g * 32, pol);
+        k[g] = ld_stream(kg + g * 32, pol);
       }
     }
     for (int j = 0; j < len; j += CH) {
@@ -261,8 +291,8 @@ __global__ void __launch_bounds__(kFastThreads) ell_product_kernel(EllDevice e, 
         const int gn = (j + CH) / kEllGroup;
 #pragma unroll
         for (int g = 0; g < NG; ++g) {
-          cn[g] = __ldcs(cg + (gn + g) * 32);
-          kn[g] = __ldcs(kg + (gn + g) * 32);
+          cn[g] = ld_stream(cg + (gn + g) * 32, pol);
+          kn[g] = ld_stream(kg + (gn + g) * 32, pol);
         }
       }
 #pragma unroll
