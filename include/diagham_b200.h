@@ -337,10 +337,10 @@ int dh_hamiltonian_count_diagonal_elements(dh_hamiltonian_t h, int64_t* total);
  * device looks up the array's device address (cudaGetSymbolAddress with that device current).
  * The device that was current when the Hamiltonian's space was created must be current for the
  * call (DH_ERR_STATE otherwise).  The call is synchronous: it waits on the handle's stream and
- * returns with the result written to out.  All calls share the one array; a process-wide mutex
- * serialises them (on every GPU), so calls never overlap on it; calls that overlapped on the GPU
- * would race.  Each call overwrites what it uses, so the contents left by a previous call do not
- * matter. */
+ * returns with the result written to out.  All calls of a process share its one array; a
+ * process-wide mutex serialises them (on every GPU), so calls never overlap on it, and every
+ * process has an array of its own.  Each call overwrites what it uses, so the contents left by a
+ * previous call do not matter. */
 #define DH_STATIC_ADJOINT_BLOCKS 148
 #define DH_STATIC_ADJOINT_MAX_FACTORS 6400
 int dh_hamiltonian_pseudopotential_adjoint_static(dh_hamiltonian_t h, const double* u, const double* v, double* out);
