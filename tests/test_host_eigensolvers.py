@@ -11,6 +11,7 @@ here by their exported Itanium C++ ABI symbol names; no GPU is involved.
 - tridiagonal_lowest_below: the lowest eigenvalue of T_k given that of its leading block T_{k-1}
   (an upper bound by interlacing), by safeguarded Newton steps; the batched engine's per-step
   convergence test at block size 1.
+- symmetric_eigen: Householder tridiagonalisation then QL, the dense fallback of the refinement.
 - band_eigenvalues / band_inverse_iteration: the block Lanczos band matrix's eigenvalues and the
   Ritz vector of the lowest one.
 """
@@ -26,6 +27,7 @@ SYMBOLS = {
     "tridiagonal_lowest": ("_ZN2dh18tridiagonal_lowestEiPKdS1_iPd", [ctypes.c_int, D, D, ctypes.c_int, D]),
     "tridiagonal_lowest_below": ("_ZN2dh24tridiagonal_lowest_belowEiPKdS1_dPd",
                                  [ctypes.c_int, D, D, ctypes.c_double, D]),
+    "symmetric_eigen": ("_ZN2dh15symmetric_eigenEiPdS0_S0_", [ctypes.c_int, D, D, D]),
     "band_eigenvalues": ("_ZN2dh16band_eigenvaluesEiiPdS0_", [ctypes.c_int, ctypes.c_int, D, D]),
     "band_inverse_iteration": ("_ZN2dh22band_inverse_iterationEiiPKddPd",
                                [ctypes.c_int, ctypes.c_int, D, ctypes.c_double, D]),
@@ -158,3 +160,23 @@ def test_band_eigenvalues_and_ritz_vector(solvers, n, b):
     assert np.linalg.norm(a @ vec - ref_vals[0] * vec) < 1e-9 * scale
     if n > 1 and ref_vals[1] - ref_vals[0] > 1e-6 * scale:
         assert abs(abs(vec @ ref_vecs[:, 0]) - 1.0) < 1e-9
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 8, 33, 100])
+def test_symmetric_eigen(solvers, n):
+    rng = np.random.default_rng(300 + n)
+    m = rng.normal(size=(n, n))
+    a = m + m.T
+    if n >= 8:
+        a[:, 3] = a[3, :] = 0.0  # a zero column: a Householder step with nothing to reflect
+        a[3, 3] = 0.5
+    ref = np.linalg.eigvalsh(a)
+    work = np.ascontiguousarray(a.copy())
+    eig = np.zeros(n)
+    z = np.zeros((n, n))
+    assert solvers["symmetric_eigen"](n, ptr(work), ptr(eig), ptr(z)) == 0
+    scale = np.max(np.abs(ref)) + 1.0
+    assert np.max(np.abs(eig - ref)) < 1e-11 * scale
+    # z row-major with the eigenvectors in its columns
+    assert np.max(np.abs(z.T @ z - np.eye(n))) < 1e-11
+    assert np.max(np.abs(a @ z - z * eig)) < 1e-10 * scale
