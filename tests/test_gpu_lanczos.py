@@ -45,6 +45,29 @@ def test_solve_graph_batches_match_run_loop(gpu, orc, batch):
     assert abs(r["iterations"] - int(z["iterations"])) <= 2
 
 
+@pytest.mark.parametrize("tag,precision", [("n8_2s21_lz0_coulomb", 1e-10), ("n8_2s21_lz0_coulomb", 1e-13),
+                                           ("n7_2s18_lz2_coulomb", 1e-12)])
+def test_graph_batches_stop_near_convergence(gpu, orc, tag, precision):
+    """Graph batches sized by the predicted convergence: the per-iteration run's energy and iteration
+    count, with no more products than batches of 16 would take (3 + 16 per batch) and at most eight
+    past the converged iteration (0, 0 and 7 when the policy is replayed on the oracle's runs of these
+    cases, against 3, 9 and 12 for batches of 16)."""
+    z, sp, H, x0 = _setup(gpu, orc, tag)
+    runs = {}
+    for batch in (1, 16):
+        lz = gpu.BasicLanczosAlgorithm(H, 1, 400)
+        lz.SetEigenvaluePrecision(precision)
+        lz.InitializeLanczosAlgorithm(x0)
+        r = lz.solve(400, graph_batch=batch)
+        assert r["converged"]
+        runs[batch] = (r["eigenvalues"][0], r["iterations"], lz.counters()[0])
+    (e1, it1, mv1), (e16, it16, mv16) = runs[1], runs[16]
+    assert it16 == it1
+    assert abs(e16 - e1) <= 1e-13 * abs(e1)
+    fixed = 3 + 16 * -(-(mv1 - 3) // 16)
+    assert mv1 <= mv16 <= min(fixed, mv1 + 8)
+
+
 def test_full_reorthogonalized(gpu, orc):
     z = golden("lanczos_n8_2s21_lz0_coulomb_full.npz")
     _, sp, H, x0 = _setup(gpu, orc, "n8_2s21_lz0_coulomb")
