@@ -733,19 +733,18 @@ int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eige
   const bool use_graph =
       graph_batch > 1 && l->algorithm != DH_LANCZOS_FULL_REORTHOGONALIZED && !l->lock_v0 && !l->disk;
   // The iterations of a batch past the converged row are discarded, so a batch is cut short where
-  // the convergence test is predicted to pass: the test's ratio to its threshold falls about
-  // geometrically once the lowest Ritz value converges, at a rate taken over the last kRateSpan
-  // rows (the ratio is sampled at each batch's end and kRateSpan rows before it), and the batch
-  // aims at kAim of the predicted rows.  A batch keeps at least kMinBatch iterations; one that ends
-  // short of convergence costs a host round trip, far less than an unneeded product.  (Replayed on
-  // the reference's Lanczos runs of seven FQHE sectors at four precisions, the products past
-  // convergence fall from 235 to 42 against batches of 16, for 140 round trips instead of 121.)
+  // the convergence test is predicted to pass (lanczos_batch_prediction): the test's ratio to its
+  // threshold falls about geometrically once the lowest Ritz value converges, at a rate taken over
+  // the last kLanczosRateSpan rows (the ratio is sampled at each batch's end and kLanczosRateSpan
+  // rows before it).  A batch that ends short of convergence costs a host round trip, far less than
+  // an unneeded product.  (Replayed on the reference's Lanczos runs of seven FQHE sectors at four
+  // precisions, the products past convergence fall from 235 to 42 against batches of 16, for 140
+  // round trips instead of 121.)
   // Under the residual test (the FP32 phase of the refined solve) the batches stay whole: there the
   // prediction saved no product (67 FP32 products either way at N = 12, 2S = 33, 1e-10).
   const bool adaptive = l->residual_target <= 0.0;
-  constexpr int kMinBatch = 2, kRateSpan = 6;
-  constexpr double kAim = 0.85;
-  std::vector<std::pair<int, double>> samples;  // (row, log ratio)
+  std::vector<int> sample_rows;
+  std::vector<double> sample_logs;
   int batch = graph_batch;
   while (!lz_converged(l) && count < max_iter) {
     if (!use_graph) {
@@ -798,9 +797,12 @@ int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eige
       l->rows = r;
       if ((rc = lz_finish_call(l)) != DH_OK) return rc;
       if (lz_converged(l) || count >= max_iter) break;
-      if (adaptive && (r == end_rows - kRateSpan || r == end_rows)) {
+      if (adaptive && (r == end_rows - kLanczosRateSpan || r == end_rows)) {
         const double ratio = lz_convergence_ratio(l);
-        if (ratio > 0.0) samples.emplace_back(r, log(ratio));
+        if (ratio > 0.0) {
+          sample_rows.push_back(r);
+          sample_logs.push_back(log(ratio));
+        }
       }
     }
     if (l->rows < end_rows) {
@@ -810,21 +812,8 @@ int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eige
       l->initialized = false;
     } else {
       batch = graph_batch;
-      if (!samples.empty() && samples.back().first == end_rows && samples.back().second > 0.0) {
-        const double lr = samples.back().second;
-        const std::pair<int, double>* ref = nullptr;
-        for (auto it = samples.rbegin() + 1; it != samples.rend(); ++it) {
-          ref = &*it;
-          if (end_rows - it->first >= kRateSpan) break;
-        }
-        if (ref) {
-          const double rate = (ref->second - lr) / (double)(end_rows - ref->first);  // log decrease per row
-          if (rate > 0.0) {
-            const double rows_left = ceil(kAim * lr / rate);
-            batch = (int)std::max((double)kMinBatch, std::min((double)graph_batch, rows_left));
-          }
-        }
-      }
+      if (!sample_rows.empty() && sample_rows.back() == end_rows)
+        batch = lanczos_batch_prediction((int)sample_rows.size(), sample_rows.data(), sample_logs.data(), graph_batch);
     }
   }
   if (l->disk) {

@@ -233,6 +233,13 @@ int band_eigenvalues(int n, int b, double* a, double* eig);
 // eigenvector of the symmetric band matrix a (dense storage, unchanged) for its eigenvalue lambda, by
 // inverse iteration with a banded LU (O(n b^2))
 int band_inverse_iteration(int n, int b, const double* a, double lambda, double* vec);
+// The next graph batch of the single-vector Lanczos solve, from the convergence test's ratio to its
+// threshold sampled as logarithms at rows rows[0..n) (the last at the newest replayed row): the
+// ratio decays about geometrically, the rate is taken over the last kLanczosRateSpan rows (or the
+// longest span sampled), and the batch aims at 0.85 of the rows predicted until the ratio reaches
+// 1, between 2 and graph_batch; graph_batch when nothing can be predicted.
+constexpr int kLanczosRateSpan = 6;
+int lanczos_batch_prediction(int n, const int* rows, const double* log_ratio, int graph_batch);
 
 int launch_fqhe_unrank(int nbr_fermions, int lz_max, int total_sum, long long dim, uint64_t* words,
                        const int64_t* counts_dev, int count_stride_o, int count_stride_s, cudaStream_t s);

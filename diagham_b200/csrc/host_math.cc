@@ -748,4 +748,21 @@ int band_inverse_iteration(int n, int b, const double* a, double lambda, double*
   return DH_OK;
 }
 
+// ------------------------------------------------------------ Lanczos batch sizes
+int lanczos_batch_prediction(int n, const int* rows, const double* log_ratio, int graph_batch) {
+  constexpr int kMinBatch = 2;
+  constexpr double kAim = 0.85;
+  if (n < 2 || graph_batch <= kMinBatch) return graph_batch;
+  const int end = rows[n - 1];
+  const double lr = log_ratio[n - 1];
+  if (!(lr > 0.0)) return graph_batch;  // passing already, or not a number
+  int ref = n - 2;
+  while (ref > 0 && end - rows[ref] < kLanczosRateSpan) --ref;
+  if (rows[ref] >= end) return graph_batch;
+  const double rate = (log_ratio[ref] - lr) / (double)(end - rows[ref]);  // log decrease per row
+  if (!(rate > 0.0)) return graph_batch;
+  const double rows_left = ceil(kAim * lr / rate);
+  return (int)std::max((double)kMinBatch, std::min((double)graph_batch, rows_left));
+}
+
 }  // namespace dh
