@@ -412,8 +412,11 @@ int dh_lanczos_get_counters(dh_lanczos_t l, int64_t* matvecs, int* rows);
 
 /* Whole driver loop of QHEOnSphereMainTask.cc:732-753: RunLanczosAlgorithm(nbrEigenvalue + 2), then
  * RunLanczosAlgorithm(1) until TestConvergence() or max_iter iterations, issued as CUDA-graph
- * batches of `graph_batch` iterations (>= 1) whose extra iterations past convergence are discarded
- * from the reported result.  *iterations follows the reference's iteration counter (in vectors:
+ * batches of at most `graph_batch` iterations (>= 1) whose extra iterations past convergence are
+ * discarded from the reported result.  Under the eigenvalue test a batch is cut short where the
+ * test is predicted to pass (its ratio to the threshold decays about geometrically), so fewer
+ * products are issued past convergence; the iterations, and so the results, are those of
+ * graph_batch = 1.  *iterations follows the reference's iteration counter (in vectors:
  * (nbrEigenvalue + 3) block_size after the first call, + block_size per step for DH_LANCZOS_BLOCK,
  * whose steps are never graph-batched). */
 int dh_lanczos_solve(dh_lanczos_t l, int max_iter, int graph_batch, double* eigenvalues, int* iterations,
