@@ -241,14 +241,24 @@ int lz_finish_call(dh_lanczos_s* l) {
     DH_CUDA(cudaMemcpyAsync(l->beta.data(), l->st.beta, (l->rows - 1) * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
   DH_CUDA(cudaStreamSynchronize(l->stream));
   const int nev = std::min(l->nev, l->rows);
-  std::vector<double> eig(l->rows);
+  std::vector<double> eig;
+  // one wanted value: the lowest from the previous call's (that of a leading block, an upper bound)
+  // by Newton steps, O(rows) where QL of the whole matrix is O(rows^2) per call
+  auto diagonalise = [&]() -> int {
+    if (l->nev == 1 && !l->ritz.empty()) {
+      eig.assign(1, 0.0);
+      return lanczos_lowest_ritz(l->rows, l->alpha.data(), l->beta.data(), &l->ritz[0], eig.data());
+    }
+    eig.assign(l->rows, 0.0);
+    return tridiagonal_eigen(l->rows, l->alpha.data(), l->beta.data(), eig.data(), nullptr);
+  };
   if (l->prev_last != 0.0) {
     l->prev_last = l->ritz[nev - 1];
     for (int i = 0; i < nev; ++i) l->prev_wanted[i] = l->ritz[i];
-    int rc = tridiagonal_eigen(l->rows, l->alpha.data(), l->beta.data(), eig.data(), nullptr);
+    int rc = diagonalise();
     if (rc != DH_OK) return rc;
   } else {
-    int rc = tridiagonal_eigen(l->rows, l->alpha.data(), l->beta.data(), eig.data(), nullptr);
+    int rc = diagonalise();
     if (rc != DH_OK) return rc;
     l->prev_last = 2.0 * eig[nev - 1];
     for (int i = 0; i < nev; ++i) l->prev_wanted[i] = 2.0 * eig[i];
@@ -644,6 +654,15 @@ int dh_lanczos_test_convergence(dh_lanczos_t l, int* converged) {
 
 int dh_lanczos_get_eigenvalues(dh_lanczos_t l, double* eigenvalues, int n) {
   DH_CHECK(l && eigenvalues, DH_ERR_ARGUMENT, "null argument");
+  if (!l->blk && n > (int)l->ritz.size() && n <= l->rows && (int)l->alpha.size() >= l->rows &&
+      (int)l->beta.size() >= l->rows - 1) {
+    // a run that wants one value keeps only the lowest: the others by QL of the current matrix
+    std::vector<double> eig(l->rows);
+    int rc = tridiagonal_eigen(l->rows, l->alpha.data(), l->beta.data(), eig.data(), nullptr);
+    if (rc != DH_OK) return rc;
+    for (int i = 0; i < n; ++i) eigenvalues[i] = eig[i];
+    return DH_OK;
+  }
   const std::vector<double>& ritz = l->blk ? block_lanczos_ritz(l->blk) : l->ritz;
   DH_CHECK(n >= 0 && n <= (int)ritz.size(), DH_ERR_ARGUMENT, "only %d Ritz values", (int)ritz.size());
   for (int i = 0; i < n; ++i) eigenvalues[i] = ritz[i];

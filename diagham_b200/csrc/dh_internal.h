@@ -233,6 +233,10 @@ int band_eigenvalues(int n, int b, double* a, double* eig);
 // eigenvector of the symmetric band matrix a (dense storage, unchanged) for its eigenvalue lambda, by
 // inverse iteration with a banded LU (O(n b^2))
 int band_inverse_iteration(int n, int b, const double* a, double lambda, double* vec);
+// The lowest Ritz value of a Lanczos tridiagonal matrix of n rows: from the previous lowest value (of
+// a leading block, an upper bound by interlacing) by safeguarded Newton steps, O(n); by implicit QL
+// when there is none, or when Newton returns the bound unchanged.
+int lanczos_lowest_ritz(int n, const double* diag, const double* off, const double* previous, double* lowest);
 // The next graph batch of the single-vector Lanczos solve, from the convergence test's ratio to its
 // threshold sampled as logarithms at rows rows[0..n) (the last at the newest replayed row): the
 // ratio decays about geometrically, the rate is taken over the last kLanczosRateSpan rows (or the

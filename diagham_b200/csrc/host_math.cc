@@ -748,6 +748,22 @@ int band_inverse_iteration(int n, int b, const double* a, double lambda, double*
   return DH_OK;
 }
 
+// ------------------------------------------------------------ Lanczos Ritz value per row
+int lanczos_lowest_ritz(int n, const double* diag, const double* off, const double* previous, double* lowest) {
+  if (previous) {
+    int rc = tridiagonal_lowest_below(n, diag, off, *previous, lowest);
+    if (rc != DH_OK) return rc;
+    if (*lowest != *previous) return DH_OK;
+    // the bound came back unchanged (the value moved by less than the Newton tolerance): the QL
+    // value, whose change the convergence test compares at full resolution
+  }
+  std::vector<double> eig(n);
+  int rc = tridiagonal_eigen(n, diag, off, eig.data(), nullptr);
+  if (rc != DH_OK) return rc;
+  *lowest = eig[0];
+  return DH_OK;
+}
+
 // ------------------------------------------------------------ Lanczos batch sizes
 int lanczos_batch_prediction(int n, const int* rows, const double* log_ratio, int graph_batch) {
   constexpr int kMinBatch = 2;

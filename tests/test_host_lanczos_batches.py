@@ -1,4 +1,4 @@
-"""The single-vector Lanczos solve's graph-batch sizes, on the CPU.
+"""The single-vector Lanczos solve's host logic on the CPU: graph-batch sizes and Ritz values.
 
 dh_lanczos_solve issues up to 16 iterations per CUDA-graph batch, then replays the reference's
 convergence test (BasicLanczosAlgorithm.cc:200-224: |E_r - E_{r-1}| < precision |E_r|) row by row on
@@ -7,7 +7,9 @@ dh::lanczos_batch_prediction (an internal C++ function of libdiagham_b200, reach
 Itanium C++ ABI name) over the test's ratio to its threshold, sampled at each batch's end and six
 rows before it.  Here the loop is replayed on the ratio sequences of Lanczos runs of the oracle's
 FQHE sectors (seeded start vectors, as the GPU tests use), and the products it issues are compared
-with fixed batches of 16.  No GPU is involved.
+with fixed batches of 16.  Each replayed row's lowest Ritz value comes from dh::lanczos_lowest_ritz
+(Newton steps from the previous row's value, QL where Newton returns that bound unchanged): the
+reference's test must stop at the same row as with QL values.  No GPU is involved.
 """
 import ctypes
 import math
@@ -121,3 +123,67 @@ def test_batches_against_fixed_batches(orc, predict):
             wasted["predicted"] += end - conv
     # 26 rows past convergence against 75 for batches of 16 over these eight runs
     assert wasted["predicted"] * 5 <= wasted["fixed"] * 2, wasted
+
+
+@pytest.fixture(scope="module")
+def lowest_ritz(dh):
+    lib = ctypes.CDLL(dh.library_path())
+    fn = lib._ZN2dh19lanczos_lowest_ritzEiPKdS1_S1_Pd
+    d = ctypes.POINTER(ctypes.c_double)
+    fn.argtypes = [ctypes.c_int, d, d, d, d]
+    fn.restype = ctypes.c_int
+
+    def call(alpha, beta, rows, previous=None):
+        out = np.zeros(1)
+        prev = None if previous is None else ctypes.pointer(ctypes.c_double(previous))
+        assert fn(rows, alpha.ctypes.data_as(d), beta.ctypes.data_as(d), prev, out.ctypes.data_as(d)) == 0
+        return out[0]
+    return call
+
+
+def converged_row(values, precision, first=FIRST + 1):
+    """BasicLanczosAlgorithm's test over (row, lowest value) pairs: the first passing row or None."""
+    prev = None
+    for r, e in values:
+        last = 2 * e if prev is None else prev
+        if r >= first and abs(e - last) < precision * abs(e):
+            return r
+        prev = e
+    return None
+
+
+@pytest.mark.parametrize("tag,nsl", [("n8_2s21_lz0_coulomb", (8, 21, 0)), ("n7_2s18_lz2_coulomb", (7, 18, 2)),
+                                     ("n8_2s21_lz0_v1", (8, 21, 0))])
+def test_lowest_ritz_stops_where_ql_stops(orc, lowest_ritz, tag, nsl):
+    """Same converged row as with QL values at every precision; on the V1 sector (E0 = 0, which the
+    reference runs to max_iter) neither converges."""
+    n, s, lz = nsl
+    z = golden("lanczos_%s_basic.npz" % tag)
+    system = orc.FQHE(n, s, lz, z["v"])
+    alpha, beta = lanczos_tridiagonal(system.pull, system.dim, orc.random_vector(0, system.dim), 200)
+    ql_values, values, prev = [], [], None
+    for rows in range(FIRST, 201):
+        t = np.diag(alpha[:rows]) + np.diag(beta[:rows - 1], 1) + np.diag(beta[:rows - 1], -1)
+        ql_values.append((rows, np.linalg.eigvalsh(t)[0]))
+        prev = lowest_ritz(alpha, beta, rows, prev)
+        values.append((rows, prev))
+    scale = np.max(np.abs(alpha)) + 2 * np.max(np.abs(beta))
+    assert max(abs(a[1] - b[1]) for a, b in zip(ql_values, values)) < 1e-13 * scale
+    for precision in (1e-14, 1e-13, 1e-12, 1e-10):
+        assert converged_row(values, precision) == converged_row(ql_values, precision)
+    if not bool(z["converged"]):
+        assert converged_row(values, 1e-14) is None
+
+
+def test_lowest_ritz_without_or_at_the_bound(lowest_ritz):
+    rng = np.random.default_rng(5)
+    alpha = rng.normal(size=40)
+    beta = rng.uniform(0.1, 1.0, 40)
+    t = np.diag(alpha) + np.diag(beta[:39], 1) + np.diag(beta[:39], -1)
+    ref = np.linalg.eigvalsh(t)[0]
+    assert abs(lowest_ritz(alpha, beta, 40) - ref) < 1e-13
+    # the bound equal to the value: Newton cannot improve on it, and the value comes from QL
+    assert abs(lowest_ritz(alpha, beta, 40, ref) - ref) < 1e-13
+    # the leading block's value as the bound
+    lead = np.linalg.eigvalsh(t[:30, :30])[0]
+    assert abs(lowest_ritz(alpha, beta, 40, lead) - ref) < 1e-13
